@@ -1,0 +1,572 @@
+/* ovl_oracle.c -- plain-C CPU restatement of the OVERLAP hot path (SU(2)).
+ *
+ * TEST INFRASTRUCTURE ONLY (see ovl_oracle.h).  Written from the definitions the
+ * reference implements, not from its code: quaternion algebra for SU(2), the
+ * Wilson operator as mass term + spin-projected hops, Wilson loops as
+ * path-ordered products anchored at a site.  Every function cites the reference
+ * routine it restates; tests/test_oracle_pin.py checks each one against the
+ * reference compiled from source.
+ */
+#define _DEFAULT_SOURCE
+#include "ovl_oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef double complex cplx;
+
+/* ---------------------------------------------------------------- lattice -- */
+
+static int wrap(int a, int n) { int r = a % n; return r < 0 ? r + n : r; }
+
+static int site_of(const orc_params *p, int x, int y, int z) {
+    return wrap(x, p->N[0]) + p->N[0] * (wrap(y, p->N[1]) + p->N[1] * wrap(z, p->N[2]));
+}
+
+static void coords_of(const orc_params *p, int s, int c[3]) {
+    c[0] = s % p->N[0];
+    c[1] = (s / p->N[0]) % p->N[1];
+    c[2] = s / (p->N[0] * p->N[1]);
+}
+
+static int shift(const orc_params *p, int s, int mu, int step) {
+    int c[3];
+    coords_of(p, s, c);
+    c[mu] += step;
+    return site_of(p, c[0], c[1], c[2]);
+}
+
+static int volume(const orc_params *p) { return p->N[0] * p->N[1] * p->N[2]; }
+
+/* ------------------------------------------------------- SU(2) quaternions -- */
+/* q = (v0, v1, v2, s) represents s*1 + i v_k sigma_k (GroupOperations.cpp:4-9). */
+
+typedef struct { double v[4]; } quat;
+
+static quat q_load(const double *U, int s, int mu) {
+    quat q;
+    memcpy(q.v, U + 4 * (mu + 3 * s), sizeof q.v);
+    return q;
+}
+
+static quat q_unit(void) { quat q = {{0.0, 0.0, 0.0, 1.0}}; return q; }
+
+static quat q_dag(quat a) { quat q = {{-a.v[0], -a.v[1], -a.v[2], a.v[3]}}; return q; }
+
+/* (a3 + i a.s)(b3 + i b.s) = a3 b3 - a.b + i (a3 b + b3 a - a x b).s */
+static quat q_mul(quat a, quat b) {
+    quat c;
+    c.v[3] = a.v[3] * b.v[3] - (a.v[0] * b.v[0] + a.v[1] * b.v[1] + a.v[2] * b.v[2]);
+    c.v[0] = a.v[3] * b.v[0] + b.v[3] * a.v[0] - (a.v[1] * b.v[2] - a.v[2] * b.v[1]);
+    c.v[1] = a.v[3] * b.v[1] + b.v[3] * a.v[1] - (a.v[2] * b.v[0] - a.v[0] * b.v[2]);
+    c.v[2] = a.v[3] * b.v[2] + b.v[3] * a.v[2] - (a.v[0] * b.v[1] - a.v[1] * b.v[0]);
+    return c;
+}
+
+/* 2x2 complex matrix of q, row-major m[i][j] (GetMatrix, GroupOperations.cpp:213-225). */
+static void q_matrix(quat q, cplx m[2][2]) {
+    m[0][0] = q.v[3] + I * q.v[2];
+    m[0][1] = q.v[1] + I * q.v[0];
+    m[1][0] = -q.v[1] + I * q.v[0];
+    m[1][1] = q.v[3] - I * q.v[2];
+}
+
+/* Re tr(i t^a q), t^a = sigma_a / 2 (ReTrIGenU, GroupOperations.cpp:78-84). */
+static double q_retr_ita(quat q, int a) { return -q.v[a]; }
+
+/* exp(i c alpha^a t^a) (MatrixIExp, SU2/AlgebraOperations.cpp:37-56). */
+static quat q_exp(double c, const double alpha[3]) {
+    double d = sqrt((c * alpha[0]) * (c * alpha[0]) + (c * alpha[1]) * (c * alpha[1]) + (c * alpha[2]) * (c * alpha[2]));
+    quat q;
+    if (d == 0.0) return q_unit();
+    double f = c * sin(0.5 * d) / d;
+    q.v[0] = f * alpha[0];
+    q.v[1] = f * alpha[1];
+    q.v[2] = f * alpha[2];
+    q.v[3] = cos(0.5 * d);
+    return q;
+}
+
+/* Adjoint representation R_ab = 2 tr(t^a q t^b q^+), evaluated with matrices. */
+static void q_adjoint(quat q, double R[3][3]) {
+    static const cplx sig[3][2][2] = {
+        {{0, 1}, {1, 0}},
+        {{0, -I}, {I, 0}},
+        {{1, 0}, {0, -1}},
+    };
+    cplx m[2][2], md[2][2];
+    q_matrix(q, m);
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) md[i][j] = conj(m[j][i]);
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            cplx tr = 0;
+            for (int i = 0; i < 2; i++)
+                for (int j = 0; j < 2; j++)
+                    for (int k = 0; k < 2; k++)
+                        for (int l = 0; l < 2; l++)
+                            tr += 0.5 * sig[a][i][j] * m[j][k] * 0.5 * sig[b][k][l] * md[l][i];
+            R[a][b] = 2.0 * creal(tr);
+        }
+}
+
+/* Path-ordered product of links along `nsteps` unit steps starting at site s:
+ * step (mu, +1) multiplies by U_mu(x), step (mu, -1) by U_mu(x - mu)^+. */
+typedef struct { int mu, dir, len; } leg;
+
+static quat q_path(const orc_params *p, const double *U, int s, const leg *legs, int nlegs) {
+    quat acc = q_unit();
+    int x = s;
+    for (int l = 0; l < nlegs; l++)
+        for (int k = 0; k < legs[l].len; k++) {
+            if (legs[l].dir > 0) {
+                acc = q_mul(acc, q_load(U, x, legs[l].mu));
+                x = shift(p, x, legs[l].mu, +1);
+            } else {
+                x = shift(p, x, legs[l].mu, -1);
+                acc = q_mul(acc, q_dag(q_load(U, x, legs[l].mu)));
+            }
+        }
+    return acc;
+}
+
+/* Counter-clockwise (first +mu, then +nu) lmu x lnu loop in the (mu, nu) plane
+ * with site s at its corner in quadrant (smu, snu), holonomy based at s. */
+static quat q_loop(const orc_params *p, const double *U, int s, int mu, int nu, int smu, int snu, int lmu, int lnu) {
+    leg ccw[4] = {{mu, +1, lmu}, {nu, +1, lnu}, {mu, -1, lmu}, {nu, -1, lnu}};
+    /* index of the leg that leaves the corner s when walking counter-clockwise */
+    int start = (smu > 0 && snu > 0) ? 0 : (smu < 0 && snu > 0) ? 1 : (smu < 0 && snu < 0) ? 2 : 3;
+    leg legs[4];
+    for (int k = 0; k < 4; k++) legs[k] = ccw[(start + k) % 4];
+    return q_path(p, U, s, legs, 4);
+}
+
+/* ----------------------------------------------------------- Dirac algebra -- */
+/* Dirac representation (DiracAlgebra.cpp:5-12). */
+static const cplx G0[4][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, -1, 0}, {0, 0, 0, -1}};
+static const cplx GX[4][4] = {{0, 0, 0, 1}, {0, 0, 1, 0}, {0, -1, 0, 0}, {-1, 0, 0, 0}};
+static const cplx GY[4][4] = {{0, 0, 0, -I}, {0, 0, I, 0}, {0, I, 0, 0}, {-I, 0, 0, 0}};
+static const cplx GZ[4][4] = {{0, 0, 1, 0}, {0, 0, 0, -1}, {-1, 0, 0, 0}, {0, 1, 0, 0}};
+static const cplx G5[4][4] = {{0, 0, 1, 0}, {0, 0, 0, 1}, {1, 0, 0, 0}, {0, 1, 0, 0}};
+
+static void mat4_mul(const cplx a[4][4], const cplx b[4][4], cplx c[4][4]) {
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+            cplx t = 0;
+            for (int k = 0; k < 4; k++) t += a[i][k] * b[k][j];
+            c[i][j] = t;
+        }
+}
+
+static void mat4_scale(cplx f, const cplx a[4][4], cplx c[4][4]) {
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) c[i][j] = f * a[i][j];
+}
+
+/* ------------------------------------------------------------ Wilson h_W -- */
+
+#define NC 2
+#define SPINOR (NC * 4)  /* complex numbers per site and mode */
+
+static const cplx *site_spinor(const double *field, int s) { return (const cplx *)field + (size_t)SPINOR * s; }
+
+void orc_wilson_apply(const orc_params *p, const double *U, const double *phi, double *out) {
+    const int V = volume(p);
+    /* Spin structure of the symmetric difference U phi(x+mu) - U^+ phi(x-mu):
+     * the hop term is  -(1 - G_mu) a - (1 + G_mu) b  with a = U_mu(x) phi(x+mu),
+     * b = U_mu(x-mu)^+ phi(x-mu) and G_mu = -i gamma_mu, hermitian with
+     * G_mu^2 = 1 (WilsonOperator.cpp:79-98).  Mass term (6r + 2m - 2M) phi
+     * (:39), overall factor -i gamma_0 / 2 (:100-109). */
+    cplx G[3][4][4];
+    mat4_scale(-I, GX, G[0]);
+    mat4_scale(-I, GY, G[1]);
+    mat4_scale(-I, GZ, G[2]);
+    const double amass = 6.0 * p->r_wilson + 2.0 * p->m_fermion - 2.0 * p->m_dw;
+    for (int s = 0; s < V; s++) {
+        const cplx *f = site_spinor(phi, s);
+        cplx acc[NC][4];
+        for (int c = 0; c < NC; c++)
+            for (int a = 0; a < 4; a++) acc[c][a] = amass * f[4 * c + a];
+        for (int mu = 0; mu < 3; mu++) {
+            cplx Mf[2][2], Mb[2][2];
+            q_matrix(q_load(U, s, mu), Mf);
+            int sb = shift(p, s, mu, -1);
+            q_matrix(q_load(U, sb, mu), Mb);
+            const cplx *fp = site_spinor(phi, shift(p, s, mu, +1));
+            const cplx *fm = site_spinor(phi, sb);
+            cplx a[NC][4], b[NC][4];
+            for (int i = 0; i < NC; i++)
+                for (int al = 0; al < 4; al++) {
+                    a[i][al] = 0;
+                    b[i][al] = 0;
+                    for (int j = 0; j < NC; j++) {
+                        a[i][al] += Mf[i][j] * fp[4 * j + al];
+                        b[i][al] += conj(Mb[j][i]) * fm[4 * j + al];
+                    }
+                }
+            for (int i = 0; i < NC; i++)
+                for (int al = 0; al < 4; al++) {
+                    cplx g = 0;
+                    for (int be = 0; be < 4; be++) g += G[mu][al][be] * (a[i][be] - b[i][be]);
+                    acc[i][al] += -a[i][al] - b[i][al] + g;
+                }
+        }
+        cplx *o = (cplx *)out + (size_t)SPINOR * s;
+        for (int c = 0; c < NC; c++)
+            for (int a = 0; a < 4; a++) o[4 * c + a] = (a < 2 ? -0.5 * I : 0.5 * I) * acc[c][a];
+    }
+}
+
+/* ----------------------------------------------------------- gauge update -- */
+
+void orc_update_links(const orc_params *p, double *U, const double *E, double dt_step) {
+    const int V = volume(p);
+    /* cU = -dt g_mumu a_mu^2 / (sqrt(-g) a^3) = -dt for Minkowski, a = 1 (Dynamics.cpp:102-104). */
+    const double cU = -dt_step;
+    for (int s = 0; s < V; s++)
+        for (int mu = 0; mu < 3; mu++) {
+            quat e = q_exp(cU, E + 3 * (mu + 3 * s));
+            quat u = q_mul(e, q_load(U, s, mu));
+            memcpy(U + 4 * (mu + 3 * s), u.v, sizeof u.v);
+        }
+}
+
+void orc_update_efield(const orc_params *p, const double *U, double *E, double dt_step) {
+    const int V = volume(p);
+    const double gamma = -2.0 * dt_step;  /* -2 dt sqrt(-g) a^3, Dynamics.cpp:150 */
+    double *dE = malloc(sizeof(double) * 9 * (size_t)V);
+    for (int s = 0; s < V; s++)
+        for (int mu = 0; mu < 3; mu++)
+            for (int a = 0; a < 3; a++) {
+                double f = 0.0;
+                for (int nu = 0; nu < 3; nu++) {
+                    if (nu == mu) continue;
+                    /* the two staples of U_mu(x) in the (mu, nu) plane, both
+                     * written to start with U_mu(x) */
+                    leg up[4] = {{mu, +1, 1}, {nu, +1, 1}, {mu, -1, 1}, {nu, -1, 1}};
+                    leg dn[4] = {{mu, +1, 1}, {nu, -1, 1}, {mu, -1, 1}, {nu, +1, 1}};
+                    f += q_retr_ita(q_path(p, U, s, up, 4), a) + q_retr_ita(q_path(p, U, s, dn, 4), a);
+                }
+                dE[a + 3 * (mu + 3 * s)] = gamma * f;
+            }
+    for (size_t k = 0; k < 9 * (size_t)V; k++) E[k] += dE[k];
+    free(dE);
+}
+
+/* --------------------------------------------------------------- leapfrog -- */
+
+static void half_step(const orc_params *p, const double *U, const double *src, double *dst, int nmodes, double *work) {
+    const int V = volume(p);
+    const size_t per_mode = (size_t)2 * SPINOR * V;
+    for (int m = 0; m < nmodes; m++) {
+        orc_wilson_apply(p, U, src + per_mode * m, work);
+        double *d = dst + per_mode * m;
+        for (size_t k = 0; k < per_mode; k++) d[k] += p->dt * work[k];
+    }
+}
+
+void orc_wilson_leapfrog(const orc_params *p, double *U, const double *E, double *psi, double *psimid,
+                         int nmodes, int *tsteps, int nsteps) {
+    double *work = malloc(sizeof(double) * 2 * SPINOR * (size_t)volume(p));
+    for (int n = 0; n < nsteps; n++) {
+        /* Update.cpp:48-79: psi += dt D(psimid); links 1/2; psimid += dt D(psi); links 1/2. */
+        half_step(p, U, psimid, psi, nmodes, work);
+        if (p->qs * (*tsteps * p->dt) < p->t_sphaleron) orc_update_links(p, U, E, 0.5 * p->dt);
+        half_step(p, U, psi, psimid, nmodes, work);
+        if (p->qs * (*tsteps * p->dt) < p->t_sphaleron) orc_update_links(p, U, E, 0.5 * p->dt);
+        (*tsteps)++;
+    }
+    free(work);
+}
+
+/* ------------------------------------------------------------ plane waves -- */
+
+static int free_spinor(const orc_params *p, const int k[3], int spin, int particle, cplx u[4], double *omega) {
+    const double TWO_PI = 2.0 * M_PI;
+    double pp[3], meff = p->m_fermion, p2 = 0.0;
+    for (int i = 0; i < 3; i++) {
+        int n = particle == 0 ? k[i] : p->N[i] - k[i];  /* antiparticles carry -p (FermionField.cpp:168-174) */
+        pp[i] = sin(TWO_PI * n / (double)p->N[i]);
+        double h = sin(M_PI * n / (double)p->N[i]);
+        meff += 2.0 * p->r_wilson * h * h;
+        p2 += pp[i] * pp[i];
+    }
+    double pabs = sqrt(p2);
+    double w = sqrt(p2 + meff * meff);
+    *omega = particle == 0 ? w : -w;
+
+    int edge[3];
+    for (int i = 0; i < 3; i++) edge[i] = (k[i] == 0 || 2 * k[i] == p->N[i]);
+    /* two-spinor of definite helicity (:185-226) */
+    cplx phi[2];
+    double hel;
+    if (edge[0] && edge[1]) {
+        if (spin == 0) { phi[0] = 1; phi[1] = 0; hel = pp[2] / fabs(pp[2]); }
+        else { phi[0] = 0; phi[1] = 1; hel = -pp[2] / fabs(pp[2]); }
+        if (edge[2]) hel = 0.0;
+    } else {
+        hel = spin == 0 ? 1.0 : -1.0;
+        cplx q = -(pp[2] - hel * pabs) / (pp[0] - I * pp[1]);
+        double d = sqrt(1.0 + creal(q) * creal(q) + cimag(q) * cimag(q));
+        phi[0] = 1.0 / d;
+        phi[1] = q / d;
+    }
+    /* four-spinor (:228-268) */
+    if (edge[0] && edge[1] && edge[2]) {
+        int upper = (particle == 0) == (meff >= 0);
+        u[0] = upper ? phi[0] : 0; u[1] = upper ? phi[1] : 0;
+        u[2] = upper ? 0 : phi[0]; u[3] = upper ? 0 : phi[1];
+    } else {
+        double norm = sqrt(2.0 * (*omega) * ((*omega) - meff) / p2);
+        u[0] = phi[0] / norm;
+        u[1] = phi[1] / norm;
+        u[2] = hel * ((*omega) - meff) / pabs * (phi[0] / norm);
+        u[3] = hel * ((*omega) - meff) / pabs * (phi[1] / norm);
+    }
+    /* eigen-residual and normalisation (:270-312) with H = gamma_0 (meff + p.gamma) */
+    cplx H[4][4], t[4][4];
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++) t[a][b] = meff * (a == b) + pp[0] * GX[a][b] + pp[1] * GY[a][b] + pp[2] * GZ[a][b];
+    mat4_mul(G0, t, H);
+    int bad = 0;
+    for (int a = 0; a < 4; a++) {
+        cplx hu = 0;
+        for (int b = 0; b < 4; b++) hu += H[a][b] * u[b];
+        if (cabs((*omega) * u[a] - hu) > 1e-6) bad = 1;
+    }
+    double n2 = 0;
+    for (int a = 0; a < 4; a++) n2 += creal(u[a]) * creal(u[a]) + cimag(u[a]) * cimag(u[a]);
+    if (fabs(n2 - 1.0) > 1e-6) bad = 1;
+    return bad;
+}
+
+int orc_free_fermions(const orc_params *p, int first, int nmodes, double *psi, double *psimid) {
+    const int V = volume(p);
+    int failures = 0;
+    for (int m = 0; m < nmodes; m++) {
+        /* mode index = particle + 2(colour + Nc(spin + 2(px + N0(py + N1 pz)))) (FermionField.cpp:38-60) */
+        int g = first + m;
+        int particle = g % 2; g /= 2;
+        int colour = g % NC; g /= NC;
+        int spin = g % 2; g /= 2;
+        int k[3];
+        k[0] = g % p->N[0]; g /= p->N[0];
+        k[1] = g % p->N[1]; g /= p->N[1];
+        k[2] = g % p->N[2];
+        cplx u[4];
+        double omega;
+        failures += free_spinor(p, k, spin, particle, u, &omega);
+        cplx half = cexp(-0.5 * I * omega * p->dt);
+        cplx *f = (cplx *)psi + (size_t)SPINOR * V * m;
+        cplx *fm = (cplx *)psimid + (size_t)SPINOR * V * m;
+        for (int s = 0; s < V; s++) {
+            int c[3];
+            coords_of(p, s, c);
+            double arg = (k[0] * c[0]) / (double)p->N[0] + (k[1] * c[1]) / (double)p->N[1] + (k[2] * c[2]) / (double)p->N[2];
+            double th = (particle == 0 ? 2.0 : -2.0) * M_PI * arg;
+            cplx phase = cos(th) + I * sin(th);
+            for (int cc = 0; cc < NC; cc++)
+                for (int a = 0; a < 4; a++) {
+                    cplx v = cc == colour ? phase * u[a] : 0;
+                    f[SPINOR * s + 4 * cc + a] = v;
+                    fm[SPINOR * s + 4 * cc + a] = cc == colour ? v * half : 0;
+                }
+        }
+    }
+    return failures;
+}
+
+/* --------------------------------------------------------------- currents -- */
+
+/* sum_{colour i,j} sum_{alpha beta} g[alpha][beta] M[i][j] conj(f_alpha^i) h_beta^j */
+static cplx bilinear(const cplx g[4][4], const cplx M[2][2], const cplx *f, const cplx *h) {
+    cplx t = 0;
+    for (int i = 0; i < NC; i++)
+        for (int j = 0; j < NC; j++) {
+            if (M[i][j] == 0) continue;
+            for (int a = 0; a < 4; a++)
+                for (int b = 0; b < 4; b++)
+                    if (g[a][b] != 0) t += g[a][b] * M[i][j] * conj(f[4 * i + a]) * h[4 * j + b];
+        }
+    return t;
+}
+
+void orc_wilson_currents(const orc_params *p, const double *U, const double *psi, int nmodes, int first,
+                         double *jV, double *jA, double *jVw, double *jAw, double *PS, double *WA) {
+    const int V = volume(p);
+    /* couplings (Currents.cpp:44-92) */
+    const cplx (*Gmu[3])[4] = {GX, GY, GZ};
+    cplx gV[4][4][4], gA[4][4][4], gPS[4][4], gVw[4][4], gAw[4][4], t[4][4];
+    mat4_mul(G0, G0, gV[0]);
+    for (int mu = 0; mu < 3; mu++) mat4_mul(G0, Gmu[mu], gV[mu + 1]);
+    for (int mu = 0; mu < 4; mu++) mat4_mul(gV[mu], G5, gA[mu]);
+    mat4_mul(G0, G5, t);
+    mat4_scale(I, t, gPS);
+    mat4_scale(-I * p->r_wilson, G0, gVw);
+    mat4_scale(-I * p->r_wilson, t, gAw);
+    const cplx one[2][2] = {{1, 0}, {0, 1}};
+
+    double *out[6] = {jV, jA, jVw, jAw, PS, WA};
+    size_t len[6] = {4 * (size_t)V, 4 * (size_t)V, 4 * (size_t)V, 4 * (size_t)V, (size_t)V, (size_t)V};
+    for (int k = 0; k < 6; k++)
+        if (out[k]) memset(out[k], 0, sizeof(double) * len[k]);
+    const double pre = 1.0 / (2.0 * V);
+    for (int m = 0; m < nmodes; m++) {
+        const double w = ((first + m) % 2 == 0) ? 1.0 : -1.0;  /* CommutatorExpectationValue, FermionField.cpp:109-122 */
+        const cplx *mode = (const cplx *)psi + (size_t)SPINOR * V * m;
+        for (int s = 0; s < V; s++) {
+            const cplx *f = mode + SPINOR * s;
+            cplx jv[4], ja[4], wv[4] = {0, 0, 0, 0}, wa[4] = {0, 0, 0, 0};
+            jv[0] = w * bilinear(gV[0], one, f, f);
+            ja[0] = w * bilinear(gA[0], one, f, f);
+            cplx ps = w * bilinear(gPS, one, f, f);
+            cplx anomaly = -2.0 * 3.0 * w * bilinear(gAw, one, f, f);
+            for (int mu = 0; mu < 3; mu++) {
+                cplx Mf[2][2], Mb[2][2], Mbd[2][2];
+                q_matrix(q_load(U, s, mu), Mf);
+                int sb = shift(p, s, mu, -1);
+                q_matrix(q_load(U, sb, mu), Mb);
+                for (int i = 0; i < 2; i++)
+                    for (int j = 0; j < 2; j++) Mbd[i][j] = conj(Mb[j][i]);
+                const cplx *fp = mode + SPINOR * shift(p, s, mu, +1);
+                const cplx *fm = mode + SPINOR * sb;
+                jv[mu + 1] = w * bilinear(gV[mu + 1], Mf, f, fp);
+                ja[mu + 1] = w * bilinear(gA[mu + 1], Mf, f, fp);
+                wv[mu + 1] = w * bilinear(gVw, Mf, f, fp);
+                wa[mu + 1] = w * bilinear(gAw, Mf, f, fp);
+                anomaly += wa[mu + 1] + w * bilinear(gAw, Mbd, f, fm);
+            }
+            for (int mu = 0; mu < 4; mu++) {
+                if (jV) jV[mu + 4 * s] += pre * creal(jv[mu]);
+                if (jA) jA[mu + 4 * s] += pre * creal(ja[mu]);
+                if (jVw && mu > 0) jVw[mu + 4 * s] += pre * creal(wv[mu]);
+                if (jAw && mu > 0) jAw[mu + 4 * s] += pre * creal(wa[mu]);
+            }
+            if (PS) PS[s] += pre * creal(ps);
+            if (WA) WA[s] += pre * creal(anomaly);
+        }
+    }
+}
+
+/* -------------------------------------------------------------- E.B, NCs -- */
+
+/* Improved colour-electric field on the mu link at s: weights -1/12, 7/12, 7/12,
+ * -1/12 on E_mu at s+mu, s, s-mu, s-2mu, each transported to s in the adjoint
+ * (ChernSimonsOperators.cpp:379-401). */
+static void improved_e(const orc_params *p, const double *U, const double *E, int s, int mu, double out[3]) {
+    const int sp = shift(p, s, mu, +1), sm = shift(p, s, mu, -1), smm = shift(p, s, mu, -2);
+    double Rp[3][3], Rm[3][3], Rmm[3][3];
+    q_adjoint(q_load(U, s, mu), Rp);                                 /* s+mu -> s */
+    q_adjoint(q_dag(q_load(U, sm, mu)), Rm);                         /* s-mu -> s */
+    q_adjoint(q_mul(q_dag(q_load(U, sm, mu)), q_dag(q_load(U, smm, mu))), Rmm);  /* s-2mu -> s */
+    const double *ep = E + 3 * (mu + 3 * sp), *e0 = E + 3 * (mu + 3 * s);
+    const double *em = E + 3 * (mu + 3 * sm), *emm = E + 3 * (mu + 3 * smm);
+    for (int a = 0; a < 3; a++) {
+        double t = (7.0 / 12.0) * e0[a];
+        for (int b = 0; b < 3; b++)
+            t += -(1.0 / 12.0) * Rp[a][b] * ep[b] + (7.0 / 12.0) * Rm[a][b] * em[b] - (1.0 / 12.0) * Rmm[a][b] * emm[b];
+        out[a] = t;
+    }
+}
+
+/* Improved colour-magnetic field B_k for the (mu, nu) plane: 5/12 of the four
+ * plaquettes and -1/24 of the eight 2x1 rectangles with s at a corner, all
+ * counter-clockwise and based at s; B^a = 2 Re tr(i t^a avg)
+ * (ChernSimonsOperators.cpp:283-421). */
+static void improved_b(const orc_params *p, const double *U, int s, int mu, int nu, double out[3]) {
+    double avg[4] = {0, 0, 0, 0};
+    const int sg[4][2] = {{+1, +1}, {-1, +1}, {-1, -1}, {+1, -1}};
+    for (int q = 0; q < 4; q++) {
+        quat box = q_loop(p, U, s, mu, nu, sg[q][0], sg[q][1], 1, 1);
+        quat r1 = q_loop(p, U, s, mu, nu, sg[q][0], sg[q][1], 2, 1);
+        quat r2 = q_loop(p, U, s, mu, nu, sg[q][0], sg[q][1], 1, 2);
+        for (int k = 0; k < 4; k++) avg[k] += (5.0 / 12.0) * box.v[k] - (1.0 / 24.0) * (r1.v[k] + r2.v[k]);
+    }
+    quat a4 = {{avg[0], avg[1], avg[2], avg[3]}};
+    for (int a = 0; a < 3; a++) out[a] = 2.0 * q_retr_ita(a4, a);
+}
+
+double orc_ncsdot(const orc_params *p, const double *U, const double *E) {
+    const int V = volume(p);
+    double edotb = 0.0;
+    for (int s = 0; s < V; s++) {
+        double e[3][3], b[3][3];
+        for (int mu = 0; mu < 3; mu++) improved_e(p, U, E, s, mu, e[mu]);
+        improved_b(p, U, s, 1, 2, b[0]);  /* B_x from the yz plane */
+        improved_b(p, U, s, 2, 0, b[1]);  /* B_y from the zx plane */
+        improved_b(p, U, s, 0, 1, b[2]);  /* B_z from the xy plane */
+        for (int mu = 0; mu < 3; mu++) edotb += e[mu][0] * b[mu][0] + e[mu][1] * b[mu][1] + e[mu][2] * b[mu][2];
+    }
+    return 0.125 * edotb / (M_PI * M_PI);
+}
+
+/* -------------------------------------------------- energy, Gauss, unitarity -- */
+
+void orc_bulk(const orc_params *p, const double *U, const double *E, double *out) {
+    const int V = volume(p);
+    double e2[3] = {0, 0, 0}, b2[3] = {0, 0, 0};
+    double gmax = 0.0, gsum = 0.0, umax = 0.0, usum = 0.0;
+    for (int s = 0; s < V; s++) {
+        for (int mu = 0; mu < 3; mu++)
+            for (int a = 0; a < 3; a++) e2[mu] += E[a + 3 * (mu + 3 * s)] * E[a + 3 * (mu + 3 * s)];
+        /* B_k^2 from the plaquette orthogonal to k: 4 Re tr(1 - U_plaq) (BulkObservables.cpp:72-77) */
+        const int planes[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+        for (int k = 0; k < 3; k++) {
+            quat pl = q_loop(p, U, s, planes[k][0], planes[k][1], +1, +1, 1, 1);
+            b2[k] += 4.0 * 2.0 * (1.0 - pl.v[3]);
+        }
+        /* G^a = sum_mu E_mu(s) - (U^+ E U)(s - mu) */
+        double g[3] = {0, 0, 0};
+        for (int mu = 0; mu < 3; mu++) {
+            int sm = shift(p, s, mu, -1);
+            double R[3][3];
+            q_adjoint(q_dag(q_load(U, sm, mu)), R);
+            for (int a = 0; a < 3; a++) {
+                double t = E[a + 3 * (mu + 3 * s)];
+                for (int b = 0; b < 3; b++) t -= R[a][b] * E[b + 3 * (mu + 3 * sm)];
+                g[a] += t;
+            }
+        }
+        for (int a = 0; a < 3; a++) {
+            if (g[a] > gmax) gmax = g[a];  /* signed maximum, as GaussLawViolation.cpp:44 */
+            gsum += g[a] * g[a];
+        }
+        for (int mu = 0; mu < 3; mu++) {
+            quat u = q_load(U, s, mu);
+            double dev = fabs(u.v[0] * u.v[0] + u.v[1] * u.v[1] + u.v[2] * u.v[2] + u.v[3] * u.v[3] - 1.0);
+            if (dev > umax) umax = dev;
+            usum += dev * dev;
+        }
+    }
+    for (int k = 0; k < 3; k++) { e2[k] /= V; b2[k] /= V; }
+    out[0] = 0.5 * (e2[0] + e2[1] + e2[2] + b2[0] + b2[1] + b2[2]);
+    out[1] = 0.5 * ((e2[1] + e2[2] + b2[1] + b2[2]) - (e2[0] + b2[0]));
+    out[2] = 0.5 * ((e2[0] + e2[2] + b2[0] + b2[2]) - (e2[1] + b2[1]));
+    out[3] = 0.5 * ((e2[0] + e2[1] + b2[0] + b2[1]) - (e2[2] + b2[2]));
+    out[4] = 0.5 * (e2[0] + e2[1] + e2[2]);
+    out[5] = 0.5 * (b2[0] + b2[1] + b2[2]);
+    out[6] = gmax;
+    out[7] = sqrt(gsum / (3.0 * V));
+    out[8] = umax;
+    out[9] = sqrt(usum / (3.0 * V));
+}
+
+void orc_u1_flux(const orc_params *p, int nb, double *out) {
+    const int N0 = p->N[0], N1 = p->N[1];
+    cplx *u = (cplx *)out;
+    for (int y = 0; y < N1; y++)
+        for (int x = 0; x < N0; x++) {
+            /* U_y = exp(-2 pi i nb x / (N0 N1)); U_x = 1 except the x = N0-1 column,
+             * which carries exp(2 pi i nb y N0 / (N0 N1)) (QED.cpp:62-84) */
+            double ty = -2.0 * M_PI * (double)(nb * x) / (double)(N0 * N1);
+            u[1 + 2 * (x + N0 * y)] = cos(ty) + I * sin(ty);
+            if (x == N0 - 1) {
+                double tx = 2.0 * M_PI * (double)(nb * y * N0) / (double)(N0 * N1);
+                u[0 + 2 * (x + N0 * y)] = cos(tx) + I * sin(tx);
+            } else {
+                u[0 + 2 * (x + N0 * y)] = 1.0;
+            }
+        }
+}

@@ -1,0 +1,81 @@
+/* ovl_oracle: plain-C CPU restatement of the OVERLAP fermion-gauge hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline leg of bench.py may load this library, and only as the checker.
+ * The product (overlap_b200) never links or calls it.
+ *
+ * Pinned against the reference's own code: tests/test_oracle_pin.py compares
+ * every function below with the reference compiled from source
+ * (oracle/_ref/libovlref_*.so, built by oracle/Makefile) and with the golden
+ * vectors under tests/golden/ that the reference produced.
+ *
+ * Conventions (all the reference's, SU(2), lattice spacing 1, Minkowski metric):
+ *   site       = x + N0*(y + N1*z)                     LATTICE/GaugeLinks.cpp:27-36
+ *   links U    = double[4] per (site, mu) at 4*(mu+3*site); U = u3 + i u_k sigma_k
+ *                                                      SUNc/SU2/GroupOperations.cpp:4-9
+ *   E field    = double[3] per (site, mu) at a+3*(mu+3*site)   LATTICE/ElectricFields.cpp:36-42
+ *   modes      = per mode V sites x [colour 2][spin 4] complex (re,im)
+ *                                                      FERMIONS/FermionField.cpp:8-9
+ */
+#ifndef OVL_ORACLE_H
+#define OVL_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int N[3];
+    double r_wilson;     /* rWilson */
+    double m_fermion;    /* mFermion */
+    double m_dw;         /* MDWHeight */
+    double dt;           /* Dynamics::dTau */
+    double qs;           /* Qs: Time() = qs * tsteps * dt */
+    double t_sphaleron;  /* links move while Time() < t_sphaleron */
+} orc_params;
+
+/* out = -i h_W phi for one mode (WilsonEvoOperator::Compute, WilsonOperator.cpp:30-114). */
+void orc_wilson_apply(const orc_params *p, const double *U, const double *phi, double *out);
+
+/* U <- exp(-i dt_step E^a t^a) U on every link (Dynamics::UpdateGaugeLinks,
+ * DYNAMICS/Dynamics.cpp:97-138). */
+void orc_update_links(const orc_params *p, double *U, const double *E, double dt_step);
+
+/* E += staple force (Dynamics::UpdateElectricFields, Dynamics.cpp:145-197, with
+ * the plaquette conventions of oracle/ref/ovl_calc_macros.h). */
+void orc_update_efield(const orc_params *p, const double *U, double *E, double dt_step);
+
+/* nsteps of Dynamics::Fermions::Update (FERMIONS/WILSON/Update.cpp:48-79) on
+ * nmodes modes; *tsteps is the step counter read by Time(). */
+void orc_wilson_leapfrog(const orc_params *p, double *U, const double *E, double *psi, double *psimid,
+                         int nmodes, int *tsteps, int nsteps);
+
+/* InitialConditions::SetFreeFermions for global modes first..first+nmodes-1
+ * (SetFreeFermions.cpp:3-56, FermionField.cpp:145-328).  Returns the number of
+ * modes whose eigen-residual or normalisation check failed (the reference prints
+ * these, FermionField.cpp:297-312). */
+int orc_free_fermions(const orc_params *p, int first, int nmodes, double *psi, double *psimid);
+
+/* Fermions::Observables::ComputeCurrents, Wilson (FERMIONS/WILSON/Currents.cpp:7-309):
+ * jV,jA,jVw,jAw: 4V doubles (component mu + 4*site), PS,WA: V doubles.  Any
+ * pointer may be NULL.  first = global index of local mode 0 (vacuum sign). */
+void orc_wilson_currents(const orc_params *p, const double *U, const double *psi, int nmodes, int first,
+                         double *jV, double *jA, double *jVw, double *jAw, double *PS, double *WA);
+
+/* ChernSimonsNumber::NCsDot: improved E.B / (8 pi^2)
+ * (CALC/ChernSimonsOperators.cpp:128-439, TOPOLOGY/ChernSimonsDerivative.cpp:31-49). */
+double orc_ncsdot(const orc_params *p, const double *U, const double *E);
+
+/* Observables::Bulk, GaussLaw, Unitarity (OBSERVABLES/BulkObservables.cpp,
+ * GaussLawViolation.cpp, UnitarityViolation.cpp):
+ * out = {T00, TXX, TYY, TZZ, E part, B part, gauss max, gauss avg, unit max, unit avg}. */
+void orc_bulk(const orc_params *p, const double *U, const double *E, double *out);
+
+/* QED::SetConstantMagneticField (QED/QED.cpp:62-84): out = 2*N0*N1 complex,
+ * index mu + 2*(x + N0*y). */
+void orc_u1_flux(const orc_params *p, int nb, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,290 @@
+/* Reference harness: compiles markmace/OVERLAP's own hot-path sources (found on
+ * the include path, never copied) into a shared library with a small C API.
+ * TEST INFRASTRUCTURE ONLY: the product never links or calls this library; the
+ * tests use it as the checker and bench.py times it as the CPU reference arm.
+ *
+ * Build: oracle/Makefile (one library per fermion kind, FERMION_FLAG=666 Wilson,
+ * 777 overlap).  Deviations from the reference build, each forced by the tree:
+ *  - stub mpi.h / gsl / fftw3.h headers (single process; see oracle/ref/stub);
+ *  - restated CALC macros (oracle/ref/ovl_calc_macros.h), missing from the tree;
+ *  - Dynamics::dTau is `static const 0.02` (DYNAMICS/Dynamics.cpp:17); every file
+ *    included after Dynamics.cpp sees `dTau` and `Time` redirected to runtime
+ *    values (harness_dt, harness_time) by macro, so the fermion leapfrog
+ *    (Update.cpp, OverlapUpdate.cpp) and SetFreeFermions run at the requested dt
+ *    without editing the reference.  Time() keeps its definition
+ *    Qs*(tSteps*dt) (Dynamics.cpp:20-22).
+ *  - the overlap build records (MinEValue, MaxEValue) each time the leapfrog
+ *    reads Time(), which it does once after each half step
+ *    (OverlapUpdate.cpp:110,124), so the Ritz bounds used by every half step can
+ *    be handed to the GPU path. */
+#include <cstdio>
+#include <chrono>
+#include <vector>
+#include <sstream>
+
+#include "Definitions.cpp"
+#define SU_Nc_FLAG SU2_FLAG
+#define METRIC_FLAG MINKOWSKI_FLAG
+#ifndef FERMION_FLAG
+#define FERMION_FLAG WILSON_FLAG
+#endif
+
+ovlref_reduce_hook_t ovlref_reduce_hook = nullptr;
+
+#include "MPI/Basic.cpp"
+#include "MISC/Timing.cpp"
+#include "SUNc/Definitions.cpp"
+#include "MISC/RNG/GSLRandomNumberGenerator.cpp"
+#include "IO/StringManipulation.cpp"
+#include "IO/OutputManagement.cpp"
+#include "LATTICE/3DGrid.cpp"
+#include "LATTICE/GaugeLinks.cpp"
+#include "LATTICE/ElectricFields.cpp"
+#include "LATTICE/GLinksEFields.cpp"
+#include "ovl_calc_macros.h"
+
+/* Globals the reference defines in Simulation.cpp:74,168,194-200. */
+DOUBLE Qs = 1.0;
+DOUBLE tSphaleron = 6.0;
+DOUBLE mFermion = 0.0;
+DOUBLE rWilson = 1.0;
+DOUBLE MDWHeight = 1.4;
+INT BFlux = 1;
+
+#include "CALC/ChernSimonsOperators.cpp"
+#include "TOPOLOGY/ChernSimonsDerivative.cpp"
+#include "DYNAMICS/Dynamics.cpp"
+
+namespace Dynamics {
+DOUBLE harness_dt = 0.02;
+std::vector<double> harness_bounds;
+DOUBLE harness_time();
+}
+#define dTau harness_dt
+#define Time harness_time
+
+#include "OBSERVABLES/BulkObservables.cpp"
+#include "OBSERVABLES/GaussLawViolation.cpp"
+#include "OBSERVABLES/UnitarityViolation.cpp"
+#include "QED/QED.cpp"
+#include "DiracAlgebra.cpp"
+#include "FERMIONS/FermionField.cpp"
+#if FERMION_FLAG == WILSON_FLAG
+#include "FERMIONS/WILSON/EvolutionOperator.cpp"
+#include "FERMIONS/WILSON/Update.cpp"
+#include "FERMIONS/WILSON/Currents.cpp"
+#else
+#include "FERMIONS/OVERLAP/OverlapEvolutionOperator.cpp"
+#include "FERMIONS/OVERLAP/OverlapUpdate.cpp"
+#include "FERMIONS/OVERLAP/OverlapCurrents.cpp"
+#endif
+#include "INITIALCONDITIONS/FERMIONS/SetFreeFermions.cpp"
+
+namespace Dynamics {
+DOUBLE harness_time() {
+#if FERMION_FLAG == OVERLAP_FLAG
+    harness_bounds.push_back(Dynamics::Fermions::MinEValue);
+    harness_bounds.push_back(Dynamics::Fermions::MaxEValue);
+#endif
+    return Qs * (tSteps * harness_dt);
+}
+}
+
+namespace {
+bool g_ready = false;
+std::vector<std::vector<double>> g_reduced;
+void capture_reduce(const double *data, int count) { g_reduced.emplace_back(data, data + count); }
+
+/* Silences std::cout/std::cerr (the reference prints progress and debug lines). */
+struct Quiet {
+    std::streambuf *out, *err;
+    std::ostringstream sink;
+    Quiet() : out(std::cout.rdbuf(sink.rdbuf())), err(std::cerr.rdbuf(sink.rdbuf())) {}
+    ~Quiet() { std::cout.rdbuf(out); std::cerr.rdbuf(err); }
+};
+}
+
+extern "C" {
+
+/* Sets up a lattice N0 x N1 x N2 and the mode partition of MPI rank `rank` of
+ * `nranks` (MPI/ModePartition.cpp:12-24).  Returns the number of local modes,
+ * or -1 when the modes do not divide evenly. */
+int ovlref_init(int N0, int N1, int N2, int nranks, int rank, double m_fermion, double r_wilson,
+                double m_dw, double t_sphaleron, double dt, double qs, long seed) {
+    Quiet q;
+    if (nranks <= 0 || rank < 0 || rank >= nranks) return -1;
+    if ((2 * 2 * Nc * N0 * N1 * N2) % nranks != 0) return -1;
+    Lattice::N[0] = N0; Lattice::N[1] = N1; Lattice::N[2] = N2;
+    Lattice::Volume = N0 * N1 * N2;
+    MPIBasic::NumberOfNodes = nranks;
+    MPIBasic::ID = rank;
+    mFermion = m_fermion; rWilson = r_wilson; MDWHeight = m_dw; tSphaleron = t_sphaleron; Qs = qs;
+    Dynamics::harness_dt = dt;
+    IO::OutputDirectory = "/dev/null/";  /* current maps are captured, not written */
+    RandomNumberGenerator::Init(seed);
+    Lattice::Init();
+    QED::Init();
+    QED::SetZero();
+    Fermions::Init();
+    EvolutionOperator::Init();
+    Dynamics::Reset();
+    GLinks::U->SetIdentity(0, 0, 0, 0);
+    EFields::E->SetZero();
+    Dynamics::harness_bounds.clear();
+    g_ready = true;
+    return MPIModePartition::ModesPerNode;
+}
+
+int ovlref_nc(void) { return Nc; }
+int ovlref_first_mode(void) { return MPIModePartition::FirstIndex; }
+int ovlref_local_modes(void) { return MPIModePartition::ModesPerNode; }
+int ovlref_step_count(void) { return Dynamics::tSteps; }
+void ovlref_set_step_count(int t) { Dynamics::tSteps = t; }
+
+void ovlref_set_links(const double *U) {
+    std::memcpy(GLinks::U->U, U, sizeof(double) * 4 * 3 * Lattice::Volume);
+}
+void ovlref_get_links(double *U) {
+    std::memcpy(U, GLinks::U->U, sizeof(double) * 4 * 3 * Lattice::Volume);
+}
+void ovlref_set_efield(const double *E) {
+    std::memcpy(EFields::E->E, E, sizeof(double) * 3 * 3 * Lattice::Volume);
+}
+void ovlref_get_efield(double *E) {
+    std::memcpy(E, EFields::E->E, sizeof(double) * 3 * 3 * Lattice::Volume);
+}
+
+/* Modes in the reference layout: local mode s, site, colour, spin, (re, im)
+ * (FERMIONS/FermionField.cpp:8-9,533-545). */
+void ovlref_set_modes(const double *psi, const double *psimid) {
+    size_t per_mode = sizeof(wcf) * Lattice::Volume;
+    for (int s = 0; s < MPIModePartition::ModesPerNode; s++) {
+        if (psi) std::memcpy(Fermions::Psi->GetMode(s), (const char *)psi + per_mode * s, per_mode);
+        if (psimid) std::memcpy(Fermions::PsiMid->GetMode(s), (const char *)psimid + per_mode * s, per_mode);
+    }
+}
+void ovlref_get_modes(double *psi, double *psimid) {
+    size_t per_mode = sizeof(wcf) * Lattice::Volume;
+    for (int s = 0; s < MPIModePartition::ModesPerNode; s++) {
+        if (psi) std::memcpy((char *)psi + per_mode * s, Fermions::Psi->GetMode(s), per_mode);
+        if (psimid) std::memcpy((char *)psimid + per_mode * s, Fermions::PsiMid->GetMode(s), per_mode);
+    }
+}
+
+/* InitialConditions::SetFreeFermions (SetFreeFermions.cpp:59-75). */
+void ovlref_set_free_fermions(void) {
+    Quiet q;
+    InitialConditions::SetFreeFermions(Fermions::Psi, Fermions::PsiMid);
+}
+
+/* nsteps x Dynamics::Fermions::Update (Update.cpp:48-79 / OverlapUpdate.cpp:99-135).
+ * Returns wall seconds. */
+double ovlref_step(int nsteps) {
+    Quiet q;
+    auto t0 = std::chrono::steady_clock::now();
+    for (int i = 0; i < nsteps; i++) Dynamics::Fermions::Update(GLinks::U, EFields::E, Fermions::Psi, Fermions::PsiMid);
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+/* Fermions::Observables::ComputeCurrents (Currents.cpp:396 / OverlapCurrents.cpp:292);
+ * the arrays are the ones it reduces: Wilson jV,jA,jVw,jAw (4V each), PS,WA (V);
+ * overlap jV,jA.  Pointers may be null.  Returns the number of arrays captured. */
+int ovlref_currents(double *jV, double *jA, double *jVw, double *jAw, double *PS, double *WA) {
+    Quiet q;
+    g_reduced.clear();
+    size_t recorded = Dynamics::harness_bounds.size();
+    ovlref_reduce_hook = capture_reduce;
+    Fermions::Observables::ComputeCurrents(GLinks::U, Fermions::Psi);
+    ovlref_reduce_hook = nullptr;
+    Dynamics::harness_bounds.resize(recorded);  /* its output lines also read Time() */
+    double *outs[6] = {jV, jA, jVw, jAw, PS, WA};
+    for (size_t k = 0; k < g_reduced.size() && k < 6; k++)
+        if (outs[k]) std::memcpy(outs[k], g_reduced[k].data(), sizeof(double) * g_reduced[k].size());
+    return (int)g_reduced.size();
+}
+
+/* ChernSimonsNumber::NCsDot (TOPOLOGY/ChernSimonsDerivative.cpp:31-49). */
+double ovlref_ncsdot(void) { return ChernSimonsNumber::NCsDot(GLinks::U, EFields::E); }
+
+/* Dynamics::UpdateGaugeLinks / UpdateElectricFields over the whole lattice
+ * (Dynamics.cpp:97-138, 145-197); the latter with the restated staple macros. */
+void ovlref_update_links(double dt_step) {
+    Dynamics::SetMetric();
+    Dynamics::UpdateGaugeLinks(0, Lattice::N[0] - 1, 0, Lattice::N[1] - 1, 0, Lattice::N[2] - 1, GLinks::U, EFields::E, dt_step);
+}
+void ovlref_update_efield(double dt_step) {
+    Dynamics::SetMetric();
+    Dynamics::UpdateElectricFields(0, Lattice::N[0] - 1, 0, Lattice::N[1] - 1, 0, Lattice::N[2] - 1, GLinks::U, EFields::E, dt_step);
+}
+
+/* Observables::Bulk::Update: out[0..7] = T00, TXX, TYY, TZZ, E-part, B-part, and
+ * the Gauss-law and unitarity max/avg violations (out[6..9]). */
+void ovlref_bulk(double *out) {
+    Dynamics::SetMetric();
+    Observables::Bulk::Update(GLinks::U, EFields::E);
+    out[0] = Observables::Bulk::T00();
+    out[1] = Observables::Bulk::TXX();
+    out[2] = Observables::Bulk::TYY();
+    out[3] = Observables::Bulk::TZZ();
+    out[4] = Observables::Bulk::ELECTRIC();
+    out[5] = Observables::Bulk::MAGNETIC();
+    Observables::GaussLaw::UpdateViolation(0, Lattice::N[0] - 1, 0, Lattice::N[1] - 1, 0, Lattice::N[2] - 1, GLinks::U, EFields::E);
+    out[6] = Observables::GaussLaw::GlobalMaxViolation;
+    out[7] = Observables::GaussLaw::GlobalAvgViolation;
+    Observables::Unitarity::UpdateViolation(0, Lattice::N[0] - 1, 0, Lattice::N[1] - 1, 0, Lattice::N[2] - 1, GLinks::U);
+    out[8] = Observables::Unitarity::GlobalMaxViolation;
+    out[9] = Observables::Unitarity::GlobalAvgViolation;
+}
+
+/* QED::SetConstantMagneticField (QED/QED.cpp:62-84); out = 2*N0*N1 complex. */
+void ovlref_u1_flux(int nb, double *out) {
+    QED::SetConstantMagneticField(nb);
+    std::memcpy(out, QED::U, sizeof(COMPLEX) * 2 * Lattice::N[0] * Lattice::N[1]);
+}
+
+/* One application of the evolution operator -i h to a single mode in the
+ * reference layout, with the current links: WilsonEvoOperator::Compute
+ * (WilsonOperator.cpp:30-114) or OverlapOperator::Compute (OverlapOperator.cpp:25-65)
+ * with the given spectral bounds. */
+void ovlref_apply(const double *phi, double *out, double lambda_min, double lambda_max) {
+    EvolutionOperator::Setup(GLinks::U);
+#if FERMION_FLAG == WILSON_FLAG
+    (void)lambda_min; (void)lambda_max;
+    EvolutionOperator::WilsonEvoOperator::Compute(EvolutionOperator::Ucc, (wcf *)phi, (wcf *)out);
+#else
+    Quiet q;
+    EvolutionOperator::OverlapOperator::Compute(EvolutionOperator::Ucc, (wcf *)phi, (wcf *)out, lambda_min, lambda_max);
+#endif
+}
+
+#if FERMION_FLAG == OVERLAP_FLAG
+/* Dynamics::Fermions::ComputeRitzEigenvalues (OverlapUpdate.cpp:61-97) on the
+ * current links: out = {MinEValue, MaxEValue}. */
+void ovlref_ritz_bounds(double *out) {
+    Quiet q;
+    EvolutionOperator::Setup(GLinks::U);
+    Dynamics::Fermions::ComputeRitzEigenvalues();
+    out[0] = Dynamics::Fermions::MinEValue;
+    out[1] = Dynamics::Fermions::MaxEValue;
+}
+
+/* Zolotarev coefficients (ZolotarevCoefficients.cpp:71-175) with the reference's
+ * tolerance and pole count (OverlapOperator.cpp:13-14): b[25], d[25]; returns eps. */
+double ovlref_zolotarev(double lambda_min, double lambda_max, double *b, double *d) {
+    return EvolutionOperator::OverlapOperations::ZolotarevCoefficients(
+        lambda_min, lambda_max, EvolutionOperator::OverlapOperator::ZolotarevErrTol,
+        EvolutionOperator::OverlapOperator::NumofZolotarevCoeffs, b, d);
+}
+
+/* Bounds recorded per half step by the leapfrog since the last call. */
+int ovlref_take_bounds(double *out, int capacity) {
+    int n = (int)Dynamics::harness_bounds.size();
+    for (int i = 0; i < n && i < capacity; i++) out[i] = Dynamics::harness_bounds[i];
+    Dynamics::harness_bounds.clear();
+    return n;
+}
+#endif
+
+long ovlref_rng_draws(void) { return (long)RandomNumberGenerator::Generator->draws; }
+
+}  /* extern "C" */
