@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark: mode-site updates per second of the Wilson fermion leapfrog.
+
+One "step" is one full leapfrog step (Dynamics::Fermions::Update,
+FERMIONS/WILSON/Update.cpp:48-79) of every mode of the workload: two half steps
+of psi += dt D psi' and two link half steps.  A mode-site update (MSU) is one
+mode at one site advanced by one step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload n16|n8]
+
+Default workload (n16): SU(2), N = 16^3, Wilson r = 1, m = 0.05, MDWHeight = 0,
+dt = 0.05, all 32768 modes (free plane waves), FP32 modes with FP64 links;
+seeded random links and electric field (links move every half step).  The
+modes (8.6 GB per field in FP32) exceed the 126 MB L2, so no L2 flush is
+needed between steps.  The line reports the FP32 fused form as `value`, the
+FP64 plain (two-phase, as the reference) and FP64 fused forms beside it, the
+roofline of the dominant kernel, the end-to-end rate through the C ABI with
+host buffers, and the reference's own CPU code on this host's cores.
+
+Under torchrun (N > 1) every rank runs an independent replica on its own GPU
+(the workload does not shard across GPUs); value = all ranks' MSU / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "n16": dict(N=(16, 16, 16), m=0.05, r=1.0, mdw=0.0, dt=0.05, link_sigma=0.3, e_sigma=0.1, seed=20261203,
+                ref_ranks=512),
+    "n8": dict(N=(8, 8, 8), m=0.1, r=1.0, mdw=0.0, dt=0.05, link_sigma=0.3, e_sigma=0.0, seed=20261203,
+               ref_ranks=64),
+}
+METRIC = "mode-site updates/s"
+
+
+# ----------------------------------------------------------------- helpers --
+def volume(N):
+    return N[0] * N[1] * N[2]
+
+
+def n_modes(N):
+    return 8 * volume(N)
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    v = d.get(kernel)
+    return None if v is None else float(v["bytes_per_launch"])
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"ovl_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        exe = shutil.which("nvidia-smi")
+        if exe:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen([exe, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                         "-i", str(self.gpu), "-lms", "200"], stdout=self.fh,
+                                        stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if not self.proc or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------ reference CPU arm --
+def _ref_worker(args):
+    """One emulated MPI rank of the reference's own code (compiled from source):
+    its mode slice advanced by `steps` Dynamics::Fermions::Update calls."""
+    wl, rank, steps, warmup = args
+    sys.path.insert(0, str(ROOT / "tests"))
+    import numpy as np
+
+    from _oracle import ptr, reference
+    from overlap_b200.inputs import random_efield, random_links
+
+    R = reference("wilson")
+    N = wl["N"]
+    m = R.ovlref_init(*N, wl["ref_ranks"], rank, wl["m"], wl["r"], wl["mdw"], 1e300, wl["dt"], 1.0, 1)
+    R.ovlref_set_links(ptr(random_links(N, wl["link_sigma"], wl["seed"])))
+    R.ovlref_set_efield(ptr(np.ascontiguousarray(random_efield(N, wl["e_sigma"], wl["seed"] + 1))))
+    R.ovlref_set_free_fermions()
+    if warmup:
+        R.ovlref_step(warmup)
+    secs = R.ovlref_step(steps)
+    return m, secs
+
+
+def reference_cpu(wl, steps: int, warmup: int, max_procs: int | None = None):
+    """Aggregate MSU/s of the reference hot path on this host: one process per
+    core, each an emulated MPI rank (MPI/ModePartition.cpp:12-24) holding
+    4*Nc*V/ref_ranks modes."""
+    cores = os.cpu_count() or 1
+    procs = min(cores, wl["ref_ranks"], max_procs or cores)
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, [(wl, r, steps, warmup) for r in range(procs)])
+    wall = time.perf_counter() - t0
+    V = volume(wl["N"])
+    msu = sum(m * V * steps for m, _ in res)
+    slowest = max(s for _, s in res)
+    modes = res[0][0]
+    return {"value": msu / slowest, "unit": METRIC, "cores": procs, "kind": "reference",
+            "sample": f"{steps} leapfrog steps of a {modes}-mode slice (MPI rank emulation, {wl['ref_ranks']} ranks) "
+                      f"per process, {procs} processes, reference C++ built -O3 -march=x86-64-v3",
+            "seconds": slowest, "wall_seconds": wall}
+
+
+# ---------------------------------------------------------------- GPU arm --
+def time_form(wl, precision, form, steps, warmup, device, profile):
+    import numpy as np
+    import torch
+
+    from overlap_b200 import Context
+    from overlap_b200.inputs import random_efield, random_links
+
+    N = wl["N"]
+    stream = torch.cuda.Stream(device)  # a real stream: the library and the events share it
+    ctx = Context(N=N, precision=precision, form=form, m_fermion=wl["m"], r_wilson=wl["r"], m_dw=wl["mdw"],
+                  dt=wl["dt"], t_sphaleron=1e300, device=device, stream=stream.cuda_stream)
+    ctx.torch_stream = stream  # keeps the stream alive as long as the context
+    ctx.set_links(random_links(N, wl["link_sigma"], wl["seed"]))
+    ctx.set_efield(random_efield(N, wl["e_sigma"], wl["seed"] + 1))
+    assert ctx.set_free_fermions() == 0
+    ctx.step(warmup)
+    ctx.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if profile:
+        ctx.profile(True)
+    l0 = ctx.launch_count
+    barrier()
+    torch.cuda.synchronize(device)
+    start.record(stream)
+    ctx.step(steps)
+    stop.record(stream)
+    torch.cuda.synchronize(device)
+    barrier()
+    ms = start.elapsed_time(stop)
+    out = {"ms": ms, "launches": ctx.launch_count - l0, "charges": ctx.charges()}
+    if profile:
+        out["prof"] = ctx.profile_read()
+        ctx.profile(False)
+    return ctx, out
+
+
+def time_e2e(ctx, wl, steps, device):
+    """Same metric through the C ABI with host buffers: each step uploads the
+    gauge fields from pinned host memory, advances one leapfrog step and reads
+    the step's charges (N_V, N_5, PS, WA) back to the host."""
+    import numpy as np
+    import torch
+
+    from overlap_b200.inputs import random_efield, random_links
+
+    N = wl["N"]
+    U = torch.empty((volume(N), 3, 4), dtype=torch.float64, pin_memory=True).numpy()
+    E = torch.empty((volume(N), 3, 3), dtype=torch.float64, pin_memory=True).numpy()
+    U[...] = random_links(N, wl["link_sigma"], wl["seed"])
+    E[...] = random_efield(N, wl["e_sigma"], wl["seed"] + 1)
+    ctx.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.step(1)
+        ch = ctx.charges()
+    ctx.synchronize()
+    secs = time.perf_counter() - t0
+    secs = max_over_ranks(secs)
+    h2d = U.nbytes + E.nbytes
+    d2h = 4 * 8
+    return secs, h2d, d2h, ch
+
+
+# ------------------------------------------------------------ distributed --
+_dist = None
+
+
+def init_dist():
+    global _dist
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        _dist = dist
+    return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def barrier():
+    if _dist is not None:
+        _dist.barrier()
+
+
+def max_over_ranks(x: float) -> float:
+    if _dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    _dist.all_reduce(t, op=_dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------- main --
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="n16")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 forms")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    N = wl["N"]
+    V, M = volume(N), n_modes(N)
+    rank, world, local = init_dist()
+    config = {"workload": f"SU(2) Wilson fermions, N={N[0]}x{N[1]}x{N[2]}, {M} modes (complete plane-wave basis), "
+                          f"r={wl['r']}, m={wl['m']}, MDWHeight={wl['mdw']}, dt={wl['dt']}",
+              "lattice": list(N), "modes": M, "gauge_init": f"seeded random links (sigma={wl['link_sigma']}) and "
+              f"E (sigma={wl['e_sigma']}), links updated every half step",
+              "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"}
+
+    if args.impl == "reference":
+        if rank == 0:
+            steps = max(1, min(args.steps, 20))
+            cpu = reference_cpu(wl, steps=steps, warmup=min(args.warmup, 1))
+            line = {"metric": METRIC, "value": cpu["value"], "unit": METRIC, "n_gpus": args.gpus, "steps": steps,
+                    "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * cpu["seconds"] / steps,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic", "config": config, "impl": "reference",
+                    "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                    "e2e": {"value": cpu["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        return
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        # before any CUDA call (spawned workers)
+        # about 2.5 s per process: 12 steps of a 64-mode slice at N=16, 60 at N=8
+        cpu = reference_cpu(wl, steps=12 if args.workload == "n16" else 60, warmup=0, max_procs=64)
+
+    import torch
+
+    device = local if torch.cuda.device_count() > local else 0
+    torch.cuda.set_device(device)
+    K, W = args.steps, max(3, args.warmup)
+
+    # FP32 batched (headline)
+    with ClockSampler(device) as clocks:
+        ctx, fp32 = time_form(wl, "fp32", "fused", K, W, device, profile=True)
+    clk = clocks.summary()
+    e2e_steps = max(3, min(K, 20))
+    e2e_secs, h2d, d2h, _ = time_e2e(ctx, wl, e2e_steps, device)
+    ctx.close()
+    del ctx
+    ms = max_over_ranks(fp32["ms"])
+    value = world * M * V * K / (ms / 1e3)
+
+    forms = {}
+    if not args.no_fp64:
+        for form in ("plain", "fused"):
+            c, r = time_form(wl, "fp64", form, max(2, K // 2), W, device, profile=True)
+            c.close()
+            del c
+            r_ms = max_over_ranks(r["ms"])
+            forms[form] = {"value": world * M * V * max(2, K // 2) / (r_ms / 1e3), "ms_per_step": r_ms / max(2, K // 2),
+                           "hop_ms_per_launch": r["prof"]["hop"][0] / max(1, r["prof"]["hop"][1]),
+                           "N5": r["charges"]["N5"]}
+
+    # roofline of the dominant kernel (Wilson fused half step, FP32)
+    hop_ms, hop_n = fp32["prof"]["hop"]
+    per_launch_ms = hop_ms / max(1, hop_n)
+    elem = 8 * 8  # 2 colours x 4 spins x complex<float>
+    alg_bytes = 3 * M * V * elem + 3 * V * 32
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    traffic = committed_traffic("wilson_kernel<float,1>")
+
+    if rank == 0:
+        total_ms = {k: v[0] for k, v in fp32["prof"].items()}
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 modes / f64 links", "data": "synthetic", "config": config,
+            "e2e": {"value": world * M * V * e2e_steps / e2e_secs, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "path": "C ABI, host buffers: ovl_set_links + ovl_set_efield (pinned) + ovl_step(1) + ovl_charges"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "kernel": "wilson_kernel<float,1> (fused half step)",
+                         "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms,
+                         "peak_source": peak_kind},
+            "gpu_launches": fp32["launches"],
+            "kernel_ms": total_ms,
+            "forms": {"fp32_fused": {"value": value, "ms_per_step": ms / K, "N5": fp32["charges"]["N5"]},
+                      **{f"fp64_{k}": v for k, v in forms.items()}},
+            "clocks": clk,
+        }
+        if "plain" in forms:
+            line["fp32_vs_fp64_plain"] = value / forms["plain"]["value"]
+        if cpu is not None:
+            line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line), flush=True)
+    if _dist is not None:
+        _dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

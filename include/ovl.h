@@ -1,0 +1,165 @@
+/* ovl.h -- C ABI of overlap_b200: the OVERLAP real-time fermion + SU(2) gauge
+ * evolution hot path on one NVIDIA B200 (sm_100a).
+ *
+ * Plain C types only (no CUDA or torch types); every function returns an
+ * ovl_status and leaves a message retrievable with ovl_last_error().  A context
+ * owns one lattice, its gauge fields and one batch of fermion modes resident in
+ * device memory.  A context is not thread-safe: drive each one from one host
+ * thread.  Host arrays use the reference's layouts (SU(2), spacing 1):
+ *
+ *   links   double[V][3][4]  U = u3 + i u_k sigma_k   (LATTICE/GaugeLinks.cpp:27-36,
+ *                                                       SUNc/SU2/GroupOperations.cpp:4-9)
+ *   efield  double[V][3][3]  E^a_mu                    (LATTICE/ElectricFields.cpp:36-42)
+ *   modes   double[M][V][2 colour][4 spin][2 re,im]    (FERMIONS/FermionField.cpp:8-9,533-545)
+ *   site    x + N0*(y + N1*z)
+ *
+ * Mode m of a context is the reference's global mode first_mode + m; its
+ * parity gives the vacuum weight +1/-1 of the current sums
+ * (FERMIONS/FermionField.cpp:109-122).
+ */
+#ifndef OVL_H
+#define OVL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    OVL_OK = 0,
+    OVL_E_ARG = 1,            /* invalid argument or size */
+    OVL_E_OOM = 2,            /* device allocation failed */
+    OVL_E_NOT_CONVERGED = 3,  /* iterative solver hit its iteration limit */
+    OVL_E_TIMEOUT = 4,        /* bounded device wait expired */
+    OVL_E_NONFINITE = 5,      /* NaN/Inf detected in a field */
+    OVL_E_CUDA = 6,           /* CUDA runtime error */
+    OVL_E_STATE = 7,          /* call out of order (e.g. fields not set) */
+    OVL_E_UNSUPPORTED = 8     /* configuration not built */
+} ovl_status;
+
+typedef enum { OVL_FERMION_WILSON = 0, OVL_FERMION_OVERLAP = 1 } ovl_fermion;
+
+typedef enum { OVL_PREC_FP64 = 0, OVL_PREC_FP32 = 1 } ovl_precision;
+
+/* OVL_FORM_PLAIN keeps the reference's two-phase half step (Update.cpp:6-27):
+ * the operator writes a derivative buffer, then psi += dt * derivative.
+ * OVL_FORM_FUSED applies psi_dst += dt * D psi_src in one pass. */
+typedef enum { OVL_FORM_PLAIN = 0, OVL_FORM_FUSED = 1 } ovl_form;
+
+typedef struct {
+    int N[3];             /* lattice extents N0, N1, N2 */
+    int Nc;               /* colours; 2 (SU(2)) */
+    int n_modes;          /* modes held by this context */
+    int first_mode;       /* global index of local mode 0 (MPI/ModePartition.cpp:12-24) */
+    int fermion;          /* ovl_fermion */
+    int precision;        /* ovl_precision of the modes and of the hopping arithmetic */
+    int form;             /* ovl_form */
+    double r_wilson;      /* rWilson */
+    double m_fermion;     /* mFermion */
+    double m_dw;          /* MDWHeight; the Wilson mass is 6r + 2m - 2 MDWHeight (WilsonOperator.cpp:39) */
+    double dt;            /* Dynamics::dTau */
+    double qs;            /* Qs: Time() = qs * steps * dt (Dynamics.cpp:20-22) */
+    double t_sphaleron;   /* links move while Time() < t_sphaleron (Update.cpp:57-60) */
+    int device;           /* CUDA device ordinal */
+    int plain_chunk_modes;/* OVL_FORM_PLAIN: modes per derivative-buffer chunk (0 = all) */
+    uint64_t stream;      /* cudaStream_t to issue work on; 0 = the context creates its own */
+} ovl_params;
+
+typedef struct ovl_ctx ovl_ctx;
+
+/* Fills p with the reference's defaults (Simulation.cpp:74,168,194-200,
+ * Dynamics.cpp:17): SU(2) Wilson, FP64 plain, r = 1, m = 0, MDWHeight = 1.4,
+ * dt = 0.02, Qs = 1, tSphaleron = 6. */
+int ovl_params_init(ovl_params *p);
+
+/* Allocates the device state for p.  Replaces Lattice::Init, Fermions::Init and
+ * EvolutionOperator::Init (Simulation.cpp:251-307, FermionField.cpp:632-641). */
+int ovl_create(const ovl_params *p, ovl_ctx **out);
+int ovl_destroy(ovl_ctx *ctx);
+const char *ovl_last_error(const ovl_ctx *ctx);
+
+/* Gauge fields, host <-> device, reference layouts (GLinks::U->U, EFields::E->E). */
+int ovl_set_links(ovl_ctx *ctx, const double *links);
+int ovl_get_links(ovl_ctx *ctx, double *links);
+int ovl_set_efield(ovl_ctx *ctx, const double *efield);
+int ovl_get_efield(ovl_ctx *ctx, double *efield);
+
+/* Modes first..first+count-1 of Psi / PsiMid in the reference layout; either
+ * pointer may be NULL to skip that field.  Replaces writing
+ * Fermions::Psi/PsiMid->GetMode(s) on the host. */
+int ovl_set_modes(ovl_ctx *ctx, int first, int count, const double *psi, const double *psimid);
+int ovl_get_modes(ovl_ctx *ctx, int first, int count, double *psi, double *psimid);
+
+/* InitialConditions::SetFreeFermions (INITIALCONDITIONS/FERMIONS/SetFreeFermions.cpp:3-56):
+ * free Wilson plane waves, computed on the device.  *n_bad receives the number of
+ * modes failing the eigen-residual/normalisation self-check (FermionField.cpp:270-312). */
+int ovl_set_free_fermions(ovl_ctx *ctx, int *n_bad);
+
+/* nsteps x Dynamics::Fermions::Update(U, E, Psi, PsiMid)
+ * (FERMIONS/WILSON/Update.cpp:48-79): psi += dt D(psimid); links half step while
+ * Time() < tSphaleron; psimid += dt D(psi); links half step; step counter + 1.
+ * Asynchronous on the context's stream. */
+int ovl_step(ovl_ctx *ctx, int nsteps);
+
+/* Leapfrog step counter Dynamics::tSteps. */
+int ovl_get_step_count(const ovl_ctx *ctx, int *steps);
+int ovl_set_step_count(ovl_ctx *ctx, int steps);
+
+/* Fermions::Observables::ComputeCurrents (FERMIONS/WILSON/Currents.cpp:7-309) of
+ * this context's modes, i.e. the arrays it MPI_Reduces (:326-333): jV, jA, jVw, jAw
+ * double[V][4]; PS, WA double[V].  NULL pointers are skipped. */
+int ovl_currents(ovl_ctx *ctx, double *jV, double *jA, double *jVw, double *jAw, double *PS, double *WA);
+
+/* Lattice sums of the current densities: out[0] = sum_x jV^0 (vector charge),
+ * out[1] = sum_x jA^0 (axial charge N_5), out[2] = sum_x PS, out[3] = sum_x WA. */
+int ovl_charges(ovl_ctx *ctx, double out[4]);
+
+/* ChernSimonsNumber::NCsDot(U, E): improved E.B / (8 pi^2)
+ * (TOPOLOGY/ChernSimonsDerivative.cpp:31-49, CALC/ChernSimonsOperators.cpp:128-439). */
+int ovl_ncsdot(ovl_ctx *ctx, double *out);
+
+/* Dynamics::UpdateGaugeLinks over the whole lattice (DYNAMICS/Dynamics.cpp:97-138):
+ * U <- exp(-i dt_step E^a t^a) U. */
+int ovl_update_links(ovl_ctx *ctx, double dt_step);
+
+/* Dynamics::UpdateElectricFields over the whole lattice (Dynamics.cpp:145-197):
+ * E_mu += -2 dt_step sum over the staples of U_mu of Re tr(i t^a U_plaq). */
+int ovl_update_efield(ovl_ctx *ctx, double dt_step);
+
+/* Observables::Bulk::Update + GaussLaw + Unitarity (OBSERVABLES/BulkObservables.cpp:133-143,
+ * GaussLawViolation.cpp:13-61, UnitarityViolation.cpp:13-51):
+ * out = {T00, TXX, TYY, TZZ, electric, magnetic, gauss max, gauss avg, unitarity max, unitarity avg}. */
+int ovl_bulk(ovl_ctx *ctx, double out[10]);
+
+/* Waits for all work queued on the context's stream. */
+int ovl_synchronize(ovl_ctx *ctx);
+
+/* Device addresses and layout of the mode fields, for callers that keep their
+ * own device buffers.  Layout: [mode/32][site][colour*4+spin][mode%32] complex of
+ * the context precision (float2 or double2); *bytes is the size of one field. */
+int ovl_device_modes(ovl_ctx *ctx, void **psi, void **psimid, size_t *bytes);
+
+/* Number of CUDA kernel launches this context has issued (for launch accounting). */
+int ovl_launch_count(const ovl_ctx *ctx, uint64_t *count);
+
+/* Per-kernel timing with CUDA events recorded on the context's stream around
+ * each launch.  Kinds: */
+enum {
+    OVL_PROF_HOP = 0,      /* Wilson operator kernel (fused half step or derivative) */
+    OVL_PROF_AXPY = 1,     /* plain form: psi += dt * derivative */
+    OVL_PROF_LINKS = 2,    /* link update */
+    OVL_PROF_OBS = 3,      /* currents / charges / NCsDot / bulk */
+    OVL_PROF_KINDS = 4
+};
+/* Turns recording on (1) or off (0); turning it on clears earlier records. */
+int ovl_profile_enable(ovl_ctx *ctx, int on);
+/* Synchronises the stream and returns, per kind, the summed kernel time in ms
+ * and the number of launches timed since recording was enabled. */
+int ovl_profile_read(ovl_ctx *ctx, double ms[OVL_PROF_KINDS], uint64_t launches[OVL_PROF_KINDS]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

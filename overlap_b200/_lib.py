@@ -1,0 +1,82 @@
+"""ctypes binding of the C ABI in include/ovl.h (libovl_b200.so).
+
+The library is the only implementation: there is no CPU fallback.  Loading
+fails with an ImportError naming the missing file when it has not been built
+(`python -m overlap_b200.build`).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libovl_b200.so"
+
+OVL_OK = 0
+STATUS_NAMES = {
+    0: "OVL_OK", 1: "OVL_E_ARG", 2: "OVL_E_OOM", 3: "OVL_E_NOT_CONVERGED", 4: "OVL_E_TIMEOUT",
+    5: "OVL_E_NONFINITE", 6: "OVL_E_CUDA", 7: "OVL_E_STATE", 8: "OVL_E_UNSUPPORTED",
+}
+
+
+class ovl_params(C.Structure):
+    _fields_ = [
+        ("N", C.c_int * 3), ("Nc", C.c_int), ("n_modes", C.c_int), ("first_mode", C.c_int),
+        ("fermion", C.c_int), ("precision", C.c_int), ("form", C.c_int),
+        ("r_wilson", C.c_double), ("m_fermion", C.c_double), ("m_dw", C.c_double), ("dt", C.c_double),
+        ("qs", C.c_double), ("t_sphaleron", C.c_double), ("device", C.c_int), ("plain_chunk_modes", C.c_int),
+        ("stream", C.c_uint64),
+    ]
+
+
+_dp = C.POINTER(C.c_double)
+_vp = C.c_void_p
+_ctx = C.c_void_p
+
+# name -> (argtypes, restype); every function of include/ovl.h
+SIGNATURES = {
+    "ovl_params_init": ([C.POINTER(ovl_params)], C.c_int),
+    "ovl_create": ([C.POINTER(ovl_params), C.POINTER(_ctx)], C.c_int),
+    "ovl_destroy": ([_ctx], C.c_int),
+    "ovl_last_error": ([_ctx], C.c_char_p),
+    "ovl_set_links": ([_ctx, _dp], C.c_int),
+    "ovl_get_links": ([_ctx, _dp], C.c_int),
+    "ovl_set_efield": ([_ctx, _dp], C.c_int),
+    "ovl_get_efield": ([_ctx, _dp], C.c_int),
+    "ovl_set_modes": ([_ctx, C.c_int, C.c_int, _dp, _dp], C.c_int),
+    "ovl_get_modes": ([_ctx, C.c_int, C.c_int, _dp, _dp], C.c_int),
+    "ovl_set_free_fermions": ([_ctx, C.POINTER(C.c_int)], C.c_int),
+    "ovl_step": ([_ctx, C.c_int], C.c_int),
+    "ovl_get_step_count": ([_ctx, C.POINTER(C.c_int)], C.c_int),
+    "ovl_set_step_count": ([_ctx, C.c_int], C.c_int),
+    "ovl_currents": ([_ctx, _dp, _dp, _dp, _dp, _dp, _dp], C.c_int),
+    "ovl_charges": ([_ctx, _dp], C.c_int),
+    "ovl_ncsdot": ([_ctx, _dp], C.c_int),
+    "ovl_update_links": ([_ctx, C.c_double], C.c_int),
+    "ovl_update_efield": ([_ctx, C.c_double], C.c_int),
+    "ovl_bulk": ([_ctx, _dp], C.c_int),
+    "ovl_synchronize": ([_ctx], C.c_int),
+    "ovl_device_modes": ([_ctx, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_size_t)], C.c_int),
+    "ovl_launch_count": ([_ctx, C.POINTER(C.c_uint64)], C.c_int),
+    "ovl_profile_enable": ([_ctx, C.c_int], C.c_int),
+    "ovl_profile_read": ([_ctx, _dp, C.POINTER(C.c_uint64)], C.c_int),
+}
+
+PROF_KINDS = ("hop", "axpy", "links", "obs")
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded library with typed signatures; ImportError if it is not built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"overlap_b200 CUDA library not built: {LIB_PATH} is missing "
+                              "(run `python -m overlap_b200.build`)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib

@@ -1,0 +1,239 @@
+"""Python host API over the C ABI.
+
+`Context` owns one lattice, its SU(2) links and electric field, and a batch of
+fermion modes resident on one GPU.  Its methods carry the names and meaning of
+the reference routines they replace:
+
+    step(n)            n x Dynamics::Fermions::Update (FERMIONS/WILSON/Update.cpp:48-79)
+    currents()         Fermions::Observables::ComputeCurrents (FERMIONS/WILSON/Currents.cpp:7-394)
+    ncsdot()           ChernSimonsNumber::NCsDot (TOPOLOGY/ChernSimonsDerivative.cpp:31-49)
+    update_links(dt)   Dynamics::UpdateGaugeLinks (DYNAMICS/Dynamics.cpp:97-138)
+    update_efield(dt)  Dynamics::UpdateElectricFields (DYNAMICS/Dynamics.cpp:145-197)
+    bulk()             Observables::Bulk / GaussLaw / Unitarity (OBSERVABLES/*.cpp)
+    set_free_fermions  InitialConditions::SetFreeFermions (INITIALCONDITIONS/FERMIONS/SetFreeFermions.cpp)
+
+Arrays cross the boundary in the reference's layouts (see overlap_b200.inputs).
+Errors raise OvlError carrying the C status code; the reference itself prints
+and exits on errors (e.g. MPI/ModePartition.cpp:18-21).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .inputs import volume
+
+PRECISIONS = {"fp64": 0, "fp32": 1}
+FORMS = {"plain": 0, "fused": 1}
+FERMIONS = {"wilson": 0, "overlap": 1}
+
+
+class OvlError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_lib.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+@dataclass
+class Params:
+    N: tuple = (8, 8, 8)
+    n_modes: int | None = None       # default: the full basis 4*Nc*V
+    first_mode: int = 0
+    fermion: str = "wilson"
+    precision: str = "fp64"
+    form: str = "plain"
+    r_wilson: float = 1.0
+    m_fermion: float = 0.0
+    m_dw: float = 1.4
+    dt: float = 0.02
+    qs: float = 1.0
+    t_sphaleron: float = 6.0
+    device: int = 0
+    plain_chunk_modes: int = 0
+    stream: int = 0
+
+    def to_c(self) -> _lib.ovl_params:
+        p = _lib.ovl_params()
+        _lib.lib().ovl_params_init(C.byref(p))
+        p.N[0], p.N[1], p.N[2] = (int(n) for n in self.N)
+        p.Nc = 2
+        p.n_modes = int(self.n_modes if self.n_modes is not None else 8 * volume(self.N))
+        p.first_mode = int(self.first_mode)
+        p.fermion = FERMIONS[self.fermion]
+        p.precision = PRECISIONS[self.precision]
+        p.form = FORMS[self.form]
+        p.r_wilson, p.m_fermion, p.m_dw = self.r_wilson, self.m_fermion, self.m_dw
+        p.dt, p.qs, p.t_sphaleron = self.dt, self.qs, self.t_sphaleron
+        p.device = int(self.device)
+        p.plain_chunk_modes = int(self.plain_chunk_modes)
+        p.stream = int(self.stream)
+        return p
+
+
+class Context:
+    """One lattice + mode batch on one GPU (ovl_create ... ovl_destroy)."""
+
+    def __init__(self, params: Params | None = None, **kw):
+        self.params = params if params is not None else Params(**kw)
+        self._L = _lib.lib()
+        self._ctx = C.c_void_p()
+        cp = self.params.to_c()
+        rc = self._L.ovl_create(C.byref(cp), C.byref(self._ctx))
+        if rc != 0:
+            raise OvlError(rc, self._L.ovl_last_error(None).decode())
+        self.N = tuple(int(n) for n in self.params.N)
+        self.V = volume(self.N)
+        self.n_modes = cp.n_modes
+
+    # -------------------------------------------------------------- plumbing
+    def _check(self, rc: int):
+        if rc != 0:
+            raise OvlError(rc, self._L.ovl_last_error(self._ctx).decode())
+
+    def close(self):
+        if self._ctx:
+            self._L.ovl_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _as_f64(a, shape) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.size != int(np.prod(shape)):
+            raise ValueError(f"expected {int(np.prod(shape))} doubles, got {a.size}")
+        return a
+
+    # ---------------------------------------------------------------- fields
+    def set_links(self, U):
+        self._check(self._L.ovl_set_links(self._ctx, _dp(self._as_f64(U, (self.V, 3, 4)))))
+
+    def get_links(self) -> np.ndarray:
+        out = np.empty((self.V, 3, 4))
+        self._check(self._L.ovl_get_links(self._ctx, _dp(out)))
+        return out
+
+    def set_efield(self, E):
+        self._check(self._L.ovl_set_efield(self._ctx, _dp(self._as_f64(E, (self.V, 3, 3)))))
+
+    def get_efield(self) -> np.ndarray:
+        out = np.empty((self.V, 3, 3))
+        self._check(self._L.ovl_get_efield(self._ctx, _dp(out)))
+        return out
+
+    def set_modes(self, psi=None, psimid=None, first: int = 0):
+        """psi / psimid: complex128[count, V, 2, 4] in the reference layout."""
+        arrs = []
+        count = None
+        for a in (psi, psimid):
+            if a is None:
+                arrs.append(None)
+                continue
+            a = np.ascontiguousarray(a, dtype=np.complex128)
+            count = a.shape[0]
+            if a.size != count * self.V * 8:
+                raise ValueError("modes must be complex[count, V, 2, 4]")
+            arrs.append(a)
+        if count is None:
+            return
+        ptrs = [None if a is None else a.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
+        self._check(self._L.ovl_set_modes(self._ctx, first, count, ptrs[0], ptrs[1]))
+
+    def get_modes(self, first: int = 0, count: int | None = None):
+        count = self.n_modes - first if count is None else count
+        psi = np.empty((count, self.V, 2, 4), np.complex128)
+        mid = np.empty_like(psi)
+        self._check(self._L.ovl_get_modes(self._ctx, first, count, _dp(psi.view(np.float64)), _dp(mid.view(np.float64))))
+        return psi, mid
+
+    def set_free_fermions(self) -> int:
+        bad = C.c_int(0)
+        self._check(self._L.ovl_set_free_fermions(self._ctx, C.byref(bad)))
+        return bad.value
+
+    # ------------------------------------------------------------- evolution
+    def step(self, nsteps: int = 1):
+        self._check(self._L.ovl_step(self._ctx, int(nsteps)))
+
+    @property
+    def step_count(self) -> int:
+        v = C.c_int(0)
+        self._check(self._L.ovl_get_step_count(self._ctx, C.byref(v)))
+        return v.value
+
+    @step_count.setter
+    def step_count(self, n: int):
+        self._check(self._L.ovl_set_step_count(self._ctx, int(n)))
+
+    def update_links(self, dt_step: float):
+        self._check(self._L.ovl_update_links(self._ctx, float(dt_step)))
+
+    def update_efield(self, dt_step: float):
+        self._check(self._L.ovl_update_efield(self._ctx, float(dt_step)))
+
+    def synchronize(self):
+        self._check(self._L.ovl_synchronize(self._ctx))
+
+    # ----------------------------------------------------------- observables
+    def currents(self) -> dict:
+        V = self.V
+        out = {k: np.empty((V, 4)) for k in ("jV", "jA", "jVw", "jAw")}
+        out["PS"] = np.empty(V)
+        out["WA"] = np.empty(V)
+        self._check(self._L.ovl_currents(self._ctx, *(_dp(out[k]) for k in ("jV", "jA", "jVw", "jAw", "PS", "WA"))))
+        return out
+
+    def charges(self) -> dict:
+        o = np.empty(4)
+        self._check(self._L.ovl_charges(self._ctx, _dp(o)))
+        return {"NV": o[0], "N5": o[1], "PS": o[2], "WA": o[3]}
+
+    def ncsdot(self) -> float:
+        o = np.empty(1)
+        self._check(self._L.ovl_ncsdot(self._ctx, _dp(o)))
+        return float(o[0])
+
+    def bulk(self) -> dict:
+        o = np.empty(10)
+        self._check(self._L.ovl_bulk(self._ctx, _dp(o)))
+        keys = ("T00", "TXX", "TYY", "TZZ", "electric", "magnetic", "gauss_max", "gauss_avg", "unitarity_max", "unitarity_avg")
+        return dict(zip(keys, o.tolist()))
+
+    def device_modes(self):
+        psi, mid, nbytes = C.c_void_p(), C.c_void_p(), C.c_size_t()
+        self._check(self._L.ovl_device_modes(self._ctx, C.byref(psi), C.byref(mid), C.byref(nbytes)))
+        return psi.value, mid.value, nbytes.value
+
+    def profile(self, on: bool = True):
+        """Starts (clearing) or stops per-kernel CUDA-event timing."""
+        self._check(self._L.ovl_profile_enable(self._ctx, 1 if on else 0))
+
+    def profile_read(self) -> dict:
+        """{kind: (total ms, launches)} for kinds hop, axpy, links, obs."""
+        ms = np.zeros(len(_lib.PROF_KINDS))
+        n = (C.c_uint64 * len(_lib.PROF_KINDS))()
+        self._check(self._L.ovl_profile_read(self._ctx, _dp(ms), n))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(_lib.PROF_KINDS)}
+
+    @property
+    def launch_count(self) -> int:
+        v = C.c_uint64(0)
+        self._check(self._L.ovl_launch_count(self._ctx, C.byref(v)))
+        return v.value

@@ -1,0 +1,561 @@
+// C ABI of overlap_b200 (include/ovl.h): context lifetime, host <-> device
+// transfers in the reference's layouts, and the leapfrog driver.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "ovl.h"
+#include "ovl_device.cuh"
+#include "ovl_internal.h"
+
+using ovl::Lattice;
+
+struct ovl_ctx {
+    ovl_params p{};
+    Lattice L{};
+    int n_mb = 0;                 // mode blocks of 32
+    size_t field_complex = 0;     // complex numbers per mode field
+    size_t elem_bytes = 0;        // bytes per complex number
+    void *psi = nullptr, *psimid = nullptr;
+    double *U = nullptr, *E = nullptr;
+    void *deriv = nullptr;        // plain form: derivative buffer
+    int deriv_mb = 0;             // mode blocks per derivative chunk
+    double *per_site = nullptr;   // currents per site
+    double *partial = nullptr;    // reduction scratch
+    size_t partial_doubles = 0;
+    double *dev_small = nullptr;  // small device results
+    double *host_small = nullptr; // pinned mirror
+    int *dev_int = nullptr;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int tsteps = 0;
+    int sm_count = 148;
+    uint64_t launches = 0;
+    std::string err;
+    // per-kernel timing (ovl_profile_enable): event pairs per kind
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[OVL_PROF_KINDS];
+    std::vector<cudaEvent_t> event_pool;
+};
+
+namespace {
+
+std::string g_err;  // errors without a context (creation)
+
+int fail(ovl_ctx *c, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf; else g_err = buf;
+    return code;
+}
+
+int cuda_fail(ovl_ctx *c, cudaError_t e, const char *what) {
+    return fail(c, OVL_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define OVL_CUDA(c, call)                                         \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return cuda_fail((c), e_, #call);  \
+    } while (0)
+
+// Brackets a launch with events when profiling is on.
+struct ProfScope {
+    ovl_ctx *c;
+    int kind;
+    cudaEvent_t start = nullptr;
+    cudaEvent_t take() {
+        if (c->event_pool.empty()) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            return e;
+        }
+        cudaEvent_t e = c->event_pool.back();
+        c->event_pool.pop_back();
+        return e;
+    }
+    ProfScope(ovl_ctx *ctx, int k) : c(ctx), kind(k) {
+        if (c->profiling && (start = take())) cudaEventRecord(start, c->stream);
+    }
+    ~ProfScope() {
+        if (!start) return;
+        cudaEvent_t stop = take();
+        if (!stop) { c->event_pool.push_back(start); return; }
+        cudaEventRecord(stop, c->stream);
+        c->prof[kind].emplace_back(start, stop);
+    }
+};
+
+// Checks for launch errors after a batch of `n` kernel launches.
+int launched(ovl_ctx *c, int n, const char *what) {
+    c->launches += (uint64_t)n;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, what);
+    return OVL_OK;
+}
+
+bool all_finite(const double *a, size_t n) {
+    for (size_t i = 0; i < n; i++)
+        if (!std::isfinite(a[i])) return false;
+    return true;
+}
+
+int set_device(ovl_ctx *c) {
+    OVL_CUDA(c, cudaSetDevice(c->p.device));
+    return OVL_OK;
+}
+
+bool fp32(const ovl_ctx *c) { return c->p.precision == OVL_PREC_FP32; }
+
+double amass(const ovl_params &p) { return 6.0 * p.r_wilson + 2.0 * p.m_fermion - 2.0 * p.m_dw; }
+
+// psi_dst += dt * D psi_src over all modes (one Update.cpp half step).
+int half_step(ovl_ctx *c, const void *src, void *dst) {
+    const Lattice &L = c->L;
+    if (c->p.form == OVL_FORM_FUSED) {
+        ProfScope ps(c, OVL_PROF_HOP);
+        if (fp32(c)) ovl::launch_wilson<float>(c->U, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        else ovl::launch_wilson<double>(c->U, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        return launched(c, 1, "wilson (fused)");
+    }
+    const size_t block_complex = (size_t)L.V * ovl::kComp * ovl::kModeBlock;
+    int n = 0;
+    for (int mb = 0; mb < c->n_mb; mb += c->deriv_mb) {
+        const int nmb = std::min(c->deriv_mb, c->n_mb - mb);
+        char *d = static_cast<char *>(dst) + block_complex * c->elem_bytes * (size_t)mb;
+        {
+            ProfScope ps(c, OVL_PROF_HOP);
+            if (fp32(c)) ovl::launch_wilson<float>(c->U, src, c->deriv, L, mb, nmb, amass(c->p), c->p.dt, false, c->stream);
+            else ovl::launch_wilson<double>(c->U, src, c->deriv, L, mb, nmb, amass(c->p), c->p.dt, false, c->stream);
+        }
+        {
+            ProfScope ps(c, OVL_PROF_AXPY);
+            if (fp32(c)) ovl::launch_axpy<float>(d, c->deriv, block_complex * nmb, c->p.dt, c->sm_count, c->stream);
+            else ovl::launch_axpy<double>(d, c->deriv, block_complex * nmb, c->p.dt, c->sm_count, c->stream);
+        }
+        n += 2;
+    }
+    return launched(c, n, "wilson (plain)");
+}
+
+int run_currents(ovl_ctx *c) {
+    ProfScope ps(c, OVL_PROF_OBS);
+    if (fp32(c))
+        ovl::launch_currents<float>(c->U, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
+                                    c->partial, c->per_site, c->stream);
+    else
+        ovl::launch_currents<double>(c->U, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
+                                     c->partial, c->per_site, c->stream);
+    return launched(c, 2, "currents");
+}
+
+}  // namespace
+
+extern "C" {
+
+int ovl_params_init(ovl_params *p) {
+    if (!p) return OVL_E_ARG;
+    std::memset(p, 0, sizeof *p);
+    p->N[0] = p->N[1] = p->N[2] = 8;
+    p->Nc = 2;
+    p->n_modes = 4 * 2 * 8 * 8 * 8;
+    p->first_mode = 0;
+    p->fermion = OVL_FERMION_WILSON;
+    p->precision = OVL_PREC_FP64;
+    p->form = OVL_FORM_PLAIN;
+    p->r_wilson = 1.0;
+    p->m_fermion = 0.0;
+    p->m_dw = 1.4;
+    p->dt = 0.02;
+    p->qs = 1.0;
+    p->t_sphaleron = 6.0;
+    p->device = 0;
+    p->plain_chunk_modes = 0;
+    p->stream = 0;
+    return OVL_OK;
+}
+
+int ovl_create(const ovl_params *p, ovl_ctx **out) {
+    if (!p || !out) return fail(nullptr, OVL_E_ARG, "ovl_create: null argument");
+    *out = nullptr;
+    for (int i = 0; i < 3; i++)
+        if (p->N[i] < 3 || p->N[i] > 1024) return fail(nullptr, OVL_E_ARG, "ovl_create: N[%d]=%d outside [3, 1024]", i, p->N[i]);
+    if (p->Nc != 2) return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: Nc=%d not built (SU(2) only)", p->Nc);
+    if (p->fermion != OVL_FERMION_WILSON) return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: fermion kind %d not built", p->fermion);
+    if (p->precision != OVL_PREC_FP64 && p->precision != OVL_PREC_FP32) return fail(nullptr, OVL_E_ARG, "ovl_create: bad precision");
+    if (p->form != OVL_FORM_PLAIN && p->form != OVL_FORM_FUSED) return fail(nullptr, OVL_E_ARG, "ovl_create: bad form");
+    if (p->n_modes <= 0 || p->first_mode < 0) return fail(nullptr, OVL_E_ARG, "ovl_create: n_modes=%d first_mode=%d", p->n_modes, p->first_mode);
+    if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return fail(nullptr, OVL_E_ARG, "ovl_create: dt must be positive");
+    const long long V = (long long)p->N[0] * p->N[1] * p->N[2];
+    if (V > (1LL << 30) / 8) return fail(nullptr, OVL_E_ARG, "ovl_create: lattice too large");
+
+    ovl_ctx *c = new (std::nothrow) ovl_ctx();
+    if (!c) return fail(nullptr, OVL_E_OOM, "ovl_create: host allocation failed");
+    c->p = *p;
+    c->L = Lattice{p->N[0], p->N[1], p->N[2], (int)V};
+    c->n_mb = (p->n_modes + ovl::kModeBlock - 1) / ovl::kModeBlock;
+    c->elem_bytes = p->precision == OVL_PREC_FP32 ? 8 : 16;
+    c->field_complex = (size_t)c->n_mb * V * ovl::kComp * ovl::kModeBlock;
+    int rc = OVL_OK;
+    auto bail = [&](int code) { g_err = c->err; ovl_destroy(c); return code; };
+    if ((rc = set_device(c)) != OVL_OK) return bail(rc);
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, p->device);
+    if (p->stream) {
+        c->stream = reinterpret_cast<cudaStream_t>(p->stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(fail(c, OVL_E_CUDA, "ovl_create: stream creation failed"));
+        c->own_stream = true;
+    }
+    const size_t field_bytes = c->field_complex * c->elem_bytes;
+    auto alloc = [&](void **ptr, size_t bytes, const char *what) -> int {
+        if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, OVL_E_OOM, "ovl_create: cannot allocate %zu bytes for %s", bytes, what);
+        }
+        return OVL_OK;
+    };
+    if ((rc = alloc(&c->psi, field_bytes, "Psi")) || (rc = alloc(&c->psimid, field_bytes, "PsiMid")) ||
+        (rc = alloc((void **)&c->U, sizeof(double) * 12 * V, "links")) ||
+        (rc = alloc((void **)&c->E, sizeof(double) * 9 * V, "efield")))
+        return bail(rc);
+    if (p->form == OVL_FORM_PLAIN) {
+        int chunk = p->plain_chunk_modes > 0 ? p->plain_chunk_modes : p->n_modes;
+        c->deriv_mb = std::min(c->n_mb, (chunk + ovl::kModeBlock - 1) / ovl::kModeBlock);
+        if ((rc = alloc(&c->deriv, (size_t)c->deriv_mb * V * ovl::kComp * ovl::kModeBlock * c->elem_bytes, "derivative buffer")))
+            return bail(rc);
+    }
+    c->partial_doubles = std::max({ovl::currents_partial_doubles(c->L, c->n_mb), ovl::ncsdot_partial_doubles(c->L),
+                                   ovl::bulk_partial_doubles(c->L)});
+    if ((rc = alloc((void **)&c->partial, sizeof(double) * c->partial_doubles, "reduction scratch")) ||
+        (rc = alloc((void **)&c->per_site, sizeof(double) * ovl::kCurrentsPerSite * V, "currents")) ||
+        (rc = alloc((void **)&c->dev_small, sizeof(double) * 64, "results")) ||
+        (rc = alloc((void **)&c->dev_int, sizeof(int) * 4, "flags")))
+        return bail(rc);
+    if (cudaMallocHost(&c->host_small, sizeof(double) * 64) != cudaSuccess)
+        return bail(fail(c, OVL_E_OOM, "ovl_create: pinned host allocation failed"));
+    cudaMemsetAsync(c->psi, 0, field_bytes, c->stream);
+    cudaMemsetAsync(c->psimid, 0, field_bytes, c->stream);
+    cudaMemsetAsync(c->E, 0, sizeof(double) * 9 * V, c->stream);
+    // links start at the identity (GaugeLinks::SetIdentity)
+    std::vector<double> unit(12 * V, 0.0);
+    for (long long l = 0; l < 3 * V; l++) unit[4 * l + 3] = 1.0;
+    cudaMemcpyAsync(c->U, unit.data(), sizeof(double) * 12 * V, cudaMemcpyHostToDevice, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(c, OVL_E_CUDA, "ovl_create: initialisation failed"));
+    *out = c;
+    return OVL_OK;
+}
+
+int ovl_destroy(ovl_ctx *c) {
+    if (!c) return OVL_OK;
+    cudaSetDevice(c->p.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void *bufs[] = {c->psi, c->psimid, c->U, c->E, c->deriv, c->per_site, c->partial, c->dev_small, c->dev_int};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (c->host_small) cudaFreeHost(c->host_small);
+    for (auto &v : c->prof)
+        for (auto &pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return OVL_OK;
+}
+
+const char *ovl_last_error(const ovl_ctx *c) { return c ? c->err.c_str() : g_err.c_str(); }
+
+int ovl_set_links(ovl_ctx *c, const double *links) {
+    if (!c || !links) return fail(c, OVL_E_ARG, "ovl_set_links: null argument");
+    const size_t n = (size_t)12 * c->L.V;
+    if (!all_finite(links, n)) return fail(c, OVL_E_NONFINITE, "ovl_set_links: non-finite link component");
+    int rc = set_device(c);
+    if (rc) return rc;
+    OVL_CUDA(c, cudaMemcpyAsync(c->U, links, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return OVL_OK;
+}
+
+int ovl_get_links(ovl_ctx *c, double *links) {
+    if (!c || !links) return fail(c, OVL_E_ARG, "ovl_get_links: null argument");
+    int rc = set_device(c);
+    if (rc) return rc;
+    OVL_CUDA(c, cudaMemcpyAsync(links, c->U, sizeof(double) * 12 * c->L.V, cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return OVL_OK;
+}
+
+int ovl_set_efield(ovl_ctx *c, const double *efield) {
+    if (!c || !efield) return fail(c, OVL_E_ARG, "ovl_set_efield: null argument");
+    const size_t n = (size_t)9 * c->L.V;
+    if (!all_finite(efield, n)) return fail(c, OVL_E_NONFINITE, "ovl_set_efield: non-finite field component");
+    int rc = set_device(c);
+    if (rc) return rc;
+    OVL_CUDA(c, cudaMemcpyAsync(c->E, efield, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return OVL_OK;
+}
+
+int ovl_get_efield(ovl_ctx *c, double *efield) {
+    if (!c || !efield) return fail(c, OVL_E_ARG, "ovl_get_efield: null argument");
+    int rc = set_device(c);
+    if (rc) return rc;
+    OVL_CUDA(c, cudaMemcpyAsync(efield, c->E, sizeof(double) * 9 * c->L.V, cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return OVL_OK;
+}
+
+// Modes move through a device staging buffer in the reference layout, in
+// chunks that bound the staging memory.
+static int transfer_modes(ovl_ctx *c, int first, int count, const double *hpsi, const double *hmid, double *opsi,
+                          double *omid, bool upload) {
+    if (!c) return OVL_E_ARG;
+    if (first < 0 || count < 0 || first + count > c->p.n_modes)
+        return fail(c, OVL_E_ARG, "modes [%d, %d) outside [0, %d)", first, first + count, c->p.n_modes);
+    if (count == 0) return OVL_OK;
+    int rc = set_device(c);
+    if (rc) return rc;
+    const size_t per_mode = (size_t)c->L.V * ovl::kComp * 2;  // doubles
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)count, ((size_t)256 << 20) / (per_mode * 8)));
+    double *stage = nullptr;
+    if (cudaMalloc(&stage, per_mode * 8 * chunk) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, OVL_E_OOM, "mode staging buffer (%zu bytes)", per_mode * 8 * chunk);
+    }
+    int status = OVL_OK;
+    for (int f = 0; f < 2 && status == OVL_OK; f++) {
+        const double *hin = f == 0 ? hpsi : hmid;
+        double *hout = f == 0 ? opsi : omid;
+        void *field = f == 0 ? c->psi : c->psimid;
+        if (upload ? !hin : !hout) continue;
+        for (int m = first; m < first + count && status == OVL_OK; m += chunk) {
+            const int n = std::min(chunk, first + count - m);
+            const size_t off = per_mode * (size_t)(m - first);
+            if (upload) {
+                cudaError_t e = cudaMemcpyAsync(stage, hin + off, per_mode * 8 * n, cudaMemcpyHostToDevice, c->stream);
+                if (e != cudaSuccess) { status = cuda_fail(c, e, "mode upload"); break; }
+                if (fp32(c)) ovl::launch_ref_to_blocks<float>(stage, field, c->L, m, n, c->stream);
+                else ovl::launch_ref_to_blocks<double>(stage, field, c->L, m, n, c->stream);
+                status = launched(c, 1, "ref_to_blocks");
+            } else {
+                if (fp32(c)) ovl::launch_blocks_to_ref<float>(field, stage, c->L, m, n, c->stream);
+                else ovl::launch_blocks_to_ref<double>(field, stage, c->L, m, n, c->stream);
+                status = launched(c, 1, "blocks_to_ref");
+                if (status) break;
+                cudaError_t e = cudaMemcpyAsync(hout + off, stage, per_mode * 8 * n, cudaMemcpyDeviceToHost, c->stream);
+                if (e != cudaSuccess) { status = cuda_fail(c, e, "mode download"); break; }
+            }
+            cudaError_t e = cudaStreamSynchronize(c->stream);
+            if (e != cudaSuccess) status = cuda_fail(c, e, "mode transfer");
+        }
+    }
+    cudaFree(stage);
+    return status;
+}
+
+int ovl_set_modes(ovl_ctx *c, int first, int count, const double *psi, const double *psimid) {
+    if (!c) return OVL_E_ARG;
+    return transfer_modes(c, first, count, psi, psimid, nullptr, nullptr, true);
+}
+
+int ovl_get_modes(ovl_ctx *c, int first, int count, double *psi, double *psimid) {
+    if (!c) return OVL_E_ARG;
+    return transfer_modes(c, first, count, nullptr, nullptr, psi, psimid, false);
+}
+
+int ovl_set_free_fermions(ovl_ctx *c, int *n_bad) {
+    if (!c) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (fp32(c))
+        ovl::launch_free_fermions<float>(c->psi, c->psimid, c->L, c->p.n_modes, c->n_mb, c->p.first_mode, c->p.r_wilson,
+                                         c->p.m_fermion, c->p.dt, c->dev_int, c->stream);
+    else
+        ovl::launch_free_fermions<double>(c->psi, c->psimid, c->L, c->p.n_modes, c->n_mb, c->p.first_mode, c->p.r_wilson,
+                                          c->p.m_fermion, c->p.dt, c->dev_int, c->stream);
+    if ((rc = launched(c, 2, "free fermions"))) return rc;
+    int bad = 0;
+    OVL_CUDA(c, cudaMemcpyAsync(&bad, c->dev_int, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (n_bad) *n_bad = bad;
+    return OVL_OK;
+}
+
+int ovl_step(ovl_ctx *c, int nsteps) {
+    if (!c) return OVL_E_ARG;
+    if (nsteps < 0) return fail(c, OVL_E_ARG, "ovl_step: nsteps=%d", nsteps);
+    int rc = set_device(c);
+    if (rc) return rc;
+    for (int n = 0; n < nsteps; n++) {
+        const bool move = c->p.qs * (c->tsteps * c->p.dt) < c->p.t_sphaleron;  // Update.cpp:57
+        if ((rc = half_step(c, c->psimid, c->psi))) return rc;
+        if (move) {
+            {
+                ProfScope ps(c, OVL_PROF_LINKS);
+                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream);
+            }
+            if ((rc = launched(c, 1, "update links"))) return rc;
+        }
+        if ((rc = half_step(c, c->psi, c->psimid))) return rc;
+        if (move) {
+            {
+                ProfScope ps(c, OVL_PROF_LINKS);
+                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream);
+            }
+            if ((rc = launched(c, 1, "update links"))) return rc;
+        }
+        c->tsteps++;
+    }
+    return OVL_OK;
+}
+
+int ovl_get_step_count(const ovl_ctx *c, int *steps) {
+    if (!c || !steps) return OVL_E_ARG;
+    *steps = c->tsteps;
+    return OVL_OK;
+}
+
+int ovl_set_step_count(ovl_ctx *c, int steps) {
+    if (!c || steps < 0) return OVL_E_ARG;
+    c->tsteps = steps;
+    return OVL_OK;
+}
+
+int ovl_currents(ovl_ctx *c, double *jV, double *jA, double *jVw, double *jAw, double *PS, double *WA) {
+    if (!c) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    if ((rc = run_currents(c))) return rc;
+    const int V = c->L.V;
+    std::vector<double> h((size_t)V * ovl::kCurrentsPerSite);
+    OVL_CUDA(c, cudaMemcpyAsync(h.data(), c->per_site, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int s = 0; s < V; s++) {
+        const double *q = h.data() + (size_t)s * ovl::kCurrentsPerSite;
+        for (int mu = 0; mu < 4; mu++) {
+            if (jV) jV[4 * s + mu] = q[mu];
+            if (jA) jA[4 * s + mu] = q[4 + mu];
+            if (jVw) jVw[4 * s + mu] = q[8 + mu];
+            if (jAw) jAw[4 * s + mu] = q[12 + mu];
+        }
+        if (PS) PS[s] = q[16];
+        if (WA) WA[s] = q[17];
+    }
+    return OVL_OK;
+}
+
+int ovl_charges(ovl_ctx *c, double out[4]) {
+    if (!c || !out) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    if ((rc = run_currents(c))) return rc;
+    ovl::launch_site_sums(c->per_site, c->L, c->partial, c->dev_small, c->stream);
+    if ((rc = launched(c, 1, "site sums"))) return rc;
+    OVL_CUDA(c, cudaMemcpyAsync(c->host_small, c->dev_small, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 4; k++) out[k] = c->host_small[k];
+    return OVL_OK;
+}
+
+int ovl_ncsdot(ovl_ctx *c, double *out) {
+    if (!c || !out) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    ovl::launch_ncsdot(c->U, c->E, c->L, c->partial, c->dev_small, c->stream);
+    if ((rc = launched(c, 2, "ncsdot"))) return rc;
+    OVL_CUDA(c, cudaMemcpyAsync(c->host_small, c->dev_small, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    *out = c->host_small[0];
+    return OVL_OK;
+}
+
+int ovl_update_links(ovl_ctx *c, double dt_step) {
+    if (!c) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    ovl::launch_update_links(c->U, c->E, c->L, dt_step, c->stream);
+    return launched(c, 1, "update links");
+}
+
+int ovl_update_efield(ovl_ctx *c, double dt_step) {
+    if (!c) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    ovl::launch_update_efield(c->U, c->E, nullptr, c->L, dt_step, c->stream);
+    return launched(c, 1, "update efield");
+}
+
+int ovl_bulk(ovl_ctx *c, double out[10]) {
+    if (!c || !out) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    ovl::launch_bulk(c->U, c->E, c->L, c->partial, c->dev_small, c->stream);
+    if ((rc = launched(c, 2, "bulk"))) return rc;
+    OVL_CUDA(c, cudaMemcpyAsync(c->host_small, c->dev_small, sizeof(double) * 10, cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 10; k++) out[k] = c->host_small[k];
+    return OVL_OK;
+}
+
+int ovl_synchronize(ovl_ctx *c) {
+    if (!c) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return OVL_OK;
+}
+
+int ovl_device_modes(ovl_ctx *c, void **psi, void **psimid, size_t *bytes) {
+    if (!c) return OVL_E_ARG;
+    if (psi) *psi = c->psi;
+    if (psimid) *psimid = c->psimid;
+    if (bytes) *bytes = c->field_complex * c->elem_bytes;
+    return OVL_OK;
+}
+
+int ovl_launch_count(const ovl_ctx *c, uint64_t *count) {
+    if (!c || !count) return OVL_E_ARG;
+    *count = c->launches;
+    return OVL_OK;
+}
+
+int ovl_profile_enable(ovl_ctx *c, int on) {
+    if (!c) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (auto &v : c->prof) {
+        for (auto &pr : v) { c->event_pool.push_back(pr.first); c->event_pool.push_back(pr.second); }
+        v.clear();
+    }
+    c->profiling = on != 0;
+    return OVL_OK;
+}
+
+int ovl_profile_read(ovl_ctx *c, double ms[OVL_PROF_KINDS], uint64_t launches[OVL_PROF_KINDS]) {
+    if (!c || !ms || !launches) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < OVL_PROF_KINDS; k++) {
+        double t = 0.0;
+        for (auto &pr : c->prof[k]) {
+            float e = 0.0f;
+            OVL_CUDA(c, cudaEventElapsedTime(&e, pr.first, pr.second));
+            t += e;
+        }
+        ms[k] = t;
+        launches[k] = c->prof[k].size();
+    }
+    return OVL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,315 @@
+// Gauge-field kernels (all FP64): link update, staple force, the improved
+// E.B of the Chern-Simons rate, and the bulk observables (energy, Gauss law,
+// unitarity).  One thread per site or link; these fields are 3V links and are
+// touched once or twice per leapfrog step, far from the fermion kernels' cost.
+// Reductions are two-stage with a fixed summation order, so results do not
+// depend on scheduling.
+
+#include "ovl_device.cuh"
+#include "ovl_internal.h"
+
+namespace ovl {
+
+constexpr int kReduceThreads = 256;
+
+// Fixed-order block sum of NV values per thread; thread 0 returns the totals.
+template <int NV, bool MAX_LAST>
+__device__ void block_reduce(double (&v)[NV], double *sh) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        double t = v[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            double u = __shfl_down_sync(0xffffffffu, t, o);
+            t = (MAX_LAST && k == NV - 1) ? fmax(t, u) : t + u;
+        }
+        v[k] = t;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int k = 0; k < NV; k++) sh[warp * NV + k] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x >> 5;
+        for (int k = 0; k < NV; k++) {
+            double t = sh[k];
+            for (int w = 1; w < nw; w++) t = (MAX_LAST && k == NV - 1) ? fmax(t, sh[w * NV + k]) : t + sh[w * NV + k];
+            v[k] = t;
+        }
+    }
+}
+
+// ------------------------------------------------------------ link update --
+// U <- exp(i cU E^a t^a) U with cU = -dt (Dynamics.cpp:97-138, Minkowski, a = 1).
+__global__ void update_links_kernel(double *U, const double *__restrict__ E, int n_links, double cU) {
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n_links) return;
+    const double *e = E + 3 * l;
+    quat g = qexp(cU, e[0], e[1], e[2]);
+    const int site = l / 3, mu = l % 3;
+    store_link(U, site, mu, qmul(g, load_link(U, site, mu)));
+}
+
+void launch_update_links(double *U, const double *E, const Lattice &L, double dt_step, cudaStream_t stream) {
+    const int n = 3 * L.V;
+    update_links_kernel<<<(n + 255) / 256, 256, 0, stream>>>(U, E, n, -dt_step);
+}
+
+// ------------------------------------------------------- Wilson loops ------
+__device__ inline quat path_step(const double *__restrict__ U, const Lattice &L, int c[3], int mu, int dir, quat acc) {
+    if (dir > 0) {
+        quat u = load_link(U, site_index(L, c[0], c[1], c[2]), mu);
+        c[mu] += 1;
+        return qmul(acc, u);
+    }
+    c[mu] -= 1;
+    return qmul(acc, qdag(load_link(U, site_index(L, c[0], c[1], c[2]), mu)));
+}
+
+// Counter-clockwise lmu x lnu loop in the (mu, nu) plane with (x, y, z) at its
+// corner in quadrant (smu, snu), holonomy based at that corner.
+__device__ quat loop(const double *__restrict__ U, const Lattice &L, int x, int y, int z, int mu, int nu, int smu,
+                     int snu, int lmu, int lnu) {
+    const int dmu[4] = {mu, nu, mu, nu}, ddir[4] = {+1, +1, -1, -1}, dlen[4] = {lmu, lnu, lmu, lnu};
+    const int start = (smu > 0 && snu > 0) ? 0 : (smu < 0 && snu > 0) ? 1 : (smu < 0 && snu < 0) ? 2 : 3;
+    int c[3] = {x, y, z};
+    quat acc = {0.0, 0.0, 0.0, 1.0};
+    for (int k = 0; k < 4; k++) {
+        const int j = (start + k) & 3;
+        for (int n = 0; n < dlen[j]; n++) acc = path_step(U, L, c, dmu[j], ddir[j], acc);
+    }
+    return acc;
+}
+
+// ------------------------------------------------------------ staple force --
+// E^a_mu(x) += -2 dt sum_{nu != mu} [Re tr(i t^a U_{mu,nu}) + Re tr(i t^a U_{mu,-nu})],
+// both staples written to start with U_mu(x) (Dynamics.cpp:145-197).
+// Re tr(i t^a q) = -q_a.
+__global__ void update_efield_kernel(const double *__restrict__ U, double *E, Lattice L, double gamma) {
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= 3 * L.V) return;
+    const int site = l / 3, mu = l % 3;
+    int x, y, z;
+    site_coords(L, site, x, y, z);
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int nu = 0; nu < 3; nu++) {
+        if (nu == mu) continue;
+        int c[3] = {x, y, z};
+        quat up = {0.0, 0.0, 0.0, 1.0};
+        up = path_step(U, L, c, mu, +1, up);
+        up = path_step(U, L, c, nu, +1, up);
+        up = path_step(U, L, c, mu, -1, up);
+        up = path_step(U, L, c, nu, -1, up);
+        int d[3] = {x, y, z};
+        quat dn = {0.0, 0.0, 0.0, 1.0};
+        dn = path_step(U, L, d, mu, +1, dn);
+        dn = path_step(U, L, d, nu, -1, dn);
+        dn = path_step(U, L, d, mu, -1, dn);
+        dn = path_step(U, L, d, nu, +1, dn);
+        for (int a = 0; a < 3; a++) f[a] += -qcomp(up, a) - qcomp(dn, a);
+    }
+    for (int a = 0; a < 3; a++) E[3 * l + a] += gamma * f[a];
+}
+
+void launch_update_efield(const double *U, double *E, double * /*unused*/, const Lattice &L, double dt_step,
+                          cudaStream_t stream) {
+    const int n = 3 * L.V;
+    update_efield_kernel<<<(n + 127) / 128, 128, 0, stream>>>(U, E, L, -2.0 * dt_step);
+}
+
+// ----------------------------------------------------------------- NCsDot --
+// Improved E_mu at x: -1/12, 7/12, 7/12, -1/12 of E_mu at x+mu, x, x-mu, x-2mu
+// transported to x (ChernSimonsOperators.cpp:379-401).
+__device__ void improved_e(const double *__restrict__ U, const double *__restrict__ E, const Lattice &L, int x, int y,
+                           int z, int mu, double out[3]) {
+    int c[3] = {x, y, z};
+    const int s0 = site_index(L, c[0], c[1], c[2]);
+    c[mu] += 1;
+    const int sp = site_index(L, c[0], c[1], c[2]);
+    c[mu] -= 2;
+    const int sm = site_index(L, c[0], c[1], c[2]);
+    c[mu] -= 1;
+    const int smm = site_index(L, c[0], c[1], c[2]);
+    const quat um = load_link(U, sm, mu);
+    adj3 Rp = adjoint(load_link(U, s0, mu));
+    adj3 Rm = adjoint(qdag(um));
+    adj3 Rmm = adjoint(qmul(qdag(um), qdag(load_link(U, smm, mu))));
+    const double *ep = E + 3 * (mu + 3 * sp), *e0 = E + 3 * (mu + 3 * s0);
+    const double *em = E + 3 * (mu + 3 * sm), *emm = E + 3 * (mu + 3 * smm);
+    for (int a = 0; a < 3; a++) {
+        double t = (7.0 / 12.0) * e0[a];
+        for (int b = 0; b < 3; b++)
+            t += -(1.0 / 12.0) * Rp.r[a][b] * ep[b] + (7.0 / 12.0) * Rm.r[a][b] * em[b] -
+                 (1.0 / 12.0) * Rmm.r[a][b] * emm[b];
+        out[a] = t;
+    }
+}
+
+// Improved B for the (mu, nu) plane: 5/12 of the four plaquettes and -1/24 of
+// the eight 2x1 rectangles with x at a corner, all counter-clockwise and based
+// at x; B^a = 2 Re tr(i t^a avg) (ChernSimonsOperators.cpp:283-421).
+__device__ void improved_b(const double *__restrict__ U, const Lattice &L, int x, int y, int z, int mu, int nu,
+                           double out[3]) {
+    double avg[4] = {0.0, 0.0, 0.0, 0.0};
+    const int sg[4][2] = {{+1, +1}, {-1, +1}, {-1, -1}, {+1, -1}};
+    for (int q = 0; q < 4; q++) {
+        quat box = loop(U, L, x, y, z, mu, nu, sg[q][0], sg[q][1], 1, 1);
+        quat r1 = loop(U, L, x, y, z, mu, nu, sg[q][0], sg[q][1], 2, 1);
+        quat r2 = loop(U, L, x, y, z, mu, nu, sg[q][0], sg[q][1], 1, 2);
+        avg[0] += (5.0 / 12.0) * box.v0 - (1.0 / 24.0) * (r1.v0 + r2.v0);
+        avg[1] += (5.0 / 12.0) * box.v1 - (1.0 / 24.0) * (r1.v1 + r2.v1);
+        avg[2] += (5.0 / 12.0) * box.v2 - (1.0 / 24.0) * (r1.v2 + r2.v2);
+    }
+    for (int a = 0; a < 3; a++) out[a] = -2.0 * avg[a];
+}
+
+__global__ void __launch_bounds__(kReduceThreads) ncsdot_kernel(const double *__restrict__ U, const double *__restrict__ E,
+                                                                 Lattice L, double *partial) {
+    __shared__ double sh[32];
+    double v[1] = {0.0};
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.V; s += gridDim.x * blockDim.x) {
+        int x, y, z;
+        site_coords(L, s, x, y, z);
+        const int plane[3][2] = {{1, 2}, {2, 0}, {0, 1}};  // B_x from yz, B_y from zx, B_z from xy
+        for (int mu = 0; mu < 3; mu++) {
+            double e[3], b[3];
+            improved_e(U, E, L, x, y, z, mu, e);
+            improved_b(U, L, x, y, z, plane[mu][0], plane[mu][1], b);
+            v[0] += e[0] * b[0] + e[1] * b[1] + e[2] * b[2];
+        }
+    }
+    block_reduce<1, false>(v, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v[0];
+}
+
+template <int NV, bool MAX_LAST>
+__global__ void finish_kernel(const double *__restrict__ partial, int n, double *out, double scale) {
+    __shared__ double sh[32 * NV];
+    double v[NV];
+    for (int k = 0; k < NV; k++) v[k] = (MAX_LAST && k == NV - 1) ? -1e300 : 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        for (int k = 0; k < NV; k++) {
+            double p = partial[(size_t)i * NV + k];
+            v[k] = (MAX_LAST && k == NV - 1) ? fmax(v[k], p) : v[k] + p;
+        }
+    block_reduce<NV, MAX_LAST>(v, sh);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NV; k++) out[k] = (MAX_LAST && k == NV - 1) ? v[k] : scale * v[k];
+}
+
+static int reduce_blocks(int V) {
+    int b = (V + kReduceThreads - 1) / kReduceThreads;
+    return b < 1024 ? b : 1024;
+}
+
+size_t ncsdot_partial_doubles(const Lattice &L) { return (size_t)reduce_blocks(L.V); }
+
+void launch_ncsdot(const double *U, const double *E, const Lattice &L, double *partial, double *out, cudaStream_t stream) {
+    const int nb = reduce_blocks(L.V);
+    ncsdot_kernel<<<nb, kReduceThreads, 0, stream>>>(U, E, L, partial);
+    // NCsDot = E.B / (8 pi^2) (ChernSimonsDerivative.cpp:48)
+    finish_kernel<1, false><<<1, kReduceThreads, 0, stream>>>(partial, nb, out, 0.125 / (M_PI * M_PI));
+}
+
+// ------------------------------------------------------------------- bulk --
+// Per-thread sums: E^2 per direction (3), B^2 per direction (3), Gauss
+// violation squares, unitarity squares, unitarity max, Gauss max (last, max-reduced).
+constexpr int kBulkVals = 10;
+
+__global__ void __launch_bounds__(kReduceThreads) bulk_kernel(const double *__restrict__ U, const double *__restrict__ E,
+                                                               Lattice L, double *partial) {
+    __shared__ double sh[32 * kBulkVals];
+    double v[kBulkVals];
+    for (int k = 0; k < kBulkVals; k++) v[k] = 0.0;
+    double umax = 0.0, gmax = 0.0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.V; s += gridDim.x * blockDim.x) {
+        int x, y, z;
+        site_coords(L, s, x, y, z);
+        for (int mu = 0; mu < 3; mu++)
+            for (int a = 0; a < 3; a++) {
+                double e = E[a + 3 * (mu + 3 * s)];
+                v[mu] += e * e;
+            }
+        // B^2_k = 4 Re tr(1 - U_plaq) of the plaquette orthogonal to k (BulkObservables.cpp:72-77)
+        const int plane[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+        for (int k = 0; k < 3; k++) {
+            quat pl = loop(U, L, x, y, z, plane[k][0], plane[k][1], +1, +1, 1, 1);
+            v[3 + k] += 4.0 * 2.0 * (1.0 - pl.s);
+        }
+        // G^a = sum_mu E_mu(x) - (U^+ E U)(x - mu)
+        double g[3] = {0.0, 0.0, 0.0};
+        for (int mu = 0; mu < 3; mu++) {
+            int c[3] = {x, y, z};
+            c[mu] -= 1;
+            const int sm = site_index(L, c[0], c[1], c[2]);
+            adj3 R = adjoint(qdag(load_link(U, sm, mu)));
+            for (int a = 0; a < 3; a++) {
+                double t = E[a + 3 * (mu + 3 * s)];
+                for (int b = 0; b < 3; b++) t -= R.r[a][b] * E[b + 3 * (mu + 3 * sm)];
+                g[a] += t;
+            }
+        }
+        for (int a = 0; a < 3; a++) {
+            gmax = fmax(gmax, g[a]);  // signed maximum, as GaussLawViolation.cpp:44
+            v[6] += g[a] * g[a];
+        }
+        for (int mu = 0; mu < 3; mu++) {
+            quat u = load_link(U, s, mu);
+            double dev = fabs(u.v0 * u.v0 + u.v1 * u.v1 + u.v2 * u.v2 + u.s * u.s - 1.0);
+            umax = fmax(umax, dev);
+            v[7] += dev * dev;
+        }
+    }
+    v[8] = umax;
+    v[9] = gmax;
+    // max-reduce slot 8 by hand; block_reduce max-reduces only the last slot
+    double vm[1] = {v[8]};
+    v[8] = 0.0;
+    block_reduce<kBulkVals, true>(v, sh);
+    __syncthreads();
+    double t = vm[0];
+    for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_down_sync(0xffffffffu, t, o));
+    __shared__ double shm[32];
+    if ((threadIdx.x & 31) == 0) shm[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) t = fmax(t, shm[w]);
+        for (int k = 0; k < kBulkVals; k++) partial[(size_t)blockIdx.x * (kBulkVals + 1) + k] = v[k];
+        partial[(size_t)blockIdx.x * (kBulkVals + 1) + kBulkVals] = t;
+    }
+}
+
+__global__ void bulk_finish_kernel(const double *__restrict__ partial, int n, Lattice L, double *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s[kBulkVals + 1];
+    for (int k = 0; k <= kBulkVals; k++) s[k] = 0.0;
+    double gmax = 0.0, umax = 0.0;
+    for (int i = 0; i < n; i++) {
+        const double *p = partial + (size_t)i * (kBulkVals + 1);
+        for (int k = 0; k < 8; k++) s[k] += p[k];
+        gmax = fmax(gmax, p[9]);
+        umax = fmax(umax, p[10]);
+    }
+    const double V = (double)L.V;
+    double e2[3], b2[3];
+    for (int k = 0; k < 3; k++) { e2[k] = s[k] / V; b2[k] = s[3 + k] / V; }
+    out[0] = 0.5 * (e2[0] + e2[1] + e2[2] + b2[0] + b2[1] + b2[2]);
+    out[1] = 0.5 * ((e2[1] + e2[2] + b2[1] + b2[2]) - (e2[0] + b2[0]));
+    out[2] = 0.5 * ((e2[0] + e2[2] + b2[0] + b2[2]) - (e2[1] + b2[1]));
+    out[3] = 0.5 * ((e2[0] + e2[1] + b2[0] + b2[1]) - (e2[2] + b2[2]));
+    out[4] = 0.5 * (e2[0] + e2[1] + e2[2]);
+    out[5] = 0.5 * (b2[0] + b2[1] + b2[2]);
+    out[6] = gmax;
+    out[7] = sqrt(s[6] / (3.0 * V));
+    out[8] = umax;
+    out[9] = sqrt(s[7] / (3.0 * V));
+}
+
+size_t bulk_partial_doubles(const Lattice &L) { return (size_t)reduce_blocks(L.V) * (kBulkVals + 1); }
+
+void launch_bulk(const double *U, const double *E, const Lattice &L, double *partial, double *out, cudaStream_t stream) {
+    const int nb = reduce_blocks(L.V);
+    bulk_kernel<<<nb, kReduceThreads, 0, stream>>>(U, E, L, partial);
+    bulk_finish_kernel<<<1, 32, 0, stream>>>(partial, nb, L, out);
+}
+
+}  // namespace ovl

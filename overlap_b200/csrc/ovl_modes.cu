@@ -1,0 +1,406 @@
+// Kernels over the mode batch other than the Wilson operator: the fermion
+// currents and their lattice sums, layout conversion between the reference's
+// per-mode arrays and the mode-block layout, and free plane-wave modes.
+
+#include "ovl_device.cuh"
+#include "ovl_internal.h"
+
+namespace ovl {
+
+// ---------------------------------------------------------------- currents --
+// Fermions::Observables::ComputeCurrents, Wilson (FERMIONS/WILSON/Currents.cpp:7-309).
+// For each mode (vacuum weight w = +1 even / -1 odd global index,
+// FermionField.cpp:109-122) and site, with chi_mu = U_mu(x) psi(x+mu) and
+// chib_mu = U_mu(x-mu)^+ psi(x-mu):
+//   jV^0 = psi^+ psi              jA^0 = psi^+ g5 psi
+//   jV^mu = Re psi^+ g0 g_mu chi   jA^mu = Re psi^+ g0 g_mu g5 chi
+//   jVw^mu = Re psi^+ (-i r g0) chi, jAw^mu = Re psi^+ (-i r g0 g5) chi
+//   PS = Re psi^+ (i g0 g5) psi
+//   WA = Re[-6 psi^+ (-i r g0 g5) psi + sum_mu psi^+ (-i r g0 g5) (chi_mu + chib_mu)]
+// summed over colours and modes, times 1/(2V) (Currents.cpp:289).
+// Output per site: jV[4] jA[4] jVw[4] jAw[4] PS WA (jVw^0 = jAw^0 = 0).
+
+constexpr int kCurrentsThreadsY = kSitesPerCta;
+
+template <typename T>
+__device__ __forceinline__ void load_site(const cpx<T> *__restrict__ f, int V, int mb, int site, int lane,
+                                          cpx<T> (&s)[kColours][kSpin]) {
+    const cpx<T> *p = f + field_index(V, mb, site, 0, lane);
+#pragma unroll
+    for (int c = 0; c < kColours; c++)
+#pragma unroll
+        for (int a = 0; a < kSpin; a++) s[c][a] = ld(p + (c * kSpin + a) * kModeBlock);
+}
+
+// sum over colours of psi^+ G h, in double
+template <typename T>
+__device__ __forceinline__ cpx<double> colour_bilinear(const mono &G, const cpx<T> (&f)[kColours][kSpin],
+                                                        const cpx<double> (&h)[kColours][kSpin]) {
+    cpx<double> t = mk<double>(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < kColours; c++) {
+        cpx<double> fd[kSpin];
+#pragma unroll
+        for (int a = 0; a < kSpin; a++) fd[a] = mk<double>((double)f[c][a].re, (double)f[c][a].im);
+        t = t + bilinear<double>(G, fd, h[c]);
+    }
+    return t;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
+    currents_kernel(const double *__restrict__ U, const cpx<T> *__restrict__ psi, Lattice L, int n_mb, int n_modes,
+                    int first_mode, int groups, double r, double *__restrict__ partial) {
+    constexpr mono G1 = {{0, 1, 2, 3}, {0, 0, 0, 0}};
+    constexpr mono G5 = kGamma5;
+    constexpr mono G05 = mono_mul(kGamma0, kGamma5);
+    constexpr mono G0 = kGamma0;
+    constexpr mono GV[3] = {mono_mul(kGamma0, kGammaX), mono_mul(kGamma0, kGammaY), mono_mul(kGamma0, kGammaZ)};
+    constexpr mono GA[3] = {mono_mul(GV[0], kGamma5), mono_mul(GV[1], kGamma5), mono_mul(GV[2], kGamma5)};
+
+    const int lane = threadIdx.x;
+    const int site = blockIdx.x * kCurrentsThreadsY + threadIdx.y;
+    const int g = blockIdx.y;
+    if (site >= L.V) return;  // whole warps exit together: a warp is one site
+    int x, y, z;
+    site_coords(L, site, x, y, z);
+    const int V = L.V;
+
+    double acc[kCurrentsPerSite];
+#pragma unroll
+    for (int k = 0; k < kCurrentsPerSite; k++) acc[k] = 0.0;
+
+    int nb[3][2];
+    for (int mu = 0; mu < 3; mu++) {
+        int cp[3] = {x, y, z}, cm[3] = {x, y, z};
+        cp[mu] += 1;
+        cm[mu] -= 1;
+        nb[mu][0] = site_index(L, cp[0], cp[1], cp[2]);
+        nb[mu][1] = site_index(L, cm[0], cm[1], cm[2]);
+    }
+
+    for (int mb = g; mb < n_mb; mb += groups) {
+        const int mode = mb * kModeBlock + lane;
+        const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
+        cpx<T> f[kColours][kSpin];
+        load_site(psi, V, mb, site, lane, f);
+        cpx<double> fd[kColours][kSpin];
+#pragma unroll
+        for (int c = 0; c < kColours; c++)
+#pragma unroll
+            for (int a = 0; a < kSpin; a++) fd[c][a] = mk<double>((double)f[c][a].re, (double)f[c][a].im);
+        double v[kCurrentsPerSite];
+#pragma unroll
+        for (int k = 0; k < kCurrentsPerSite; k++) v[k] = 0.0;
+        v[0] = colour_bilinear(G1, f, fd).re;
+        v[4] = colour_bilinear(G5, f, fd).re;
+        const cpx<double> b05 = colour_bilinear(G05, f, fd);
+        v[16] = -b05.im;                 // Re(i x)
+        double wa = -6.0 * r * b05.im;   // -6 Re(-i r x)
+#pragma unroll
+        for (int mu = 0; mu < 3; mu++) {
+            cpx<T> h[kColours][kSpin];
+            cpx<double> chi[kColours][kSpin];
+            // forward: chi = U_mu(x) psi(x+mu)
+            load_site(psi, V, mb, nb[mu][0], lane, h);
+            {
+                const cmat2<double> M = link_matrix<double>(load_link(U, site, mu));
+#pragma unroll
+                for (int a = 0; a < kSpin; a++) {
+                    cpx<double> h0 = mk<double>(h[0][a].re, h[0][a].im), h1 = mk<double>(h[1][a].re, h[1][a].im);
+                    mul(M, h0, h1, chi[0][a], chi[1][a]);
+                }
+            }
+            v[1 + mu] = colour_bilinear(GV[mu], f, chi).re;
+            v[5 + mu] = colour_bilinear(GA[mu], f, chi).re;
+            v[9 + mu] = r * colour_bilinear(G0, f, chi).im;
+            const double aw = r * colour_bilinear(G05, f, chi).im;
+            v[13 + mu] = aw;
+            wa += aw;
+            // backward: chib = U_mu(x-mu)^+ psi(x-mu)
+            load_site(psi, V, mb, nb[mu][1], lane, h);
+            {
+                const cmat2<double> M = link_matrix<double>(load_link(U, nb[mu][1], mu));
+#pragma unroll
+                for (int a = 0; a < kSpin; a++) {
+                    cpx<double> h0 = mk<double>(h[0][a].re, h[0][a].im), h1 = mk<double>(h[1][a].re, h[1][a].im);
+                    mul_dag(M, h0, h1, chi[0][a], chi[1][a]);
+                }
+            }
+            wa += r * colour_bilinear(G05, f, chi).im;
+        }
+        v[17] = wa;
+#pragma unroll
+        for (int k = 0; k < kCurrentsPerSite; k++) acc[k] += w * v[k];
+    }
+    // sum over the 32 modes of the warp, fixed order
+#pragma unroll
+    for (int k = 0; k < kCurrentsPerSite; k++) {
+        double t = acc[k];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        acc[k] = t;
+    }
+    if (lane == 0) {
+        double *p = partial + ((size_t)g * V + site) * kCurrentsPerSite;
+#pragma unroll
+        for (int k = 0; k < kCurrentsPerSite; k++) p[k] = acc[k];
+    }
+}
+
+__global__ void currents_finish_kernel(const double *__restrict__ partial, int groups, int V, double scale,
+                                       double *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = V * kCurrentsPerSite;
+    if (i >= n) return;
+    double t = 0.0;
+    for (int g = 0; g < groups; g++) t += partial[(size_t)g * n + i];
+    out[i] = scale * t;
+}
+
+int currents_groups(int n_mb) { return n_mb < 16 ? n_mb : 16; }
+
+size_t currents_partial_doubles(const Lattice &L, int n_mb) {
+    return (size_t)currents_groups(n_mb) * L.V * kCurrentsPerSite;
+}
+
+template <typename T>
+void launch_currents(const double *U, const void *psi, const Lattice &L, int n_mb, int n_modes, int first_mode,
+                     double r_wilson, double *partial, double *per_site, cudaStream_t stream) {
+    const int groups = currents_groups(n_mb);
+    dim3 block(kModeBlock, kCurrentsThreadsY);
+    dim3 grid((L.V + kCurrentsThreadsY - 1) / kCurrentsThreadsY, groups);
+    currents_kernel<T><<<grid, block, 0, stream>>>(U, reinterpret_cast<const cpx<T> *>(psi), L, n_mb, n_modes,
+                                                   first_mode, groups, r_wilson, partial);
+    const int n = L.V * kCurrentsPerSite;
+    currents_finish_kernel<<<(n + 255) / 256, 256, 0, stream>>>(partial, groups, L.V, 1.0 / (2.0 * L.V), per_site);
+}
+
+// Lattice sums of jV^0, jA^0, PS, WA from the per-site array, fixed order.
+__global__ void site_sums_kernel(const double *__restrict__ per_site, int V, double *__restrict__ out4) {
+    __shared__ double sh[4][256];
+    double t[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int s = threadIdx.x; s < V; s += blockDim.x) {
+        const double *p = per_site + (size_t)s * kCurrentsPerSite;
+        t[0] += p[0];
+        t[1] += p[4];
+        t[2] += p[16];
+        t[3] += p[17];
+    }
+    for (int k = 0; k < 4; k++) sh[k][threadIdx.x] = t[k];
+    __syncthreads();
+    for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+        if ((int)threadIdx.x < stride)
+            for (int k = 0; k < 4; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + stride];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 4; k++) out4[k] = sh[k][0];
+}
+
+void launch_site_sums(const double *per_site, const Lattice &L, double * /*partial*/, double *out4, cudaStream_t stream) {
+    site_sums_kernel<<<1, 256, 0, stream>>>(per_site, L.V, out4);
+}
+
+// ---------------------------------------------------------- layout change --
+template <typename T>
+__global__ void ref_to_blocks_kernel(const double2 *__restrict__ ref, cpx<T> *__restrict__ blocks, int V, int m0,
+                                     int count) {
+    const size_t n = (size_t)count * V * kComp;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int comp = (int)(i % kComp);
+        const size_t ms = i / kComp;
+        const int site = (int)(ms % V);
+        const int m = m0 + (int)(ms / V);
+        const double2 v = ref[i];
+        st(blocks + field_index(V, m / kModeBlock, site, comp, m % kModeBlock), mk<T>((T)v.x, (T)v.y));
+    }
+}
+
+template <typename T>
+__global__ void blocks_to_ref_kernel(const cpx<T> *__restrict__ blocks, double2 *__restrict__ ref, int V, int m0,
+                                     int count) {
+    const size_t n = (size_t)count * V * kComp;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int comp = (int)(i % kComp);
+        const size_t ms = i / kComp;
+        const int site = (int)(ms % V);
+        const int m = m0 + (int)(ms / V);
+        const cpx<T> v = blocks[field_index(V, m / kModeBlock, site, comp, m % kModeBlock)];
+        ref[i] = double2{(double)v.re, (double)v.im};
+    }
+}
+
+static int grid_for(size_t n) {
+    size_t b = (n + 255) / 256;
+    return (int)(b < 65535 ? b : 65535);
+}
+
+template <typename T>
+void launch_ref_to_blocks(const double *ref, void *blocks, const Lattice &L, int m0, int count, cudaStream_t stream) {
+    const size_t n = (size_t)count * L.V * kComp;
+    if (n == 0) return;
+    ref_to_blocks_kernel<T><<<grid_for(n), 256, 0, stream>>>(reinterpret_cast<const double2 *>(ref),
+                                                             reinterpret_cast<cpx<T> *>(blocks), L.V, m0, count);
+}
+
+template <typename T>
+void launch_blocks_to_ref(const void *blocks, double *ref, const Lattice &L, int m0, int count, cudaStream_t stream) {
+    const size_t n = (size_t)count * L.V * kComp;
+    if (n == 0) return;
+    blocks_to_ref_kernel<T><<<grid_for(n), 256, 0, stream>>>(reinterpret_cast<const cpx<T> *>(blocks),
+                                                             reinterpret_cast<double2 *>(ref), L.V, m0, count);
+}
+
+// ------------------------------------------------------------ plane waves --
+// InitialConditions::SetFreeFermions with GetWilsonDiracSpinor / GetWilsonPhase
+// (SetFreeFermions.cpp:3-56, FermionField.cpp:145-328): mode index
+// particle + 2(colour + Nc(spin + 2(px + N0(py + N1 pz)))); particles
+// exp(+i p.x) with frequency +w, antiparticles exp(-i p.x) with -w; psimid =
+// psi exp(-i w dt / 2).
+struct FreeMode { double u[8]; double omega; int colour, k0, k1, k2, particle, bad; };
+
+__device__ FreeMode free_mode(const Lattice &L, int g, double r, double m) {
+    FreeMode fm;
+    const int N[3] = {L.N0, L.N1, L.N2};
+    fm.particle = g % 2; g /= 2;
+    fm.colour = g % kColours; g /= kColours;
+    const int spin = g % 2; g /= 2;
+    int k[3];
+    k[0] = g % N[0]; g /= N[0];
+    k[1] = g % N[1]; g /= N[1];
+    k[2] = g % N[2];
+    fm.k0 = k[0]; fm.k1 = k[1]; fm.k2 = k[2];
+    double pp[3], meff = m, p2 = 0.0;
+    for (int i = 0; i < 3; i++) {
+        const int n = fm.particle == 0 ? k[i] : N[i] - k[i];
+        pp[i] = sin(2.0 * M_PI * n / (double)N[i]);
+        const double h = sin(M_PI * n / (double)N[i]);
+        meff += 2.0 * r * h * h;
+        p2 += pp[i] * pp[i];
+    }
+    const double pabs = sqrt(p2);
+    const double w = sqrt(p2 + meff * meff);
+    const double omega = fm.particle == 0 ? w : -w;
+    fm.omega = omega;
+    bool edge[3];
+    for (int i = 0; i < 3; i++) edge[i] = (k[i] == 0 || 2 * k[i] == N[i]);
+    cpx<double> phi0, phi1;
+    double hel;
+    if (edge[0] && edge[1]) {
+        phi0 = mk<double>(spin == 0 ? 1.0 : 0.0, 0.0);
+        phi1 = mk<double>(spin == 0 ? 0.0 : 1.0, 0.0);
+        hel = (spin == 0 ? 1.0 : -1.0) * pp[2] / fabs(pp[2]);
+        if (edge[2]) hel = 0.0;
+    } else {
+        hel = spin == 0 ? 1.0 : -1.0;
+        // q = -(pz - hel |p|) / (px - i py)
+        const double nr = -(pp[2] - hel * pabs);
+        const double den = pp[0] * pp[0] + pp[1] * pp[1];
+        const cpx<double> q = mk<double>(nr * pp[0] / den, nr * pp[1] / den);
+        const double d = sqrt(1.0 + q.re * q.re + q.im * q.im);
+        phi0 = mk<double>(1.0 / d, 0.0);
+        phi1 = mk<double>(q.re / d, q.im / d);
+    }
+    cpx<double> u[4];
+    if (edge[0] && edge[1] && edge[2]) {
+        const bool upper = (fm.particle == 0) == (meff >= 0.0);
+        const cpx<double> zero = mk<double>(0.0, 0.0);
+        u[0] = upper ? phi0 : zero;
+        u[1] = upper ? phi1 : zero;
+        u[2] = upper ? zero : phi0;
+        u[3] = upper ? zero : phi1;
+    } else {
+        const double norm = sqrt(2.0 * omega * (omega - meff) / p2);
+        const double lower = hel * (omega - meff) / pabs;
+        u[0] = (1.0 / norm) * phi0;
+        u[1] = (1.0 / norm) * phi1;
+        u[2] = (lower / norm) * phi0;
+        u[3] = (lower / norm) * phi1;
+    }
+    // eigen-residual |w u - H u| and |u|^2 - 1 with H = g0 (meff + p.gamma) (FermionField.cpp:270-312)
+    constexpr mono G0 = kGamma0;
+    constexpr mono GX0 = mono_mul(kGamma0, kGammaX), GY0 = mono_mul(kGamma0, kGammaY), GZ0 = mono_mul(kGamma0, kGammaZ);
+    bool bad = false;
+    double n2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        cpx<double> hu = (G0.ph[a] == 0 ? meff : -meff) * u[G0.perm[a]];
+        hu = hu + pp[0] * iphase(GX0.ph[a], u[GX0.perm[a]]) + pp[1] * iphase(GY0.ph[a], u[GY0.perm[a]]) +
+             pp[2] * iphase(GZ0.ph[a], u[GZ0.perm[a]]);
+        const cpx<double> dlt = omega * u[a] - hu;
+        if (sqrt(dlt.re * dlt.re + dlt.im * dlt.im) > 1e-6) bad = true;
+        n2 += u[a].re * u[a].re + u[a].im * u[a].im;
+    }
+    if (fabs(n2 - 1.0) > 1e-6) bad = true;
+    fm.bad = bad ? 1 : 0;
+    for (int a = 0; a < 4; a++) { fm.u[2 * a] = u[a].re; fm.u[2 * a + 1] = u[a].im; }
+    return fm;
+}
+
+__global__ void free_modes_kernel(FreeMode *info, int n_modes, int first_mode, Lattice L, double r, double m, int *bad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_modes) return;
+    FreeMode fm = free_mode(L, first_mode + i, r, m);
+    info[i] = fm;
+    if (fm.bad) atomicAdd(bad, 1);
+}
+
+template <typename T>
+__global__ void free_fill_kernel(const FreeMode *__restrict__ info, cpx<T> *psi, cpx<T> *psimid, Lattice L, int n_modes,
+                                 int n_mb, double dt) {
+    const int lane = threadIdx.x;
+    const int site = blockIdx.x * blockDim.y + threadIdx.y;
+    const int mb = blockIdx.y;
+    if (site >= L.V) return;
+    const int m = mb * kModeBlock + lane;
+    int x, y, z;
+    site_coords(L, site, x, y, z);
+    cpx<double> u[4] = {mk<double>(0, 0), mk<double>(0, 0), mk<double>(0, 0), mk<double>(0, 0)};
+    cpx<double> phase = mk<double>(0, 0), half = mk<double>(1, 0);
+    int colour = -1;
+    if (m < n_modes) {
+        const FreeMode fm = info[m];
+        for (int a = 0; a < 4; a++) u[a] = mk<double>(fm.u[2 * a], fm.u[2 * a + 1]);
+        const double arg = (fm.k0 * x) / (double)L.N0 + (fm.k1 * y) / (double)L.N1 + (fm.k2 * z) / (double)L.N2;
+        double sn, cs;
+        sincos((fm.particle == 0 ? 2.0 : -2.0) * M_PI * arg, &sn, &cs);
+        phase = mk<double>(cs, sn);
+        sincos(-0.5 * fm.omega * dt, &sn, &cs);
+        half = mk<double>(cs, sn);
+        colour = fm.colour;
+    }
+    for (int c = 0; c < kColours; c++)
+        for (int a = 0; a < kSpin; a++) {
+            cpx<double> v = c == colour ? phase * u[a] : mk<double>(0, 0);
+            cpx<double> vm = c == colour ? v * half : mk<double>(0, 0);
+            const size_t idx = field_index(L.V, mb, site, c * kSpin + a, lane);
+            st(psi + idx, mk<T>((T)v.re, (T)v.im));
+            st(psimid + idx, mk<T>((T)vm.re, (T)vm.im));
+        }
+}
+
+template <typename T>
+void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes, int n_mb, int first_mode,
+                          double r_wilson, double m_fermion, double dt, int *bad, cudaStream_t stream) {
+    FreeMode *info = nullptr;
+    cudaMallocAsync(&info, sizeof(FreeMode) * (size_t)n_modes, stream);
+    cudaMemsetAsync(bad, 0, sizeof(int), stream);
+    free_modes_kernel<<<(n_modes + 127) / 128, 128, 0, stream>>>(info, n_modes, first_mode, L, r_wilson, m_fermion, bad);
+    dim3 block(kModeBlock, kSitesPerCta);
+    dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
+    free_fill_kernel<T><<<grid, block, 0, stream>>>(info, reinterpret_cast<cpx<T> *>(psi), reinterpret_cast<cpx<T> *>(psimid),
+                                                    L, n_modes, n_mb, dt);
+    cudaFreeAsync(info, stream);
+}
+
+#define OVL_INSTANTIATE(T)                                                                                          \
+    template void launch_currents<T>(const double *, const void *, const Lattice &, int, int, int, double, double *, \
+                                     double *, cudaStream_t);                                                       \
+    template void launch_ref_to_blocks<T>(const double *, void *, const Lattice &, int, int, cudaStream_t);          \
+    template void launch_blocks_to_ref<T>(const void *, double *, const Lattice &, int, int, cudaStream_t);         \
+    template void launch_free_fermions<T>(void *, void *, const Lattice &, int, int, int, double, double, double,    \
+                                          int *, cudaStream_t);
+OVL_INSTANTIATE(double)
+OVL_INSTANTIATE(float)
+
+}  // namespace ovl

@@ -1,0 +1,73 @@
+"""Generates tests/golden/*.npz from the reference's own code.
+
+Runs the reference hot path compiled from source (oracle/_ref/libovlref_*.so,
+built by `make -C oracle ref` where the reference tree is available) on small
+seeded inputs and stores inputs and outputs.  The fixtures pin the oracle
+restatement (tests/test_oracle_pin.py) and the GPU path (tests/test_gpu_*.py)
+on machines without the reference.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent))
+sys.path.insert(0, str(HERE.parents[1]))
+
+from _oracle import ptr, reference  # noqa: E402
+from overlap_b200.inputs import random_efield, random_links, volume  # noqa: E402
+
+# name: lattice, MPI emulation (nranks, rank), physics, steps, seeds
+CASES = {
+    "wilson_n4": dict(N=(4, 4, 4), nranks=16, rank=3, m=0.1, r=1.0, mdw=0.0, dt=0.05, steps=4,
+                      link_sigma=0.3, e_sigma=0.1, seed=11, t_sph=1e300),
+    "wilson_n465": dict(N=(4, 6, 5), nranks=30, rank=5, m=0.05, r=1.0, mdw=0.0, dt=0.05, steps=3,
+                        link_sigma=0.5, e_sigma=0.2, seed=12, t_sph=0.08),
+}
+
+
+def run_case(name: str, c: dict) -> dict:
+    R = reference("wilson")
+    N = c["N"]
+    V = volume(N)
+    m = R.ovlref_init(*N, c["nranks"], c["rank"], c["m"], c["r"], c["mdw"], c["t_sph"], c["dt"], 1.0, 1)
+    assert m > 0
+    U = random_links(N, c["link_sigma"], c["seed"])
+    E = random_efield(N, c["e_sigma"], c["seed"] + 1000)
+    R.ovlref_set_links(ptr(U))
+    R.ovlref_set_efield(ptr(E))
+    R.ovlref_set_free_fermions()
+    psi0 = np.zeros((m, V, 2, 4), np.complex128)
+    mid0 = np.zeros_like(psi0)
+    R.ovlref_get_modes(ptr(psi0.view(np.float64)), ptr(mid0.view(np.float64)))
+    ncs0 = R.ovlref_ncsdot()
+    bulk0 = np.zeros(10)
+    R.ovlref_bulk(ptr(bulk0))
+    R.ovlref_step(c["steps"])
+    psi = np.zeros_like(psi0)
+    mid = np.zeros_like(psi0)
+    R.ovlref_get_modes(ptr(psi.view(np.float64)), ptr(mid.view(np.float64)))
+    U1 = np.zeros_like(U)
+    R.ovlref_get_links(ptr(U1))
+    cur = [np.zeros(4 * V) for _ in range(4)] + [np.zeros(V), np.zeros(V)]
+    assert R.ovlref_currents(*[ptr(a) for a in cur]) == 6
+    E1 = E.copy()
+    R.ovlref_update_efield(c["dt"])
+    R.ovlref_get_efield(ptr(E1))
+    first = R.ovlref_first_mode()
+    return dict(N=np.array(N), first_mode=first, n_modes=m, m_fermion=c["m"], r_wilson=c["r"], m_dw=c["mdw"],
+                dt=c["dt"], steps=c["steps"], t_sphaleron=c["t_sph"], links=U, efield=E, psi0=psi0, psimid0=mid0,
+                ncsdot0=ncs0, bulk0=bulk0, psi=psi, psimid=mid, links_after=U1, jV=cur[0], jA=cur[1], jVw=cur[2],
+                jAw=cur[3], PS=cur[4], WA=cur[5], efield_after_update=E1)
+
+
+if __name__ == "__main__":
+    for name, c in CASES.items():
+        out = HERE / f"{name}.npz"
+        np.savez_compressed(out, **run_case(name, c))
+        print(out, out.stat().st_size, "bytes")

@@ -1,0 +1,206 @@
+"""GPU parity of the fermion leapfrog, plane-wave init and currents.
+
+Every test drives the CUDA library through the C ABI (overlap_b200.Context) and
+compares with the oracle, the golden vectors the reference produced, or the
+reference compiled from source.  Tolerances: FP64 forms 1e-12 relative (the
+bar stated for the plain form); FP32 modes 2e-5 relative per step count used
+here.  Current densities are compared after normalising by the size of one
+mode's contribution (the vacuum-weighted mode sum cancels)."""
+import numpy as np
+import pytest
+
+from _helpers import current_scale, oracle_currents, oracle_leapfrog, oracle_params, random_modes, rel_err
+from _oracle import have_reference, ptr, reference
+from overlap_b200 import Context, OvlError
+from overlap_b200.inputs import random_efield, random_links, unit_links, volume
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["wilson_n4", "wilson_n465"]
+FORMS = [("fp64", "plain"), ("fp64", "fused"), ("fp32", "fused"), ("fp32", "plain")]
+
+
+def load(golden_dir, name):
+    g = dict(np.load(golden_dir / f"{name}.npz"))
+    g["N"] = tuple(int(n) for n in g["N"])
+    return g
+
+
+def ctx_for(g, precision, form, **kw):
+    return Context(N=g["N"], n_modes=int(g["n_modes"]), first_mode=int(g["first_mode"]), precision=precision,
+                   form=form, r_wilson=float(g["r_wilson"]), m_fermion=float(g["m_fermion"]), m_dw=float(g["m_dw"]),
+                   dt=float(g["dt"]), qs=1.0, t_sphaleron=float(g["t_sphaleron"]), **kw)
+
+
+def tol(precision):
+    return 1e-12 if precision == "fp64" else 2e-5
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("precision,form", FORMS)
+def test_leapfrog_matches_reference_golden(golden_dir, name, precision, form):
+    g = load(golden_dir, name)
+    with ctx_for(g, precision, form) as ctx:
+        ctx.set_links(g["links"])
+        ctx.set_efield(g["efield"])
+        ctx.set_modes(g["psi0"], g["psimid0"])
+        ctx.step(int(g["steps"]))
+        assert ctx.step_count == int(g["steps"])
+        psi, mid = ctx.get_modes()
+        assert rel_err(psi, g["psi"]) < tol(precision)
+        assert rel_err(mid, g["psimid"]) < tol(precision)
+        assert rel_err(ctx.get_links(), g["links_after"]) < 1e-13
+        cur = ctx.currents()
+        scale = current_scale(g["psi"])
+        ctol = 1e-12 if precision == "fp64" else 1e-5
+        for k in ("jV", "jA", "jVw", "jAw", "PS", "WA"):
+            assert np.max(np.abs(cur[k].ravel() - g[k])) <= ctol * scale, k
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_free_fermions_match_reference_golden(golden_dir, name, precision):
+    g = load(golden_dir, name)
+    with ctx_for(g, precision, "fused") as ctx:
+        assert ctx.set_free_fermions() == 0
+        psi, mid = ctx.get_modes()
+        t = 1e-13 if precision == "fp64" else 1e-6
+        assert np.max(np.abs(psi - g["psi0"])) < t
+        assert np.max(np.abs(mid - g["psimid0"])) < t
+
+
+@pytest.mark.parametrize("precision,form", FORMS)
+def test_ragged_modes_odd_offset_asymmetric_lattice(precision, form):
+    """45 modes (one partial mode block), odd first mode, N = (5, 4, 6), random
+    modes and links, links frozen after the second step."""
+    N = (5, 4, 6)
+    n, first = 45, 7
+    U = random_links(N, 0.9, 31)
+    E = random_efield(N, 0.4, 32)
+    psi0 = random_modes(n, N, 33)
+    mid0 = random_modes(n, N, 34)
+    p = oracle_params(N, m=0.07, r=1.0, mdw=0.2, dt=0.03, t_sph=0.05)
+    opsi, omid, oU, _ = oracle_leapfrog(p, U, E, psi0, mid0, 6)
+    with Context(N=N, n_modes=n, first_mode=first, precision=precision, form=form, m_fermion=0.07, r_wilson=1.0,
+                 m_dw=0.2, dt=0.03, t_sphaleron=0.05, plain_chunk_modes=40) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_modes(psi0, mid0)
+        ctx.step(6)
+        psi, mid = ctx.get_modes()
+        assert rel_err(psi, opsi) < tol(precision)
+        assert rel_err(mid, omid) < tol(precision)
+        assert rel_err(ctx.get_links(), oU) < 1e-13
+        ocur = oracle_currents(p, oU, opsi, first)
+        cur = ctx.currents()
+        scale = current_scale(opsi)
+        for k in ocur:
+            assert np.max(np.abs(cur[k] - ocur[k])) <= (1e-12 if precision == "fp64" else 1e-5) * scale, k
+        ch = ctx.charges()
+        assert abs(ch["N5"] - cur["jA"][:, 0].sum()) <= 1e-12 * scale * volume(N)
+        assert abs(ch["NV"] - cur["jV"][:, 0].sum()) <= 1e-12 * scale * volume(N)
+
+
+def test_partial_mode_transfers_roundtrip():
+    N = (4, 4, 4)
+    with Context(N=N, n_modes=70, precision="fp32", form="fused") as ctx:
+        a = random_modes(70, N, 41)
+        ctx.set_modes(a, a)
+        b = random_modes(9, N, 42)
+        ctx.set_modes(b, None, first=33)
+        psi, mid = ctx.get_modes()
+        expect = a.copy()
+        expect[33:42] = b
+        assert np.max(np.abs(psi - expect)) < 1e-6
+        assert np.max(np.abs(mid - a)) < 1e-6
+        part, _ = ctx.get_modes(first=60, count=10)
+        assert np.max(np.abs(part - a[60:70])) < 1e-6
+
+
+def test_free_plane_waves_evolve_by_their_frequency():
+    """U = 1: each free Wilson mode is an eigenmode; over many steps the leapfrog
+    keeps |psi| per site constant and the plain and fused forms agree."""
+    N = (6, 6, 6)
+    out = {}
+    for form in ("plain", "fused"):
+        with Context(N=N, precision="fp64", form=form, m_fermion=0.1, m_dw=0.0, dt=0.05) as ctx:
+            ctx.set_links(unit_links(N))
+            assert ctx.set_free_fermions() == 0
+            ctx.step(40)
+            out[form] = ctx.get_modes()[0]
+    assert rel_err(out["fused"], out["plain"]) < 1e-12
+    dens = np.sum(np.abs(out["fused"]) ** 2, axis=(2, 3))
+    assert np.max(np.abs(dens - dens[:, :1])) < 1e-10
+
+
+@pytest.mark.skipif(not have_reference("wilson"), reason="reference library not built")
+def test_config1_against_reference_mode_slice():
+    """SU(2), N = 8, m = 0.1, r = 1, MDWHeight = 0, dt = 0.05, all 4096 plane-wave
+    modes on the GPU, links exp(i A.sigma/2) with A ~ N(0, 0.3^2), E = 0, 200
+    steps.  The reference (compiled from source) evolves the 64-mode slice of MPI
+    rank 37 of 64; the GPU's copy of that slice must agree to 1e-12."""
+    N = (8, 8, 8)
+    V = volume(N)
+    U = random_links(N, 0.3, 20261203)
+    E = np.zeros((V, 3, 3))
+    R = reference("wilson")
+    m = R.ovlref_init(*N, 64, 37, 0.1, 1.0, 0.0, 6.0, 0.05, 1.0, 1)
+    first = R.ovlref_first_mode()
+    R.ovlref_set_links(ptr(U))
+    R.ovlref_set_efield(ptr(E))
+    R.ovlref_set_free_fermions()
+    R.ovlref_step(200)
+    rpsi = np.zeros((m, V, 2, 4), np.complex128)
+    rmid = np.zeros_like(rpsi)
+    R.ovlref_get_modes(ptr(rpsi.view(np.float64)), ptr(rmid.view(np.float64)))
+    for form in ("plain", "fused"):
+        with Context(N=N, precision="fp64", form=form, m_fermion=0.1, r_wilson=1.0, m_dw=0.0, dt=0.05,
+                     t_sphaleron=6.0) as ctx:
+            ctx.set_links(U)
+            ctx.set_efield(E)
+            assert ctx.set_free_fermions() == 0
+            ctx.step(200)
+            psi, mid = ctx.get_modes(first=first, count=m)
+            assert rel_err(psi, rpsi) < 1e-12, form
+            assert rel_err(mid, rmid) < 1e-12, form
+
+
+def test_fp32_tracks_fp64_axial_charge():
+    """FP32 modes against FP64 on the same inputs: after 50..200 steps N_5 agrees
+    to 1e-6 of the scale of its terms (sum over modes and sites of
+    |psi|^2 / 2V = n_modes / 2 for plane waves)."""
+    N = (8, 8, 8)
+    U = random_links(N, 0.3, 5)
+    E = random_efield(N, 0.05, 6)
+    res = {}
+    for prec in ("fp64", "fp32"):
+        with Context(N=N, precision=prec, form="fused", m_fermion=0.1, m_dw=0.0, dt=0.05, t_sphaleron=1e9) as ctx:
+            ctx.set_links(U)
+            ctx.set_efield(E)
+            ctx.set_free_fermions()
+            n5 = []
+            for _ in range(4):
+                ctx.step(50)
+                n5.append(ctx.charges()["N5"])
+            res[prec] = np.array(n5)
+    scale = 8 * volume(N) / 2.0
+    assert np.max(np.abs(res["fp32"] - res["fp64"])) <= 1e-6 * scale
+
+
+def test_errors_leave_the_context_usable():
+    N = (4, 4, 4)
+    with Context(N=N, n_modes=32, precision="fp64", form="fused") as ctx:
+        bad = unit_links(N)
+        bad[3, 1, 2] = np.nan
+        with pytest.raises(OvlError, match="NONFINITE"):
+            ctx.set_links(bad)
+        with pytest.raises(OvlError, match="OVL_E_ARG"):
+            ctx.get_modes(first=30, count=5)
+        with pytest.raises(OvlError, match="OVL_E_ARG"):
+            ctx.step(-1)
+        ctx.set_links(unit_links(N))
+        ctx.set_free_fermions()
+        before = ctx.launch_count
+        ctx.step(2)
+        assert ctx.launch_count > before
+        assert np.isfinite(ctx.charges()["NV"])
