@@ -50,7 +50,7 @@ typedef enum { OVL_FORM_PLAIN = 0, OVL_FORM_FUSED = 1 } ovl_form;
 
 typedef struct {
     int N[3];             /* lattice extents N0, N1, N2 */
-    int Nc;               /* colours; 2 (SU(2)) */
+    int n_colours;        /* colours; 2 (SU(2)) */
     int n_modes;          /* modes held by this context */
     int first_mode;       /* global index of local mode 0 (MPI/ModePartition.cpp:12-24) */
     int fermion;          /* ovl_fermion */

@@ -20,7 +20,7 @@ STATUS_NAMES = {
 
 class ovl_params(C.Structure):
     _fields_ = [
-        ("N", C.c_int * 3), ("Nc", C.c_int), ("n_modes", C.c_int), ("first_mode", C.c_int),
+        ("N", C.c_int * 3), ("n_colours", C.c_int), ("n_modes", C.c_int), ("first_mode", C.c_int),
         ("fermion", C.c_int), ("precision", C.c_int), ("form", C.c_int),
         ("r_wilson", C.c_double), ("m_fermion", C.c_double), ("m_dw", C.c_double), ("dt", C.c_double),
         ("qs", C.c_double), ("t_sphaleron", C.c_double), ("device", C.c_int), ("plain_chunk_modes", C.c_int),

@@ -63,7 +63,7 @@ class Params:
         p = _lib.ovl_params()
         _lib.lib().ovl_params_init(C.byref(p))
         p.N[0], p.N[1], p.N[2] = (int(n) for n in self.N)
-        p.Nc = 2
+        p.n_colours = 2
         p.n_modes = int(self.n_modes if self.n_modes is not None else 8 * volume(self.N))
         p.first_mode = int(self.first_mode)
         p.fermion = FERMIONS[self.fermion]

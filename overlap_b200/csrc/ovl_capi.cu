@@ -166,7 +166,7 @@ int ovl_params_init(ovl_params *p) {
     if (!p) return OVL_E_ARG;
     std::memset(p, 0, sizeof *p);
     p->N[0] = p->N[1] = p->N[2] = 8;
-    p->Nc = 2;
+    p->n_colours = 2;
     p->n_modes = 4 * 2 * 8 * 8 * 8;
     p->first_mode = 0;
     p->fermion = OVL_FERMION_WILSON;
@@ -189,7 +189,7 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     *out = nullptr;
     for (int i = 0; i < 3; i++)
         if (p->N[i] < 3 || p->N[i] > 1024) return fail(nullptr, OVL_E_ARG, "ovl_create: N[%d]=%d outside [3, 1024]", i, p->N[i]);
-    if (p->Nc != 2) return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: Nc=%d not built (SU(2) only)", p->Nc);
+    if (p->n_colours != 2) return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: n_colours=%d not built (SU(2) only)", p->n_colours);
     if (p->fermion != OVL_FERMION_WILSON) return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: fermion kind %d not built", p->fermion);
     if (p->precision != OVL_PREC_FP64 && p->precision != OVL_PREC_FP32) return fail(nullptr, OVL_E_ARG, "ovl_create: bad precision");
     if (p->form != OVL_FORM_PLAIN && p->form != OVL_FORM_FUSED) return fail(nullptr, OVL_E_ARG, "ovl_create: bad form");

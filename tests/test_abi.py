@@ -34,7 +34,7 @@ def test_params_init_matches_reference_defaults():
     assert _lib.lib().ovl_params_init(C.byref(p)) == 0
     # Simulation.cpp:74,168,194-200 and Dynamics.cpp:17
     assert (p.r_wilson, p.m_fermion, p.m_dw, p.dt, p.qs, p.t_sphaleron) == (1.0, 0.0, 1.4, 0.02, 1.0, 6.0)
-    assert p.Nc == 2
+    assert p.n_colours == 2
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
