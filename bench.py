@@ -178,7 +178,7 @@ def time_form(wl, precision, form, steps, warmup, device, profile):
 
     N = wl["N"]
     stream = torch.cuda.Stream(device)  # a real stream: the library and the events share it
-    ctx = Context(N=N, precision=precision, form=form, m_fermion=wl["m"], r_wilson=wl["r"], m_dw=wl["mdw"],
+    ctx = Context(N=N, n_modes=wl.get("modes"), precision=precision, form=form, m_fermion=wl["m"], r_wilson=wl["r"], m_dw=wl["mdw"],
                   dt=wl["dt"], t_sphaleron=1e300, device=device, stream=stream.cuda_stream)
     ctx.torch_stream = stream  # keeps the stream alive as long as the context
     ctx.set_links(random_links(N, wl["link_sigma"], wl["seed"]))
@@ -235,6 +235,45 @@ def time_e2e(ctx, wl, steps, device):
     return secs, h2d, d2h, ch
 
 
+def accuracy(wl, steps, every, device):
+    """FP32 modes against FP64 on the same inputs over `steps` leapfrog steps:
+    for o in (N_5, N_CS) the error max_t |o_32(t) - o_64(t)| / max_t |o_64(t) - o_64(0)|,
+    N_CS accumulated every `every` steps by the cooling-path rule
+    (CoolingMethod::GetDeltaNCs, cooling off)."""
+    import numpy as np
+    import torch
+
+    from overlap_b200 import Context
+    from overlap_b200.inputs import random_efield, random_links
+
+    N = wl["N"]
+    series = {}
+    for prec in ("fp64", "fp32"):
+        ctx = Context(N=N, n_modes=wl.get("modes"), precision=prec, form="fused", m_fermion=wl["m"], r_wilson=wl["r"],
+                      m_dw=wl["mdw"], dt=wl["dt"], t_sphaleron=1e300, device=device)
+        ctx.set_links(random_links(N, wl["link_sigma"], wl["seed"]))
+        ctx.set_efield(random_efield(N, wl["e_sigma"], wl["seed"] + 1))
+        ctx.set_free_fermions()
+        ctx.ncs_update()
+        n5 = [ctx.charges()["N5"]]
+        ncs = [0.0]
+        for _ in range(steps // every):
+            ctx.step(every)
+            n5.append(ctx.charges()["N5"])
+            ncs.append(ctx.ncs_update()[1])
+        ctx.close()
+        series[prec] = (np.array(n5), np.array(ncs))
+        torch.cuda.synchronize(device)
+    out = {"steps": (steps // every) * every, "every": every}
+    for k, name in ((0, "N5"), (1, "NCS")):
+        a, b = series["fp32"][k], series["fp64"][k]
+        span = np.max(np.abs(b - b[0]))
+        out[f"{name}_rel_err"] = float(np.max(np.abs(a - b)) / span) if span > 0 else 0.0
+        out[f"{name}_fp64_final"] = float(b[-1])
+        out[f"{name}_fp64_span"] = float(span)
+    return out
+
+
 # ------------------------------------------------------------ distributed --
 _dist = None
 
@@ -281,12 +320,17 @@ def main():
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="n16")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 forms")
+    ap.add_argument("--modes", type=int, default=0, help="run a smaller case with this many modes (profiling)")
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="FP32-vs-FP64 accuracy leg length in leapfrog steps (0 = skip)")
     args = ap.parse_args()
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
     N = wl["N"]
     V, M = volume(N), n_modes(N)
+    if args.modes:
+        M = wl["modes"] = min(args.modes, M)
     rank, world, local = init_dist()
-    config = {"workload": f"SU(2) Wilson fermions, N={N[0]}x{N[1]}x{N[2]}, {M} modes (complete plane-wave basis), "
+    config = {"workload": f"SU(2) Wilson fermions, N={N[0]}x{N[1]}x{N[2]}, {M} modes (plane-wave basis), "
                           f"r={wl['r']}, m={wl['m']}, MDWHeight={wl['mdw']}, dt={wl['dt']}",
               "lattice": list(N), "modes": M, "gauge_init": f"seeded random links (sigma={wl['link_sigma']}) and "
               f"E (sigma={wl['e_sigma']}), links updated every half step",
@@ -339,6 +383,10 @@ def main():
                            "hop_ms_per_launch": r["prof"]["hop"][0] / max(1, r["prof"]["hop"][1]),
                            "N5": r["charges"]["N5"]}
 
+    acc = None
+    if args.accuracy_steps > 0 and rank == 0:
+        acc = accuracy(wl, args.accuracy_steps, 50, device)
+
     # roofline of the dominant kernel (Wilson fused half step, FP32)
     hop_ms, hop_n = fp32["prof"]["hop"]
     per_launch_ms = hop_ms / max(1, hop_n)
@@ -369,6 +417,8 @@ def main():
         }
         if "plain" in forms:
             line["fp32_vs_fp64_plain"] = value / forms["plain"]["value"]
+        if acc is not None:
+            line["accuracy_fp32_vs_fp64"] = acc
         if cpu is not None:
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)

@@ -65,7 +65,21 @@ typedef struct {
     int device;           /* CUDA device ordinal */
     int plain_chunk_modes;/* OVL_FORM_PLAIN: modes per derivative-buffer chunk (0 = all) */
     uint64_t stream;      /* cudaStream_t to issue work on; 0 = the context creates its own */
+    /* overlap sign function (FERMIONS/OVERLAP/OPERATOR/OverlapOperator.cpp:13-18) */
+    int zolo_poles;       /* NumofZolotarevCoeffs = 25 */
+    double zolo_tol;      /* ZolotarevErrTol = 1e-12 */
+    int cg_max_iter;      /* MaximumCGIter = 1000 */
+    double cg_tol;        /* ConGradErr = 1e-16 */
+    /* OVL_SIGN_ZOLOTAREV (the reference's rational approximation, FP64) or
+     * OVL_SIGN_CHEBYSHEV: (h_W^2)^(-1/2) as a degree-cheb_degree Chebyshev
+     * series of x^(-1/2) on [cheb_eps, 1] after scaling h_W^2 by lambda_max
+     * (FP32 or FP64). */
+    int sign_method;
+    int cheb_degree;
+    double cheb_eps;
 } ovl_params;
+
+typedef enum { OVL_SIGN_ZOLOTAREV = 0, OVL_SIGN_CHEBYSHEV = 1 } ovl_sign_method;
 
 typedef struct ovl_ctx ovl_ctx;
 
@@ -86,6 +100,15 @@ int ovl_get_links(ovl_ctx *ctx, double *links);
 int ovl_set_efield(ovl_ctx *ctx, const double *efield);
 int ovl_get_efield(ovl_ctx *ctx, double *efield);
 
+/* U(1) background of the hopping term: u1 = complex double[N1][N0][2] (re, im),
+ * index mu + 2 (x + N0 y), the layout of QED::U (QED/QED.cpp:6-23); the x and y
+ * links of every z slice are multiplied by these phases, the z links by 1.
+ * NULL removes the background.  In the reference the U(1) field enters only the
+ * initial eigenmodes (INITIALCONDITIONS/FERMIONS/BASIS/OverlapQEDEigenfunctions.cpp:20-49);
+ * coupling it into the evolution is an extension without a reference counterpart.
+ * QED::SetConstantMagneticField (QED.cpp:62-84) gives the flux-n_B field. */
+int ovl_set_u1(ovl_ctx *ctx, const double *u1);
+
 /* Modes first..first+count-1 of Psi / PsiMid in the reference layout; either
  * pointer may be NULL to skip that field.  Replaces writing
  * Fermions::Psi/PsiMid->GetMode(s) on the host. */
@@ -97,10 +120,43 @@ int ovl_get_modes(ovl_ctx *ctx, int first, int count, double *psi, double *psimi
  * modes failing the eigen-residual/normalisation self-check (FermionField.cpp:270-312). */
 int ovl_set_free_fermions(ovl_ctx *ctx, int *n_bad);
 
+/* Spectral bounds (lambda_min, lambda_max) of h_W^2 that place the Zolotarev
+ * approximation of the overlap sign function, as pairs[2*i], pairs[2*i+1] for
+ * the i-th overlap application (two per leapfrog step, one per ovl_currents
+ * call), consumed in order; with count == 1 the one pair serves every
+ * application.  Replaces Dynamics::Fermions::ComputeRitzEigenvalues
+ * (FERMIONS/OVERLAP/OverlapUpdate.cpp:61-97), whose Ritz iteration starts from
+ * a random vector drawn from the reference's RNG. */
+int ovl_set_spectral_bounds(ovl_ctx *ctx, const double *pairs, int count);
+
+/* out = D phi for `count` modes given in the reference layout (host), with the
+ * context's current links: D = -i h_W, WilsonEvoOperator::Compute
+ * (FERMIONS/WILSON/OPERATOR/WilsonOperator.cpp:30-114), or D = -i h_ov,
+ * OverlapOperator::Compute (FERMIONS/OVERLAP/OPERATOR/OverlapOperator.cpp:25-65),
+ * using the current spectral bounds without consuming them.  The context's
+ * modes are not touched. */
+int ovl_apply(ovl_ctx *ctx, int count, const double *phi, double *out);
+
+/* Zolotarev coefficients of the overlap sign function for spectral bounds
+ * [lambda_min, lambda_max] of h_W^2: (h_W^2)^(-1/2) ~ sum_l b[l] / (h_W^2 + d[l]),
+ * l < npoles (OverlapOperations::ZolotarevCoefficients,
+ * FERMIONS/OVERLAP/OPERATOR/ZolotarevCoefficients.cpp:71-175).  *eps receives the
+ * relative error estimate of the approximation on the interval. */
+int ovl_zolotarev(double lambda_min, double lambda_max, double tol, int npoles, double *b, double *d, double *eps);
+
+/* Statistics of the last overlap application.  Zolotarev: out[0] = lockstep
+ * CG iterations, out[1] = largest per-mode iteration count, out[2] = modes
+ * stopped by cg_max_iter (the reference prints a warning and keeps the
+ * result, OverlapU.cpp:113-117).  Chebyshev: out[0] = out[1] = degree,
+ * out[2] = 1 when the bounds put lambda_min below cheb_eps * lambda_max (the
+ * spectrum leaves the approximation interval). */
+int ovl_solver_stats(const ovl_ctx *ctx, int out[3]);
+
 /* nsteps x Dynamics::Fermions::Update(U, E, Psi, PsiMid)
- * (FERMIONS/WILSON/Update.cpp:48-79): psi += dt D(psimid); links half step while
- * Time() < tSphaleron; psimid += dt D(psi); links half step; step counter + 1.
- * Asynchronous on the context's stream. */
+ * (FERMIONS/WILSON/Update.cpp:48-79; overlap: FERMIONS/OVERLAP/OverlapUpdate.cpp:99-135):
+ * psi += dt D(psimid); links half step while Time() < tSphaleron;
+ * psimid += dt D(psi); links half step; step counter + 1.
+ * Asynchronous on the context's stream (overlap: synchronises once per CG iteration). */
 int ovl_step(ovl_ctx *ctx, int nsteps);
 
 /* Leapfrog step counter Dynamics::tSteps. */
@@ -109,7 +165,9 @@ int ovl_set_step_count(ovl_ctx *ctx, int steps);
 
 /* Fermions::Observables::ComputeCurrents (FERMIONS/WILSON/Currents.cpp:7-309) of
  * this context's modes, i.e. the arrays it MPI_Reduces (:326-333): jV, jA, jVw, jAw
- * double[V][4]; PS, WA double[V].  NULL pointers are skipped. */
+ * double[V][4]; PS, WA double[V].  NULL pointers are skipped.  Overlap contexts
+ * compute the overlap currents (FERMIONS/OVERLAP/OverlapCurrents.cpp:5-290): jV, jA
+ * with the -i/2 g0 G g0 h_ov term; jVw, jAw, PS, WA are zero. */
 int ovl_currents(ovl_ctx *ctx, double *jV, double *jA, double *jVw, double *jAw, double *PS, double *WA);
 
 /* Lattice sums of the current densities: out[0] = sum_x jV^0 (vector charge),
@@ -119,6 +177,16 @@ int ovl_charges(ovl_ctx *ctx, double out[4]);
 /* ChernSimonsNumber::NCsDot(U, E): improved E.B / (8 pi^2)
  * (TOPOLOGY/ChernSimonsDerivative.cpp:31-49, CALC/ChernSimonsOperators.cpp:128-439). */
 int ovl_ncsdot(ovl_ctx *ctx, double *out);
+
+/* ChernSimonsNumber::CoolingMethod::Update(1) with cooling switched off (the
+ * production driver runs it with zero cooling steps, Simulation.cpp:258,504-511):
+ * the change of the Chern-Simons number between the links stored by the
+ * previous call (U_old) and the current links (U_new), by the Simpson rule of
+ * GetDeltaNCs(1) (TOPOLOGY/CoolingMethod.cpp:80-125) along the geodesic
+ * U_old -> U_new; then U_old = U_new.  *delta receives the change and *total the
+ * running sum DeltaNCsCoolRealTime.  The first call only stores U_old
+ * (CoolingMethod::Start) and returns 0. */
+int ovl_ncs_update(ovl_ctx *ctx, double *delta, double *total);
 
 /* Dynamics::UpdateGaugeLinks over the whole lattice (DYNAMICS/Dynamics.cpp:97-138):
  * U <- exp(-i dt_step E^a t^a) U. */

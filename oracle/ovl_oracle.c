@@ -143,6 +143,21 @@ static quat q_loop(const orc_params *p, const double *U, int s, int mu, int nu, 
     return q_path(p, U, s, legs, 4);
 }
 
+/* ------------------------------------------------------ U(1) background -- */
+/* Phases multiplying the x and y links of the hopping term (the U(1)
+ * background extension); NULL = none.  Layout of QED::U: mu + 2 (x + N0 y). */
+static const double *g_u1 = NULL;
+
+void orc_set_u1(const double *u1) { g_u1 = u1; }
+
+static void dress(const orc_params *p, int s, int mu, cplx m[2][2]) {
+    if (!g_u1 || mu >= 2) return;
+    const int plane = s % (p->N[0] * p->N[1]);
+    const cplx ph = g_u1[2 * (mu + 2 * plane)] + I * g_u1[2 * (mu + 2 * plane) + 1];
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) m[i][j] *= ph;
+}
+
 /* ----------------------------------------------------------- Dirac algebra -- */
 /* Dirac representation (DiracAlgebra.cpp:5-12). */
 static const cplx G0[4][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, -1, 0}, {0, 0, 0, -1}};
@@ -192,8 +207,10 @@ void orc_wilson_apply(const orc_params *p, const double *U, const double *phi, d
         for (int mu = 0; mu < 3; mu++) {
             cplx Mf[2][2], Mb[2][2];
             q_matrix(q_load(U, s, mu), Mf);
+            dress(p, s, mu, Mf);
             int sb = shift(p, s, mu, -1);
             q_matrix(q_load(U, sb, mu), Mb);
+            dress(p, sb, mu, Mb);
             const cplx *fp = site_spinor(phi, shift(p, s, mu, +1));
             const cplx *fm = site_spinor(phi, sb);
             cplx a[NC][4], b[NC][4];
@@ -426,8 +443,10 @@ void orc_wilson_currents(const orc_params *p, const double *U, const double *psi
             for (int mu = 0; mu < 3; mu++) {
                 cplx Mf[2][2], Mb[2][2], Mbd[2][2];
                 q_matrix(q_load(U, s, mu), Mf);
+                dress(p, s, mu, Mf);
                 int sb = shift(p, s, mu, -1);
                 q_matrix(q_load(U, sb, mu), Mb);
+                dress(p, sb, mu, Mb);
                 for (int i = 0; i < 2; i++)
                     for (int j = 0; j < 2; j++) Mbd[i][j] = conj(Mb[j][i]);
                 const cplx *fp = mode + SPINOR * shift(p, s, mu, +1);

@@ -34,6 +34,13 @@ typedef struct {
     double t_sphaleron;  /* links move while Time() < t_sphaleron */
 } orc_params;
 
+/* U(1) background phases for the hopping term (the x and y links are
+ * multiplied by u1[mu + 2 (x + N0 y)], complex), used by orc_wilson_apply,
+ * orc_wilson_leapfrog and orc_wilson_currents until reset with NULL.  An
+ * extension: the reference couples the U(1) field only into its initial
+ * eigenmodes (OverlapQEDEigenfunctions.cpp:20-49). */
+void orc_set_u1(const double *u1);
+
 /* out = -i h_W phi for one mode (WilsonEvoOperator::Compute, WilsonOperator.cpp:30-114). */
 void orc_wilson_apply(const orc_params *p, const double *U, const double *phi, double *out);
 

@@ -203,6 +203,29 @@ int ovlref_currents(double *jV, double *jA, double *jVw, double *jAw, double *PS
     return (int)g_reduced.size();
 }
 
+/* ChernSimonsNumber::CoolingMethod::GetDeltaNCs(1) with zero cooling steps
+ * (TOPOLOGY/CoolingMethod.cpp:37-125), from the reference's
+ * GeodesicInterpolation and NCsDot; CoolingMethod.cpp itself needs the
+ * gradient-flow module, so the Simpson combination of :80-125 is spelt out. */
+double ovlref_delta_ncs(const double *Uold_in, const double *Unew_in) {
+    GaugeLinks UOld(Lattice::N[0], Lattice::N[1], Lattice::N[2], 1, 1, 1), UNew(Lattice::N[0], Lattice::N[1], Lattice::N[2], 1, 1, 1),
+        UMid(Lattice::N[0], Lattice::N[1], Lattice::N[2], 1, 1, 1);
+    ElectricFields EMid(Lattice::N[0], Lattice::N[1], Lattice::N[2], 1, 1, 1);
+    const size_t nl = 4 * 3 * (size_t)Lattice::Volume;
+    std::memcpy(UOld.U, Uold_in, sizeof(double) * nl);
+    std::memcpy(UNew.U, Unew_in, sizeof(double) * nl);
+    for (INT z = 0; z < Lattice::N[2]; z++)
+        for (INT y = 0; y < Lattice::N[1]; y++)
+            for (INT x = 0; x < Lattice::N[0]; x++)
+                for (INT mu = 0; mu < 3; mu++)
+                    SUNcGroup::AdvancedOperations::GeodesicInterpolation(0.5, UOld.Get(x, y, z, mu), UNew.Get(x, y, z, mu),
+                                                                         UMid.Get(x, y, z, mu), EMid.Get(x, y, z, mu, 0));
+    double value = 4.0 * ChernSimonsNumber::NCsDot(&UMid, &EMid);
+    value += ChernSimonsNumber::NCsDot(&UOld, &EMid);
+    value += ChernSimonsNumber::NCsDot(&UNew, &EMid);
+    return value / 6.0;
+}
+
 /* ChernSimonsNumber::NCsDot (TOPOLOGY/ChernSimonsDerivative.cpp:31-49). */
 double ovlref_ncsdot(void) { return ChernSimonsNumber::NCsDot(GLinks::U, EFields::E); }
 
@@ -274,6 +297,13 @@ double ovlref_zolotarev(double lambda_min, double lambda_max, double *b, double 
     return EvolutionOperator::OverlapOperations::ZolotarevCoefficients(
         lambda_min, lambda_max, EvolutionOperator::OverlapOperator::ZolotarevErrTol,
         EvolutionOperator::OverlapOperator::NumofZolotarevCoeffs, b, d);
+}
+
+/* (MinEValue, MaxEValue) last set by ComputeRitzEigenvalues, e.g. by the
+ * ComputeCurrents call (OverlapCurrents.cpp:106-110). */
+void ovlref_last_bounds(double *out) {
+    out[0] = Dynamics::Fermions::MinEValue;
+    out[1] = Dynamics::Fermions::MaxEValue;
 }
 
 /* Bounds recorded per half step by the leapfrog since the last call. */

@@ -24,7 +24,8 @@ class ovl_params(C.Structure):
         ("fermion", C.c_int), ("precision", C.c_int), ("form", C.c_int),
         ("r_wilson", C.c_double), ("m_fermion", C.c_double), ("m_dw", C.c_double), ("dt", C.c_double),
         ("qs", C.c_double), ("t_sphaleron", C.c_double), ("device", C.c_int), ("plain_chunk_modes", C.c_int),
-        ("stream", C.c_uint64),
+        ("stream", C.c_uint64), ("zolo_poles", C.c_int), ("zolo_tol", C.c_double), ("cg_max_iter", C.c_int),
+        ("cg_tol", C.c_double), ("sign_method", C.c_int), ("cheb_degree", C.c_int), ("cheb_eps", C.c_double),
     ]
 
 
@@ -42,6 +43,7 @@ SIGNATURES = {
     "ovl_get_links": ([_ctx, _dp], C.c_int),
     "ovl_set_efield": ([_ctx, _dp], C.c_int),
     "ovl_get_efield": ([_ctx, _dp], C.c_int),
+    "ovl_set_u1": ([_ctx, _dp], C.c_int),
     "ovl_set_modes": ([_ctx, C.c_int, C.c_int, _dp, _dp], C.c_int),
     "ovl_get_modes": ([_ctx, C.c_int, C.c_int, _dp, _dp], C.c_int),
     "ovl_set_free_fermions": ([_ctx, C.POINTER(C.c_int)], C.c_int),
@@ -51,11 +53,16 @@ SIGNATURES = {
     "ovl_currents": ([_ctx, _dp, _dp, _dp, _dp, _dp, _dp], C.c_int),
     "ovl_charges": ([_ctx, _dp], C.c_int),
     "ovl_ncsdot": ([_ctx, _dp], C.c_int),
+    "ovl_ncs_update": ([_ctx, _dp, _dp], C.c_int),
     "ovl_update_links": ([_ctx, C.c_double], C.c_int),
     "ovl_update_efield": ([_ctx, C.c_double], C.c_int),
     "ovl_bulk": ([_ctx, _dp], C.c_int),
     "ovl_synchronize": ([_ctx], C.c_int),
     "ovl_device_modes": ([_ctx, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_size_t)], C.c_int),
+    "ovl_set_spectral_bounds": ([_ctx, _dp, C.c_int], C.c_int),
+    "ovl_apply": ([_ctx, C.c_int, _dp, _dp], C.c_int),
+    "ovl_zolotarev": ([C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp], C.c_int),
+    "ovl_solver_stats": ([_ctx, C.POINTER(C.c_int)], C.c_int),
     "ovl_launch_count": ([_ctx, C.POINTER(C.c_uint64)], C.c_int),
     "ovl_profile_enable": ([_ctx, C.c_int], C.c_int),
     "ovl_profile_read": ([_ctx, _dp, C.POINTER(C.c_uint64)], C.c_int),

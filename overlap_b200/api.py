@@ -27,8 +27,20 @@ from . import _lib
 from .inputs import volume
 
 PRECISIONS = {"fp64": 0, "fp32": 1}
+SIGN_METHODS = {"zolotarev": 0, "chebyshev": 1}
 FORMS = {"plain": 0, "fused": 1}
 FERMIONS = {"wilson": 0, "overlap": 1}
+
+
+def zolotarev(lambda_min: float, lambda_max: float, tol: float = 1e-12, npoles: int = 25):
+    """Zolotarev coefficients (b, d, eps) of (h_W^2)^(-1/2) on [lambda_min, lambda_max]."""
+    b = np.zeros(npoles)
+    d = np.zeros(npoles)
+    eps = np.zeros(1)
+    rc = _lib.lib().ovl_zolotarev(float(lambda_min), float(lambda_max), float(tol), int(npoles), _dp(b), _dp(d), _dp(eps))
+    if rc != 0:
+        raise OvlError(rc, _lib.lib().ovl_last_error(None).decode())
+    return b, d, float(eps[0])
 
 
 class OvlError(RuntimeError):
@@ -58,6 +70,13 @@ class Params:
     device: int = 0
     plain_chunk_modes: int = 0
     stream: int = 0
+    zolo_poles: int = 25         # OverlapOperator.cpp:13-18
+    zolo_tol: float = 1e-12
+    cg_max_iter: int = 1000
+    cg_tol: float = 1e-16
+    sign_method: str = "zolotarev"  # or "chebyshev" (the FP32-capable polynomial form)
+    cheb_degree: int = 96
+    cheb_eps: float = 0.01
 
     def to_c(self) -> _lib.ovl_params:
         p = _lib.ovl_params()
@@ -74,6 +93,10 @@ class Params:
         p.device = int(self.device)
         p.plain_chunk_modes = int(self.plain_chunk_modes)
         p.stream = int(self.stream)
+        p.zolo_poles, p.zolo_tol = int(self.zolo_poles), float(self.zolo_tol)
+        p.cg_max_iter, p.cg_tol = int(self.cg_max_iter), float(self.cg_tol)
+        p.sign_method = SIGN_METHODS[self.sign_method]
+        p.cheb_degree, p.cheb_eps = int(self.cheb_degree), float(self.cheb_eps)
         return p
 
 
@@ -133,6 +156,16 @@ class Context:
     def set_efield(self, E):
         self._check(self._L.ovl_set_efield(self._ctx, _dp(self._as_f64(E, (self.V, 3, 3)))))
 
+    def set_u1(self, u1):
+        """U(1) background phases complex[N1, N0, 2] (QED::U layout), or None to remove."""
+        if u1 is None:
+            self._check(self._L.ovl_set_u1(self._ctx, None))
+            return
+        a = np.ascontiguousarray(u1, dtype=np.complex128)
+        if a.size != 2 * self.N[0] * self.N[1]:
+            raise ValueError("u1 must hold 2*N0*N1 complex phases")
+        self._check(self._L.ovl_set_u1(self._ctx, _dp(a.view(np.float64))))
+
     def get_efield(self) -> np.ndarray:
         out = np.empty((self.V, 3, 3))
         self._check(self._L.ovl_get_efield(self._ctx, _dp(out)))
@@ -167,6 +200,25 @@ class Context:
         bad = C.c_int(0)
         self._check(self._L.ovl_set_free_fermions(self._ctx, C.byref(bad)))
         return bad.value
+
+    # ------------------------------------------------------------- operator
+    def set_spectral_bounds(self, pairs):
+        """(lambda_min, lambda_max) of h_W^2 per overlap application, in order;
+        one pair serves every application (replaces ComputeRitzEigenvalues)."""
+        a = np.ascontiguousarray(np.asarray(pairs, dtype=np.float64).reshape(-1, 2))
+        self._check(self._L.ovl_set_spectral_bounds(self._ctx, _dp(a), a.shape[0]))
+
+    def apply(self, phi) -> np.ndarray:
+        """-i h phi (Wilson or overlap) for modes complex[count, V, 2, 4]."""
+        a = np.ascontiguousarray(phi, dtype=np.complex128)
+        out = np.empty_like(a)
+        self._check(self._L.ovl_apply(self._ctx, a.shape[0], _dp(a.view(np.float64)), _dp(out.view(np.float64))))
+        return out
+
+    def solver_stats(self) -> dict:
+        o = (C.c_int * 3)()
+        self._check(self._L.ovl_solver_stats(self._ctx, o))
+        return {"iterations": o[0], "max_mode_iterations": o[1], "not_converged": o[2]}
 
     # ------------------------------------------------------------- evolution
     def step(self, nsteps: int = 1):
@@ -209,6 +261,14 @@ class Context:
         o = np.empty(1)
         self._check(self._L.ovl_ncsdot(self._ctx, _dp(o)))
         return float(o[0])
+
+    def ncs_update(self):
+        """ChernSimonsNumber::CoolingMethod::Update(1) without cooling: returns
+        (change since the previous call, running sum)."""
+        d = np.zeros(1)
+        t = np.zeros(1)
+        self._check(self._L.ovl_ncs_update(self._ctx, _dp(d), _dp(t)))
+        return float(d[0]), float(t[0])
 
     def bulk(self) -> dict:
         o = np.empty(10)

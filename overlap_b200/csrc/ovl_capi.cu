@@ -38,6 +38,23 @@ struct ovl_ctx {
     int sm_count = 148;
     uint64_t launches = 0;
     std::string err;
+    // overlap fermions
+    ovl::OverlapWork ow;
+    std::vector<double> bounds;   // (lambda_min, lambda_max) per overlap application
+    size_t bound_next = 0;
+    double coeff_lo = -1.0, coeff_hi = -1.0;
+    ovl::OverlapCoeffs coeffs{};
+    ovl::OverlapStats ostats;
+    ovl::ChebyshevWork cw;
+    std::vector<double> cheb;     // Chebyshev coefficients c_0..c_K
+    void *aux_src = nullptr, *aux_dst = nullptr;  // ovl_apply / overlap currents
+    // U(1) background phases of the hopping term (ovl_set_u1)
+    double *u1 = nullptr;
+    bool u1_on = false;
+    // Chern-Simons number along the cooling path (ovl_ncs_update)
+    double *u_old = nullptr, *u_mid = nullptr, *e_mid = nullptr;
+    bool have_u_old = false;
+    double ncs_total = 0.0;
     // per-kernel timing (ovl_profile_enable): event pairs per kind
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[OVL_PROF_KINDS];
@@ -118,13 +135,68 @@ bool fp32(const ovl_ctx *c) { return c->p.precision == OVL_PREC_FP32; }
 
 double amass(const ovl_params &p) { return 6.0 * p.r_wilson + 2.0 * p.m_fermion - 2.0 * p.m_dw; }
 
+bool overlap(const ovl_ctx *c) { return c->p.fermion == OVL_FERMION_OVERLAP; }
+
+// Zolotarev coefficients for the next overlap application; `consume` advances
+// the bounds schedule (OverlapUpdate.cpp:105,119 recompute the bounds before
+// every half step).
+int next_coeffs(ovl_ctx *c, bool consume) {
+    if (c->bounds.empty()) return fail(c, OVL_E_STATE, "overlap: no spectral bounds set (ovl_set_spectral_bounds)");
+    const size_t pairs = c->bounds.size() / 2;
+    size_t i = pairs == 1 ? 0 : c->bound_next;
+    if (i >= pairs) return fail(c, OVL_E_STATE, "overlap: spectral-bounds schedule exhausted after %zu applications", pairs);
+    const double lo = c->bounds[2 * i], hi = c->bounds[2 * i + 1];
+    if (consume && pairs > 1) c->bound_next++;
+    if (lo != c->coeff_lo || hi != c->coeff_hi) {
+        c->coeffs.npoles = c->p.zolo_poles;
+        ovl::zolotarev(lo, hi, c->p.zolo_tol, c->p.zolo_poles, c->coeffs.b, c->coeffs.d);
+        c->coeffs.cg_tol = c->p.cg_tol;
+        c->coeffs.cg_max_iter = c->p.cg_max_iter;
+        c->coeff_lo = lo;
+        c->coeff_hi = hi;
+    }
+    return OVL_OK;
+}
+
+int run_overlap(ovl_ctx *c, const void *src, void *dst, int n_mb, int n_modes, bool accumulate, bool consume) {
+    if (c->p.sign_method == OVL_SIGN_CHEBYSHEV) {
+        if (c->bounds.empty()) return fail(c, OVL_E_STATE, "overlap: no spectral bounds set (ovl_set_spectral_bounds)");
+        const size_t pairs = c->bounds.size() / 2;
+        const size_t i = pairs == 1 ? 0 : c->bound_next;
+        if (i >= pairs) return fail(c, OVL_E_STATE, "overlap: spectral-bounds schedule exhausted after %zu applications", pairs);
+        if (consume && pairs > 1) c->bound_next++;
+        const double lo = c->bounds[2 * i], hi = c->bounds[2 * i + 1];
+        ProfScope ps(c, OVL_PROF_HOP);
+        uint64_t nl = 0;
+        if (fp32(c))
+            ovl::chebyshev_apply<float>(c->cw, c->U, c->u1_on ? c->u1 : nullptr, src, dst, c->L, n_mb, c->cheb.data(),
+                                        c->p.cheb_degree, c->p.cheb_eps, hi, amass(c->p), c->p.m_dw, c->p.m_fermion,
+                                        c->p.dt, accumulate, c->sm_count, c->stream, &nl);
+        else
+            ovl::chebyshev_apply<double>(c->cw, c->U, c->u1_on ? c->u1 : nullptr, src, dst, c->L, n_mb, c->cheb.data(),
+                                         c->p.cheb_degree, c->p.cheb_eps, hi, amass(c->p), c->p.m_dw, c->p.m_fermion,
+                                         c->p.dt, accumulate, c->sm_count, c->stream, &nl);
+        c->ostats.iterations = c->ostats.max_mode_iterations = c->p.cheb_degree;
+        c->ostats.not_converged = lo < c->p.cheb_eps * hi ? 1 : 0;
+        return launched(c, (int)nl, "overlap operator (Chebyshev)");
+    }
+    int rc = next_coeffs(c, consume);
+    if (rc) return rc;
+    ProfScope ps(c, OVL_PROF_HOP);
+    c->ostats.launches = 0;
+    ovl::overlap_apply(c->ow, c->U, c->u1_on ? c->u1 : nullptr, src, dst, c->L, n_mb, n_modes, c->coeffs, amass(c->p), c->p.m_dw, c->p.m_fermion,
+                       c->p.dt, accumulate, c->sm_count, c->stream, &c->ostats);
+    return launched(c, (int)c->ostats.launches, "overlap operator");
+}
+
 // psi_dst += dt * D psi_src over all modes (one Update.cpp half step).
 int half_step(ovl_ctx *c, const void *src, void *dst) {
     const Lattice &L = c->L;
+    if (overlap(c)) return run_overlap(c, src, dst, c->n_mb, c->p.n_modes, true, true);
     if (c->p.form == OVL_FORM_FUSED) {
         ProfScope ps(c, OVL_PROF_HOP);
-        if (fp32(c)) ovl::launch_wilson<float>(c->U, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
-        else ovl::launch_wilson<double>(c->U, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        if (fp32(c)) ovl::launch_wilson<float>(c->U, c->u1_on ? c->u1 : nullptr, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        else ovl::launch_wilson<double>(c->U, c->u1_on ? c->u1 : nullptr, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
         return launched(c, 1, "wilson (fused)");
     }
     const size_t block_complex = (size_t)L.V * ovl::kComp * ovl::kModeBlock;
@@ -134,8 +206,8 @@ int half_step(ovl_ctx *c, const void *src, void *dst) {
         char *d = static_cast<char *>(dst) + block_complex * c->elem_bytes * (size_t)mb;
         {
             ProfScope ps(c, OVL_PROF_HOP);
-            if (fp32(c)) ovl::launch_wilson<float>(c->U, src, c->deriv, L, mb, nmb, amass(c->p), c->p.dt, false, c->stream);
-            else ovl::launch_wilson<double>(c->U, src, c->deriv, L, mb, nmb, amass(c->p), c->p.dt, false, c->stream);
+            if (fp32(c)) ovl::launch_wilson<float>(c->U, c->u1_on ? c->u1 : nullptr, src, c->deriv, L, mb, nmb, amass(c->p), c->p.dt, false, c->stream);
+            else ovl::launch_wilson<double>(c->U, c->u1_on ? c->u1 : nullptr, src, c->deriv, L, mb, nmb, amass(c->p), c->p.dt, false, c->stream);
         }
         {
             ProfScope ps(c, OVL_PROF_AXPY);
@@ -148,12 +220,22 @@ int half_step(ovl_ctx *c, const void *src, void *dst) {
 }
 
 int run_currents(ovl_ctx *c) {
+    if (overlap(c)) {
+        // ComputeCurrents recomputes the bounds and applies h_ov to every mode
+        // (OverlapCurrents.cpp:106-117)
+        int rc = run_overlap(c, c->psi, c->aux_dst, c->n_mb, c->p.n_modes, false, true);
+        if (rc) return rc;
+        ProfScope ps(c, OVL_PROF_OBS);
+        ovl::launch_overlap_currents(c->psi, c->aux_dst, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->partial,
+                                     c->per_site, c->stream);
+        return launched(c, 2, "overlap currents");
+    }
     ProfScope ps(c, OVL_PROF_OBS);
     if (fp32(c))
-        ovl::launch_currents<float>(c->U, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
+        ovl::launch_currents<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
                                     c->partial, c->per_site, c->stream);
     else
-        ovl::launch_currents<double>(c->U, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
+        ovl::launch_currents<double>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
                                      c->partial, c->per_site, c->stream);
     return launched(c, 2, "currents");
 }
@@ -181,6 +263,13 @@ int ovl_params_init(ovl_params *p) {
     p->device = 0;
     p->plain_chunk_modes = 0;
     p->stream = 0;
+    p->zolo_poles = 25;
+    p->zolo_tol = 1e-12;
+    p->cg_max_iter = 1000;
+    p->cg_tol = 1e-16;
+    p->sign_method = OVL_SIGN_ZOLOTAREV;
+    p->cheb_degree = 96;
+    p->cheb_eps = 0.01;
     return OVL_OK;
 }
 
@@ -190,7 +279,19 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     for (int i = 0; i < 3; i++)
         if (p->N[i] < 3 || p->N[i] > 1024) return fail(nullptr, OVL_E_ARG, "ovl_create: N[%d]=%d outside [3, 1024]", i, p->N[i]);
     if (p->n_colours != 2) return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: n_colours=%d not built (SU(2) only)", p->n_colours);
-    if (p->fermion != OVL_FERMION_WILSON) return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: fermion kind %d not built", p->fermion);
+    if (p->fermion != OVL_FERMION_WILSON && p->fermion != OVL_FERMION_OVERLAP)
+        return fail(nullptr, OVL_E_ARG, "ovl_create: fermion kind %d", p->fermion);
+    if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method != OVL_SIGN_ZOLOTAREV && p->sign_method != OVL_SIGN_CHEBYSHEV)
+        return fail(nullptr, OVL_E_ARG, "ovl_create: sign_method=%d", p->sign_method);
+    if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method == OVL_SIGN_ZOLOTAREV && p->precision != OVL_PREC_FP64)
+        return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: the Zolotarev overlap operator is built in FP64 only");
+    if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method == OVL_SIGN_CHEBYSHEV &&
+        (p->cheb_degree < 1 || p->cheb_degree > ovl::kMaxChebDegree || !(p->cheb_eps > 0.0) || !(p->cheb_eps < 1.0)))
+        return fail(nullptr, OVL_E_ARG, "ovl_create: cheb_degree=%d (1..%d), cheb_eps=%g (0..1)", p->cheb_degree,
+                    ovl::kMaxChebDegree, p->cheb_eps);
+    if (p->fermion == OVL_FERMION_OVERLAP && (p->zolo_poles < 1 || p->zolo_poles > ovl::kMaxPoles || p->cg_max_iter < 1))
+        return fail(nullptr, OVL_E_ARG, "ovl_create: zolo_poles=%d (1..%d), cg_max_iter=%d", p->zolo_poles, ovl::kMaxPoles,
+                    p->cg_max_iter);
     if (p->precision != OVL_PREC_FP64 && p->precision != OVL_PREC_FP32) return fail(nullptr, OVL_E_ARG, "ovl_create: bad precision");
     if (p->form != OVL_FORM_PLAIN && p->form != OVL_FORM_FUSED) return fail(nullptr, OVL_E_ARG, "ovl_create: bad form");
     if (p->n_modes <= 0 || p->first_mode < 0) return fail(nullptr, OVL_E_ARG, "ovl_create: n_modes=%d first_mode=%d", p->n_modes, p->first_mode);
@@ -235,7 +336,7 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
             return bail(rc);
     }
     c->partial_doubles = std::max({ovl::currents_partial_doubles(c->L, c->n_mb), ovl::ncsdot_partial_doubles(c->L),
-                                   ovl::bulk_partial_doubles(c->L)});
+                                   ovl::bulk_partial_doubles(c->L), ovl::charges_partial_doubles(c->L, c->n_mb)});
     if ((rc = alloc((void **)&c->partial, sizeof(double) * c->partial_doubles, "reduction scratch")) ||
         (rc = alloc((void **)&c->per_site, sizeof(double) * ovl::kCurrentsPerSite * V, "currents")) ||
         (rc = alloc((void **)&c->dev_small, sizeof(double) * 64, "results")) ||
@@ -243,6 +344,35 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
         return bail(rc);
     if (cudaMallocHost(&c->host_small, sizeof(double) * 64) != cudaSuccess)
         return bail(fail(c, OVL_E_OOM, "ovl_create: pinned host allocation failed"));
+    if ((rc = alloc(&c->aux_src, field_bytes, "operator input")) || (rc = alloc(&c->aux_dst, field_bytes, "operator output")))
+        return bail(rc);
+    if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method == OVL_SIGN_CHEBYSHEV) {
+        ovl::ChebyshevWork &w = c->cw;
+        if ((rc = alloc(&w.b0, field_bytes, "Clenshaw b")) || (rc = alloc(&w.b1, field_bytes, "Clenshaw b")) ||
+            (rc = alloc(&w.b2, field_bytes, "Clenshaw b")) || (rc = alloc(&w.w, field_bytes, "Clenshaw temporary")))
+            return bail(rc);
+        c->cheb.assign(p->cheb_degree + 1, 0.0);
+        ovl::chebyshev_inverse_sqrt(p->cheb_degree, p->cheb_eps, c->cheb.data());
+    }
+    if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method == OVL_SIGN_ZOLOTAREV) {
+        ovl::OverlapWork &w = c->ow;
+        const size_t mp = (size_t)c->n_mb * ovl::kModeBlock, np = (size_t)p->zolo_poles;
+        if ((rc = alloc(&w.r, field_bytes, "CG residual")) || (rc = alloc(&w.q, field_bytes, "CG direction image")) ||
+            (rc = alloc(&w.t, field_bytes, "CG temporary")) || (rc = alloc(&w.x, field_bytes * np, "shifted solutions")) ||
+            (rc = alloc(&w.p, field_bytes * np, "shifted directions")) ||
+            (rc = alloc((void **)&w.part, sizeof(double) * ovl::kDotChunks * mp, "dot partials")) ||
+            (rc = alloc((void **)&w.rnorm, sizeof(double) * mp * 5, "CG scalars")) ||
+            (rc = alloc((void **)&w.alpha, sizeof(double) * mp * np * 4, "shift scalars")) ||
+            (rc = alloc((void **)&w.active, sizeof(int) * (mp * 3 + 1), "CG flags")) ||
+            (rc = alloc((void **)&w.dz, sizeof(double) * 2 * ovl::kMaxPoles, "Zolotarev coefficients")))
+            return bail(rc);
+        w.bnorm = w.rnorm + mp; w.betam = w.rnorm + 2 * mp; w.pap = w.rnorm + 3 * mp; w.rr = w.rnorm + 4 * mp;
+        w.beta = w.alpha + mp * np; w.z = w.alpha + 2 * mp * np; w.g = w.alpha + 3 * mp * np;
+        w.next = w.active + mp; w.iters = w.active + 2 * mp; w.count = w.active + 3 * mp;
+        w.bz = w.dz + ovl::kMaxPoles;
+        if (cudaMallocHost(&w.host_count, sizeof(int)) != cudaSuccess)
+            return bail(fail(c, OVL_E_OOM, "ovl_create: pinned host allocation failed"));
+    }
     cudaMemsetAsync(c->psi, 0, field_bytes, c->stream);
     cudaMemsetAsync(c->psimid, 0, field_bytes, c->stream);
     cudaMemsetAsync(c->E, 0, sizeof(double) * 9 * V, c->stream);
@@ -259,7 +389,11 @@ int ovl_destroy(ovl_ctx *c) {
     if (!c) return OVL_OK;
     cudaSetDevice(c->p.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void *bufs[] = {c->psi, c->psimid, c->U, c->E, c->deriv, c->per_site, c->partial, c->dev_small, c->dev_int};
+    void *bufs[] = {c->psi, c->psimid, c->U, c->E, c->deriv, c->per_site, c->partial, c->dev_small, c->dev_int,
+                    c->aux_src, c->aux_dst, c->ow.r, c->ow.q, c->ow.t, c->ow.x, c->ow.p, c->ow.part, c->ow.rnorm,
+                    c->ow.alpha, c->ow.active, c->ow.dz, c->u_old, c->u_mid, c->e_mid, c->u1,
+                    c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w};
+    if (c->ow.host_count) cudaFreeHost(c->ow.host_count);
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (c->host_small) cudaFreeHost(c->host_small);
@@ -301,6 +435,26 @@ int ovl_set_efield(ovl_ctx *c, const double *efield) {
     if (rc) return rc;
     OVL_CUDA(c, cudaMemcpyAsync(c->E, efield, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return OVL_OK;
+}
+
+int ovl_set_u1(ovl_ctx *c, const double *u1) {
+    if (!c) return OVL_E_ARG;
+    if (!u1) {
+        c->u1_on = false;
+        return OVL_OK;
+    }
+    const size_t n = (size_t)4 * c->L.N0 * c->L.N1;
+    if (!all_finite(u1, n)) return fail(c, OVL_E_NONFINITE, "ovl_set_u1: non-finite phase");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (!c->u1 && cudaMalloc(&c->u1, sizeof(double) * n) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, OVL_E_OOM, "ovl_set_u1: phases");
+    }
+    OVL_CUDA(c, cudaMemcpyAsync(c->u1, u1, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->u1_on = true;
     return OVL_OK;
 }
 
@@ -456,9 +610,20 @@ int ovl_charges(ovl_ctx *c, double out[4]) {
     if (!c || !out) return OVL_E_ARG;
     int rc = set_device(c);
     if (rc) return rc;
-    if ((rc = run_currents(c))) return rc;
-    ovl::launch_site_sums(c->per_site, c->L, c->partial, c->dev_small, c->stream);
-    if ((rc = launched(c, 1, "site sums"))) return rc;
+    if (overlap(c)) {
+        if ((rc = run_currents(c))) return rc;
+        ovl::launch_site_sums(c->per_site, c->L, c->partial, c->dev_small, c->stream);
+        if ((rc = launched(c, 1, "site sums"))) return rc;
+    } else {
+        ProfScope ps(c, OVL_PROF_OBS);
+        if (fp32(c))
+            ovl::launch_charges<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
+                                       c->partial, c->dev_small, c->stream);
+        else
+            ovl::launch_charges<double>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
+                                        c->partial, c->dev_small, c->stream);
+    }
+    if ((rc = launched(c, 2, "charges"))) return rc;
     OVL_CUDA(c, cudaMemcpyAsync(c->host_small, c->dev_small, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->stream));
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     for (int k = 0; k < 4; k++) out[k] = c->host_small[k];
@@ -474,6 +639,46 @@ int ovl_ncsdot(ovl_ctx *c, double *out) {
     OVL_CUDA(c, cudaMemcpyAsync(c->host_small, c->dev_small, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     *out = c->host_small[0];
+    return OVL_OK;
+}
+
+int ovl_ncs_update(ovl_ctx *c, double *delta, double *total) {
+    if (!c) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    const size_t V = (size_t)c->L.V;
+    if (!c->u_old) {
+        if (cudaMalloc(&c->u_old, sizeof(double) * 12 * V) != cudaSuccess ||
+            cudaMalloc(&c->u_mid, sizeof(double) * 12 * V) != cudaSuccess ||
+            cudaMalloc(&c->e_mid, sizeof(double) * 9 * V) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, OVL_E_OOM, "ovl_ncs_update: link copies");
+        }
+    }
+    double d = 0.0;
+    if (c->have_u_old) {
+        // GetDeltaNCs(1): Simpson weights 1, 4, 1 at x = 0, 1/2, 1 (CoolingMethod.cpp:80-125)
+        double *out = c->dev_small;
+        ovl::launch_geodesic(c->u_old, c->U, 0.5, c->u_mid, c->e_mid, c->L, c->stream);
+        ovl::launch_ncsdot(c->u_mid, c->e_mid, c->L, c->partial, out, c->stream);
+        ovl::launch_ncsdot(c->u_old, c->e_mid, c->L, c->partial, out + 1, c->stream);
+        ovl::launch_ncsdot(c->U, c->e_mid, c->L, c->partial, out + 2, c->stream);
+        if ((rc = launched(c, 7, "ncs update"))) return rc;
+        OVL_CUDA(c, cudaMemcpyAsync(c->host_small, out, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->stream));
+        OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+        const double *h = c->host_small;
+        double value = 0.0, weight = 0.0;
+        value += 4.0 * h[0]; weight += 4.0;
+        value += h[1]; weight += 1.0;
+        value += h[2]; weight += 1.0;
+        d = value / weight;
+        c->ncs_total += d;
+    }
+    OVL_CUDA(c, cudaMemcpyAsync(c->u_old, c->U, sizeof(double) * 12 * V, cudaMemcpyDeviceToDevice, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->have_u_old = true;
+    if (delta) *delta = d;
+    if (total) *total = c->ncs_total;
     return OVL_OK;
 }
 
@@ -524,6 +729,69 @@ int ovl_device_modes(ovl_ctx *c, void **psi, void **psimid, size_t *bytes) {
 int ovl_launch_count(const ovl_ctx *c, uint64_t *count) {
     if (!c || !count) return OVL_E_ARG;
     *count = c->launches;
+    return OVL_OK;
+}
+
+int ovl_set_spectral_bounds(ovl_ctx *c, const double *pairs, int count) {
+    if (!c || !pairs || count < 1) return fail(c, OVL_E_ARG, "ovl_set_spectral_bounds: need at least one pair");
+    for (int i = 0; i < count; i++)
+        if (!(pairs[2 * i] > 0.0) || !(pairs[2 * i + 1] > pairs[2 * i]) || !std::isfinite(pairs[2 * i + 1]))
+            return fail(c, OVL_E_ARG, "ovl_set_spectral_bounds: pair %d = (%g, %g) is not 0 < min < max", i, pairs[2 * i],
+                        pairs[2 * i + 1]);
+    c->bounds.assign(pairs, pairs + 2 * (size_t)count);
+    c->bound_next = 0;
+    return OVL_OK;
+}
+
+int ovl_apply(ovl_ctx *c, int count, const double *phi, double *out) {
+    if (!c || !phi || !out) return OVL_E_ARG;
+    if (count < 1 || count > c->p.n_modes) return fail(c, OVL_E_ARG, "ovl_apply: count=%d outside [1, %d]", count, c->p.n_modes);
+    int rc = set_device(c);
+    if (rc) return rc;
+    const size_t per_mode = (size_t)c->L.V * ovl::kComp * 2;
+    const int n_mb = (count + ovl::kModeBlock - 1) / ovl::kModeBlock;
+    double *stage = nullptr;
+    if (cudaMalloc(&stage, per_mode * 8 * (size_t)count) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, OVL_E_OOM, "ovl_apply: staging buffer");
+    }
+    auto done = [&](int status) { cudaFree(stage); return status; };
+    cudaMemsetAsync(c->aux_src, 0, c->field_complex * c->elem_bytes, c->stream);
+    if (cudaMemcpyAsync(stage, phi, per_mode * 8 * count, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+        return done(fail(c, OVL_E_CUDA, "ovl_apply: upload"));
+    if (fp32(c)) ovl::launch_ref_to_blocks<float>(stage, c->aux_src, c->L, 0, count, c->stream);
+    else ovl::launch_ref_to_blocks<double>(stage, c->aux_src, c->L, 0, count, c->stream);
+    if ((rc = launched(c, 1, "ref_to_blocks"))) return done(rc);
+    if (overlap(c)) {
+        if ((rc = run_overlap(c, c->aux_src, c->aux_dst, n_mb, count, false, false))) return done(rc);
+    } else {
+        if (fp32(c)) ovl::launch_wilson<float>(c->U, c->u1_on ? c->u1 : nullptr, c->aux_src, c->aux_dst, c->L, 0, n_mb, amass(c->p), 0.0, false, c->stream);
+        else ovl::launch_wilson<double>(c->U, c->u1_on ? c->u1 : nullptr, c->aux_src, c->aux_dst, c->L, 0, n_mb, amass(c->p), 0.0, false, c->stream);
+        if ((rc = launched(c, 1, "wilson operator"))) return done(rc);
+    }
+    if (fp32(c)) ovl::launch_blocks_to_ref<float>(c->aux_dst, stage, c->L, 0, count, c->stream);
+    else ovl::launch_blocks_to_ref<double>(c->aux_dst, stage, c->L, 0, count, c->stream);
+    if ((rc = launched(c, 1, "blocks_to_ref"))) return done(rc);
+    if (cudaMemcpyAsync(out, stage, per_mode * 8 * count, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+        return done(fail(c, OVL_E_CUDA, "ovl_apply: download"));
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return done(fail(c, OVL_E_CUDA, "ovl_apply: synchronise"));
+    return done(OVL_OK);
+}
+
+int ovl_zolotarev(double lambda_min, double lambda_max, double tol, int npoles, double *b, double *d, double *eps) {
+    if (!b || !d || npoles < 1 || npoles > ovl::kMaxPoles || !(lambda_min > 0.0) || !(lambda_max > lambda_min) ||
+        !(tol > 0.0))
+        return fail(nullptr, OVL_E_ARG, "ovl_zolotarev: invalid interval, tolerance or pole count");
+    const double e = ovl::zolotarev(lambda_min, lambda_max, tol, npoles, b, d);
+    if (eps) *eps = e;
+    return OVL_OK;
+}
+
+int ovl_solver_stats(const ovl_ctx *c, int out[3]) {
+    if (!c || !out) return OVL_E_ARG;
+    out[0] = c->ostats.iterations;
+    out[1] = c->ostats.max_mode_iterations;
+    out[2] = c->ostats.not_converged;
     return OVL_OK;
 }
 

@@ -101,6 +101,24 @@ template <typename T> struct cmat2 { cpx<T> m00, m01, m10, m11; };
 template <typename T> __device__ __forceinline__ cmat2<T> link_matrix(quat q) {
     return {mk<T>((T)q.s, (T)q.v2), mk<T>((T)q.v1, (T)q.v0), mk<T>((T)-q.v1, (T)q.v0), mk<T>((T)q.s, (T)-q.v2)};
 }
+// Link of direction mu at `site`, dressed by the U(1) background phase of the
+// (x, y) plane when one is set: u1 holds QED::U, index mu + 2 (x + N0 y) for
+// mu = 0, 1 (QED/QED.cpp:6-23); the z links carry no U(1) phase.
+template <typename T>
+__device__ __forceinline__ cmat2<T> dressed_link(const double *__restrict__ U, const double2 *__restrict__ u1,
+                                                 int site, int mu, int n01) {
+    cmat2<T> M = link_matrix<T>(load_link(U, site, mu));
+    if (u1 != nullptr && mu < 2) {
+        const double2 ph = __ldg(u1 + 2 * (site % n01) + mu);
+        const cpx<T> p = mk<T>((T)ph.x, (T)ph.y);
+        M.m00 = p * M.m00;
+        M.m01 = p * M.m01;
+        M.m10 = p * M.m10;
+        M.m11 = p * M.m11;
+    }
+    return M;
+}
+
 // M h
 template <typename T> __device__ __forceinline__ void mul(const cmat2<T> &M, cpx<T> h0, cpx<T> h1, cpx<T> &k0, cpx<T> &k1) {
     k0 = M.m00 * h0 + M.m01 * h1;

@@ -210,6 +210,39 @@ void launch_ncsdot(const double *U, const double *E, const Lattice &L, double *p
     finish_kernel<1, false><<<1, kReduceThreads, 0, stream>>>(partial, nb, out, 0.125 / (M_PI * M_PI));
 }
 
+// ----------------------------------------------------- geodesic interpolation --
+// GeodesicInterpolation (SUNc/AdvancedOperations.cpp:432-443) on every link:
+// E_mid = -i log(U_new U_old^+) (MatrixILog with C = -1, SU2/AlgebraOperations.cpp:59-74),
+// U_mid = exp(-i c E_mid) U_old; E_mid carries the Minkowski factor cE = 1
+// (CoolingMethod.cpp:37-66).
+__global__ void geodesic_kernel(const double *__restrict__ Uold, const double *__restrict__ Unew, double c,
+                                double *Umid, double *Emid, int n_links) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n_links) return;
+    const int site = l / 3, mu = l % 3;
+    const quat uo = load_link(Uold, site, mu);
+    const quat b = qmul(load_link(Unew, site, mu), qdag(uo));
+    const double d = sqrt(b.v0 * b.v0 + b.v1 * b.v1 + b.v2 * b.v2);
+    double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+    if (d != 0.0) {
+        const double arg = atan2(d, b.s);
+        const double M = 2.0 * arg / (-1.0 * d);
+        e0 = M * b.v0;
+        e1 = M * b.v1;
+        e2 = M * b.v2;
+    }
+    Emid[3 * l + 0] = e0;
+    Emid[3 * l + 1] = e1;
+    Emid[3 * l + 2] = e2;
+    store_link(Umid, site, mu, qmul(qexp(-c, e0, e1, e2), uo));
+}
+
+void launch_geodesic(const double *Uold, const double *Unew, double c, double *Umid, double *Emid, const Lattice &L,
+                     cudaStream_t stream) {
+    const int n = 3 * L.V;
+    geodesic_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Uold, Unew, c, Umid, Emid, n);
+}
+
 // ------------------------------------------------------------------- bulk --
 // Per-thread sums: E^2 per direction (3), B^2 per direction (3), Gauss
 // violation squares, unitarity squares, unitarity max, Gauss max (last, max-reduced).

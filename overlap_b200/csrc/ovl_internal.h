@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <stddef.h>
+#include <stdint.h>
 
 namespace ovl {
 
@@ -13,9 +14,10 @@ constexpr int kSitesPerCta = 8;  // sites per CTA of the Wilson kernels (8 warps
 // Wilson operator on mode blocks [mb_first, mb_first + n_mb) of src.
 // accumulate: dst(+same offset) += dt * D src; otherwise dst (a buffer of
 // n_mb blocks) = D src.
+// u1: U(1) background phases (complex per (x, y) plane site and mu = 0, 1), or null.
 template <typename T>
-void launch_wilson(const double *links, const void *src, void *dst, const Lattice &L, int mb_first, int n_mb,
-                   double amass, double dt, bool accumulate, cudaStream_t stream);
+void launch_wilson(const double *links, const double *u1, const void *src, void *dst, const Lattice &L, int mb_first,
+                   int n_mb, double amass, double dt, bool accumulate, cudaStream_t stream);
 template <typename T>
 void launch_axpy(void *dst, const void *deriv, size_t n_complex, double dt, int sm_count, cudaStream_t stream);
 
@@ -27,6 +29,8 @@ void launch_update_efield(const double *U, double *E, double *dE, const Lattice 
 // doubles; out: device array of the result size.
 size_t ncsdot_partial_doubles(const Lattice &L);
 void launch_ncsdot(const double *U, const double *E, const Lattice &L, double *partial, double *out, cudaStream_t stream);
+void launch_geodesic(const double *Uold, const double *Unew, double c, double *Umid, double *Emid, const Lattice &L,
+                     cudaStream_t stream);
 size_t bulk_partial_doubles(const Lattice &L);
 void launch_bulk(const double *U, const double *E, const Lattice &L, double *partial, double *out, cudaStream_t stream);
 
@@ -35,9 +39,17 @@ constexpr int kCurrentsPerSite = 18;
 int currents_groups(int n_mb);
 size_t currents_partial_doubles(const Lattice &L, int n_mb);
 template <typename T>
-void launch_currents(const double *U, const void *psi, const Lattice &L, int n_mb, int n_modes, int first_mode,
-                     double r_wilson, double *partial, double *per_site, cudaStream_t stream);
+void launch_currents(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                     int first_mode, double r_wilson, double *partial, double *per_site, cudaStream_t stream);
 void launch_site_sums(const double *per_site, const Lattice &L, double *partial, double *out4, cudaStream_t stream);
+void launch_currents_finish(const double *partial, int groups, const Lattice &L, double *per_site, cudaStream_t stream);
+void launch_overlap_currents(const void *psi, const void *opsi, const Lattice &L, int n_mb, int n_modes,
+                             int first_mode, double *partial, double *per_site, cudaStream_t stream);
+// Lattice sums N_V, N_5, PS, WA straight from the modes (no per-site maps).
+size_t charges_partial_doubles(const Lattice &L, int n_mb);
+template <typename T>
+void launch_charges(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                    int first_mode, double r_wilson, double *partial, double *out4, cudaStream_t stream);
 
 // Layout conversion between the reference layout (double, [mode][site][comp])
 // and the mode-block layout of precision T.  Modes [m0, m0+count).
@@ -45,6 +57,56 @@ template <typename T>
 void launch_ref_to_blocks(const double *ref, void *blocks, const Lattice &L, int m0, int count, cudaStream_t stream);
 template <typename T>
 void launch_blocks_to_ref(const void *blocks, double *ref, const Lattice &L, int m0, int count, cudaStream_t stream);
+
+// ------------------------------------------------------------------ overlap --
+// Zolotarev coefficients on the host (ovl_zolotarev.cpp); returns the relative
+// error estimate of the approximation.
+double zolotarev(double amin, double amax, double errtol, int npoles, double *b, double *d);
+
+constexpr int kMaxPoles = 64;
+constexpr int kDotChunks = 64;  // site chunks per mode in the two-stage dot products
+
+struct OverlapCoeffs {
+    int npoles;
+    double b[kMaxPoles], d[kMaxPoles];
+    double cg_tol;
+    int cg_max_iter;
+};
+
+// Device work space of the batched multi-shift CG (all FP64, mode-block layout).
+struct OverlapWork {
+    void *r = nullptr, *q = nullptr, *t = nullptr;  // one field each
+    void *x = nullptr, *p = nullptr;                // npoles fields each
+    double *part = nullptr;                         // kDotChunks x modes
+    double *rnorm = nullptr, *bnorm = nullptr, *betam = nullptr, *pap = nullptr, *rr = nullptr;
+    double *alpha = nullptr, *beta = nullptr, *z = nullptr, *g = nullptr;  // npoles x modes
+    int *active = nullptr, *next = nullptr, *iters = nullptr, *count = nullptr;
+    int *host_count = nullptr;                      // pinned
+    double *dz = nullptr, *bz = nullptr;            // npoles
+};
+
+struct OverlapStats {
+    uint64_t launches = 0;
+    int iterations = 0;           // lockstep iterations of the last application
+    int max_mode_iterations = 0;  // largest per-mode count
+    int not_converged = 0;        // modes stopped by the iteration limit
+};
+
+// dst = out or dst += dt * out, out = -i h_ov src, for all modes.
+void overlap_apply(OverlapWork &w, const double *U, const double *u1, const void *src, void *dst, const Lattice &L, int n_mb,
+                   int n_modes, const OverlapCoeffs &co, double amass, double mdw, double mf, double dt,
+                   bool accumulate, int sm_count, cudaStream_t stream, OverlapStats *stats);
+
+// Chebyshev form of the overlap sign function (ovl_chebyshev.cu).
+constexpr int kMaxChebDegree = 1024;
+void chebyshev_inverse_sqrt(int K, double eps, double *c);
+struct ChebyshevWork {
+    void *b0 = nullptr, *b1 = nullptr, *b2 = nullptr, *w = nullptr;  // one field each, mode precision
+};
+template <typename T>
+void chebyshev_apply(ChebyshevWork &w, const double *U, const double *u1, const void *src, void *dst, const Lattice &L,
+                     int n_mb, const double *coeff, int K, double eps, double lambda_max, double amass, double mdw,
+                     double mf, double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches);
 
 // Free Wilson plane waves for local modes [0, n_modes) (global index first_mode + m).
 template <typename T>

@@ -49,8 +49,8 @@ __device__ __forceinline__ cpx<double> colour_bilinear(const mono &G, const cpx<
 
 template <typename T>
 __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
-    currents_kernel(const double *__restrict__ U, const cpx<T> *__restrict__ psi, Lattice L, int n_mb, int n_modes,
-                    int first_mode, int groups, double r, double *__restrict__ partial) {
+    currents_kernel(const double *__restrict__ U, const double2 *__restrict__ u1, const cpx<T> *__restrict__ psi,
+                    Lattice L, int n_mb, int n_modes, int first_mode, int groups, double r, double *__restrict__ partial) {
     constexpr mono G1 = {{0, 1, 2, 3}, {0, 0, 0, 0}};
     constexpr mono G5 = kGamma5;
     constexpr mono G05 = mono_mul(kGamma0, kGamma5);
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
             // forward: chi = U_mu(x) psi(x+mu)
             load_site(psi, V, mb, nb[mu][0], lane, h);
             {
-                const cmat2<double> M = link_matrix<double>(load_link(U, site, mu));
+                const cmat2<double> M = dressed_link<double>(U, u1, site, mu, L.N0 * L.N1);
 #pragma unroll
                 for (int a = 0; a < kSpin; a++) {
                     cpx<double> h0 = mk<double>(h[0][a].re, h[0][a].im), h1 = mk<double>(h[1][a].re, h[1][a].im);
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
             // backward: chib = U_mu(x-mu)^+ psi(x-mu)
             load_site(psi, V, mb, nb[mu][1], lane, h);
             {
-                const cmat2<double> M = link_matrix<double>(load_link(U, nb[mu][1], mu));
+                const cmat2<double> M = dressed_link<double>(U, u1, nb[mu][1], mu, L.N0 * L.N1);
 #pragma unroll
                 for (int a = 0; a < kSpin; a++) {
                     cpx<double> h0 = mk<double>(h[0][a].re, h[0][a].im), h1 = mk<double>(h[1][a].re, h[1][a].im);
@@ -159,20 +159,144 @@ __global__ void currents_finish_kernel(const double *__restrict__ partial, int g
 
 int currents_groups(int n_mb) { return n_mb < 16 ? n_mb : 16; }
 
+void launch_currents_finish(const double *partial, int groups, const Lattice &L, double *per_site, cudaStream_t stream) {
+    const int n = L.V * kCurrentsPerSite;
+    currents_finish_kernel<<<(n + 255) / 256, 256, 0, stream>>>(partial, groups, L.V, 1.0 / (2.0 * L.V), per_site);
+}
+
 size_t currents_partial_doubles(const Lattice &L, int n_mb) {
     return (size_t)currents_groups(n_mb) * L.V * kCurrentsPerSite;
 }
 
 template <typename T>
-void launch_currents(const double *U, const void *psi, const Lattice &L, int n_mb, int n_modes, int first_mode,
-                     double r_wilson, double *partial, double *per_site, cudaStream_t stream) {
+void launch_currents(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                     int first_mode, double r_wilson, double *partial, double *per_site, cudaStream_t stream) {
     const int groups = currents_groups(n_mb);
     dim3 block(kModeBlock, kCurrentsThreadsY);
     dim3 grid((L.V + kCurrentsThreadsY - 1) / kCurrentsThreadsY, groups);
-    currents_kernel<T><<<grid, block, 0, stream>>>(U, reinterpret_cast<const cpx<T> *>(psi), L, n_mb, n_modes,
-                                                   first_mode, groups, r_wilson, partial);
+    currents_kernel<T><<<grid, block, 0, stream>>>(U, reinterpret_cast<const double2 *>(u1),
+                                                   reinterpret_cast<const cpx<T> *>(psi), L, n_mb, n_modes, first_mode,
+                                                   groups, r_wilson, partial);
     const int n = L.V * kCurrentsPerSite;
     currents_finish_kernel<<<(n + 255) / 256, 256, 0, stream>>>(partial, groups, L.V, 1.0 / (2.0 * L.V), per_site);
+}
+
+// ----------------------------------------------------------------- charges --
+// The lattice sums of the current densities without the per-site maps:
+//   N_V = sum psi^+ psi,  N_5 = sum psi^+ g5 psi = 2 Re z,  PS = -2 Im z,
+//   z = sum_c conj(psi_0) psi_2 + conj(psi_1) psi_3,
+//   WA  = -12 r Im z + 2 r sum_mu Im psi^+(x) g0 g5 U_mu(x) psi(x+mu).
+// For the WA sum the backward hop of Currents.cpp:273-283 is not evaluated:
+// with Gamma = -i r g0 g5 hermitian, shifting x -> x+mu turns
+// sum_x psi^+(x) Gamma U_mu(x-mu)^+ psi(x-mu) into the complex conjugate of the
+// forward sum, whose real part is the same.  Each thread evaluates its mode
+// and site in the mode precision T and accumulates in double; partial sums
+// per CTA are added in a fixed order.
+constexpr int kChargeVals = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
+    charges_kernel(const double *__restrict__ U, const double2 *__restrict__ u1, const cpx<T> *__restrict__ psi,
+                   Lattice L, int n_mb, int n_modes, int first_mode, int groups, T r, double *__restrict__ partial) {
+    __shared__ double sh[kCurrentsThreadsY][kChargeVals];
+    const int lane = threadIdx.x;
+    const int site = blockIdx.x * kCurrentsThreadsY + threadIdx.y;
+    const int g = blockIdx.y;
+    double acc[kChargeVals] = {0.0, 0.0, 0.0, 0.0};
+    if (site < L.V) {
+        int x, y, z;
+        site_coords(L, site, x, y, z);
+        int nb[3];
+        for (int mu = 0; mu < 3; mu++) {
+            int c[3] = {x, y, z};
+            c[mu] += 1;
+            nb[mu] = site_index(L, c[0], c[1], c[2]);
+        }
+        cmat2<T> M[3];
+        for (int mu = 0; mu < 3; mu++) M[mu] = dressed_link<T>(U, u1, site, mu, L.N0 * L.N1);
+        for (int mb = g; mb < n_mb; mb += groups) {
+            const int mode = mb * kModeBlock + lane;
+            const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
+            cpx<T> f[kColours][kSpin];
+            load_site(psi, L.V, mb, site, lane, f);
+            T nv = 0;
+            cpx<T> zz = mk<T>(0, 0);
+#pragma unroll
+            for (int c = 0; c < kColours; c++) {
+#pragma unroll
+                for (int a = 0; a < kSpin; a++) nv += f[c][a].re * f[c][a].re + f[c][a].im * f[c][a].im;
+                zz = zz + cdot(f[c][0], f[c][2]) + cdot(f[c][1], f[c][3]);
+            }
+            T hop = 0;
+#pragma unroll
+            for (int mu = 0; mu < 3; mu++) {
+                cpx<T> h[kColours][kSpin];
+                load_site(psi, L.V, mb, nb[mu], lane, h);
+                cpx<T> chi[kColours][kSpin];
+#pragma unroll
+                for (int a = 0; a < kSpin; a++) mul(M[mu], h[0][a], h[1][a], chi[0][a], chi[1][a]);
+                cpx<T> b = mk<T>(0, 0);
+#pragma unroll
+                for (int c = 0; c < kColours; c++)
+                    b = b + cdot(f[c][0], chi[c][2]) + cdot(f[c][1], chi[c][3]) - cdot(f[c][2], chi[c][0]) -
+                        cdot(f[c][3], chi[c][1]);
+                hop += b.im;
+            }
+            acc[0] += w * (double)nv;
+            acc[1] += w * 2.0 * (double)zz.re;
+            acc[2] += w * -2.0 * (double)zz.im;
+            acc[3] += w * ((double)r * (-12.0 * (double)zz.im + 2.0 * (double)hop));
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kChargeVals; k++) {
+        double t = acc[k];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        acc[k] = t;
+    }
+    if (lane == 0)
+        for (int k = 0; k < kChargeVals; k++) sh[threadIdx.y][k] = acc[k];
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        double *p = partial + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * kChargeVals;
+        for (int k = 0; k < kChargeVals; k++) {
+            double t = 0.0;
+            for (int j = 0; j < kCurrentsThreadsY; j++) t += sh[j][k];
+            p[k] = t;
+        }
+    }
+}
+
+__global__ void charges_finish_kernel(const double *__restrict__ partial, int n, double scale, double *__restrict__ out4) {
+    __shared__ double sh[kChargeVals][256];
+    double t[kChargeVals] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        for (int k = 0; k < kChargeVals; k++) t[k] += partial[(size_t)i * kChargeVals + k];
+    for (int k = 0; k < kChargeVals; k++) sh[k][threadIdx.x] = t[k];
+    __syncthreads();
+    for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
+        if ((int)threadIdx.x < stride)
+            for (int k = 0; k < kChargeVals; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + stride];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < kChargeVals; k++) out4[k] = scale * sh[k][0];
+}
+
+size_t charges_partial_doubles(const Lattice &L, int n_mb) {
+    return (size_t)currents_groups(n_mb) * ((L.V + kCurrentsThreadsY - 1) / kCurrentsThreadsY) * kChargeVals;
+}
+
+template <typename T>
+void launch_charges(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                    int first_mode, double r_wilson, double *partial, double *out4, cudaStream_t stream) {
+    const int groups = currents_groups(n_mb);
+    dim3 block(kModeBlock, kCurrentsThreadsY);
+    dim3 grid((L.V + kCurrentsThreadsY - 1) / kCurrentsThreadsY, groups);
+    charges_kernel<T><<<grid, block, 0, stream>>>(U, reinterpret_cast<const double2 *>(u1),
+                                                  reinterpret_cast<const cpx<T> *>(psi), L, n_mb, n_modes, first_mode,
+                                                  groups, (T)r_wilson, partial);
+    charges_finish_kernel<<<1, 256, 0, stream>>>(partial, (int)(grid.x * grid.y), 1.0 / (2.0 * L.V), out4);
 }
 
 // Lattice sums of jV^0, jA^0, PS, WA from the per-site array, fixed order.
@@ -394,8 +518,10 @@ void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes
 }
 
 #define OVL_INSTANTIATE(T)                                                                                          \
-    template void launch_currents<T>(const double *, const void *, const Lattice &, int, int, int, double, double *, \
-                                     double *, cudaStream_t);                                                       \
+    template void launch_charges<T>(const double *, const double *, const void *, const Lattice &, int, int, int,     \
+                                    double, double *, double *, cudaStream_t);                                      \
+    template void launch_currents<T>(const double *, const double *, const void *, const Lattice &, int, int, int,   \
+                                     double, double *, double *, cudaStream_t);                                     \
     template void launch_ref_to_blocks<T>(const double *, void *, const Lattice &, int, int, cudaStream_t);          \
     template void launch_blocks_to_ref<T>(const void *, double *, const Lattice &, int, int, cudaStream_t);         \
     template void launch_free_fermions<T>(void *, void *, const Lattice &, int, int, int, double, double, double,    \

@@ -58,6 +58,7 @@ def oracle():
         L.orc_ncsdot.restype = C.c_double
         L.orc_bulk.argtypes = [P, _dp, _dp, _dp]
         L.orc_u1_flux.argtypes = [P, C.c_int, _dp]
+        L.orc_set_u1.argtypes = [_dp]
         _oracle = L
     return _oracle
 
@@ -87,6 +88,8 @@ def reference(kind: str = "wilson"):
         L.ovlref_currents.argtypes = [_dp] * 6
         L.ovlref_currents.restype = C.c_int
         L.ovlref_ncsdot.restype = C.c_double
+        L.ovlref_delta_ncs.argtypes = [_dp, _dp]
+        L.ovlref_delta_ncs.restype = C.c_double
         L.ovlref_update_links.argtypes = [C.c_double]
         L.ovlref_update_efield.argtypes = [C.c_double]
         L.ovlref_u1_flux.argtypes = [C.c_int, _dp]
@@ -98,5 +101,6 @@ def reference(kind: str = "wilson"):
             L.ovlref_zolotarev.restype = C.c_double
             L.ovlref_take_bounds.argtypes = [_dp, C.c_int]
             L.ovlref_take_bounds.restype = C.c_int
+            L.ovlref_last_bounds.argtypes = [_dp]
         _refs[kind] = L
     return _refs[kind]

@@ -50,6 +50,16 @@ def test_create_rejects_bad_arguments_before_touching_a_gpu():
     with pytest.raises(OvlError, match="OVL_E_ARG"):
         Context(N=(2, 8, 8))
     with pytest.raises(OvlError, match="OVL_E_UNSUPPORTED"):
-        Context(N=(4, 4, 4), fermion="overlap")
+        Context(N=(4, 4, 4), fermion="overlap", precision="fp32")
+    with pytest.raises(OvlError, match="OVL_E_ARG"):
+        Context(N=(4, 4, 4), fermion="overlap", zolo_poles=0)
     with pytest.raises(OvlError, match="OVL_E_ARG"):
         Context(N=(4, 4, 4), dt=-1.0)
+
+
+def test_zolotarev_rejects_bad_intervals():
+    from overlap_b200 import OvlError, zolotarev
+    with pytest.raises(OvlError, match="OVL_E_ARG"):
+        zolotarev(1.0, 0.5)
+    with pytest.raises(OvlError, match="OVL_E_ARG"):
+        zolotarev(0.1, 2.0, npoles=0)

@@ -101,3 +101,28 @@ def test_ncsdot_against_reference_n8():
     ref = R.ovlref_ncsdot()
     with ctx_with(N, U, E) as ctx:
         assert abs(ctx.ncsdot() - ref) <= 1e-13 * max(1.0, abs(ref))
+
+
+@pytest.mark.skipif(not have_reference("wilson"), reason="reference library not built")
+def test_cooled_ncs_update_matches_reference_simpson_rule():
+    """Delta N_CS between stored and current links (CoolingMethod::GetDeltaNCs(1),
+    cooling off) against the reference's GeodesicInterpolation + NCsDot."""
+    N = (6, 4, 5)
+    U0 = random_links(N, 0.8, 41)
+    E = random_efield(N, 0.6, 42)
+    p = oracle_params(N)
+    U1 = U0.copy()
+    for _ in range(5):
+        oracle().orc_update_links(C.byref(p), ptr(U1), ptr(E), 0.05)
+    R = reference("wilson")
+    R.ovlref_init(*N, 1, 0, 0.1, 1.0, 0.0, 6.0, 0.05, 1.0, 1)
+    ref = R.ovlref_delta_ncs(ptr(U0), ptr(U1))
+    with ctx_with(N, U0, E) as ctx:
+        assert ctx.ncs_update() == (0.0, 0.0)
+        ctx.set_links(U1)
+        d, total = ctx.ncs_update()
+        assert abs(d - ref) <= 1e-13 * max(1.0, abs(ref))
+        assert total == d
+        # U_new became U_old: no further change
+        d2, total2 = ctx.ncs_update()
+        assert abs(d2) < 1e-15 and abs(total2 - total) < 1e-15

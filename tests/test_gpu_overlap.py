@@ -1,0 +1,160 @@
+"""GPU parity of the overlap operator (batched multi-shift CG, FP64) with the
+reference's overlap code compiled from source (oracle/_ref/libovlref_overlap.so).
+
+The reference draws the start vector of its Ritz bound estimate from its RNG
+(FERMIONS/OVERLAP/OverlapUpdate.cpp:66-84); the tests replay the bounds the
+reference used, through ovl_set_spectral_bounds.  The reference's Zolotarev
+approximation is accurate to ~1e-7 (single-precision square roots in its
+coefficients) and its CG stops at a relative residual ~1e-8: both sides run the
+same coefficients and the same per-mode stopping rule, and agree to 1e-11."""
+import numpy as np
+import pytest
+
+from _helpers import current_scale, random_modes, rel_err
+from _oracle import have_reference, ptr, reference
+from overlap_b200 import Context
+from overlap_b200.inputs import random_efield, random_links, volume
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not have_reference("overlap"), reason="reference overlap build not present")]
+
+TOL = 1e-11
+
+
+def ref_setup(N, nranks, rank, m, r, mdw, tsph, dt, U, E):
+    R = reference("overlap")
+    nm = R.ovlref_init(*N, nranks, rank, m, r, mdw, tsph, dt, 1.0, 7)
+    R.ovlref_set_links(ptr(U))
+    R.ovlref_set_efield(ptr(E))
+    return R, nm
+
+
+def test_overlap_operator_matches_reference():
+    N = (4, 4, 4)
+    U = random_links(N, 0.5, 101)
+    E = np.zeros((volume(N), 3, 3))
+    R, _ = ref_setup(N, 16, 0, 0.1, 1.0, 1.4, 6.0, 0.05, U, E)
+    b = np.zeros(2)
+    R.ovlref_ritz_bounds(ptr(b))
+    phis = random_modes(20, N, 102)
+    ref = np.zeros_like(phis)
+    for i in range(phis.shape[0]):
+        R.ovlref_apply(ptr(phis[i].view(np.float64)), ptr(ref[i].view(np.float64)), b[0], b[1])
+    with Context(N=N, n_modes=20, fermion="overlap", precision="fp64", m_fermion=0.1, r_wilson=1.0, m_dw=1.4,
+                 dt=0.05) as ctx:
+        ctx.set_links(U)
+        ctx.set_spectral_bounds([b])
+        out = ctx.apply(phis)
+        st = ctx.solver_stats()
+    assert st["not_converged"] == 0 and st["iterations"] > 5
+    assert rel_err(out, ref) < TOL
+
+
+def test_overlap_operator_is_anti_hermitian():
+    """D = -i h_ov with h_ov hermitian: <a, D b> = -<D a, b>."""
+    N = (4, 4, 4)
+    U = random_links(N, 0.6, 111)
+    R, _ = ref_setup(N, 16, 0, 0.0, 1.0, 1.4, 6.0, 0.05, U, np.zeros((volume(N), 3, 3)))
+    b = np.zeros(2)
+    R.ovlref_ritz_bounds(ptr(b))
+    ab = random_modes(2, N, 112)
+    with Context(N=N, n_modes=2, fermion="overlap", m_fermion=0.0, m_dw=1.4) as ctx:
+        ctx.set_links(U)
+        ctx.set_spectral_bounds([b])
+        d = ctx.apply(ab)
+    lhs = np.vdot(ab[0], d[1])
+    rhs = -np.vdot(d[0], ab[1])
+    assert abs(lhs - rhs) <= 1e-7 * np.linalg.norm(ab[0]) * np.linalg.norm(d[1])
+
+
+def test_overlap_leapfrog_and_currents_match_reference():
+    N = (4, 4, 4)
+    m, r, mdw, dt, tsph, steps = 0.1, 1.0, 1.4, 0.05, 1e9, 2
+    U = random_links(N, 0.4, 121)
+    E = random_efield(N, 0.2, 122)
+    R, nm = ref_setup(N, 16, 5, m, r, mdw, tsph, dt, U, E)
+    first = R.ovlref_first_mode()
+    R.ovlref_set_free_fermions()  # free overlap spinors (GetOverlapDiracSpinor, FermionField.cpp:331-517)
+    V = volume(N)
+    psi0 = np.zeros((nm, V, 2, 4), np.complex128)
+    mid0 = np.zeros_like(psi0)
+    R.ovlref_get_modes(ptr(psi0.view(np.float64)), ptr(mid0.view(np.float64)))
+    scratch = np.zeros(64)
+    R.ovlref_take_bounds(ptr(scratch), 32)  # clear
+    R.ovlref_step(steps)
+    bounds = np.zeros(64)
+    nb = R.ovlref_take_bounds(ptr(bounds), 64)
+    assert nb == 4 * steps  # (min, max) after each of the 2*steps half steps
+    rpsi = np.zeros_like(psi0)
+    rmid = np.zeros_like(psi0)
+    R.ovlref_get_modes(ptr(rpsi.view(np.float64)), ptr(rmid.view(np.float64)))
+    rU = np.zeros_like(U)
+    R.ovlref_get_links(ptr(rU))
+    rcur = [np.zeros(4 * V) for _ in range(2)]
+    assert R.ovlref_currents(ptr(rcur[0]), ptr(rcur[1]), None, None, None, None) == 2
+    cb = np.zeros(2)
+    R.ovlref_last_bounds(ptr(cb))
+
+    with Context(N=N, n_modes=nm, first_mode=first, fermion="overlap", precision="fp64", m_fermion=m, r_wilson=r,
+                 m_dw=mdw, dt=dt, t_sphaleron=tsph) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_modes(psi0, mid0)
+        ctx.set_spectral_bounds(bounds[:nb].reshape(-1, 2))
+        ctx.step(steps)
+        psi, mid = ctx.get_modes()
+        assert rel_err(psi, rpsi) < TOL
+        assert rel_err(mid, rmid) < TOL
+        assert rel_err(ctx.get_links(), rU) < 1e-13
+        ctx.set_spectral_bounds([cb])
+        cur = ctx.currents()
+    scale = current_scale(rpsi)
+    assert np.max(np.abs(cur["jV"].ravel() - rcur[0])) <= TOL * scale
+    assert np.max(np.abs(cur["jA"].ravel() - rcur[1])) <= TOL * scale
+
+
+def test_chebyshev_sign_agrees_with_zolotarev_form():
+    """Chebyshev series of x^(-1/2) (degree 200 on [0.9 lambda_min / lambda_max, 1])
+    against the reference's Zolotarev form on the same links and bounds; the
+    Zolotarev coefficients are accurate to ~1e-7, so the forms agree to 1e-6.
+    FP32 Chebyshev agrees with FP64 Chebyshev to 1e-5."""
+    N = (4, 4, 4)
+    U = random_links(N, 0.5, 131)
+    R, _ = ref_setup(N, 16, 0, 0.1, 1.0, 1.4, 6.0, 0.05, U, np.zeros((volume(N), 3, 3)))
+    b = np.zeros(2)
+    R.ovlref_ritz_bounds(ptr(b))
+    eps = 0.9 * b[0] / b[1]
+    phis = random_modes(12, N, 132)
+    outs = {}
+    for name, kw in (("zolo", dict(precision="fp64")),
+                     ("cheb64", dict(precision="fp64", sign_method="chebyshev", cheb_degree=200, cheb_eps=eps)),
+                     ("cheb32", dict(precision="fp32", sign_method="chebyshev", cheb_degree=200, cheb_eps=eps))):
+        with Context(N=N, n_modes=12, fermion="overlap", m_fermion=0.1, m_dw=1.4, dt=0.05, **kw) as ctx:
+            ctx.set_links(U)
+            ctx.set_spectral_bounds([b])
+            outs[name] = ctx.apply(phis)
+            if name != "zolo":
+                assert ctx.solver_stats()["not_converged"] == 0
+    assert rel_err(outs["cheb64"], outs["zolo"]) < 1e-6
+    assert rel_err(outs["cheb32"], outs["cheb64"]) < 1e-5
+
+
+def test_chebyshev_overlap_leapfrog_fp32_runs_and_conserves_norm():
+    """FP32 Chebyshev overlap leapfrog: h_ov is hermitian, so the leapfrog keeps
+    the mode norms bounded; the charges stay finite."""
+    N = (4, 4, 4)
+    U = random_links(N, 0.4, 141)
+    R, _ = ref_setup(N, 16, 0, 0.1, 1.0, 1.4, 6.0, 0.05, U, np.zeros((volume(N), 3, 3)))
+    b = np.zeros(2)
+    R.ovlref_ritz_bounds(ptr(b))
+    psi0 = random_modes(32, N, 142)
+    with Context(N=N, n_modes=32, fermion="overlap", precision="fp32", sign_method="chebyshev", cheb_degree=96,
+                 cheb_eps=0.9 * b[0] / b[1], m_fermion=0.1, m_dw=1.4, dt=0.05) as ctx:
+        ctx.set_links(U)
+        ctx.set_spectral_bounds([b])
+        ctx.set_modes(psi0, psi0)
+        n0 = np.sum(np.abs(psi0) ** 2)
+        ctx.step(10)
+        psi, _ = ctx.get_modes()
+        assert abs(np.sum(np.abs(psi) ** 2) / n0 - 1.0) < 0.2
+        assert np.isfinite(ctx.charges()["N5"])

@@ -96,9 +96,13 @@ def test_ragged_modes_odd_offset_asymmetric_lattice(precision, form):
         scale = current_scale(opsi)
         for k in ocur:
             assert np.max(np.abs(cur[k] - ocur[k])) <= (1e-12 if precision == "fp64" else 1e-5) * scale, k
+        # lattice sums straight from the modes (the WA sum uses forward hops only)
         ch = ctx.charges()
-        assert abs(ch["N5"] - cur["jA"][:, 0].sum()) <= 1e-12 * scale * volume(N)
-        assert abs(ch["NV"] - cur["jV"][:, 0].sum()) <= 1e-12 * scale * volume(N)
+        qtol = (1e-12 if precision == "fp64" else 1e-6) * scale * volume(N)
+        assert abs(ch["N5"] - ocur["jA"][:, 0].sum()) <= qtol
+        assert abs(ch["NV"] - ocur["jV"][:, 0].sum()) <= qtol
+        assert abs(ch["PS"] - ocur["PS"].sum()) <= qtol
+        assert abs(ch["WA"] - ocur["WA"].sum()) <= qtol
 
 
 def test_partial_mode_transfers_roundtrip():
