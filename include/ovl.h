@@ -209,6 +209,20 @@ int ovl_synchronize(ovl_ctx *ctx);
  * the context precision (float2 or double2); *bytes is the size of one field. */
 int ovl_device_modes(ovl_ctx *ctx, void **psi, void **psimid, size_t *bytes);
 
+/* NCsDot of fields the caller already holds in device memory, computed without
+ * allocating anything; the only entry point without a counterpart in the
+ * reference.  For callers that cannot allocate device memory: a time-step loop
+ * that must never block on an allocation, or code whose device memory belongs
+ * to another allocator.  links: device double[V][3][4], efield: device
+ * double[V][3][3], out: device double[1]; work is queued on `stream`
+ * (a cudaStream_t, 0 for the default stream) of the current device.  Scratch is
+ * a fixed 8 KiB device array inside the library, so lattices above 262144
+ * sites (64^3) are rejected with OVL_E_ARG.  The first call on a device looks
+ * up that array's address: make it before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race and must be serialised. */
+int ovl_ncsdot_noalloc(const double *links, const double *efield, int N0, int N1, int N2, double *out,
+                       uint64_t stream);
+
 /* Number of CUDA kernel launches this context has issued (for launch accounting). */
 int ovl_launch_count(const ovl_ctx *ctx, uint64_t *count);
 

@@ -210,6 +210,16 @@ void launch_ncsdot(const double *U, const double *E, const Lattice &L, double *p
     finish_kernel<1, false><<<1, kReduceThreads, 0, stream>>>(partial, nb, out, 0.125 / (M_PI * M_PI));
 }
 
+// One partial sum per block of kReduceThreads sites, for callers that provide
+// their own partial-sum storage of `blocks` doubles.
+int ncsdot_blocks_exact(const Lattice &L) { return (L.V + kReduceThreads - 1) / kReduceThreads; }
+
+void launch_ncsdot_into(const double *U, const double *E, const Lattice &L, int blocks, double *partial, double *out,
+                        cudaStream_t stream) {
+    ncsdot_kernel<<<blocks, kReduceThreads, 0, stream>>>(U, E, L, partial);
+    finish_kernel<1, false><<<1, kReduceThreads, 0, stream>>>(partial, blocks, out, 0.125 / (M_PI * M_PI));
+}
+
 // ----------------------------------------------------- geodesic interpolation --
 // GeodesicInterpolation (SUNc/AdvancedOperations.cpp:432-443) on every link:
 // E_mid = -i log(U_new U_old^+) (MatrixILog with C = -1, SU2/AlgebraOperations.cpp:59-74),

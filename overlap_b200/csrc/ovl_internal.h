@@ -29,6 +29,9 @@ void launch_update_efield(const double *U, double *E, double *dE, const Lattice 
 // doubles; out: device array of the result size.
 size_t ncsdot_partial_doubles(const Lattice &L);
 void launch_ncsdot(const double *U, const double *E, const Lattice &L, double *partial, double *out, cudaStream_t stream);
+int ncsdot_blocks_exact(const Lattice &L);
+void launch_ncsdot_into(const double *U, const double *E, const Lattice &L, int blocks, double *partial, double *out,
+                        cudaStream_t stream);
 void launch_geodesic(const double *Uold, const double *Unew, double c, double *Umid, double *Emid, const Lattice &L,
                      cudaStream_t stream);
 size_t bulk_partial_doubles(const Lattice &L);
