@@ -184,6 +184,7 @@ def time_form(wl, precision, form, steps, warmup, device, profile):
     ctx.set_links(random_links(N, wl["link_sigma"], wl["seed"]))
     ctx.set_efield(random_efield(N, wl["e_sigma"], wl["seed"] + 1))
     assert ctx.set_free_fermions() == 0
+    variant, variant_ms = ctx.autotune()
     ctx.step(warmup)
     ctx.synchronize()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -198,7 +199,8 @@ def time_form(wl, precision, form, steps, warmup, device, profile):
     torch.cuda.synchronize(device)
     barrier()
     ms = start.elapsed_time(stop)
-    out = {"ms": ms, "launches": ctx.launch_count - l0, "charges": ctx.charges()}
+    out = {"ms": ms, "launches": ctx.launch_count - l0, "charges": ctx.charges(),
+           "hop_variant": variant, "hop_variant_ms": variant_ms}
     if profile:
         out["prof"] = ctx.profile_read()
         ctx.profile(False)
@@ -381,7 +383,8 @@ def main():
             r_ms = max_over_ranks(r["ms"])
             forms[form] = {"value": world * M * V * max(2, K // 2) / (r_ms / 1e3), "ms_per_step": r_ms / max(2, K // 2),
                            "hop_ms_per_launch": r["prof"]["hop"][0] / max(1, r["prof"]["hop"][1]),
-                           "N5": r["charges"]["N5"]}
+                           "N5": r["charges"]["N5"], "hop_variant": r["hop_variant"],
+                           "hop_variant_ms": r["hop_variant_ms"]}
 
     acc = None
     if args.accuracy_steps > 0 and rank == 0:
@@ -411,7 +414,8 @@ def main():
                          "peak_source": peak_kind},
             "gpu_launches": fp32["launches"],
             "kernel_ms": total_ms,
-            "forms": {"fp32_fused": {"value": value, "ms_per_step": ms / K, "N5": fp32["charges"]["N5"]},
+            "forms": {"fp32_fused": {"value": value, "ms_per_step": ms / K, "N5": fp32["charges"]["N5"],
+                                     "hop_variant": fp32["hop_variant"], "hop_variant_ms": fp32["hop_variant_ms"]},
                       **{f"fp64_{k}": v for k, v in forms.items()}},
             "clocks": clk,
         }

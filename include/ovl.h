@@ -77,6 +77,10 @@ typedef struct {
     int sign_method;
     int cheb_degree;
     double cheb_eps;
+    /* Leapfrog hop kernel variant: -1 = time the variants on the first step and
+     * keep the fastest (ovl_autotune); 0, 1, 2 = fixed.  All variants give the
+     * same results. */
+    int hop_variant;
 } ovl_params;
 
 typedef enum { OVL_SIGN_ZOLOTAREV = 0, OVL_SIGN_CHEBYSHEV = 1 } ovl_sign_method;
@@ -136,6 +140,13 @@ int ovl_set_spectral_bounds(ovl_ctx *ctx, const double *pairs, int count);
  * using the current spectral bounds without consuming them.  The context's
  * modes are not touched. */
 int ovl_apply(ovl_ctx *ctx, int count, const double *phi, double *out);
+
+/* Times the hop-kernel variants of the leapfrog half step on this context's
+ * fields (its state is not changed) and keeps the fastest for later steps:
+ * 0 = one site per thread, 1 = the same with neighbour loads issued one hop
+ * ahead, 2 = (x, y) columns marching in z with register reuse.  *variant
+ * receives the choice, ms[v] the time of one half step with variant v. */
+int ovl_autotune(ovl_ctx *ctx, int *variant, double ms[3]);
 
 /* Zolotarev coefficients of the overlap sign function for spectral bounds
  * [lambda_min, lambda_max] of h_W^2: (h_W^2)^(-1/2) ~ sum_l b[l] / (h_W^2 + d[l]),

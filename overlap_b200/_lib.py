@@ -26,6 +26,7 @@ class ovl_params(C.Structure):
         ("qs", C.c_double), ("t_sphaleron", C.c_double), ("device", C.c_int), ("plain_chunk_modes", C.c_int),
         ("stream", C.c_uint64), ("zolo_poles", C.c_int), ("zolo_tol", C.c_double), ("cg_max_iter", C.c_int),
         ("cg_tol", C.c_double), ("sign_method", C.c_int), ("cheb_degree", C.c_int), ("cheb_eps", C.c_double),
+        ("hop_variant", C.c_int),
     ]
 
 
@@ -61,6 +62,7 @@ SIGNATURES = {
     "ovl_device_modes": ([_ctx, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_size_t)], C.c_int),
     "ovl_set_spectral_bounds": ([_ctx, _dp, C.c_int], C.c_int),
     "ovl_apply": ([_ctx, C.c_int, _dp, _dp], C.c_int),
+    "ovl_autotune": ([_ctx, C.POINTER(C.c_int), _dp], C.c_int),
     "ovl_zolotarev": ([C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp], C.c_int),
     "ovl_solver_stats": ([_ctx, C.POINTER(C.c_int)], C.c_int),
     "ovl_ncsdot_noalloc": ([_vp, _vp, C.c_int, C.c_int, C.c_int, _vp, C.c_uint64], C.c_int),

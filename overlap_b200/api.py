@@ -74,6 +74,7 @@ class Params:
     zolo_tol: float = 1e-12
     cg_max_iter: int = 1000
     cg_tol: float = 1e-16
+    hop_variant: int = -1            # -1: autotune on the first step; 0, 1, 2 fixed
     sign_method: str = "zolotarev"  # or "chebyshev" (the FP32-capable polynomial form)
     cheb_degree: int = 96
     cheb_eps: float = 0.01
@@ -95,6 +96,7 @@ class Params:
         p.stream = int(self.stream)
         p.zolo_poles, p.zolo_tol = int(self.zolo_poles), float(self.zolo_tol)
         p.cg_max_iter, p.cg_tol = int(self.cg_max_iter), float(self.cg_tol)
+        p.hop_variant = int(self.hop_variant)
         p.sign_method = SIGN_METHODS[self.sign_method]
         p.cheb_degree, p.cheb_eps = int(self.cheb_degree), float(self.cheb_eps)
         return p
@@ -214,6 +216,14 @@ class Context:
         out = np.empty_like(a)
         self._check(self._L.ovl_apply(self._ctx, a.shape[0], _dp(a.view(np.float64)), _dp(out.view(np.float64))))
         return out
+
+    def autotune(self):
+        """Times the hop-kernel variants on this context's fields (state unchanged)
+        and keeps the fastest: returns (variant, [ms per half step of each])."""
+        v = C.c_int(0)
+        ms = np.zeros(3)
+        self._check(self._L.ovl_autotune(self._ctx, C.byref(v), _dp(ms)))
+        return v.value, ms.tolist()
 
     def solver_stats(self) -> dict:
         o = (C.c_int * 3)()

@@ -51,6 +51,9 @@ struct ovl_ctx {
     // U(1) background phases of the hopping term (ovl_set_u1)
     double *u1 = nullptr;
     bool u1_on = false;
+    // FP32 copies of links and phases for the FP32 hopping kernels; kernel variant
+    float *U32 = nullptr, *u1_32 = nullptr;
+    int hop_variant = -1;  // -1: autotune before the first step
     // Chern-Simons number along the cooling path (ovl_ncs_update)
     double *u_old = nullptr, *u_mid = nullptr, *e_mid = nullptr;
     bool have_u_old = false;
@@ -189,14 +192,70 @@ int run_overlap(ovl_ctx *c, const void *src, void *dst, int n_mb, int n_modes, b
     return launched(c, (int)c->ostats.launches, "overlap operator");
 }
 
+ovl::HopConfig hop_config(const ovl_ctx *c) {
+    ovl::HopConfig h;
+    h.U = c->U;
+    h.u1 = c->u1_on ? c->u1 : nullptr;
+    if (c->p.precision == OVL_PREC_FP32) {
+        h.U32 = c->U32;
+        h.u1_32 = c->u1_on ? c->u1_32 : nullptr;
+    }
+    h.variant = c->hop_variant < 0 ? 0 : c->hop_variant;
+    return h;
+}
+
+void refresh_links32(ovl_ctx *c) {
+    if (c->U32) {
+        ovl::launch_links_to_f32(c->U, c->U32, (size_t)12 * c->L.V, c->stream);
+        c->launches++;
+    }
+}
+
+// Times each hop-kernel variant on the live fields (psi -> operator buffer,
+// the context's state is not touched) and keeps the fastest.
+int autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        return fail(c, OVL_E_CUDA, "autotune: events");
+    ovl::HopConfig h = hop_config(c);
+    double best = 1e300;
+    int pick = 0;
+    for (int v = 0; v < ovl::kHopVariants; v++) {
+        h.variant = v;
+        float total = 0.0f;
+        for (int rep = 0; rep < 4; rep++) {
+            cudaEventRecord(e0, c->stream);
+            if (fp32(c)) ovl::launch_wilson_tuned<float>(h, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+            else ovl::launch_wilson_tuned<double>(h, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+            cudaEventRecord(e1, c->stream);
+            cudaEventSynchronize(e1);
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (rep > 0) total += t;  // first run warms caches and clocks
+        }
+        const double ms = total / 3.0;
+        if (ms_out) ms_out[v] = ms;
+        if (ms < best) { best = ms; pick = v; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->hop_variant = pick;
+    return launched(c, 4 * ovl::kHopVariants, "autotune");
+}
+
 // psi_dst += dt * D psi_src over all modes (one Update.cpp half step).
 int half_step(ovl_ctx *c, const void *src, void *dst) {
     const Lattice &L = c->L;
     if (overlap(c)) return run_overlap(c, src, dst, c->n_mb, c->p.n_modes, true, true);
+    if (c->hop_variant < 0) {
+        int rc = autotune(c, nullptr);
+        if (rc) return rc;
+    }
+    const ovl::HopConfig hc = hop_config(c);
     if (c->p.form == OVL_FORM_FUSED) {
         ProfScope ps(c, OVL_PROF_HOP);
-        if (fp32(c)) ovl::launch_wilson<float>(c->U, c->u1_on ? c->u1 : nullptr, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
-        else ovl::launch_wilson<double>(c->U, c->u1_on ? c->u1 : nullptr, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        if (fp32(c)) ovl::launch_wilson_tuned<float>(hc, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        else ovl::launch_wilson_tuned<double>(hc, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
         return launched(c, 1, "wilson (fused)");
     }
     const size_t block_complex = (size_t)L.V * ovl::kComp * ovl::kModeBlock;
@@ -206,8 +265,8 @@ int half_step(ovl_ctx *c, const void *src, void *dst) {
         char *d = static_cast<char *>(dst) + block_complex * c->elem_bytes * (size_t)mb;
         {
             ProfScope ps(c, OVL_PROF_HOP);
-            if (fp32(c)) ovl::launch_wilson<float>(c->U, c->u1_on ? c->u1 : nullptr, src, c->deriv, L, mb, nmb, amass(c->p), c->p.dt, false, c->stream);
-            else ovl::launch_wilson<double>(c->U, c->u1_on ? c->u1 : nullptr, src, c->deriv, L, mb, nmb, amass(c->p), c->p.dt, false, c->stream);
+            if (fp32(c)) ovl::launch_wilson_tuned<float>(hc, src, c->deriv, L, mb, nmb, amass(c->p), c->p.dt, false, c->stream);
+            else ovl::launch_wilson_tuned<double>(hc, src, c->deriv, L, mb, nmb, amass(c->p), c->p.dt, false, c->stream);
         }
         {
             ProfScope ps(c, OVL_PROF_AXPY);
@@ -267,6 +326,7 @@ int ovl_params_init(ovl_params *p) {
     p->zolo_tol = 1e-12;
     p->cg_max_iter = 1000;
     p->cg_tol = 1e-16;
+    p->hop_variant = -1;
     p->sign_method = OVL_SIGN_ZOLOTAREV;
     p->cheb_degree = 96;
     p->cheb_eps = 0.01;
@@ -296,6 +356,8 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     if (p->form != OVL_FORM_PLAIN && p->form != OVL_FORM_FUSED) return fail(nullptr, OVL_E_ARG, "ovl_create: bad form");
     if (p->n_modes <= 0 || p->first_mode < 0) return fail(nullptr, OVL_E_ARG, "ovl_create: n_modes=%d first_mode=%d", p->n_modes, p->first_mode);
     if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return fail(nullptr, OVL_E_ARG, "ovl_create: dt must be positive");
+    if (p->hop_variant < -1 || p->hop_variant >= ovl::kHopVariants)
+        return fail(nullptr, OVL_E_ARG, "ovl_create: hop_variant=%d (-1 = autotune, 0..%d)", p->hop_variant, ovl::kHopVariants - 1);
     const long long V = (long long)p->N[0] * p->N[1] * p->N[2];
     if (V > (1LL << 30) / 8) return fail(nullptr, OVL_E_ARG, "ovl_create: lattice too large");
 
@@ -346,6 +408,9 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
         return bail(fail(c, OVL_E_OOM, "ovl_create: pinned host allocation failed"));
     if ((rc = alloc(&c->aux_src, field_bytes, "operator input")) || (rc = alloc(&c->aux_dst, field_bytes, "operator output")))
         return bail(rc);
+    if (p->precision == OVL_PREC_FP32 && (rc = alloc((void **)&c->U32, sizeof(float) * 12 * V, "FP32 links")))
+        return bail(rc);
+    c->hop_variant = p->hop_variant;
     if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method == OVL_SIGN_CHEBYSHEV) {
         ovl::ChebyshevWork &w = c->cw;
         if ((rc = alloc(&w.b0, field_bytes, "Clenshaw b")) || (rc = alloc(&w.b1, field_bytes, "Clenshaw b")) ||
@@ -380,6 +445,7 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     std::vector<double> unit(12 * V, 0.0);
     for (long long l = 0; l < 3 * V; l++) unit[4 * l + 3] = 1.0;
     cudaMemcpyAsync(c->U, unit.data(), sizeof(double) * 12 * V, cudaMemcpyHostToDevice, c->stream);
+    refresh_links32(c);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(c, OVL_E_CUDA, "ovl_create: initialisation failed"));
     *out = c;
     return OVL_OK;
@@ -392,7 +458,7 @@ int ovl_destroy(ovl_ctx *c) {
     void *bufs[] = {c->psi, c->psimid, c->U, c->E, c->deriv, c->per_site, c->partial, c->dev_small, c->dev_int,
                     c->aux_src, c->aux_dst, c->ow.r, c->ow.q, c->ow.t, c->ow.x, c->ow.p, c->ow.part, c->ow.rnorm,
                     c->ow.alpha, c->ow.active, c->ow.dz, c->u_old, c->u_mid, c->e_mid, c->u1,
-                    c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w};
+                    c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w, c->U32, c->u1_32};
     if (c->ow.host_count) cudaFreeHost(c->ow.host_count);
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -414,6 +480,7 @@ int ovl_set_links(ovl_ctx *c, const double *links) {
     int rc = set_device(c);
     if (rc) return rc;
     OVL_CUDA(c, cudaMemcpyAsync(c->U, links, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    refresh_links32(c);
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     return OVL_OK;
 }
@@ -453,6 +520,14 @@ int ovl_set_u1(ovl_ctx *c, const double *u1) {
         return fail(c, OVL_E_OOM, "ovl_set_u1: phases");
     }
     OVL_CUDA(c, cudaMemcpyAsync(c->u1, u1, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    if (fp32(c)) {
+        if (!c->u1_32 && cudaMalloc(&c->u1_32, sizeof(float) * n) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, OVL_E_OOM, "ovl_set_u1: FP32 phases");
+        }
+        ovl::launch_links_to_f32(c->u1, c->u1_32, n, c->stream);
+        c->launches++;
+    }
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     c->u1_on = true;
     return OVL_OK;
@@ -554,7 +629,7 @@ int ovl_step(ovl_ctx *c, int nsteps) {
         if (move) {
             {
                 ProfScope ps(c, OVL_PROF_LINKS);
-                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream);
+                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream, c->U32);
             }
             if ((rc = launched(c, 1, "update links"))) return rc;
         }
@@ -562,7 +637,7 @@ int ovl_step(ovl_ctx *c, int nsteps) {
         if (move) {
             {
                 ProfScope ps(c, OVL_PROF_LINKS);
-                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream);
+                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream, c->U32);
             }
             if ((rc = launched(c, 1, "update links"))) return rc;
         }
@@ -686,7 +761,7 @@ int ovl_update_links(ovl_ctx *c, double dt_step) {
     if (!c) return OVL_E_ARG;
     int rc = set_device(c);
     if (rc) return rc;
-    ovl::launch_update_links(c->U, c->E, c->L, dt_step, c->stream);
+    ovl::launch_update_links(c->U, c->E, c->L, dt_step, c->stream, c->U32);
     return launched(c, 1, "update links");
 }
 
@@ -776,6 +851,18 @@ int ovl_apply(ovl_ctx *c, int count, const double *phi, double *out) {
         return done(fail(c, OVL_E_CUDA, "ovl_apply: download"));
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return done(fail(c, OVL_E_CUDA, "ovl_apply: synchronise"));
     return done(OVL_OK);
+}
+
+int ovl_autotune(ovl_ctx *c, int *variant, double ms[3]) {
+    if (!c) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    double t[ovl::kHopVariants];
+    if ((rc = autotune(c, t))) return rc;
+    if (variant) *variant = c->hop_variant;
+    if (ms)
+        for (int v = 0; v < ovl::kHopVariants; v++) ms[v] = t[v];
+    return OVL_OK;
 }
 
 int ovl_zolotarev(double lambda_min, double lambda_max, double tol, int npoles, double *b, double *d, double *eps) {

@@ -18,11 +18,26 @@ constexpr int kSitesPerCta = 8;  // sites per CTA of the Wilson kernels (8 warps
 template <typename T>
 void launch_wilson(const double *links, const double *u1, const void *src, void *dst, const Lattice &L, int mb_first,
                    int n_mb, double amass, double dt, bool accumulate, cudaStream_t stream);
+// Link sources and kernel variant of the leapfrog half step (chosen by the
+// autotuner, see ovl_autotune): U/u1 FP64 links and phases; U32/u1_32 their FP32
+// copies (used by the FP32 path when set); variant 0, 1 or 2.
+struct HopConfig {
+    const double *U = nullptr, *u1 = nullptr;
+    const float *U32 = nullptr, *u1_32 = nullptr;
+    int variant = 0;
+};
+constexpr int kHopVariants = 3;
+template <typename T>
+void launch_wilson_tuned(const HopConfig &hc, const void *src, void *dst, const Lattice &L, int mb_first, int n_mb,
+                         double amass, double dt, bool accumulate, cudaStream_t stream);
+void launch_links_to_f32(const double *U, float *U32, size_t n, cudaStream_t stream);
+
 template <typename T>
 void launch_axpy(void *dst, const void *deriv, size_t n_complex, double dt, int sm_count, cudaStream_t stream);
 
 // Gauge fields (FP64).
-void launch_update_links(double *U, const double *E, const Lattice &L, double dt_step, cudaStream_t stream);
+void launch_update_links(double *U, const double *E, const Lattice &L, double dt_step, cudaStream_t stream,
+                         float *U32 = nullptr);
 void launch_update_efield(const double *U, double *E, double *dE, const Lattice &L, double dt_step, cudaStream_t stream);
 
 // Reductions.  partial: caller-provided device scratch of reduce_partial_doubles()

@@ -190,14 +190,14 @@ void launch_currents(const double *U, const double *u1, const void *psi, const L
 // with Gamma = -i r g0 g5 hermitian, shifting x -> x+mu turns
 // sum_x psi^+(x) Gamma U_mu(x-mu)^+ psi(x-mu) into the complex conjugate of the
 // forward sum, whose real part is the same.  Each thread evaluates its mode
-// and site in the mode precision T and accumulates in double; partial sums
-// per CTA are added in a fixed order.
+// and site in double whatever the mode precision; partial sums per CTA are
+// added in a fixed order.
 constexpr int kChargeVals = 4;
 
 template <typename T>
 __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
     charges_kernel(const double *__restrict__ U, const double2 *__restrict__ u1, const cpx<T> *__restrict__ psi,
-                   Lattice L, int n_mb, int n_modes, int first_mode, int groups, T r, double *__restrict__ partial) {
+                   Lattice L, int n_mb, int n_modes, int first_mode, int groups, double r, double *__restrict__ partial) {
     __shared__ double sh[kCurrentsThreadsY][kChargeVals];
     const int lane = threadIdx.x;
     const int site = blockIdx.x * kCurrentsThreadsY + threadIdx.y;
@@ -212,40 +212,49 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
             c[mu] += 1;
             nb[mu] = site_index(L, c[0], c[1], c[2]);
         }
-        cmat2<T> M[3];
-        for (int mu = 0; mu < 3; mu++) M[mu] = dressed_link<T>(U, u1, site, mu, L.N0 * L.N1);
+        cmat2<double> M[3];
+        for (int mu = 0; mu < 3; mu++) M[mu] = dressed_link<double>(U, u1, site, mu, L.N0 * L.N1);
         for (int mb = g; mb < n_mb; mb += groups) {
             const int mode = mb * kModeBlock + lane;
             const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
-            cpx<T> f[kColours][kSpin];
-            load_site(psi, L.V, mb, site, lane, f);
-            T nv = 0;
-            cpx<T> zz = mk<T>(0, 0);
+            // the bilinears in double for every mode precision: each of the
+            // ~1e8 terms of a lattice sum then carries a 1e-16 rounding error
+            cpx<T> ft[kColours][kSpin];
+            load_site(psi, L.V, mb, site, lane, ft);
+            cpx<double> f[kColours][kSpin];
+#pragma unroll
+            for (int c = 0; c < kColours; c++)
+#pragma unroll
+                for (int a = 0; a < kSpin; a++) f[c][a] = mk<double>((double)ft[c][a].re, (double)ft[c][a].im);
+            double nv = 0.0;
+            cpx<double> zz = mk<double>(0.0, 0.0);
 #pragma unroll
             for (int c = 0; c < kColours; c++) {
 #pragma unroll
                 for (int a = 0; a < kSpin; a++) nv += f[c][a].re * f[c][a].re + f[c][a].im * f[c][a].im;
                 zz = zz + cdot(f[c][0], f[c][2]) + cdot(f[c][1], f[c][3]);
             }
-            T hop = 0;
+            double hop = 0.0;
 #pragma unroll
             for (int mu = 0; mu < 3; mu++) {
-                cpx<T> h[kColours][kSpin];
-                load_site(psi, L.V, mb, nb[mu], lane, h);
-                cpx<T> chi[kColours][kSpin];
+                cpx<T> ht[kColours][kSpin];
+                load_site(psi, L.V, mb, nb[mu], lane, ht);
+                cpx<double> chi[kColours][kSpin];
 #pragma unroll
-                for (int a = 0; a < kSpin; a++) mul(M[mu], h[0][a], h[1][a], chi[0][a], chi[1][a]);
-                cpx<T> b = mk<T>(0, 0);
+                for (int a = 0; a < kSpin; a++)
+                    mul(M[mu], mk<double>(ht[0][a].re, ht[0][a].im), mk<double>(ht[1][a].re, ht[1][a].im), chi[0][a],
+                        chi[1][a]);
+                cpx<double> b = mk<double>(0.0, 0.0);
 #pragma unroll
                 for (int c = 0; c < kColours; c++)
                     b = b + cdot(f[c][0], chi[c][2]) + cdot(f[c][1], chi[c][3]) - cdot(f[c][2], chi[c][0]) -
                         cdot(f[c][3], chi[c][1]);
                 hop += b.im;
             }
-            acc[0] += w * (double)nv;
-            acc[1] += w * 2.0 * (double)zz.re;
-            acc[2] += w * -2.0 * (double)zz.im;
-            acc[3] += w * ((double)r * (-12.0 * (double)zz.im + 2.0 * (double)hop));
+            acc[0] += w * nv;
+            acc[1] += w * 2.0 * zz.re;
+            acc[2] += w * -2.0 * zz.im;
+            acc[3] += w * (r * (-12.0 * zz.im + 2.0 * hop));
         }
     }
 #pragma unroll

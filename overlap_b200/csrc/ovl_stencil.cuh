@@ -72,42 +72,118 @@ __device__ __forceinline__ void hop(Spinor<T> &acc, const Spinor<T> &f, const cm
     }
 }
 
-// (D phi)(site) for the 32 modes of block mb (one per lane), before the
-// -i gamma_0 / 2 factor: amass phi(x) - sum of the six projected hops.
-template <typename T>
-__device__ __forceinline__ void wilson_site(const double *__restrict__ links, const double2 *__restrict__ u1,
-                                            const cpx<T> *__restrict__ src, const Lattice &L, int site, int mb,
-                                            int lane, T amass, Spinor<T> &acc) {
+// Where the hop kernels read links from.  LinksF64: the FP64 4-real links
+// (converted to the arithmetic precision at use); LinksF32: an FP32 copy kept
+// next to them for the FP32 path (one 16-byte load per link, no conversion).
+// Both give the same matrices: each component is rounded to T once.  U1: the
+// x and y links carry the U(1) background phase (compiled in only when set).
+template <bool U1> struct LinksF64 {
+    const double *U;
+    const double2 *u1;
+    int n01;
+    template <typename T> __device__ __forceinline__ cmat2<T> get(int site, int mu) const {
+        if (U1) return dressed_link<T>(U, u1, site, mu, n01);
+        return link_matrix<T>(load_link(U, site, mu));
+    }
+};
+
+template <bool U1> struct LinksF32 {
+    const float4 *U;
+    const float2 *u1;
+    int n01;
+    template <typename T> __device__ __forceinline__ cmat2<T> get(int site, int mu) const {
+        const float4 q = __ldg(U + 3 * site + mu);
+        cmat2<T> M = {mk<T>(q.w, q.z), mk<T>(q.y, q.x), mk<T>(-q.y, q.x), mk<T>(q.w, -q.z)};
+        if (U1 && mu < 2) {
+            const float2 ph = __ldg(u1 + 2 * (site % n01) + mu);
+            const cpx<T> p = mk<T>(ph.x, ph.y);
+            M.m00 = p * M.m00;
+            M.m01 = p * M.m01;
+            M.m10 = p * M.m10;
+            M.m11 = p * M.m11;
+        }
+        return M;
+    }
+};
+
+// Neighbour sites of `site` (periodic).
+struct Nbrs {
+    int xp, xm, yp, ym, zp, zm;
+};
+__device__ __forceinline__ Nbrs neighbours(const Lattice &L, int site) {
     int x, y, z;
     site_coords(L, site, x, y, z);
+    const int n01 = L.N0 * L.N1, V = L.V;
+    Nbrs n;
+    n.xp = x + 1 == L.N0 ? site + 1 - L.N0 : site + 1;
+    n.xm = x == 0 ? site - 1 + L.N0 : site - 1;
+    n.yp = y + 1 == L.N1 ? site + L.N0 - n01 : site + L.N0;
+    n.ym = y == 0 ? site - L.N0 + n01 : site - L.N0;
+    n.zp = z + 1 == L.N2 ? site + n01 - V : site + n01;
+    n.zm = z == 0 ? site - n01 + V : site - n01;
+    return n;
+}
+
+// The same stencil with every neighbour load issued one hop ahead of its use
+// (two spinor registers in flight), for more memory-level parallelism per warp.
+template <typename T, class LK>
+__device__ __forceinline__ void wilson_site_pipelined(const LK &lk, const cpx<T> *__restrict__ src, const Lattice &L,
+                                                      int site, int mb, int lane, T amass, Spinor<T> &acc) {
     const int V = L.V;
+    const Nbrs n = neighbours(L, site);
+    Spinor<T> a, b;
+    load_spinor(src, V, mb, site, lane, a);
+    load_spinor(src, V, mb, n.xp, lane, b);
+#pragma unroll
+    for (int c = 0; c < kColours; c++)
+#pragma unroll
+        for (int s = 0; s < kSpin; s++) acc.c[c][s] = amass * a.c[c][s];
+    load_spinor(src, V, mb, n.xm, lane, a);
+    hop<T, 0, true>(acc, b, lk.template get<T>(site, 0));
+    load_spinor(src, V, mb, n.yp, lane, b);
+    hop<T, 0, false>(acc, a, lk.template get<T>(n.xm, 0));
+    load_spinor(src, V, mb, n.ym, lane, a);
+    hop<T, 1, true>(acc, b, lk.template get<T>(site, 1));
+    load_spinor(src, V, mb, n.zp, lane, b);
+    hop<T, 1, false>(acc, a, lk.template get<T>(n.ym, 1));
+    load_spinor(src, V, mb, n.zm, lane, a);
+    hop<T, 2, true>(acc, b, lk.template get<T>(site, 2));
+    hop<T, 2, false>(acc, a, lk.template get<T>(n.zm, 2));
+}
+
+// (D phi)(site) for the 32 modes of block mb (one per lane), before the
+// -i gamma_0 / 2 factor: amass phi(x) - sum of the six projected hops.
+template <typename T, class LK>
+__device__ __forceinline__ void wilson_site_lk(const LK &lk, const cpx<T> *__restrict__ src, const Lattice &L, int site,
+                                               int mb, int lane, T amass, Spinor<T> &acc) {
+    const int V = L.V;
+    const Nbrs n = neighbours(L, site);
     Spinor<T> f;
     load_spinor(src, V, mb, site, lane, f);
 #pragma unroll
     for (int c = 0; c < kColours; c++)
 #pragma unroll
         for (int a = 0; a < kSpin; a++) acc.c[c][a] = amass * f.c[c][a];
+    load_spinor(src, V, mb, n.xp, lane, f);
+    hop<T, 0, true>(acc, f, lk.template get<T>(site, 0));
+    load_spinor(src, V, mb, n.xm, lane, f);
+    hop<T, 0, false>(acc, f, lk.template get<T>(n.xm, 0));
+    load_spinor(src, V, mb, n.yp, lane, f);
+    hop<T, 1, true>(acc, f, lk.template get<T>(site, 1));
+    load_spinor(src, V, mb, n.ym, lane, f);
+    hop<T, 1, false>(acc, f, lk.template get<T>(n.ym, 1));
+    load_spinor(src, V, mb, n.zp, lane, f);
+    hop<T, 2, true>(acc, f, lk.template get<T>(site, 2));
+    load_spinor(src, V, mb, n.zm, lane, f);
+    hop<T, 2, false>(acc, f, lk.template get<T>(n.zm, 2));
+}
 
-    const int xp = x + 1 == L.N0 ? site + 1 - L.N0 : site + 1;
-    const int xm = x == 0 ? site - 1 + L.N0 : site - 1;
-    const int n01 = L.N0 * L.N1;
-    const int yp = y + 1 == L.N1 ? site + L.N0 - n01 : site + L.N0;
-    const int ym = y == 0 ? site - L.N0 + n01 : site - L.N0;
-    const int zp = z + 1 == L.N2 ? site + n01 - V : site + n01;
-    const int zm = z == 0 ? site - n01 + V : site - n01;
-
-    load_spinor(src, V, mb, xp, lane, f);
-    hop<T, 0, true>(acc, f, dressed_link<T>(links, u1, site, 0, n01));
-    load_spinor(src, V, mb, xm, lane, f);
-    hop<T, 0, false>(acc, f, dressed_link<T>(links, u1, xm, 0, n01));
-    load_spinor(src, V, mb, yp, lane, f);
-    hop<T, 1, true>(acc, f, dressed_link<T>(links, u1, site, 1, n01));
-    load_spinor(src, V, mb, ym, lane, f);
-    hop<T, 1, false>(acc, f, dressed_link<T>(links, u1, ym, 1, n01));
-    load_spinor(src, V, mb, zp, lane, f);
-    hop<T, 2, true>(acc, f, dressed_link<T>(links, u1, site, 2, n01));
-    load_spinor(src, V, mb, zm, lane, f);
-    hop<T, 2, false>(acc, f, dressed_link<T>(links, u1, zm, 2, n01));
+template <typename T>
+__device__ __forceinline__ void wilson_site(const double *__restrict__ links, const double2 *__restrict__ u1,
+                                            const cpx<T> *__restrict__ src, const Lattice &L, int site, int mb,
+                                            int lane, T amass, Spinor<T> &acc) {
+    if (u1 != nullptr) wilson_site_lk(LinksF64<true>{links, u1, L.N0 * L.N1}, src, L, site, mb, lane, amass, acc);
+    else wilson_site_lk(LinksF64<false>{links, nullptr, L.N0 * L.N1}, src, L, site, mb, lane, amass, acc);
 }
 
 // Component (c, a) of -i gamma_0 / 2 acc: spins 0,1 times -i/2, spins 2,3 times +i/2.

@@ -16,6 +16,8 @@
 // CTAs resident at one time cover a compact window of one mode block and the
 // six neighbour reads of a site come from L1/L2 rather than HBM.
 
+#include <type_traits>
+
 #include "ovl_internal.h"
 #include "ovl_stencil.cuh"
 
@@ -47,6 +49,140 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
                 st(o, v + dt * d);
             }
         }
+}
+
+// Variants of the same half step for the autotuner (identical arithmetic):
+//   VARIANT 0  one site per thread, loads issued as the hops need them
+//   VARIANT 1  one site per thread, each neighbour load one hop ahead
+//   VARIANT 2  one (x, y) column per thread marching in z: the z neighbours and
+//              the site itself come from registers (5 spinor loads per site
+//              instead of 7)
+// LK selects FP64 links or the FP32 copy (FP32 path).
+template <typename T, int MODE>
+__device__ __forceinline__ void store_result(cpx<T> *__restrict__ dst, int V, int mb, int site, int lane,
+                                             const Spinor<T> &acc, T dt) {
+    cpx<T> *out = dst + field_index(V, mb, site, 0, lane);
+#pragma unroll
+    for (int c = 0; c < kColours; c++)
+#pragma unroll
+        for (int a = 0; a < kSpin; a++) {
+            const cpx<T> d = finish_component(acc.c[c][a], a);
+            cpx<T> *o = out + (c * kSpin + a) * kModeBlock;
+            if (MODE == 0) {
+                st(o, d);
+            } else {
+                cpx<T> v = ld(o);
+                st(o, v + dt * d);
+            }
+        }
+}
+
+// CTAs of 8 warps per SM the compiler must fit: FP32 4 (<= 64 registers; 3 for
+// the pipelined variant, which holds two neighbour spinors), FP64 2.
+template <typename T, int VARIANT> struct HopOccupancy {
+    static constexpr int kMinBlocks = sizeof(T) == 4 ? (VARIANT == 1 ? 3 : 4) : 2;
+};
+
+template <typename T, int MODE, int VARIANT, class LK>
+__global__ void __launch_bounds__(kModeBlock *kSitesPerCta, HopOccupancy<T, VARIANT>::kMinBlocks)
+    wilson_tuned_kernel(LK lk, const cpx<T> *__restrict__ src, cpx<T> *__restrict__ dst, Lattice L, T amass, T dt) {
+    const int lane = threadIdx.x;
+    const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
+    const int mb = blockIdx.y;
+    if (site >= L.V) return;
+    Spinor<T> acc;
+    if (VARIANT == 1) wilson_site_pipelined(lk, src, L, site, mb, lane, amass, acc);
+    else wilson_site_lk(lk, src, L, site, mb, lane, amass, acc);
+    store_result<T, MODE>(dst, L.V, mb, site, lane, acc, dt);
+}
+
+constexpr int kZChunk = 4;  // z sites per thread in the z-marching variant
+
+template <typename T, int MODE, class LK>
+__global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2)
+    wilson_zmarch_kernel(LK lk, const cpx<T> *__restrict__ src, cpx<T> *__restrict__ dst, Lattice L, T amass, T dt) {
+    const int lane = threadIdx.x;
+    const int n01 = L.N0 * L.N1;
+    const int pxy = blockIdx.x * kSitesPerCta + threadIdx.y;  // site in the (x, y) plane
+    const int mb = blockIdx.y;
+    const int z0 = blockIdx.z * kZChunk;
+    if (pxy >= n01 || z0 >= L.N2) return;
+    const int z1 = min(z0 + kZChunk, L.N2);
+    const int V = L.V;
+    Spinor<T> fm, f0, fp, f;
+    load_spinor(src, V, mb, pxy + n01 * ((z0 - 1 + L.N2) % L.N2), lane, fm);
+    load_spinor(src, V, mb, pxy + n01 * z0, lane, f0);
+    for (int z = z0; z < z1; z++) {
+        const int site = pxy + n01 * z;
+        const int zp = pxy + n01 * (z + 1 == L.N2 ? 0 : z + 1);
+        const int zm = pxy + n01 * (z == 0 ? L.N2 - 1 : z - 1);
+        load_spinor(src, V, mb, zp, lane, fp);
+        const Nbrs n = neighbours(L, site);
+        Spinor<T> acc;
+#pragma unroll
+        for (int c = 0; c < kColours; c++)
+#pragma unroll
+            for (int a = 0; a < kSpin; a++) acc.c[c][a] = amass * f0.c[c][a];
+        load_spinor(src, V, mb, n.xp, lane, f);
+        hop<T, 0, true>(acc, f, lk.template get<T>(site, 0));
+        load_spinor(src, V, mb, n.xm, lane, f);
+        hop<T, 0, false>(acc, f, lk.template get<T>(n.xm, 0));
+        load_spinor(src, V, mb, n.yp, lane, f);
+        hop<T, 1, true>(acc, f, lk.template get<T>(site, 1));
+        load_spinor(src, V, mb, n.ym, lane, f);
+        hop<T, 1, false>(acc, f, lk.template get<T>(n.ym, 1));
+        hop<T, 2, true>(acc, fp, lk.template get<T>(site, 2));
+        hop<T, 2, false>(acc, fm, lk.template get<T>(zm, 2));
+        store_result<T, MODE>(dst, V, mb, site, lane, acc, dt);
+        fm = f0;
+        f0 = fp;
+    }
+}
+
+template <typename T, int MODE, class LK>
+static void launch_variant(int variant, const LK &lk, const cpx<T> *s, cpx<T> *d, const Lattice &L, int n_mb, T amass,
+                           T dt, cudaStream_t stream) {
+    dim3 block(kModeBlock, kSitesPerCta);
+    if (variant == 2) {
+        dim3 grid((L.N0 * L.N1 + kSitesPerCta - 1) / kSitesPerCta, n_mb, (L.N2 + kZChunk - 1) / kZChunk);
+        wilson_zmarch_kernel<T, MODE, LK><<<grid, block, 0, stream>>>(lk, s, d, L, amass, dt);
+        return;
+    }
+    dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
+    if (variant == 1) wilson_tuned_kernel<T, MODE, 1, LK><<<grid, block, 0, stream>>>(lk, s, d, L, amass, dt);
+    else wilson_tuned_kernel<T, MODE, 0, LK><<<grid, block, 0, stream>>>(lk, s, d, L, amass, dt);
+}
+
+template <typename T>
+void launch_wilson_tuned(const HopConfig &hc, const void *src, void *dst, const Lattice &L, int mb_first, int n_mb,
+                         double amass, double dt, bool accumulate, cudaStream_t stream) {
+    if (n_mb <= 0) return;
+    const size_t off = field_index(L.V, mb_first, 0, 0, 0);
+    const cpx<T> *s = reinterpret_cast<const cpx<T> *>(src) + off;
+    cpx<T> *d = reinterpret_cast<cpx<T> *>(dst) + (accumulate ? off : 0);
+    const int n01 = L.N0 * L.N1;
+    auto go = [&](const auto &lk) {
+        if (accumulate) launch_variant<T, 1>(hc.variant, lk, s, d, L, n_mb, (T)amass, (T)dt, stream);
+        else launch_variant<T, 0>(hc.variant, lk, s, d, L, n_mb, (T)amass, (T)dt, stream);
+    };
+    if (std::is_same<T, float>::value && hc.U32 != nullptr) {
+        const float4 *u = reinterpret_cast<const float4 *>(hc.U32);
+        if (hc.u1_32) go(LinksF32<true>{u, reinterpret_cast<const float2 *>(hc.u1_32), n01});
+        else go(LinksF32<false>{u, nullptr, n01});
+    } else {
+        if (hc.u1) go(LinksF64<true>{hc.U, reinterpret_cast<const double2 *>(hc.u1), n01});
+        else go(LinksF64<false>{hc.U, nullptr, n01});
+    }
+}
+
+// FP32 copy of the links (and of the U(1) phases) for the FP32 path.
+__global__ void links_to_f32_kernel(const double *__restrict__ U, float *U32, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) U32[i] = (float)U[i];
+}
+
+void launch_links_to_f32(const double *U, float *U32, size_t n, cudaStream_t stream) {
+    links_to_f32_kernel<<<(int)((n + 255) / 256), 256, 0, stream>>>(U, U32, (int)n);
 }
 
 // dst += dt * deriv over n complex numbers (plain form, second phase).
@@ -95,6 +231,10 @@ template void launch_wilson<double>(const double *, const double *, const void *
 template void launch_wilson<float>(const double *, const double *, const void *, void *, const Lattice &, int, int, double,
                                    double, bool, cudaStream_t);
 template void launch_axpy<double>(void *, const void *, size_t, double, int, cudaStream_t);
+template void launch_wilson_tuned<double>(const HopConfig &, const void *, void *, const Lattice &, int, int, double,
+                                          double, bool, cudaStream_t);
+template void launch_wilson_tuned<float>(const HopConfig &, const void *, void *, const Lattice &, int, int, double,
+                                         double, bool, cudaStream_t);
 template void launch_axpy<float>(void *, const void *, size_t, double, int, cudaStream_t);
 
 }  // namespace ovl

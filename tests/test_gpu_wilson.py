@@ -208,3 +208,41 @@ def test_errors_leave_the_context_usable():
         ctx.step(2)
         assert ctx.launch_count > before
         assert np.isfinite(ctx.charges()["NV"])
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("precision,form", [("fp64", "fused"), ("fp32", "fused"), ("fp64", "plain")])
+def test_every_hop_variant_matches_the_oracle(variant, precision, form):
+    """The autotuner picks among kernel variants; each must give the same
+    evolution (N = (4, 6, 5): an odd z extent exercises the partial z chunk of
+    the z-marching variant)."""
+    N = (4, 6, 5)
+    n = 33
+    U = random_links(N, 0.7, 51)
+    E = random_efield(N, 0.3, 52)
+    psi0 = random_modes(n, N, 53)
+    mid0 = random_modes(n, N, 54)
+    p = oracle_params(N, m=0.1, mdw=0.0, dt=0.05, t_sph=1e9)
+    opsi, omid, _, _ = oracle_leapfrog(p, U, E, psi0, mid0, 3)
+    with Context(N=N, n_modes=n, precision=precision, form=form, m_fermion=0.1, m_dw=0.0, dt=0.05, t_sphaleron=1e9,
+                 hop_variant=variant) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_modes(psi0, mid0)
+        ctx.step(3)
+        psi, mid = ctx.get_modes()
+        assert rel_err(psi, opsi) < tol(precision)
+        assert rel_err(mid, omid) < tol(precision)
+
+
+def test_autotune_keeps_state_and_reports_each_variant():
+    N = (6, 6, 6)
+    U = random_links(N, 0.5, 61)
+    with Context(N=N, precision="fp32", form="fused", m_fermion=0.1, m_dw=0.0, dt=0.05) as ctx:
+        ctx.set_links(U)
+        ctx.set_free_fermions()
+        before = ctx.get_modes()
+        v, ms = ctx.autotune()
+        after = ctx.get_modes()
+        assert v in (0, 1, 2) and len(ms) == 3 and all(t > 0 for t in ms)
+        assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
