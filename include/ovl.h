@@ -81,6 +81,21 @@ typedef struct {
      * keep the fastest (ovl_autotune); 0, 1, 2 = fixed.  All variants give the
      * same results. */
     int hop_variant;
+    /* 1: project every link back onto SU(2) after each update (U / |U|,
+     * MaxTraceProjection, SUNc/SU2/GroupOperations.cpp:261-281).  The reference
+     * only measures the unitarity violation (OBSERVABLES/UnitarityViolation.cpp),
+     * so 0 reproduces it. */
+    int reunitarize;
+    /* Coupled gauge + fermion evolution (no reference counterpart: the
+     * reference keeps E fixed under the fermion loop, FERMIONS/WILSON/Update.cpp:48-79).
+     * After each leapfrog step, E += dt (gauge_force ? staple force : 0)
+     *                             + dt backreaction dH_F/dtheta
+     * from the links and modes at the end of the step, with
+     * H_F = (1/2V) sum_m w_m Re <psi_m, h_W psi_m> (ovl_fermion_energy) and
+     * backreaction the coupling g^2; H_gauge + g^2 H_F is then conserved to
+     * O(dt^2).  0 and 0 reproduce the reference.  Wilson fermions only. */
+    int gauge_force;
+    double backreaction;
 } ovl_params;
 
 typedef enum { OVL_SIGN_ZOLOTAREV = 0, OVL_SIGN_CHEBYSHEV = 1 } ovl_sign_method;
@@ -206,6 +221,16 @@ int ovl_update_links(ovl_ctx *ctx, double dt_step);
 /* Dynamics::UpdateElectricFields over the whole lattice (Dynamics.cpp:145-197):
  * E_mu += -2 dt_step sum over the staples of U_mu of Re tr(i t^a U_plaq). */
 int ovl_update_efield(ovl_ctx *ctx, double dt_step);
+
+/* Fermion force on the links: out[a + 3 (mu + 3 site)] = dH_F/dtheta^a_mu(site)
+ * for U_mu(site) -> exp(i theta^a t^a) U_mu(site) and
+ * H_F = (1/2V) sum_m w_m Re <psi_m, h_W psi_m> (mode weights w_m as the
+ * currents, FermionField.cpp:109-122).  No reference counterpart.  Wilson only. */
+int ovl_color_force(ovl_ctx *ctx, double *out);
+
+/* H_F = (1/2V) sum_m w_m Re <psi_m, h_W psi_m> of the current modes and links.
+ * No reference counterpart.  Wilson only. */
+int ovl_fermion_energy(ovl_ctx *ctx, double *out);
 
 /* Observables::Bulk::Update + GaussLaw + Unitarity (OBSERVABLES/BulkObservables.cpp:133-143,
  * GaussLawViolation.cpp:13-61, UnitarityViolation.cpp:13-51):

@@ -589,3 +589,95 @@ void orc_u1_flux(const orc_params *p, int nb, double *out) {
             }
         }
 }
+
+/* ------------------------------------------------------------ back-reaction -- */
+/* Fermion back-reaction: an extension without reference counterpart (the
+ * reference never updates E from the fermions, FERMIONS/WILSON/Update.cpp:48-79).
+ * With U_mu(x) -> exp(i theta^a t^a) U_mu(x) and the fermion energy
+ *   H_F = (1/2V) sum_m w_m Re <psi_m, h_W psi_m>,  h_W = i D,
+ * the hop terms of h_W that contain U_mu(x) give
+ *   dH_F/dtheta^a_mu(x) = -(1/2V) sum_m w_m Re[psi_m(x)^+ g0 (1 - G_mu) i t^a U_mu(x) psi_m(x+mu)],
+ * G_mu = -i gamma_mu.  The coupled equations are dE/dt = dH/dtheta with
+ * H = H_gauge + g^2 H_F, the gauge part being the staple force of
+ * orc_update_efield, so H_gauge + g^2 H_F is conserved. */
+void orc_color_force(const orc_params *p, const double *U, const double *psi, int nmodes, int first, double *out) {
+    const int V = volume(p);
+    cplx G[3][4][4], gp[3][4][4];
+    mat4_scale(-I, GX, G[0]);
+    mat4_scale(-I, GY, G[1]);
+    mat4_scale(-I, GZ, G[2]);
+    for (int mu = 0; mu < 3; mu++) {
+        cplx t[4][4];
+        for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) t[a][b] = (a == b) - G[mu][a][b];
+        mat4_mul(G0, t, gp[mu]);  /* g0 (1 - G_mu) */
+    }
+    static const cplx sig[3][2][2] = {{{0, 1}, {1, 0}}, {{0, -I}, {I, 0}}, {{1, 0}, {0, -1}}};
+    memset(out, 0, sizeof(double) * 9 * (size_t)V);
+    const double pre = 1.0 / (2.0 * V);
+    for (int m = 0; m < nmodes; m++) {
+        const double w = ((first + m) % 2 == 0) ? 1.0 : -1.0;
+        const cplx *mode = (const cplx *)psi + (size_t)SPINOR * V * m;
+        for (int s = 0; s < V; s++) {
+            const cplx *f = mode + SPINOR * s;
+            for (int mu = 0; mu < 3; mu++) {
+                cplx M[2][2];
+                q_matrix(q_load(U, s, mu), M);
+                dress(p, s, mu, M);
+                const cplx *h = mode + SPINOR * shift(p, s, mu, +1);
+                for (int a = 0; a < 3; a++) {
+                    /* colour matrix i t^a M */
+                    cplx A[2][2];
+                    for (int i = 0; i < 2; i++)
+                        for (int j = 0; j < 2; j++) {
+                            A[i][j] = 0;
+                            for (int k = 0; k < 2; k++) A[i][j] += I * 0.5 * sig[a][i][k] * M[k][j];
+                        }
+                    cplx b = 0;
+                    for (int i = 0; i < NC; i++)
+                        for (int j = 0; j < NC; j++)
+                            for (int al = 0; al < 4; al++)
+                                for (int be = 0; be < 4; be++)
+                                    if (gp[mu][al][be] != 0) b += conj(f[4 * i + al]) * gp[mu][al][be] * A[i][j] * h[4 * j + be];
+                    out[a + 3 * (mu + 3 * s)] += -pre * w * creal(b);
+                }
+            }
+        }
+    }
+}
+
+/* (1/2V) sum_m w_m Re <psi_m, i D psi_m>: the fermion energy H_F. */
+double orc_fermion_energy(const orc_params *p, const double *U, const double *psi, int nmodes, int first) {
+    const int V = volume(p);
+    const size_t per_mode = (size_t)2 * SPINOR * V;
+    double *work = malloc(sizeof(double) * per_mode);
+    double e = 0.0;
+    for (int m = 0; m < nmodes; m++) {
+        const double w = ((first + m) % 2 == 0) ? 1.0 : -1.0;
+        orc_wilson_apply(p, U, psi + per_mode * m, work);
+        const cplx *f = (const cplx *)(psi + per_mode * m), *d = (const cplx *)work;
+        cplx t = 0;
+        for (int k = 0; k < SPINOR * V; k++) t += conj(f[k]) * I * d[k];
+        e += w * creal(t);
+    }
+    free(work);
+    return e / (2.0 * V);
+}
+
+/* Coupled leapfrog: the reference step (orc_wilson_leapfrog, links moving every
+ * half step) followed by E += dt (gauge ? staple force : 0) + dt g2 dH_F/dtheta
+ * from the integer-time modes and links. */
+void orc_coupled_leapfrog(const orc_params *p, double *U, double *E, double *psi, double *psimid, int nmodes, int first,
+                          int *tsteps, int nsteps, double g2, int gauge) {
+    const int V = volume(p);
+    double *force = malloc(sizeof(double) * 9 * (size_t)V);
+    for (int n = 0; n < nsteps; n++) {
+        orc_wilson_leapfrog(p, U, E, psi, psimid, nmodes, tsteps, 1);
+        if (gauge) orc_update_efield(p, U, E, p->dt);
+        if (g2 != 0.0) {
+            orc_color_force(p, U, psi, nmodes, first, force);
+            for (size_t k = 0; k < 9 * (size_t)V; k++) E[k] += p->dt * g2 * force[k];
+        }
+    }
+    free(force);
+}

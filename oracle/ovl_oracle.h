@@ -82,6 +82,17 @@ void orc_bulk(const orc_params *p, const double *U, const double *E, double *out
  * index mu + 2*(x + N0*y). */
 void orc_u1_flux(const orc_params *p, int nb, double *out);
 
+/* Fermion back-reaction (an extension: the reference keeps E fixed in the
+ * fermion loop).  out[a + 3 (mu + 3 site)] = dH_F/dtheta^a_mu(site) for
+ * H_F = (1/2V) sum_m w_m Re <psi_m, h_W psi_m> and U_mu -> exp(i theta^a t^a) U_mu. */
+void orc_color_force(const orc_params *p, const double *U, const double *psi, int nmodes, int first, double *out);
+/* H_F = (1/2V) sum_m w_m Re <psi_m, h_W psi_m>. */
+double orc_fermion_energy(const orc_params *p, const double *U, const double *psi, int nmodes, int first);
+/* nsteps of: the reference leapfrog step, then E += dt (staple force if gauge)
+ * + dt g2 dH_F/dtheta (modes and links at the integer time). */
+void orc_coupled_leapfrog(const orc_params *p, double *U, double *E, double *psi, double *psimid, int nmodes, int first,
+                          int *tsteps, int nsteps, double g2, int gauge);
+
 #ifdef __cplusplus
 }
 #endif

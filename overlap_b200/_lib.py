@@ -26,7 +26,7 @@ class ovl_params(C.Structure):
         ("qs", C.c_double), ("t_sphaleron", C.c_double), ("device", C.c_int), ("plain_chunk_modes", C.c_int),
         ("stream", C.c_uint64), ("zolo_poles", C.c_int), ("zolo_tol", C.c_double), ("cg_max_iter", C.c_int),
         ("cg_tol", C.c_double), ("sign_method", C.c_int), ("cheb_degree", C.c_int), ("cheb_eps", C.c_double),
-        ("hop_variant", C.c_int),
+        ("hop_variant", C.c_int), ("reunitarize", C.c_int), ("gauge_force", C.c_int), ("backreaction", C.c_double),
     ]
 
 
@@ -57,6 +57,8 @@ SIGNATURES = {
     "ovl_ncs_update": ([_ctx, _dp, _dp], C.c_int),
     "ovl_update_links": ([_ctx, C.c_double], C.c_int),
     "ovl_update_efield": ([_ctx, C.c_double], C.c_int),
+    "ovl_color_force": ([_ctx, _dp], C.c_int),
+    "ovl_fermion_energy": ([_ctx, _dp], C.c_int),
     "ovl_bulk": ([_ctx, _dp], C.c_int),
     "ovl_synchronize": ([_ctx], C.c_int),
     "ovl_device_modes": ([_ctx, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_size_t)], C.c_int),

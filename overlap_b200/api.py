@@ -75,6 +75,9 @@ class Params:
     cg_max_iter: int = 1000
     cg_tol: float = 1e-16
     hop_variant: int = -1            # -1: autotune on the first step; 0, 1, 2 fixed
+    reunitarize: bool = False        # project links onto SU(2) after each update
+    gauge_force: bool = False        # coupled evolution: staple force on E every step
+    backreaction: float = 0.0        # coupled evolution: g^2 of the fermion force on E
     sign_method: str = "zolotarev"  # or "chebyshev" (the FP32-capable polynomial form)
     cheb_degree: int = 96
     cheb_eps: float = 0.01
@@ -97,6 +100,9 @@ class Params:
         p.zolo_poles, p.zolo_tol = int(self.zolo_poles), float(self.zolo_tol)
         p.cg_max_iter, p.cg_tol = int(self.cg_max_iter), float(self.cg_tol)
         p.hop_variant = int(self.hop_variant)
+        p.reunitarize = int(bool(self.reunitarize))
+        p.gauge_force = int(bool(self.gauge_force))
+        p.backreaction = float(self.backreaction)
         p.sign_method = SIGN_METHODS[self.sign_method]
         p.cheb_degree, p.cheb_eps = int(self.cheb_degree), float(self.cheb_eps)
         return p
@@ -279,6 +285,18 @@ class Context:
         t = np.zeros(1)
         self._check(self._L.ovl_ncs_update(self._ctx, _dp(d), _dp(t)))
         return float(d[0]), float(t[0])
+
+    def color_force(self) -> np.ndarray:
+        """dH_F/dtheta^a_mu(x) as [V, 3 (mu), 3 (a)] (Wilson fermions)."""
+        o = np.empty((volume(self.params.N), 3, 3))
+        self._check(self._L.ovl_color_force(self._ctx, _dp(o)))
+        return o
+
+    def fermion_energy(self) -> float:
+        """H_F = (1/2V) sum_m w_m Re <psi_m, h_W psi_m> (Wilson fermions)."""
+        o = np.empty(1)
+        self._check(self._L.ovl_fermion_energy(self._ctx, _dp(o)))
+        return float(o[0])
 
     def bulk(self) -> dict:
         o = np.empty(10)

@@ -327,6 +327,9 @@ int ovl_params_init(ovl_params *p) {
     p->cg_max_iter = 1000;
     p->cg_tol = 1e-16;
     p->hop_variant = -1;
+    p->reunitarize = 0;
+    p->gauge_force = 0;
+    p->backreaction = 0.0;
     p->sign_method = OVL_SIGN_ZOLOTAREV;
     p->cheb_degree = 96;
     p->cheb_eps = 0.01;
@@ -352,6 +355,9 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     if (p->fermion == OVL_FERMION_OVERLAP && (p->zolo_poles < 1 || p->zolo_poles > ovl::kMaxPoles || p->cg_max_iter < 1))
         return fail(nullptr, OVL_E_ARG, "ovl_create: zolo_poles=%d (1..%d), cg_max_iter=%d", p->zolo_poles, ovl::kMaxPoles,
                     p->cg_max_iter);
+    if (p->backreaction != 0.0 && p->fermion != OVL_FERMION_WILSON)
+        return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: fermion back-reaction is built for Wilson fermions only");
+    if (!std::isfinite(p->backreaction)) return fail(nullptr, OVL_E_ARG, "ovl_create: backreaction must be finite");
     if (p->precision != OVL_PREC_FP64 && p->precision != OVL_PREC_FP32) return fail(nullptr, OVL_E_ARG, "ovl_create: bad precision");
     if (p->form != OVL_FORM_PLAIN && p->form != OVL_FORM_FUSED) return fail(nullptr, OVL_E_ARG, "ovl_create: bad form");
     if (p->n_modes <= 0 || p->first_mode < 0) return fail(nullptr, OVL_E_ARG, "ovl_create: n_modes=%d first_mode=%d", p->n_modes, p->first_mode);
@@ -398,7 +404,8 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
             return bail(rc);
     }
     c->partial_doubles = std::max({ovl::currents_partial_doubles(c->L, c->n_mb), ovl::ncsdot_partial_doubles(c->L),
-                                   ovl::bulk_partial_doubles(c->L), ovl::charges_partial_doubles(c->L, c->n_mb)});
+                                   ovl::bulk_partial_doubles(c->L), ovl::charges_partial_doubles(c->L, c->n_mb),
+                                   ovl::force_partial_doubles(c->L, c->n_mb), ovl::energy_partial_doubles()});
     if ((rc = alloc((void **)&c->partial, sizeof(double) * c->partial_doubles, "reduction scratch")) ||
         (rc = alloc((void **)&c->per_site, sizeof(double) * ovl::kCurrentsPerSite * V, "currents")) ||
         (rc = alloc((void **)&c->dev_small, sizeof(double) * 64, "results")) ||
@@ -618,6 +625,34 @@ int ovl_set_free_fermions(ovl_ctx *c, int *n_bad) {
     return OVL_OK;
 }
 
+// E += dt (staple force) + dt g^2 dH_F/dtheta after a step of the coupled
+// evolution (ovl_params.gauge_force, ovl_params.backreaction).
+int coupled_efield(ovl_ctx *c) {
+    if (c->p.gauge_force) {
+        {
+            ProfScope ps(c, OVL_PROF_LINKS);
+            ovl::launch_update_efield(c->U, c->E, nullptr, c->L, c->p.dt, c->stream);
+        }
+        int rc = launched(c, 1, "gauge force");
+        if (rc) return rc;
+    }
+    if (c->p.backreaction != 0.0) {
+        {
+            ProfScope ps(c, OVL_PROF_OBS);
+            const double coef = c->p.dt * c->p.backreaction;
+            if (fp32(c))
+                ovl::launch_color_force<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
+                                               c->p.first_mode, c->partial, nullptr, c->E, coef, c->stream);
+            else
+                ovl::launch_color_force<double>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
+                                                c->p.first_mode, c->partial, nullptr, c->E, coef, c->stream);
+        }
+        int rc = launched(c, 2, "fermion force");
+        if (rc) return rc;
+    }
+    return OVL_OK;
+}
+
 int ovl_step(ovl_ctx *c, int nsteps) {
     if (!c) return OVL_E_ARG;
     if (nsteps < 0) return fail(c, OVL_E_ARG, "ovl_step: nsteps=%d", nsteps);
@@ -629,7 +664,7 @@ int ovl_step(ovl_ctx *c, int nsteps) {
         if (move) {
             {
                 ProfScope ps(c, OVL_PROF_LINKS);
-                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream, c->U32);
+                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream, c->U32, c->p.reunitarize != 0);
             }
             if ((rc = launched(c, 1, "update links"))) return rc;
         }
@@ -637,11 +672,12 @@ int ovl_step(ovl_ctx *c, int nsteps) {
         if (move) {
             {
                 ProfScope ps(c, OVL_PROF_LINKS);
-                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream, c->U32);
+                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream, c->U32, c->p.reunitarize != 0);
             }
             if ((rc = launched(c, 1, "update links"))) return rc;
         }
         c->tsteps++;
+        if ((rc = coupled_efield(c))) return rc;
     }
     return OVL_OK;
 }
@@ -761,7 +797,7 @@ int ovl_update_links(ovl_ctx *c, double dt_step) {
     if (!c) return OVL_E_ARG;
     int rc = set_device(c);
     if (rc) return rc;
-    ovl::launch_update_links(c->U, c->E, c->L, dt_step, c->stream, c->U32);
+    ovl::launch_update_links(c->U, c->E, c->L, dt_step, c->stream, c->U32, c->p.reunitarize != 0);
     return launched(c, 1, "update links");
 }
 
@@ -771,6 +807,54 @@ int ovl_update_efield(ovl_ctx *c, double dt_step) {
     if (rc) return rc;
     ovl::launch_update_efield(c->U, c->E, nullptr, c->L, dt_step, c->stream);
     return launched(c, 1, "update efield");
+}
+
+int ovl_color_force(ovl_ctx *c, double *out) {
+    if (!c || !out) return OVL_E_ARG;
+    if (c->p.fermion != OVL_FERMION_WILSON) return fail(c, OVL_E_UNSUPPORTED, "ovl_color_force: Wilson fermions only");
+    int rc = set_device(c);
+    if (rc) return rc;
+    double *dev = nullptr;
+    const size_t n = (size_t)9 * c->L.V;
+    if (cudaMalloc(&dev, sizeof(double) * n) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, OVL_E_OOM, "ovl_color_force: output buffer");
+    }
+    if (fp32(c))
+        ovl::launch_color_force<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
+                                       c->p.first_mode, c->partial, dev, nullptr, 0.0, c->stream);
+    else
+        ovl::launch_color_force<double>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
+                                        c->p.first_mode, c->partial, dev, nullptr, 0.0, c->stream);
+    rc = launched(c, 2, "fermion force");
+    cudaError_t e = rc ? cudaSuccess : cudaMemcpyAsync(out, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && !rc) e = cudaStreamSynchronize(c->stream);
+    cudaFree(dev);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(c, e, "ovl_color_force: copy");
+    return OVL_OK;
+}
+
+int ovl_fermion_energy(ovl_ctx *c, double *out) {
+    if (!c || !out) return OVL_E_ARG;
+    if (c->p.fermion != OVL_FERMION_WILSON) return fail(c, OVL_E_UNSUPPORTED, "ovl_fermion_energy: Wilson fermions only");
+    int rc = set_device(c);
+    if (rc) return rc;
+    const double *u1 = c->u1_on ? c->u1 : nullptr;
+    if (fp32(c)) {
+        ovl::launch_wilson<float>(c->U, u1, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), 0.0, false, c->stream);
+        ovl::launch_fermion_energy<float>(c->psi, c->aux_dst, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->partial,
+                                          c->dev_small, c->stream);
+    } else {
+        ovl::launch_wilson<double>(c->U, u1, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), 0.0, false, c->stream);
+        ovl::launch_fermion_energy<double>(c->psi, c->aux_dst, c->L, c->n_mb, c->p.n_modes, c->p.first_mode,
+                                           c->partial, c->dev_small, c->stream);
+    }
+    if ((rc = launched(c, 3, "fermion energy"))) return rc;
+    OVL_CUDA(c, cudaMemcpyAsync(c->host_small, c->dev_small, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    *out = c->host_small[0];
+    return OVL_OK;
 }
 
 int ovl_bulk(ovl_ctx *c, double out[10]) {

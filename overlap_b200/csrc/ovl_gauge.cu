@@ -41,21 +41,30 @@ __device__ void block_reduce(double (&v)[NV], double *sh) {
 // ------------------------------------------------------------ link update --
 // U <- exp(i cU E^a t^a) U with cU = -dt (Dynamics.cpp:97-138, Minkowski, a = 1).
 // U32 (optional): FP32 copy of the updated links for the FP32 hopping kernels.
-__global__ void update_links_kernel(double *U, const double *__restrict__ E, int n_links, double cU, float4 *U32) {
+// reunit: project the updated link back onto SU(2), U / |U| (MaxTraceProjection,
+// SUNc/SU2/GroupOperations.cpp:261-281); the reference never does this during
+// the evolution (it only measures the violation), so it is off by default.
+__global__ void update_links_kernel(double *U, const double *__restrict__ E, int n_links, double cU, float4 *U32,
+                                    int reunit) {
     int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= n_links) return;
     const double *e = E + 3 * l;
     quat g = qexp(cU, e[0], e[1], e[2]);
     const int site = l / 3, mu = l % 3;
-    const quat u = qmul(g, load_link(U, site, mu));
+    quat u = qmul(g, load_link(U, site, mu));
+    if (reunit) {
+        const double nrm = sqrt(u.v0 * u.v0 + u.v1 * u.v1 + u.v2 * u.v2 + u.s * u.s);
+        u = {u.v0 / nrm, u.v1 / nrm, u.v2 / nrm, u.s / nrm};
+    }
     store_link(U, site, mu, u);
     if (U32) U32[l] = float4{(float)u.v0, (float)u.v1, (float)u.v2, (float)u.s};
 }
 
 void launch_update_links(double *U, const double *E, const Lattice &L, double dt_step, cudaStream_t stream,
-                         float *U32) {
+                         float *U32, bool reunit) {
     const int n = 3 * L.V;
-    update_links_kernel<<<(n + 255) / 256, 256, 0, stream>>>(U, E, n, -dt_step, reinterpret_cast<float4 *>(U32));
+    update_links_kernel<<<(n + 255) / 256, 256, 0, stream>>>(U, E, n, -dt_step, reinterpret_cast<float4 *>(U32),
+                                                             reunit ? 1 : 0);
 }
 
 // ------------------------------------------------------- Wilson loops ------

@@ -37,7 +37,7 @@ void launch_axpy(void *dst, const void *deriv, size_t n_complex, double dt, int 
 
 // Gauge fields (FP64).
 void launch_update_links(double *U, const double *E, const Lattice &L, double dt_step, cudaStream_t stream,
-                         float *U32 = nullptr);
+                         float *U32 = nullptr, bool reunit = false);
 void launch_update_efield(const double *U, double *E, double *dE, const Lattice &L, double dt_step, cudaStream_t stream);
 
 // Reductions.  partial: caller-provided device scratch of reduce_partial_doubles()
@@ -63,6 +63,18 @@ void launch_site_sums(const double *per_site, const Lattice &L, double *partial,
 void launch_currents_finish(const double *partial, int groups, const Lattice &L, double *per_site, cudaStream_t stream);
 void launch_overlap_currents(const void *psi, const void *opsi, const Lattice &L, int n_mb, int n_modes,
                              int first_mode, double *partial, double *per_site, cudaStream_t stream);
+// Fermion back-reaction: dH_F/dtheta^a_mu(x) per link (24 doubles of colour
+// bilinears per site and group in `partial`); into out[9 V] when out is set,
+// else E += coef * force.  Fermion energy H_F from psi and dpsi = D psi.
+constexpr int kForcePerSite = 24;
+size_t force_partial_doubles(const Lattice &L, int n_mb);
+template <typename T>
+void launch_color_force(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                        int first_mode, double *partial, double *out, double *E, double coef, cudaStream_t stream);
+size_t energy_partial_doubles();
+template <typename T>
+void launch_fermion_energy(const void *psi, const void *dpsi, const Lattice &L, int n_mb, int n_modes, int first_mode,
+                           double *partial, double *out, cudaStream_t stream);
 // Lattice sums N_V, N_5, PS, WA straight from the modes (no per-site maps).
 size_t charges_partial_doubles(const Lattice &L, int n_mb);
 template <typename T>

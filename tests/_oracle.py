@@ -59,6 +59,11 @@ def oracle():
         L.orc_bulk.argtypes = [P, _dp, _dp, _dp]
         L.orc_u1_flux.argtypes = [P, C.c_int, _dp]
         L.orc_set_u1.argtypes = [_dp]
+        L.orc_color_force.argtypes = [P, _dp, _dp, C.c_int, C.c_int, _dp]
+        L.orc_fermion_energy.argtypes = [P, _dp, _dp, C.c_int, C.c_int]
+        L.orc_fermion_energy.restype = C.c_double
+        L.orc_coupled_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
+                                           C.c_double, C.c_int]
         _oracle = L
     return _oracle
 
