@@ -62,6 +62,12 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+# The FP32 fused half-step kernel of each hop variant (ovl_wilson.cu).
+HOP_KERNELS = {0: "wilson_tuned_kernel<float,1,0,LinksF32<false>>",
+               1: "wilson_tuned_kernel<float,1,1,LinksF32<false>>",
+               2: "wilson_zmarch_kernel<float,1,LinksF32<false>>"}
+
+
 def committed_traffic(kernel: str):
     """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
     p = ROOT / "profiles" / "traffic.json"
@@ -169,7 +175,7 @@ def reference_cpu(wl, steps: int, warmup: int, max_procs: int | None = None):
 
 
 # ---------------------------------------------------------------- GPU arm --
-def time_form(wl, precision, form, steps, warmup, device, profile):
+def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-1):
     import numpy as np
     import torch
 
@@ -179,12 +185,15 @@ def time_form(wl, precision, form, steps, warmup, device, profile):
     N = wl["N"]
     stream = torch.cuda.Stream(device)  # a real stream: the library and the events share it
     ctx = Context(N=N, n_modes=wl.get("modes"), precision=precision, form=form, m_fermion=wl["m"], r_wilson=wl["r"], m_dw=wl["mdw"],
-                  dt=wl["dt"], t_sphaleron=1e300, device=device, stream=stream.cuda_stream)
+                  dt=wl["dt"], t_sphaleron=1e300, device=device, stream=stream.cuda_stream, hop_variant=hop_variant)
     ctx.torch_stream = stream  # keeps the stream alive as long as the context
     ctx.set_links(random_links(N, wl["link_sigma"], wl["seed"]))
     ctx.set_efield(random_efield(N, wl["e_sigma"], wl["seed"] + 1))
     assert ctx.set_free_fermions() == 0
-    variant, variant_ms = ctx.autotune()
+    if hop_variant < 0:
+        variant, variant_ms = ctx.autotune()
+    else:
+        variant, variant_ms = hop_variant, None
     ctx.step(warmup)
     ctx.synchronize()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -321,6 +330,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="n16")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--hop-variant", type=int, default=-1, choices=(-1, 0, 1, 2),
+                    help="-1: autotune the hop kernel before warm-up; 0-2: fixed variant")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 forms")
     ap.add_argument("--modes", type=int, default=0, help="run a smaller case with this many modes (profiling)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
@@ -365,7 +376,7 @@ def main():
 
     # FP32 batched (headline)
     with ClockSampler(device) as clocks:
-        ctx, fp32 = time_form(wl, "fp32", "fused", K, W, device, profile=True)
+        ctx, fp32 = time_form(wl, "fp32", "fused", K, W, device, profile=True, hop_variant=args.hop_variant)
     clk = clocks.summary()
     e2e_steps = max(3, min(K, 20))
     e2e_secs, h2d, d2h, _ = time_e2e(ctx, wl, e2e_steps, device)
@@ -377,7 +388,7 @@ def main():
     forms = {}
     if not args.no_fp64:
         for form in ("plain", "fused"):
-            c, r = time_form(wl, "fp64", form, max(2, K // 2), W, device, profile=True)
+            c, r = time_form(wl, "fp64", form, max(2, K // 2), W, device, profile=True, hop_variant=args.hop_variant)
             c.close()
             del c
             r_ms = max_over_ranks(r["ms"])
@@ -397,7 +408,8 @@ def main():
     alg_bytes = 3 * M * V * elem + 3 * V * 32
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
-    traffic = committed_traffic("wilson_kernel<float,1>")
+    kernel = HOP_KERNELS[fp32["hop_variant"]]
+    traffic = committed_traffic(kernel)
 
     if rank == 0:
         total_ms = {k: v[0] for k, v in fp32["prof"].items()}
@@ -409,7 +421,7 @@ def main():
                     "d2h_bytes_per_step": d2h,
                     "path": "C ABI, host buffers: ovl_set_links + ovl_set_efield (pinned) + ovl_step(1) + ovl_charges"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "kernel": "wilson_kernel<float,1> (fused half step)",
+                         "traffic": traffic, "kernel": kernel + " (FP32 fused half step)",
                          "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms,
                          "peak_source": peak_kind},
             "gpu_launches": fp32["launches"],

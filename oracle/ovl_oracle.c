@@ -681,3 +681,96 @@ void orc_coupled_leapfrog(const orc_params *p, double *U, double *E, double *psi
     }
     free(force);
 }
+
+/* ------------------------------------------------------------------- Ritz -- */
+/* OverlapOperations::RitzSolver with one eigenvalue (FERMIONS/OVERLAP/OPERATOR/
+ * RitzSolver.cpp:91-292; orthog is then a no-op): a conjugate-gradient
+ * minimisation of the Rayleigh quotient of sign * A, A = -D^2 = h_W^2
+ * (WilsonUU, :48-88), from `start` (one mode, [V][Nc][4] complex).  Returns the
+ * extreme Rayleigh quotient (the smallest eigenvalue of sign * A); *iters = the
+ * reference's ittot.  Vectors are kept in the mode layout; only the start
+ * vector's layout matters for the result. */
+static cplx vdot(const cplx *a, const cplx *b, size_t n) {
+    cplx t = 0;
+    for (size_t i = 0; i < n; i++) t += b[i] * conj(a[i]);
+    return t;
+}
+
+static void apply_a(const orc_params *p, const double *U, double sign, const cplx *in, cplx *out, cplx *tmp) {
+    const size_t n = (size_t)SPINOR * volume(p);
+    orc_wilson_apply(p, U, (const double *)in, (double *)tmp);
+    orc_wilson_apply(p, U, (const double *)tmp, (double *)out);
+    for (size_t i = 0; i < n; i++) out[i] = -sign * out[i];
+}
+
+double orc_ritz(const orc_params *p, const double *U, const double *start, double sign, int max_iter, int nrestart,
+                double delitr, int *iters) {
+    const size_t n = (size_t)SPINOR * volume(p);
+    cplx *x = malloc(sizeof(cplx) * n), *y = malloc(sizeof(cplx) * n), *z = malloc(sizeof(cplx) * n);
+    cplx *g = malloc(sizeof(cplx) * n), *pv = malloc(sizeof(cplx) * n), *tmp = malloc(sizeof(cplx) * n);
+    memcpy(x, start, sizeof(cplx) * n);
+    double xn = 1.0 / sqrt(creal(vdot(x, x, n)));
+    for (size_t i = 0; i < n; i++) x[i] *= xn;
+    int ittot = 0, done = 0;
+    cplx xy = 0;
+    while (!done) {
+        apply_a(p, U, sign, x, y, tmp);
+        xy = vdot(x, y, n);
+        for (size_t i = 0; i < n; i++) g[i] = pv[i] = y[i] - xy * x[i];
+        double gnormim = creal(vdot(g, g, n));
+        double pnorm = sqrt(gnormim);
+        for (size_t i = 0; i < n; i++) pv[i] /= pnorm;
+        for (int itt = 1; itt <= nrestart; itt++) {
+            ittot++;
+            apply_a(p, U, sign, pv, z, tmp);
+            const cplx amb = xy - creal(vdot(pv, z, n));
+            const double ccc = creal(vdot(x, z, n));
+            const double cox = 2.0 * ccc / creal(amb);
+            const double sig1 = -copysign(1.0, creal(amb));
+            const double sig2 = copysign(1.0, cox) * sig1;
+            const double c2 = cox * cox;
+            double ct, st;
+            if (c2 <= 1.0e-3) {
+                /* the reference's series for the rotation (:197-200), constants as there */
+                const double sqp = 1.0 - 0.125 * c2 + 0.0859375 * c2 * c2 - 0.0673828125 * c2 * c2 * c2 +
+                                   0.0562439 * c2 * c2 * c2 * c2 + 0.0487 * c2 * c2 * c2 * c2 * c2;
+                const double sqm = 0.5 * sig1 * sig2 * cox *
+                                   (1.0 - 0.375 * c2 + 0.2421875 * c2 * c2 - 0.182617875 * c2 * c2 * c2 +
+                                    0.1482849 * c2 * c2 * c2 * c2 - 0.12575 * c2 * c2 * c2 * c2 * c2 +
+                                    0.1097 * c2 * c2 * c2 * c2 * c2 * c2);
+                if (sig1 < 0.0) { ct = sqm; st = sig2 * sqp; }
+                else { ct = sqp; st = sig2 * sqm; }
+            } else {
+                const double sox = sig1 / sqrt(1.0 + c2);
+                ct = sqrt((1.0 + sox) * 0.5);
+                st = sqrt((1.0 - sox) * 0.5) * sig2;
+            }
+            for (size_t i = 0; i < n; i++) {
+                x[i] = x[i] * ct + pv[i] * st;
+                y[i] = y[i] * ct + z[i] * st;
+            }
+            double xnorm = creal(vdot(x, x, n));
+            const cplx oxy = xy;
+            xy = vdot(x, y, n);
+            xnorm = 1.0 / sqrt(xnorm);
+            xy = xy * xnorm;
+            for (size_t i = 0; i < n; i++) {
+                x[i] = x[i] * xnorm;
+                g[i] = y[i] - xy * x[i];
+            }
+            const double gnorm = creal(vdot(g, g, n));
+            const cplx xp = vdot(x, pv, n);
+            if (creal(xy) > creal(oxy)) { done = 1; break; }
+            if (gnorm < delitr * sign * creal(xy)) { done = 1; break; }
+            const double beta = gnorm / gnormim * pnorm;
+            for (size_t i = 0; i < n; i++) pv[i] = g[i] + beta * (pv[i] - x[i] * xp);
+            pnorm = sqrt(creal(vdot(pv, pv, n)));
+            for (size_t i = 0; i < n; i++) pv[i] /= pnorm;
+            gnormim = gnorm;
+            if (ittot >= max_iter) { done = 1; break; }
+        }
+    }
+    free(x); free(y); free(z); free(g); free(pv); free(tmp);
+    if (iters) *iters = ittot;
+    return creal(xy);
+}

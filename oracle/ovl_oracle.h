@@ -93,6 +93,13 @@ double orc_fermion_energy(const orc_params *p, const double *U, const double *ps
 void orc_coupled_leapfrog(const orc_params *p, double *U, double *E, double *psi, double *psimid, int nmodes, int first,
                           int *tsteps, int nsteps, double g2, int gauge);
 
+/* RitzSolver (FERMIONS/OVERLAP/OPERATOR/RitzSolver.cpp:91-292) with one
+ * eigenvalue: smallest eigenvalue of sign * h_W^2 from `start` ([V][Nc][4]
+ * complex); *iters = iterations.  The reference calls it with max_iter 2000,
+ * nrestart 100, delitr 1e-16 (OverlapUpdate.cpp:53-58). */
+double orc_ritz(const orc_params *p, const double *U, const double *start, double sign, int max_iter, int nrestart,
+                double delitr, int *iters);
+
 #ifdef __cplusplus
 }
 #endif

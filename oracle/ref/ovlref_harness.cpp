@@ -291,6 +291,27 @@ void ovlref_ritz_bounds(double *out) {
     out[1] = Dynamics::Fermions::MaxEValue;
 }
 
+/* OverlapOperations::RitzSolver (RitzSolver.cpp:91-292) on the current links
+ * with the reference's settings (OverlapUpdate.cpp:53-58), one eigenvalue, from
+ * `start` given as one mode [V][Nc][4] complex (the solver's own order is
+ * site + V (spin + 4 colour), RitzSolver.cpp:56-63). */
+double ovlref_ritz_solve(const double *start, double sign) {
+    Quiet q;
+    EvolutionOperator::Setup(GLinks::U);
+    const INT V = Lattice::N[0] * Lattice::N[1] * Lattice::N[2];
+    const INT n = V * Nc * DiracAlgebra::SpinorComponents;
+    std::vector<COMPLEX> v(n);
+    for (INT i = 0; i < V; i++)
+        for (INT j = 0; j < Nc; j++)
+            for (INT k = 0; k < DiracAlgebra::SpinorComponents; k++) {
+                const INT src = (i * Nc + j) * DiracAlgebra::SpinorComponents + k;
+                v[i + V * (k + j * DiracAlgebra::SpinorComponents)] = COMPLEX(start[2 * src], start[2 * src + 1]);
+            }
+    return EvolutionOperator::OverlapOperations::RitzSolver(
+        EvolutionOperator::Ucc, v.data(), Dynamics::Fermions::NumberOfEVals, Dynamics::Fermions::NormRatio,
+        Dynamics::Fermions::MaximumIterations, sign, Dynamics::Fermions::NumberOfRestarts, n);
+}
+
 /* Zolotarev coefficients (ZolotarevCoefficients.cpp:71-175) with the reference's
  * tolerance and pole count (OverlapOperator.cpp:13-14): b[25], d[25]; returns eps. */
 double ovlref_zolotarev(double lambda_min, double lambda_max, double *b, double *d) {

@@ -66,8 +66,37 @@ def run_case(name: str, c: dict) -> dict:
                 jAw=cur[3], PS=cur[4], WA=cur[5], efield_after_update=E1)
 
 
+# Ritz extreme eigenvalues of h_W^2 (FERMIONS/OVERLAP/OPERATOR/RitzSolver.cpp) from a
+# seeded start vector with the reference's distribution (Re, Im uniform in [0, 1),
+# OverlapUpdate.cpp:69-84).
+RITZ_CASES = {
+    "ritz_n4": dict(N=(4, 4, 4), m=0.1, r=1.0, mdw=1.4, link_sigma=0.5, seed=21),
+    "ritz_n465": dict(N=(4, 6, 5), m=0.0, r=1.0, mdw=1.2, link_sigma=0.4, seed=22),
+}
+
+
+def run_ritz_case(name: str, c: dict) -> dict:
+    R = reference("overlap")
+    N = c["N"]
+    V = volume(N)
+    R.ovlref_init(*N, 16, 0, c["m"], c["r"], c["mdw"], 6.0, 0.05, 1.0, 1)
+    U = random_links(N, c["link_sigma"], c["seed"])
+    R.ovlref_set_links(ptr(U))
+    rng = np.random.default_rng(c["seed"] + 1000)
+    start = rng.uniform(0.0, 1.0, (V, 2, 4)) + 1j * rng.uniform(0.0, 1.0, (V, 2, 4))
+    start = np.ascontiguousarray(start / np.linalg.norm(start))
+    lam_min = R.ovlref_ritz_solve(ptr(start.view(np.float64)), 1.0)
+    lam_max = -R.ovlref_ritz_solve(ptr(start.view(np.float64)), -1.0)
+    return dict(N=np.array(N), m_fermion=c["m"], r_wilson=c["r"], m_dw=c["mdw"], links=U, start=start,
+                lambda_min=lam_min, lambda_max=lam_max)
+
+
 if __name__ == "__main__":
     for name, c in CASES.items():
         out = HERE / f"{name}.npz"
         np.savez_compressed(out, **run_case(name, c))
+        print(out, out.stat().st_size, "bytes")
+    for name, c in RITZ_CASES.items():
+        out = HERE / f"{name}.npz"
+        np.savez_compressed(out, **run_ritz_case(name, c))
         print(out, out.stat().st_size, "bytes")

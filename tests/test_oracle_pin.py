@@ -168,3 +168,22 @@ def test_gauge_leapfrog_preserves_gauss_law_and_energy():
         spreads.append(max(abs(e - e0) for e in energies) / e0)
     assert spreads[0] < 0.1
     assert spreads[1] < 0.6 * spreads[0]
+
+
+@pytest.mark.parametrize("name", ["ritz_n4", "ritz_n465"])
+def test_ritz_matches_golden(golden_dir, name):
+    """RitzSolver (RitzSolver.cpp:91-292) restated: the smallest and largest
+    eigenvalues of h_W^2 from the reference's start vector agree with the
+    reference's to 1e-12 (the iteration stops at round-off, so the last few
+    iterates may differ)."""
+    g = dict(np.load(golden_dir / f"{name}.npz"))
+    N = tuple(int(n) for n in g["N"])
+    p = oracle_params(N, m=float(g["m_fermion"]), r=float(g["r_wilson"]), mdw=float(g["m_dw"]))
+    it = C.c_int(0)
+    lo = oracle().orc_ritz(C.byref(p), ptr(g["links"]), ptr(g["start"].view(np.float64)), 1.0, 2000, 100, 1e-16,
+                           C.byref(it))
+    assert 10 < it.value < 2000
+    hi = -oracle().orc_ritz(C.byref(p), ptr(g["links"]), ptr(g["start"].view(np.float64)), -1.0, 2000, 100, 1e-16,
+                            C.byref(it))
+    assert abs(lo - float(g["lambda_min"])) <= 1e-12 * abs(float(g["lambda_min"]))
+    assert abs(hi - float(g["lambda_max"])) <= 1e-12 * abs(float(g["lambda_max"]))
