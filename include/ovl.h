@@ -96,6 +96,14 @@ typedef struct {
      * O(dt^2).  0 and 0 reproduce the reference.  Wilson fermions only. */
     int gauge_force;
     double backreaction;
+    /* Overlap spectral bounds when no schedule is set (ovl_set_spectral_bounds):
+     * 1 = compute them on the GPU before every overlap application, as
+     * Dynamics::Fermions::ComputeRitzEigenvalues does before every half step and
+     * every current measurement (OverlapUpdate.cpp:100-125,
+     * OverlapCurrents.cpp:106-110), from a fresh start vector drawn from the
+     * context's generator (seed ritz_seed); 0 = an unset schedule is an error. */
+    int ritz_auto;
+    uint64_t ritz_seed;
 } ovl_params;
 
 typedef enum { OVL_SIGN_ZOLOTAREV = 0, OVL_SIGN_CHEBYSHEV = 1 } ovl_sign_method;
@@ -169,6 +177,17 @@ int ovl_autotune(ovl_ctx *ctx, int *variant, double ms[3]);
  * FERMIONS/OVERLAP/OPERATOR/ZolotarevCoefficients.cpp:71-175).  *eps receives the
  * relative error estimate of the approximation on the interval. */
 int ovl_zolotarev(double lambda_min, double lambda_max, double tol, int npoles, double *b, double *d, double *eps);
+
+/* Dynamics::Fermions::ComputeRitzEigenvalues (OverlapUpdate.cpp:61-97) on the
+ * GPU: OverlapOperations::RitzSolver (OPERATOR/RitzSolver.cpp:91-292) with the
+ * reference's settings (one eigenvalue, 2000 iterations, restarts every 100,
+ * NormRatio 1e-16) for the smallest and the largest eigenvalue of h_W^2 on the
+ * context's links, both from `start` (one mode, complex [V][Nc][4]; NULL: a
+ * vector of the reference's distribution from the context's generator).
+ * out = {MinEValue, MaxEValue} = {0.95 lambda_min, 1.05 lambda_max};
+ * raw = {lambda_min, lambda_max} and iters = iterations per problem when not
+ * NULL.  Works for both fermion kinds (the Wilson kernel of the context). */
+int ovl_ritz_bounds(ovl_ctx *ctx, const double *start, double out[2], double raw[2], int iters[2]);
 
 /* Statistics of the last overlap application.  Zolotarev: out[0] = lockstep
  * CG iterations, out[1] = largest per-mode iteration count, out[2] = modes

@@ -27,6 +27,7 @@ class ovl_params(C.Structure):
         ("stream", C.c_uint64), ("zolo_poles", C.c_int), ("zolo_tol", C.c_double), ("cg_max_iter", C.c_int),
         ("cg_tol", C.c_double), ("sign_method", C.c_int), ("cheb_degree", C.c_int), ("cheb_eps", C.c_double),
         ("hop_variant", C.c_int), ("reunitarize", C.c_int), ("gauge_force", C.c_int), ("backreaction", C.c_double),
+        ("ritz_auto", C.c_int), ("ritz_seed", C.c_uint64),
     ]
 
 
@@ -57,6 +58,7 @@ SIGNATURES = {
     "ovl_ncs_update": ([_ctx, _dp, _dp], C.c_int),
     "ovl_update_links": ([_ctx, C.c_double], C.c_int),
     "ovl_update_efield": ([_ctx, C.c_double], C.c_int),
+    "ovl_ritz_bounds": ([_ctx, _dp, _dp, _dp, C.POINTER(C.c_int)], C.c_int),
     "ovl_color_force": ([_ctx, _dp], C.c_int),
     "ovl_fermion_energy": ([_ctx, _dp], C.c_int),
     "ovl_bulk": ([_ctx, _dp], C.c_int),

@@ -78,6 +78,8 @@ class Params:
     reunitarize: bool = False        # project links onto SU(2) after each update
     gauge_force: bool = False        # coupled evolution: staple force on E every step
     backreaction: float = 0.0        # coupled evolution: g^2 of the fermion force on E
+    ritz_auto: bool = False          # overlap: GPU Ritz bounds before every application (no schedule set)
+    ritz_seed: int = 0               # generator seed of the Ritz start vectors
     sign_method: str = "zolotarev"  # or "chebyshev" (the FP32-capable polynomial form)
     cheb_degree: int = 96
     cheb_eps: float = 0.01
@@ -103,6 +105,8 @@ class Params:
         p.reunitarize = int(bool(self.reunitarize))
         p.gauge_force = int(bool(self.gauge_force))
         p.backreaction = float(self.backreaction)
+        p.ritz_auto = int(bool(self.ritz_auto))
+        p.ritz_seed = int(self.ritz_seed) & (2**64 - 1)
         p.sign_method = SIGN_METHODS[self.sign_method]
         p.cheb_degree, p.cheb_eps = int(self.cheb_degree), float(self.cheb_eps)
         return p
@@ -285,6 +289,22 @@ class Context:
         t = np.zeros(1)
         self._check(self._L.ovl_ncs_update(self._ctx, _dp(d), _dp(t)))
         return float(d[0]), float(t[0])
+
+    def ritz_bounds(self, start: np.ndarray | None = None) -> dict:
+        """ComputeRitzEigenvalues on the GPU: {"bounds": (MinEValue, MaxEValue),
+        "raw": (lambda_min, lambda_max), "iters": (n_min, n_max)}; start is one
+        mode [V, 2, 4] complex (None: drawn from the context's generator)."""
+        out, raw = np.empty(2), np.empty(2)
+        it = (C.c_int * 2)()
+        sp = None
+        if start is not None:
+            start = np.ascontiguousarray(start, dtype=np.complex128)
+            if start.size != 8 * volume(self.params.N):
+                raise ValueError("start must hold one mode (V x 2 x 4 complex)")
+            sp = _dp(start.view(np.float64))
+        self._check(self._L.ovl_ritz_bounds(self._ctx, sp, _dp(out), _dp(raw), it))
+        return {"bounds": (float(out[0]), float(out[1])), "raw": (float(raw[0]), float(raw[1])),
+                "iters": (int(it[0]), int(it[1]))}
 
     def color_force(self) -> np.ndarray:
         """dH_F/dtheta^a_mu(x) as [V, 3 (mu), 3 (a)] (Wilson fermions)."""

@@ -58,6 +58,10 @@ struct ovl_ctx {
     double *u_old = nullptr, *u_mid = nullptr, *e_mid = nullptr;
     bool have_u_old = false;
     double ncs_total = 0.0;
+    // Ritz solver for the overlap spectral bounds (ovl_ritz_bounds, ritz_auto)
+    void *ritz = nullptr;
+    uint64_t ritz_calls = 0;
+    double ritz_last[2] = {0.0, 0.0};
     // per-kernel timing (ovl_profile_enable): event pairs per kind
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[OVL_PROF_KINDS];
@@ -143,13 +147,68 @@ bool overlap(const ovl_ctx *c) { return c->p.fermion == OVL_FERMION_OVERLAP; }
 // Zolotarev coefficients for the next overlap application; `consume` advances
 // the bounds schedule (OverlapUpdate.cpp:105,119 recompute the bounds before
 // every half step).
-int next_coeffs(ovl_ctx *c, bool consume) {
-    if (c->bounds.empty()) return fail(c, OVL_E_STATE, "overlap: no spectral bounds set (ovl_set_spectral_bounds)");
+// ComputeRitzEigenvalues (OverlapUpdate.cpp:61-97): MinEValue = 0.95 lambda_min,
+// MaxEValue = 1.05 lambda_max, with MaximumIterations 2000, NumberOfRestarts 100,
+// NormRatio 1e-16 (:53-58).
+int ritz_bounds(ovl_ctx *c, const double *start, double out[2], double raw[2], int iters[2]) {
+    if (!c->ritz && !(c->ritz = ovl::ritz_create(c->L.V))) return fail(c, OVL_E_OOM, "Ritz solver: work space");
+    const size_t n = (size_t)c->L.V * ovl::kComp;
+    if (start)
+        OVL_CUDA(c, cudaMemcpyAsync(ovl::ritz_start_buffer(c->ritz), start, sizeof(double2) * n, cudaMemcpyHostToDevice,
+                                    c->stream));
+    else
+        ovl::launch_ritz_random_start(c->ritz, c->p.ritz_seed, c->ritz_calls++, c->stream);
+    double r[2];
+    int it[2];
+    uint64_t nl = start ? 0 : 1;
+    cudaError_t e;
+    {
+        ProfScope ps(c, OVL_PROF_OBS);
+        e = ovl::ritz_run(c->ritz, c->U, c->u1_on ? c->u1 : nullptr, c->L, amass(c->p), 2000, 100, 1e-16, r, it,
+                          c->stream, &nl);
+    }
+    c->launches += nl;
+    if (e != cudaSuccess) return cuda_fail(c, e, "Ritz solver");
+    const double lmin = r[0], lmax = -r[1];
+    if (!(lmin > 0.0) || !(lmax > lmin) || !std::isfinite(lmax))
+        return fail(c, OVL_E_STATE, "Ritz solver: bounds (%g, %g) are not 0 < min < max", lmin, lmax);
+    out[0] = 0.95 * lmin;
+    out[1] = 1.05 * lmax;
+    c->ritz_last[0] = out[0];
+    c->ritz_last[1] = out[1];
+    if (raw) { raw[0] = lmin; raw[1] = lmax; }
+    if (iters) { iters[0] = it[0]; iters[1] = it[1]; }
+    return OVL_OK;
+}
+
+
+// (lambda_min, lambda_max) for the next overlap application: the next pair of
+// the schedule set by ovl_set_spectral_bounds, or, with no schedule and
+// ritz_auto, fresh Ritz bounds (OverlapUpdate.cpp:105,119 compute them before
+// every half step).  `consume` advances the schedule.
+int take_bounds(ovl_ctx *c, bool consume, double &lo, double &hi) {
+    if (c->bounds.empty()) {
+        if (!c->p.ritz_auto) return fail(c, OVL_E_STATE, "overlap: no spectral bounds set (ovl_set_spectral_bounds)");
+        double b[2];
+        int rc = ritz_bounds(c, nullptr, b, nullptr, nullptr);
+        if (rc) return rc;
+        lo = b[0];
+        hi = b[1];
+        return OVL_OK;
+    }
     const size_t pairs = c->bounds.size() / 2;
     size_t i = pairs == 1 ? 0 : c->bound_next;
     if (i >= pairs) return fail(c, OVL_E_STATE, "overlap: spectral-bounds schedule exhausted after %zu applications", pairs);
-    const double lo = c->bounds[2 * i], hi = c->bounds[2 * i + 1];
+    lo = c->bounds[2 * i];
+    hi = c->bounds[2 * i + 1];
     if (consume && pairs > 1) c->bound_next++;
+    return OVL_OK;
+}
+
+int next_coeffs(ovl_ctx *c, bool consume) {
+    double lo, hi;
+    int rc = take_bounds(c, consume, lo, hi);
+    if (rc) return rc;
     if (lo != c->coeff_lo || hi != c->coeff_hi) {
         c->coeffs.npoles = c->p.zolo_poles;
         ovl::zolotarev(lo, hi, c->p.zolo_tol, c->p.zolo_poles, c->coeffs.b, c->coeffs.d);
@@ -163,12 +222,9 @@ int next_coeffs(ovl_ctx *c, bool consume) {
 
 int run_overlap(ovl_ctx *c, const void *src, void *dst, int n_mb, int n_modes, bool accumulate, bool consume) {
     if (c->p.sign_method == OVL_SIGN_CHEBYSHEV) {
-        if (c->bounds.empty()) return fail(c, OVL_E_STATE, "overlap: no spectral bounds set (ovl_set_spectral_bounds)");
-        const size_t pairs = c->bounds.size() / 2;
-        const size_t i = pairs == 1 ? 0 : c->bound_next;
-        if (i >= pairs) return fail(c, OVL_E_STATE, "overlap: spectral-bounds schedule exhausted after %zu applications", pairs);
-        if (consume && pairs > 1) c->bound_next++;
-        const double lo = c->bounds[2 * i], hi = c->bounds[2 * i + 1];
+        double lo, hi;
+        int rc = take_bounds(c, consume, lo, hi);
+        if (rc) return rc;
         ProfScope ps(c, OVL_PROF_HOP);
         uint64_t nl = 0;
         if (fp32(c))
@@ -330,6 +386,8 @@ int ovl_params_init(ovl_params *p) {
     p->reunitarize = 0;
     p->gauge_force = 0;
     p->backreaction = 0.0;
+    p->ritz_auto = 0;
+    p->ritz_seed = 0;
     p->sign_method = OVL_SIGN_ZOLOTAREV;
     p->cheb_degree = 96;
     p->cheb_eps = 0.01;
@@ -470,6 +528,7 @@ int ovl_destroy(ovl_ctx *c) {
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (c->host_small) cudaFreeHost(c->host_small);
+    ovl::ritz_destroy(c->ritz);
     for (auto &v : c->prof)
         for (auto &pr : v) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
@@ -889,6 +948,13 @@ int ovl_launch_count(const ovl_ctx *c, uint64_t *count) {
     if (!c || !count) return OVL_E_ARG;
     *count = c->launches;
     return OVL_OK;
+}
+
+int ovl_ritz_bounds(ovl_ctx *c, const double *start, double out[2], double raw[2], int iters[2]) {
+    if (!c || !out) return OVL_E_ARG;
+    int rc = set_device(c);
+    if (rc) return rc;
+    return ritz_bounds(c, start, out, raw, iters);
 }
 
 int ovl_set_spectral_bounds(ovl_ctx *c, const double *pairs, int count) {

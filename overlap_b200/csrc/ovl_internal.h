@@ -75,6 +75,16 @@ size_t energy_partial_doubles();
 template <typename T>
 void launch_fermion_energy(const void *psi, const void *dpsi, const Lattice &L, int n_mb, int n_modes, int first_mode,
                            double *partial, double *out, cudaStream_t stream);
+// Ritz solver for the overlap spectral bounds (ovl_ritz.cu): work space for a
+// lattice of V sites, the start vector buffer (compact [V][8] double2), a
+// seeded uniform start vector, and the run: out = {lambda_min, -lambda_max}.
+void *ritz_create(int V);
+void ritz_destroy(void *work);
+double2 *ritz_start_buffer(void *work);
+void launch_ritz_random_start(void *work, uint64_t seed, uint64_t call, cudaStream_t stream);
+cudaError_t ritz_run(void *work, const double *U, const double *u1, const Lattice &L, double amass, int max_iter,
+                     int nrestart, double delitr, double out[2], int iters[2], cudaStream_t stream,
+                     uint64_t *launches);
 // Lattice sums N_V, N_5, PS, WA straight from the modes (no per-site maps).
 size_t charges_partial_doubles(const Lattice &L, int n_mb);
 template <typename T>

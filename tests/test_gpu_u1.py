@@ -91,7 +91,8 @@ def test_u1_unit_phases_change_nothing():
     psi0 = random_modes(8, N, 222)
     res = []
     for ph in (None, np.ones((N[1], N[0], 2), np.complex128)):
-        # one fixed hop variant: the variants agree to rounding, not bit for bit
+        # one fixed hop variant; the phase-dressed kernel is compiled separately
+        # (FMA contraction may differ), so agreement is to rounding
         with Context(N=N, n_modes=8, precision="fp64", form="fused", m_fermion=0.05, m_dw=0.0, dt=0.05,
                      hop_variant=0) as ctx:
             ctx.set_links(U)
@@ -99,4 +100,4 @@ def test_u1_unit_phases_change_nothing():
             ctx.set_modes(psi0, psi0)
             ctx.step(3)
             res.append(ctx.get_modes()[0])
-    assert np.array_equal(res[0], res[1])
+    assert rel_err(res[1], res[0]) < 1e-14
