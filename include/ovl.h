@@ -27,6 +27,11 @@
 extern "C" {
 #endif
 
+/* Layout version of ovl_params and of the entry points; ovl_abi_version()
+ * returns the value the library was built with.  A caller compiled against
+ * another version must not pass its ovl_params to the library. */
+#define OVL_ABI_VERSION 4
+
 typedef enum {
     OVL_OK = 0,
     OVL_E_ARG = 1,            /* invalid argument or size */
@@ -114,6 +119,10 @@ typedef struct ovl_ctx ovl_ctx;
  * Dynamics.cpp:17): SU(2) Wilson, FP64 plain, r = 1, m = 0, MDWHeight = 1.4,
  * dt = 0.02, Qs = 1, tSphaleron = 6. */
 int ovl_params_init(ovl_params *p);
+
+/* OVL_ABI_VERSION of the library (compare with the header's before
+ * ovl_params_init). */
+int ovl_abi_version(void);
 
 /* Allocates the device state for p.  Replaces Lattice::Init, Fermions::Init and
  * EvolutionOperator::Init (Simulation.cpp:251-307, FermionField.cpp:632-641). */

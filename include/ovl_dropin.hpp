@@ -73,6 +73,10 @@ inline void SyncModesToHost(FermionField *Psi, FermionField *PsiMid) {
 
 inline void Create(FermionField *Psi, FermionField *PsiMid, int precision, int form) {
     ovl_params p;
+    if (ovl_abi_version() != OVL_ABI_VERSION) {
+        std::fprintf(stderr, "ovl_dropin: libovl_b200 ABI %d, header %d: rebuild\n", ovl_abi_version(), OVL_ABI_VERSION);
+        std::exit(1);
+    }
     ovl_params_init(&p);
     p.N[0] = Lattice::N[0];
     p.N[1] = Lattice::N[1];

@@ -18,6 +18,9 @@ STATUS_NAMES = {
 }
 
 
+ABI_VERSION = 4  # OVL_ABI_VERSION of include/ovl.h
+
+
 class ovl_params(C.Structure):
     _fields_ = [
         ("N", C.c_int * 3), ("n_colours", C.c_int), ("n_modes", C.c_int), ("first_mode", C.c_int),
@@ -38,6 +41,7 @@ _ctx = C.c_void_p
 # name -> (argtypes, restype); every function of include/ovl.h
 SIGNATURES = {
     "ovl_params_init": ([C.POINTER(ovl_params)], C.c_int),
+    "ovl_abi_version": ([], C.c_int),
     "ovl_create": ([C.POINTER(ovl_params), C.POINTER(_ctx)], C.c_int),
     "ovl_destroy": ([_ctx], C.c_int),
     "ovl_last_error": ([_ctx], C.c_char_p),
@@ -88,6 +92,11 @@ def lib() -> C.CDLL:
             raise ImportError(f"overlap_b200 CUDA library not built: {LIB_PATH} is missing "
                               "(run `python -m overlap_b200.build`)")
         L = C.CDLL(str(LIB_PATH))
+        L.ovl_abi_version.argtypes = []
+        L.ovl_abi_version.restype = C.c_int
+        if L.ovl_abi_version() != ABI_VERSION:
+            raise ImportError(f"{LIB_PATH} has ABI {L.ovl_abi_version()}, the bindings expect {ABI_VERSION} "
+                              "(run `python -m overlap_b200.build`)")
         for name, (args, res) in SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args

@@ -359,6 +359,8 @@ int run_currents(ovl_ctx *c) {
 
 extern "C" {
 
+int ovl_abi_version(void) { return OVL_ABI_VERSION; }
+
 int ovl_params_init(ovl_params *p) {
     if (!p) return OVL_E_ARG;
     std::memset(p, 0, sizeof *p);

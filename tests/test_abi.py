@@ -63,3 +63,31 @@ def test_zolotarev_rejects_bad_intervals():
         zolotarev(1.0, 0.5)
     with pytest.raises(OvlError, match="OVL_E_ARG"):
         zolotarev(0.1, 2.0, npoles=0)
+
+
+def test_abi_version_agrees_between_header_bindings_and_library():
+    from overlap_b200 import _lib
+    m = re.search(r"#define OVL_ABI_VERSION (\d+)", (ROOT / "include" / "ovl.h").read_text())
+    assert int(m.group(1)) == _lib.ABI_VERSION == _lib.lib().ovl_abi_version()
+
+
+def test_ctypes_params_layout_matches_the_c_compiler(tmp_path):
+    """Offsets of every ovl_params field as gcc lays them out from include/ovl.h
+    against the ctypes mirror: a mismatch would let ovl_params_init write past
+    the caller's struct."""
+    import shutil
+    import subprocess
+    from overlap_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    fields = [f[0] for f in _lib.ovl_params._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "ovl.h"\nint main(void) {\n'
+                   + "".join(f'  printf("%zu\\n", offsetof(ovl_params, {f}));\n' for f in fields)
+                   + '  printf("%zu\\n", sizeof(ovl_params));\n  return 0;\n}\n')
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", str(ROOT / "include"), "-o", str(exe), str(src)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [getattr(_lib.ovl_params, f).offset for f in fields] + [C.sizeof(_lib.ovl_params)]
+    assert got == want
