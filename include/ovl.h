@@ -260,6 +260,15 @@ int ovl_color_force(ovl_ctx *ctx, double *out);
  * No reference counterpart.  Wilson only. */
 int ovl_fermion_energy(ovl_ctx *ctx, double *out);
 
+/* GaussLawRestoration::Restore (GAUSSLAWFIXING/GaussRestore.cpp:132-168) on the
+ * context's links and E: while the signed maximum of the Gauss-law violation
+ * exceeds tol and fewer than max_iter iterations ran, three damped steps
+ * E_mu -= gamma (G(x) - U_mu(x) G(x+mu) U_mu(x)^+), gamma = 7/24, 7/48, 7/72.
+ * The reference uses max_iter 10000, tol 1e-14.  *iterations = iterations
+ * run; out = {signed max, rms} of the last violation computed (either may be
+ * NULL). */
+int ovl_gauss_restore(ovl_ctx *ctx, int max_iter, double tol, int *iterations, double out[2]);
+
 /* Observables::Bulk::Update + GaussLaw + Unitarity (OBSERVABLES/BulkObservables.cpp:133-143,
  * GaussLawViolation.cpp:13-61, UnitarityViolation.cpp:13-51):
  * out = {T00, TXX, TYY, TZZ, electric, magnetic, gauss max, gauss avg, unitarity max, unitarity avg}. */

@@ -774,3 +774,69 @@ double orc_ritz(const orc_params *p, const double *U, const double *start, doubl
     if (iters) *iters = ittot;
     return creal(xy);
 }
+
+/* ------------------------------------------------------- Gauss restoration -- */
+/* GaussLawRestoration (GAUSSLAWFIXING/GaussRestore.cpp:13-168): G^a(x) =
+ * sum_mu E_mu(x) - U_mu(x-mu)^+ E_mu(x-mu) U_mu(x-mu) (the violation of
+ * orc_bulk), then E_mu(x) -= gamma (G(x) - U_mu(x) G(x+mu) U_mu(x)^+) with
+ * gamma = 7/24, 7/48, 7/72 per iteration, until the signed maximum of G
+ * (:46-49) is at most 1e-14 (10^(1 - digits10), :152) or 10000 iterations.
+ * Returns the iterations; out2 = {max, avg} of the last violation. */
+static double gauss_violation(const orc_params *p, const double *U, const double *E, double *G, double *avg) {
+    const int V = volume(p);
+    double mx = 0.0, sq = 0.0;
+    for (int s = 0; s < V; s++) {
+        double g[3] = {0, 0, 0};
+        for (int mu = 0; mu < 3; mu++) {
+            int sm = shift(p, s, mu, -1);
+            double R[3][3];
+            q_adjoint(q_dag(q_load(U, sm, mu)), R);
+            for (int a = 0; a < 3; a++) {
+                double t = E[a + 3 * (mu + 3 * s)];
+                for (int b = 0; b < 3; b++) t -= R[a][b] * E[b + 3 * (mu + 3 * sm)];
+                g[a] += t;
+            }
+        }
+        for (int a = 0; a < 3; a++) {
+            G[a + 3 * s] = g[a];
+            if (g[a] > mx) mx = g[a];
+            sq += g[a] * g[a];
+        }
+    }
+    *avg = sqrt(sq / (3.0 * V));
+    return mx;
+}
+
+static void gauss_update(const orc_params *p, const double *U, const double *G, double *E, double gamma) {
+    const int V = volume(p);
+    for (int s = 0; s < V; s++)
+        for (int mu = 0; mu < 3; mu++) {
+            double R[3][3];
+            q_adjoint(q_load(U, s, mu), R);
+            const double *gp = G + 3 * shift(p, s, mu, +1);
+            for (int a = 0; a < 3; a++) {
+                double up = 0.0;
+                for (int b = 0; b < 3; b++) up += R[a][b] * gp[b];
+                E[a + 3 * (mu + 3 * s)] -= gamma * (G[a + 3 * s] - up);
+            }
+        }
+}
+
+int orc_gauss_restore(const orc_params *p, const double *U, double *E, int max_iter, double tol, double *out2) {
+    const int V = volume(p);
+    double *G = malloc(sizeof(double) * 3 * (size_t)V);
+    double avg = 0.0;
+    double mx = gauss_violation(p, U, E, G, &avg);
+    int n = 0;
+    static const double gammas[3] = {7.0 / 24.0, 7.0 / 48.0, 7.0 / 72.0};
+    while (n < max_iter && mx > tol) {
+        for (int k = 0; k < 3; k++) {
+            mx = gauss_violation(p, U, E, G, &avg);
+            gauss_update(p, U, G, E, gammas[k]);
+        }
+        n++;
+    }
+    free(G);
+    if (out2) { out2[0] = mx; out2[1] = avg; }
+    return n;
+}

@@ -100,6 +100,11 @@ void orc_coupled_leapfrog(const orc_params *p, double *U, double *E, double *psi
 double orc_ritz(const orc_params *p, const double *U, const double *start, double sign, int max_iter, int nrestart,
                 double delitr, int *iters);
 
+/* GaussLawRestoration::Restore (GAUSSLAWFIXING/GaussRestore.cpp:132-168): the
+ * reference runs max_iter 10000, tol 1e-14.  Returns the iterations; out2 =
+ * {signed max, rms} of the last violation computed. */
+int orc_gauss_restore(const orc_params *p, const double *U, double *E, int max_iter, double tol, double *out2);
+
 #ifdef __cplusplus
 }
 #endif

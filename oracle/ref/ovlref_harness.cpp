@@ -66,6 +66,7 @@ DOUBLE harness_time();
 #include "OBSERVABLES/BulkObservables.cpp"
 #include "OBSERVABLES/GaussLawViolation.cpp"
 #include "OBSERVABLES/UnitarityViolation.cpp"
+#include "GAUSSLAWFIXING/GaussRestore.cpp"
 #include "QED/QED.cpp"
 #include "DiracAlgebra.cpp"
 #include "FERMIONS/FermionField.cpp"
@@ -238,6 +239,15 @@ void ovlref_update_links(double dt_step) {
 void ovlref_update_efield(double dt_step) {
     Dynamics::SetMetric();
     Dynamics::UpdateElectricFields(0, Lattice::N[0] - 1, 0, Lattice::N[1] - 1, 0, Lattice::N[2] - 1, GLinks::U, EFields::E, dt_step);
+}
+
+/* GaussLawRestoration::Restore (GAUSSLAWFIXING/GaussRestore.cpp:132-168) on the
+ * current links and E; out2 = {GlobalMaxViolation, GlobalAvgViolation} after it. */
+void ovlref_gauss_restore(double *out2) {
+    Quiet q;
+    GaussLawRestoration::Restore(GLinks::U, EFields::E);
+    out2[0] = GaussLawRestoration::GlobalMaxViolation;
+    out2[1] = GaussLawRestoration::GlobalAvgViolation;
 }
 
 /* Observables::Bulk::Update: out[0..7] = T00, TXX, TYY, TZZ, E-part, B-part, and

@@ -65,6 +65,7 @@ SIGNATURES = {
     "ovl_ritz_bounds": ([_ctx, _dp, _dp, _dp, C.POINTER(C.c_int)], C.c_int),
     "ovl_color_force": ([_ctx, _dp], C.c_int),
     "ovl_fermion_energy": ([_ctx, _dp], C.c_int),
+    "ovl_gauss_restore": ([_ctx, C.c_int, C.c_double, C.POINTER(C.c_int), _dp], C.c_int),
     "ovl_bulk": ([_ctx, _dp], C.c_int),
     "ovl_synchronize": ([_ctx], C.c_int),
     "ovl_device_modes": ([_ctx, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_size_t)], C.c_int),

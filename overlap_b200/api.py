@@ -318,6 +318,13 @@ class Context:
         self._check(self._L.ovl_fermion_energy(self._ctx, _dp(o)))
         return float(o[0])
 
+    def gauss_restore(self, max_iter: int = 10000, tol: float = 1e-14) -> dict:
+        """GaussLawRestoration::Restore on the device: {"iterations", "max", "avg"}."""
+        n = C.c_int(0)
+        o = np.empty(2)
+        self._check(self._L.ovl_gauss_restore(self._ctx, int(max_iter), float(tol), C.byref(n), _dp(o)))
+        return {"iterations": n.value, "max": float(o[0]), "avg": float(o[1])}
+
     def bulk(self) -> dict:
         o = np.empty(10)
         self._check(self._L.ovl_bulk(self._ctx, _dp(o)))

@@ -465,7 +465,8 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     }
     c->partial_doubles = std::max({ovl::currents_partial_doubles(c->L, c->n_mb), ovl::ncsdot_partial_doubles(c->L),
                                    ovl::bulk_partial_doubles(c->L), ovl::charges_partial_doubles(c->L, c->n_mb),
-                                   ovl::force_partial_doubles(c->L, c->n_mb), ovl::energy_partial_doubles()});
+                                   ovl::force_partial_doubles(c->L, c->n_mb), ovl::energy_partial_doubles(),
+                                   ovl::gauss_partial_doubles(c->L)});
     if ((rc = alloc((void **)&c->partial, sizeof(double) * c->partial_doubles, "reduction scratch")) ||
         (rc = alloc((void **)&c->per_site, sizeof(double) * ovl::kCurrentsPerSite * V, "currents")) ||
         (rc = alloc((void **)&c->dev_small, sizeof(double) * 64, "results")) ||
@@ -916,6 +917,52 @@ int ovl_fermion_energy(ovl_ctx *c, double *out) {
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     *out = c->host_small[0];
     return OVL_OK;
+}
+
+int ovl_gauss_restore(ovl_ctx *c, int max_iter, double tol, int *iterations, double out[2]) {
+    if (!c) return OVL_E_ARG;
+    if (max_iter < 0 || !(tol >= 0.0)) return fail(c, OVL_E_ARG, "ovl_gauss_restore: max_iter=%d tol=%g", max_iter, tol);
+    int rc = set_device(c);
+    if (rc) return rc;
+    double *G = nullptr;
+    if (cudaMalloc(&G, sizeof(double) * 3 * (size_t)c->L.V) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, OVL_E_OOM, "ovl_gauss_restore: violation buffer");
+    }
+    auto done = [&](int status) { cudaFree(G); return status; };
+    double *dv = c->dev_small + 16;  // {sum G^2, max}
+    auto violation = [&]() -> int {
+        ovl::launch_gauss_violation(c->U, c->E, c->L, G, c->partial, dv, c->stream);
+        return launched(c, 2, "gauss violation");
+    };
+    auto read_max = [&](double &mx) -> int {
+        cudaError_t e = cudaMemcpyAsync(c->host_small, dv, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "ovl_gauss_restore");
+        mx = c->host_small[1];
+        return OVL_OK;
+    };
+    // GaussRestore.cpp:132-168: three damped steps per iteration while the
+    // signed maximum of the violation exceeds tol (reference: 1e-14, 10000)
+    static const double gammas[3] = {7.0 / 24.0, 7.0 / 48.0, 7.0 / 72.0};
+    double mx = 0.0;
+    if ((rc = violation()) || (rc = read_max(mx))) return done(rc);
+    int n = 0;
+    while (n < max_iter && mx > tol) {
+        for (double g : gammas) {
+            if ((rc = violation())) return done(rc);
+            ovl::launch_gauss_update(c->U, G, c->E, c->L, g, c->stream);
+            if ((rc = launched(c, 1, "gauss update"))) return done(rc);
+        }
+        n++;
+        if ((rc = read_max(mx))) return done(rc);
+    }
+    if (iterations) *iterations = n;
+    if (out) {
+        out[0] = c->host_small[1];
+        out[1] = std::sqrt(c->host_small[0] / (3.0 * c->L.V));
+    }
+    return done(OVL_OK);
 }
 
 int ovl_bulk(ovl_ctx *c, double out[10]) {

@@ -360,6 +360,78 @@ __global__ void bulk_finish_kernel(const double *__restrict__ partial, int n, La
     out[9] = sqrt(s[7] / (3.0 * V));
 }
 
+// ------------------------------------------------------ Gauss restoration --
+// GaussLawRestoration (GAUSSLAWFIXING/GaussRestore.cpp:13-168).  The violation
+// G^a(x) = sum_mu E_mu(x) - (U^+ E U)_mu(x - mu) per site into G, with the sum of
+// squares and the signed maximum (starting from 0, as :46-49) per block.
+__global__ void __launch_bounds__(kReduceThreads) gauss_violation_kernel(const double *__restrict__ U,
+                                                                         const double *__restrict__ E, Lattice L,
+                                                                         double *__restrict__ G, double *partial) {
+    __shared__ double sh[32 * 2];
+    double v[2] = {0.0, 0.0};
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.V; s += gridDim.x * blockDim.x) {
+        int x, y, z;
+        site_coords(L, s, x, y, z);
+        double g[3] = {0.0, 0.0, 0.0};
+        for (int mu = 0; mu < 3; mu++) {
+            int c[3] = {x, y, z};
+            c[mu] -= 1;
+            const int sm = site_index(L, c[0], c[1], c[2]);
+            adj3 R = adjoint(qdag(load_link(U, sm, mu)));
+            for (int a = 0; a < 3; a++) {
+                double t = E[a + 3 * (mu + 3 * s)];
+                for (int b = 0; b < 3; b++) t -= R.r[a][b] * E[b + 3 * (mu + 3 * sm)];
+                g[a] += t;
+            }
+        }
+        for (int a = 0; a < 3; a++) {
+            G[a + 3 * s] = g[a];
+            v[0] += g[a] * g[a];
+            v[1] = fmax(v[1], g[a]);
+        }
+    }
+    block_reduce<2, true>(v, sh);
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = v[0];
+        partial[2 * blockIdx.x + 1] = v[1];
+    }
+}
+
+// E_mu(x) -= gamma (G(x) - U_mu(x) G(x + mu) U_mu(x)^+)   (GaussRestore.cpp:72-118)
+__global__ void gauss_update_kernel(const double *__restrict__ U, const double *__restrict__ G, double *__restrict__ E,
+                                    Lattice L, double gamma) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * L.V) return;
+    const int s = t / 3, mu = t % 3;
+    int x, y, z;
+    site_coords(L, s, x, y, z);
+    int c[3] = {x, y, z};
+    c[mu] += 1;
+    const int sp = site_index(L, c[0], c[1], c[2]);
+    const adj3 R = adjoint(load_link(U, s, mu));
+    for (int a = 0; a < 3; a++) {
+        double up = 0.0;
+        for (int b = 0; b < 3; b++) up += R.r[a][b] * G[b + 3 * sp];
+        E[a + 3 * (mu + 3 * s)] -= gamma * (G[a + 3 * s] - up);
+    }
+}
+
+size_t gauss_partial_doubles(const Lattice &L) { return (size_t)reduce_blocks(L.V) * 2; }
+
+// out[0] = sum of G^2, out[1] = signed maximum.
+void launch_gauss_violation(const double *U, const double *E, const Lattice &L, double *G, double *partial,
+                            double *out, cudaStream_t stream) {
+    const int nb = reduce_blocks(L.V);
+    gauss_violation_kernel<<<nb, kReduceThreads, 0, stream>>>(U, E, L, G, partial);
+    finish_kernel<2, true><<<1, 256, 0, stream>>>(partial, nb, out, 1.0);
+}
+
+void launch_gauss_update(const double *U, const double *G, double *E, const Lattice &L, double gamma,
+                         cudaStream_t stream) {
+    const int n = 3 * L.V;
+    gauss_update_kernel<<<(n + 127) / 128, 128, 0, stream>>>(U, G, E, L, gamma);
+}
+
 size_t bulk_partial_doubles(const Lattice &L) { return (size_t)reduce_blocks(L.V) * (kBulkVals + 1); }
 
 void launch_bulk(const double *U, const double *E, const Lattice &L, double *partial, double *out, cudaStream_t stream) {

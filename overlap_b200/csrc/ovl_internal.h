@@ -50,6 +50,13 @@ void launch_ncsdot_into(const double *U, const double *E, const Lattice &L, int 
 void launch_geodesic(const double *Uold, const double *Unew, double c, double *Umid, double *Emid, const Lattice &L,
                      cudaStream_t stream);
 size_t bulk_partial_doubles(const Lattice &L);
+// Gauss-law restoration: violation G[3V] with out[0] = sum G^2, out[1] = signed
+// max; then E_mu -= gamma (G - U G(x+mu) U^+).
+size_t gauss_partial_doubles(const Lattice &L);
+void launch_gauss_violation(const double *U, const double *E, const Lattice &L, double *G, double *partial,
+                            double *out, cudaStream_t stream);
+void launch_gauss_update(const double *U, const double *G, double *E, const Lattice &L, double gamma,
+                         cudaStream_t stream);
 void launch_bulk(const double *U, const double *E, const Lattice &L, double *partial, double *out, cudaStream_t stream);
 
 // Currents: 16 doubles per site (jV[4], jA[4], jVw[4], jAw[4]) + PS + WA = 18.

@@ -62,6 +62,8 @@ def oracle():
         L.orc_color_force.argtypes = [P, _dp, _dp, C.c_int, C.c_int, _dp]
         L.orc_fermion_energy.argtypes = [P, _dp, _dp, C.c_int, C.c_int]
         L.orc_fermion_energy.restype = C.c_double
+        L.orc_gauss_restore.argtypes = [P, _dp, _dp, C.c_int, C.c_double, _dp]
+        L.orc_gauss_restore.restype = C.c_int
         L.orc_ritz.argtypes = [P, _dp, _dp, C.c_double, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_int)]
         L.orc_ritz.restype = C.c_double
         L.orc_coupled_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
@@ -102,6 +104,7 @@ def reference(kind: str = "wilson"):
         L.ovlref_u1_flux.argtypes = [C.c_int, _dp]
         L.ovlref_apply.argtypes = [_dp, _dp, C.c_double, C.c_double]
         L.ovlref_set_step_count.argtypes = [C.c_int]
+        L.ovlref_gauss_restore.argtypes = [_dp]
         if kind == "overlap":
             L.ovlref_ritz_bounds.argtypes = [_dp]
             L.ovlref_ritz_solve.argtypes = [_dp, C.c_double]

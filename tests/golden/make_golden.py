@@ -91,6 +91,26 @@ def run_ritz_case(name: str, c: dict) -> dict:
                 lambda_min=lam_min, lambda_max=lam_max)
 
 
+# Gauss-law restoration (GAUSSLAWFIXING/GaussRestore.cpp:132-168) of a random E
+# on random links.
+GAUSS_CASES = {"gauss_n465": dict(N=(4, 6, 5), link_sigma=0.5, e_sigma=0.3, seed=31)}
+
+
+def run_gauss_case(name: str, c: dict) -> dict:
+    R = reference("wilson")
+    N = c["N"]
+    R.ovlref_init(*N, 1, 0, 0.1, 1.0, 0.0, 6.0, 0.05, 1.0, 1)
+    U = random_links(N, c["link_sigma"], c["seed"])
+    E = random_efield(N, c["e_sigma"], c["seed"] + 1)
+    R.ovlref_set_links(ptr(U))
+    R.ovlref_set_efield(ptr(E))
+    out = np.zeros(2)
+    R.ovlref_gauss_restore(ptr(out))
+    E1 = np.zeros_like(E)
+    R.ovlref_get_efield(ptr(E1))
+    return dict(N=np.array(N), links=U, efield=E, efield_restored=E1, max_violation=out[0], avg_violation=out[1])
+
+
 if __name__ == "__main__":
     for name, c in CASES.items():
         out = HERE / f"{name}.npz"
@@ -99,4 +119,8 @@ if __name__ == "__main__":
     for name, c in RITZ_CASES.items():
         out = HERE / f"{name}.npz"
         np.savez_compressed(out, **run_ritz_case(name, c))
+        print(out, out.stat().st_size, "bytes")
+    for name, c in GAUSS_CASES.items():
+        out = HERE / f"{name}.npz"
+        np.savez_compressed(out, **run_gauss_case(name, c))
         print(out, out.stat().st_size, "bytes")

@@ -187,3 +187,19 @@ def test_ritz_matches_golden(golden_dir, name):
                             C.byref(it))
     assert abs(lo - float(g["lambda_min"])) <= 1e-12 * abs(float(g["lambda_min"]))
     assert abs(hi - float(g["lambda_max"])) <= 1e-12 * abs(float(g["lambda_max"]))
+
+
+def test_gauss_restore_matches_golden(golden_dir):
+    """GaussLawRestoration::Restore (GaussRestore.cpp:132-168) restated: the
+    restored E equals the reference's (whose Gauss-violation macro is itself a
+    restatement, see oracle/ref/ovl_calc_macros.h) and the violation ends
+    below 1e-14."""
+    g = dict(np.load(golden_dir / "gauss_n465.npz"))
+    N = tuple(int(n) for n in g["N"])
+    p = oracle_params(N)
+    E = g["efield"].copy()
+    out = np.zeros(2)
+    n = oracle().orc_gauss_restore(C.byref(p), ptr(g["links"]), ptr(E), 10000, 1e-14, ptr(out))
+    assert 5 < n < 10000
+    assert out[0] <= 1e-14
+    assert rel_err(E, g["efield_restored"]) < 1e-12
