@@ -175,7 +175,7 @@ def reference_cpu(wl, steps: int, warmup: int, max_procs: int | None = None):
 
 
 # ---------------------------------------------------------------- GPU arm --
-def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-1):
+def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-1, mode_group=-1):
     import numpy as np
     import torch
 
@@ -185,7 +185,8 @@ def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-
     N = wl["N"]
     stream = torch.cuda.Stream(device)  # a real stream: the library and the events share it
     ctx = Context(N=N, n_modes=wl.get("modes"), precision=precision, form=form, m_fermion=wl["m"], r_wilson=wl["r"], m_dw=wl["mdw"],
-                  dt=wl["dt"], t_sphaleron=1e300, device=device, stream=stream.cuda_stream, hop_variant=hop_variant)
+                  dt=wl["dt"], t_sphaleron=1e300, device=device, stream=stream.cuda_stream, hop_variant=hop_variant,
+                  mode_group=mode_group)
     ctx.torch_stream = stream  # keeps the stream alive as long as the context
     ctx.set_links(random_links(N, wl["link_sigma"], wl["seed"]))
     ctx.set_efield(random_efield(N, wl["e_sigma"], wl["seed"] + 1))
@@ -209,7 +210,7 @@ def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-
     barrier()
     ms = start.elapsed_time(stop)
     out = {"ms": ms, "launches": ctx.launch_count - l0, "charges": ctx.charges(),
-           "hop_variant": variant, "hop_variant_ms": variant_ms}
+           "hop_variant": variant, "hop_variant_ms": variant_ms, "mode_group": ctx.tuning()[1]}
     if profile:
         out["prof"] = ctx.profile_read()
         ctx.profile(False)
@@ -330,6 +331,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="n16")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode-group", type=int, default=-1,
+                    help="fused form: mode blocks per group (-1: autotune with the variant, 0: whole batch)")
     ap.add_argument("--hop-variant", type=int, default=-1, choices=(-1, 0, 1, 2),
                     help="-1: autotune the hop kernel before warm-up; 0-2: fixed variant")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 forms")
@@ -376,7 +379,8 @@ def main():
 
     # FP32 batched (headline)
     with ClockSampler(device) as clocks:
-        ctx, fp32 = time_form(wl, "fp32", "fused", K, W, device, profile=True, hop_variant=args.hop_variant)
+        ctx, fp32 = time_form(wl, "fp32", "fused", K, W, device, profile=True, hop_variant=args.hop_variant,
+                                 mode_group=args.mode_group)
     clk = clocks.summary()
     e2e_steps = max(3, min(K, 20))
     e2e_secs, h2d, d2h, _ = time_e2e(ctx, wl, e2e_steps, device)
@@ -388,28 +392,41 @@ def main():
     forms = {}
     if not args.no_fp64:
         for form in ("plain", "fused"):
-            c, r = time_form(wl, "fp64", form, max(2, K // 2), W, device, profile=True, hop_variant=args.hop_variant)
+            c, r = time_form(wl, "fp64", form, max(2, K // 2), W, device, profile=True, hop_variant=args.hop_variant,
+                                 mode_group=args.mode_group)
             c.close()
             del c
             r_ms = max_over_ranks(r["ms"])
             forms[form] = {"value": world * M * V * max(2, K // 2) / (r_ms / 1e3), "ms_per_step": r_ms / max(2, K // 2),
                            "hop_ms_per_launch": r["prof"]["hop"][0] / max(1, r["prof"]["hop"][1]),
-                           "N5": r["charges"]["N5"], "hop_variant": r["hop_variant"],
+                           "N5": r["charges"]["N5"], "hop_variant": r["hop_variant"], "mode_group": r["mode_group"],
                            "hop_variant_ms": r["hop_variant_ms"]}
 
     acc = None
     if args.accuracy_steps > 0 and rank == 0:
         acc = accuracy(wl, args.accuracy_steps, 50, device)
 
-    # roofline of the dominant kernel (Wilson fused half step, FP32)
+    # roofline of the dominant kernel (Wilson fused half step, FP32).  Ungrouped:
+    # one event pair per half-step launch, 3 elements per mode-site (read the
+    # source, read and write the destination).  Grouped (mode_group > 0): one
+    # event pair around a step's launches, whose minimal traffic is 4 elements
+    # per mode-site (read psi and psimid, write both: the second half step
+    # re-reads the first one's output from L2).
     hop_ms, hop_n = fp32["prof"]["hop"]
     per_launch_ms = hop_ms / max(1, hop_n)
     elem = 8 * 8  # 2 colours x 4 spins x complex<float>
-    alg_bytes = 3 * M * V * elem + 3 * V * 32
+    n_mb = (M + 31) // 32
+    grouped = 0 < fp32["mode_group"] < n_mb
+    if grouped:
+        alg_bytes = 4 * M * V * elem + 2 * 3 * V * 32
+        unit = f"one leapfrog step: both half steps in groups of {fp32['mode_group']} mode blocks"
+    else:
+        alg_bytes = 3 * M * V * elem + 3 * V * 32
+        unit = "one half step (one launch)"
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
     kernel = HOP_KERNELS[fp32["hop_variant"]]
-    traffic = committed_traffic(kernel)
+    traffic = committed_traffic(kernel + (" grouped" if grouped else ""))
 
     if rank == 0:
         total_ms = {k: v[0] for k, v in fp32["prof"].items()}
@@ -423,11 +440,13 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "kernel": kernel + " (FP32 fused half step)",
                          "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms,
+                         "unit_of_work": unit,
                          "peak_source": peak_kind},
             "gpu_launches": fp32["launches"],
             "kernel_ms": total_ms,
             "forms": {"fp32_fused": {"value": value, "ms_per_step": ms / K, "N5": fp32["charges"]["N5"],
-                                     "hop_variant": fp32["hop_variant"], "hop_variant_ms": fp32["hop_variant_ms"]},
+                                     "hop_variant": fp32["hop_variant"], "hop_variant_ms": fp32["hop_variant_ms"],
+                                     "mode_group": fp32["mode_group"]},
                       **{f"fp64_{k}": v for k, v in forms.items()}},
             "clocks": clk,
         }

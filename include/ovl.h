@@ -30,7 +30,7 @@ extern "C" {
 /* Layout version of ovl_params and of the entry points; ovl_abi_version()
  * returns the value the library was built with.  A caller compiled against
  * another version must not pass its ovl_params to the library. */
-#define OVL_ABI_VERSION 4
+#define OVL_ABI_VERSION 5
 
 typedef enum {
     OVL_OK = 0,
@@ -109,6 +109,13 @@ typedef struct {
      * context's generator (seed ritz_seed); 0 = an unset schedule is an error. */
     int ritz_auto;
     uint64_t ritz_seed;
+    /* Fused Wilson form: the two half steps of a leapfrog step run group by
+     * group of mode_group mode blocks (32 modes each), so that a group's fields,
+     * written by the first half step, are still in L2 when the second reads
+     * them (4 instead of 6 field passes through HBM per step; the same
+     * arithmetic, so the same results).  -1 = chosen by the autotuner with
+     * the hop variant; 0 = whole batch per half step; k > 0 = k blocks. */
+    int mode_group;
 } ovl_params;
 
 typedef enum { OVL_SIGN_ZOLOTAREV = 0, OVL_SIGN_CHEBYSHEV = 1 } ovl_sign_method;
@@ -179,6 +186,10 @@ int ovl_apply(ovl_ctx *ctx, int count, const double *phi, double *out);
  * ahead, 2 = (x, y) columns marching in z with register reuse.  *variant
  * receives the choice, ms[v] the time of one half step with variant v. */
 int ovl_autotune(ovl_ctx *ctx, int *variant, double ms[3]);
+
+/* The hop variant and mode grouping in use (after the autotuner ran, or as
+ * set in ovl_params); -1 before either is known. */
+int ovl_tuning(const ovl_ctx *ctx, int *variant, int *mode_group);
 
 /* Zolotarev coefficients of the overlap sign function for spectral bounds
  * [lambda_min, lambda_max] of h_W^2: (h_W^2)^(-1/2) ~ sum_l b[l] / (h_W^2 + d[l]),

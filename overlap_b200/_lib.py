@@ -18,7 +18,7 @@ STATUS_NAMES = {
 }
 
 
-ABI_VERSION = 4  # OVL_ABI_VERSION of include/ovl.h
+ABI_VERSION = 5  # OVL_ABI_VERSION of include/ovl.h
 
 
 class ovl_params(C.Structure):
@@ -30,7 +30,7 @@ class ovl_params(C.Structure):
         ("stream", C.c_uint64), ("zolo_poles", C.c_int), ("zolo_tol", C.c_double), ("cg_max_iter", C.c_int),
         ("cg_tol", C.c_double), ("sign_method", C.c_int), ("cheb_degree", C.c_int), ("cheb_eps", C.c_double),
         ("hop_variant", C.c_int), ("reunitarize", C.c_int), ("gauge_force", C.c_int), ("backreaction", C.c_double),
-        ("ritz_auto", C.c_int), ("ritz_seed", C.c_uint64),
+        ("ritz_auto", C.c_int), ("ritz_seed", C.c_uint64), ("mode_group", C.c_int),
     ]
 
 
@@ -62,6 +62,7 @@ SIGNATURES = {
     "ovl_ncs_update": ([_ctx, _dp, _dp], C.c_int),
     "ovl_update_links": ([_ctx, C.c_double], C.c_int),
     "ovl_update_efield": ([_ctx, C.c_double], C.c_int),
+    "ovl_tuning": ([_ctx, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "ovl_ritz_bounds": ([_ctx, _dp, _dp, _dp, C.POINTER(C.c_int)], C.c_int),
     "ovl_color_force": ([_ctx, _dp], C.c_int),
     "ovl_fermion_energy": ([_ctx, _dp], C.c_int),

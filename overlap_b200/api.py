@@ -80,6 +80,7 @@ class Params:
     backreaction: float = 0.0        # coupled evolution: g^2 of the fermion force on E
     ritz_auto: bool = False          # overlap: GPU Ritz bounds before every application (no schedule set)
     ritz_seed: int = 0               # generator seed of the Ritz start vectors
+    mode_group: int = -1             # fused form: mode blocks per group (-1 autotune, 0 whole batch)
     sign_method: str = "zolotarev"  # or "chebyshev" (the FP32-capable polynomial form)
     cheb_degree: int = 96
     cheb_eps: float = 0.01
@@ -107,6 +108,7 @@ class Params:
         p.backreaction = float(self.backreaction)
         p.ritz_auto = int(bool(self.ritz_auto))
         p.ritz_seed = int(self.ritz_seed) & (2**64 - 1)
+        p.mode_group = int(self.mode_group)
         p.sign_method = SIGN_METHODS[self.sign_method]
         p.cheb_degree, p.cheb_eps = int(self.cheb_degree), float(self.cheb_eps)
         return p
@@ -234,6 +236,12 @@ class Context:
         ms = np.zeros(3)
         self._check(self._L.ovl_autotune(self._ctx, C.byref(v), _dp(ms)))
         return v.value, ms.tolist()
+
+    def tuning(self) -> tuple[int, int]:
+        """(hop variant, mode blocks per group) in use; -1 before the autotuner ran."""
+        v, g = C.c_int(-1), C.c_int(-1)
+        self._check(self._L.ovl_tuning(self._ctx, C.byref(v), C.byref(g)))
+        return v.value, g.value
 
     def solver_stats(self) -> dict:
         o = (C.c_int * 3)()

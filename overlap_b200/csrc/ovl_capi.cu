@@ -54,6 +54,9 @@ struct ovl_ctx {
     // FP32 copies of links and phases for the FP32 hopping kernels; kernel variant
     float *U32 = nullptr, *u1_32 = nullptr;
     int hop_variant = -1;  // -1: autotune before the first step
+    int mode_group = -1;   // mode blocks per group of the grouped fused step (0: whole batch)
+    double *U_b = nullptr; // links at the half step (grouped fused step)
+    float *U32_b = nullptr;
     // Chern-Simons number along the cooling path (ovl_ncs_update)
     double *u_old = nullptr, *u_mid = nullptr, *e_mid = nullptr;
     bool have_u_old = false;
@@ -267,6 +270,61 @@ void refresh_links32(ovl_ctx *c) {
     }
 }
 
+// One leapfrog step's hop work in the fused form, group by group:
+// dst1 += dt D(src1) with links h1, then dst2 += dt D(src2) with links h2, for
+// each group of `group` mode blocks (group <= 0 or >= n_mb: the whole batch).
+void grouped_pass(ovl_ctx *c, const ovl::HopConfig &h1, const ovl::HopConfig &h2, const void *src1, void *dst1,
+                  const void *src2, void *dst2, int group) {
+    const int G = (group <= 0 || group >= c->n_mb) ? c->n_mb : group;
+    for (int g0 = 0; g0 < c->n_mb; g0 += G) {
+        const int nmb = std::min(G, c->n_mb - g0);
+        if (fp32(c)) {
+            ovl::launch_wilson_tuned<float>(h1, src1, dst1, c->L, g0, nmb, amass(c->p), c->p.dt, true, c->stream);
+            ovl::launch_wilson_tuned<float>(h2, src2, dst2, c->L, g0, nmb, amass(c->p), c->p.dt, true, c->stream);
+        } else {
+            ovl::launch_wilson_tuned<double>(h1, src1, dst1, c->L, g0, nmb, amass(c->p), c->p.dt, true, c->stream);
+            ovl::launch_wilson_tuned<double>(h2, src2, dst2, c->L, g0, nmb, amass(c->p), c->p.dt, true, c->stream);
+        }
+        c->launches += 2;
+    }
+}
+
+// Candidate group sizes (mode blocks) of the grouped fused step; 0 = whole batch.
+constexpr int kGroupCandidates[] = {0, 1, 2, 4, 8};
+
+// Times the grouped step pattern (psimid -> aux_dst -> aux_src: the state is
+// not touched) for each candidate group size and keeps the fastest.
+int autotune_groups(ovl_ctx *c) {
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        return fail(c, OVL_E_CUDA, "autotune: events");
+    const size_t bytes = c->field_complex * c->elem_bytes;
+    cudaMemsetAsync(c->aux_src, 0, bytes, c->stream);
+    cudaMemsetAsync(c->aux_dst, 0, bytes, c->stream);
+    const ovl::HopConfig h = hop_config(c);
+    double best = 1e300;
+    int pick = 0;
+    for (int G : kGroupCandidates) {
+        if (G >= c->n_mb) continue;
+        float total = 0.0f;
+        for (int rep = 0; rep < 4; rep++) {
+            cudaEventRecord(e0, c->stream);
+            grouped_pass(c, h, h, c->psimid, c->aux_dst, c->aux_dst, c->aux_src, G);
+            cudaEventRecord(e1, c->stream);
+            cudaEventSynchronize(e1);
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (rep > 0) total += t;
+        }
+        if (total < best) { best = total; pick = G; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->mode_group = pick;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? OVL_OK : cuda_fail(c, e, "autotune (groups)");
+}
+
 // Times each hop-kernel variant on the live fields (psi -> operator buffer,
 // the context's state is not touched) and keeps the fastest.
 int autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
@@ -296,7 +354,9 @@ int autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->hop_variant = pick;
-    return launched(c, 4 * ovl::kHopVariants, "autotune");
+    int rc = launched(c, 4 * ovl::kHopVariants, "autotune");
+    if (!rc && c->mode_group < 0) rc = autotune_groups(c);
+    return rc;
 }
 
 // psi_dst += dt * D psi_src over all modes (one Update.cpp half step).
@@ -390,6 +450,7 @@ int ovl_params_init(ovl_params *p) {
     p->backreaction = 0.0;
     p->ritz_auto = 0;
     p->ritz_seed = 0;
+    p->mode_group = -1;
     p->sign_method = OVL_SIGN_ZOLOTAREV;
     p->cheb_degree = 96;
     p->cheb_eps = 0.01;
@@ -422,6 +483,7 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     if (p->form != OVL_FORM_PLAIN && p->form != OVL_FORM_FUSED) return fail(nullptr, OVL_E_ARG, "ovl_create: bad form");
     if (p->n_modes <= 0 || p->first_mode < 0) return fail(nullptr, OVL_E_ARG, "ovl_create: n_modes=%d first_mode=%d", p->n_modes, p->first_mode);
     if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return fail(nullptr, OVL_E_ARG, "ovl_create: dt must be positive");
+    if (p->mode_group < -1) return fail(nullptr, OVL_E_ARG, "ovl_create: mode_group=%d", p->mode_group);
     if (p->hop_variant < -1 || p->hop_variant >= ovl::kHopVariants)
         return fail(nullptr, OVL_E_ARG, "ovl_create: hop_variant=%d (-1 = autotune, 0..%d)", p->hop_variant, ovl::kHopVariants - 1);
     const long long V = (long long)p->N[0] * p->N[1] * p->N[2];
@@ -479,6 +541,10 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     if (p->precision == OVL_PREC_FP32 && (rc = alloc((void **)&c->U32, sizeof(float) * 12 * V, "FP32 links")))
         return bail(rc);
     c->hop_variant = p->hop_variant;
+    // grouping applies to the fused Wilson form; fixed when the variant is fixed
+    if (p->form != OVL_FORM_FUSED || p->fermion != OVL_FERMION_WILSON) c->mode_group = 0;
+    else if (p->mode_group >= 0) c->mode_group = p->mode_group;
+    else c->mode_group = p->hop_variant >= 0 ? 0 : -1;
     if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method == OVL_SIGN_CHEBYSHEV) {
         ovl::ChebyshevWork &w = c->cw;
         if ((rc = alloc(&w.b0, field_bytes, "Clenshaw b")) || (rc = alloc(&w.b1, field_bytes, "Clenshaw b")) ||
@@ -526,7 +592,7 @@ int ovl_destroy(ovl_ctx *c) {
     void *bufs[] = {c->psi, c->psimid, c->U, c->E, c->deriv, c->per_site, c->partial, c->dev_small, c->dev_int,
                     c->aux_src, c->aux_dst, c->ow.r, c->ow.q, c->ow.t, c->ow.x, c->ow.p, c->ow.part, c->ow.rnorm,
                     c->ow.alpha, c->ow.active, c->ow.dz, c->u_old, c->u_mid, c->e_mid, c->u1,
-                    c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w, c->U32, c->u1_32};
+                    c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w, c->U32, c->u1_32, c->U_b, c->U32_b};
     if (c->ow.host_count) cudaFreeHost(c->ow.host_count);
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -715,12 +781,70 @@ int coupled_efield(ovl_ctx *c) {
     return OVL_OK;
 }
 
+// One leapfrog step of the fused Wilson form, group by group of mode blocks
+// (ovl_params.mode_group).  The second half step needs the links of the half
+// step while later groups' first half steps still need the step's starting
+// links: the half-step links are built out of place in U_b (and U32_b), the
+// step-end links are U_b advanced in place, and U/U_b swap.  Per element the
+// arithmetic is that of ovl_step's ungrouped path.
+int grouped_step(ovl_ctx *c) {
+    const bool move = c->p.qs * (c->tsteps * c->p.dt) < c->p.t_sphaleron;  // Update.cpp:57
+    const size_t nl = (size_t)12 * c->L.V;
+    if (move && !c->U_b) {
+        if (cudaMalloc(&c->U_b, sizeof(double) * nl) != cudaSuccess ||
+            (c->U32 && cudaMalloc(&c->U32_b, sizeof(float) * nl) != cudaSuccess)) {
+            cudaGetLastError();
+            return fail(c, OVL_E_OOM, "ovl_step: half-step links");
+        }
+    }
+    ovl::HopConfig h1 = hop_config(c), h2 = h1;
+    if (move) {
+        OVL_CUDA(c, cudaMemcpyAsync(c->U_b, c->U, sizeof(double) * nl, cudaMemcpyDeviceToDevice, c->stream));
+        {
+            ProfScope ps(c, OVL_PROF_LINKS);
+            ovl::launch_update_links(c->U_b, c->E, c->L, 0.5 * c->p.dt, c->stream, c->U32_b, c->p.reunitarize != 0);
+        }
+        int rc = launched(c, 1, "update links");
+        if (rc) return rc;
+        h2.U = c->U_b;
+        if (c->U32) h2.U32 = c->U32_b;
+    }
+    {
+        ProfScope ps(c, OVL_PROF_HOP);
+        grouped_pass(c, h1, h2, c->psimid, c->psi, c->psi, c->psimid, c->mode_group);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "wilson (grouped)");
+    if (move) {
+        {
+            ProfScope ps(c, OVL_PROF_LINKS);
+            ovl::launch_update_links(c->U_b, c->E, c->L, 0.5 * c->p.dt, c->stream, c->U32_b, c->p.reunitarize != 0);
+        }
+        int rc = launched(c, 1, "update links");
+        if (rc) return rc;
+        std::swap(c->U, c->U_b);
+        std::swap(c->U32, c->U32_b);
+    }
+    return OVL_OK;
+}
+
 int ovl_step(ovl_ctx *c, int nsteps) {
     if (!c) return OVL_E_ARG;
     if (nsteps < 0) return fail(c, OVL_E_ARG, "ovl_step: nsteps=%d", nsteps);
     int rc = set_device(c);
     if (rc) return rc;
+    if (!overlap(c) && c->p.form == OVL_FORM_FUSED && nsteps > 0) {
+        if (c->hop_variant < 0) rc = autotune(c, nullptr);
+        else if (c->mode_group < 0) rc = autotune_groups(c);
+        if (rc) return rc;
+    }
     for (int n = 0; n < nsteps; n++) {
+        if (!overlap(c) && c->p.form == OVL_FORM_FUSED && c->mode_group > 0 && c->mode_group < c->n_mb) {
+            if ((rc = grouped_step(c))) return rc;
+            c->tsteps++;
+            if ((rc = coupled_efield(c))) return rc;
+            continue;
+        }
         const bool move = c->p.qs * (c->tsteps * c->p.dt) < c->p.t_sphaleron;  // Update.cpp:57
         if ((rc = half_step(c, c->psimid, c->psi))) return rc;
         if (move) {
@@ -1050,6 +1174,13 @@ int ovl_apply(ovl_ctx *c, int count, const double *phi, double *out) {
         return done(fail(c, OVL_E_CUDA, "ovl_apply: download"));
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return done(fail(c, OVL_E_CUDA, "ovl_apply: synchronise"));
     return done(OVL_OK);
+}
+
+int ovl_tuning(const ovl_ctx *c, int *variant, int *mode_group) {
+    if (!c) return OVL_E_ARG;
+    if (variant) *variant = c->hop_variant;
+    if (mode_group) *mode_group = c->mode_group;
+    return OVL_OK;
 }
 
 int ovl_autotune(ovl_ctx *c, int *variant, double ms[3]) {

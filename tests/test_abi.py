@@ -91,3 +91,9 @@ def test_ctypes_params_layout_matches_the_c_compiler(tmp_path):
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [getattr(_lib.ovl_params, f).offset for f in fields] + [C.sizeof(_lib.ovl_params)]
     assert got == want
+
+
+def test_mode_group_is_validated():
+    from overlap_b200 import Context, OvlError
+    with pytest.raises(OvlError):
+        Context(N=(4, 4, 4), n_modes=8, form="fused", mode_group=-2)
