@@ -62,6 +62,10 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+# What each FP32-class form stores and computes in.
+DTYPES = {"fp32": "f32 modes and hop arithmetic, f64 links",
+          "fp40": "modes in 40 bits (top bits of f64), f64 hop arithmetic, observables and links"}
+
 # The FP32 fused half-step kernel of each hop variant (ovl_wilson.cu).
 HOP_KERNELS = {0: "wilson_tuned_kernel<float,1,0,LinksF32<false>>",
                1: "wilson_tuned_kernel<float,1,1,LinksF32<false>>",
@@ -175,7 +179,7 @@ def reference_cpu(wl, steps: int, warmup: int, max_procs: int | None = None):
 
 
 # ---------------------------------------------------------------- GPU arm --
-def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-1, mode_group=-1):
+def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-1, mode_group=0):
     import numpy as np
     import torch
 
@@ -248,8 +252,8 @@ def time_e2e(ctx, wl, steps, device):
 
 
 def accuracy(wl, steps, every, device):
-    """FP32 modes against FP64 on the same inputs over `steps` leapfrog steps:
-    for o in (N_5, N_CS) the error max_t |o_32(t) - o_64(t)| / max_t |o_64(t) - o_64(0)|,
+    """FP32 and FP40 modes against FP64 on the same inputs over `steps` leapfrog
+    steps: for o in (N_5, N_CS) the error max_t |o(t) - o_64(t)| / max_t |o_64(t) - o_64(0)|,
     N_CS accumulated every `every` steps by the cooling-path rule
     (CoolingMethod::GetDeltaNCs, cooling off)."""
     import numpy as np
@@ -260,7 +264,7 @@ def accuracy(wl, steps, every, device):
 
     N = wl["N"]
     series = {}
-    for prec in ("fp64", "fp32"):
+    for prec in ("fp64", "fp32", "fp40"):
         ctx = Context(N=N, n_modes=wl.get("modes"), precision=prec, form="fused", m_fermion=wl["m"], r_wilson=wl["r"],
                       m_dw=wl["mdw"], dt=wl["dt"], t_sphaleron=1e300, device=device)
         ctx.set_links(random_links(N, wl["link_sigma"], wl["seed"]))
@@ -277,12 +281,15 @@ def accuracy(wl, steps, every, device):
         series[prec] = (np.array(n5), np.array(ncs))
         torch.cuda.synchronize(device)
     out = {"steps": (steps // every) * every, "every": every}
-    for k, name in ((0, "N5"), (1, "NCS")):
-        a, b = series["fp32"][k], series["fp64"][k]
-        span = np.max(np.abs(b - b[0]))
-        out[f"{name}_rel_err"] = float(np.max(np.abs(a - b)) / span) if span > 0 else 0.0
-        out[f"{name}_fp64_final"] = float(b[-1])
-        out[f"{name}_fp64_span"] = float(span)
+    for prec in ("fp32", "fp40"):
+        o = {}
+        for k, name in ((0, "N5"), (1, "NCS")):
+            a, b = series[prec][k], series["fp64"][k]
+            span = np.max(np.abs(b - b[0]))
+            o[f"{name}_rel_err"] = float(np.max(np.abs(a - b)) / span) if span > 0 else 0.0
+            out[f"{name}_fp64_final"] = float(b[-1])
+            out[f"{name}_fp64_span"] = float(span)
+        out[prec] = o
     return out
 
 
@@ -331,8 +338,10 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="n16")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode-group", type=int, default=-1,
-                    help="fused form: mode blocks per group (-1: autotune with the variant, 0: whole batch)")
+    ap.add_argument("--headline", choices=("fp40", "fp32"), default="fp40",
+                    help="the FP32-class form of the headline value (the other is reported beside it)")
+    ap.add_argument("--mode-group", type=int, default=0,
+                    help="fused form: mode blocks per group (0: whole batch, -1: autotune with the variant)")
     ap.add_argument("--hop-variant", type=int, default=-1, choices=(-1, 0, 1, 2),
                     help="-1: autotune the hop kernel before warm-up; 0-2: fixed variant")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 forms")
@@ -377,9 +386,10 @@ def main():
     torch.cuda.set_device(device)
     K, W = args.steps, max(3, args.warmup)
 
-    # FP32 batched (headline)
+    # batched form of FP32 storage class (headline: --headline, FP40 by default)
+    head = args.headline
     with ClockSampler(device) as clocks:
-        ctx, fp32 = time_form(wl, "fp32", "fused", K, W, device, profile=True, hop_variant=args.hop_variant,
+        ctx, fp32 = time_form(wl, head, "fused", K, W, device, profile=True, hop_variant=args.hop_variant,
                                  mode_group=args.mode_group)
     clk = clocks.summary()
     e2e_steps = max(3, min(K, 20))
@@ -390,6 +400,15 @@ def main():
     value = world * M * V * K / (ms / 1e3)
 
     forms = {}
+    other = "fp32" if head == "fp40" else "fp40"
+    c, r = time_form(wl, other, "fused", K, W, device, profile=True, hop_variant=args.hop_variant,
+                     mode_group=args.mode_group)
+    c.close()
+    del c
+    r_ms = max_over_ranks(r["ms"])
+    other_form = {"value": world * M * V * K / (r_ms / 1e3), "ms_per_step": r_ms / K,
+                  "hop_ms_per_launch": r["prof"]["hop"][0] / max(1, r["prof"]["hop"][1]), "N5": r["charges"]["N5"],
+                  "hop_variant": r["hop_variant"], "mode_group": r["mode_group"], "hop_variant_ms": r["hop_variant_ms"]}
     if not args.no_fp64:
         for form in ("plain", "fused"):
             c, r = time_form(wl, "fp64", form, max(2, K // 2), W, device, profile=True, hop_variant=args.hop_variant,
@@ -414,7 +433,7 @@ def main():
     # re-reads the first one's output from L2).
     hop_ms, hop_n = fp32["prof"]["hop"]
     per_launch_ms = hop_ms / max(1, hop_n)
-    elem = 8 * 8  # 2 colours x 4 spins x complex<float>
+    elem = 8 * 8 if head == "fp32" else 8 * 10  # 2 colours x 4 spins x (8 B [+ 2 extension bytes]) per complex
     n_mb = (M + 31) // 32
     grouped = 0 < fp32["mode_group"] < n_mb
     if grouped:
@@ -425,7 +444,7 @@ def main():
         unit = "one half step (one launch)"
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
-    kernel = HOP_KERNELS[fp32["hop_variant"]]
+    kernel = HOP_KERNELS[fp32["hop_variant"]] if head == "fp32" else "wilson_fp40_kernel<1,LinksF64<false>>"
     traffic = committed_traffic(kernel + (" grouped" if grouped else ""))
 
     if rank == 0:
@@ -433,27 +452,28 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 modes / f64 links", "data": "synthetic", "config": config,
+            "dtype": DTYPES[head], "data": "synthetic", "config": config,
             "e2e": {"value": world * M * V * e2e_steps / e2e_secs, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "path": "C ABI, host buffers: ovl_set_links + ovl_set_efield (pinned) + ovl_step(1) + ovl_charges"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "kernel": kernel + " (FP32 fused half step)",
+                         "traffic": traffic, "kernel": kernel + f" ({head} fused half step)",
                          "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms,
                          "unit_of_work": unit,
                          "peak_source": peak_kind},
             "gpu_launches": fp32["launches"],
             "kernel_ms": total_ms,
-            "forms": {"fp32_fused": {"value": value, "ms_per_step": ms / K, "N5": fp32["charges"]["N5"],
+            "forms": {f"{head}_fused": {"value": value, "ms_per_step": ms / K, "N5": fp32["charges"]["N5"],
                                      "hop_variant": fp32["hop_variant"], "hop_variant_ms": fp32["hop_variant_ms"],
                                      "mode_group": fp32["mode_group"]},
+                      f"{other}_fused": other_form,
                       **{f"fp64_{k}": v for k, v in forms.items()}},
             "clocks": clk,
         }
         if "plain" in forms:
-            line["fp32_vs_fp64_plain"] = value / forms["plain"]["value"]
+            line["headline_vs_fp64_plain"] = value / forms["plain"]["value"]
         if acc is not None:
-            line["accuracy_fp32_vs_fp64"] = acc
+            line["accuracy_vs_fp64"] = acc
         if cpu is not None:
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)

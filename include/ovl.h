@@ -46,7 +46,12 @@ typedef enum {
 
 typedef enum { OVL_FERMION_WILSON = 0, OVL_FERMION_OVERLAP = 1 } ovl_fermion;
 
-typedef enum { OVL_PREC_FP64 = 0, OVL_PREC_FP32 = 1 } ovl_precision;
+/* FP64: modes and arithmetic in FP64.  FP32: modes and hop arithmetic in FP32
+ * (FP64 links).  FP40: each real of the modes stored as the top 40 bits of its
+ * FP64 value (sign, exponent, 28 mantissa bits; relative rounding 2^-29), hop
+ * arithmetic, observables and links in FP64: 1.25x the bytes of FP32, and an
+ * axial-charge error against FP64 far below FP32's (Wilson, fused form). */
+typedef enum { OVL_PREC_FP64 = 0, OVL_PREC_FP32 = 1, OVL_PREC_FP40 = 2 } ovl_precision;
 
 /* OVL_FORM_PLAIN keeps the reference's two-phase half step (Update.cpp:6-27):
  * the operator writes a derivative buffer, then psi += dt * derivative.
@@ -113,8 +118,10 @@ typedef struct {
      * group of mode_group mode blocks (32 modes each), so that a group's fields,
      * written by the first half step, are still in L2 when the second reads
      * them (4 instead of 6 field passes through HBM per step; the same
-     * arithmetic, so the same results).  -1 = chosen by the autotuner with
-     * the hop variant; 0 = whole batch per half step; k > 0 = k blocks. */
+     * arithmetic, so the same results).  0 (default) = whole batch per half
+     * step; k > 0 = k blocks; -1 = chosen by the autotuner with the hop
+     * variant.  On B200 at 16^3 the launch overhead of the groups outweighs the
+     * L2 reuse, and the autotuner keeps the whole batch. */
     int mode_group;
 } ovl_params;
 

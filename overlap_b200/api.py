@@ -26,7 +26,7 @@ import numpy as np
 from . import _lib
 from .inputs import volume
 
-PRECISIONS = {"fp64": 0, "fp32": 1}
+PRECISIONS = {"fp64": 0, "fp32": 1, "fp40": 2}  # fp40: modes in 40 bits (top bits of FP64), FP64 arithmetic
 SIGN_METHODS = {"zolotarev": 0, "chebyshev": 1}
 FORMS = {"plain": 0, "fused": 1}
 FERMIONS = {"wilson": 0, "overlap": 1}
@@ -80,7 +80,7 @@ class Params:
     backreaction: float = 0.0        # coupled evolution: g^2 of the fermion force on E
     ritz_auto: bool = False          # overlap: GPU Ritz bounds before every application (no schedule set)
     ritz_seed: int = 0               # generator seed of the Ritz start vectors
-    mode_group: int = -1             # fused form: mode blocks per group (-1 autotune, 0 whole batch)
+    mode_group: int = 0              # fused form: mode blocks per group (0 whole batch, -1 autotune)
     sign_method: str = "zolotarev"  # or "chebyshev" (the FP32-capable polynomial form)
     cheb_degree: int = 96
     cheb_eps: float = 0.01

@@ -56,6 +56,8 @@ struct ovl_ctx {
     int hop_variant = -1;  // -1: autotune before the first step
     int mode_group = -1;   // mode blocks per group of the grouped fused step (0: whole batch)
     double *U_b = nullptr; // links at the half step (grouped fused step)
+    void *psi_lo = nullptr, *psimid_lo = nullptr;      // FP40 extension bytes of the mode fields
+    void *aux_src_lo = nullptr, *aux_dst_lo = nullptr; // and of the operator buffers (autotuner)
     float *U32_b = nullptr;
     // Chern-Simons number along the cooling path (ovl_ncs_update)
     double *u_old = nullptr, *u_mid = nullptr, *e_mid = nullptr;
@@ -142,6 +144,8 @@ int set_device(ovl_ctx *c) {
 }
 
 bool fp32(const ovl_ctx *c) { return c->p.precision == OVL_PREC_FP32; }
+// 40-bit storage: high words in the field, extension bytes in a parallel array
+bool fp40(const ovl_ctx *c) { return c->p.precision == OVL_PREC_FP40; }
 
 double amass(const ovl_params &p) { return 6.0 * p.r_wilson + 2.0 * p.m_fermion - 2.0 * p.m_dw; }
 
@@ -273,12 +277,26 @@ void refresh_links32(ovl_ctx *c) {
 // One leapfrog step's hop work in the fused form, group by group:
 // dst1 += dt D(src1) with links h1, then dst2 += dt D(src2) with links h2, for
 // each group of `group` mode blocks (group <= 0 or >= n_mb: the whole batch).
+// The extension bytes of a mode field or operator buffer in 40-bit storage.
+void *lo_of(const ovl_ctx *c, const void *field) {
+    if (field == c->psi) return c->psi_lo;
+    if (field == c->psimid) return c->psimid_lo;
+    if (field == c->aux_src) return c->aux_src_lo;
+    if (field == c->aux_dst) return c->aux_dst_lo;
+    return nullptr;
+}
+
 void grouped_pass(ovl_ctx *c, const ovl::HopConfig &h1, const ovl::HopConfig &h2, const void *src1, void *dst1,
                   const void *src2, void *dst2, int group) {
     const int G = (group <= 0 || group >= c->n_mb) ? c->n_mb : group;
     for (int g0 = 0; g0 < c->n_mb; g0 += G) {
         const int nmb = std::min(G, c->n_mb - g0);
-        if (fp32(c)) {
+        if (fp40(c)) {
+            ovl::launch_wilson40(h1, src1, lo_of(c, src1), dst1, lo_of(c, dst1), c->L, g0, nmb, amass(c->p), c->p.dt,
+                                 true, c->stream);
+            ovl::launch_wilson40(h2, src2, lo_of(c, src2), dst2, lo_of(c, dst2), c->L, g0, nmb, amass(c->p), c->p.dt,
+                                 true, c->stream);
+        } else if (fp32(c)) {
             ovl::launch_wilson_tuned<float>(h1, src1, dst1, c->L, g0, nmb, amass(c->p), c->p.dt, true, c->stream);
             ovl::launch_wilson_tuned<float>(h2, src2, dst2, c->L, g0, nmb, amass(c->p), c->p.dt, true, c->stream);
         } else {
@@ -301,6 +319,10 @@ int autotune_groups(ovl_ctx *c) {
     const size_t bytes = c->field_complex * c->elem_bytes;
     cudaMemsetAsync(c->aux_src, 0, bytes, c->stream);
     cudaMemsetAsync(c->aux_dst, 0, bytes, c->stream);
+    if (fp40(c)) {
+        cudaMemsetAsync(c->aux_src_lo, 0, c->field_complex * 2, c->stream);
+        cudaMemsetAsync(c->aux_dst_lo, 0, c->field_complex * 2, c->stream);
+    }
     const ovl::HopConfig h = hop_config(c);
     double best = 1e300;
     int pick = 0;
@@ -334,12 +356,19 @@ int autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
     ovl::HopConfig h = hop_config(c);
     double best = 1e300;
     int pick = 0;
-    for (int v = 0; v < ovl::kHopVariants; v++) {
+    const int nv = fp40(c) ? ovl::kFp40Variants : ovl::kHopVariants;
+    if (fp40(c)) cudaMemsetAsync(c->aux_dst_lo, 0, c->field_complex * 2, c->stream);
+    if (ms_out)
+        for (int v = 0; v < ovl::kHopVariants; v++) ms_out[v] = 0.0;
+    for (int v = 0; v < nv; v++) {
         h.variant = v;
         float total = 0.0f;
         for (int rep = 0; rep < 4; rep++) {
             cudaEventRecord(e0, c->stream);
-            if (fp32(c)) ovl::launch_wilson_tuned<float>(h, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+            if (fp40(c))
+                ovl::launch_wilson40(h, c->psi, c->psi_lo, c->aux_dst, c->aux_dst_lo, c->L, 0, c->n_mb, amass(c->p),
+                                     c->p.dt, true, c->stream);
+            else if (fp32(c)) ovl::launch_wilson_tuned<float>(h, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
             else ovl::launch_wilson_tuned<double>(h, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
             cudaEventRecord(e1, c->stream);
             cudaEventSynchronize(e1);
@@ -354,7 +383,7 @@ int autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->hop_variant = pick;
-    int rc = launched(c, 4 * ovl::kHopVariants, "autotune");
+    int rc = launched(c, 4 * nv, "autotune");
     if (!rc && c->mode_group < 0) rc = autotune_groups(c);
     return rc;
 }
@@ -370,7 +399,10 @@ int half_step(ovl_ctx *c, const void *src, void *dst) {
     const ovl::HopConfig hc = hop_config(c);
     if (c->p.form == OVL_FORM_FUSED) {
         ProfScope ps(c, OVL_PROF_HOP);
-        if (fp32(c)) ovl::launch_wilson_tuned<float>(hc, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        if (fp40(c))
+            ovl::launch_wilson40(hc, src, lo_of(c, src), dst, lo_of(c, dst), L, 0, c->n_mb, amass(c->p), c->p.dt, true,
+                                 c->stream);
+        else if (fp32(c)) ovl::launch_wilson_tuned<float>(hc, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
         else ovl::launch_wilson_tuned<double>(hc, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
         return launched(c, 1, "wilson (fused)");
     }
@@ -406,7 +438,10 @@ int run_currents(ovl_ctx *c) {
         return launched(c, 2, "overlap currents");
     }
     ProfScope ps(c, OVL_PROF_OBS);
-    if (fp32(c))
+    if (fp40(c))
+        ovl::launch_currents40(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->psi_lo, c->L, c->n_mb, c->p.n_modes,
+                               c->p.first_mode, c->p.r_wilson, c->partial, c->per_site, c->stream);
+    else if (fp32(c))
         ovl::launch_currents<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
                                     c->partial, c->per_site, c->stream);
     else
@@ -450,7 +485,7 @@ int ovl_params_init(ovl_params *p) {
     p->backreaction = 0.0;
     p->ritz_auto = 0;
     p->ritz_seed = 0;
-    p->mode_group = -1;
+    p->mode_group = 0;
     p->sign_method = OVL_SIGN_ZOLOTAREV;
     p->cheb_degree = 96;
     p->cheb_eps = 0.01;
@@ -479,7 +514,10 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     if (p->backreaction != 0.0 && p->fermion != OVL_FERMION_WILSON)
         return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: fermion back-reaction is built for Wilson fermions only");
     if (!std::isfinite(p->backreaction)) return fail(nullptr, OVL_E_ARG, "ovl_create: backreaction must be finite");
-    if (p->precision != OVL_PREC_FP64 && p->precision != OVL_PREC_FP32) return fail(nullptr, OVL_E_ARG, "ovl_create: bad precision");
+    if (p->precision != OVL_PREC_FP64 && p->precision != OVL_PREC_FP32 && p->precision != OVL_PREC_FP40)
+        return fail(nullptr, OVL_E_ARG, "ovl_create: bad precision");
+    if (p->precision == OVL_PREC_FP40 && (p->fermion != OVL_FERMION_WILSON || p->form != OVL_FORM_FUSED))
+        return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: FP40 storage is built for the fused Wilson form");
     if (p->form != OVL_FORM_PLAIN && p->form != OVL_FORM_FUSED) return fail(nullptr, OVL_E_ARG, "ovl_create: bad form");
     if (p->n_modes <= 0 || p->first_mode < 0) return fail(nullptr, OVL_E_ARG, "ovl_create: n_modes=%d first_mode=%d", p->n_modes, p->first_mode);
     if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return fail(nullptr, OVL_E_ARG, "ovl_create: dt must be positive");
@@ -494,7 +532,7 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     c->p = *p;
     c->L = Lattice{p->N[0], p->N[1], p->N[2], (int)V};
     c->n_mb = (p->n_modes + ovl::kModeBlock - 1) / ovl::kModeBlock;
-    c->elem_bytes = p->precision == OVL_PREC_FP32 ? 8 : 16;
+    c->elem_bytes = p->precision == OVL_PREC_FP64 ? 16 : 8;  // FP40: the 32-bit high words
     c->field_complex = (size_t)c->n_mb * V * ovl::kComp * ovl::kModeBlock;
     int rc = OVL_OK;
     auto bail = [&](int code) { g_err = c->err; ovl_destroy(c); return code; };
@@ -515,6 +553,13 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
         }
         return OVL_OK;
     };
+    if (p->precision == OVL_PREC_FP40) {
+        const size_t lo_bytes = c->field_complex * 2;
+        if ((rc = alloc(&c->psi_lo, lo_bytes, "Psi extension bytes")) || (rc = alloc(&c->psimid_lo, lo_bytes, "PsiMid extension bytes")) ||
+            (rc = alloc(&c->aux_src_lo, lo_bytes, "operator input extension")) ||
+            (rc = alloc(&c->aux_dst_lo, lo_bytes, "operator output extension")))
+            return bail(rc);
+    }
     if ((rc = alloc(&c->psi, field_bytes, "Psi")) || (rc = alloc(&c->psimid, field_bytes, "PsiMid")) ||
         (rc = alloc((void **)&c->U, sizeof(double) * 12 * V, "links")) ||
         (rc = alloc((void **)&c->E, sizeof(double) * 9 * V, "efield")))
@@ -543,8 +588,7 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     c->hop_variant = p->hop_variant;
     // grouping applies to the fused Wilson form; fixed when the variant is fixed
     if (p->form != OVL_FORM_FUSED || p->fermion != OVL_FERMION_WILSON) c->mode_group = 0;
-    else if (p->mode_group >= 0) c->mode_group = p->mode_group;
-    else c->mode_group = p->hop_variant >= 0 ? 0 : -1;
+    else c->mode_group = p->mode_group;
     if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method == OVL_SIGN_CHEBYSHEV) {
         ovl::ChebyshevWork &w = c->cw;
         if ((rc = alloc(&w.b0, field_bytes, "Clenshaw b")) || (rc = alloc(&w.b1, field_bytes, "Clenshaw b")) ||
@@ -592,7 +636,8 @@ int ovl_destroy(ovl_ctx *c) {
     void *bufs[] = {c->psi, c->psimid, c->U, c->E, c->deriv, c->per_site, c->partial, c->dev_small, c->dev_int,
                     c->aux_src, c->aux_dst, c->ow.r, c->ow.q, c->ow.t, c->ow.x, c->ow.p, c->ow.part, c->ow.rnorm,
                     c->ow.alpha, c->ow.active, c->ow.dz, c->u_old, c->u_mid, c->e_mid, c->u1,
-                    c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w, c->U32, c->u1_32, c->U_b, c->U32_b};
+                    c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w, c->U32, c->u1_32, c->U_b, c->U32_b,
+                    c->psi_lo, c->psimid_lo, c->aux_src_lo, c->aux_dst_lo};
     if (c->ow.host_count) cudaFreeHost(c->ow.host_count);
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -707,11 +752,11 @@ static int transfer_modes(ovl_ctx *c, int first, int count, const double *hpsi, 
                 cudaError_t e = cudaMemcpyAsync(stage, hin + off, per_mode * 8 * n, cudaMemcpyHostToDevice, c->stream);
                 if (e != cudaSuccess) { status = cuda_fail(c, e, "mode upload"); break; }
                 if (fp32(c)) ovl::launch_ref_to_blocks<float>(stage, field, c->L, m, n, c->stream);
-                else ovl::launch_ref_to_blocks<double>(stage, field, c->L, m, n, c->stream);
+                else ovl::launch_ref_to_blocks<double>(stage, field, c->L, m, n, c->stream, lo_of(c, field));
                 status = launched(c, 1, "ref_to_blocks");
             } else {
                 if (fp32(c)) ovl::launch_blocks_to_ref<float>(field, stage, c->L, m, n, c->stream);
-                else ovl::launch_blocks_to_ref<double>(field, stage, c->L, m, n, c->stream);
+                else ovl::launch_blocks_to_ref<double>(field, stage, c->L, m, n, c->stream, lo_of(c, field));
                 status = launched(c, 1, "blocks_to_ref");
                 if (status) break;
                 cudaError_t e = cudaMemcpyAsync(hout + off, stage, per_mode * 8 * n, cudaMemcpyDeviceToHost, c->stream);
@@ -742,9 +787,9 @@ int ovl_set_free_fermions(ovl_ctx *c, int *n_bad) {
     if (fp32(c))
         ovl::launch_free_fermions<float>(c->psi, c->psimid, c->L, c->p.n_modes, c->n_mb, c->p.first_mode, c->p.r_wilson,
                                          c->p.m_fermion, c->p.dt, c->dev_int, c->stream);
-    else
+    else  // FP64, or FP40 (the extension arrays set)
         ovl::launch_free_fermions<double>(c->psi, c->psimid, c->L, c->p.n_modes, c->n_mb, c->p.first_mode, c->p.r_wilson,
-                                          c->p.m_fermion, c->p.dt, c->dev_int, c->stream);
+                                          c->p.m_fermion, c->p.dt, c->dev_int, c->stream, c->psi_lo, c->psimid_lo);
     if ((rc = launched(c, 2, "free fermions"))) return rc;
     int bad = 0;
     OVL_CUDA(c, cudaMemcpyAsync(&bad, c->dev_int, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -768,7 +813,10 @@ int coupled_efield(ovl_ctx *c) {
         {
             ProfScope ps(c, OVL_PROF_OBS);
             const double coef = c->p.dt * c->p.backreaction;
-            if (fp32(c))
+            if (fp40(c))
+                ovl::launch_color_force40(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->psi_lo, c->L, c->n_mb,
+                                          c->p.n_modes, c->p.first_mode, c->partial, nullptr, c->E, coef, c->stream);
+            else if (fp32(c))
                 ovl::launch_color_force<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
                                                c->p.first_mode, c->partial, nullptr, c->E, coef, c->stream);
             else
@@ -913,7 +961,10 @@ int ovl_charges(ovl_ctx *c, double out[4]) {
         if ((rc = launched(c, 1, "site sums"))) return rc;
     } else {
         ProfScope ps(c, OVL_PROF_OBS);
-        if (fp32(c))
+        if (fp40(c))
+            ovl::launch_charges40(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->psi_lo, c->L, c->n_mb, c->p.n_modes,
+                                  c->p.first_mode, c->p.r_wilson, c->partial, c->dev_small, c->stream);
+        else if (fp32(c))
             ovl::launch_charges<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
                                        c->partial, c->dev_small, c->stream);
         else
@@ -1006,7 +1057,10 @@ int ovl_color_force(ovl_ctx *c, double *out) {
         cudaGetLastError();
         return fail(c, OVL_E_OOM, "ovl_color_force: output buffer");
     }
-    if (fp32(c))
+    if (fp40(c))
+        ovl::launch_color_force40(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->psi_lo, c->L, c->n_mb, c->p.n_modes,
+                                  c->p.first_mode, c->partial, dev, nullptr, 0.0, c->stream);
+    else if (fp32(c))
         ovl::launch_color_force<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
                                        c->p.first_mode, c->partial, dev, nullptr, 0.0, c->stream);
     else
@@ -1027,7 +1081,15 @@ int ovl_fermion_energy(ovl_ctx *c, double *out) {
     int rc = set_device(c);
     if (rc) return rc;
     const double *u1 = c->u1_on ? c->u1 : nullptr;
-    if (fp32(c)) {
+    if (fp40(c)) {
+        ovl::HopConfig h;
+        h.U = c->U;
+        h.u1 = u1;
+        ovl::launch_wilson40(h, c->psi, c->psi_lo, c->aux_dst, c->aux_dst_lo, c->L, 0, c->n_mb, amass(c->p), 0.0, false,
+                             c->stream);
+        ovl::launch_fermion_energy40(c->psi, c->psi_lo, c->aux_dst, c->aux_dst_lo, c->L, c->n_mb, c->p.n_modes,
+                                     c->p.first_mode, c->partial, c->dev_small, c->stream);
+    } else if (fp32(c)) {
         ovl::launch_wilson<float>(c->U, u1, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), 0.0, false, c->stream);
         ovl::launch_fermion_energy<float>(c->psi, c->aux_dst, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->partial,
                                           c->dev_small, c->stream);
@@ -1157,17 +1219,28 @@ int ovl_apply(ovl_ctx *c, int count, const double *phi, double *out) {
     cudaMemsetAsync(c->aux_src, 0, c->field_complex * c->elem_bytes, c->stream);
     if (cudaMemcpyAsync(stage, phi, per_mode * 8 * count, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
         return done(fail(c, OVL_E_CUDA, "ovl_apply: upload"));
-    if (fp32(c)) ovl::launch_ref_to_blocks<float>(stage, c->aux_src, c->L, 0, count, c->stream);
+    if (fp40(c)) {
+        cudaMemsetAsync(c->aux_src_lo, 0, c->field_complex * 2, c->stream);
+        ovl::launch_ref_to_blocks<double>(stage, c->aux_src, c->L, 0, count, c->stream, c->aux_src_lo);
+    } else if (fp32(c)) ovl::launch_ref_to_blocks<float>(stage, c->aux_src, c->L, 0, count, c->stream);
     else ovl::launch_ref_to_blocks<double>(stage, c->aux_src, c->L, 0, count, c->stream);
     if ((rc = launched(c, 1, "ref_to_blocks"))) return done(rc);
     if (overlap(c)) {
         if ((rc = run_overlap(c, c->aux_src, c->aux_dst, n_mb, count, false, false))) return done(rc);
+    } else if (fp40(c)) {
+        ovl::HopConfig h;
+        h.U = c->U;
+        h.u1 = c->u1_on ? c->u1 : nullptr;
+        ovl::launch_wilson40(h, c->aux_src, c->aux_src_lo, c->aux_dst, c->aux_dst_lo, c->L, 0, n_mb, amass(c->p), 0.0,
+                             false, c->stream);
+        if ((rc = launched(c, 1, "wilson operator"))) return done(rc);
     } else {
         if (fp32(c)) ovl::launch_wilson<float>(c->U, c->u1_on ? c->u1 : nullptr, c->aux_src, c->aux_dst, c->L, 0, n_mb, amass(c->p), 0.0, false, c->stream);
         else ovl::launch_wilson<double>(c->U, c->u1_on ? c->u1 : nullptr, c->aux_src, c->aux_dst, c->L, 0, n_mb, amass(c->p), 0.0, false, c->stream);
         if ((rc = launched(c, 1, "wilson operator"))) return done(rc);
     }
-    if (fp32(c)) ovl::launch_blocks_to_ref<float>(c->aux_dst, stage, c->L, 0, count, c->stream);
+    if (fp40(c)) ovl::launch_blocks_to_ref<double>(c->aux_dst, stage, c->L, 0, count, c->stream, c->aux_dst_lo);
+    else if (fp32(c)) ovl::launch_blocks_to_ref<float>(c->aux_dst, stage, c->L, 0, count, c->stream);
     else ovl::launch_blocks_to_ref<double>(c->aux_dst, stage, c->L, 0, count, c->stream);
     if ((rc = launched(c, 1, "blocks_to_ref"))) return done(rc);
     if (cudaMemcpyAsync(out, stage, per_mode * 8 * count, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)

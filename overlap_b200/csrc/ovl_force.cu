@@ -16,31 +16,31 @@
 // the reference makes d theta / dt = -E, so dE/dt = dH/dtheta conserves
 // H_gauge + g^2 H_F.
 #include "ovl_device.cuh"
+#include "ovl_fp40.cuh"
 #include "ovl_internal.h"
 
 namespace ovl {
 
 constexpr int kForceThreadsY = kSitesPerCta;
 
-template <typename T>
-__device__ __forceinline__ void force_load(const cpx<T> *__restrict__ f, int V, int mb, int site, int lane,
+// One site's spinor of the lane's mode as complex doubles, from a field view
+// (SrcPlain<T> or Src40, ovl_fp40.cuh).
+template <class SRC>
+__device__ __forceinline__ void force_load(const SRC &f, int V, int mb, int site, int lane,
                                            cpx<double> (&s)[kColours][kSpin]) {
-    const cpx<T> *p = f + field_index(V, mb, site, 0, lane);
+    const size_t base = field_index(V, mb, site, 0, lane);
 #pragma unroll
     for (int c = 0; c < kColours; c++)
 #pragma unroll
-        for (int a = 0; a < kSpin; a++) {
-            const cpx<T> v = ld(p + (c * kSpin + a) * kModeBlock);
-            s[c][a] = mk<double>((double)v.re, (double)v.im);
-        }
+        for (int a = 0; a < kSpin; a++) s[c][a] = f(base + (c * kSpin + a) * kModeBlock);
 }
 
 // partial[(g V + site) kForcePerSite + 8 mu + 2 (2 i + j) + {re, im}] = C_ij of
 // mode-block group g (a warp is one site, its lanes the 32 modes of a block).
-template <typename T>
+template <class SRC>
 __global__ void __launch_bounds__(kModeBlock *kForceThreadsY)
-    color_force_modes_kernel(const cpx<T> *__restrict__ psi, Lattice L, int n_mb, int n_modes, int first_mode,
-                             int groups, double *__restrict__ partial) {
+    color_force_modes_kernel(SRC psi, Lattice L, int n_mb, int n_modes, int first_mode, int groups,
+                             double *__restrict__ partial) {
     constexpr mono G0 = kGamma0;
     constexpr mono G0M[3] = {mono_mul(kGamma0, kGammaX), mono_mul(kGamma0, kGammaY), mono_mul(kGamma0, kGammaZ)};
     const int lane = threadIdx.x;
@@ -140,18 +140,32 @@ int force_groups(int n_mb) { return n_mb < 16 ? n_mb : 16; }
 
 size_t force_partial_doubles(const Lattice &L, int n_mb) { return (size_t)force_groups(n_mb) * L.V * kForcePerSite; }
 
-template <typename T>
-void launch_color_force(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
-                        int first_mode, double *partial, double *out, double *E, double coef, cudaStream_t stream) {
+template <class SRC>
+static void color_force_from(const SRC &src, const double *U, const double *u1, const Lattice &L, int n_mb,
+                             int n_modes, int first_mode, double *partial, double *out, double *E, double coef,
+                             cudaStream_t stream) {
     const int groups = force_groups(n_mb);
     dim3 block(kModeBlock, kForceThreadsY);
     dim3 grid((L.V + kForceThreadsY - 1) / kForceThreadsY, groups);
-    color_force_modes_kernel<T><<<grid, block, 0, stream>>>(reinterpret_cast<const cpx<T> *>(psi), L, n_mb, n_modes,
-                                                            first_mode, groups, partial);
+    color_force_modes_kernel<SRC><<<grid, block, 0, stream>>>(src, L, n_mb, n_modes, first_mode, groups, partial);
     const int n = 3 * L.V;
     color_force_finish_kernel<<<(n + 127) / 128, 128, 0, stream>>>(partial, groups, U,
                                                                    reinterpret_cast<const double2 *>(u1), L, out, E,
                                                                    coef);
+}
+
+template <typename T>
+void launch_color_force(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                        int first_mode, double *partial, double *out, double *E, double coef, cudaStream_t stream) {
+    color_force_from(SrcPlain<T>{reinterpret_cast<const cpx<T> *>(psi)}, U, u1, L, n_mb, n_modes, first_mode, partial,
+                     out, E, coef, stream);
+}
+
+void launch_color_force40(const double *U, const double *u1, const void *hi, const void *lo, const Lattice &L, int n_mb,
+                          int n_modes, int first_mode, double *partial, double *out, double *E, double coef,
+                          cudaStream_t stream) {
+    color_force_from(Src40{reinterpret_cast<const uint2 *>(hi), reinterpret_cast<const unsigned char *>(lo)}, U, u1, L, n_mb,
+                     n_modes, first_mode, partial, out, E, coef, stream);
 }
 
 template void launch_color_force<float>(const double *, const double *, const void *, const Lattice &, int, int, int,
@@ -167,18 +181,17 @@ template void launch_color_force<double>(const double *, const double *, const v
 constexpr int kEnergyThreads = 256;
 constexpr int kEnergyBlocks = 1024;
 
-template <typename T>
+template <class SRC>
 __global__ void __launch_bounds__(kEnergyThreads)
-    energy_partial_kernel(const cpx<T> *__restrict__ psi, const cpx<T> *__restrict__ dpsi, size_t n, int V,
-                          int n_modes, int first_mode, double *__restrict__ partial) {
+    energy_partial_kernel(SRC psi, SRC dpsi, size_t n, int V, int n_modes, int first_mode, double *__restrict__ partial) {
     __shared__ double sh[kEnergyThreads];
     const size_t per_mb = (size_t)V * kComp * kModeBlock;
     double acc = 0.0;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         const int mode = (int)(e / per_mb) * kModeBlock + (int)(e % kModeBlock);
         if (mode >= n_modes) continue;
-        const cpx<T> a = ld(psi + e), d = ld(dpsi + e);
-        const double im = (double)a.re * (double)d.im - (double)a.im * (double)d.re;  // Im conj(a) d
+        const cpx<double> a = psi(e), d = dpsi(e);
+        const double im = a.re * d.im - a.im * d.re;  // Im conj(a) d
         acc += (((first_mode + mode) & 1) == 0) ? -im : im;
     }
     sh[threadIdx.x] = acc;
@@ -206,16 +219,28 @@ __global__ void __launch_bounds__(kEnergyThreads)
 
 size_t energy_partial_doubles() { return kEnergyBlocks; }
 
-template <typename T>
-void launch_fermion_energy(const void *psi, const void *dpsi, const Lattice &L, int n_mb, int n_modes, int first_mode,
-                           double *partial, double *out, cudaStream_t stream) {
+template <class SRC>
+static void energy_from(const SRC &psi, const SRC &dpsi, const Lattice &L, int n_mb, int n_modes, int first_mode,
+                        double *partial, double *out, cudaStream_t stream) {
     const size_t n = (size_t)n_mb * L.V * kComp * kModeBlock;
     const size_t want = (n + kEnergyThreads - 1) / kEnergyThreads;
     const int blocks = (int)(want < (size_t)kEnergyBlocks ? want : (size_t)kEnergyBlocks);
-    energy_partial_kernel<T><<<blocks, kEnergyThreads, 0, stream>>>(reinterpret_cast<const cpx<T> *>(psi),
-                                                                    reinterpret_cast<const cpx<T> *>(dpsi), n, L.V,
-                                                                    n_modes, first_mode, partial);
+    energy_partial_kernel<SRC><<<blocks, kEnergyThreads, 0, stream>>>(psi, dpsi, n, L.V, n_modes, first_mode, partial);
     energy_finish_kernel<<<1, kEnergyThreads, 0, stream>>>(partial, blocks, 1.0 / (2.0 * L.V), out);
+}
+
+template <typename T>
+void launch_fermion_energy(const void *psi, const void *dpsi, const Lattice &L, int n_mb, int n_modes, int first_mode,
+                           double *partial, double *out, cudaStream_t stream) {
+    energy_from(SrcPlain<T>{reinterpret_cast<const cpx<T> *>(psi)}, SrcPlain<T>{reinterpret_cast<const cpx<T> *>(dpsi)},
+                L, n_mb, n_modes, first_mode, partial, out, stream);
+}
+
+void launch_fermion_energy40(const void *hi, const void *lo, const void *dhi, const void *dlo, const Lattice &L,
+                             int n_mb, int n_modes, int first_mode, double *partial, double *out, cudaStream_t stream) {
+    energy_from(Src40{reinterpret_cast<const uint2 *>(hi), reinterpret_cast<const unsigned char *>(lo)},
+                Src40{reinterpret_cast<const uint2 *>(dhi), reinterpret_cast<const unsigned char *>(dlo)}, L, n_mb, n_modes,
+                first_mode, partial, out, stream);
 }
 
 template void launch_fermion_energy<float>(const void *, const void *, const Lattice &, int, int, int, double *,

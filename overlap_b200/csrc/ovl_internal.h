@@ -31,6 +31,14 @@ template <typename T>
 void launch_wilson_tuned(const HopConfig &hc, const void *src, void *dst, const Lattice &L, int mb_first, int n_mb,
                          double amass, double dt, bool accumulate, cudaStream_t stream);
 void launch_links_to_f32(const double *U, float *U32, size_t n, cudaStream_t stream);
+// Half step on 40-bit storage (uint2 high words + packed extension bytes,
+// ovl_fp40.cuh), FP64 arithmetic and FP64 links (hc.U, hc.u1); accumulate:
+// dst += dt D src, else dst (a buffer of n_mb blocks) = D src.  hc.variant:
+// 0 = 128 registers (2 CTAs per SM), 1 = 80 registers (3 CTAs per SM).
+constexpr int kFp40Variants = 2;
+void launch_wilson40(const HopConfig &hc, const void *src, const void *src_lo, void *dst, void *dst_lo,
+                     const Lattice &L, int mb_first, int n_mb, double amass, double dt, bool accumulate,
+                     cudaStream_t stream);
 
 template <typename T>
 void launch_axpy(void *dst, const void *deriv, size_t n_complex, double dt, int sm_count, cudaStream_t stream);
@@ -92,6 +100,17 @@ void launch_ritz_random_start(void *work, uint64_t seed, uint64_t call, cudaStre
 cudaError_t ritz_run(void *work, const double *U, const double *u1, const Lattice &L, double amass, int max_iter,
                      int nrestart, double delitr, double out[2], int iters[2], cudaStream_t stream,
                      uint64_t *launches);
+// The same observables on 40-bit storage (hi words + extension bytes).
+void launch_currents40(const double *U, const double *u1, const void *hi, const void *lo, const Lattice &L, int n_mb,
+                       int n_modes, int first_mode, double r_wilson, double *partial, double *per_site,
+                       cudaStream_t stream);
+void launch_charges40(const double *U, const double *u1, const void *hi, const void *lo, const Lattice &L, int n_mb,
+                      int n_modes, int first_mode, double r_wilson, double *partial, double *out4, cudaStream_t stream);
+void launch_color_force40(const double *U, const double *u1, const void *hi, const void *lo, const Lattice &L, int n_mb,
+                          int n_modes, int first_mode, double *partial, double *out, double *E, double coef,
+                          cudaStream_t stream);
+void launch_fermion_energy40(const void *hi, const void *lo, const void *dhi, const void *dlo, const Lattice &L,
+                             int n_mb, int n_modes, int first_mode, double *partial, double *out, cudaStream_t stream);
 // Lattice sums N_V, N_5, PS, WA straight from the modes (no per-site maps).
 size_t charges_partial_doubles(const Lattice &L, int n_mb);
 template <typename T>
@@ -101,9 +120,11 @@ void launch_charges(const double *U, const double *u1, const void *psi, const La
 // Layout conversion between the reference layout (double, [mode][site][comp])
 // and the mode-block layout of precision T.  Modes [m0, m0+count).
 template <typename T>
-void launch_ref_to_blocks(const double *ref, void *blocks, const Lattice &L, int m0, int count, cudaStream_t stream);
+void launch_ref_to_blocks(const double *ref, void *blocks, const Lattice &L, int m0, int count, cudaStream_t stream,
+                          void *lo = nullptr);
 template <typename T>
-void launch_blocks_to_ref(const void *blocks, double *ref, const Lattice &L, int m0, int count, cudaStream_t stream);
+void launch_blocks_to_ref(const void *blocks, double *ref, const Lattice &L, int m0, int count, cudaStream_t stream,
+                          const void *lo = nullptr);
 
 // ------------------------------------------------------------------ overlap --
 // Zolotarev coefficients on the host (ovl_zolotarev.cpp); returns the relative
@@ -158,6 +179,7 @@ void chebyshev_apply(ChebyshevWork &w, const double *U, const double *u1, const 
 // Free Wilson plane waves for local modes [0, n_modes) (global index first_mode + m).
 template <typename T>
 void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes, int n_mb, int first_mode,
-                          double r_wilson, double m_fermion, double dt, int *bad, cudaStream_t stream);
+                          double r_wilson, double m_fermion, double dt, int *bad, cudaStream_t stream,
+                          void *lo_psi = nullptr, void *lo_mid = nullptr);
 
 }  // namespace ovl

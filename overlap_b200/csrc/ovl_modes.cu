@@ -3,6 +3,7 @@
 // per-mode arrays and the mode-block layout, and free plane-wave modes.
 
 #include "ovl_device.cuh"
+#include "ovl_fp40.cuh"
 #include "ovl_internal.h"
 
 namespace ovl {
@@ -32,6 +33,18 @@ __device__ __forceinline__ void load_site(const cpx<T> *__restrict__ f, int V, i
         for (int a = 0; a < kSpin; a++) s[c][a] = ld(p + (c * kSpin + a) * kModeBlock);
 }
 
+// One site's spinor of the lane's mode as complex doubles, from a field view
+// (SrcPlain<T> or Src40, ovl_fp40.cuh).
+template <class SRC>
+__device__ __forceinline__ void load_site_d(const SRC &f, int V, int mb, int site, int lane,
+                                            cpx<double> (&s)[kColours][kSpin]) {
+    const size_t base = field_index(V, mb, site, 0, lane);
+#pragma unroll
+    for (int c = 0; c < kColours; c++)
+#pragma unroll
+        for (int a = 0; a < kSpin; a++) s[c][a] = f(base + (c * kSpin + a) * kModeBlock);
+}
+
 // sum over colours of psi^+ G h, in double
 template <typename T>
 __device__ __forceinline__ cpx<double> colour_bilinear(const mono &G, const cpx<T> (&f)[kColours][kSpin],
@@ -47,10 +60,10 @@ __device__ __forceinline__ cpx<double> colour_bilinear(const mono &G, const cpx<
     return t;
 }
 
-template <typename T>
+template <class SRC>
 __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
-    currents_kernel(const double *__restrict__ U, const double2 *__restrict__ u1, const cpx<T> *__restrict__ psi,
-                    Lattice L, int n_mb, int n_modes, int first_mode, int groups, double r, double *__restrict__ partial) {
+    currents_kernel(const double *__restrict__ U, const double2 *__restrict__ u1, SRC psi, Lattice L, int n_mb,
+                    int n_modes, int first_mode, int groups, double r, double *__restrict__ partial) {
     constexpr mono G1 = {{0, 1, 2, 3}, {0, 0, 0, 0}};
     constexpr mono G5 = kGamma5;
     constexpr mono G05 = mono_mul(kGamma0, kGamma5);
@@ -82,13 +95,9 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
     for (int mb = g; mb < n_mb; mb += groups) {
         const int mode = mb * kModeBlock + lane;
         const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
-        cpx<T> f[kColours][kSpin];
-        load_site(psi, V, mb, site, lane, f);
-        cpx<double> fd[kColours][kSpin];
-#pragma unroll
-        for (int c = 0; c < kColours; c++)
-#pragma unroll
-            for (int a = 0; a < kSpin; a++) fd[c][a] = mk<double>((double)f[c][a].re, (double)f[c][a].im);
+        cpx<double> f[kColours][kSpin];
+        load_site_d(psi, V, mb, site, lane, f);
+        const cpx<double>(&fd)[kColours][kSpin] = f;
         double v[kCurrentsPerSite];
 #pragma unroll
         for (int k = 0; k < kCurrentsPerSite; k++) v[k] = 0.0;
@@ -99,17 +108,14 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
         double wa = -6.0 * r * b05.im;   // -6 Re(-i r x)
 #pragma unroll
         for (int mu = 0; mu < 3; mu++) {
-            cpx<T> h[kColours][kSpin];
+            cpx<double> h[kColours][kSpin];
             cpx<double> chi[kColours][kSpin];
             // forward: chi = U_mu(x) psi(x+mu)
-            load_site(psi, V, mb, nb[mu][0], lane, h);
+            load_site_d(psi, V, mb, nb[mu][0], lane, h);
             {
                 const cmat2<double> M = dressed_link<double>(U, u1, site, mu, L.N0 * L.N1);
 #pragma unroll
-                for (int a = 0; a < kSpin; a++) {
-                    cpx<double> h0 = mk<double>(h[0][a].re, h[0][a].im), h1 = mk<double>(h[1][a].re, h[1][a].im);
-                    mul(M, h0, h1, chi[0][a], chi[1][a]);
-                }
+                for (int a = 0; a < kSpin; a++) mul(M, h[0][a], h[1][a], chi[0][a], chi[1][a]);
             }
             v[1 + mu] = colour_bilinear(GV[mu], f, chi).re;
             v[5 + mu] = colour_bilinear(GA[mu], f, chi).re;
@@ -118,14 +124,11 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
             v[13 + mu] = aw;
             wa += aw;
             // backward: chib = U_mu(x-mu)^+ psi(x-mu)
-            load_site(psi, V, mb, nb[mu][1], lane, h);
+            load_site_d(psi, V, mb, nb[mu][1], lane, h);
             {
                 const cmat2<double> M = dressed_link<double>(U, u1, nb[mu][1], mu, L.N0 * L.N1);
 #pragma unroll
-                for (int a = 0; a < kSpin; a++) {
-                    cpx<double> h0 = mk<double>(h[0][a].re, h[0][a].im), h1 = mk<double>(h[1][a].re, h[1][a].im);
-                    mul_dag(M, h0, h1, chi[0][a], chi[1][a]);
-                }
+                for (int a = 0; a < kSpin; a++) mul_dag(M, h[0][a], h[1][a], chi[0][a], chi[1][a]);
             }
             wa += r * colour_bilinear(G05, f, chi).im;
         }
@@ -168,17 +171,30 @@ size_t currents_partial_doubles(const Lattice &L, int n_mb) {
     return (size_t)currents_groups(n_mb) * L.V * kCurrentsPerSite;
 }
 
-template <typename T>
-void launch_currents(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
-                     int first_mode, double r_wilson, double *partial, double *per_site, cudaStream_t stream) {
+template <class SRC>
+static void currents_from(const SRC &src, const double *U, const double *u1, const Lattice &L, int n_mb, int n_modes,
+                          int first_mode, double r_wilson, double *partial, double *per_site, cudaStream_t stream) {
     const int groups = currents_groups(n_mb);
     dim3 block(kModeBlock, kCurrentsThreadsY);
     dim3 grid((L.V + kCurrentsThreadsY - 1) / kCurrentsThreadsY, groups);
-    currents_kernel<T><<<grid, block, 0, stream>>>(U, reinterpret_cast<const double2 *>(u1),
-                                                   reinterpret_cast<const cpx<T> *>(psi), L, n_mb, n_modes, first_mode,
-                                                   groups, r_wilson, partial);
+    currents_kernel<SRC><<<grid, block, 0, stream>>>(U, reinterpret_cast<const double2 *>(u1), src, L, n_mb, n_modes,
+                                                     first_mode, groups, r_wilson, partial);
     const int n = L.V * kCurrentsPerSite;
     currents_finish_kernel<<<(n + 255) / 256, 256, 0, stream>>>(partial, groups, L.V, 1.0 / (2.0 * L.V), per_site);
+}
+
+template <typename T>
+void launch_currents(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                     int first_mode, double r_wilson, double *partial, double *per_site, cudaStream_t stream) {
+    currents_from(SrcPlain<T>{reinterpret_cast<const cpx<T> *>(psi)}, U, u1, L, n_mb, n_modes, first_mode, r_wilson,
+                  partial, per_site, stream);
+}
+
+void launch_currents40(const double *U, const double *u1, const void *hi, const void *lo, const Lattice &L, int n_mb,
+                       int n_modes, int first_mode, double r_wilson, double *partial, double *per_site,
+                       cudaStream_t stream) {
+    currents_from(Src40{reinterpret_cast<const uint2 *>(hi), reinterpret_cast<const unsigned char *>(lo)}, U, u1, L, n_mb,
+                  n_modes, first_mode, r_wilson, partial, per_site, stream);
 }
 
 // ----------------------------------------------------------------- charges --
@@ -194,10 +210,10 @@ void launch_currents(const double *U, const double *u1, const void *psi, const L
 // added in a fixed order.
 constexpr int kChargeVals = 4;
 
-template <typename T>
+template <class SRC>
 __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
-    charges_kernel(const double *__restrict__ U, const double2 *__restrict__ u1, const cpx<T> *__restrict__ psi,
-                   Lattice L, int n_mb, int n_modes, int first_mode, int groups, double r, double *__restrict__ partial) {
+    charges_kernel(const double *__restrict__ U, const double2 *__restrict__ u1, SRC psi, Lattice L, int n_mb,
+                   int n_modes, int first_mode, int groups, double r, double *__restrict__ partial) {
     __shared__ double sh[kCurrentsThreadsY][kChargeVals];
     const int lane = threadIdx.x;
     const int site = blockIdx.x * kCurrentsThreadsY + threadIdx.y;
@@ -219,13 +235,8 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
             const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
             // the bilinears in double for every mode precision: each of the
             // ~1e8 terms of a lattice sum then carries a 1e-16 rounding error
-            cpx<T> ft[kColours][kSpin];
-            load_site(psi, L.V, mb, site, lane, ft);
             cpx<double> f[kColours][kSpin];
-#pragma unroll
-            for (int c = 0; c < kColours; c++)
-#pragma unroll
-                for (int a = 0; a < kSpin; a++) f[c][a] = mk<double>((double)ft[c][a].re, (double)ft[c][a].im);
+            load_site_d(psi, L.V, mb, site, lane, f);
             double nv = 0.0;
             cpx<double> zz = mk<double>(0.0, 0.0);
 #pragma unroll
@@ -237,13 +248,11 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
             double hop = 0.0;
 #pragma unroll
             for (int mu = 0; mu < 3; mu++) {
-                cpx<T> ht[kColours][kSpin];
-                load_site(psi, L.V, mb, nb[mu], lane, ht);
+                cpx<double> ht[kColours][kSpin];
+                load_site_d(psi, L.V, mb, nb[mu], lane, ht);
                 cpx<double> chi[kColours][kSpin];
 #pragma unroll
-                for (int a = 0; a < kSpin; a++)
-                    mul(M[mu], mk<double>(ht[0][a].re, ht[0][a].im), mk<double>(ht[1][a].re, ht[1][a].im), chi[0][a],
-                        chi[1][a]);
+                for (int a = 0; a < kSpin; a++) mul(M[mu], ht[0][a], ht[1][a], chi[0][a], chi[1][a]);
                 cpx<double> b = mk<double>(0.0, 0.0);
 #pragma unroll
                 for (int c = 0; c < kColours; c++)
@@ -296,16 +305,29 @@ size_t charges_partial_doubles(const Lattice &L, int n_mb) {
     return (size_t)currents_groups(n_mb) * ((L.V + kCurrentsThreadsY - 1) / kCurrentsThreadsY) * kChargeVals;
 }
 
-template <typename T>
-void launch_charges(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
-                    int first_mode, double r_wilson, double *partial, double *out4, cudaStream_t stream) {
+template <class SRC>
+static void charges_from(const SRC &src, const double *U, const double *u1, const Lattice &L, int n_mb, int n_modes,
+                         int first_mode, double r, double *partial, double *out4, cudaStream_t stream) {
     const int groups = currents_groups(n_mb);
     dim3 block(kModeBlock, kCurrentsThreadsY);
     dim3 grid((L.V + kCurrentsThreadsY - 1) / kCurrentsThreadsY, groups);
-    charges_kernel<T><<<grid, block, 0, stream>>>(U, reinterpret_cast<const double2 *>(u1),
-                                                  reinterpret_cast<const cpx<T> *>(psi), L, n_mb, n_modes, first_mode,
-                                                  groups, (T)r_wilson, partial);
+    charges_kernel<SRC><<<grid, block, 0, stream>>>(U, reinterpret_cast<const double2 *>(u1), src, L, n_mb, n_modes,
+                                                    first_mode, groups, r, partial);
     charges_finish_kernel<<<1, 256, 0, stream>>>(partial, (int)(grid.x * grid.y), 1.0 / (2.0 * L.V), out4);
+}
+
+template <typename T>
+void launch_charges(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                    int first_mode, double r_wilson, double *partial, double *out4, cudaStream_t stream) {
+    // the arithmetic precision of r as before: the FP32 path rounds it to float
+    charges_from(SrcPlain<T>{reinterpret_cast<const cpx<T> *>(psi)}, U, u1, L, n_mb, n_modes, first_mode,
+                 (double)(T)r_wilson, partial, out4, stream);
+}
+
+void launch_charges40(const double *U, const double *u1, const void *hi, const void *lo, const Lattice &L, int n_mb,
+                      int n_modes, int first_mode, double r_wilson, double *partial, double *out4, cudaStream_t stream) {
+    charges_from(Src40{reinterpret_cast<const uint2 *>(hi), reinterpret_cast<const unsigned char *>(lo)}, U, u1, L, n_mb,
+                 n_modes, first_mode, r_wilson, partial, out4, stream);
 }
 
 // Lattice sums of jV^0, jA^0, PS, WA from the per-site array, fixed order.
@@ -337,7 +359,7 @@ void launch_site_sums(const double *per_site, const Lattice &L, double * /*parti
 // ---------------------------------------------------------- layout change --
 template <typename T>
 __global__ void ref_to_blocks_kernel(const double2 *__restrict__ ref, cpx<T> *__restrict__ blocks, int V, int m0,
-                                     int count) {
+                                     int count, unsigned char *__restrict__ lo) {
     const size_t n = (size_t)count * V * kComp;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const int comp = (int)(i % kComp);
@@ -345,21 +367,29 @@ __global__ void ref_to_blocks_kernel(const double2 *__restrict__ ref, cpx<T> *__
         const int site = (int)(ms % V);
         const int m = m0 + (int)(ms / V);
         const double2 v = ref[i];
-        st(blocks + field_index(V, m / kModeBlock, site, comp, m % kModeBlock), mk<T>((T)v.x, (T)v.y));
+        const size_t j = field_index(V, m / kModeBlock, site, comp, m % kModeBlock);
+        if (lo) store40(reinterpret_cast<uint2 *>(blocks), lo, j, v.x, v.y);  // 40-bit storage
+        else st(blocks + j, mk<T>((T)v.x, (T)v.y));
     }
 }
 
 template <typename T>
 __global__ void blocks_to_ref_kernel(const cpx<T> *__restrict__ blocks, double2 *__restrict__ ref, int V, int m0,
-                                     int count) {
+                                     int count, const unsigned char *__restrict__ lo) {
     const size_t n = (size_t)count * V * kComp;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const int comp = (int)(i % kComp);
         const size_t ms = i / kComp;
         const int site = (int)(ms % V);
         const int m = m0 + (int)(ms / V);
-        const cpx<T> v = blocks[field_index(V, m / kModeBlock, site, comp, m % kModeBlock)];
-        ref[i] = double2{(double)v.re, (double)v.im};
+        const size_t j = field_index(V, m / kModeBlock, site, comp, m % kModeBlock);
+        if (lo) {  // 40-bit storage
+            const cpx<double> v = Src40{reinterpret_cast<const uint2 *>(blocks), lo}(j);
+            ref[i] = double2{v.re, v.im};
+        } else {
+            const cpx<T> v = blocks[j];
+            ref[i] = double2{(double)v.re, (double)v.im};
+        }
     }
 }
 
@@ -369,19 +399,23 @@ static int grid_for(size_t n) {
 }
 
 template <typename T>
-void launch_ref_to_blocks(const double *ref, void *blocks, const Lattice &L, int m0, int count, cudaStream_t stream) {
+void launch_ref_to_blocks(const double *ref, void *blocks, const Lattice &L, int m0, int count, cudaStream_t stream,
+                          void *lo) {
     const size_t n = (size_t)count * L.V * kComp;
     if (n == 0) return;
     ref_to_blocks_kernel<T><<<grid_for(n), 256, 0, stream>>>(reinterpret_cast<const double2 *>(ref),
-                                                             reinterpret_cast<cpx<T> *>(blocks), L.V, m0, count);
+                                                             reinterpret_cast<cpx<T> *>(blocks), L.V, m0, count,
+                                                             reinterpret_cast<unsigned char *>(lo));
 }
 
 template <typename T>
-void launch_blocks_to_ref(const void *blocks, double *ref, const Lattice &L, int m0, int count, cudaStream_t stream) {
+void launch_blocks_to_ref(const void *blocks, double *ref, const Lattice &L, int m0, int count, cudaStream_t stream,
+                          const void *lo) {
     const size_t n = (size_t)count * L.V * kComp;
     if (n == 0) return;
     blocks_to_ref_kernel<T><<<grid_for(n), 256, 0, stream>>>(reinterpret_cast<const cpx<T> *>(blocks),
-                                                             reinterpret_cast<double2 *>(ref), L.V, m0, count);
+                                                             reinterpret_cast<double2 *>(ref), L.V, m0, count,
+                                                             reinterpret_cast<const unsigned char *>(lo));
 }
 
 // ------------------------------------------------------------ plane waves --
@@ -480,7 +514,7 @@ __global__ void free_modes_kernel(FreeMode *info, int n_modes, int first_mode, L
 
 template <typename T>
 __global__ void free_fill_kernel(const FreeMode *__restrict__ info, cpx<T> *psi, cpx<T> *psimid, Lattice L, int n_modes,
-                                 int n_mb, double dt) {
+                                 int n_mb, double dt, unsigned char *lo_psi, unsigned char *lo_mid) {
     const int lane = threadIdx.x;
     const int site = blockIdx.x * blockDim.y + threadIdx.y;
     const int mb = blockIdx.y;
@@ -507,14 +541,20 @@ __global__ void free_fill_kernel(const FreeMode *__restrict__ info, cpx<T> *psi,
             cpx<double> v = c == colour ? phase * u[a] : mk<double>(0, 0);
             cpx<double> vm = c == colour ? v * half : mk<double>(0, 0);
             const size_t idx = field_index(L.V, mb, site, c * kSpin + a, lane);
-            st(psi + idx, mk<T>((T)v.re, (T)v.im));
-            st(psimid + idx, mk<T>((T)vm.re, (T)vm.im));
+            if (lo_psi) {  // 40-bit storage
+                store40(reinterpret_cast<uint2 *>(psi), lo_psi, idx, v.re, v.im);
+                store40(reinterpret_cast<uint2 *>(psimid), lo_mid, idx, vm.re, vm.im);
+            } else {
+                st(psi + idx, mk<T>((T)v.re, (T)v.im));
+                st(psimid + idx, mk<T>((T)vm.re, (T)vm.im));
+            }
         }
 }
 
 template <typename T>
 void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes, int n_mb, int first_mode,
-                          double r_wilson, double m_fermion, double dt, int *bad, cudaStream_t stream) {
+                          double r_wilson, double m_fermion, double dt, int *bad, cudaStream_t stream, void *lo_psi,
+                          void *lo_mid) {
     FreeMode *info = nullptr;
     cudaMallocAsync(&info, sizeof(FreeMode) * (size_t)n_modes, stream);
     cudaMemsetAsync(bad, 0, sizeof(int), stream);
@@ -522,7 +562,8 @@ void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes
     dim3 block(kModeBlock, kSitesPerCta);
     dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
     free_fill_kernel<T><<<grid, block, 0, stream>>>(info, reinterpret_cast<cpx<T> *>(psi), reinterpret_cast<cpx<T> *>(psimid),
-                                                    L, n_modes, n_mb, dt);
+                                                    L, n_modes, n_mb, dt, reinterpret_cast<unsigned char *>(lo_psi),
+                                                    reinterpret_cast<unsigned char *>(lo_mid));
     cudaFreeAsync(info, stream);
 }
 
@@ -531,10 +572,11 @@ void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes
                                     double, double *, double *, cudaStream_t);                                      \
     template void launch_currents<T>(const double *, const double *, const void *, const Lattice &, int, int, int,   \
                                      double, double *, double *, cudaStream_t);                                     \
-    template void launch_ref_to_blocks<T>(const double *, void *, const Lattice &, int, int, cudaStream_t);          \
-    template void launch_blocks_to_ref<T>(const void *, double *, const Lattice &, int, int, cudaStream_t);         \
+    template void launch_ref_to_blocks<T>(const double *, void *, const Lattice &, int, int, cudaStream_t, void *);  \
+    template void launch_blocks_to_ref<T>(const void *, double *, const Lattice &, int, int, cudaStream_t,          \
+                                          const void *);                                                            \
     template void launch_free_fermions<T>(void *, void *, const Lattice &, int, int, int, double, double, double,    \
-                                          int *, cudaStream_t);
+                                          int *, cudaStream_t, void *, void *);
 OVL_INSTANTIATE(double)
 OVL_INSTANTIATE(float)
 

@@ -18,6 +18,7 @@
 
 #include <type_traits>
 
+#include "ovl_fp40.cuh"
 #include "ovl_internal.h"
 #include "ovl_stencil.cuh"
 
@@ -173,6 +174,133 @@ void launch_wilson_tuned(const HopConfig &hc, const void *src, void *dst, const 
         if (hc.u1) go(LinksF64<true>{hc.U, reinterpret_cast<const double2 *>(hc.u1), n01});
         else go(LinksF64<false>{hc.U, nullptr, n01});
     }
+}
+
+// ------------------------------------------------------ 40-bit storage --
+// Half step on fields in 40-bit storage (ovl_fp40.cuh): a spinor is 8 uint2
+// high words plus one uint4 of extension bytes per lane (9 loads); the raw
+// words of the next neighbour are loaded one hop ahead (20 registers in
+// flight), decode to FP64 by register moves, and the stencil runs in FP64 with
+// the FP64 links; the destination is rounded back to 40 bits.  MODE 0:
+// dst = D src; MODE 1: dst += dt D src.  Same launch shape as variant 0.
+struct Raw40 {
+    uint2 h[kComp];
+    uint4 l;
+};
+
+__device__ __forceinline__ void load_raw40(const uint2 *__restrict__ hi, const uint4 *__restrict__ lo, int V, int mb,
+                                           int site, int lane, Raw40 &r) {
+    const size_t base = field_index(V, mb, site, 0, lane);
+#pragma unroll
+    for (int k = 0; k < kComp; k++) r.h[k] = __ldg(hi + base + k * kModeBlock);
+    r.l = __ldg(lo + ((size_t)mb * V + site) * kModeBlock + lane);
+}
+
+// Extension byte b of the packed word, moved to the top byte of a 32-bit word
+// (the low word of the decoded double) by one byte permute.
+__device__ __forceinline__ unsigned ext_low(const uint4 &l, int b) {
+    const unsigned w = b < 4 ? l.x : b < 8 ? l.y : b < 12 ? l.z : l.w;
+    return __byte_perm(w, 0u, 0x0444u | ((unsigned)(b & 3) << 12));
+}
+
+__device__ __forceinline__ void decode40(const Raw40 &r, Spinor<double> &s) {
+#pragma unroll
+    for (int c = 0; c < kColours; c++)
+#pragma unroll
+        for (int a = 0; a < kSpin; a++) {
+            const int k = c * kSpin + a;
+            s.c[c][a] = mk<double>(__hiloint2double((int)r.h[k].x, (int)ext_low(r.l, 2 * k)),
+                                   __hiloint2double((int)r.h[k].y, (int)ext_low(r.l, 2 * k + 1)));
+        }
+}
+
+// MINB: CTAs of 8 warps per SM the register allocation must allow (2: 128
+// registers, 3: 80 registers with a few spills); the autotuner picks.
+template <int MODE, int MINB, class LK>
+__global__ void __launch_bounds__(kModeBlock *kSitesPerCta, MINB)
+    wilson_fp40_kernel(LK lk, const uint2 *__restrict__ src, const uint4 *__restrict__ src_lo, uint2 *__restrict__ dst,
+                       uint4 *__restrict__ dst_lo, Lattice L, double amass, double dt) {
+    const int lane = threadIdx.x;
+    const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
+    const int mb = blockIdx.y;
+    if (site >= L.V) return;
+    const int V = L.V;
+    const Nbrs n = neighbours(L, site);
+    Raw40 a, b;
+    Spinor<double> acc, f;
+    load_raw40(src, src_lo, V, mb, site, lane, a);
+    load_raw40(src, src_lo, V, mb, n.xp, lane, b);
+    decode40(a, f);
+#pragma unroll
+    for (int c = 0; c < kColours; c++)
+#pragma unroll
+        for (int s2 = 0; s2 < kSpin; s2++) acc.c[c][s2] = amass * f.c[c][s2];
+    load_raw40(src, src_lo, V, mb, n.xm, lane, a);
+    decode40(b, f);
+    hop<double, 0, true>(acc, f, lk.template get<double>(site, 0));
+    load_raw40(src, src_lo, V, mb, n.yp, lane, b);
+    decode40(a, f);
+    hop<double, 0, false>(acc, f, lk.template get<double>(n.xm, 0));
+    load_raw40(src, src_lo, V, mb, n.ym, lane, a);
+    decode40(b, f);
+    hop<double, 1, true>(acc, f, lk.template get<double>(site, 1));
+    load_raw40(src, src_lo, V, mb, n.zp, lane, b);
+    decode40(a, f);
+    hop<double, 1, false>(acc, f, lk.template get<double>(n.ym, 1));
+    load_raw40(src, src_lo, V, mb, n.zm, lane, a);
+    decode40(b, f);
+    hop<double, 2, true>(acc, f, lk.template get<double>(site, 2));
+    if (MODE == 1) load_raw40(dst, dst_lo, V, mb, site, lane, b);  // the destination, one hop ahead
+    decode40(a, f);
+    hop<double, 2, false>(acc, f, lk.template get<double>(n.zm, 2));
+    const size_t base = field_index(V, mb, site, 0, lane);
+    unsigned lw[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int c = 0; c < kColours; c++)
+#pragma unroll
+        for (int s2 = 0; s2 < kSpin; s2++) {
+            const int k = c * kSpin + s2;
+            cpx<double> d = finish_component(acc.c[c][s2], s2);
+            if (MODE == 1) {
+                d.re = __hiloint2double((int)b.h[k].x, (int)ext_low(b.l, 2 * k)) + dt * d.re;
+                d.im = __hiloint2double((int)b.h[k].y, (int)ext_low(b.l, 2 * k + 1)) + dt * d.im;
+            }
+            // round to 40 bits: add half a unit of the last kept bit, keep the
+            // high word and the top byte of the low word
+            const unsigned long long bre = (unsigned long long)__double_as_longlong(d.re) + (1ull << 23);
+            const unsigned long long bim = (unsigned long long)__double_as_longlong(d.im) + (1ull << 23);
+            dst[base + k * kModeBlock] = make_uint2((unsigned)(bre >> 32), (unsigned)(bim >> 32));
+            // bytes 3 of the two low words -> bytes 2(k&1), 2(k&1)+1 of word k/2
+            const unsigned pair = __byte_perm((unsigned)bre, (unsigned)bim, 0x0073u) & 0xffffu;
+            lw[k >> 1] |= pair << (16 * (k & 1));
+        }
+    dst_lo[((size_t)mb * V + site) * kModeBlock + lane] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+
+void launch_wilson40(const HopConfig &hc, const void *src, const void *src_lo, void *dst, void *dst_lo,
+                     const Lattice &L, int mb_first, int n_mb, double amass, double dt, bool accumulate,
+                     cudaStream_t stream) {
+    if (n_mb <= 0) return;
+    const size_t off = field_index(L.V, mb_first, 0, 0, 0);    // complex numbers
+    const size_t loff = (size_t)mb_first * L.V * kModeBlock;  // uint4 words
+    const uint2 *s = reinterpret_cast<const uint2 *>(src) + off;
+    const uint4 *sl = reinterpret_cast<const uint4 *>(src_lo) + loff;
+    uint2 *d = reinterpret_cast<uint2 *>(dst) + (accumulate ? off : 0);
+    uint4 *dl = reinterpret_cast<uint4 *>(dst_lo) + (accumulate ? loff : 0);
+    dim3 block(kModeBlock, kSitesPerCta);
+    dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
+    const int n01 = L.N0 * L.N1;
+    auto go = [&](const auto &lk) {
+        using LK = std::decay_t<decltype(lk)>;
+        if (accumulate) {
+            if (hc.variant == 1) wilson_fp40_kernel<1, 3, LK><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt);
+            else wilson_fp40_kernel<1, 2, LK><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt);
+        } else {
+            wilson_fp40_kernel<0, 2, LK><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt);
+        }
+    };
+    if (hc.u1) go(LinksF64<true>{hc.U, reinterpret_cast<const double2 *>(hc.u1), n01});
+    else go(LinksF64<false>{hc.U, nullptr, n01});
 }
 
 // FP32 copy of the links (and of the U(1) phases) for the FP32 path.

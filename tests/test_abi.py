@@ -97,3 +97,10 @@ def test_mode_group_is_validated():
     from overlap_b200 import Context, OvlError
     with pytest.raises(OvlError):
         Context(N=(4, 4, 4), n_modes=8, form="fused", mode_group=-2)
+
+
+def test_fp40_is_rejected_outside_the_fused_wilson_form():
+    from overlap_b200 import Context, OvlError
+    for kw in (dict(form="plain"), dict(fermion="overlap", form="fused", sign_method="chebyshev")):
+        with pytest.raises(OvlError, match="FP40"):
+            Context(N=(4, 4, 4), n_modes=8, precision="fp40", **kw)

@@ -248,7 +248,7 @@ def test_autotune_keeps_state_and_reports_each_variant():
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp40"])
 @pytest.mark.parametrize("group", [1, 3])
 def test_grouped_step_equals_the_ungrouped_step(precision, group):
     """The grouped fused step (both half steps per group of mode blocks, with the
@@ -276,3 +276,50 @@ def test_grouped_step_equals_the_ungrouped_step(precision, group):
     for k in range(3):
         assert np.array_equal(a[k], b[k])
     assert a[3] == b[3]
+
+
+def test_fp40_storage_tracks_fp64_to_its_rounding():
+    """40-bit storage (the top 40 bits of each FP64 real, FP64 hop arithmetic):
+    the leapfrog follows the oracle to the storage rounding (2^-29 per write),
+    and modes round-trip through ovl_set_modes / ovl_get_modes to 2^-29."""
+    N = (4, 6, 5)
+    n = 45
+    U = random_links(N, 0.6, 81)
+    E = random_efield(N, 0.3, 82)
+    psi0 = random_modes(n, N, 83)
+    mid0 = random_modes(n, N, 84)
+    p = oracle_params(N, m=0.1, mdw=0.0, dt=0.05, t_sph=1e9)
+    opsi, omid, oU, _ = oracle_leapfrog(p, U, E, psi0, mid0, 6)
+    ocur = oracle_currents(p, oU, opsi, 3)
+    with Context(N=N, n_modes=n, first_mode=3, precision="fp40", form="fused", m_fermion=0.1, m_dw=0.0, dt=0.05,
+                 t_sphaleron=1e9) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_modes(psi0, mid0)
+        a, b = ctx.get_modes()
+        assert rel_err(a, psi0) < 2.0 ** -28 and rel_err(b, mid0) < 2.0 ** -28
+        ctx.step(6)
+        psi, mid = ctx.get_modes()
+        assert rel_err(psi, opsi) < 1e-7
+        assert rel_err(mid, omid) < 1e-7
+        assert rel_err(ctx.get_links(), oU) < 1e-13
+        cur = ctx.currents()
+        scale = current_scale(opsi)
+        for k in ocur:
+            assert np.max(np.abs(cur[k] - ocur[k])) <= 1e-7 * scale, k
+
+
+def test_fp40_free_fermions_and_observables_match_fp64():
+    N = (4, 4, 6)
+    out = {}
+    for prec in ("fp64", "fp40"):
+        with Context(N=N, precision=prec, form="fused", m_fermion=0.05, m_dw=0.0, dt=0.05) as ctx:
+            assert ctx.set_free_fermions() == 0
+            ctx.set_links(random_links(N, 0.4, 91))
+            out[prec] = (ctx.get_modes(), ctx.charges(), ctx.fermion_energy(), ctx.color_force())
+    for k in range(2):
+        assert rel_err(out["fp40"][0][k], out["fp64"][0][k]) < 2.0 ** -28
+    for k in ("NV", "N5", "PS", "WA"):
+        assert abs(out["fp40"][1][k] - out["fp64"][1][k]) < 1e-7
+    assert abs(out["fp40"][2] - out["fp64"][2]) < 1e-9 * abs(out["fp64"][2])
+    assert np.max(np.abs(out["fp40"][3] - out["fp64"][3])) < 1e-8
