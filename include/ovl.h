@@ -260,6 +260,18 @@ int ovl_ncsdot(ovl_ctx *ctx, double *out);
  * (CoolingMethod::Start) and returns 0. */
 int ovl_ncs_update(ovl_ctx *ctx, double *delta, double *total);
 
+/* Stochastic vacuum modes in place of the complete plane-wave basis (no
+ * reference counterpart): modes 2r and 2r+1 (global index) are P+ eta_r and
+ * P- eta_r, divided by sqrt(total_pairs), with eta_r complex Z2 noise
+ * ((+-1 +- i)/sqrt 2 per component, drawn in momentum space from `seed`) and
+ * P+- the projectors on the positive- and negative-energy states of the free
+ * Wilson Hamiltonian (those the plane-wave particles and antiparticles span);
+ * psimid = exp(-i h dt/2) psi.  The vacuum-weighted mode sums of the currents
+ * are then unbiased estimates of the complete basis's, and the free vacuum
+ * energy is reproduced exactly.  total_pairs: pairs over all contexts that
+ * share the estimate (0: n_modes / 2 of this one; first_mode and n_modes even). */
+int ovl_set_stochastic_modes(ovl_ctx *ctx, uint64_t seed, int total_pairs);
+
 /* Dynamics::UpdateGaugeLinks over the whole lattice (DYNAMICS/Dynamics.cpp:97-138):
  * U <- exp(-i dt_step E^a t^a) U. */
 int ovl_update_links(ovl_ctx *ctx, double dt_step);
@@ -331,6 +343,35 @@ int ovl_profile_enable(ovl_ctx *ctx, int on);
 /* Synchronises the stream and returns, per kind, the summed kernel time in ms
  * and the number of launches timed since recording was enabled. */
 int ovl_profile_read(ovl_ctx *ctx, double ms[OVL_PROF_KINDS], uint64_t launches[OVL_PROF_KINDS]);
+
+/* ------------------------------------------------------------ ensembles --
+ * An ensemble: independent trajectories (members), each a context of its own
+ * lattice size, mode count, physics and gauge fields, advanced together.  A
+ * leapfrog step of all members is one launch for all hop work per half step,
+ * one launch for all link updates per half step and one for the step counters
+ * (Update.cpp:48-79 per member, its tSphaleron gate evaluated on the device),
+ * captured once as a CUDA graph and replayed per step.  The reference has no
+ * counterpart: its MPI ranks split the modes of one trajectory.  Members:
+ * Wilson fermions, fused form, FP32 or FP64 (one precision and device for
+ * all), no coupled evolution.  Members are set up and measured through their
+ * contexts (ovl_ensemble_member; do not destroy them: the ensemble owns them). */
+typedef struct ovl_ensemble ovl_ensemble;
+int ovl_ensemble_create(const ovl_params *members, int count, ovl_ensemble **out);
+int ovl_ensemble_destroy(ovl_ensemble *ens);
+const char *ovl_ensemble_last_error(const ovl_ensemble *ens);
+int ovl_ensemble_member(ovl_ensemble *ens, int index, ovl_ctx **ctx);
+/* nsteps leapfrog steps of every member.  The first call times tiles of 4 and
+ * 8 sites (x 32 modes) of the batched hop on the members' operator buffers and
+ * keeps the faster. */
+int ovl_ensemble_step(ovl_ensemble *ens, int nsteps);
+/* ovl_charges of every member: out[4 i + k]. */
+int ovl_ensemble_charges(ovl_ensemble *ens, double *out);
+/* Sites per tile chosen (0 before the first step), the tuning times (ms, for
+ * 8 and 4 sites) and the kernels launched. */
+int ovl_ensemble_info(const ovl_ensemble *ens, int *sites, double tile_ms[2], uint64_t *launches);
+int ovl_ensemble_synchronize(ovl_ensemble *ens);
+/* The ensemble's CUDA stream (cudaStream_t as an integer). */
+uint64_t ovl_ensemble_stream(const ovl_ensemble *ens);
 
 #ifdef __cplusplus
 }

@@ -62,6 +62,16 @@ SIGNATURES = {
     "ovl_ncs_update": ([_ctx, _dp, _dp], C.c_int),
     "ovl_update_links": ([_ctx, C.c_double], C.c_int),
     "ovl_update_efield": ([_ctx, C.c_double], C.c_int),
+    "ovl_ensemble_create": ([C.POINTER(ovl_params), C.c_int, C.POINTER(_ctx)], C.c_int),
+    "ovl_ensemble_destroy": ([_ctx], C.c_int),
+    "ovl_ensemble_last_error": ([_ctx], C.c_char_p),
+    "ovl_ensemble_member": ([_ctx, C.c_int, C.POINTER(_ctx)], C.c_int),
+    "ovl_ensemble_step": ([_ctx, C.c_int], C.c_int),
+    "ovl_ensemble_charges": ([_ctx, _dp], C.c_int),
+    "ovl_ensemble_info": ([_ctx, C.POINTER(C.c_int), _dp, C.POINTER(C.c_uint64)], C.c_int),
+    "ovl_ensemble_synchronize": ([_ctx], C.c_int),
+    "ovl_ensemble_stream": ([_ctx], C.c_uint64),
+    "ovl_set_stochastic_modes": ([_ctx, C.c_uint64, C.c_int], C.c_int),
     "ovl_tuning": ([_ctx, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "ovl_ritz_bounds": ([_ctx, _dp, _dp, _dp, C.POINTER(C.c_int)], C.c_int),
     "ovl_color_force": ([_ctx, _dp], C.c_int),

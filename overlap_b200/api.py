@@ -135,9 +135,23 @@ class Context:
             raise OvlError(rc, self._L.ovl_last_error(self._ctx).decode())
 
     def close(self):
-        if self._ctx:
+        if self._ctx and getattr(self, "_owned", True):
             self._L.ovl_destroy(self._ctx)
-            self._ctx = C.c_void_p()
+        self._ctx = C.c_void_p()
+
+    @classmethod
+    def _member(cls, handle: C.c_void_p, params: "Params", owner) -> "Context":
+        """A view of a context owned by an Ensemble (not destroyed by close())."""
+        self = cls.__new__(cls)
+        self.params = params
+        self._L = _lib.lib()
+        self._ctx = handle
+        self._owned = False
+        self._owner = owner  # keeps the ensemble alive
+        self.N = tuple(int(n) for n in params.N)
+        self.V = volume(self.N)
+        self.n_modes = int(params.n_modes if params.n_modes is not None else 8 * self.V)
+        return self
 
     def __enter__(self):
         return self
@@ -236,6 +250,10 @@ class Context:
         ms = np.zeros(3)
         self._check(self._L.ovl_autotune(self._ctx, C.byref(v), _dp(ms)))
         return v.value, ms.tolist()
+
+    def set_stochastic_modes(self, seed: int = 0, total_pairs: int = 0):
+        """Z2-noise vacuum modes (pairs P+ eta, P- eta / sqrt(pairs)) in place of plane waves."""
+        self._check(self._L.ovl_set_stochastic_modes(self._ctx, int(seed) & (2**64 - 1), int(total_pairs)))
 
     def tuning(self) -> tuple[int, int]:
         """(hop variant, mode blocks per group) in use; -1 before the autotuner ran."""
@@ -360,3 +378,76 @@ class Context:
         v = C.c_uint64(0)
         self._check(self._L.ovl_launch_count(self._ctx, C.byref(v)))
         return v.value
+
+
+class Ensemble:
+    """Independent trajectories of mixed lattice sizes stepped together
+    (ovl_ensemble_*): one batched launch per half step and per link update,
+    one CUDA graph per leapfrog step.  members: a list of Params (Wilson, fused
+    form, one precision).  ens[i] is member i's Context (set links, modes,
+    measure); step(n) advances all of them."""
+
+    def __init__(self, members):
+        self._L = _lib.lib()
+        self.params = [m if isinstance(m, Params) else Params(**m) for m in members]
+        arr = (_lib.ovl_params * len(self.params))(*[p.to_c() for p in self.params])
+        self._e = C.c_void_p()
+        rc = self._L.ovl_ensemble_create(arr, len(self.params), C.byref(self._e))
+        if rc != 0:
+            raise OvlError(rc, self._L.ovl_ensemble_last_error(None).decode())
+        self.members = []
+        for i, p in enumerate(self.params):
+            h = C.c_void_p()
+            self._check(self._L.ovl_ensemble_member(self._e, i, C.byref(h)))
+            self.members.append(Context._member(h, p, self))
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise OvlError(rc, self._L.ovl_ensemble_last_error(self._e).decode())
+
+    def __len__(self):
+        return len(self.members)
+
+    def __getitem__(self, i) -> Context:
+        return self.members[i]
+
+    def step(self, nsteps: int = 1):
+        self._check(self._L.ovl_ensemble_step(self._e, int(nsteps)))
+
+    def charges(self) -> np.ndarray:
+        """[members, 4]: N_V, N_5, PS, WA of each member."""
+        o = np.empty((len(self.members), 4))
+        self._check(self._L.ovl_ensemble_charges(self._e, _dp(o)))
+        return o
+
+    def info(self) -> dict:
+        sites, launches = C.c_int(0), C.c_uint64(0)
+        ms = np.zeros(2)
+        self._check(self._L.ovl_ensemble_info(self._e, C.byref(sites), _dp(ms), C.byref(launches)))
+        return {"sites": sites.value, "tile_ms": {8: float(ms[0]), 4: float(ms[1])}, "launches": launches.value}
+
+    def synchronize(self):
+        self._check(self._L.ovl_ensemble_synchronize(self._e))
+
+    @property
+    def stream(self) -> int:
+        return int(self._L.ovl_ensemble_stream(self._e))
+
+    def close(self):
+        if self._e:
+            for m in self.members:
+                m._ctx = C.c_void_p()
+            self._L.ovl_ensemble_destroy(self._e)
+            self._e = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,122 @@
+// Ensembles: independent trajectories (members) of their own lattice size
+// and mode count, stepped together.  One launch advances the hop work of every
+// member by a half step and one launch updates every member's links, so a
+// leapfrog step of the whole ensemble is five kernels (two half steps, two
+// link updates, the step counters), captured once as a CUDA graph.
+//
+// Work is cut into tiles of SITES sites x one block of 32 modes (a warp per
+// site, as the single-trajectory kernels); tiles are numbered member by member
+// and a CTA finds its member by binary search over the members' first tiles.
+// The Update.cpp:57 gate (links move while qs t < tSphaleron) is evaluated on
+// the device from each member's step counter, so the captured step needs no
+// host decisions.
+#include "ovl_fp40.cuh"
+#include "ovl_internal.h"
+#include "ovl_stencil.cuh"
+
+namespace ovl {
+
+__device__ __forceinline__ int find_member(const BatchMember *__restrict__ m, int count, long long key,
+                                           long long BatchMember::*first) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {  // last member whose first index <= key
+        const int mid = (lo + hi + 1) >> 1;
+        if (m[mid].*first <= key) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// phase 0: psi += dt D psimid; phase 1: psimid += dt D psi
+// CTAs per SM the register allocation must allow: FP32 64 registers, FP64 128.
+template <typename T, int SITES> struct BatchOcc {
+    static constexpr int kMinBlocks = (sizeof(T) == 4 ? 1024 : 512) / (kModeBlock * SITES);
+};
+
+template <typename T, int SITES>
+__global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlocks)
+    wilson_batch_kernel(const BatchMember *__restrict__ members, int count, int phase) {
+    const int mi = find_member(members, count, (long long)blockIdx.x, &BatchMember::tile0);
+    const BatchMember &m = members[mi];
+    const Lattice L{m.N0, m.N1, m.N2, m.V};
+    const int nsb = (L.V + SITES - 1) / SITES;
+    const long long local = (long long)blockIdx.x - m.tile0;
+    const int mb = (int)(local / nsb);
+    const int site = (int)(local % nsb) * SITES + threadIdx.y;
+    if (site >= L.V) return;
+    const int lane = threadIdx.x;
+    const cpx<T> *src = reinterpret_cast<const cpx<T> *>(phase == 0 ? m.psimid : m.psi);
+    cpx<T> *dst = reinterpret_cast<cpx<T> *>(phase == 0 ? m.psi : m.psimid);
+    const int n01 = L.N0 * L.N1;
+    Spinor<T> acc;
+    if constexpr (sizeof(T) == 4) {
+        const float4 *u = reinterpret_cast<const float4 *>(m.U32);
+        if (m.u1_32) wilson_site_lk(LinksF32<true>{u, reinterpret_cast<const float2 *>(m.u1_32), n01}, src, L, site, mb, lane, (T)m.amass, acc);
+        else wilson_site_lk(LinksF32<false>{u, nullptr, n01}, src, L, site, mb, lane, (T)m.amass, acc);
+    } else {
+        if (m.u1) wilson_site_lk(LinksF64<true>{m.U, reinterpret_cast<const double2 *>(m.u1), n01}, src, L, site, mb, lane, (T)m.amass, acc);
+        else wilson_site_lk(LinksF64<false>{m.U, nullptr, n01}, src, L, site, mb, lane, (T)m.amass, acc);
+    }
+    cpx<T> *out = dst + field_index(L.V, mb, site, 0, lane);
+    const T dt = (T)m.dt;
+#pragma unroll
+    for (int c = 0; c < kColours; c++)
+#pragma unroll
+        for (int a = 0; a < kSpin; a++) {
+            const cpx<T> d = finish_component(acc.c[c][a], a);
+            cpx<T> *o = out + (c * kSpin + a) * kModeBlock;
+            const cpx<T> v = ld(o);
+            st(o, v + dt * d);
+        }
+}
+
+// Link updates of every member, U <- exp(-i dt/2 E^a t^a) U where the member's
+// links move (Update.cpp:57 on its own step counter), with the FP32 copy kept.
+__global__ void links_batch_kernel(const BatchMember *__restrict__ members, int count, long long total) {
+    const long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (l >= total) return;
+    const int mi = find_member(members, count, l, &BatchMember::link0);
+    const BatchMember &m = members[mi];
+    const int k = (int)(l - m.link0);  // link of the member: 3 site + mu
+    if (!(m.qs * (*m.tsteps * m.dt) < m.t_sphaleron)) return;
+    const double *e = m.E + 3 * k;
+    const quat g = qexp(-0.5 * m.dt, e[0], e[1], e[2]);
+    const int site = k / 3, mu = k % 3;
+    quat u = qmul(g, load_link(m.U, site, mu));
+    if (m.reunit) {
+        const double nrm = sqrt(u.v0 * u.v0 + u.v1 * u.v1 + u.v2 * u.v2 + u.s * u.s);
+        u = {u.v0 / nrm, u.v1 / nrm, u.v2 / nrm, u.s / nrm};
+    }
+    store_link(m.U, site, mu, u);
+    if (m.U32) reinterpret_cast<float4 *>(m.U32)[k] = float4{(float)u.v0, (float)u.v1, (float)u.v2, (float)u.s};
+}
+
+__global__ void advance_batch_kernel(const BatchMember *__restrict__ members, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) *members[i].tsteps += 1;
+}
+
+long long batch_tiles(int V, int n_mb, int sites) { return (long long)((V + sites - 1) / sites) * n_mb; }
+
+template <int SITES>
+static void launch_hop(const BatchMember *members, int count, long long tiles, int phase, bool fp32, cudaStream_t s) {
+    const dim3 block(kModeBlock, SITES);
+    if (fp32) wilson_batch_kernel<float, SITES><<<(unsigned)tiles, block, 0, s>>>(members, count, phase);
+    else wilson_batch_kernel<double, SITES><<<(unsigned)tiles, block, 0, s>>>(members, count, phase);
+}
+
+void launch_batch_hop(const BatchMember *members, int count, long long tiles, int sites, int phase, bool fp32,
+                      cudaStream_t stream) {
+    if (sites == 4) launch_hop<4>(members, count, tiles, phase, fp32, stream);
+    else launch_hop<8>(members, count, tiles, phase, fp32, stream);
+}
+
+void launch_batch_links(const BatchMember *members, int count, long long total_links, cudaStream_t stream) {
+    links_batch_kernel<<<(unsigned)((total_links + 255) / 256), 256, 0, stream>>>(members, count, total_links);
+}
+
+void launch_batch_advance(const BatchMember *members, int count, cudaStream_t stream) {
+    advance_batch_kernel<<<(count + 127) / 128, 128, 0, stream>>>(members, count);
+}
+
+}  // namespace ovl

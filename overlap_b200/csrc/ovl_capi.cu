@@ -780,6 +780,38 @@ int ovl_get_modes(ovl_ctx *c, int first, int count, double *psi, double *psimid)
     return transfer_modes(c, first, count, nullptr, nullptr, psi, psimid, false);
 }
 
+int ovl_set_stochastic_modes(ovl_ctx *c, uint64_t seed, int total_pairs) {
+    if (!c) return OVL_E_ARG;
+    if (c->p.fermion != OVL_FERMION_WILSON) return fail(c, OVL_E_UNSUPPORTED, "ovl_set_stochastic_modes: Wilson fermions only");
+    if (total_pairs < 0) return fail(c, OVL_E_ARG, "ovl_set_stochastic_modes: total_pairs=%d", total_pairs);
+    if (total_pairs == 0) {
+        if ((c->p.first_mode | c->p.n_modes) & 1)
+            return fail(c, OVL_E_ARG, "ovl_set_stochastic_modes: pairs need an even first_mode and n_modes");
+        total_pairs = c->p.n_modes / 2;
+    }
+    int rc = set_device(c);
+    if (rc) return rc;
+    const int chunk = std::min(c->n_mb, 64);
+    const size_t bytes = sizeof(double) * 2 * (size_t)chunk * c->L.V * ovl::kComp * ovl::kModeBlock;
+    double *a = nullptr, *b = nullptr;
+    if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        if (a) cudaFree(a);
+        return fail(c, OVL_E_OOM, "ovl_set_stochastic_modes: scratch");
+    }
+    const int kind = fp40(c) ? 2 : fp32(c) ? 1 : 0;
+    uint64_t nl = 0;
+    ovl::launch_stochastic_modes(c->psi, c->psimid, c->psi_lo, c->psimid_lo, kind, c->L, c->n_mb, c->p.n_modes,
+                                 c->p.first_mode, amass(c->p), c->p.dt, seed, total_pairs, a, b, chunk, c->stream, &nl);
+    rc = launched(c, (int)nl, "stochastic modes");
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(a);
+    cudaFree(b);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(c, e, "ovl_set_stochastic_modes");
+    return OVL_OK;
+}
+
 int ovl_set_free_fermions(ovl_ctx *c, int *n_bad) {
     if (!c) return OVL_E_ARG;
     int rc = set_device(c);
@@ -1315,5 +1347,286 @@ int ovl_profile_read(ovl_ctx *c, double ms[OVL_PROF_KINDS], uint64_t launches[OV
     }
     return OVL_OK;
 }
+
+// ---------------------------------------------------------------- ensembles --
+
+}  // extern "C"
+
+struct ovl_ensemble {
+    std::vector<ovl_ctx *> members;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool fp32 = true;
+    int sites = 0;  // sites per tile of the batched hop; 0 until tuned
+    double tile_ms[2] = {0.0, 0.0};
+    std::vector<ovl::BatchMember> host;
+    ovl::BatchMember *dev = nullptr;
+    int *dev_tsteps = nullptr;
+    long long tiles = 0, links = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_sites = 0;
+    uint64_t launches = 0;
+    std::string err;
+};
+
+namespace {
+
+std::string g_ens_err;
+
+int ens_fail(ovl_ensemble *e, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (e) e->err = buf; else g_ens_err = buf;
+    return code;
+}
+
+// Descriptors of all members for tiles of `sites` sites; `tuning`: the hop
+// writes each member's operator buffer instead of psi (the state is kept).
+void ens_describe(ovl_ensemble *e, int sites, bool tuning) {
+    e->host.resize(e->members.size());
+    long long tile = 0, link = 0;
+    for (size_t i = 0; i < e->members.size(); i++) {
+        ovl_ctx *c = e->members[i];
+        ovl::BatchMember &m = e->host[i];
+        m.psi = tuning ? c->aux_dst : c->psi;
+        m.psimid = c->psimid;
+        m.U = c->U;
+        m.u1 = c->u1_on ? c->u1 : nullptr;
+        m.U32 = c->U32;
+        m.u1_32 = c->u1_on ? c->u1_32 : nullptr;
+        m.E = c->E;
+        m.tsteps = e->dev_tsteps + i;
+        m.N0 = c->L.N0;
+        m.N1 = c->L.N1;
+        m.N2 = c->L.N2;
+        m.V = c->L.V;
+        m.n_mb = c->n_mb;
+        m.reunit = c->p.reunitarize != 0;
+        m.amass = amass(c->p);
+        m.dt = c->p.dt;
+        m.qs = c->p.qs;
+        m.t_sphaleron = c->p.t_sphaleron;
+        m.tile0 = tile;
+        m.link0 = link;
+        tile += ovl::batch_tiles(c->L.V, c->n_mb, sites);
+        link += 3LL * c->L.V;
+    }
+    e->tiles = tile;
+    e->links = link;
+}
+
+int ens_upload(ovl_ensemble *e) {
+    std::vector<int> ts(e->members.size());
+    for (size_t i = 0; i < ts.size(); i++) ts[i] = e->members[i]->tsteps;
+    cudaError_t r = cudaMemcpyAsync(e->dev, e->host.data(), sizeof(ovl::BatchMember) * e->host.size(),
+                                    cudaMemcpyHostToDevice, e->stream);
+    if (r == cudaSuccess)
+        r = cudaMemcpyAsync(e->dev_tsteps, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice, e->stream);
+    if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);  // ts lives on this stack frame
+    return r == cudaSuccess ? OVL_OK : ens_fail(e, OVL_E_CUDA, "ensemble: descriptor upload: %s", cudaGetErrorString(r));
+}
+
+void ens_free_graph(ovl_ensemble *e) {
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->exec = nullptr;
+    e->graph = nullptr;
+    e->graph_sites = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ovl_ensemble_create(const ovl_params *members, int count, ovl_ensemble **out) {
+    if (!members || !out || count < 1) return ens_fail(nullptr, OVL_E_ARG, "ovl_ensemble_create: need members");
+    *out = nullptr;
+    const ovl_params &p0 = members[0];
+    for (int i = 0; i < count; i++) {
+        const ovl_params &p = members[i];
+        if (p.fermion != OVL_FERMION_WILSON || p.form != OVL_FORM_FUSED)
+            return ens_fail(nullptr, OVL_E_UNSUPPORTED, "ovl_ensemble_create: member %d: Wilson fermions, fused form only", i);
+        if (p.precision != OVL_PREC_FP32 && p.precision != OVL_PREC_FP64)
+            return ens_fail(nullptr, OVL_E_UNSUPPORTED, "ovl_ensemble_create: member %d: FP32 or FP64 modes only", i);
+        if (p.precision != p0.precision || p.device != p0.device)
+            return ens_fail(nullptr, OVL_E_ARG, "ovl_ensemble_create: member %d: one precision and device for all", i);
+        if (p.backreaction != 0.0 || p.gauge_force)
+            return ens_fail(nullptr, OVL_E_UNSUPPORTED, "ovl_ensemble_create: member %d: no coupled evolution", i);
+    }
+    ovl_ensemble *e = new (std::nothrow) ovl_ensemble();
+    if (!e) return ens_fail(nullptr, OVL_E_OOM, "ovl_ensemble_create: host allocation");
+    auto bail = [&](int code) {
+        g_ens_err = e->err;
+        ovl_ensemble_destroy(e);
+        return code;
+    };
+    e->device = p0.device;
+    e->fp32 = p0.precision == OVL_PREC_FP32;
+    if (cudaSetDevice(e->device) != cudaSuccess || cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(ens_fail(e, OVL_E_CUDA, "ovl_ensemble_create: device %d / stream", e->device));
+    for (int i = 0; i < count; i++) {
+        ovl_params p = members[i];
+        p.stream = reinterpret_cast<uint64_t>(e->stream);
+        p.hop_variant = 0;
+        p.mode_group = 0;
+        ovl_ctx *c = nullptr;
+        int rc = ovl_create(&p, &c);
+        if (rc) return bail(ens_fail(e, rc, "ovl_ensemble_create: member %d: %s", i, ovl_last_error(nullptr)));
+        e->members.push_back(c);
+    }
+    if (cudaMalloc(&e->dev, sizeof(ovl::BatchMember) * count) != cudaSuccess ||
+        cudaMalloc(&e->dev_tsteps, sizeof(int) * count) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(ens_fail(e, OVL_E_OOM, "ovl_ensemble_create: descriptors"));
+    }
+    *out = e;
+    return OVL_OK;
+}
+
+int ovl_ensemble_destroy(ovl_ensemble *e) {
+    if (!e) return OVL_OK;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    ens_free_graph(e);
+    for (ovl_ctx *c : e->members) ovl_destroy(c);
+    if (e->dev) cudaFree(e->dev);
+    if (e->dev_tsteps) cudaFree(e->dev_tsteps);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return OVL_OK;
+}
+
+const char *ovl_ensemble_last_error(const ovl_ensemble *e) { return e ? e->err.c_str() : g_ens_err.c_str(); }
+
+int ovl_ensemble_member(ovl_ensemble *e, int index, ovl_ctx **ctx) {
+    if (!e || !ctx || index < 0 || index >= (int)e->members.size())
+        return ens_fail(e, OVL_E_ARG, "ovl_ensemble_member: index %d", index);
+    *ctx = e->members[index];
+    return OVL_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Sites per tile of the batched hop: times tiles of 4 and 8 sites on a half
+// step that writes the members' operator buffers (the state is kept).
+int ens_tune(ovl_ensemble *e) {
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess)
+        return ens_fail(e, OVL_E_CUDA, "ensemble: events");
+    for (ovl_ctx *c : e->members) cudaMemsetAsync(c->aux_dst, 0, c->field_complex * c->elem_bytes, e->stream);
+    const int cand[2] = {8, 4};
+    double best = 1e300;
+    int pick = 8;
+    int rc = OVL_OK;
+    for (int k = 0; k < 2 && rc == OVL_OK; k++) {
+        ens_describe(e, cand[k], true);
+        if ((rc = ens_upload(e))) break;
+        float total = 0.0f;
+        for (int rep = 0; rep < 4; rep++) {
+            cudaEventRecord(a, e->stream);
+            ovl::launch_batch_hop(e->dev, (int)e->members.size(), e->tiles, cand[k], 0, e->fp32, e->stream);
+            cudaEventRecord(b, e->stream);
+            cudaEventSynchronize(b);
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, a, b);
+            if (rep > 0) total += t;
+        }
+        e->launches += 4;
+        e->tile_ms[k] = total / 3.0;
+        if (e->tile_ms[k] < best) { best = e->tile_ms[k]; pick = cand[k]; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaError_t r = cudaGetLastError();
+    if (rc == OVL_OK && r != cudaSuccess) rc = ens_fail(e, OVL_E_CUDA, "ensemble tuning: %s", cudaGetErrorString(r));
+    e->sites = pick;
+    return rc;
+}
+
+// One leapfrog step of every member (Update.cpp:48-79 per member): half step,
+// links, half step, links, step counters.
+void ens_enqueue_step(ovl_ensemble *e) {
+    const int n = (int)e->members.size();
+    ovl::launch_batch_hop(e->dev, n, e->tiles, e->sites, 0, e->fp32, e->stream);
+    ovl::launch_batch_links(e->dev, n, e->links, e->stream);
+    ovl::launch_batch_hop(e->dev, n, e->tiles, e->sites, 1, e->fp32, e->stream);
+    ovl::launch_batch_links(e->dev, n, e->links, e->stream);
+    ovl::launch_batch_advance(e->dev, n, e->stream);
+}
+
+int ens_capture(ovl_ensemble *e) {
+    ens_free_graph(e);
+    cudaError_t r = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+    if (r == cudaSuccess) {
+        ens_enqueue_step(e);
+        r = cudaStreamEndCapture(e->stream, &e->graph);
+    }
+    if (r == cudaSuccess) r = cudaGraphInstantiate(&e->exec, e->graph, 0);
+    if (r != cudaSuccess) {
+        cudaGetLastError();
+        ens_free_graph(e);
+        return ens_fail(e, OVL_E_CUDA, "ensemble: step graph: %s", cudaGetErrorString(r));
+    }
+    e->graph_sites = e->sites;
+    return OVL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ovl_ensemble_step(ovl_ensemble *e, int nsteps) {
+    if (!e) return OVL_E_ARG;
+    if (nsteps < 0) return ens_fail(e, OVL_E_ARG, "ovl_ensemble_step: nsteps=%d", nsteps);
+    if (nsteps == 0) return OVL_OK;
+    if (cudaSetDevice(e->device) != cudaSuccess) return ens_fail(e, OVL_E_CUDA, "ovl_ensemble_step: device");
+    int rc;
+    if (e->sites == 0 && (rc = ens_tune(e))) return rc;
+    // descriptors are rebuilt every call (links, phases and counters may have
+    // been set on the members); the captured graph reads them from device memory
+    ens_describe(e, e->sites, false);
+    if ((rc = ens_upload(e))) return rc;
+    if (e->graph_sites != e->sites && (rc = ens_capture(e))) return rc;
+    for (int n = 0; n < nsteps; n++) {
+        cudaError_t r = cudaGraphLaunch(e->exec, e->stream);
+        if (r != cudaSuccess) return ens_fail(e, OVL_E_CUDA, "ovl_ensemble_step: graph launch: %s", cudaGetErrorString(r));
+    }
+    e->launches += 5ull * nsteps;
+    for (ovl_ctx *c : e->members) c->tsteps += nsteps;
+    cudaError_t r = cudaGetLastError();
+    return r == cudaSuccess ? OVL_OK : ens_fail(e, OVL_E_CUDA, "ovl_ensemble_step: %s", cudaGetErrorString(r));
+}
+
+int ovl_ensemble_charges(ovl_ensemble *e, double *out) {
+    if (!e || !out) return OVL_E_ARG;
+    for (size_t i = 0; i < e->members.size(); i++) {
+        int rc = ovl_charges(e->members[i], out + 4 * i);
+        if (rc) return ens_fail(e, rc, "ovl_ensemble_charges: member %zu: %s", i, e->members[i]->err.c_str());
+    }
+    return OVL_OK;
+}
+
+int ovl_ensemble_info(const ovl_ensemble *e, int *sites, double tile_ms[2], uint64_t *launches) {
+    if (!e) return OVL_E_ARG;
+    if (sites) *sites = e->sites;
+    if (tile_ms) { tile_ms[0] = e->tile_ms[0]; tile_ms[1] = e->tile_ms[1]; }
+    if (launches) *launches = e->launches;
+    return OVL_OK;
+}
+
+int ovl_ensemble_synchronize(ovl_ensemble *e) {
+    if (!e) return OVL_E_ARG;
+    cudaSetDevice(e->device);
+    cudaError_t r = cudaStreamSynchronize(e->stream);
+    return r == cudaSuccess ? OVL_OK : ens_fail(e, OVL_E_CUDA, "ovl_ensemble_synchronize: %s", cudaGetErrorString(r));
+}
+
+uint64_t ovl_ensemble_stream(const ovl_ensemble *e) { return e ? reinterpret_cast<uint64_t>(e->stream) : 0; }
 
 }  // extern "C"

@@ -111,6 +111,37 @@ void launch_color_force40(const double *U, const double *u1, const void *hi, con
                           cudaStream_t stream);
 void launch_fermion_energy40(const void *hi, const void *lo, const void *dhi, const void *dlo, const Lattice &L,
                              int n_mb, int n_modes, int first_mode, double *partial, double *out, cudaStream_t stream);
+// Ensembles (ovl_batch.cu): one descriptor per member in device memory.
+// tile0: first tile of the member in the batched hop launch (tiles of `sites`
+// sites x one mode block, member by member); link0: first link in the batched
+// link update.  tsteps: the member's step counter on the device.
+struct BatchMember {
+    void *psi, *psimid;
+    double *U;
+    const double *u1;
+    float *U32;
+    const float *u1_32;
+    const double *E;
+    int *tsteps;
+    int N0, N1, N2, V;
+    int n_mb;
+    int reunit;
+    double amass, dt, qs, t_sphaleron;
+    long long tile0, link0;
+};
+long long batch_tiles(int V, int n_mb, int sites);
+// phase 0: psi += dt D psimid, phase 1: psimid += dt D psi, for every member;
+// FP32 (fp32) or FP64 modes; sites per tile 4 or 8.
+void launch_batch_hop(const BatchMember *members, int count, long long tiles, int sites, int phase, bool fp32,
+                      cudaStream_t stream);
+void launch_batch_links(const BatchMember *members, int count, long long total_links, cudaStream_t stream);
+void launch_batch_advance(const BatchMember *members, int count, cudaStream_t stream);
+// Stochastic vacuum modes (ovl_stochastic.cu): kind 0 FP64, 1 FP32, 2 FP40
+// storage; scratch_a/b: FP64 buffers of chunk_mb mode blocks each.
+void launch_stochastic_modes(void *psi, void *psimid, void *psi_lo, void *psimid_lo, int kind, const Lattice &L,
+                             int n_mb, int n_modes, int first_mode, double amass, double dt, uint64_t seed, int pairs,
+                             double *scratch_a, double *scratch_b, int chunk_mb, cudaStream_t stream,
+                             uint64_t *launches);
 // Lattice sums N_V, N_5, PS, WA straight from the modes (no per-site maps).
 size_t charges_partial_doubles(const Lattice &L, int n_mb);
 template <typename T>

@@ -1,0 +1,77 @@
+"""Ensembles (ovl_ensemble_*): trajectories of mixed lattice sizes, mode counts
+and physics stepped together by batched launches under a CUDA graph.  Each
+member must evolve exactly as the same context stepped alone (the batched hop
+runs the single-context stencil; separately compiled kernels may contract
+multiply-adds differently, so the comparison allows the last bits), including a
+U(1) background, reunitarisation and a tSphaleron gate crossed mid-run."""
+import numpy as np
+import pytest
+
+from _helpers import random_modes, rel_err
+from overlap_b200 import Context, Ensemble, OvlError, Params
+from overlap_b200.inputs import random_efield, random_links
+
+pytestmark = pytest.mark.gpu
+
+MEMBERS = [
+    dict(N=(4, 5, 6), n_modes=70, first_mode=1, m_fermion=0.1, dt=0.05, t_sphaleron=1e9),
+    dict(N=(6, 6, 6), n_modes=33, first_mode=0, m_fermion=0.05, dt=0.04, t_sphaleron=0.1, reunitarize=True),
+    dict(N=(5, 4, 4), n_modes=64, first_mode=2, m_fermion=0.2, dt=0.05, t_sphaleron=1e9),
+]
+
+
+def inputs(i, kw):
+    N = kw["N"]
+    n = kw["n_modes"]
+    return (random_links(N, 0.5, 10 * i + 1), random_efield(N, 0.3, 10 * i + 2), random_modes(n, N, 10 * i + 3),
+            random_modes(n, N, 10 * i + 4))
+
+
+def phases(N, seed):
+    return np.exp(1j * np.random.default_rng(seed).uniform(-np.pi, np.pi, (N[1], N[0], 2)))
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_ensemble_members_evolve_as_alone(precision):
+    params = [Params(precision=precision, form="fused", m_dw=0.0, hop_variant=0, **kw) for kw in MEMBERS]
+    alone = []
+    for i, (p, kw) in enumerate(zip(params, MEMBERS)):
+        U, E, psi0, mid0 = inputs(i, kw)
+        with Context(p) as ctx:
+            ctx.set_links(U)
+            ctx.set_efield(E)
+            if i == 2:
+                ctx.set_u1(phases(kw["N"], 5))
+            ctx.set_modes(psi0, mid0)
+            ctx.step(5)
+            alone.append((ctx.get_modes(), ctx.get_links(), ctx.charges()))
+    with Ensemble(params) as ens:
+        for i, kw in enumerate(MEMBERS):
+            U, E, psi0, mid0 = inputs(i, kw)
+            ens[i].set_links(U)
+            ens[i].set_efield(E)
+            if i == 2:
+                ens[i].set_u1(phases(kw["N"], 5))
+            ens[i].set_modes(psi0, mid0)
+        ens.step(2)
+        ens.step(3)  # the step graph is replayed with re-uploaded descriptors
+        ch = ens.charges()
+        info = ens.info()
+        tol = 1e-13 if precision == "fp64" else 1e-5
+        for i in range(len(MEMBERS)):
+            (psi, mid), U, c = alone[i]
+            bpsi, bmid = ens[i].get_modes()
+            assert rel_err(bpsi, psi) < tol and rel_err(bmid, mid) < tol, i
+            assert rel_err(ens[i].get_links(), U) < 1e-14, i
+            assert ens[i].step_count == 5
+            for k, name in enumerate(("NV", "N5", "PS", "WA")):
+                assert abs(ch[i, k] - c[name]) <= tol * max(1.0, abs(c[name])), (i, name)
+    assert info["sites"] in (4, 8) and info["launches"] >= 25
+
+
+def test_ensemble_rejects_unsupported_members():
+    with pytest.raises(OvlError):
+        Ensemble([Params(N=(4, 4, 4), n_modes=8, form="plain")])
+    with pytest.raises(OvlError):
+        Ensemble([Params(N=(4, 4, 4), n_modes=8, form="fused", precision="fp32"),
+                  Params(N=(4, 4, 4), n_modes=8, form="fused", precision="fp64")])
