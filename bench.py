@@ -293,6 +293,61 @@ def accuracy(wl, steps, every, device):
     return out
 
 
+def ensemble_leg(steps, warmup, device):
+    """The batched-ensemble configuration: 64 independent SU(2) trajectories,
+    16 each at N = 8, 10, 12, 16, 4096 Z2 stochastic vacuum modes each, U(1)
+    flux n_B in {0, 2, 4, 8}, dt = 0.05, FP32 modes, seeded random links
+    (sigma 0.3) and E (sigma 0.1).  Times `steps` leapfrog steps of the
+    ensemble (one CUDA graph per step) against the same members stepped one
+    context at a time."""
+    import numpy as np
+    import torch
+
+    from overlap_b200 import Ensemble, Params
+    from overlap_b200.inputs import random_efield, random_links, u1_flux
+
+    sizes = [8] * 16 + [10] * 16 + [12] * 16 + [16] * 16
+    params = [Params(N=(n, n, n), n_modes=4096, precision="fp32", form="fused", m_fermion=0.05, r_wilson=1.0,
+                     m_dw=0.0, dt=0.05, t_sphaleron=1e300, device=device) for n in sizes]
+    work = sum(p.n_modes * n ** 3 for p, n in zip(params, sizes))  # mode-sites per step
+    ens = Ensemble(params)
+    try:
+        for i, n in enumerate(sizes):
+            N = (n, n, n)
+            ens[i].set_links(random_links(N, 0.3, 1000 + i))
+            ens[i].set_efield(random_efield(N, 0.1, 2000 + i))
+            nb = (0, 2, 4, 8)[i % 4]
+            if nb:
+                ens[i].set_u1(u1_flux(N, nb))
+            ens[i].set_stochastic_modes(seed=3000 + i)
+        stream = torch.cuda.ExternalStream(ens.stream, device=device)
+        ens.step(warmup)
+        ens.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ens.step(steps)
+        b.record(stream)
+        b.synchronize()
+        t_ens = a.elapsed_time(b) / 1e3
+        # the same members, one context at a time (same stream, same kernels)
+        a.record(stream)
+        for _ in range(steps):
+            for i in range(len(sizes)):
+                ens[i].step(1)
+        b.record(stream)
+        b.synchronize()
+        t_seq = a.elapsed_time(b) / 1e3
+        info = ens.info()
+        n5 = ens.charges()[:, 1]
+    finally:
+        ens.close()
+    return {"config": "64 trajectories (16 each at N=8,10,12,16), 4096 Z2 stochastic modes each, "
+                      "n_B in {0,2,4,8}, dt=0.05, FP32 modes",
+            "value": work * steps / t_ens, "unit": METRIC, "ms_per_step": 1e3 * t_ens / steps,
+            "one_context_at_a_time": work * steps / t_seq, "tile_sites": info["sites"],
+            "tile_ms": info["tile_ms"], "launches_per_step": 5, "N5_finite": bool(np.all(np.isfinite(n5)))}
+
+
 # ------------------------------------------------------------ distributed --
 _dist = None
 
@@ -338,6 +393,7 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="n16")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--headline", choices=("fp40", "fp32"), default="fp40",
                     help="the FP32-class form of the headline value (the other is reported beside it)")
     ap.add_argument("--mode-group", type=int, default=0,
@@ -421,6 +477,10 @@ def main():
                            "N5": r["charges"]["N5"], "hop_variant": r["hop_variant"], "mode_group": r["mode_group"],
                            "hop_variant_ms": r["hop_variant_ms"]}
 
+    ens = None
+    if not args.no_ensemble:
+        ens = ensemble_leg(max(3, min(K, 20)), 2, device)
+
     acc = None
     if args.accuracy_steps > 0 and rank == 0:
         acc = accuracy(wl, args.accuracy_steps, 50, device)
@@ -474,6 +534,8 @@ def main():
             line["headline_vs_fp64_plain"] = value / forms["plain"]["value"]
         if acc is not None:
             line["accuracy_vs_fp64"] = acc
+        if ens is not None:
+            line["ensemble"] = ens
         if cpu is not None:
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)

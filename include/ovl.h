@@ -262,7 +262,8 @@ int ovl_ncs_update(ovl_ctx *ctx, double *delta, double *total);
 
 /* Stochastic vacuum modes in place of the complete plane-wave basis (no
  * reference counterpart): modes 2r and 2r+1 (global index) are P+ eta_r and
- * P- eta_r, divided by sqrt(total_pairs), with eta_r complex Z2 noise
+ * P- eta_r times sqrt(V / total_pairs) (the plane-wave modes have
+ * |psi(x)|^2 = 1 per site), with eta_r complex Z2 noise
  * ((+-1 +- i)/sqrt 2 per component, drawn in momentum space from `seed`) and
  * P+- the projectors on the positive- and negative-energy states of the free
  * Wilson Hamiltonian (those the plane-wave particles and antiparticles span);

@@ -252,7 +252,7 @@ class Context:
         return v.value, ms.tolist()
 
     def set_stochastic_modes(self, seed: int = 0, total_pairs: int = 0):
-        """Z2-noise vacuum modes (pairs P+ eta, P- eta / sqrt(pairs)) in place of plane waves."""
+        """Z2-noise vacuum modes (pairs sqrt(V / pairs) (P+ eta, P- eta)) in place of plane waves."""
         self._check(self._L.ovl_set_stochastic_modes(self._ctx, int(seed) & (2**64 - 1), int(total_pairs)))
 
     def tuning(self) -> tuple[int, int]:

@@ -2,14 +2,15 @@
 // the complete plane-wave basis, FermionField.cpp:145-328).
 //
 // The vacuum-subtracted mode sums of the currents are traces against
-//   S = sum_m w_m |psi_m><psi_m| = P+ - P-,
+//   S = sum_m w_m |psi_m><psi_m| = V (P+ - P-),
 // the difference of the projectors on the positive- and negative-energy
 // states of the free Wilson Hamiltonian h = i D (particles carry w = +1,
-// antiparticles w = -1).  With R noise vectors eta_r whose components are
-// independent complex Z2 numbers ((+-1 +- i)/sqrt 2: E[eta eta^+] = 1),
-//   S ~ (1/R) sum_r (P+ eta_r)(P+ eta_r)^+ - (P- eta_r)(P- eta_r)^+,
-// unbiased; so modes 2r and 2r+1 of a context are set to P+ eta_r / sqrt R and
-// P- eta_r / sqrt R.  The noise is drawn in momentum space, where P+- are 4x4
+// antiparticles w = -1; the plane waves have |psi(x)|^2 = 1 per site, hence V).
+// With R noise vectors eta_r whose components are independent complex Z2
+// numbers ((+-1 +- i)/sqrt 2: E[eta eta^+] = 1),
+//   S ~ (V/R) sum_r (P+ eta_r)(P+ eta_r)^+ - (P- eta_r)(P- eta_r)^+,
+// unbiased; so modes 2r and 2r+1 of a context are set to sqrt(V/R) P+ eta_r
+// and sqrt(V/R) P- eta_r.  The noise is drawn in momentum space, where P+- are 4x4
 // spin projectors per momentum: for unit links and a plane wave e^{ipx} u,
 //   h(p) = g0 M(p) + sum_mu g0 g_mu sin p_mu,   M(p) = (6r + 2m - 2M)/2 - sum_mu cos p_mu,
 // h(p)^2 = omega(p)^2 = M(p)^2 + sum_mu sin^2 p_mu, and P+-(p) = (1 +- h(p)/omega(p))/2
@@ -18,7 +19,7 @@
 // e^{-+ i omega dt/2} on the two parts.  A unitary inverse DFT, done as three
 // passes of one-dimensional transforms, takes the vectors to position space.
 // With Z2 noise, |eta(p)|^2 is exactly 1 per component, so the vacuum energy
-// (1/2V) sum_m w_m <psi_m, h psi_m> = (1/2V) Tr |h| is reproduced exactly by
+// (1/2V) sum_m w_m <psi_m, h psi_m> = (1/2) Tr |h| is reproduced exactly by
 // every sample.
 #include <algorithm>
 
@@ -83,7 +84,7 @@ __global__ void stochastic_fill_kernel(cpx<double> *__restrict__ out, Lattice L,
                     h[a] = mk<double>(h[a].re + s[mu] * w.re, h[a].im + s[mu] * w.im);
                 }
             }
-            // (1 +- h/omega)/2 eta / sqrt R, times e^{-+ i omega dt/2} for psimid
+            // (1 +- h/omega)/2 eta sqrt(V/R), times e^{-+ i omega dt/2} for psimid
             const double f = 0.5 * inv_sqrt_r, ho = sign / omega;
             double ph_re = 1.0, ph_im = 0.0;
             if (mid) sincos(-sign * 0.5 * omega * dt, &ph_im, &ph_re);
@@ -148,7 +149,7 @@ void launch_stochastic_modes(void *psi, void *psimid, void *psi_lo, void *psimid
                              int n_mb, int n_modes, int first_mode, double amass, double dt, uint64_t seed, int pairs,
                              double *scratch_a, double *scratch_b, int chunk_mb, cudaStream_t stream,
                              uint64_t *launches) {
-    const double inv_sqrt_r = 1.0 / std::sqrt((double)pairs);
+    const double inv_sqrt_r = std::sqrt((double)L.V / (double)pairs);  // sqrt(V / R)
     cpx<double> *a = reinterpret_cast<cpx<double> *>(scratch_a), *b = reinterpret_cast<cpx<double> *>(scratch_b);
     const int maxN = std::max(L.N0, std::max(L.N1, L.N2));
     uint64_t nl = 0;

@@ -50,3 +50,17 @@ def unit_links(N) -> np.ndarray:
 def mode_count(N, Nc: int = 2) -> int:
     """All modes of the complete plane-wave basis: 2 particle x Nc x 2 spin x V (MPI/ModePartition.cpp:19)."""
     return 4 * Nc * volume(N)
+
+
+def u1_flux(N, n_b: int) -> np.ndarray:
+    """Constant magnetic field along z with n_b flux quanta through the (x, y)
+    plane, as QED::SetConstantMagneticField (QED/QED.cpp:62-84): complex
+    [N1, N0, 2] phases of the x and y links, U_y(x, y) = exp(-2 pi i n_b x / (N0 N1)),
+    U_x = 1 except on the last x column, U_x(N0 - 1, y) = exp(2 pi i n_b y N0 / (N0 N1))."""
+    N0, N1 = int(N[0]), int(N[1])
+    x = np.arange(N0)[None, :]
+    y = np.arange(N1)[:, None]
+    u = np.ones((N1, N0, 2), np.complex128)
+    u[:, :, 1] = np.exp(-2j * np.pi * n_b * x / (N0 * N1)) * np.ones((N1, 1))
+    u[:, N0 - 1, 0] = np.exp(2j * np.pi * n_b * y[:, 0] * N0 / (N0 * N1))
+    return u

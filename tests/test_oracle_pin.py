@@ -203,3 +203,15 @@ def test_gauss_restore_matches_golden(golden_dir):
     assert 5 < n < 10000
     assert out[0] <= 1e-14
     assert rel_err(E, g["efield_restored"]) < 1e-12
+
+
+def test_u1_flux_input_matches_oracle():
+    """inputs.u1_flux (the package's restatement of QED.cpp:62-84 for bench
+    inputs) equals the oracle's phases."""
+    from overlap_b200.inputs import u1_flux
+    for N, nb in (((4, 6, 5), 3), ((8, 8, 8), 4)):
+        p = oracle_params(N)
+        out = np.zeros(4 * N[0] * N[1])
+        oracle().orc_u1_flux(C.byref(p), nb, ptr(out))
+        ref = out.view(np.complex128).reshape(N[1], N[0], 2)
+        assert np.max(np.abs(u1_flux(N, nb) - ref)) < 1e-15
