@@ -324,11 +324,13 @@ def ensemble_leg(steps, warmup, device):
         ens.step(warmup)
         ens.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ens.info()["launches"]
         a.record(stream)
         ens.step(steps)
         b.record(stream)
         b.synchronize()
         t_ens = a.elapsed_time(b) / 1e3
+        launches_per_step = (ens.info()["launches"] - l0) / steps
         # the same members, one context at a time (same stream, same kernels)
         a.record(stream)
         for _ in range(steps):
@@ -345,7 +347,31 @@ def ensemble_leg(steps, warmup, device):
                       "n_B in {0,2,4,8}, dt=0.05, FP32 modes",
             "value": work * steps / t_ens, "unit": METRIC, "ms_per_step": 1e3 * t_ens / steps,
             "one_context_at_a_time": work * steps / t_seq, "tile_sites": info["sites"],
-            "tile_ms": info["tile_ms"], "launches_per_step": 5, "N5_finite": bool(np.all(np.isfinite(n5)))}
+            "tile_ms": info["tile_ms"], "launches_per_step": launches_per_step,
+            "N5_finite": bool(np.all(np.isfinite(n5)))}
+
+
+def serving_leg(count, device):
+    """The serving configuration: Poisson arrivals (mean 20/s) of SU(2) Wilson
+    trajectory requests, N uniform over {8, 12, 16, 24}, 4096-8192 Z2
+    stochastic modes, 200-2000 steps, U(1) flux n_B in {0, 2, 4, 8}, FP32
+    modes, admitted by device memory into one continuously batched ensemble;
+    N_5, N_CS and energy streamed every 50 steps.  A fixed number of requests
+    (time-boxed: the offered load exceeds the GPU's capacity)."""
+    from overlap_b200.serve import Server, poisson_requests
+
+    reqs = poisson_requests(count, 20.0, seed=7)
+    offered = sum(r.mode_sites() * r.steps for r in reqs) / max(reqs[-1].arrival, 1e-9)
+    srv = Server(precision="fp32", device=device, tick_steps=50)
+    try:
+        m = srv.serve(reqs)
+        streamed = sum(len(r.observables) for r in srv.done)
+    finally:
+        srv.close()
+    m.update({"config": f"{count} requests, Poisson 20/s, N in {{8,12,16,24}}, 4096-8192 Z2 modes, 200-2000 steps, "
+                        "n_B in {0,2,4,8}, FP32, observables every 50 steps",
+              "offered_mode_site_updates_per_s": offered, "observations_streamed": streamed})
+    return m
 
 
 # ------------------------------------------------------------ distributed --
@@ -394,6 +420,8 @@ def main():
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="n16")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serving-requests", type=int, default=12, help="requests of the serving leg")
     ap.add_argument("--headline", choices=("fp40", "fp32"), default="fp40",
                     help="the FP32-class form of the headline value (the other is reported beside it)")
     ap.add_argument("--mode-group", type=int, default=0,
@@ -481,6 +509,10 @@ def main():
     if not args.no_ensemble:
         ens = ensemble_leg(max(3, min(K, 20)), 2, device)
 
+    srv = None
+    if not args.no_serving:
+        srv = serving_leg(args.serving_requests, device)
+
     acc = None
     if args.accuracy_steps > 0 and rank == 0:
         acc = accuracy(wl, args.accuracy_steps, 50, device)
@@ -536,6 +568,8 @@ def main():
             line["accuracy_vs_fp64"] = acc
         if ens is not None:
             line["ensemble"] = ens
+        if srv is not None:
+            line["serving"] = srv
         if cpu is not None:
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)

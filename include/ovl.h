@@ -365,6 +365,13 @@ int ovl_ensemble_member(ovl_ensemble *ens, int index, ovl_ctx **ctx);
  * 8 sites (x 32 modes) of the batched hop on the members' operator buffers and
  * keeps the faster. */
 int ovl_ensemble_step(ovl_ensemble *ens, int nsteps);
+/* Continuous batching: add a member (created on the ensemble's device and
+ * stream, same precision; *index = its position) or remove member `index`
+ * (its context is destroyed; later members move down by one).  Either makes
+ * the next step capture its graph again. */
+int ovl_ensemble_add(ovl_ensemble *ens, const ovl_params *member, int *index);
+int ovl_ensemble_remove(ovl_ensemble *ens, int index);
+int ovl_ensemble_size(const ovl_ensemble *ens);
 /* ovl_charges of every member: out[4 i + k]. */
 int ovl_ensemble_charges(ovl_ensemble *ens, double *out);
 /* Sites per tile chosen (0 before the first step), the tuning times (ms, for

@@ -66,6 +66,9 @@ SIGNATURES = {
     "ovl_ensemble_destroy": ([_ctx], C.c_int),
     "ovl_ensemble_last_error": ([_ctx], C.c_char_p),
     "ovl_ensemble_member": ([_ctx, C.c_int, C.POINTER(_ctx)], C.c_int),
+    "ovl_ensemble_add": ([_ctx, C.POINTER(ovl_params), C.POINTER(C.c_int)], C.c_int),
+    "ovl_ensemble_remove": ([_ctx, C.c_int], C.c_int),
+    "ovl_ensemble_size": ([_ctx], C.c_int),
     "ovl_ensemble_step": ([_ctx, C.c_int], C.c_int),
     "ovl_ensemble_charges": ([_ctx, _dp], C.c_int),
     "ovl_ensemble_info": ([_ctx, C.POINTER(C.c_int), _dp, C.POINTER(C.c_uint64)], C.c_int),

@@ -414,6 +414,27 @@ class Ensemble:
     def step(self, nsteps: int = 1):
         self._check(self._L.ovl_ensemble_step(self._e, int(nsteps)))
 
+    def add(self, params) -> Context:
+        """Admits a member (continuous batching); returns its Context."""
+        p = params if isinstance(params, Params) else Params(**params)
+        cp = p.to_c()
+        idx = C.c_int(0)
+        self._check(self._L.ovl_ensemble_add(self._e, C.byref(cp), C.byref(idx)))
+        h = C.c_void_p()
+        self._check(self._L.ovl_ensemble_member(self._e, idx.value, C.byref(h)))
+        m = Context._member(h, p, self)
+        self.params.append(p)
+        self.members.append(m)
+        return m
+
+    def remove(self, index: int):
+        """Retires member `index` (its context is destroyed; later members move down)."""
+        m = self.members[index]
+        self._check(self._L.ovl_ensemble_remove(self._e, int(index)))
+        m._ctx = C.c_void_p()
+        del self.members[index]
+        del self.params[index]
+
     def charges(self) -> np.ndarray:
         """[members, 4]: N_V, N_5, PS, WA of each member."""
         o = np.empty((len(self.members), 4))

@@ -27,20 +27,44 @@ __device__ __forceinline__ int find_member(const BatchMember *__restrict__ m, in
     return lo;
 }
 
-// phase 0: psi += dt D psimid; phase 1: psimid += dt D psi
-// CTAs per SM the register allocation must allow: FP32 64 registers, FP64 128.
+// CTAs per SM the register allocation must allow: FP32 64 registers, FP64 128
+// (as the single-context kernels).
 template <typename T, int SITES> struct BatchOcc {
     static constexpr int kMinBlocks = (sizeof(T) == 4 ? 1024 : 512) / (kModeBlock * SITES);
 };
 
-template <typename T, int SITES>
+constexpr int kMaxBatchLookup = 1024;  // members whose first tiles a CTA stages in shared memory
+
+// The member of tile `key`: the members' first tiles are staged in shared
+// memory (one coalesced load) and searched there.
+__device__ __forceinline__ int find_tile_member(const BatchMember *__restrict__ m, int count, long long key) {
+    __shared__ long long first[kMaxBatchLookup];
+    const int nthreads = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int n = count < kMaxBatchLookup ? count : kMaxBatchLookup;
+    for (int i = tid; i < n; i += nthreads) first[i] = m[i].tile0;
+    __syncthreads();
+    if (count > kMaxBatchLookup) return find_member(m, count, key, &BatchMember::tile0);
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (first[mid] <= key) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// phase 0: psi += dt D psimid; phase 1: psimid += dt D psi.  One launch covers
+// the members [0, count) of `members`: a group all with a U(1) background (U1)
+// or all without, tiles numbered on from the group's first member.
+template <typename T, int SITES, bool U1>
 __global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlocks)
     wilson_batch_kernel(const BatchMember *__restrict__ members, int count, int phase) {
-    const int mi = find_member(members, count, (long long)blockIdx.x, &BatchMember::tile0);
+    const long long key = (long long)blockIdx.x + members[0].tile0;
+    const int mi = find_tile_member(members, count, key);
     const BatchMember &m = members[mi];
     const Lattice L{m.N0, m.N1, m.N2, m.V};
     const int nsb = (L.V + SITES - 1) / SITES;
-    const long long local = (long long)blockIdx.x - m.tile0;
+    const long long local = key - m.tile0;
     const int mb = (int)(local / nsb);
     const int site = (int)(local % nsb) * SITES + threadIdx.y;
     if (site >= L.V) return;
@@ -49,14 +73,58 @@ __global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlo
     cpx<T> *dst = reinterpret_cast<cpx<T> *>(phase == 0 ? m.psi : m.psimid);
     const int n01 = L.N0 * L.N1;
     Spinor<T> acc;
-    if constexpr (sizeof(T) == 4) {
-        const float4 *u = reinterpret_cast<const float4 *>(m.U32);
-        if (m.u1_32) wilson_site_lk(LinksF32<true>{u, reinterpret_cast<const float2 *>(m.u1_32), n01}, src, L, site, mb, lane, (T)m.amass, acc);
-        else wilson_site_lk(LinksF32<false>{u, nullptr, n01}, src, L, site, mb, lane, (T)m.amass, acc);
-    } else {
-        if (m.u1) wilson_site_lk(LinksF64<true>{m.U, reinterpret_cast<const double2 *>(m.u1), n01}, src, L, site, mb, lane, (T)m.amass, acc);
-        else wilson_site_lk(LinksF64<false>{m.U, nullptr, n01}, src, L, site, mb, lane, (T)m.amass, acc);
+    if constexpr (sizeof(T) == 4)
+        wilson_site_lk(LinksF32<U1>{reinterpret_cast<const float4 *>(m.U32), reinterpret_cast<const float2 *>(m.u1_32),
+                                    n01},
+                       src, L, site, mb, lane, (T)m.amass, acc);
+    else
+        wilson_site_lk(LinksF64<U1>{m.U, reinterpret_cast<const double2 *>(m.u1), n01}, src, L, site, mb, lane,
+                       (T)m.amass, acc);
+    cpx<T> *out = dst + field_index(L.V, mb, site, 0, lane);
+    const T dt = (T)m.dt;
+#pragma unroll
+    for (int c = 0; c < kColours; c++)
+#pragma unroll
+        for (int a = 0; a < kSpin; a++) {
+            const cpx<T> d = finish_component(acc.c[c][a], a);
+            cpx<T> *o = out + (c * kSpin + a) * kModeBlock;
+            const cpx<T> v = ld(o);
+            st(o, v + dt * d);
+        }
+}
+
+// The same with the group's descriptors passed by value (kernel parameter
+// space, read through the constant cache: no dependent global loads before a
+// CTA knows its member).
+template <typename T, int SITES, bool U1>
+__global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlocks)
+    wilson_batch_param_kernel(const __grid_constant__ BatchGroup g, int phase) {
+    const long long key = (long long)blockIdx.x + g.m[0].tile0;
+    int lo = 0, hi = g.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (g.m[mid].tile0 <= key) lo = mid;
+        else hi = mid - 1;
     }
+    const BatchMember &m = g.m[lo];
+    const Lattice L{m.N0, m.N1, m.N2, m.V};
+    const int nsb = (L.V + SITES - 1) / SITES;
+    const long long local = key - m.tile0;
+    const int mb = (int)(local / nsb);
+    const int site = (int)(local % nsb) * SITES + threadIdx.y;
+    if (site >= L.V) return;
+    const int lane = threadIdx.x;
+    const cpx<T> *src = reinterpret_cast<const cpx<T> *>(phase == 0 ? m.psimid : m.psi);
+    cpx<T> *dst = reinterpret_cast<cpx<T> *>(phase == 0 ? m.psi : m.psimid);
+    const int n01 = L.N0 * L.N1;
+    Spinor<T> acc;
+    if constexpr (sizeof(T) == 4)
+        wilson_site_lk(LinksF32<U1>{reinterpret_cast<const float4 *>(m.U32), reinterpret_cast<const float2 *>(m.u1_32),
+                                    n01},
+                       src, L, site, mb, lane, (T)m.amass, acc);
+    else
+        wilson_site_lk(LinksF64<U1>{m.U, reinterpret_cast<const double2 *>(m.u1), n01}, src, L, site, mb, lane,
+                       (T)m.amass, acc);
     cpx<T> *out = dst + field_index(L.V, mb, site, 0, lane);
     const T dt = (T)m.dt;
 #pragma unroll
@@ -98,17 +166,42 @@ __global__ void advance_batch_kernel(const BatchMember *__restrict__ members, in
 
 long long batch_tiles(int V, int n_mb, int sites) { return (long long)((V + sites - 1) / sites) * n_mb; }
 
-template <int SITES>
+template <int SITES, bool U1>
 static void launch_hop(const BatchMember *members, int count, long long tiles, int phase, bool fp32, cudaStream_t s) {
     const dim3 block(kModeBlock, SITES);
-    if (fp32) wilson_batch_kernel<float, SITES><<<(unsigned)tiles, block, 0, s>>>(members, count, phase);
-    else wilson_batch_kernel<double, SITES><<<(unsigned)tiles, block, 0, s>>>(members, count, phase);
+    if (fp32) wilson_batch_kernel<float, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(members, count, phase);
+    else wilson_batch_kernel<double, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(members, count, phase);
 }
 
-void launch_batch_hop(const BatchMember *members, int count, long long tiles, int sites, int phase, bool fp32,
+void launch_batch_hop(const BatchMember *members, int count, long long tiles, int sites, int phase, bool fp32, bool u1,
                       cudaStream_t stream) {
-    if (sites == 4) launch_hop<4>(members, count, tiles, phase, fp32, stream);
-    else launch_hop<8>(members, count, tiles, phase, fp32, stream);
+    if (count <= 0 || tiles <= 0) return;
+    if (u1) {
+        if (sites == 4) launch_hop<4, true>(members, count, tiles, phase, fp32, stream);
+        else launch_hop<8, true>(members, count, tiles, phase, fp32, stream);
+    } else {
+        if (sites == 4) launch_hop<4, false>(members, count, tiles, phase, fp32, stream);
+        else launch_hop<8, false>(members, count, tiles, phase, fp32, stream);
+    }
+}
+
+template <int SITES, bool U1>
+static void launch_hop_param(const BatchGroup &g, long long tiles, int phase, bool fp32, cudaStream_t s) {
+    const dim3 block(kModeBlock, SITES);
+    if (fp32) wilson_batch_param_kernel<float, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(g, phase);
+    else wilson_batch_param_kernel<double, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(g, phase);
+}
+
+void launch_batch_hop_param(const BatchGroup &g, long long tiles, int sites, int phase, bool fp32, bool u1,
+                            cudaStream_t stream) {
+    if (g.count <= 0 || tiles <= 0) return;
+    if (u1) {
+        if (sites == 4) launch_hop_param<4, true>(g, tiles, phase, fp32, stream);
+        else launch_hop_param<8, true>(g, tiles, phase, fp32, stream);
+    } else {
+        if (sites == 4) launch_hop_param<4, false>(g, tiles, phase, fp32, stream);
+        else launch_hop_param<8, false>(g, tiles, phase, fp32, stream);
+    }
 }
 
 void launch_batch_links(const BatchMember *members, int count, long long total_links, cudaStream_t stream) {

@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -1359,13 +1360,16 @@ struct ovl_ensemble {
     bool fp32 = true;
     int sites = 0;  // sites per tile of the batched hop; 0 until tuned
     double tile_ms[2] = {0.0, 0.0};
-    std::vector<ovl::BatchMember> host;
+    std::vector<ovl::BatchMember> host;  // members without a U(1) background first, then those with
     ovl::BatchMember *dev = nullptr;
     int *dev_tsteps = nullptr;
+    int groups[2] = {0, 0};            // members without / with U(1)
+    long long group_tiles[2] = {0, 0};
     long long tiles = 0, links = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int graph_sites = 0;
+    std::vector<ovl::BatchMember> captured;    // descriptors the captured graph holds by value
+    std::unique_ptr<ovl::BatchGroup> param = std::make_unique<ovl::BatchGroup>();
     uint64_t launches = 0;
     std::string err;
 };
@@ -1388,10 +1392,21 @@ int ens_fail(ovl_ensemble *e, int code, const char *fmt, ...) {
 // writes each member's operator buffer instead of psi (the state is kept).
 void ens_describe(ovl_ensemble *e, int sites, bool tuning) {
     e->host.resize(e->members.size());
+    // members without a U(1) background first (one kernel instance per group)
+    std::vector<int> order;
+    for (int g = 0; g < 2; g++)
+        for (size_t i = 0; i < e->members.size(); i++)
+            if ((int)e->members[i]->u1_on == g) order.push_back((int)i);
+    e->groups[0] = e->groups[1] = 0;
+    e->group_tiles[0] = e->group_tiles[1] = 0;
     long long tile = 0, link = 0;
-    for (size_t i = 0; i < e->members.size(); i++) {
+    for (size_t k = 0; k < order.size(); k++) {
+        const int i = order[k];
         ovl_ctx *c = e->members[i];
-        ovl::BatchMember &m = e->host[i];
+        ovl::BatchMember &m = e->host[k];
+        const int g = c->u1_on ? 1 : 0;
+        e->groups[g]++;
+        e->group_tiles[g] += ovl::batch_tiles(c->L.V, c->n_mb, sites);
         m.psi = tuning ? c->aux_dst : c->psi;
         m.psimid = c->psimid;
         m.U = c->U;
@@ -1435,7 +1450,31 @@ void ens_free_graph(ovl_ensemble *e) {
     if (e->graph) cudaGraphDestroy(e->graph);
     e->exec = nullptr;
     e->graph = nullptr;
-    e->graph_sites = 0;
+    e->captured.clear();
+}
+
+bool ens_same_graph(const ovl_ensemble *e) {
+    return e->exec && e->captured.size() == e->host.size() &&
+           std::memcmp(e->captured.data(), e->host.data(), sizeof(ovl::BatchMember) * e->host.size()) == 0;
+}
+
+// The launches of one batched half step: each member group by its kernel,
+// its descriptors passed by value when they fit the parameter space (a
+// captured graph then holds them: it is recaptured when they change).
+void ens_hop(ovl_ensemble *e, int sites, int phase) {
+    int first = 0;
+    for (int g = 0; g < 2; g++) {
+        const int n = e->groups[g];
+        if (n > 0 && n <= ovl::kParamMembers) {
+            ovl::BatchGroup &bg = *e->param;
+            bg.count = n;
+            std::copy(e->host.begin() + first, e->host.begin() + first + n, bg.m);
+            ovl::launch_batch_hop_param(bg, e->group_tiles[g], sites, phase, e->fp32, g == 1, e->stream);
+        } else {
+            ovl::launch_batch_hop(e->dev + first, n, e->group_tiles[g], sites, phase, e->fp32, g == 1, e->stream);
+        }
+        first += n;
+    }
 }
 
 }  // namespace
@@ -1445,7 +1484,7 @@ extern "C" {
 int ovl_ensemble_create(const ovl_params *members, int count, ovl_ensemble **out) {
     if (!members || !out || count < 1) return ens_fail(nullptr, OVL_E_ARG, "ovl_ensemble_create: need members");
     *out = nullptr;
-    const ovl_params &p0 = members[0];
+    const ovl_params &p0 = members[0];  // sets the precision and device of the ensemble
     for (int i = 0; i < count; i++) {
         const ovl_params &p = members[i];
         if (p.fermion != OVL_FERMION_WILSON || p.form != OVL_FORM_FUSED)
@@ -1502,6 +1541,58 @@ int ovl_ensemble_destroy(ovl_ensemble *e) {
 
 const char *ovl_ensemble_last_error(const ovl_ensemble *e) { return e ? e->err.c_str() : g_ens_err.c_str(); }
 
+int ovl_ensemble_add(ovl_ensemble *e, const ovl_params *member, int *index) {
+    if (!e || !member) return OVL_E_ARG;
+    const ovl_params &p = *member;
+    if (p.fermion != OVL_FERMION_WILSON || p.form != OVL_FORM_FUSED)
+        return ens_fail(e, OVL_E_UNSUPPORTED, "ovl_ensemble_add: Wilson fermions, fused form only");
+    if ((p.precision == OVL_PREC_FP32) != e->fp32 || (p.precision != OVL_PREC_FP32 && p.precision != OVL_PREC_FP64) ||
+        p.device != e->device)
+        return ens_fail(e, OVL_E_ARG, "ovl_ensemble_add: the ensemble's precision and device");
+    if (p.backreaction != 0.0 || p.gauge_force) return ens_fail(e, OVL_E_UNSUPPORTED, "ovl_ensemble_add: no coupled evolution");
+    if (cudaSetDevice(e->device) != cudaSuccess) return ens_fail(e, OVL_E_CUDA, "ovl_ensemble_add: device");
+    ovl_params q = p;
+    q.stream = reinterpret_cast<uint64_t>(e->stream);
+    q.hop_variant = 0;
+    q.mode_group = 0;
+    ovl_ctx *c = nullptr;
+    int rc = ovl_create(&q, &c);
+    if (rc) return ens_fail(e, rc, "ovl_ensemble_add: %s", ovl_last_error(nullptr));
+    // descriptor arrays sized for the new count (the step graph bakes in
+    // their address, the count and the tiles: it is captured again)
+    ovl::BatchMember *dev = nullptr;
+    int *ts = nullptr;
+    const size_t n = e->members.size() + 1;
+    if (cudaMalloc(&dev, sizeof(ovl::BatchMember) * n) != cudaSuccess || cudaMalloc(&ts, sizeof(int) * n) != cudaSuccess) {
+        cudaGetLastError();
+        if (dev) cudaFree(dev);
+        ovl_destroy(c);
+        return ens_fail(e, OVL_E_OOM, "ovl_ensemble_add: descriptors");
+    }
+    cudaStreamSynchronize(e->stream);
+    ens_free_graph(e);
+    cudaFree(e->dev);
+    cudaFree(e->dev_tsteps);
+    e->dev = dev;
+    e->dev_tsteps = ts;
+    e->members.push_back(c);
+    if (index) *index = (int)n - 1;
+    return OVL_OK;
+}
+
+int ovl_ensemble_remove(ovl_ensemble *e, int index) {
+    if (!e || index < 0 || index >= (int)e->members.size())
+        return ens_fail(e, OVL_E_ARG, "ovl_ensemble_remove: index %d", index);
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    ens_free_graph(e);
+    ovl_destroy(e->members[index]);
+    e->members.erase(e->members.begin() + index);
+    return OVL_OK;
+}
+
+int ovl_ensemble_size(const ovl_ensemble *e) { return e ? (int)e->members.size() : 0; }
+
 int ovl_ensemble_member(ovl_ensemble *e, int index, ovl_ctx **ctx) {
     if (!e || !ctx || index < 0 || index >= (int)e->members.size())
         return ens_fail(e, OVL_E_ARG, "ovl_ensemble_member: index %d", index);
@@ -1530,7 +1621,7 @@ int ens_tune(ovl_ensemble *e) {
         float total = 0.0f;
         for (int rep = 0; rep < 4; rep++) {
             cudaEventRecord(a, e->stream);
-            ovl::launch_batch_hop(e->dev, (int)e->members.size(), e->tiles, cand[k], 0, e->fp32, e->stream);
+            ens_hop(e, cand[k], 0);
             cudaEventRecord(b, e->stream);
             cudaEventSynchronize(b);
             float t = 0.0f;
@@ -1553,9 +1644,9 @@ int ens_tune(ovl_ensemble *e) {
 // links, half step, links, step counters.
 void ens_enqueue_step(ovl_ensemble *e) {
     const int n = (int)e->members.size();
-    ovl::launch_batch_hop(e->dev, n, e->tiles, e->sites, 0, e->fp32, e->stream);
+    ens_hop(e, e->sites, 0);
     ovl::launch_batch_links(e->dev, n, e->links, e->stream);
-    ovl::launch_batch_hop(e->dev, n, e->tiles, e->sites, 1, e->fp32, e->stream);
+    ens_hop(e, e->sites, 1);
     ovl::launch_batch_links(e->dev, n, e->links, e->stream);
     ovl::launch_batch_advance(e->dev, n, e->stream);
 }
@@ -1573,7 +1664,7 @@ int ens_capture(ovl_ensemble *e) {
         ens_free_graph(e);
         return ens_fail(e, OVL_E_CUDA, "ensemble: step graph: %s", cudaGetErrorString(r));
     }
-    e->graph_sites = e->sites;
+    e->captured = e->host;
     return OVL_OK;
 }
 
@@ -1584,7 +1675,7 @@ extern "C" {
 int ovl_ensemble_step(ovl_ensemble *e, int nsteps) {
     if (!e) return OVL_E_ARG;
     if (nsteps < 0) return ens_fail(e, OVL_E_ARG, "ovl_ensemble_step: nsteps=%d", nsteps);
-    if (nsteps == 0) return OVL_OK;
+    if (nsteps == 0 || e->members.empty()) return OVL_OK;
     if (cudaSetDevice(e->device) != cudaSuccess) return ens_fail(e, OVL_E_CUDA, "ovl_ensemble_step: device");
     int rc;
     if (e->sites == 0 && (rc = ens_tune(e))) return rc;
@@ -1592,12 +1683,12 @@ int ovl_ensemble_step(ovl_ensemble *e, int nsteps) {
     // been set on the members); the captured graph reads them from device memory
     ens_describe(e, e->sites, false);
     if ((rc = ens_upload(e))) return rc;
-    if (e->graph_sites != e->sites && (rc = ens_capture(e))) return rc;
+    if (!ens_same_graph(e) && (rc = ens_capture(e))) return rc;
     for (int n = 0; n < nsteps; n++) {
         cudaError_t r = cudaGraphLaunch(e->exec, e->stream);
         if (r != cudaSuccess) return ens_fail(e, OVL_E_CUDA, "ovl_ensemble_step: graph launch: %s", cudaGetErrorString(r));
     }
-    e->launches += 5ull * nsteps;
+    e->launches += (uint64_t)(3 + (e->groups[0] > 0) * 2 + (e->groups[1] > 0) * 2) * nsteps;
     for (ovl_ctx *c : e->members) c->tsteps += nsteps;
     cudaError_t r = cudaGetLastError();
     return r == cudaSuccess ? OVL_OK : ens_fail(e, OVL_E_CUDA, "ovl_ensemble_step: %s", cudaGetErrorString(r));

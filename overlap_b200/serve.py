@@ -1,0 +1,201 @@
+"""Serving: trajectory requests arrive over time, are admitted as device
+memory frees up, and advance together in one batched ensemble (continuous
+batching: a request that arrives while others run joins the ensemble at the
+next tick, and a finished one leaves it).  Each request's observables --
+N_5, N_CS along the cooling-free path (ovl_ncs_update) and the gauge energy --
+are streamed back every `observe_every` steps.
+
+No counterpart in the reference, whose driver runs one trajectory per job
+(Simulation.cpp).  Requests are SU(2) Wilson fermions in the fused form; all
+requests of a server share its precision.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .api import Ensemble, Params
+from .inputs import random_efield, random_links, u1_flux, volume
+
+
+@dataclass
+class Request:
+    """One trajectory: lattice N, modes, physics, steps, inputs by seed."""
+    N: tuple
+    n_modes: int
+    steps: int
+    m_fermion: float = 0.05
+    dt: float = 0.05
+    n_b: int = 0                 # U(1) flux quanta (QED.cpp:62-84); 0: none
+    link_sigma: float = 0.3      # seeded random links, exp(i A.sigma/2), A ~ N(0, sigma^2)
+    e_sigma: float = 0.1         # seeded random E
+    stochastic: bool = True      # Z2 stochastic vacuum modes; False: plane waves (n_modes = 8V)
+    seed: int = 0
+    observe_every: int = 50
+    arrival: float = 0.0         # seconds after the server's start
+    # filled by the server
+    rid: int = -1
+    admitted: float = float("nan")
+    finished: float = float("nan")
+    observables: list = field(default_factory=list)  # (step, N5, N_CS, energy)
+
+    def mode_sites(self) -> int:
+        return self.n_modes * volume(self.N)
+
+
+def request_bytes(req: Request, precision: str) -> int:
+    """Device memory of a request's context: four mode fields (psi, psimid,
+    and the two operator buffers), links, E and reduction scratch."""
+    n_mb = (req.n_modes + 31) // 32
+    V = volume(req.N)
+    per_complex = {"fp64": 16, "fp32": 8, "fp40": 10}[precision]
+    return 4 * n_mb * V * 8 * 32 * per_complex + V * (96 + 72 + 48) + 64 * V * 8 + (8 << 20)
+
+
+class Server:
+    """Continuous-batching server on one GPU.
+
+    tick_steps: steps between admission rounds (shortened so that no request
+    passes an observation point or its last step inside a tick).
+    memory_bytes: device memory the requests may hold (default: 80 % of the
+    free memory at start).
+    """
+
+    def __init__(self, precision: str = "fp32", device: int = 0, tick_steps: int = 25,
+                 memory_bytes: int | None = None):
+        import torch
+
+        self.precision = precision
+        self.device = device
+        self.tick_steps = int(tick_steps)
+        if memory_bytes is None:
+            free, _ = torch.cuda.mem_get_info(device)
+            memory_bytes = int(0.8 * free)
+        self.memory_bytes = int(memory_bytes)
+        self.ensemble: Ensemble | None = None
+        self.active: list[Request] = []  # in ensemble member order
+        self.done: list[Request] = []
+        self.used_bytes = 0
+        self._next_id = 0
+
+    # ------------------------------------------------------------ members
+    def _params(self, r: Request) -> Params:
+        return Params(N=tuple(r.N), n_modes=r.n_modes, first_mode=0, precision=self.precision, form="fused",
+                      m_fermion=r.m_fermion, r_wilson=1.0, m_dw=0.0, dt=r.dt, t_sphaleron=1e300,
+                      device=self.device)
+
+    def _admit(self, r: Request, now: float):
+        p = self._params(r)
+        if self.ensemble is None:
+            self.ensemble = Ensemble([p])
+            ctx = self.ensemble[0]
+        else:
+            ctx = self.ensemble.add(p)
+        ctx.set_links(random_links(r.N, r.link_sigma, r.seed))
+        ctx.set_efield(random_efield(r.N, r.e_sigma, r.seed + 1))
+        if r.n_b:
+            ctx.set_u1(u1_flux(r.N, r.n_b))
+        if r.stochastic:
+            ctx.set_stochastic_modes(seed=r.seed + 2)
+        else:
+            ctx.set_free_fermions()
+        ctx.ncs_update()
+        r.admitted = now
+        r._step = 0
+        r._ncs = 0.0
+        self._observe(r, ctx)
+        self.active.append(r)
+        self.used_bytes += request_bytes(r, self.precision)
+
+    def _observe(self, r: Request, ctx):
+        n5 = ctx.charges()["N5"]
+        _, ncs = ctx.ncs_update()
+        energy = ctx.bulk()["T00"]
+        r.observables.append((r._step, n5, ncs, energy))
+
+    def _retire(self, i: int, now: float):
+        r = self.active.pop(i)
+        self.ensemble.remove(i)
+        r.finished = now
+        self.used_bytes -= request_bytes(r, self.precision)
+        self.done.append(r)
+
+    # ---------------------------------------------------------------- loop
+    def serve(self, requests: list[Request]) -> dict:
+        """Runs `requests` (arrival times relative to now) to completion and
+        returns latency and throughput figures.  A request larger than the
+        whole memory budget is rejected (finished = NaN, in `rejected`)."""
+        self.done = []  # figures of this call only
+        pending = sorted(requests, key=lambda r: r.arrival)
+        for r in pending:  # a request object may be served again: start it afresh
+            r.rid = self._next_id
+            self._next_id += 1
+            r.observables = []
+            r.admitted = r.finished = float("nan")
+        queue: list[Request] = []
+        rejected = []
+        t0 = time.perf_counter()
+        work = 0
+        while pending or queue or self.active:
+            now = time.perf_counter() - t0
+            while pending and pending[0].arrival <= now:
+                r = pending.pop(0)
+                if request_bytes(r, self.precision) > self.memory_bytes:
+                    rejected.append(r)
+                else:
+                    queue.append(r)
+            while queue and self.used_bytes + request_bytes(queue[0], self.precision) <= self.memory_bytes:
+                self._admit(queue.pop(0), time.perf_counter() - t0)
+            if not self.active:
+                if pending:
+                    time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - t0))))
+                continue
+            # a tick: as many steps as no active request passes an observation or its end
+            k = self.tick_steps
+            for r in self.active:
+                k = min(k, r.steps - r._step, r.observe_every - r._step % r.observe_every)
+            self.ensemble.step(k)
+            for r in self.active:
+                r._step += k
+                work += k * r.mode_sites()
+            for i in range(len(self.active) - 1, -1, -1):
+                r = self.active[i]
+                if r._step % r.observe_every == 0 or r._step == r.steps:
+                    self._observe(r, self.ensemble[i])
+            now = time.perf_counter() - t0
+            for i in range(len(self.active) - 1, -1, -1):
+                if self.active[i]._step >= self.active[i].steps:
+                    self._retire(i, now)
+        wall = time.perf_counter() - t0
+        lat = np.array([r.finished - r.arrival for r in self.done]) if self.done else np.zeros(1)
+        wait = np.array([r.admitted - r.arrival for r in self.done]) if self.done else np.zeros(1)
+        return {"requests": len(self.done), "rejected": len(rejected), "wall_s": wall,
+                "throughput": work / wall if wall > 0 else 0.0, "unit": "mode-site updates/s",
+                "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                "queue_wait_p50_s": float(np.percentile(wait, 50)), "queue_wait_p99_s": float(np.percentile(wait, 99))}
+
+    def close(self):
+        if self.ensemble is not None:
+            self.ensemble.close()
+            self.ensemble = None
+
+
+def poisson_requests(count: int, rate: float, seed: int, sizes=(8, 12, 16, 24), modes=(4096, 8192),
+                     steps=(200, 2000), observe_every: int = 50) -> list[Request]:
+    """`count` requests with exponential inter-arrival times (mean 1/rate s),
+    N uniform over `sizes`, modes uniform over [modes[0], modes[1]] in pairs,
+    steps uniform over [steps[0], steps[1]] in multiples of observe_every,
+    U(1) flux n_b uniform over {0, 2, 4, 8}."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += rng.exponential(1.0 / rate)
+        n = int(rng.choice(sizes))
+        m = int(rng.integers(modes[0] // 64, modes[1] // 64 + 1)) * 64
+        s = int(rng.integers(steps[0] // observe_every, steps[1] // observe_every + 1)) * observe_every
+        out.append(Request(N=(n, n, n), n_modes=m, steps=s, n_b=int(rng.choice((0, 2, 4, 8))),
+                           seed=1000 * i + 17, observe_every=observe_every, arrival=t))
+    return out

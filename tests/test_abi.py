@@ -104,3 +104,13 @@ def test_fp40_is_rejected_outside_the_fused_wilson_form():
     for kw in (dict(form="plain"), dict(fermion="overlap", form="fused", sign_method="chebyshev")):
         with pytest.raises(OvlError, match="FP40"):
             Context(N=(4, 4, 4), n_modes=8, precision="fp40", **kw)
+
+
+def test_poisson_requests_are_seeded_and_in_range():
+    from overlap_b200.serve import poisson_requests, request_bytes
+    a = poisson_requests(20, 20.0, seed=5)
+    b = poisson_requests(20, 20.0, seed=5)
+    assert [(r.N, r.n_modes, r.steps, r.arrival) for r in a] == [(r.N, r.n_modes, r.steps, r.arrival) for r in b]
+    assert all(r.N[0] in (8, 12, 16, 24) and 4096 <= r.n_modes <= 8192 and 200 <= r.steps <= 2000 for r in a)
+    assert all(x.arrival < y.arrival for x, y in zip(a, a[1:]))
+    assert request_bytes(a[0], "fp32") < request_bytes(a[0], "fp64")
