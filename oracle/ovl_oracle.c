@@ -840,3 +840,634 @@ int orc_gauss_restore(const orc_params *p, const double *U, double *E, int max_i
     if (out2) { out2[0] = mx; out2[1] = avg; }
     return n;
 }
+
+/* ======================================================================== */
+/* SU(3): the same operators for three colours.                             */
+/*                                                                          */
+/* The reference's fermion code is written for two colours                  */
+/* (FermionField.cpp:8-9, WilsonOperator.cpp:45-46) and its SU(3) group      */
+/* code does not build (LATTICE/GaugeLinks.cpp:46 returns the links as       */
+/* DOUBLE*, SUNc/SU3/AlgebraOperations.cpp:197 calls an undeclared           */
+/* ComplexEigensystem), so these functions restate the operators above from  */
+/* their definitions for Nc = 3:                                             */
+/*   links: 9 complex numbers per link, U_ij at i + 3j                       */
+/*          (SUNc/SU3/GroupOperations.cpp:4-12), link (site, mu) at          */
+/*          18 (mu + 3 site) doubles;                                        */
+/*   E:     8 components per link, generators t^a = lambda^a / 2             */
+/*          (SU3/AlgebraOperations.cpp:6), E[a + 8 (mu + 3 site)];           */
+/*   modes: [mode][site][colour 3][spin 4] complex.                          */
+/* With SU(2) embedded in the upper-left block (sigma_k -> lambda_k, a < 3)  */
+/* every function reproduces its SU(2) counterpart above, which is pinned to */
+/* the reference.                                                            */
+/* ======================================================================== */
+
+#define SPINOR3 12
+
+typedef struct { cplx m[3][3]; } m3;
+
+static m3 m3_load(const double *U, int s, int mu) {
+    m3 a;
+    const double *p = U + 18 * (size_t)(mu + 3 * s);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) a.m[i][j] = p[2 * (i + 3 * j)] + I * p[2 * (i + 3 * j) + 1];
+    return a;
+}
+
+static void m3_store(double *U, int s, int mu, const m3 *a) {
+    double *p = U + 18 * (size_t)(mu + 3 * s);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            p[2 * (i + 3 * j)] = creal(a->m[i][j]);
+            p[2 * (i + 3 * j) + 1] = cimag(a->m[i][j]);
+        }
+}
+
+static m3 m3_unit(void) {
+    m3 a;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) a.m[i][j] = i == j ? 1.0 : 0.0;
+    return a;
+}
+
+static m3 m3_mul(const m3 *a, const m3 *b) {
+    m3 c;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            cplx t = 0;
+            for (int k = 0; k < 3; k++) t += a->m[i][k] * b->m[k][j];
+            c.m[i][j] = t;
+        }
+    return c;
+}
+
+static m3 m3_dag(const m3 *a) {
+    m3 c;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) c.m[i][j] = conj(a->m[j][i]);
+    return c;
+}
+
+/* t^a alpha^a (MatrixForm, SU3/AlgebraOperations.cpp:89-105) */
+static m3 su3_matrix_form(const double al[8]) {
+    const double r3 = 1.0 / sqrt(3.0);
+    m3 A;
+    A.m[0][0] = 0.5 * (al[2] + al[7] * r3);
+    A.m[1][1] = -0.5 * (al[2] - al[7] * r3);
+    A.m[2][2] = -al[7] * r3;
+    A.m[1][0] = 0.5 * (al[0] + I * al[1]);
+    A.m[2][0] = 0.5 * (al[3] + I * al[4]);
+    A.m[2][1] = 0.5 * (al[5] + I * al[6]);
+    A.m[0][1] = conj(A.m[1][0]);
+    A.m[0][2] = conj(A.m[2][0]);
+    A.m[1][2] = conj(A.m[2][1]);
+    return A;
+}
+
+static m3 su3_generator(int a) {
+    double al[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    al[a] = 1.0;
+    return su3_matrix_form(al);
+}
+
+/* 2 tr(t^a V), the algebra components of a hermitian traceless V */
+static void su3_components(const m3 *V, double out[8]) {
+    for (int a = 0; a < 8; a++) {
+        m3 t = su3_generator(a);
+        cplx s = 0;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) s += t.m[i][j] * V->m[j][i];
+        out[a] = 2.0 * creal(s);
+    }
+}
+
+/* Re tr(i t^a V) (ReTrIGenU, SU3/GroupOperations.cpp:108-119) */
+static double su3_retr_ita(const m3 *V, int a) {
+    m3 t = su3_generator(a);
+    cplx s = 0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) s += t.m[i][j] * V->m[j][i];
+    return -cimag(s);
+}
+
+/* R_ab = 2 tr(t^a V t^b V^+) (GetAdjoint's definition, SU3/GroupOperations.cpp:213) */
+static void su3_adjoint(const m3 *V, double R[8][8]) {
+    m3 Vd = m3_dag(V), T[8];
+    for (int a = 0; a < 8; a++) T[a] = su3_generator(a);
+    for (int b = 0; b < 8; b++) {
+        m3 x = m3_mul(V, &T[b]);
+        m3 y = m3_mul(&x, &Vd);
+        for (int a = 0; a < 8; a++) {
+            cplx s = 0;
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) s += T[a].m[i][j] * y.m[j][i];
+            R[a][b] = 2.0 * creal(s);
+        }
+    }
+}
+
+/* Eigensystem of a hermitian 3x3 matrix by cyclic Jacobi rotations:
+ * A = Vec diag(lam) Vec^+.  Each rotation J = diag(1, e^{-i phi}) R(theta) on
+ * the (p, q) pair, a_pq = r e^{i phi}, tan 2 theta = 2 r / (a_qq - a_pp). */
+static void herm3_eigen(m3 A, double lam[3], m3 *Vec) {
+    m3 Vm = m3_unit();
+    for (int sweep = 0; sweep < 64; sweep++) {
+        double off = 0.0, diag = 0.0;
+        for (int i = 0; i < 3; i++) {
+            diag += creal(A.m[i][i]) * creal(A.m[i][i]);
+            for (int j = i + 1; j < 3; j++) off += creal(A.m[i][j] * conj(A.m[i][j]));
+        }
+        if (off <= 1e-34 * diag || off < 1e-300) break;
+        for (int p = 0; p < 2; p++)
+            for (int q = p + 1; q < 3; q++) {
+                const double r = cabs(A.m[p][q]);
+                if (r == 0.0) continue;
+                const cplx ph = A.m[p][q] / r;
+                const double th = 0.5 * atan2(2.0 * r, creal(A.m[q][q]) - creal(A.m[p][p]));
+                const double c = cos(th), s = sin(th);
+                m3 J = m3_unit();
+                J.m[p][p] = c;
+                J.m[p][q] = s;
+                J.m[q][p] = -s * conj(ph);
+                J.m[q][q] = c * conj(ph);
+                m3 Jd = m3_dag(&J);
+                m3 t = m3_mul(&A, &J);
+                A = m3_mul(&Jd, &t);
+                Vm = m3_mul(&Vm, &J);
+            }
+    }
+    for (int i = 0; i < 3; i++) lam[i] = creal(A.m[i][i]);
+    *Vec = Vm;
+}
+
+/* exp(i c t^a alpha^a) through the eigensystem of t^a alpha^a, the method of
+ * MatrixIExp (SU3/AlgebraOperations.cpp:141-183) with a Jacobi eigensolver. */
+void orc3_exp(double c, const double alpha[8], double out[18]) {
+    m3 A = su3_matrix_form(alpha), Vec, R;
+    double lam[3];
+    herm3_eigen(A, lam, &Vec);
+    for (int i = 0; i < 3; i++)
+        for (int k = 0; k < 3; k++) {
+            cplx t = 0;
+            for (int j = 0; j < 3; j++) t += Vec.m[i][j] * cexp(I * c * lam[j]) * conj(Vec.m[k][j]);
+            R.m[i][k] = t;
+        }
+    m3_store(out, 0, 0, &R);
+}
+
+/* A^a with exp(-i A^a t^a) = W for unitary W of unit determinant (MatrixILog
+ * with C = -1, SU3/AlgebraOperations.cpp:186-234): the eigenvectors of the
+ * hermitian H = (W + W^+)/2 + (W - W^+)/2i are those of W while no two of
+ * W's eigenphases add up to pi/2 (geodesics between nearby links); the
+ * phases theta_j = arg(v_j^+ W v_j) are made to sum to zero. */
+static void su3_log(const m3 *W, double out[8]) {
+    m3 Wd = m3_dag(W), H, Vec;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) H.m[i][j] = 0.5 * (W->m[i][j] + Wd.m[i][j]) - 0.5 * I * (W->m[i][j] - Wd.m[i][j]);
+    double lam[3], th[3], sum = 0.0;
+    herm3_eigen(H, lam, &Vec);
+    for (int j = 0; j < 3; j++) {
+        cplx e = 0;
+        for (int i = 0; i < 3; i++)
+            for (int k = 0; k < 3; k++) e += conj(Vec.m[i][j]) * W->m[i][k] * Vec.m[k][j];
+        th[j] = carg(e);
+        sum += th[j];
+    }
+    if (fabs(sum) > M_PI) {  /* one phase on the other branch */
+        int big = 0;
+        for (int j = 1; j < 3; j++)
+            if (fabs(th[j]) > fabs(th[big])) big = j;
+        th[big] -= sum > 0 ? 2.0 * M_PI : -2.0 * M_PI;
+        sum = th[0] + th[1] + th[2];
+    }
+    for (int j = 0; j < 3; j++) th[j] -= sum / 3.0;
+    m3 G;  /* generator of W = exp(i G); A^a t^a = -G */
+    for (int i = 0; i < 3; i++)
+        for (int k = 0; k < 3; k++) {
+            cplx t = 0;
+            for (int j = 0; j < 3; j++) t += Vec.m[i][j] * th[j] * conj(Vec.m[k][j]);
+            G.m[i][k] = -t;
+        }
+    su3_components(&G, out);
+}
+
+static void dress3(const orc_params *p, int s, int mu, m3 *m) {
+    if (!g_u1 || mu >= 2) return;
+    const int plane = s % (p->N[0] * p->N[1]);
+    const cplx ph = g_u1[2 * (mu + 2 * plane)] + I * g_u1[2 * (mu + 2 * plane) + 1];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) m->m[i][j] *= ph;
+}
+
+/* out = -i h_W phi for one three-colour mode (orc_wilson_apply with 3x3 links). */
+void orc3_wilson_apply(const orc_params *p, const double *U, const double *phi, double *out) {
+    const int V = volume(p);
+    cplx G[3][4][4];
+    mat4_scale(-I, GX, G[0]);
+    mat4_scale(-I, GY, G[1]);
+    mat4_scale(-I, GZ, G[2]);
+    const double amass = 6.0 * p->r_wilson + 2.0 * p->m_fermion - 2.0 * p->m_dw;
+    const cplx *fld = (const cplx *)phi;
+    for (int s = 0; s < V; s++) {
+        const cplx *f = fld + (size_t)SPINOR3 * s;
+        cplx acc[3][4];
+        for (int c = 0; c < 3; c++)
+            for (int a = 0; a < 4; a++) acc[c][a] = amass * f[4 * c + a];
+        for (int mu = 0; mu < 3; mu++) {
+            const int sb = shift(p, s, mu, -1);
+            m3 Mf = m3_load(U, s, mu), Mb = m3_load(U, sb, mu);
+            dress3(p, s, mu, &Mf);
+            dress3(p, sb, mu, &Mb);
+            const cplx *fp = fld + (size_t)SPINOR3 * shift(p, s, mu, +1);
+            const cplx *fm = fld + (size_t)SPINOR3 * sb;
+            cplx a[3][4], b[3][4];
+            for (int i = 0; i < 3; i++)
+                for (int al = 0; al < 4; al++) {
+                    a[i][al] = 0;
+                    b[i][al] = 0;
+                    for (int j = 0; j < 3; j++) {
+                        a[i][al] += Mf.m[i][j] * fp[4 * j + al];
+                        b[i][al] += conj(Mb.m[j][i]) * fm[4 * j + al];
+                    }
+                }
+            for (int i = 0; i < 3; i++)
+                for (int al = 0; al < 4; al++) {
+                    cplx g = 0;
+                    for (int be = 0; be < 4; be++) g += G[mu][al][be] * (a[i][be] - b[i][be]);
+                    acc[i][al] += -a[i][al] - b[i][al] + g;
+                }
+        }
+        cplx *o = (cplx *)out + (size_t)SPINOR3 * s;
+        for (int c = 0; c < 3; c++)
+            for (int a = 0; a < 4; a++) o[4 * c + a] = (a < 2 ? -0.5 * I : 0.5 * I) * acc[c][a];
+    }
+}
+
+/* U <- exp(i cU t^a E^a) U, cU = -dt_step (Dynamics.cpp:97-138). */
+void orc3_update_links(const orc_params *p, double *U, const double *E, double dt_step) {
+    const int V = volume(p);
+    for (int s = 0; s < V; s++)
+        for (int mu = 0; mu < 3; mu++) {
+            double g[18];
+            orc3_exp(-dt_step, E + 8 * (mu + 3 * s), g);
+            m3 G = m3_load(g, 0, 0), u = m3_load(U, s, mu);
+            m3 n = m3_mul(&G, &u);
+            m3_store(U, s, mu, &n);
+        }
+}
+
+static m3 m3_path(const orc_params *p, const double *U, int s, const leg *legs, int nlegs) {
+    m3 acc = m3_unit();
+    int cur = s;
+    for (int k = 0; k < nlegs; k++)
+        for (int n = 0; n < legs[k].len; n++) {
+            if (legs[k].dir > 0) {
+                m3 u = m3_load(U, cur, legs[k].mu);
+                acc = m3_mul(&acc, &u);
+                cur = shift(p, cur, legs[k].mu, +1);
+            } else {
+                cur = shift(p, cur, legs[k].mu, -1);
+                m3 u = m3_load(U, cur, legs[k].mu), ud = m3_dag(&u);
+                acc = m3_mul(&acc, &ud);
+            }
+        }
+    return acc;
+}
+
+static m3 m3_loop(const orc_params *p, const double *U, int s, int mu, int nu, int smu, int snu, int lmu, int lnu) {
+    /* the leg order of q_loop: counter-clockwise from the corner in quadrant (smu, snu) */
+    leg L4[4] = {{mu, +1, lmu}, {nu, +1, lnu}, {mu, -1, lmu}, {nu, -1, lnu}};
+    const int start = (smu > 0 && snu > 0) ? 0 : (smu < 0 && snu > 0) ? 1 : (smu < 0 && snu < 0) ? 2 : 3;
+    leg legs[4];
+    for (int k = 0; k < 4; k++) legs[k] = L4[(start + k) & 3];
+    return m3_path(p, U, s, legs, 4);
+}
+
+/* Staple force, the SU(3) form of orc_update_efield (Dynamics.cpp:145-197). */
+void orc3_update_efield(const orc_params *p, const double *U, double *E, double dt_step) {
+    const int V = volume(p);
+    const double gamma = -2.0 * dt_step;
+    double *dE = malloc(sizeof(double) * 24 * (size_t)V);
+    for (int s = 0; s < V; s++)
+        for (int mu = 0; mu < 3; mu++) {
+            double f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int nu = 0; nu < 3; nu++) {
+                if (nu == mu) continue;
+                leg up[4] = {{mu, +1, 1}, {nu, +1, 1}, {mu, -1, 1}, {nu, -1, 1}};
+                leg dn[4] = {{mu, +1, 1}, {nu, -1, 1}, {mu, -1, 1}, {nu, +1, 1}};
+                m3 a = m3_path(p, U, s, up, 4), b = m3_path(p, U, s, dn, 4);
+                for (int k = 0; k < 8; k++) f[k] += su3_retr_ita(&a, k) + su3_retr_ita(&b, k);
+            }
+            for (int k = 0; k < 8; k++) dE[k + 8 * (mu + 3 * s)] = gamma * f[k];
+        }
+    for (size_t k = 0; k < 24 * (size_t)V; k++) E[k] += dE[k];
+    free(dE);
+}
+
+static void half_step3(const orc_params *p, const double *U, const double *src, double *dst, int nmodes,
+                       double *work) {
+    const size_t per_mode = (size_t)2 * SPINOR3 * volume(p);
+    for (int m = 0; m < nmodes; m++) {
+        orc3_wilson_apply(p, U, src + per_mode * m, work);
+        double *d = dst + per_mode * m;
+        for (size_t k = 0; k < per_mode; k++) d[k] += p->dt * work[k];
+    }
+}
+
+/* The Wilson leapfrog (Update.cpp:48-79) for three colours. */
+void orc3_wilson_leapfrog(const orc_params *p, double *U, const double *E, double *psi, double *psimid, int nmodes,
+                          int *tsteps, int nsteps) {
+    double *work = malloc(sizeof(double) * 2 * SPINOR3 * (size_t)volume(p));
+    for (int n = 0; n < nsteps; n++) {
+        half_step3(p, U, psimid, psi, nmodes, work);
+        if (p->qs * (*tsteps * p->dt) < p->t_sphaleron) orc3_update_links(p, U, E, 0.5 * p->dt);
+        half_step3(p, U, psi, psimid, nmodes, work);
+        if (p->qs * (*tsteps * p->dt) < p->t_sphaleron) orc3_update_links(p, U, E, 0.5 * p->dt);
+        (*tsteps)++;
+    }
+    free(work);
+}
+
+/* Plane waves for three colours (SetFreeFermions.cpp:3-56 with Nc = 3). */
+int orc3_free_fermions(const orc_params *p, int first, int nmodes, double *psi, double *psimid) {
+    const int V = volume(p);
+    int failures = 0;
+    for (int m = 0; m < nmodes; m++) {
+        int g = first + m;
+        int particle = g % 2; g /= 2;
+        int colour = g % 3; g /= 3;
+        int spin = g % 2; g /= 2;
+        int k[3];
+        k[0] = g % p->N[0]; g /= p->N[0];
+        k[1] = g % p->N[1]; g /= p->N[1];
+        k[2] = g % p->N[2];
+        cplx u[4];
+        double omega;
+        failures += free_spinor(p, k, spin, particle, u, &omega);
+        cplx half = cexp(-0.5 * I * omega * p->dt);
+        cplx *f = (cplx *)psi + (size_t)SPINOR3 * V * m;
+        cplx *fm = (cplx *)psimid + (size_t)SPINOR3 * V * m;
+        for (int s = 0; s < V; s++) {
+            int c[3];
+            coords_of(p, s, c);
+            double arg = (k[0] * c[0]) / (double)p->N[0] + (k[1] * c[1]) / (double)p->N[1] + (k[2] * c[2]) / (double)p->N[2];
+            double th = (particle == 0 ? 2.0 : -2.0) * M_PI * arg;
+            cplx phase = cos(th) + I * sin(th);
+            for (int cc = 0; cc < 3; cc++)
+                for (int a = 0; a < 4; a++) {
+                    cplx v = cc == colour ? phase * u[a] : 0;
+                    f[SPINOR3 * s + 4 * cc + a] = v;
+                    fm[SPINOR3 * s + 4 * cc + a] = cc == colour ? v * half : 0;
+                }
+        }
+    }
+    return failures;
+}
+
+static cplx bilinear3(const cplx g[4][4], const m3 *M, const cplx *f, const cplx *h) {
+    cplx t = 0;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            const cplx mij = M ? M->m[i][j] : (i == j ? 1.0 : 0.0);
+            if (mij == 0) continue;
+            for (int a = 0; a < 4; a++)
+                for (int b = 0; b < 4; b++)
+                    if (g[a][b] != 0) t += g[a][b] * mij * conj(f[4 * i + a]) * h[4 * j + b];
+        }
+    return t;
+}
+
+/* Lattice sums of the Wilson currents (Currents.cpp:7-394 for three colours):
+ * out = {sum jV^0, N_5 = sum jA^0, sum PS, sum WA}. */
+void orc3_charges(const orc_params *p, const double *U, const double *psi, int nmodes, int first, double out[4]) {
+    const int V = volume(p);
+    cplx gV0[4][4], gA0[4][4], gPS[4][4], gAw[4][4], t[4][4];
+    mat4_mul(G0, G0, gV0);
+    mat4_mul(gV0, G5, gA0);
+    mat4_mul(G0, G5, t);
+    mat4_scale(I, t, gPS);
+    mat4_scale(-I * p->r_wilson, t, gAw);
+    double acc[4] = {0, 0, 0, 0};
+    for (int m = 0; m < nmodes; m++) {
+        const double w = ((first + m) % 2 == 0) ? 1.0 : -1.0;
+        const cplx *mode = (const cplx *)psi + (size_t)SPINOR3 * V * m;
+        for (int s = 0; s < V; s++) {
+            const cplx *f = mode + SPINOR3 * s;
+            acc[0] += w * creal(bilinear3(gV0, NULL, f, f));
+            acc[1] += w * creal(bilinear3(gA0, NULL, f, f));
+            acc[2] += w * creal(bilinear3(gPS, NULL, f, f));
+            cplx anomaly = -2.0 * 3.0 * bilinear3(gAw, NULL, f, f);
+            for (int mu = 0; mu < 3; mu++) {
+                const int sb = shift(p, s, mu, -1);
+                m3 Mf = m3_load(U, s, mu), Mb = m3_load(U, sb, mu);
+                dress3(p, s, mu, &Mf);
+                dress3(p, sb, mu, &Mb);
+                m3 Mbd = m3_dag(&Mb);
+                anomaly += bilinear3(gAw, &Mf, f, mode + SPINOR3 * shift(p, s, mu, +1)) +
+                           bilinear3(gAw, &Mbd, f, mode + SPINOR3 * sb);
+            }
+            acc[3] += w * creal(anomaly);
+        }
+    }
+    for (int k = 0; k < 4; k++) out[k] = acc[k] / (2.0 * V);
+}
+
+/* Improved E and B for three colours (ChernSimonsOperators.cpp:128-439, as
+ * improved_e / improved_b above). */
+static void improved_e3(const orc_params *p, const double *U, const double *E, int s, int mu, double out[8]) {
+    const int sp = shift(p, s, mu, +1), sm = shift(p, s, mu, -1), smm = shift(p, s, mu, -2);
+    double Rp[8][8], Rm[8][8], Rmm[8][8];
+    m3 u0 = m3_load(U, s, mu), um = m3_load(U, sm, mu), umm = m3_load(U, smm, mu);
+    m3 umd = m3_dag(&um), ummd = m3_dag(&umm), t = m3_mul(&umd, &ummd);
+    su3_adjoint(&u0, Rp);
+    su3_adjoint(&umd, Rm);
+    su3_adjoint(&t, Rmm);
+    const double *ep = E + 8 * (mu + 3 * sp), *e0 = E + 8 * (mu + 3 * s);
+    const double *em = E + 8 * (mu + 3 * sm), *emm = E + 8 * (mu + 3 * smm);
+    for (int a = 0; a < 8; a++) {
+        double v = (7.0 / 12.0) * e0[a];
+        for (int b = 0; b < 8; b++)
+            v += -(1.0 / 12.0) * Rp[a][b] * ep[b] + (7.0 / 12.0) * Rm[a][b] * em[b] - (1.0 / 12.0) * Rmm[a][b] * emm[b];
+        out[a] = v;
+    }
+}
+
+static void improved_b3(const orc_params *p, const double *U, int s, int mu, int nu, double out[8]) {
+    m3 avg;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) avg.m[i][j] = 0;
+    const int sg[4][2] = {{+1, +1}, {-1, +1}, {-1, -1}, {+1, -1}};
+    for (int q = 0; q < 4; q++) {
+        m3 box = m3_loop(p, U, s, mu, nu, sg[q][0], sg[q][1], 1, 1);
+        m3 r1 = m3_loop(p, U, s, mu, nu, sg[q][0], sg[q][1], 2, 1);
+        m3 r2 = m3_loop(p, U, s, mu, nu, sg[q][0], sg[q][1], 1, 2);
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                avg.m[i][j] += (5.0 / 12.0) * box.m[i][j] - (1.0 / 24.0) * (r1.m[i][j] + r2.m[i][j]);
+    }
+    for (int a = 0; a < 8; a++) out[a] = 2.0 * su3_retr_ita(&avg, a);
+}
+
+double orc3_ncsdot(const orc_params *p, const double *U, const double *E) {
+    const int V = volume(p);
+    const int plane[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+    double edotb = 0.0;
+    for (int s = 0; s < V; s++)
+        for (int mu = 0; mu < 3; mu++) {
+            double e[8], b[8];
+            improved_e3(p, U, E, s, mu, e);
+            improved_b3(p, U, s, plane[mu][0], plane[mu][1], b);
+            for (int a = 0; a < 8; a++) edotb += e[a] * b[a];
+        }
+    return 0.125 * edotb / (M_PI * M_PI);
+}
+
+/* Geodesic interpolation between two link sets and Delta N_CS along it with
+ * Simpson weights 1, 4, 1 (CoolingMethod.cpp:80-125, as ovl_ncs_update). */
+double orc3_delta_ncs(const orc_params *p, const double *Uold, const double *Unew) {
+    const int V = volume(p);
+    double *Umid = malloc(sizeof(double) * 54 * (size_t)V), *Emid = malloc(sizeof(double) * 24 * (size_t)V);
+    for (int s = 0; s < V; s++)
+        for (int mu = 0; mu < 3; mu++) {
+            m3 uo = m3_load(Uold, s, mu), un = m3_load(Unew, s, mu), uod = m3_dag(&uo);
+            m3 W = m3_mul(&un, &uod);
+            double *e = Emid + 8 * (mu + 3 * s), g[18];
+            su3_log(&W, e);
+            orc3_exp(-0.5, e, g);  /* exp(-i c E_mid t), c = 1/2 */
+            m3 G = m3_load(g, 0, 0), um = m3_mul(&G, &uo);
+            m3_store(Umid, s, mu, &um);
+        }
+    const double d = (4.0 * orc3_ncsdot(p, Umid, Emid) + orc3_ncsdot(p, Uold, Emid) + orc3_ncsdot(p, Unew, Emid)) / 6.0;
+    free(Umid);
+    free(Emid);
+    return d;
+}
+
+/* {T00, TXX, TYY, TZZ, E part, B part, gauss max, gauss rms, unit max, unit rms}
+ * for three colours (BulkObservables.cpp:17-152, GaussLawViolation.cpp:13-67,
+ * UnitarityViolation.cpp:13-51): B^2 = 4 Re tr(1 - U_plaq). */
+void orc3_bulk(const orc_params *p, const double *U, const double *E, double *out) {
+    const int V = volume(p);
+    const int plane[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+    double e2[3] = {0, 0, 0}, b2[3] = {0, 0, 0}, gmax = 0.0, gsum = 0.0, umax = 0.0, usum = 0.0;
+    for (int s = 0; s < V; s++) {
+        for (int mu = 0; mu < 3; mu++)
+            for (int a = 0; a < 8; a++) e2[mu] += E[a + 8 * (mu + 3 * s)] * E[a + 8 * (mu + 3 * s)];
+        for (int k = 0; k < 3; k++) {
+            m3 pl = m3_loop(p, U, s, plane[k][0], plane[k][1], +1, +1, 1, 1);
+            b2[k] += 4.0 * (3.0 - creal(pl.m[0][0] + pl.m[1][1] + pl.m[2][2]));
+        }
+        double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int mu = 0; mu < 3; mu++) {
+            const int sm = shift(p, s, mu, -1);
+            m3 um = m3_load(U, sm, mu), umd = m3_dag(&um);
+            double R[8][8];
+            su3_adjoint(&umd, R);
+            for (int a = 0; a < 8; a++) {
+                double t = E[a + 8 * (mu + 3 * s)];
+                for (int b = 0; b < 8; b++) t -= R[a][b] * E[b + 8 * (mu + 3 * sm)];
+                g[a] += t;
+            }
+        }
+        for (int a = 0; a < 8; a++) {
+            gmax = fmax(gmax, g[a]);
+            gsum += g[a] * g[a];
+        }
+        for (int mu = 0; mu < 3; mu++) {
+            m3 u = m3_load(U, s, mu), ud = m3_dag(&u), c = m3_mul(&u, &ud);
+            double n = 0.0;
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) {
+                    cplx d = c.m[i][j] - (i == j ? 1.0 : 0.0);
+                    n += creal(d * conj(d));
+                }
+            n = sqrt(n);
+            umax = fmax(umax, n);
+            usum += n * n;
+        }
+    }
+    for (int k = 0; k < 3; k++) { e2[k] /= V; b2[k] /= V; }
+    out[0] = 0.5 * (e2[0] + e2[1] + e2[2] + b2[0] + b2[1] + b2[2]);
+    out[1] = 0.5 * ((e2[1] + e2[2] + b2[1] + b2[2]) - (e2[0] + b2[0]));
+    out[2] = 0.5 * ((e2[0] + e2[2] + b2[0] + b2[2]) - (e2[1] + b2[1]));
+    out[3] = 0.5 * ((e2[0] + e2[1] + b2[0] + b2[1]) - (e2[2] + b2[2]));
+    out[4] = 0.5 * (e2[0] + e2[1] + e2[2]);
+    out[5] = 0.5 * (b2[0] + b2[1] + b2[2]);
+    out[6] = gmax;
+    out[7] = sqrt(gsum / (3.0 * V));
+    out[8] = umax;
+    out[9] = sqrt(usum / (3.0 * V));
+}
+
+/* Chebyshev coefficients of x^(-1/2) on [eps, 1] (c_0 with weight 1/2), by
+ * Chebyshev-Gauss quadrature on max(4K, 256) nodes. */
+void orc_chebyshev_coeffs(int K, double eps, double *c) {
+    const int M = 4 * K > 256 ? 4 * K : 256;
+    for (int k = 0; k <= K; k++) {
+        double s = 0.0;
+        for (int j = 0; j < M; j++) {
+            const double th = M_PI * (j + 0.5) / M;
+            const double x = 0.5 * (1.0 + eps) + 0.5 * (1.0 - eps) * cos(th);
+            s += cos(k * th) / sqrt(x);
+        }
+        c[k] = 2.0 * s / M;
+    }
+}
+
+/* The overlap evolution operator with the Chebyshev inverse square root, for
+ * three colours:  out = M [ -i g0 (1 + m/2) phi + (1 - m/2) D chi ],
+ * chi = lambda_max^(-1/2) [c_0/2 + sum_k c_k T_k(t)] phi,
+ * t = (2 h^2 / lambda_max - 1 - eps) / (1 - eps),  h^2 = -D^2  (OverlapU.cpp:188-202
+ * with the series in place of the Zolotarev solve). */
+void orc3_overlap_apply(const orc_params *p, const double *U, const double *phi, double *out, int K, double eps,
+                        double lambda_max) {
+    const size_t n = (size_t)SPINOR3 * volume(p);
+    cplx *b0 = calloc(n, sizeof(cplx)), *b1 = calloc(n, sizeof(cplx)), *b2 = calloc(n, sizeof(cplx));
+    cplx *w = malloc(n * sizeof(cplx)), *x = malloc(n * sizeof(cplx));
+    double *c = malloc(sizeof(double) * (K + 1));
+    orc_chebyshev_coeffs(K, eps, c);
+    const double a = 2.0 / ((1.0 - eps) * lambda_max), beta = -(1.0 + eps) / (1.0 - eps);
+    const double scale = 1.0 / sqrt(lambda_max);
+    const cplx *f = (const cplx *)phi;
+    for (int k = K; k >= 0; k--) {
+        /* x = t(X) b1 = a (-D^2 b1) + beta b1 */
+        orc3_wilson_apply(p, U, (const double *)b1, (double *)w);
+        orc3_wilson_apply(p, U, (const double *)w, (double *)x);
+        const double factor = k > 0 ? 2.0 : 1.0, ck = (k > 0 ? c[k] : 0.5 * c[0]) * scale;
+        for (size_t e = 0; e < n; e++) b0[e] = factor * (-a * x[e] + beta * b1[e]) - b2[e] + ck * f[e];
+        cplx *t = b2;
+        b2 = b1;
+        b1 = b0;
+        b0 = t;
+    }
+    /* chi = b1; D chi */
+    orc3_wilson_apply(p, U, (const double *)b1, (double *)w);
+    const double cp = 1.0 + 0.5 * p->m_fermion, cm = 1.0 - 0.5 * p->m_fermion;
+    cplx *o = (cplx *)out;
+    for (size_t e = 0; e < n; e++) {
+        const int spin = (int)(e % 4);
+        const cplx g = (spin < 2 ? -I : I) * cp * f[e];
+        o[e] = p->m_dw * (g + cm * w[e]);
+    }
+    free(b0); free(b1); free(b2); free(w); free(x); free(c);
+}
+
+/* The overlap leapfrog (OverlapUpdate.cpp:99-135) for three colours with the
+ * Chebyshev operator and a fixed lambda_max. */
+void orc3_overlap_leapfrog(const orc_params *p, double *U, const double *E, double *psi, double *psimid, int nmodes,
+                           int *tsteps, int nsteps, int K, double eps, double lambda_max) {
+    const size_t per_mode = (size_t)2 * SPINOR3 * volume(p);
+    double *work = malloc(sizeof(double) * per_mode);
+    for (int n = 0; n < nsteps; n++) {
+        for (int h = 0; h < 2; h++) {
+            const double *src = h == 0 ? psimid : psi;
+            double *dst = h == 0 ? psi : psimid;
+            for (int m = 0; m < nmodes; m++) {
+                orc3_overlap_apply(p, U, src + per_mode * m, work, K, eps, lambda_max);
+                for (size_t k = 0; k < per_mode; k++) dst[per_mode * m + k] += p->dt * work[k];
+            }
+            if (p->qs * (*tsteps * p->dt) < p->t_sphaleron) orc3_update_links(p, U, E, 0.5 * p->dt);
+        }
+        (*tsteps)++;
+    }
+    free(work);
+}

@@ -105,6 +105,26 @@ double orc_ritz(const orc_params *p, const double *U, const double *start, doubl
  * {signed max, rms} of the last violation computed. */
 int orc_gauss_restore(const orc_params *p, const double *U, double *E, int max_iter, double tol, double *out2);
 
+/* ---- SU(3) (three colours; no reference counterpart, see ovl_oracle.c) ----
+ * links double[V][3][9][2] (U_ij at i + 3j), E double[V][3][8],
+ * modes [mode][site][colour 3][spin 4][re, im]. */
+void orc3_exp(double c, const double alpha[8], double out[18]);
+void orc3_wilson_apply(const orc_params *p, const double *U, const double *phi, double *out);
+void orc3_update_links(const orc_params *p, double *U, const double *E, double dt_step);
+void orc3_update_efield(const orc_params *p, const double *U, double *E, double dt_step);
+void orc3_wilson_leapfrog(const orc_params *p, double *U, const double *E, double *psi, double *psimid, int nmodes,
+                          int *tsteps, int nsteps);
+int orc3_free_fermions(const orc_params *p, int first, int nmodes, double *psi, double *psimid);
+void orc3_charges(const orc_params *p, const double *U, const double *psi, int nmodes, int first, double out[4]);
+double orc3_ncsdot(const orc_params *p, const double *U, const double *E);
+double orc3_delta_ncs(const orc_params *p, const double *Uold, const double *Unew);
+void orc3_bulk(const orc_params *p, const double *U, const double *E, double *out);
+void orc_chebyshev_coeffs(int K, double eps, double *c);
+void orc3_overlap_apply(const orc_params *p, const double *U, const double *phi, double *out, int K, double eps,
+                        double lambda_max);
+void orc3_overlap_leapfrog(const orc_params *p, double *U, const double *E, double *psi, double *psimid, int nmodes,
+                           int *tsteps, int nsteps, int K, double eps, double lambda_max);
+
 #ifdef __cplusplus
 }
 #endif

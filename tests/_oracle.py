@@ -68,6 +68,23 @@ def oracle():
         L.orc_ritz.restype = C.c_double
         L.orc_coupled_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
                                            C.c_double, C.c_int]
+        L.orc3_exp.argtypes = [C.c_double, _dp, _dp]
+        L.orc3_wilson_apply.argtypes = [P, _dp, _dp, _dp]
+        L.orc3_update_links.argtypes = [P, _dp, _dp, C.c_double]
+        L.orc3_update_efield.argtypes = [P, _dp, _dp, C.c_double]
+        L.orc3_wilson_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.POINTER(C.c_int), C.c_int]
+        L.orc3_free_fermions.argtypes = [P, C.c_int, C.c_int, _dp, _dp]
+        L.orc3_free_fermions.restype = C.c_int
+        L.orc3_charges.argtypes = [P, _dp, _dp, C.c_int, C.c_int, _dp]
+        L.orc3_ncsdot.argtypes = [P, _dp, _dp]
+        L.orc3_ncsdot.restype = C.c_double
+        L.orc3_delta_ncs.argtypes = [P, _dp, _dp]
+        L.orc3_delta_ncs.restype = C.c_double
+        L.orc3_bulk.argtypes = [P, _dp, _dp, _dp]
+        L.orc_chebyshev_coeffs.argtypes = [C.c_int, C.c_double, _dp]
+        L.orc3_overlap_apply.argtypes = [P, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double]
+        L.orc3_overlap_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int,
+                                            C.c_double, C.c_double]
         _oracle = L
     return _oracle
 
