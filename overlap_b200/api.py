@@ -56,6 +56,7 @@ def _dp(a: np.ndarray):
 @dataclass
 class Params:
     N: tuple = (8, 8, 8)
+    n_colours: int = 2               # 2: SU(2) links (u0, u1, u2, u3); 3: SU(3), 9 complex per link
     n_modes: int | None = None       # default: the full basis 4*Nc*V
     first_mode: int = 0
     fermion: str = "wilson"
@@ -89,8 +90,8 @@ class Params:
         p = _lib.ovl_params()
         _lib.lib().ovl_params_init(C.byref(p))
         p.N[0], p.N[1], p.N[2] = (int(n) for n in self.N)
-        p.n_colours = 2
-        p.n_modes = int(self.n_modes if self.n_modes is not None else 8 * volume(self.N))
+        p.n_colours = int(self.n_colours)
+        p.n_modes = int(self.n_modes if self.n_modes is not None else 4 * int(self.n_colours) * volume(self.N))
         p.first_mode = int(self.first_mode)
         p.fermion = FERMIONS[self.fermion]
         p.precision = PRECISIONS[self.precision]
@@ -128,6 +129,7 @@ class Context:
         self.N = tuple(int(n) for n in self.params.N)
         self.V = volume(self.N)
         self.n_modes = cp.n_modes
+        self.nc = int(cp.n_colours)
 
     # -------------------------------------------------------------- plumbing
     def _check(self, rc: int):
@@ -150,7 +152,8 @@ class Context:
         self._owner = owner  # keeps the ensemble alive
         self.N = tuple(int(n) for n in params.N)
         self.V = volume(self.N)
-        self.n_modes = int(params.n_modes if params.n_modes is not None else 8 * self.V)
+        self.nc = int(params.n_colours)
+        self.n_modes = int(params.n_modes if params.n_modes is not None else 4 * self.nc * self.V)
         return self
 
     def __enter__(self):
@@ -173,16 +176,24 @@ class Context:
         return a
 
     # ---------------------------------------------------------------- fields
+    # Two colours: links float64[V, 3, 4] (u0, u1, u2, u3), E float64[V, 3, 3];
+    # three colours: links complex128[V, 3, 9] (U_ij at i + 3j), E float64[V, 3, 8].
     def set_links(self, U):
-        self._check(self._L.ovl_set_links(self._ctx, _dp(self._as_f64(U, (self.V, 3, 4)))))
+        if self.nc == 3:
+            U = np.ascontiguousarray(U, dtype=np.complex128).view(np.float64)
+        self._check(self._L.ovl_set_links(self._ctx, _dp(self._as_f64(U, (self.V, 3, 18 if self.nc == 3 else 4)))))
 
     def get_links(self) -> np.ndarray:
+        if self.nc == 3:
+            out = np.empty((self.V, 3, 9), np.complex128)
+            self._check(self._L.ovl_get_links(self._ctx, _dp(out.view(np.float64))))
+            return out
         out = np.empty((self.V, 3, 4))
         self._check(self._L.ovl_get_links(self._ctx, _dp(out)))
         return out
 
     def set_efield(self, E):
-        self._check(self._L.ovl_set_efield(self._ctx, _dp(self._as_f64(E, (self.V, 3, 3)))))
+        self._check(self._L.ovl_set_efield(self._ctx, _dp(self._as_f64(E, (self.V, 3, self.nc * self.nc - 1)))))
 
     def set_u1(self, u1):
         """U(1) background phases complex[N1, N0, 2] (QED::U layout), or None to remove."""
@@ -195,12 +206,12 @@ class Context:
         self._check(self._L.ovl_set_u1(self._ctx, _dp(a.view(np.float64))))
 
     def get_efield(self) -> np.ndarray:
-        out = np.empty((self.V, 3, 3))
+        out = np.empty((self.V, 3, self.nc * self.nc - 1))
         self._check(self._L.ovl_get_efield(self._ctx, _dp(out)))
         return out
 
     def set_modes(self, psi=None, psimid=None, first: int = 0):
-        """psi / psimid: complex128[count, V, 2, 4] in the reference layout."""
+        """psi / psimid: complex128[count, V, Nc, 4] in the reference layout."""
         arrs = []
         count = None
         for a in (psi, psimid):
@@ -209,8 +220,8 @@ class Context:
                 continue
             a = np.ascontiguousarray(a, dtype=np.complex128)
             count = a.shape[0]
-            if a.size != count * self.V * 8:
-                raise ValueError("modes must be complex[count, V, 2, 4]")
+            if a.size != count * self.V * 4 * self.nc:
+                raise ValueError(f"modes must be complex[count, V, {self.nc}, 4]")
             arrs.append(a)
         if count is None:
             return
@@ -219,7 +230,7 @@ class Context:
 
     def get_modes(self, first: int = 0, count: int | None = None):
         count = self.n_modes - first if count is None else count
-        psi = np.empty((count, self.V, 2, 4), np.complex128)
+        psi = np.empty((count, self.V, self.nc, 4), np.complex128)
         mid = np.empty_like(psi)
         self._check(self._L.ovl_get_modes(self._ctx, first, count, _dp(psi.view(np.float64)), _dp(mid.view(np.float64))))
         return psi, mid
@@ -237,7 +248,7 @@ class Context:
         self._check(self._L.ovl_set_spectral_bounds(self._ctx, _dp(a), a.shape[0]))
 
     def apply(self, phi) -> np.ndarray:
-        """-i h phi (Wilson or overlap) for modes complex[count, V, 2, 4]."""
+        """-i h phi (Wilson or overlap) for modes complex[count, V, Nc, 4]."""
         a = np.ascontiguousarray(phi, dtype=np.complex128)
         out = np.empty_like(a)
         self._check(self._L.ovl_apply(self._ctx, a.shape[0], _dp(a.view(np.float64)), _dp(out.view(np.float64))))

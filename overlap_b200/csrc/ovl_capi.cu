@@ -19,6 +19,10 @@ using ovl::Lattice;
 
 struct ovl_ctx {
     ovl_params p{};
+    int nc = 2;                   // colours: 2 (quaternion links) or 3 (3x3 complex links)
+    int comp = 8;                 // complex components per mode and site (4 nc)
+    int link_doubles = 4;         // doubles per link
+    int e_comp = 3;               // E components per link (nc^2 - 1)
     Lattice L{};
     int n_mb = 0;                 // mode blocks of 32
     size_t field_complex = 0;     // complex numbers per mode field
@@ -152,6 +156,30 @@ double amass(const ovl_params &p) { return 6.0 * p.r_wilson + 2.0 * p.m_fermion 
 
 bool overlap(const ovl_ctx *c) { return c->p.fermion == OVL_FERMION_OVERLAP; }
 
+bool su3(const ovl_ctx *c) { return c->nc == 3; }
+
+ovl::Su3Links su3_links(const ovl_ctx *c) {
+    ovl::Su3Links lk;
+    lk.U = c->U;
+    lk.u1 = c->u1_on ? c->u1 : nullptr;
+    lk.U32 = c->U32;
+    lk.u1_32 = c->u1_on ? c->u1_32 : nullptr;
+    return lk;
+}
+
+// The link update of either colour count (Dynamics.cpp:97-138).
+void launch_links(ovl_ctx *c, double *U, float *U32, double dt_step) {
+    if (su3(c)) ovl::su3_launch_update_links(U, c->E, c->L, dt_step, U32, c->p.reunitarize != 0, c->stream);
+    else ovl::launch_update_links(U, c->E, c->L, dt_step, c->stream, U32, c->p.reunitarize != 0);
+}
+
+// Upper bound on h_W^2 for any gauge field: ||h_W|| <= |6r + 2m - 2M| / 2 + 3
+// (the hopping term is a sum of three operators of norm one).
+double wilson_norm_bound2(const ovl_params &p) {
+    const double b = 0.5 * std::fabs(amass(p)) + 3.0;
+    return b * b;
+}
+
 // Zolotarev coefficients for the next overlap application; `consume` advances
 // the bounds schedule (OverlapUpdate.cpp:105,119 recompute the bounds before
 // every half step).
@@ -195,6 +223,11 @@ int ritz_bounds(ovl_ctx *c, const double *start, double out[2], double raw[2], i
 // ritz_auto, fresh Ritz bounds (OverlapUpdate.cpp:105,119 compute them before
 // every half step).  `consume` advances the schedule.
 int take_bounds(ovl_ctx *c, bool consume, double &lo, double &hi) {
+    if (c->bounds.empty() && su3(c)) {  // the series on [eps, 1] of h^2 / bound
+        hi = wilson_norm_bound2(c->p);
+        lo = c->p.cheb_eps * hi;
+        return OVL_OK;
+    }
     if (c->bounds.empty()) {
         if (!c->p.ritz_auto) return fail(c, OVL_E_STATE, "overlap: no spectral bounds set (ovl_set_spectral_bounds)");
         double b[2];
@@ -235,7 +268,15 @@ int run_overlap(ovl_ctx *c, const void *src, void *dst, int n_mb, int n_modes, b
         if (rc) return rc;
         ProfScope ps(c, OVL_PROF_HOP);
         uint64_t nl = 0;
-        if (fp32(c))
+        if (su3(c) && fp32(c))
+            ovl::su3_chebyshev_apply<float>(c->cw, su3_links(c), src, dst, c->L, n_mb, c->cheb.data(), c->p.cheb_degree,
+                                            c->p.cheb_eps, hi, amass(c->p), c->p.m_dw, c->p.m_fermion, c->p.dt,
+                                            accumulate, c->sm_count, c->stream, &nl);
+        else if (su3(c))
+            ovl::su3_chebyshev_apply<double>(c->cw, su3_links(c), src, dst, c->L, n_mb, c->cheb.data(),
+                                             c->p.cheb_degree, c->p.cheb_eps, hi, amass(c->p), c->p.m_dw,
+                                             c->p.m_fermion, c->p.dt, accumulate, c->sm_count, c->stream, &nl);
+        else if (fp32(c))
             ovl::chebyshev_apply<float>(c->cw, c->U, c->u1_on ? c->u1 : nullptr, src, dst, c->L, n_mb, c->cheb.data(),
                                         c->p.cheb_degree, c->p.cheb_eps, hi, amass(c->p), c->p.m_dw, c->p.m_fermion,
                                         c->p.dt, accumulate, c->sm_count, c->stream, &nl);
@@ -270,7 +311,8 @@ ovl::HopConfig hop_config(const ovl_ctx *c) {
 
 void refresh_links32(ovl_ctx *c) {
     if (c->U32) {
-        ovl::launch_links_to_f32(c->U, c->U32, (size_t)12 * c->L.V, c->stream);
+        if (su3(c)) ovl::su3_launch_links_to_f32(c->U, c->U32, c->L, c->stream);
+        else ovl::launch_links_to_f32(c->U, c->U32, (size_t)12 * c->L.V, c->stream);
         c->launches++;
     }
 }
@@ -389,10 +431,42 @@ int autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
     return rc;
 }
 
+// The three-colour half step: fused (dst += dt D src in one pass) or plain
+// (D src into the derivative buffer chunk by chunk, then the axpy).
+int su3_half_step(ovl_ctx *c, const void *src, void *dst) {
+    const ovl::Su3Links lk = su3_links(c);
+    const Lattice &L = c->L;
+    if (c->p.form == OVL_FORM_FUSED) {
+        ProfScope ps(c, OVL_PROF_HOP);
+        if (fp32(c)) ovl::su3_launch_hop<float>(lk, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        else ovl::su3_launch_hop<double>(lk, src, dst, L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        return launched(c, 1, "wilson (fused, three colours)");
+    }
+    const size_t block_complex = (size_t)L.V * c->comp * ovl::kModeBlock;
+    int n = 0;
+    for (int mb = 0; mb < c->n_mb; mb += c->deriv_mb) {
+        const int nmb = std::min(c->deriv_mb, c->n_mb - mb);
+        char *d = static_cast<char *>(dst) + block_complex * c->elem_bytes * (size_t)mb;
+        {
+            ProfScope ps(c, OVL_PROF_HOP);
+            if (fp32(c)) ovl::su3_launch_hop<float>(lk, src, c->deriv, L, mb, nmb, amass(c->p), 0.0, false, c->stream);
+            else ovl::su3_launch_hop<double>(lk, src, c->deriv, L, mb, nmb, amass(c->p), 0.0, false, c->stream);
+        }
+        {
+            ProfScope ps(c, OVL_PROF_AXPY);
+            if (fp32(c)) ovl::launch_axpy<float>(d, c->deriv, block_complex * nmb, c->p.dt, c->sm_count, c->stream);
+            else ovl::launch_axpy<double>(d, c->deriv, block_complex * nmb, c->p.dt, c->sm_count, c->stream);
+        }
+        n += 2;
+    }
+    return launched(c, n, "wilson (plain, three colours)");
+}
+
 // psi_dst += dt * D psi_src over all modes (one Update.cpp half step).
 int half_step(ovl_ctx *c, const void *src, void *dst) {
     const Lattice &L = c->L;
     if (overlap(c)) return run_overlap(c, src, dst, c->n_mb, c->p.n_modes, true, true);
+    if (su3(c)) return su3_half_step(c, src, dst);
     if (c->hop_variant < 0) {
         int rc = autotune(c, nullptr);
         if (rc) return rc;
@@ -435,9 +509,12 @@ int run_currents(ovl_ctx *c) {
         if (rc) return rc;
         ProfScope ps(c, OVL_PROF_OBS);
         ovl::launch_overlap_currents(c->psi, c->aux_dst, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->partial,
-                                     c->per_site, c->stream);
+                                     c->per_site, c->stream, fp32(c), c->nc);
         return launched(c, 2, "overlap currents");
     }
+    if (su3(c))
+        return fail(c, OVL_E_UNSUPPORTED, "ovl_currents: per-site Wilson currents are built for two colours "
+                                          "(ovl_charges gives the lattice sums for three)");
     ProfScope ps(c, OVL_PROF_OBS);
     if (fp40(c))
         ovl::launch_currents40(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->psi_lo, c->L, c->n_mb, c->p.n_modes,
@@ -498,7 +575,19 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     *out = nullptr;
     for (int i = 0; i < 3; i++)
         if (p->N[i] < 3 || p->N[i] > 1024) return fail(nullptr, OVL_E_ARG, "ovl_create: N[%d]=%d outside [3, 1024]", i, p->N[i]);
-    if (p->n_colours != 2) return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: n_colours=%d not built (SU(2) only)", p->n_colours);
+    if (p->n_colours != 2 && p->n_colours != 3)
+        return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: n_colours=%d (2 or 3)", p->n_colours);
+    if (p->n_colours == 3) {
+        if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method != OVL_SIGN_CHEBYSHEV)
+            return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: three-colour overlap fermions use the Chebyshev sign function");
+        if (p->precision == OVL_PREC_FP40)
+            return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: FP40 storage is built for two colours");
+        if (p->backreaction != 0.0)
+            return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: fermion back-reaction is built for two colours");
+        if (p->ritz_auto)
+            return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: three colours take spectral bounds from "
+                                                    "ovl_set_spectral_bounds or the analytic bound, not ritz_auto");
+    }
     if (p->fermion != OVL_FERMION_WILSON && p->fermion != OVL_FERMION_OVERLAP)
         return fail(nullptr, OVL_E_ARG, "ovl_create: fermion kind %d", p->fermion);
     if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method != OVL_SIGN_ZOLOTAREV && p->sign_method != OVL_SIGN_CHEBYSHEV)
@@ -531,10 +620,15 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     ovl_ctx *c = new (std::nothrow) ovl_ctx();
     if (!c) return fail(nullptr, OVL_E_OOM, "ovl_create: host allocation failed");
     c->p = *p;
+    c->nc = p->n_colours;
+    c->comp = 4 * c->nc;
+    c->link_doubles = c->nc == 3 ? 18 : 4;
+    c->e_comp = c->nc == 3 ? 8 : 3;
     c->L = Lattice{p->N[0], p->N[1], p->N[2], (int)V};
     c->n_mb = (p->n_modes + ovl::kModeBlock - 1) / ovl::kModeBlock;
     c->elem_bytes = p->precision == OVL_PREC_FP64 ? 16 : 8;  // FP40: the 32-bit high words
-    c->field_complex = (size_t)c->n_mb * V * ovl::kComp * ovl::kModeBlock;
+    c->field_complex = (size_t)c->n_mb * V * c->comp * ovl::kModeBlock;
+    const size_t n_link = (size_t)c->link_doubles * 3 * V, n_e = (size_t)c->e_comp * 3 * V;
     int rc = OVL_OK;
     auto bail = [&](int code) { g_err = c->err; ovl_destroy(c); return code; };
     if ((rc = set_device(c)) != OVL_OK) return bail(rc);
@@ -562,19 +656,20 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
             return bail(rc);
     }
     if ((rc = alloc(&c->psi, field_bytes, "Psi")) || (rc = alloc(&c->psimid, field_bytes, "PsiMid")) ||
-        (rc = alloc((void **)&c->U, sizeof(double) * 12 * V, "links")) ||
-        (rc = alloc((void **)&c->E, sizeof(double) * 9 * V, "efield")))
+        (rc = alloc((void **)&c->U, sizeof(double) * n_link, "links")) ||
+        (rc = alloc((void **)&c->E, sizeof(double) * n_e, "efield")))
         return bail(rc);
     if (p->form == OVL_FORM_PLAIN) {
         int chunk = p->plain_chunk_modes > 0 ? p->plain_chunk_modes : p->n_modes;
         c->deriv_mb = std::min(c->n_mb, (chunk + ovl::kModeBlock - 1) / ovl::kModeBlock);
-        if ((rc = alloc(&c->deriv, (size_t)c->deriv_mb * V * ovl::kComp * ovl::kModeBlock * c->elem_bytes, "derivative buffer")))
+        if ((rc = alloc(&c->deriv, (size_t)c->deriv_mb * V * c->comp * ovl::kModeBlock * c->elem_bytes, "derivative buffer")))
             return bail(rc);
     }
     c->partial_doubles = std::max({ovl::currents_partial_doubles(c->L, c->n_mb), ovl::ncsdot_partial_doubles(c->L),
                                    ovl::bulk_partial_doubles(c->L), ovl::charges_partial_doubles(c->L, c->n_mb),
                                    ovl::force_partial_doubles(c->L, c->n_mb), ovl::energy_partial_doubles(),
-                                   ovl::gauss_partial_doubles(c->L)});
+                                   ovl::gauss_partial_doubles(c->L), ovl::su3_charges_partial_doubles(c->L, c->n_mb),
+                                   ovl::su3_reduce_partial_doubles(c->L)});
     if ((rc = alloc((void **)&c->partial, sizeof(double) * c->partial_doubles, "reduction scratch")) ||
         (rc = alloc((void **)&c->per_site, sizeof(double) * ovl::kCurrentsPerSite * V, "currents")) ||
         (rc = alloc((void **)&c->dev_small, sizeof(double) * 64, "results")) ||
@@ -584,11 +679,11 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
         return bail(fail(c, OVL_E_OOM, "ovl_create: pinned host allocation failed"));
     if ((rc = alloc(&c->aux_src, field_bytes, "operator input")) || (rc = alloc(&c->aux_dst, field_bytes, "operator output")))
         return bail(rc);
-    if (p->precision == OVL_PREC_FP32 && (rc = alloc((void **)&c->U32, sizeof(float) * 12 * V, "FP32 links")))
+    if (p->precision == OVL_PREC_FP32 && (rc = alloc((void **)&c->U32, sizeof(float) * n_link, "FP32 links")))
         return bail(rc);
-    c->hop_variant = p->hop_variant;
-    // grouping applies to the fused Wilson form; fixed when the variant is fixed
-    if (p->form != OVL_FORM_FUSED || p->fermion != OVL_FERMION_WILSON) c->mode_group = 0;
+    c->hop_variant = c->nc == 3 ? 0 : p->hop_variant;  // one three-colour kernel: nothing to tune
+    // grouping applies to the fused two-colour Wilson form; fixed when the variant is fixed
+    if (p->form != OVL_FORM_FUSED || p->fermion != OVL_FERMION_WILSON || c->nc == 3) c->mode_group = 0;
     else c->mode_group = p->mode_group;
     if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method == OVL_SIGN_CHEBYSHEV) {
         ovl::ChebyshevWork &w = c->cw;
@@ -619,11 +714,14 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     }
     cudaMemsetAsync(c->psi, 0, field_bytes, c->stream);
     cudaMemsetAsync(c->psimid, 0, field_bytes, c->stream);
-    cudaMemsetAsync(c->E, 0, sizeof(double) * 9 * V, c->stream);
+    cudaMemsetAsync(c->E, 0, sizeof(double) * n_e, c->stream);
     // links start at the identity (GaugeLinks::SetIdentity)
-    std::vector<double> unit(12 * V, 0.0);
-    for (long long l = 0; l < 3 * V; l++) unit[4 * l + 3] = 1.0;
-    cudaMemcpyAsync(c->U, unit.data(), sizeof(double) * 12 * V, cudaMemcpyHostToDevice, c->stream);
+    std::vector<double> unit(n_link, 0.0);
+    for (long long l = 0; l < 3 * V; l++) {
+        if (c->nc == 3) unit[18 * l] = unit[18 * l + 8] = unit[18 * l + 16] = 1.0;  // U_ii at 2 (i + 3 i)
+        else unit[4 * l + 3] = 1.0;
+    }
+    cudaMemcpyAsync(c->U, unit.data(), sizeof(double) * n_link, cudaMemcpyHostToDevice, c->stream);
     refresh_links32(c);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(c, OVL_E_CUDA, "ovl_create: initialisation failed"));
     *out = c;
@@ -656,7 +754,7 @@ const char *ovl_last_error(const ovl_ctx *c) { return c ? c->err.c_str() : g_err
 
 int ovl_set_links(ovl_ctx *c, const double *links) {
     if (!c || !links) return fail(c, OVL_E_ARG, "ovl_set_links: null argument");
-    const size_t n = (size_t)12 * c->L.V;
+    const size_t n = (size_t)c->link_doubles * 3 * c->L.V;
     if (!all_finite(links, n)) return fail(c, OVL_E_NONFINITE, "ovl_set_links: non-finite link component");
     int rc = set_device(c);
     if (rc) return rc;
@@ -670,14 +768,15 @@ int ovl_get_links(ovl_ctx *c, double *links) {
     if (!c || !links) return fail(c, OVL_E_ARG, "ovl_get_links: null argument");
     int rc = set_device(c);
     if (rc) return rc;
-    OVL_CUDA(c, cudaMemcpyAsync(links, c->U, sizeof(double) * 12 * c->L.V, cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaMemcpyAsync(links, c->U, sizeof(double) * c->link_doubles * 3 * c->L.V, cudaMemcpyDeviceToHost,
+                                c->stream));
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     return OVL_OK;
 }
 
 int ovl_set_efield(ovl_ctx *c, const double *efield) {
     if (!c || !efield) return fail(c, OVL_E_ARG, "ovl_set_efield: null argument");
-    const size_t n = (size_t)9 * c->L.V;
+    const size_t n = (size_t)c->e_comp * 3 * c->L.V;
     if (!all_finite(efield, n)) return fail(c, OVL_E_NONFINITE, "ovl_set_efield: non-finite field component");
     int rc = set_device(c);
     if (rc) return rc;
@@ -718,7 +817,8 @@ int ovl_get_efield(ovl_ctx *c, double *efield) {
     if (!c || !efield) return fail(c, OVL_E_ARG, "ovl_get_efield: null argument");
     int rc = set_device(c);
     if (rc) return rc;
-    OVL_CUDA(c, cudaMemcpyAsync(efield, c->E, sizeof(double) * 9 * c->L.V, cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaMemcpyAsync(efield, c->E, sizeof(double) * c->e_comp * 3 * c->L.V, cudaMemcpyDeviceToHost,
+                                c->stream));
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     return OVL_OK;
 }
@@ -733,7 +833,7 @@ static int transfer_modes(ovl_ctx *c, int first, int count, const double *hpsi, 
     if (count == 0) return OVL_OK;
     int rc = set_device(c);
     if (rc) return rc;
-    const size_t per_mode = (size_t)c->L.V * ovl::kComp * 2;  // doubles
+    const size_t per_mode = (size_t)c->L.V * c->comp * 2;  // doubles
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)count, ((size_t)256 << 20) / (per_mode * 8)));
     double *stage = nullptr;
     if (cudaMalloc(&stage, per_mode * 8 * chunk) != cudaSuccess) {
@@ -752,12 +852,12 @@ static int transfer_modes(ovl_ctx *c, int first, int count, const double *hpsi, 
             if (upload) {
                 cudaError_t e = cudaMemcpyAsync(stage, hin + off, per_mode * 8 * n, cudaMemcpyHostToDevice, c->stream);
                 if (e != cudaSuccess) { status = cuda_fail(c, e, "mode upload"); break; }
-                if (fp32(c)) ovl::launch_ref_to_blocks<float>(stage, field, c->L, m, n, c->stream);
-                else ovl::launch_ref_to_blocks<double>(stage, field, c->L, m, n, c->stream, lo_of(c, field));
+                if (fp32(c)) ovl::launch_ref_to_blocks<float>(stage, field, c->L, m, n, c->stream, nullptr, c->nc);
+                else ovl::launch_ref_to_blocks<double>(stage, field, c->L, m, n, c->stream, lo_of(c, field), c->nc);
                 status = launched(c, 1, "ref_to_blocks");
             } else {
-                if (fp32(c)) ovl::launch_blocks_to_ref<float>(field, stage, c->L, m, n, c->stream);
-                else ovl::launch_blocks_to_ref<double>(field, stage, c->L, m, n, c->stream, lo_of(c, field));
+                if (fp32(c)) ovl::launch_blocks_to_ref<float>(field, stage, c->L, m, n, c->stream, nullptr, c->nc);
+                else ovl::launch_blocks_to_ref<double>(field, stage, c->L, m, n, c->stream, lo_of(c, field), c->nc);
                 status = launched(c, 1, "blocks_to_ref");
                 if (status) break;
                 cudaError_t e = cudaMemcpyAsync(hout + off, stage, per_mode * 8 * n, cudaMemcpyDeviceToHost, c->stream);
@@ -793,7 +893,7 @@ int ovl_set_stochastic_modes(ovl_ctx *c, uint64_t seed, int total_pairs) {
     int rc = set_device(c);
     if (rc) return rc;
     const int chunk = std::min(c->n_mb, 64);
-    const size_t bytes = sizeof(double) * 2 * (size_t)chunk * c->L.V * ovl::kComp * ovl::kModeBlock;
+    const size_t bytes = sizeof(double) * 2 * (size_t)chunk * c->L.V * c->comp * ovl::kModeBlock;
     double *a = nullptr, *b = nullptr;
     if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -803,7 +903,8 @@ int ovl_set_stochastic_modes(ovl_ctx *c, uint64_t seed, int total_pairs) {
     const int kind = fp40(c) ? 2 : fp32(c) ? 1 : 0;
     uint64_t nl = 0;
     ovl::launch_stochastic_modes(c->psi, c->psimid, c->psi_lo, c->psimid_lo, kind, c->L, c->n_mb, c->p.n_modes,
-                                 c->p.first_mode, amass(c->p), c->p.dt, seed, total_pairs, a, b, chunk, c->stream, &nl);
+                                 c->p.first_mode, amass(c->p), c->p.dt, seed, total_pairs, a, b, chunk, c->stream, &nl,
+                                 c->nc);
     rc = launched(c, (int)nl, "stochastic modes");
     cudaError_t e = cudaStreamSynchronize(c->stream);
     cudaFree(a);
@@ -819,10 +920,11 @@ int ovl_set_free_fermions(ovl_ctx *c, int *n_bad) {
     if (rc) return rc;
     if (fp32(c))
         ovl::launch_free_fermions<float>(c->psi, c->psimid, c->L, c->p.n_modes, c->n_mb, c->p.first_mode, c->p.r_wilson,
-                                         c->p.m_fermion, c->p.dt, c->dev_int, c->stream);
+                                         c->p.m_fermion, c->p.dt, c->dev_int, c->stream, nullptr, nullptr, c->nc);
     else  // FP64, or FP40 (the extension arrays set)
         ovl::launch_free_fermions<double>(c->psi, c->psimid, c->L, c->p.n_modes, c->n_mb, c->p.first_mode, c->p.r_wilson,
-                                          c->p.m_fermion, c->p.dt, c->dev_int, c->stream, c->psi_lo, c->psimid_lo);
+                                          c->p.m_fermion, c->p.dt, c->dev_int, c->stream, c->psi_lo, c->psimid_lo,
+                                          c->nc);
     if ((rc = launched(c, 2, "free fermions"))) return rc;
     int bad = 0;
     OVL_CUDA(c, cudaMemcpyAsync(&bad, c->dev_int, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -837,7 +939,8 @@ int coupled_efield(ovl_ctx *c) {
     if (c->p.gauge_force) {
         {
             ProfScope ps(c, OVL_PROF_LINKS);
-            ovl::launch_update_efield(c->U, c->E, nullptr, c->L, c->p.dt, c->stream);
+            if (su3(c)) ovl::su3_launch_update_efield(c->U, c->E, c->L, c->p.dt, c->stream);
+            else ovl::launch_update_efield(c->U, c->E, nullptr, c->L, c->p.dt, c->stream);
         }
         int rc = launched(c, 1, "gauge force");
         if (rc) return rc;
@@ -914,7 +1017,7 @@ int ovl_step(ovl_ctx *c, int nsteps) {
     if (nsteps < 0) return fail(c, OVL_E_ARG, "ovl_step: nsteps=%d", nsteps);
     int rc = set_device(c);
     if (rc) return rc;
-    if (!overlap(c) && c->p.form == OVL_FORM_FUSED && nsteps > 0) {
+    if (!overlap(c) && !su3(c) && c->p.form == OVL_FORM_FUSED && nsteps > 0) {
         if (c->hop_variant < 0) rc = autotune(c, nullptr);
         else if (c->mode_group < 0) rc = autotune_groups(c);
         if (rc) return rc;
@@ -931,7 +1034,7 @@ int ovl_step(ovl_ctx *c, int nsteps) {
         if (move) {
             {
                 ProfScope ps(c, OVL_PROF_LINKS);
-                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream, c->U32, c->p.reunitarize != 0);
+                launch_links(c, c->U, c->U32, 0.5 * c->p.dt);
             }
             if ((rc = launched(c, 1, "update links"))) return rc;
         }
@@ -939,7 +1042,7 @@ int ovl_step(ovl_ctx *c, int nsteps) {
         if (move) {
             {
                 ProfScope ps(c, OVL_PROF_LINKS);
-                ovl::launch_update_links(c->U, c->E, c->L, 0.5 * c->p.dt, c->stream, c->U32, c->p.reunitarize != 0);
+                launch_links(c, c->U, c->U32, 0.5 * c->p.dt);
             }
             if ((rc = launched(c, 1, "update links"))) return rc;
         }
@@ -992,6 +1095,14 @@ int ovl_charges(ovl_ctx *c, double out[4]) {
         if ((rc = run_currents(c))) return rc;
         ovl::launch_site_sums(c->per_site, c->L, c->partial, c->dev_small, c->stream);
         if ((rc = launched(c, 1, "site sums"))) return rc;
+    } else if (su3(c)) {
+        ProfScope ps(c, OVL_PROF_OBS);
+        if (fp32(c))
+            ovl::su3_launch_charges<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
+                                           c->p.first_mode, c->p.r_wilson, c->partial, c->dev_small, c->stream);
+        else
+            ovl::su3_launch_charges<double>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
+                                            c->p.first_mode, c->p.r_wilson, c->partial, c->dev_small, c->stream);
     } else {
         ProfScope ps(c, OVL_PROF_OBS);
         if (fp40(c))
@@ -1015,7 +1126,8 @@ int ovl_ncsdot(ovl_ctx *c, double *out) {
     if (!c || !out) return OVL_E_ARG;
     int rc = set_device(c);
     if (rc) return rc;
-    ovl::launch_ncsdot(c->U, c->E, c->L, c->partial, c->dev_small, c->stream);
+    if (su3(c)) ovl::su3_launch_ncsdot(c->U, c->E, c->L, c->partial, c->dev_small, c->stream);
+    else ovl::launch_ncsdot(c->U, c->E, c->L, c->partial, c->dev_small, c->stream);
     if ((rc = launched(c, 2, "ncsdot"))) return rc;
     OVL_CUDA(c, cudaMemcpyAsync(c->host_small, c->dev_small, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1029,9 +1141,9 @@ int ovl_ncs_update(ovl_ctx *c, double *delta, double *total) {
     if (rc) return rc;
     const size_t V = (size_t)c->L.V;
     if (!c->u_old) {
-        if (cudaMalloc(&c->u_old, sizeof(double) * 12 * V) != cudaSuccess ||
-            cudaMalloc(&c->u_mid, sizeof(double) * 12 * V) != cudaSuccess ||
-            cudaMalloc(&c->e_mid, sizeof(double) * 9 * V) != cudaSuccess) {
+        if (cudaMalloc(&c->u_old, sizeof(double) * c->link_doubles * 3 * V) != cudaSuccess ||
+            cudaMalloc(&c->u_mid, sizeof(double) * c->link_doubles * 3 * V) != cudaSuccess ||
+            cudaMalloc(&c->e_mid, sizeof(double) * c->e_comp * 3 * V) != cudaSuccess) {
             cudaGetLastError();
             return fail(c, OVL_E_OOM, "ovl_ncs_update: link copies");
         }
@@ -1040,10 +1152,17 @@ int ovl_ncs_update(ovl_ctx *c, double *delta, double *total) {
     if (c->have_u_old) {
         // GetDeltaNCs(1): Simpson weights 1, 4, 1 at x = 0, 1/2, 1 (CoolingMethod.cpp:80-125)
         double *out = c->dev_small;
-        ovl::launch_geodesic(c->u_old, c->U, 0.5, c->u_mid, c->e_mid, c->L, c->stream);
-        ovl::launch_ncsdot(c->u_mid, c->e_mid, c->L, c->partial, out, c->stream);
-        ovl::launch_ncsdot(c->u_old, c->e_mid, c->L, c->partial, out + 1, c->stream);
-        ovl::launch_ncsdot(c->U, c->e_mid, c->L, c->partial, out + 2, c->stream);
+        if (su3(c)) {
+            ovl::su3_launch_geodesic(c->u_old, c->U, 0.5, c->u_mid, c->e_mid, c->L, c->stream);
+            ovl::su3_launch_ncsdot(c->u_mid, c->e_mid, c->L, c->partial, out, c->stream);
+            ovl::su3_launch_ncsdot(c->u_old, c->e_mid, c->L, c->partial, out + 1, c->stream);
+            ovl::su3_launch_ncsdot(c->U, c->e_mid, c->L, c->partial, out + 2, c->stream);
+        } else {
+            ovl::launch_geodesic(c->u_old, c->U, 0.5, c->u_mid, c->e_mid, c->L, c->stream);
+            ovl::launch_ncsdot(c->u_mid, c->e_mid, c->L, c->partial, out, c->stream);
+            ovl::launch_ncsdot(c->u_old, c->e_mid, c->L, c->partial, out + 1, c->stream);
+            ovl::launch_ncsdot(c->U, c->e_mid, c->L, c->partial, out + 2, c->stream);
+        }
         if ((rc = launched(c, 7, "ncs update"))) return rc;
         OVL_CUDA(c, cudaMemcpyAsync(c->host_small, out, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->stream));
         OVL_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1055,7 +1174,8 @@ int ovl_ncs_update(ovl_ctx *c, double *delta, double *total) {
         d = value / weight;
         c->ncs_total += d;
     }
-    OVL_CUDA(c, cudaMemcpyAsync(c->u_old, c->U, sizeof(double) * 12 * V, cudaMemcpyDeviceToDevice, c->stream));
+    OVL_CUDA(c, cudaMemcpyAsync(c->u_old, c->U, sizeof(double) * c->link_doubles * 3 * V, cudaMemcpyDeviceToDevice,
+                                c->stream));
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_u_old = true;
     if (delta) *delta = d;
@@ -1067,7 +1187,7 @@ int ovl_update_links(ovl_ctx *c, double dt_step) {
     if (!c) return OVL_E_ARG;
     int rc = set_device(c);
     if (rc) return rc;
-    ovl::launch_update_links(c->U, c->E, c->L, dt_step, c->stream, c->U32, c->p.reunitarize != 0);
+    launch_links(c, c->U, c->U32, dt_step);
     return launched(c, 1, "update links");
 }
 
@@ -1075,13 +1195,15 @@ int ovl_update_efield(ovl_ctx *c, double dt_step) {
     if (!c) return OVL_E_ARG;
     int rc = set_device(c);
     if (rc) return rc;
-    ovl::launch_update_efield(c->U, c->E, nullptr, c->L, dt_step, c->stream);
+    if (su3(c)) ovl::su3_launch_update_efield(c->U, c->E, c->L, dt_step, c->stream);
+    else ovl::launch_update_efield(c->U, c->E, nullptr, c->L, dt_step, c->stream);
     return launched(c, 1, "update efield");
 }
 
 int ovl_color_force(ovl_ctx *c, double *out) {
     if (!c || !out) return OVL_E_ARG;
     if (c->p.fermion != OVL_FERMION_WILSON) return fail(c, OVL_E_UNSUPPORTED, "ovl_color_force: Wilson fermions only");
+    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_color_force: built for two colours");
     int rc = set_device(c);
     if (rc) return rc;
     double *dev = nullptr;
@@ -1111,6 +1233,7 @@ int ovl_color_force(ovl_ctx *c, double *out) {
 int ovl_fermion_energy(ovl_ctx *c, double *out) {
     if (!c || !out) return OVL_E_ARG;
     if (c->p.fermion != OVL_FERMION_WILSON) return fail(c, OVL_E_UNSUPPORTED, "ovl_fermion_energy: Wilson fermions only");
+    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_fermion_energy: built for two colours");
     int rc = set_device(c);
     if (rc) return rc;
     const double *u1 = c->u1_on ? c->u1 : nullptr;
@@ -1141,6 +1264,7 @@ int ovl_fermion_energy(ovl_ctx *c, double *out) {
 int ovl_gauss_restore(ovl_ctx *c, int max_iter, double tol, int *iterations, double out[2]) {
     if (!c) return OVL_E_ARG;
     if (max_iter < 0 || !(tol >= 0.0)) return fail(c, OVL_E_ARG, "ovl_gauss_restore: max_iter=%d tol=%g", max_iter, tol);
+    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_gauss_restore: built for two colours");
     int rc = set_device(c);
     if (rc) return rc;
     double *G = nullptr;
@@ -1188,7 +1312,8 @@ int ovl_bulk(ovl_ctx *c, double out[10]) {
     if (!c || !out) return OVL_E_ARG;
     int rc = set_device(c);
     if (rc) return rc;
-    ovl::launch_bulk(c->U, c->E, c->L, c->partial, c->dev_small, c->stream);
+    if (su3(c)) ovl::su3_launch_bulk(c->U, c->E, c->L, c->partial, c->dev_small, c->stream);
+    else ovl::launch_bulk(c->U, c->E, c->L, c->partial, c->dev_small, c->stream);
     if ((rc = launched(c, 2, "bulk"))) return rc;
     OVL_CUDA(c, cudaMemcpyAsync(c->host_small, c->dev_small, sizeof(double) * 10, cudaMemcpyDeviceToHost, c->stream));
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1220,6 +1345,7 @@ int ovl_launch_count(const ovl_ctx *c, uint64_t *count) {
 
 int ovl_ritz_bounds(ovl_ctx *c, const double *start, double out[2], double raw[2], int iters[2]) {
     if (!c || !out) return OVL_E_ARG;
+    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_ritz_bounds: built for two colours");
     int rc = set_device(c);
     if (rc) return rc;
     return ritz_bounds(c, start, out, raw, iters);
@@ -1241,7 +1367,7 @@ int ovl_apply(ovl_ctx *c, int count, const double *phi, double *out) {
     if (count < 1 || count > c->p.n_modes) return fail(c, OVL_E_ARG, "ovl_apply: count=%d outside [1, %d]", count, c->p.n_modes);
     int rc = set_device(c);
     if (rc) return rc;
-    const size_t per_mode = (size_t)c->L.V * ovl::kComp * 2;
+    const size_t per_mode = (size_t)c->L.V * c->comp * 2;
     const int n_mb = (count + ovl::kModeBlock - 1) / ovl::kModeBlock;
     double *stage = nullptr;
     if (cudaMalloc(&stage, per_mode * 8 * (size_t)count) != cudaSuccess) {
@@ -1255,11 +1381,15 @@ int ovl_apply(ovl_ctx *c, int count, const double *phi, double *out) {
     if (fp40(c)) {
         cudaMemsetAsync(c->aux_src_lo, 0, c->field_complex * 2, c->stream);
         ovl::launch_ref_to_blocks<double>(stage, c->aux_src, c->L, 0, count, c->stream, c->aux_src_lo);
-    } else if (fp32(c)) ovl::launch_ref_to_blocks<float>(stage, c->aux_src, c->L, 0, count, c->stream);
-    else ovl::launch_ref_to_blocks<double>(stage, c->aux_src, c->L, 0, count, c->stream);
+    } else if (fp32(c)) ovl::launch_ref_to_blocks<float>(stage, c->aux_src, c->L, 0, count, c->stream, nullptr, c->nc);
+    else ovl::launch_ref_to_blocks<double>(stage, c->aux_src, c->L, 0, count, c->stream, nullptr, c->nc);
     if ((rc = launched(c, 1, "ref_to_blocks"))) return done(rc);
     if (overlap(c)) {
         if ((rc = run_overlap(c, c->aux_src, c->aux_dst, n_mb, count, false, false))) return done(rc);
+    } else if (su3(c)) {
+        if (fp32(c)) ovl::su3_launch_hop<float>(su3_links(c), c->aux_src, c->aux_dst, c->L, 0, n_mb, amass(c->p), 0.0, false, c->stream);
+        else ovl::su3_launch_hop<double>(su3_links(c), c->aux_src, c->aux_dst, c->L, 0, n_mb, amass(c->p), 0.0, false, c->stream);
+        if ((rc = launched(c, 1, "wilson operator"))) return done(rc);
     } else if (fp40(c)) {
         ovl::HopConfig h;
         h.U = c->U;
@@ -1273,8 +1403,8 @@ int ovl_apply(ovl_ctx *c, int count, const double *phi, double *out) {
         if ((rc = launched(c, 1, "wilson operator"))) return done(rc);
     }
     if (fp40(c)) ovl::launch_blocks_to_ref<double>(c->aux_dst, stage, c->L, 0, count, c->stream, c->aux_dst_lo);
-    else if (fp32(c)) ovl::launch_blocks_to_ref<float>(c->aux_dst, stage, c->L, 0, count, c->stream);
-    else ovl::launch_blocks_to_ref<double>(c->aux_dst, stage, c->L, 0, count, c->stream);
+    else if (fp32(c)) ovl::launch_blocks_to_ref<float>(c->aux_dst, stage, c->L, 0, count, c->stream, nullptr, c->nc);
+    else ovl::launch_blocks_to_ref<double>(c->aux_dst, stage, c->L, 0, count, c->stream, nullptr, c->nc);
     if ((rc = launched(c, 1, "blocks_to_ref"))) return done(rc);
     if (cudaMemcpyAsync(out, stage, per_mode * 8 * count, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
         return done(fail(c, OVL_E_CUDA, "ovl_apply: download"));
@@ -1291,6 +1421,7 @@ int ovl_tuning(const ovl_ctx *c, int *variant, int *mode_group) {
 
 int ovl_autotune(ovl_ctx *c, int *variant, double ms[3]) {
     if (!c) return OVL_E_ARG;
+    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_autotune: one three-colour kernel, nothing to tune");
     int rc = set_device(c);
     if (rc) return rc;
     double t[ovl::kHopVariants];
@@ -1495,6 +1626,8 @@ int ovl_ensemble_create(const ovl_params *members, int count, ovl_ensemble **out
             return ens_fail(nullptr, OVL_E_ARG, "ovl_ensemble_create: member %d: one precision and device for all", i);
         if (p.backreaction != 0.0 || p.gauge_force)
             return ens_fail(nullptr, OVL_E_UNSUPPORTED, "ovl_ensemble_create: member %d: no coupled evolution", i);
+        if (p.n_colours != 2)
+            return ens_fail(nullptr, OVL_E_UNSUPPORTED, "ovl_ensemble_create: member %d: two colours only", i);
     }
     ovl_ensemble *e = new (std::nothrow) ovl_ensemble();
     if (!e) return ens_fail(nullptr, OVL_E_OOM, "ovl_ensemble_create: host allocation");
@@ -1550,6 +1683,7 @@ int ovl_ensemble_add(ovl_ensemble *e, const ovl_params *member, int *index) {
         p.device != e->device)
         return ens_fail(e, OVL_E_ARG, "ovl_ensemble_add: the ensemble's precision and device");
     if (p.backreaction != 0.0 || p.gauge_force) return ens_fail(e, OVL_E_UNSUPPORTED, "ovl_ensemble_add: no coupled evolution");
+    if (p.n_colours != 2) return ens_fail(e, OVL_E_UNSUPPORTED, "ovl_ensemble_add: two colours only");
     if (cudaSetDevice(e->device) != cudaSuccess) return ens_fail(e, OVL_E_CUDA, "ovl_ensemble_add: device");
     ovl_params q = p;
     q.stream = reinterpret_cast<uint64_t>(e->stream);

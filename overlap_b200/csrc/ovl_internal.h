@@ -77,7 +77,8 @@ void launch_currents(const double *U, const double *u1, const void *psi, const L
 void launch_site_sums(const double *per_site, const Lattice &L, double *partial, double *out4, cudaStream_t stream);
 void launch_currents_finish(const double *partial, int groups, const Lattice &L, double *per_site, cudaStream_t stream);
 void launch_overlap_currents(const void *psi, const void *opsi, const Lattice &L, int n_mb, int n_modes,
-                             int first_mode, double *partial, double *per_site, cudaStream_t stream);
+                             int first_mode, double *partial, double *per_site, cudaStream_t stream, bool fp32 = false,
+                             int nc = 2);
 // Fermion back-reaction: dH_F/dtheta^a_mu(x) per link (24 doubles of colour
 // bilinears per site and group in `partial`); into out[9 V] when out is set,
 // else E += coef * force.  Fermion energy H_F from psi and dpsi = D psi.
@@ -153,7 +154,7 @@ void launch_batch_advance(const BatchMember *members, int count, cudaStream_t st
 void launch_stochastic_modes(void *psi, void *psimid, void *psi_lo, void *psimid_lo, int kind, const Lattice &L,
                              int n_mb, int n_modes, int first_mode, double amass, double dt, uint64_t seed, int pairs,
                              double *scratch_a, double *scratch_b, int chunk_mb, cudaStream_t stream,
-                             uint64_t *launches);
+                             uint64_t *launches, int nc = 2);
 // Lattice sums N_V, N_5, PS, WA straight from the modes (no per-site maps).
 size_t charges_partial_doubles(const Lattice &L, int n_mb);
 template <typename T>
@@ -161,13 +162,13 @@ void launch_charges(const double *U, const double *u1, const void *psi, const La
                     int first_mode, double r_wilson, double *partial, double *out4, cudaStream_t stream);
 
 // Layout conversion between the reference layout (double, [mode][site][comp])
-// and the mode-block layout of precision T.  Modes [m0, m0+count).
+// and the mode-block layout of precision T.  Modes [m0, m0+count); nc colours.
 template <typename T>
 void launch_ref_to_blocks(const double *ref, void *blocks, const Lattice &L, int m0, int count, cudaStream_t stream,
-                          void *lo = nullptr);
+                          void *lo = nullptr, int nc = 2);
 template <typename T>
 void launch_blocks_to_ref(const void *blocks, double *ref, const Lattice &L, int m0, int count, cudaStream_t stream,
-                          const void *lo = nullptr);
+                          const void *lo = nullptr, int nc = 2);
 
 // ------------------------------------------------------------------ overlap --
 // Zolotarev coefficients on the host (ovl_zolotarev.cpp); returns the relative
@@ -223,6 +224,37 @@ void chebyshev_apply(ChebyshevWork &w, const double *U, const double *u1, const 
 template <typename T>
 void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes, int n_mb, int first_mode,
                           double r_wilson, double m_fermion, double dt, int *bad, cudaStream_t stream,
-                          void *lo_psi = nullptr, void *lo_mid = nullptr);
+                          void *lo_psi = nullptr, void *lo_mid = nullptr, int nc = 2);
+
+// ------------------------------------------------------------ three colours --
+// ovl_su3.cu; layouts in ovl_su3.cuh.  Links of the hop kernels: FP64 (U,
+// u1) for FP64 modes, the FP32 copies (U32, u1_32) for FP32 modes; u1 / u1_32
+// null without a U(1) background.
+struct Su3Links {
+    const double *U = nullptr, *u1 = nullptr;
+    const float *U32 = nullptr, *u1_32 = nullptr;
+};
+template <typename T>
+void su3_launch_hop(const Su3Links &lk, const void *src, void *dst, const Lattice &L, int mb0, int n_mb, double amass,
+                    double dt, bool accumulate, cudaStream_t stream);
+void su3_launch_update_links(double *U, const double *E, const Lattice &L, double dt_step, float *U32, bool reunit,
+                             cudaStream_t stream);
+void su3_launch_update_efield(const double *U, double *E, const Lattice &L, double dt_step, cudaStream_t stream);
+void su3_launch_links_to_f32(const double *U, float *U32, const Lattice &L, cudaStream_t stream);
+template <typename T>
+void su3_chebyshev_apply(ChebyshevWork &w, const Su3Links &lk, const void *src, void *dst, const Lattice &L, int n_mb,
+                         const double *coeff, int K, double eps, double lambda_max, double amass, double mdw, double mf,
+                         double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches);
+size_t su3_charges_partial_doubles(const Lattice &L, int n_mb);
+template <typename T>
+void su3_launch_charges(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                        int first_mode, double r_wilson, double *partial, double *out4, cudaStream_t stream);
+size_t su3_reduce_partial_doubles(const Lattice &L);
+void su3_launch_ncsdot(const double *U, const double *E, const Lattice &L, double *partial, double *out,
+                       cudaStream_t stream);
+void su3_launch_geodesic(const double *Uold, const double *Unew, double c, double *Umid, double *Emid, const Lattice &L,
+                         cudaStream_t stream);
+void su3_launch_bulk(const double *U, const double *E, const Lattice &L, double *partial, double *out,
+                     cudaStream_t stream);
 
 }  // namespace ovl

@@ -357,17 +357,22 @@ void launch_site_sums(const double *per_site, const Lattice &L, double * /*parti
 }
 
 // ---------------------------------------------------------- layout change --
+// ncomp complex components per mode and site: 8 (two colours) or 12 (three).
+__device__ __forceinline__ size_t block_index(int V, int ncomp, int m, int site, int comp) {
+    return (((size_t)(m / kModeBlock) * V + site) * ncomp + comp) * kModeBlock + m % kModeBlock;
+}
+
 template <typename T>
 __global__ void ref_to_blocks_kernel(const double2 *__restrict__ ref, cpx<T> *__restrict__ blocks, int V, int m0,
-                                     int count, unsigned char *__restrict__ lo) {
-    const size_t n = (size_t)count * V * kComp;
+                                     int count, unsigned char *__restrict__ lo, int ncomp) {
+    const size_t n = (size_t)count * V * ncomp;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int comp = (int)(i % kComp);
-        const size_t ms = i / kComp;
+        const int comp = (int)(i % ncomp);
+        const size_t ms = i / ncomp;
         const int site = (int)(ms % V);
         const int m = m0 + (int)(ms / V);
         const double2 v = ref[i];
-        const size_t j = field_index(V, m / kModeBlock, site, comp, m % kModeBlock);
+        const size_t j = block_index(V, ncomp, m, site, comp);
         if (lo) store40(reinterpret_cast<uint2 *>(blocks), lo, j, v.x, v.y);  // 40-bit storage
         else st(blocks + j, mk<T>((T)v.x, (T)v.y));
     }
@@ -375,14 +380,14 @@ __global__ void ref_to_blocks_kernel(const double2 *__restrict__ ref, cpx<T> *__
 
 template <typename T>
 __global__ void blocks_to_ref_kernel(const cpx<T> *__restrict__ blocks, double2 *__restrict__ ref, int V, int m0,
-                                     int count, const unsigned char *__restrict__ lo) {
-    const size_t n = (size_t)count * V * kComp;
+                                     int count, const unsigned char *__restrict__ lo, int ncomp) {
+    const size_t n = (size_t)count * V * ncomp;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int comp = (int)(i % kComp);
-        const size_t ms = i / kComp;
+        const int comp = (int)(i % ncomp);
+        const size_t ms = i / ncomp;
         const int site = (int)(ms % V);
         const int m = m0 + (int)(ms / V);
-        const size_t j = field_index(V, m / kModeBlock, site, comp, m % kModeBlock);
+        const size_t j = block_index(V, ncomp, m, site, comp);
         if (lo) {  // 40-bit storage
             const cpx<double> v = Src40{reinterpret_cast<const uint2 *>(blocks), lo}(j);
             ref[i] = double2{v.re, v.im};
@@ -400,22 +405,22 @@ static int grid_for(size_t n) {
 
 template <typename T>
 void launch_ref_to_blocks(const double *ref, void *blocks, const Lattice &L, int m0, int count, cudaStream_t stream,
-                          void *lo) {
-    const size_t n = (size_t)count * L.V * kComp;
+                          void *lo, int nc) {
+    const size_t n = (size_t)count * L.V * nc * kSpin;
     if (n == 0) return;
     ref_to_blocks_kernel<T><<<grid_for(n), 256, 0, stream>>>(reinterpret_cast<const double2 *>(ref),
                                                              reinterpret_cast<cpx<T> *>(blocks), L.V, m0, count,
-                                                             reinterpret_cast<unsigned char *>(lo));
+                                                             reinterpret_cast<unsigned char *>(lo), nc * kSpin);
 }
 
 template <typename T>
 void launch_blocks_to_ref(const void *blocks, double *ref, const Lattice &L, int m0, int count, cudaStream_t stream,
-                          const void *lo) {
-    const size_t n = (size_t)count * L.V * kComp;
+                          const void *lo, int nc) {
+    const size_t n = (size_t)count * L.V * nc * kSpin;
     if (n == 0) return;
     blocks_to_ref_kernel<T><<<grid_for(n), 256, 0, stream>>>(reinterpret_cast<const cpx<T> *>(blocks),
                                                              reinterpret_cast<double2 *>(ref), L.V, m0, count,
-                                                             reinterpret_cast<const unsigned char *>(lo));
+                                                             reinterpret_cast<const unsigned char *>(lo), nc * kSpin);
 }
 
 // ------------------------------------------------------------ plane waves --
@@ -426,11 +431,11 @@ void launch_blocks_to_ref(const void *blocks, double *ref, const Lattice &L, int
 // psi exp(-i w dt / 2).
 struct FreeMode { double u[8]; double omega; int colour, k0, k1, k2, particle, bad; };
 
-__device__ FreeMode free_mode(const Lattice &L, int g, double r, double m) {
+__device__ FreeMode free_mode(const Lattice &L, int g, double r, double m, int nc) {
     FreeMode fm;
     const int N[3] = {L.N0, L.N1, L.N2};
     fm.particle = g % 2; g /= 2;
-    fm.colour = g % kColours; g /= kColours;
+    fm.colour = g % nc; g /= nc;
     const int spin = g % 2; g /= 2;
     int k[3];
     k[0] = g % N[0]; g /= N[0];
@@ -504,17 +509,18 @@ __device__ FreeMode free_mode(const Lattice &L, int g, double r, double m) {
     return fm;
 }
 
-__global__ void free_modes_kernel(FreeMode *info, int n_modes, int first_mode, Lattice L, double r, double m, int *bad) {
+__global__ void free_modes_kernel(FreeMode *info, int n_modes, int first_mode, Lattice L, double r, double m, int *bad,
+                                  int nc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_modes) return;
-    FreeMode fm = free_mode(L, first_mode + i, r, m);
+    FreeMode fm = free_mode(L, first_mode + i, r, m, nc);
     info[i] = fm;
     if (fm.bad) atomicAdd(bad, 1);
 }
 
 template <typename T>
 __global__ void free_fill_kernel(const FreeMode *__restrict__ info, cpx<T> *psi, cpx<T> *psimid, Lattice L, int n_modes,
-                                 int n_mb, double dt, unsigned char *lo_psi, unsigned char *lo_mid) {
+                                 int n_mb, double dt, unsigned char *lo_psi, unsigned char *lo_mid, int nc) {
     const int lane = threadIdx.x;
     const int site = blockIdx.x * blockDim.y + threadIdx.y;
     const int mb = blockIdx.y;
@@ -536,11 +542,11 @@ __global__ void free_fill_kernel(const FreeMode *__restrict__ info, cpx<T> *psi,
         half = mk<double>(cs, sn);
         colour = fm.colour;
     }
-    for (int c = 0; c < kColours; c++)
+    for (int c = 0; c < nc; c++)
         for (int a = 0; a < kSpin; a++) {
             cpx<double> v = c == colour ? phase * u[a] : mk<double>(0, 0);
             cpx<double> vm = c == colour ? v * half : mk<double>(0, 0);
-            const size_t idx = field_index(L.V, mb, site, c * kSpin + a, lane);
+            const size_t idx = block_index(L.V, nc * kSpin, m, site, c * kSpin + a);
             if (lo_psi) {  // 40-bit storage
                 store40(reinterpret_cast<uint2 *>(psi), lo_psi, idx, v.re, v.im);
                 store40(reinterpret_cast<uint2 *>(psimid), lo_mid, idx, vm.re, vm.im);
@@ -554,16 +560,17 @@ __global__ void free_fill_kernel(const FreeMode *__restrict__ info, cpx<T> *psi,
 template <typename T>
 void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes, int n_mb, int first_mode,
                           double r_wilson, double m_fermion, double dt, int *bad, cudaStream_t stream, void *lo_psi,
-                          void *lo_mid) {
+                          void *lo_mid, int nc) {
     FreeMode *info = nullptr;
     cudaMallocAsync(&info, sizeof(FreeMode) * (size_t)n_modes, stream);
     cudaMemsetAsync(bad, 0, sizeof(int), stream);
-    free_modes_kernel<<<(n_modes + 127) / 128, 128, 0, stream>>>(info, n_modes, first_mode, L, r_wilson, m_fermion, bad);
+    free_modes_kernel<<<(n_modes + 127) / 128, 128, 0, stream>>>(info, n_modes, first_mode, L, r_wilson, m_fermion, bad,
+                                                                 nc);
     dim3 block(kModeBlock, kSitesPerCta);
     dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
     free_fill_kernel<T><<<grid, block, 0, stream>>>(info, reinterpret_cast<cpx<T> *>(psi), reinterpret_cast<cpx<T> *>(psimid),
                                                     L, n_modes, n_mb, dt, reinterpret_cast<unsigned char *>(lo_psi),
-                                                    reinterpret_cast<unsigned char *>(lo_mid));
+                                                    reinterpret_cast<unsigned char *>(lo_mid), nc);
     cudaFreeAsync(info, stream);
 }
 
@@ -572,11 +579,12 @@ void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes
                                     double, double *, double *, cudaStream_t);                                      \
     template void launch_currents<T>(const double *, const double *, const void *, const Lattice &, int, int, int,   \
                                      double, double *, double *, cudaStream_t);                                     \
-    template void launch_ref_to_blocks<T>(const double *, void *, const Lattice &, int, int, cudaStream_t, void *);  \
+    template void launch_ref_to_blocks<T>(const double *, void *, const Lattice &, int, int, cudaStream_t, void *,    \
+                                          int);                                                                     \
     template void launch_blocks_to_ref<T>(const void *, double *, const Lattice &, int, int, cudaStream_t,          \
-                                          const void *);                                                            \
+                                          const void *, int);                                                       \
     template void launch_free_fermions<T>(void *, void *, const Lattice &, int, int, int, double, double, double,    \
-                                          int *, cudaStream_t, void *, void *);
+                                          int *, cudaStream_t, void *, void *, int);
 OVL_INSTANTIATE(double)
 OVL_INSTANTIATE(float)
 

@@ -230,8 +230,10 @@ __global__ void cg_scalars_alpha_kernel(CgScalars s, int modes_padded, int npole
 //   jA^mu = Re[psi^+ g0 g_mu g5 psi + psi^+ (-i/2) g0 g_mu g5 g0 O]      (g_0 for mu = 0)
 // weighted by the vacuum sign and summed over colours and modes; per site the
 // output slots are those of the Wilson currents (jV, jA; the rest zero).
+// Modes of precision T and NC colours; the bilinears in FP64.
+template <typename T, int NC>
 __global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
-    overlap_currents_kernel(const cpx<double> *__restrict__ psi, const cpx<double> *__restrict__ opsi, Lattice L,
+    overlap_currents_kernel(const cpx<T> *__restrict__ psi, const cpx<T> *__restrict__ opsi, Lattice L,
                             int n_mb, int n_modes, int first_mode, int groups, double *__restrict__ partial) {
     constexpr mono GV[4] = {mono_mul(kGamma0, kGamma0), mono_mul(kGamma0, kGammaX), mono_mul(kGamma0, kGammaY),
                             mono_mul(kGamma0, kGammaZ)};
@@ -249,20 +251,22 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
     for (int mb = g; mb < n_mb; mb += groups) {
         const int mode = mb * kModeBlock + lane;
         const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
-        cpx<double> f[kColours][kSpin], o[kColours][kSpin];
-        const size_t base = field_index(L.V, mb, site, 0, lane);
+        cpx<double> f[NC][kSpin], o[NC][kSpin];
+        const size_t base = (((size_t)mb * L.V + site) * (NC * kSpin)) * kModeBlock + lane;
 #pragma unroll
-        for (int c = 0; c < kColours; c++)
+        for (int c = 0; c < NC; c++)
 #pragma unroll
             for (int a = 0; a < kSpin; a++) {
-                f[c][a] = ld(psi + base + (c * kSpin + a) * kModeBlock);
-                o[c][a] = ld(opsi + base + (c * kSpin + a) * kModeBlock);
+                const cpx<T> x = ld(psi + base + (c * kSpin + a) * kModeBlock);
+                const cpx<T> y = ld(opsi + base + (c * kSpin + a) * kModeBlock);
+                f[c][a] = mk<double>((double)x.re, (double)x.im);
+                o[c][a] = mk<double>((double)y.re, (double)y.im);
             }
 #pragma unroll
         for (int mu = 0; mu < 4; mu++) {
             cpx<double> v1 = mk<double>(0, 0), v2 = mk<double>(0, 0), a1 = mk<double>(0, 0), a2 = mk<double>(0, 0);
 #pragma unroll
-            for (int c = 0; c < kColours; c++) {
+            for (int c = 0; c < NC; c++) {
                 v1 = v1 + bilinear<double>(GV[mu], f[c], f[c]);
                 v2 = v2 + bilinear<double>(GV2[mu], f[c], o[c]);
                 a1 = a1 + bilinear<double>(GA[mu], f[c], f[c]);
@@ -285,14 +289,26 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
     }
 }
 
-void launch_overlap_currents(const void *psi, const void *opsi, const Lattice &L, int n_mb, int n_modes,
-                             int first_mode, double *partial, double *per_site, cudaStream_t stream) {
-    const int groups = currents_groups(n_mb);
+template <typename T, int NC>
+static void overlap_currents_t(const void *psi, const void *opsi, const Lattice &L, int n_mb, int n_modes,
+                               int first_mode, int groups, double *partial, cudaStream_t stream) {
     dim3 block(kModeBlock, kSitesPerCta);
     dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, groups);
-    overlap_currents_kernel<<<grid, block, 0, stream>>>(reinterpret_cast<const cpx<double> *>(psi),
-                                                        reinterpret_cast<const cpx<double> *>(opsi), L, n_mb, n_modes,
-                                                        first_mode, groups, partial);
+    overlap_currents_kernel<T, NC><<<grid, block, 0, stream>>>(reinterpret_cast<const cpx<T> *>(psi),
+                                                               reinterpret_cast<const cpx<T> *>(opsi), L, n_mb, n_modes,
+                                                               first_mode, groups, partial);
+}
+
+void launch_overlap_currents(const void *psi, const void *opsi, const Lattice &L, int n_mb, int n_modes,
+                             int first_mode, double *partial, double *per_site, cudaStream_t stream, bool fp32, int nc) {
+    const int groups = currents_groups(n_mb);
+    if (nc == 3) {
+        if (fp32) overlap_currents_t<float, 3>(psi, opsi, L, n_mb, n_modes, first_mode, groups, partial, stream);
+        else overlap_currents_t<double, 3>(psi, opsi, L, n_mb, n_modes, first_mode, groups, partial, stream);
+    } else {
+        if (fp32) overlap_currents_t<float, 2>(psi, opsi, L, n_mb, n_modes, first_mode, groups, partial, stream);
+        else overlap_currents_t<double, 2>(psi, opsi, L, n_mb, n_modes, first_mode, groups, partial, stream);
+    }
     launch_currents_finish(partial, groups, L, per_site, stream);
 }
 

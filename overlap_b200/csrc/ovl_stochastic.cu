@@ -40,13 +40,14 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 // (block, momentum, colour, lane).  mid: write the psimid version.
 __global__ void stochastic_fill_kernel(cpx<double> *__restrict__ out, Lattice L, int mb0, int nmb, int n_modes,
                                        int first_mode, double amass, double dt, double inv_sqrt_r, uint64_t seed,
-                                       int mid) {
-    const size_t n = (size_t)nmb * L.V * kColours * kModeBlock;
+                                       int mid, int nc) {
+    const size_t n = (size_t)nmb * L.V * nc * kModeBlock;
+    const int ncomp = nc * kSpin;
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
         const int lane = (int)(t % kModeBlock);
-        const int c = (int)((t / kModeBlock) % kColours);
-        const int q = (int)((t / ((size_t)kModeBlock * kColours)) % L.V);
-        const int mbl = (int)(t / ((size_t)kModeBlock * kColours * L.V));
+        const int c = (int)((t / kModeBlock) % nc);
+        const int q = (int)((t / ((size_t)kModeBlock * nc)) % L.V);
+        const int mbl = (int)(t / ((size_t)kModeBlock * nc * L.V));
         const int mode = (mb0 + mbl) * kModeBlock + lane;
         cpx<double> res[kSpin];
         for (int a = 0; a < kSpin; a++) res[a] = mk<double>(0.0, 0.0);
@@ -93,14 +94,15 @@ __global__ void stochastic_fill_kernel(cpx<double> *__restrict__ out, Lattice L,
                 res[a] = mk<double>(vr * ph_re - vi * ph_im, vr * ph_im + vi * ph_re);
             }
         }
-        for (int a = 0; a < kSpin; a++) out[field_index(L.V, mbl, q, c * kSpin + a, lane)] = res[a];
+        for (int a = 0; a < kSpin; a++)
+            out[(((size_t)mbl * L.V + q) * ncomp + c * kSpin + a) * kModeBlock + lane] = res[a];
     }
 }
 
 // One pass of the unitary inverse DFT along axis `ax` of a chunk in the
 // mode-block layout: out(x_ax) = N^-1/2 sum_k in(k) e^{+2 pi i k x_ax / N}.
 __global__ void idft_axis_kernel(const cpx<double> *__restrict__ in, cpx<double> *__restrict__ out, Lattice L, int nmb,
-                                 int ax) {
+                                 int ax, int ncomp) {
     extern __shared__ cpx<double> tw[];  // e^{2 pi i j / N}, j < N
     const int N = ax == 0 ? L.N0 : ax == 1 ? L.N1 : L.N2;
     for (int j = threadIdx.x; j < N; j += blockDim.x) {
@@ -111,19 +113,19 @@ __global__ void idft_axis_kernel(const cpx<double> *__restrict__ in, cpx<double>
     __syncthreads();
     const double norm = rsqrt((double)N);
     const int stride = ax == 0 ? 1 : ax == 1 ? L.N0 : L.N0 * L.N1;
-    const size_t n = (size_t)nmb * L.V * kComp * kModeBlock;
+    const size_t n = (size_t)nmb * L.V * ncomp * kModeBlock;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         const int lane = (int)(e % kModeBlock);
-        const int comp = (int)((e / kModeBlock) % kComp);
-        const int site = (int)((e / ((size_t)kModeBlock * kComp)) % L.V);
-        const int mb = (int)(e / ((size_t)kModeBlock * kComp * L.V));
+        const int comp = (int)((e / kModeBlock) % ncomp);
+        const int site = (int)((e / ((size_t)kModeBlock * ncomp)) % L.V);
+        const int mb = (int)(e / ((size_t)kModeBlock * ncomp * L.V));
         int x, y, z;
         site_coords(L, site, x, y, z);
         const int xa = ax == 0 ? x : ax == 1 ? y : z;
         const int base = site - xa * stride;
         double re = 0.0, im = 0.0;
         for (int k = 0; k < N; k++) {
-            const cpx<double> v = in[field_index(L.V, mb, base + k * stride, comp, lane)];
+            const cpx<double> v = in[(((size_t)mb * L.V + base + k * stride) * ncomp + comp) * kModeBlock + lane];
             const cpx<double> w = tw[(k * xa) % N];
             re += v.re * w.re - v.im * w.im;
             im += v.re * w.im + v.im * w.re;
@@ -148,7 +150,8 @@ static int grid_of(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 655
 void launch_stochastic_modes(void *psi, void *psimid, void *psi_lo, void *psimid_lo, int kind, const Lattice &L,
                              int n_mb, int n_modes, int first_mode, double amass, double dt, uint64_t seed, int pairs,
                              double *scratch_a, double *scratch_b, int chunk_mb, cudaStream_t stream,
-                             uint64_t *launches) {
+                             uint64_t *launches, int nc) {
+    const int ncomp = nc * kSpin;
     const double inv_sqrt_r = std::sqrt((double)L.V / (double)pairs);  // sqrt(V / R)
     cpx<double> *a = reinterpret_cast<cpx<double> *>(scratch_a), *b = reinterpret_cast<cpx<double> *>(scratch_b);
     const int maxN = std::max(L.N0, std::max(L.N1, L.N2));
@@ -158,14 +161,15 @@ void launch_stochastic_modes(void *psi, void *psimid, void *psi_lo, void *psimid
         unsigned char *lo = reinterpret_cast<unsigned char *>(f == 0 ? psi_lo : psimid_lo);
         for (int mb0 = 0; mb0 < n_mb; mb0 += chunk_mb) {
             const int nmb = std::min(chunk_mb, n_mb - mb0);
-            const size_t nfill = (size_t)nmb * L.V * kColours * kModeBlock;
-            const size_t nel = (size_t)nmb * L.V * kComp * kModeBlock;
+            const size_t nfill = (size_t)nmb * L.V * nc * kModeBlock;
+            const size_t nel = (size_t)nmb * L.V * ncomp * kModeBlock;
             stochastic_fill_kernel<<<grid_of(nfill), 256, 0, stream>>>(a, L, mb0, nmb, n_modes, first_mode, amass, dt,
-                                                                    inv_sqrt_r, seed, f);
-            idft_axis_kernel<<<grid_of(nel), 256, sizeof(cpx<double>) * maxN, stream>>>(a, b, L, nmb, 0);
-            idft_axis_kernel<<<grid_of(nel), 256, sizeof(cpx<double>) * maxN, stream>>>(b, a, L, nmb, 1);
-            idft_axis_kernel<<<grid_of(nel), 256, sizeof(cpx<double>) * maxN, stream>>>(a, b, L, nmb, 2);
-            store_blocks_kernel<<<grid_of(nel), 256, 0, stream>>>(b, dst, lo, field_index(L.V, mb0, 0, 0, 0), nel, kind);
+                                                                    inv_sqrt_r, seed, f, nc);
+            idft_axis_kernel<<<grid_of(nel), 256, sizeof(cpx<double>) * maxN, stream>>>(a, b, L, nmb, 0, ncomp);
+            idft_axis_kernel<<<grid_of(nel), 256, sizeof(cpx<double>) * maxN, stream>>>(b, a, L, nmb, 1, ncomp);
+            idft_axis_kernel<<<grid_of(nel), 256, sizeof(cpx<double>) * maxN, stream>>>(a, b, L, nmb, 2, ncomp);
+            store_blocks_kernel<<<grid_of(nel), 256, 0, stream>>>(b, dst, lo, (size_t)mb0 * L.V * ncomp * kModeBlock, nel,
+                                                                  kind);
             nl += 5;
         }
     }
