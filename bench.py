@@ -374,6 +374,69 @@ def serving_leg(count, device):
     return m
 
 
+def su3_overlap_leg(steps, warmup, device, modes=0):
+    """The SU(3) overlap configuration: N = 12^3, overlap fermions
+    D_ov = 1 + gamma_5 sign(H_W) with Wilson kernel mass -1 (MDWHeight 1, m = 0),
+    sign(H_W) through the Chebyshev series of degree 96 of (H_W^2)^(-1/2) on the
+    spectrum rescaled to [0.01, 1] (lambda_max the bound (|6r - 2M|/2 + 3)^2 on
+    H_W^2), all 20736 plane-wave modes in FP32, FP64 links with
+    reunitarisation; seeded random links exp(i A^a t^a), A ~ N(0, 0.5^2), and E
+    ~ N(0, 0.1^2) (links move every half step).  Times `steps` leapfrog steps;
+    N_5 (one more overlap application, OverlapCurrents.cpp) and N_CS (geodesic
+    Delta N_CS) are timed once after them as the per-step observables."""
+    import torch
+
+    from overlap_b200 import Context
+    from overlap_b200.inputs import random_efield_su3, random_links_su3
+
+    N = (12, 12, 12)
+    V = volume(N)
+    M = modes or 12 * V
+    K, eps = 96, 0.01
+    stream = torch.cuda.Stream(device)
+    ctx = Context(N=N, n_colours=3, n_modes=M, fermion="overlap", sign_method="chebyshev", cheb_degree=K,
+                  cheb_eps=eps, precision="fp32", m_fermion=0.0, m_dw=1.0, r_wilson=1.0, dt=0.05, t_sphaleron=1e300,
+                  reunitarize=True, device=device, stream=stream.cuda_stream)
+    try:
+        ctx.set_links(random_links_su3(N, 0.5, 20261203))
+        ctx.set_efield(random_efield_su3(N, 0.1, 20261204))
+        assert ctx.set_free_fermions() == 0
+        ctx.step(warmup)
+        ctx.ncs_update()
+        ctx.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.launch_count
+        torch.cuda.synchronize(device)
+        a.record(stream)
+        ctx.step(steps)
+        b.record(stream)
+        b.synchronize()
+        ms = a.elapsed_time(b)
+        launches = ctx.launch_count - l0
+        t0 = time.perf_counter()
+        ch = ctx.charges()
+        t1 = time.perf_counter()
+        d, total = ctx.ncs_update()
+        t2 = time.perf_counter()
+    finally:
+        ctx.close()
+    field = M * V * 12 * 8  # one FP32 mode field
+    # per overlap application: 7 field passes per Clenshaw term (w = D b: read b,
+    # write w; term: read w, b_1, b_2, phi, write b_0), K + 1 terms, then D chi
+    # (2) and the combination into the destination (4); two memsets (2)
+    alg = field * (7 * (K + 1) + 8)
+    half_ms = ms / (2 * steps)
+    peak, peak_kind = measured_peaks()
+    return {"config": f"SU(3), N=12^3, overlap (Chebyshev degree {K}, [eps, 1] = [{eps}, 1]), Wilson kernel mass -1, "
+                      f"{M} plane-wave modes FP32, FP64 links reunitarised, random links sigma 0.5, E sigma 0.1",
+            "value": M * V * steps / (ms / 1e3), "unit": METRIC, "steps": steps, "ms_per_step": ms / steps,
+            "launches_per_step": launches / steps,
+            "overlap_application": {"ms": half_ms, "algorithmic_bytes": alg, "achieved_GBs": alg / (half_ms / 1e3) / 1e9,
+                                    "frac_of_peak": alg / (half_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind},
+            "observables_per_step_ms": {"N5": 1e3 * (t1 - t0), "N_CS": 1e3 * (t2 - t1)},
+            "N5": ch["N5"], "delta_NCS": d}
+
+
 # ------------------------------------------------------------ distributed --
 _dist = None
 
@@ -421,6 +484,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
+    ap.add_argument("--no-su3", action="store_true", help="skip the SU(3) overlap leg")
+    ap.add_argument("--su3-steps", type=int, default=3, help="timed leapfrog steps of the SU(3) overlap leg")
     ap.add_argument("--serving-requests", type=int, default=12, help="requests of the serving leg")
     ap.add_argument("--headline", choices=("fp40", "fp32"), default="fp40",
                     help="the FP32-class form of the headline value (the other is reported beside it)")
@@ -513,6 +578,10 @@ def main():
     if not args.no_serving:
         srv = serving_leg(args.serving_requests, device)
 
+    su3 = None
+    if not args.no_su3:
+        su3 = su3_overlap_leg(args.su3_steps, 1, device, modes=args.modes)
+
     acc = None
     if args.accuracy_steps > 0 and rank == 0:
         acc = accuracy(wl, args.accuracy_steps, 50, device)
@@ -570,6 +639,8 @@ def main():
             line["ensemble"] = ens
         if srv is not None:
             line["serving"] = srv
+        if su3 is not None:
+            line["su3_overlap"] = su3
         if cpu is not None:
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)

@@ -679,7 +679,8 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
         return bail(fail(c, OVL_E_OOM, "ovl_create: pinned host allocation failed"));
     if ((rc = alloc(&c->aux_src, field_bytes, "operator input")) || (rc = alloc(&c->aux_dst, field_bytes, "operator output")))
         return bail(rc);
-    if (p->precision == OVL_PREC_FP32 && (rc = alloc((void **)&c->U32, sizeof(float) * n_link, "FP32 links")))
+    const size_t n_link32 = c->nc == 3 ? (size_t)ovl::kSu3Link32Floats * 3 * V : n_link;  // padded records
+    if (p->precision == OVL_PREC_FP32 && (rc = alloc((void **)&c->U32, sizeof(float) * n_link32, "FP32 links")))
         return bail(rc);
     c->hop_variant = c->nc == 3 ? 0 : p->hop_variant;  // one three-colour kernel: nothing to tune
     // grouping applies to the fused two-colour Wilson form; fixed when the variant is fixed

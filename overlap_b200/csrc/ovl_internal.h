@@ -230,6 +230,7 @@ void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes
 // ovl_su3.cu; layouts in ovl_su3.cuh.  Links of the hop kernels: FP64 (U,
 // u1) for FP64 modes, the FP32 copies (U32, u1_32) for FP32 modes; u1 / u1_32
 // null without a U(1) background.
+constexpr int kSu3Link32Floats = 20;  // FP32 link copy: 18 floats per link padded to 80 bytes
 struct Su3Links {
     const double *U = nullptr, *u1 = nullptr;
     const float *U32 = nullptr, *u1_32 = nullptr;

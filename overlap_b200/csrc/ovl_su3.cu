@@ -15,8 +15,11 @@ namespace ovl {
 
 // ------------------------------------------------------------ hop kernel --
 // MODE 0: out = D src; MODE 1: out += dt D src (the fused half step).
+// CTAs per SM the register allocation must allow: FP32 6 (85 registers; 64 for 8 spill).
+template <typename T> struct Occ3 { static constexpr int kMinBlocks = sizeof(T) == 4 ? 6 : 1; };
+
 template <typename T, int MODE, class LK>
-__global__ void __launch_bounds__(kModeBlock *kSites3)
+__global__ void __launch_bounds__(kModeBlock *kSites3, Occ3<T>::kMinBlocks)
     su3_wilson_kernel(LK lk, const cpx<T> *__restrict__ src, cpx<T> *__restrict__ out, Lattice L, int mb0, T amass,
                       T dt) {
     const int lane = threadIdx.x;
@@ -80,11 +83,12 @@ __global__ void su3_links_kernel(double *U, const double *__restrict__ E, int n_
     if (reunit) u = su3_reunitarize(u);
     store_su3(U, site, mu, u);
     if (U32) {
-        float2 *p = reinterpret_cast<float2 *>(U32) + 9 * (size_t)l;
+        float2 *p = reinterpret_cast<float2 *>(U32 + (size_t)kLink32Floats * l);
 #pragma unroll
         for (int i = 0; i < 3; i++)
 #pragma unroll
             for (int j = 0; j < 3; j++) p[i + 3 * j] = float2{(float)u.m[i][j].re, (float)u.m[i][j].im};
+        p[9] = float2{0.0f, 0.0f};
     }
 }
 
@@ -98,7 +102,7 @@ void su3_launch_update_links(double *U, const double *E, const Lattice &L, doubl
 // One Clenshaw term b_out = factor (a (-D w) + beta b1) - b2 + ck phi, -D w
 // the stencil applied to w = D b1 (ovl_chebyshev.cu, three colours).
 template <typename T, class LK>
-__global__ void __launch_bounds__(kModeBlock *kSites3)
+__global__ void __launch_bounds__(kModeBlock *kSites3, Occ3<T>::kMinBlocks)
     su3_clenshaw_kernel(LK lk, const cpx<T> *__restrict__ w, const cpx<T> *__restrict__ b1,
                         const cpx<T> *__restrict__ b2, const cpx<T> *__restrict__ phi, cpx<T> *__restrict__ bout,
                         Lattice L, T amass, T a, T beta, T factor, T ck) {
@@ -660,13 +664,16 @@ void su3_launch_update_efield(const double *U, double *E, const Lattice &L, doub
 }
 
 // ------------------------------------------------------------ FP32 links --
+// n = padded floats: link l's 18 doubles into floats [20 l, 20 l + 18), zeros after.
 __global__ void su3_links_f32_kernel(const double *__restrict__ U, float *U32, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        U32[i] = (float)U[i];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t l = i / kLink32Floats, k = i % kLink32Floats;
+        U32[i] = k < 18 ? (float)U[18 * l + k] : 0.0f;
+    }
 }
 
 void su3_launch_links_to_f32(const double *U, float *U32, const Lattice &L, cudaStream_t s) {
-    const size_t n = (size_t)54 * L.V;
+    const size_t n = (size_t)kLink32Floats * 3 * L.V;
     su3_links_f32_kernel<<<(int)std::min<size_t>((n + 255) / 256, 65535), 256, 0, s>>>(U, U32, n);
 }
 

@@ -5,7 +5,7 @@
 // (ovl_stencil.cuh) with 3x3 links.
 //   links: 9 complex numbers per link, U_ij at i + 3j (SUNc/SU3/GroupOperations.cpp:4-12),
 //          link (site, mu) at 18 (mu + 3 site) doubles; an FP32 copy keeps the
-//          same order in floats;
+//          same order in floats, each link padded to 20 floats (80 bytes);
 //   E:     8 components per link (t^a = lambda^a / 2), E[a + 8 (mu + 3 site)];
 //   modes: mode blocks [mb][site][colour * 4 + spin][32 lanes].
 #pragma once
@@ -17,6 +17,9 @@ namespace ovl {
 constexpr int kColours3 = 3;
 constexpr int kComp3 = kColours3 * kSpin;
 constexpr int kSites3 = 4;  // sites (warps) per CTA of the three-colour stencil kernels
+// The FP32 link copy: each link's 18 floats (the FP64 order) padded to 80 bytes.
+constexpr int kLink32Floats = 20;
+constexpr int kLink32Vec4 = kLink32Floats / 4;
 
 __host__ __device__ inline size_t field_index3(int V, int mb, int site, int comp, int lane) {
     return (((size_t)mb * V + site) * kComp3 + comp) * kModeBlock + lane;
@@ -187,15 +190,21 @@ template <bool F32, bool U1> struct Links3 {
     int n01;
     template <typename T> __device__ __forceinline__ cmat3<T> get(int site, int mu) const {
         cmat3<T> M;
-        if (F32) {
-            const float2 *p = reinterpret_cast<const float2 *>(U) + 9 * (size_t)(3 * site + mu);
+        if (F32) {  // 80-byte records: five 16-byte loads
+            const float4 *p = reinterpret_cast<const float4 *>(U) + kLink32Vec4 * (size_t)(3 * site + mu);
+            float f[20];
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                const float4 v = __ldg(p + k);
+                f[4 * k] = v.x;
+                f[4 * k + 1] = v.y;
+                f[4 * k + 2] = v.z;
+                f[4 * k + 3] = v.w;
+            }
 #pragma unroll
             for (int i = 0; i < 3; i++)
 #pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    const float2 v = __ldg(p + i + 3 * j);
-                    M.m[i][j] = mk<T>((T)v.x, (T)v.y);
-                }
+                for (int j = 0; j < 3; j++) M.m[i][j] = mk<T>((T)f[2 * (i + 3 * j)], (T)f[2 * (i + 3 * j) + 1]);
         } else {
             const double2 *p = reinterpret_cast<const double2 *>(U) + 9 * (size_t)(3 * site + mu);
 #pragma unroll
