@@ -9,8 +9,10 @@ mode at one site advanced by one step.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload n16|n8]
 
 Default workload (n16): SU(2), N = 16^3, Wilson r = 1, m = 0.05, MDWHeight = 0,
-dt = 0.05, all 32768 modes (free plane waves), FP32 modes with FP64 links;
-seeded random links and electric field (links move every half step).  The
+dt = 0.05, all 32768 modes (free plane waves), FP32-class modes with FP64 links;
+quasi-particle gauge fields (occupancy 1/g^2 = 4 below Qs = 1, Gauss's law
+restored on the device) and a U(1) background with n_B = 4 flux quanta in the
+hopping term; links move every half step.  The
 modes (8.6 GB per field in FP32) exceed the 126 MB L2, so no L2 flush is
 needed between steps.  The line reports the FP32 fused form as `value`, the
 FP64 plain (two-phase, as the reference) and FP64 fused forms beside it, the
@@ -37,8 +39,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOADS = {
-    "n16": dict(N=(16, 16, 16), m=0.05, r=1.0, mdw=0.0, dt=0.05, link_sigma=0.3, e_sigma=0.1, seed=20261203,
-                ref_ranks=512),
+    "n16": dict(N=(16, 16, 16), m=0.05, r=1.0, mdw=0.0, dt=0.05, init="quasi", n0=4.0, qs=1.0, nb=4,
+                seed=20261203, ref_ranks=512),
     "n8": dict(N=(8, 8, 8), m=0.1, r=1.0, mdw=0.0, dt=0.05, link_sigma=0.3, e_sigma=0.0, seed=20261203,
                ref_ranks=64),
 }
@@ -46,6 +48,31 @@ METRIC = "mode-site updates/s"
 
 
 # ----------------------------------------------------------------- helpers --
+def gauge_fields(wl):
+    """(links, E) of a workload before Gauss's law is restored: quasi-particles
+    (occupancy n0 = 1/g^2 below Qs) or seeded random links and E."""
+    from overlap_b200.inputs import quasi_particles, random_efield, random_links
+
+    if wl.get("init") == "quasi":
+        return quasi_particles(wl["N"], wl["n0"], wl["qs"], wl["seed"])
+    return random_links(wl["N"], wl["link_sigma"], wl["seed"]), random_efield(wl["N"], wl["e_sigma"], wl["seed"] + 1)
+
+
+def setup_gauge(ctx, wl):
+    """Links, E (Gauss's law restored for the quasi-particle start, as
+    SetQuasiParticles does) and the U(1) background of the workload."""
+    from overlap_b200.inputs import u1_flux
+
+    U, E = gauge_fields(wl)
+    ctx.set_links(U)
+    ctx.set_efield(E)
+    if wl.get("init") == "quasi":
+        ctx.gauss_restore()
+    if wl.get("nb"):
+        ctx.set_u1(u1_flux(wl["N"], wl["nb"]))
+
+
+
 def volume(N):
     return N[0] * N[1] * N[2]
 
@@ -143,13 +170,15 @@ def _ref_worker(args):
     import numpy as np
 
     from _oracle import ptr, reference
-    from overlap_b200.inputs import random_efield, random_links
 
     R = reference("wilson")
     N = wl["N"]
     m = R.ovlref_init(*N, wl["ref_ranks"], rank, wl["m"], wl["r"], wl["mdw"], 1e300, wl["dt"], 1.0, 1)
-    R.ovlref_set_links(ptr(random_links(N, wl["link_sigma"], wl["seed"])))
-    R.ovlref_set_efield(ptr(np.ascontiguousarray(random_efield(N, wl["e_sigma"], wl["seed"] + 1))))
+    U, E = gauge_fields(wl)
+    R.ovlref_set_links(ptr(np.ascontiguousarray(U)))
+    R.ovlref_set_efield(ptr(np.ascontiguousarray(E)))
+    if wl.get("init") == "quasi":
+        R.ovlref_gauss_restore(ptr(np.zeros(2)))  # the reference's own GaussLawRestoration::Restore
     R.ovlref_set_free_fermions()
     if warmup:
         R.ovlref_step(warmup)
@@ -184,7 +213,6 @@ def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-
     import torch
 
     from overlap_b200 import Context
-    from overlap_b200.inputs import random_efield, random_links
 
     N = wl["N"]
     stream = torch.cuda.Stream(device)  # a real stream: the library and the events share it
@@ -192,8 +220,7 @@ def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-
                   dt=wl["dt"], t_sphaleron=1e300, device=device, stream=stream.cuda_stream, hop_variant=hop_variant,
                   mode_group=mode_group)
     ctx.torch_stream = stream  # keeps the stream alive as long as the context
-    ctx.set_links(random_links(N, wl["link_sigma"], wl["seed"]))
-    ctx.set_efield(random_efield(N, wl["e_sigma"], wl["seed"] + 1))
+    setup_gauge(ctx, wl)
     assert ctx.set_free_fermions() == 0
     if hop_variant < 0:
         variant, variant_ms = ctx.autotune()
@@ -228,13 +255,11 @@ def time_e2e(ctx, wl, steps, device):
     import numpy as np
     import torch
 
-    from overlap_b200.inputs import random_efield, random_links
-
     N = wl["N"]
     U = torch.empty((volume(N), 3, 4), dtype=torch.float64, pin_memory=True).numpy()
     E = torch.empty((volume(N), 3, 3), dtype=torch.float64, pin_memory=True).numpy()
-    U[...] = random_links(N, wl["link_sigma"], wl["seed"])
-    E[...] = random_efield(N, wl["e_sigma"], wl["seed"] + 1)
+    U[...] = ctx.get_links()
+    E[...] = ctx.get_efield()
     ctx.synchronize()
     barrier()
     t0 = time.perf_counter()
@@ -260,15 +285,13 @@ def accuracy(wl, steps, every, device):
     import torch
 
     from overlap_b200 import Context
-    from overlap_b200.inputs import random_efield, random_links
 
     N = wl["N"]
     series = {}
     for prec in ("fp64", "fp32", "fp40"):
         ctx = Context(N=N, n_modes=wl.get("modes"), precision=prec, form="fused", m_fermion=wl["m"], r_wilson=wl["r"],
                       m_dw=wl["mdw"], dt=wl["dt"], t_sphaleron=1e300, device=device)
-        ctx.set_links(random_links(N, wl["link_sigma"], wl["seed"]))
-        ctx.set_efield(random_efield(N, wl["e_sigma"], wl["seed"] + 1))
+        setup_gauge(ctx, wl)
         ctx.set_free_fermions()
         ctx.ncs_update()
         n5 = [ctx.charges()["N5"]]
@@ -504,10 +527,18 @@ def main():
     if args.modes:
         M = wl["modes"] = min(args.modes, M)
     rank, world, local = init_dist()
+    if wl.get("init") == "quasi":
+        init = (f"quasi-particles (occupancy n0=1/g^2={wl['n0']} below Qs={wl['qs']}, seed {wl['seed']}), Gauss law "
+                f"restored; links updated every half step")
+    else:
+        init = (f"seeded random links (sigma={wl['link_sigma']}) and E (sigma={wl['e_sigma']}), links updated every "
+                f"half step")
+    if wl.get("nb"):
+        init += (f"; U(1) background B along z, n_B={wl['nb']} flux quanta, in the hopping term (the reference arm's "
+                 f"hop has no U(1) term; its cost does not depend on the background)")
     config = {"workload": f"SU(2) Wilson fermions, N={N[0]}x{N[1]}x{N[2]}, {M} modes (plane-wave basis), "
                           f"r={wl['r']}, m={wl['m']}, MDWHeight={wl['mdw']}, dt={wl['dt']}",
-              "lattice": list(N), "modes": M, "gauge_init": f"seeded random links (sigma={wl['link_sigma']}) and "
-              f"E (sigma={wl['e_sigma']}), links updated every half step",
+              "lattice": list(N), "modes": M, "gauge_init": init,
               "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"}
 
     if args.impl == "reference":

@@ -136,3 +136,62 @@ def embed_su2_efield(E2: np.ndarray) -> np.ndarray:
     E = np.zeros(np.asarray(E2).shape[:-1] + (8,))
     E[..., :3] = E2
     return E
+
+
+# -------------------------------------------------------- quasi-particles --
+def quasi_particles(N, n0: float, qs: float, seed: int, n_colours: int = 2):
+    """Quasi-particle gauge fields, InitialConditions::SetQuasiParticles
+    (INITIALCONDITIONS/SetQuasiParticles.cpp:28-157) for a = 1, Minkowski metric:
+    per lattice momentum p_mu = -i (1 - e^{-2 pi i k_mu / N_mu}) (LATTICE/Momenta.cpp:4-8),
+    two transverse polarisations xi_1, xi_2 from the base vector
+    (1/sqrt3, 1/sqrt2, 1/sqrt6) (MISC/MinkowskiWaveVectors.cpp:7-44), occupancy
+    f(p) = n0 / sqrt(p^2/Qs^2 + 0.1) below Qs, zero above; per colour component
+    complex Gaussians c_1, c_2 (variance 1); A(p) = sqrt(f V) (c_1 xi_1 + c_2 xi_2),
+    E(p) = sqrt(f V) i omega (c_1 xi_1 + c_2 xi_2); the unnormalised inverse FFT
+    (FFTW_BACKWARD), A(x) = 2 Re A / V, E(x) = 2 Re E / V, and U = exp(-i A^a t^a).
+
+    The reference draws c_1, c_2 from its GSL generator in (kx, ky, kz, a) order;
+    here numpy's generator draws them in the same order, so the fields follow the
+    same distribution but are not the same numbers.  Returns (links, E) in the
+    layouts of Context.set_links / set_efield; restore Gauss's law afterwards
+    (Context.gauss_restore), as the reference does.
+    """
+    N = tuple(int(n) for n in N)
+    ncomp = n_colours * n_colours - 1
+    rng = np.random.default_rng(seed)
+    k = np.meshgrid(*[np.arange(n) for n in N], indexing="ij")  # (kx, ky, kz)
+    cdp = [-1j * (1.0 - np.exp(-2j * np.pi * k[m] / N[m])) for m in range(3)]
+    p2 = sum(np.abs(c) ** 2 for c in cdp)
+    omega = np.sqrt(p2)
+    pv = [np.sign(c.real) * np.abs(c) for c in cdp]
+    psq = sum(v * v for v in pv)
+    occ = np.where(psq < qs * qs, n0 / np.sqrt(psq / (qs * qs) + 0.1), 0.0)
+    base = np.array([1 / np.sqrt(3.0), 1 / np.sqrt(2.0), 1 / (np.sqrt(2.0) * np.sqrt(3.0))])
+    safe = np.where(p2 > 0, p2, 1.0)
+    bdp = base[0] * cdp[0] + base[1] * cdp[1] + base[2] * cdp[2]
+    norm = np.sqrt(np.abs(base @ base - (bdp * np.conj(bdp)).real / safe))
+    norm = np.where(p2 > 0, norm, 1.0)
+    om = np.where(p2 > 0, omega, 1.0)
+    xi1 = [np.where(p2 > 0, (base[m] - bdp * np.conj(cdp[m]) / safe) / (norm * np.sqrt(2.0 * om)), 0.0) for m in range(3)]
+    xi2 = [np.where(p2 > 0, (cdp[(m + 1) % 3] * np.conj(xi1[(m + 2) % 3]) - cdp[(m + 2) % 3] * np.conj(xi1[(m + 1) % 3])) / om,
+                    0.0) for m in range(3)]
+    # complex Gaussians c_1, c_2 per (kx, ky, kz, a), drawn in that loop order
+    g = rng.normal(size=N + (ncomp, 2, 2))
+    c = (g[..., 0] + 1j * g[..., 1]) / np.sqrt(2.0)  # [..., a, (c1, c2)]
+    V = N[0] * N[1] * N[2]
+    amp = np.sqrt(occ) * np.sqrt(V)
+    A = np.empty((3,) + N + (ncomp,), complex)
+    E = np.empty_like(A)
+    for m in range(3):
+        mode = c[..., 0] * xi1[m][..., None] + c[..., 1] * xi2[m][..., None]
+        A[m] = amp[..., None] * mode
+        E[m] = amp[..., None] * 1j * omega[..., None] * mode
+    # unnormalised backward transform over (x, y, z) times 1/V: numpy's ifftn; then 2 Re
+    Ax = 2.0 * np.fft.ifftn(A, axes=(1, 2, 3)).real
+    Ex = 2.0 * np.fft.ifftn(E, axes=(1, 2, 3)).real
+    # [mu, x, y, z, a] -> [site = x + N0 (y + N1 z), mu, a]
+    Ax = np.transpose(Ax, (3, 2, 1, 0, 4)).reshape(V, 3, ncomp)
+    Ex = np.ascontiguousarray(np.transpose(Ex, (3, 2, 1, 0, 4)).reshape(V, 3, ncomp))
+    if n_colours == 2:
+        return np.ascontiguousarray(su2_exp(Ax, -1.0)), Ex
+    return su3_pack(su3_exp(Ax, -1.0)), Ex

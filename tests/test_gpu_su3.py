@@ -231,19 +231,19 @@ def _overlap_kw(precision):
 def test_chebyshev_overlap_operator_and_leapfrog(precision):
     U = random_links_su3(N, 0.6, 16)
     E = random_efield_su3(N, 0.3, 17)
-    phi = modes3(8, 18)
-    mid = modes3(8, 19)
+    phi = modes3(40, 18)  # two mode blocks: the split recurrence
+    mid = modes3(40, 19)
     p = oracle_params(N, m=0.05, mdw=1.0, dt=0.05)
     lmax = (0.5 * abs(6 + 2 * 0.05 - 2 * 1.0) + 3.0) ** 2  # the context's default bound on h_W^2
     want = np.zeros_like(phi)
-    for m in range(8):
+    for m in range(40):
         oracle().orc3_overlap_apply(C.byref(p), ptr(f64(U)), ptr(f64(phi[m])), ptr(f64(want[m])), 48, 0.01, lmax)
     t = C.c_int(0)
     o_psi, o_mid, o_U = phi.copy(), mid.copy(), f64(U).copy()
-    oracle().orc3_overlap_leapfrog(C.byref(p), ptr(o_U), ptr(E), ptr(f64(o_psi)), ptr(f64(o_mid)), 8, C.byref(t), 2, 48,
+    oracle().orc3_overlap_leapfrog(C.byref(p), ptr(o_U), ptr(E), ptr(f64(o_psi)), ptr(f64(o_mid)), 40, C.byref(t), 2, 48,
                                    0.01, lmax)
     tol = 1e-11 if precision == "fp64" else 1e-4
-    with ctx3(n_modes=8, **_overlap_kw(precision)) as ctx:
+    with ctx3(n_modes=40, **_overlap_kw(precision)) as ctx:
         ctx.set_links(U)
         ctx.set_efield(E)
         assert rel_err(ctx.apply(phi), want) < tol
@@ -255,11 +255,11 @@ def test_chebyshev_overlap_operator_and_leapfrog(precision):
     assert max(rel_err(g_psi, o_psi), rel_err(g_mid, o_mid)) < tol
     # overlap N_5: local bilinears with O = -i h_ov psi (OverlapCurrents.cpp:35-212, three colours)
     O = np.zeros_like(o_psi)
-    for m in range(8):
+    for m in range(40):
         oracle().orc3_overlap_apply(C.byref(p), ptr(o_U), ptr(f64(o_psi[m])), ptr(f64(O[m])), 48, 0.01, lmax)
     g5 = np.array([[0, 0, 1, 0], [0, 0, 0, 1], [1, 0, 0, 0], [0, 1, 0, 0]], complex)
     g0 = np.diag([1, 1, -1, -1]).astype(complex)
-    w = np.where(np.arange(8) % 2 == 0, 1.0, -1.0)
+    w = np.where(np.arange(40) % 2 == 0, 1.0, -1.0)
     a1 = np.einsum("msca,ab,mscb->m", np.conj(o_psi), g5, o_psi).real
     a2 = np.einsum("msca,ab,mscb->m", np.conj(o_psi), g5 @ g0, O).imag
     n5 = float(np.sum(w * (a1 + 0.5 * a2)) / (2 * volume(N)))
