@@ -60,7 +60,9 @@ typedef enum { OVL_FORM_PLAIN = 0, OVL_FORM_FUSED = 1 } ovl_form;
 
 typedef struct {
     int N[3];             /* lattice extents N0, N1, N2 */
-    int n_colours;        /* colours; 2 (SU(2)) */
+    int n_colours;        /* colours: 2 (SU(2), the reference's) or 3 (SU(3): links 9 complex
+                             doubles per (site, mu) at U_ij = i + 3j, SUNc/SU3/GroupOperations.cpp:4-12;
+                             E 8 per (site, mu); modes [mode][site][colour 3][spin 4]) */
     int n_modes;          /* modes held by this context */
     int first_mode;       /* global index of local mode 0 (MPI/ModePartition.cpp:12-24) */
     int fermion;          /* ovl_fermion */
@@ -83,7 +85,9 @@ typedef struct {
     /* OVL_SIGN_ZOLOTAREV (the reference's rational approximation, FP64) or
      * OVL_SIGN_CHEBYSHEV: (h_W^2)^(-1/2) as a degree-cheb_degree Chebyshev
      * series of x^(-1/2) on [cheb_eps, 1] after scaling h_W^2 by lambda_max
-     * (FP32 or FP64). */
+     * (FP32 or FP64).  Without a bounds schedule (and, for two colours, without
+     * ritz_auto) lambda_max = (|6r + 2m - 2M|/2 + 3)^2, a bound on h_W^2 for every
+     * gauge field.  Three colours: Chebyshev only. */
     int sign_method;
     int cheb_degree;
     double cheb_eps;
@@ -92,7 +96,8 @@ typedef struct {
      * same results. */
     int hop_variant;
     /* 1: project every link back onto SU(2) after each update (U / |U|,
-     * MaxTraceProjection, SUNc/SU2/GroupOperations.cpp:261-281).  The reference
+     * MaxTraceProjection, SUNc/SU2/GroupOperations.cpp:261-281), or onto SU(3)
+     * (Gram-Schmidt of the rows, unit determinant).  The reference
      * only measures the unitarity violation (OBSERVABLES/UnitarityViolation.cpp),
      * so 0 reproduces it. */
     int reunitarize;

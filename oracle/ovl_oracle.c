@@ -300,22 +300,45 @@ void orc_wilson_leapfrog(const orc_params *p, double *U, const double *E, double
 
 /* ------------------------------------------------------------ plane waves -- */
 
-static int free_spinor(const orc_params *p, const int k[3], int spin, int particle, cplx u[4], double *omega) {
+/* Wilson spinors (GetWilsonDiracSpinor, FermionField.cpp:145-317) or, with
+ * `overlap`, overlap spinors (GetOverlapDiracSpinor, :331-517): the same
+ * helicity construction with p = M hp / s, meff = M (1 + hp5 / s),
+ * hp = sin(2 pi n / N), hp5 = 3 - M - sum cos(2 pi n / N), s = |(hp, hp5)|. */
+static int free_spinor_kind(const orc_params *p, const int k[3], int spin, int particle, int overlap, cplx u[4],
+                            double *omega) {
     const double TWO_PI = 2.0 * M_PI;
     double pp[3], meff = p->m_fermion, p2 = 0.0;
-    for (int i = 0; i < 3; i++) {
-        int n = particle == 0 ? k[i] : p->N[i] - k[i];  /* antiparticles carry -p (FermionField.cpp:168-174) */
-        pp[i] = sin(TWO_PI * n / (double)p->N[i]);
-        double h = sin(M_PI * n / (double)p->N[i]);
-        meff += 2.0 * p->r_wilson * h * h;
-        p2 += pp[i] * pp[i];
+    if (overlap) {
+        double hp5 = 3.0 - p->m_dw, s2 = 0.0;
+        for (int i = 0; i < 3; i++) {
+            int n = particle == 0 ? k[i] : p->N[i] - k[i];
+            pp[i] = sin(TWO_PI * n / (double)p->N[i]);
+            hp5 -= cos(TWO_PI * n / (double)p->N[i]);
+            s2 += pp[i] * pp[i];
+        }
+        double sabs = sqrt(s2 + hp5 * hp5);
+        for (int i = 0; i < 3; i++) {
+            pp[i] = p->m_dw * pp[i] / sabs;
+            p2 += pp[i] * pp[i];
+        }
+        meff = p->m_dw * (1.0 + hp5 / sabs);
+    } else {
+        for (int i = 0; i < 3; i++) {
+            int n = particle == 0 ? k[i] : p->N[i] - k[i];  /* antiparticles carry -p (FermionField.cpp:168-174) */
+            pp[i] = sin(TWO_PI * n / (double)p->N[i]);
+            double h = sin(M_PI * n / (double)p->N[i]);
+            meff += 2.0 * p->r_wilson * h * h;
+            p2 += pp[i] * pp[i];
+        }
     }
     double pabs = sqrt(p2);
     double w = sqrt(p2 + meff * meff);
     *omega = particle == 0 ? w : -w;
 
+    /* the axis cases test k == 0 or k == N/2 in integer division (FermionField.cpp:188,229):
+     * for odd N the momentum index (N-1)/2 takes them too */
     int edge[3];
-    for (int i = 0; i < 3; i++) edge[i] = (k[i] == 0 || 2 * k[i] == p->N[i]);
+    for (int i = 0; i < 3; i++) edge[i] = (k[i] == 0 || k[i] == p->N[i] / 2);
     /* two-spinor of definite helicity (:185-226) */
     cplx phi[2];
     double hel;
@@ -359,6 +382,9 @@ static int free_spinor(const orc_params *p, const int k[3], int spin, int partic
     return bad;
 }
 
+static int g_free_overlap = 0;  /* plane waves of orc_free_fermions / orc3_free_fermions: 1 = overlap spinors */
+void orc_set_free_kind(int overlap) { g_free_overlap = overlap; }
+
 int orc_free_fermions(const orc_params *p, int first, int nmodes, double *psi, double *psimid) {
     const int V = volume(p);
     int failures = 0;
@@ -374,7 +400,7 @@ int orc_free_fermions(const orc_params *p, int first, int nmodes, double *psi, d
         k[2] = g % p->N[2];
         cplx u[4];
         double omega;
-        failures += free_spinor(p, k, spin, particle, u, &omega);
+        failures += free_spinor_kind(p, k, spin, particle, g_free_overlap, u, &omega);
         cplx half = cexp(-0.5 * I * omega * p->dt);
         cplx *f = (cplx *)psi + (size_t)SPINOR * V * m;
         cplx *fm = (cplx *)psimid + (size_t)SPINOR * V * m;
@@ -1202,7 +1228,7 @@ int orc3_free_fermions(const orc_params *p, int first, int nmodes, double *psi, 
         k[2] = g % p->N[2];
         cplx u[4];
         double omega;
-        failures += free_spinor(p, k, spin, particle, u, &omega);
+        failures += free_spinor_kind(p, k, spin, particle, g_free_overlap, u, &omega);
         cplx half = cexp(-0.5 * I * omega * p->dt);
         cplx *f = (cplx *)psi + (size_t)SPINOR3 * V * m;
         cplx *fm = (cplx *)psimid + (size_t)SPINOR3 * V * m;

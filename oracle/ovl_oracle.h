@@ -109,6 +109,9 @@ int orc_gauss_restore(const orc_params *p, const double *U, double *E, int max_i
  * links double[V][3][9][2] (U_ij at i + 3j), E double[V][3][8],
  * modes [mode][site][colour 3][spin 4][re, im]. */
 void orc3_exp(double c, const double alpha[8], double out[18]);
+/* Plane waves of orc_free_fermions / orc3_free_fermions: 0 Wilson spinors
+ * (default), 1 overlap spinors (FermionField.cpp:331-517). */
+void orc_set_free_kind(int overlap);
 void orc3_wilson_apply(const orc_params *p, const double *U, const double *phi, double *out);
 void orc3_update_links(const orc_params *p, double *U, const double *E, double dt_step);
 void orc3_update_efield(const orc_params *p, const double *U, double *E, double dt_step);

@@ -223,7 +223,9 @@ int ritz_bounds(ovl_ctx *c, const double *start, double out[2], double raw[2], i
 // ritz_auto, fresh Ritz bounds (OverlapUpdate.cpp:105,119 compute them before
 // every half step).  `consume` advances the schedule.
 int take_bounds(ovl_ctx *c, bool consume, double &lo, double &hi) {
-    if (c->bounds.empty() && su3(c)) {  // the series on [eps, 1] of h^2 / bound
+    // the Chebyshev series without a schedule or Ritz bounds: on [eps, 1] of
+    // h^2 / (the bound on h_W^2 that holds for every gauge field)
+    if (c->bounds.empty() && c->p.sign_method == OVL_SIGN_CHEBYSHEV && (su3(c) || !c->p.ritz_auto)) {
         hi = wilson_norm_bound2(c->p);
         lo = c->p.cheb_eps * hi;
         return OVL_OK;
@@ -921,11 +923,12 @@ int ovl_set_free_fermions(ovl_ctx *c, int *n_bad) {
     if (rc) return rc;
     if (fp32(c))
         ovl::launch_free_fermions<float>(c->psi, c->psimid, c->L, c->p.n_modes, c->n_mb, c->p.first_mode, c->p.r_wilson,
-                                         c->p.m_fermion, c->p.dt, c->dev_int, c->stream, nullptr, nullptr, c->nc);
+                                         c->p.m_fermion, c->p.dt, c->dev_int, c->stream, nullptr, nullptr, c->nc,
+                                         overlap(c), c->p.m_dw);
     else  // FP64, or FP40 (the extension arrays set)
         ovl::launch_free_fermions<double>(c->psi, c->psimid, c->L, c->p.n_modes, c->n_mb, c->p.first_mode, c->p.r_wilson,
                                           c->p.m_fermion, c->p.dt, c->dev_int, c->stream, c->psi_lo, c->psimid_lo,
-                                          c->nc);
+                                          c->nc, overlap(c), c->p.m_dw);
     if ((rc = launched(c, 2, "free fermions"))) return rc;
     int bad = 0;
     OVL_CUDA(c, cudaMemcpyAsync(&bad, c->dev_int, sizeof(int), cudaMemcpyDeviceToHost, c->stream));

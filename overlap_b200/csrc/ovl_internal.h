@@ -220,11 +220,13 @@ void chebyshev_apply(ChebyshevWork &w, const double *U, const double *u1, const 
                      int n_mb, const double *coeff, int K, double eps, double lambda_max, double amass, double mdw,
                      double mf, double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches);
 
-// Free Wilson plane waves for local modes [0, n_modes) (global index first_mode + m).
+// Free plane waves for local modes [0, n_modes) (global index first_mode + m):
+// Wilson spinors, or overlap spinors of Wilson kernel mass -m_dw.
 template <typename T>
 void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes, int n_mb, int first_mode,
                           double r_wilson, double m_fermion, double dt, int *bad, cudaStream_t stream,
-                          void *lo_psi = nullptr, void *lo_mid = nullptr, int nc = 2);
+                          void *lo_psi = nullptr, void *lo_mid = nullptr, int nc = 2, bool overlap = false,
+                          double m_dw = 0.0);
 
 // ------------------------------------------------------------ three colours --
 // ovl_su3.cu; layouts in ovl_su3.cuh.  Links of the hop kernels: FP64 (U,

@@ -425,13 +425,18 @@ void launch_blocks_to_ref(const void *blocks, double *ref, const Lattice &L, int
 
 // ------------------------------------------------------------ plane waves --
 // InitialConditions::SetFreeFermions with GetWilsonDiracSpinor / GetWilsonPhase
-// (SetFreeFermions.cpp:3-56, FermionField.cpp:145-328): mode index
+// (SetFreeFermions.cpp:3-56, FermionField.cpp:145-328), or for overlap
+// fermions GetOverlapDiracSpinor / GetOverlapPhase (FermionField.cpp:331-528):
+// the same helicity spinors of the momentum p and mass meff, which for the
+// overlap operator are p = M hp / s and meff = M (1 + hp5 / s) with
+// hp = sin(2 pi n / N), hp5 = 3 - M - sum cos(2 pi n / N), s = |(hp, hp5)|.
+// Mode index
 // particle + 2(colour + Nc(spin + 2(px + N0(py + N1 pz)))); particles
 // exp(+i p.x) with frequency +w, antiparticles exp(-i p.x) with -w; psimid =
 // psi exp(-i w dt / 2).
 struct FreeMode { double u[8]; double omega; int colour, k0, k1, k2, particle, bad; };
 
-__device__ FreeMode free_mode(const Lattice &L, int g, double r, double m, int nc) {
+__device__ FreeMode free_mode(const Lattice &L, int g, double r, double m, int nc, int overlap, double mdw) {
     FreeMode fm;
     const int N[3] = {L.N0, L.N1, L.N2};
     fm.particle = g % 2; g /= 2;
@@ -443,19 +448,37 @@ __device__ FreeMode free_mode(const Lattice &L, int g, double r, double m, int n
     k[2] = g % N[2];
     fm.k0 = k[0]; fm.k1 = k[1]; fm.k2 = k[2];
     double pp[3], meff = m, p2 = 0.0;
-    for (int i = 0; i < 3; i++) {
-        const int n = fm.particle == 0 ? k[i] : N[i] - k[i];
-        pp[i] = sin(2.0 * M_PI * n / (double)N[i]);
-        const double h = sin(M_PI * n / (double)N[i]);
-        meff += 2.0 * r * h * h;
-        p2 += pp[i] * pp[i];
+    if (overlap) {
+        double hp5 = 3.0 - mdw, s2 = 0.0;
+        for (int i = 0; i < 3; i++) {
+            const int n = fm.particle == 0 ? k[i] : N[i] - k[i];
+            pp[i] = sin(2.0 * M_PI * n / (double)N[i]);
+            hp5 -= cos(2.0 * M_PI * n / (double)N[i]);
+            s2 += pp[i] * pp[i];
+        }
+        const double sabs = sqrt(s2 + hp5 * hp5);
+        for (int i = 0; i < 3; i++) {
+            pp[i] = mdw * pp[i] / sabs;
+            p2 += pp[i] * pp[i];
+        }
+        meff = mdw * (1.0 + hp5 / sabs);
+    } else {
+        for (int i = 0; i < 3; i++) {
+            const int n = fm.particle == 0 ? k[i] : N[i] - k[i];
+            pp[i] = sin(2.0 * M_PI * n / (double)N[i]);
+            const double h = sin(M_PI * n / (double)N[i]);
+            meff += 2.0 * r * h * h;
+            p2 += pp[i] * pp[i];
+        }
     }
     const double pabs = sqrt(p2);
     const double w = sqrt(p2 + meff * meff);
     const double omega = fm.particle == 0 ? w : -w;
     fm.omega = omega;
+    // the axis cases test k == 0 or k == N/2 in integer division (FermionField.cpp:188,229):
+    // for odd N the index (N-1)/2 takes them too, and its spinor fails the eigen check
     bool edge[3];
-    for (int i = 0; i < 3; i++) edge[i] = (k[i] == 0 || 2 * k[i] == N[i]);
+    for (int i = 0; i < 3; i++) edge[i] = (k[i] == 0 || k[i] == N[i] / 2);
     cpx<double> phi0, phi1;
     double hel;
     if (edge[0] && edge[1]) {
@@ -510,10 +533,10 @@ __device__ FreeMode free_mode(const Lattice &L, int g, double r, double m, int n
 }
 
 __global__ void free_modes_kernel(FreeMode *info, int n_modes, int first_mode, Lattice L, double r, double m, int *bad,
-                                  int nc) {
+                                  int nc, int overlap, double mdw) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_modes) return;
-    FreeMode fm = free_mode(L, first_mode + i, r, m, nc);
+    FreeMode fm = free_mode(L, first_mode + i, r, m, nc, overlap, mdw);
     info[i] = fm;
     if (fm.bad) atomicAdd(bad, 1);
 }
@@ -560,12 +583,12 @@ __global__ void free_fill_kernel(const FreeMode *__restrict__ info, cpx<T> *psi,
 template <typename T>
 void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes, int n_mb, int first_mode,
                           double r_wilson, double m_fermion, double dt, int *bad, cudaStream_t stream, void *lo_psi,
-                          void *lo_mid, int nc) {
+                          void *lo_mid, int nc, bool overlap, double m_dw) {
     FreeMode *info = nullptr;
     cudaMallocAsync(&info, sizeof(FreeMode) * (size_t)n_modes, stream);
     cudaMemsetAsync(bad, 0, sizeof(int), stream);
     free_modes_kernel<<<(n_modes + 127) / 128, 128, 0, stream>>>(info, n_modes, first_mode, L, r_wilson, m_fermion, bad,
-                                                                 nc);
+                                                                 nc, overlap ? 1 : 0, m_dw);
     dim3 block(kModeBlock, kSitesPerCta);
     dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
     free_fill_kernel<T><<<grid, block, 0, stream>>>(info, reinterpret_cast<cpx<T> *>(psi), reinterpret_cast<cpx<T> *>(psimid),
@@ -584,7 +607,7 @@ void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes
     template void launch_blocks_to_ref<T>(const void *, double *, const Lattice &, int, int, cudaStream_t,          \
                                           const void *, int);                                                       \
     template void launch_free_fermions<T>(void *, void *, const Lattice &, int, int, int, double, double, double,    \
-                                          int *, cudaStream_t, void *, void *, int);
+                                          int *, cudaStream_t, void *, void *, int, bool, double);
 OVL_INSTANTIATE(double)
 OVL_INSTANTIATE(float)
 

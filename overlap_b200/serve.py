@@ -1,13 +1,16 @@
 """Serving: trajectory requests arrive over time, are admitted as device
-memory frees up, and advance together in one batched ensemble (continuous
-batching: a request that arrives while others run joins the ensemble at the
-next tick, and a finished one leaves it).  Each request's observables --
-N_5, N_CS along the cooling-free path (ovl_ncs_update) and the gauge energy --
-are streamed back every `observe_every` steps.
+memory frees up, and advance together (continuous batching: a request that
+arrives while others run joins at the next tick, and a finished one leaves).
+SU(2) Wilson requests share one batched ensemble (one CUDA graph per step for
+all of them); SU(3) and overlap requests, which the batched kernels do not
+cover, run as contexts of their own on their own streams, stepped in the same
+ticks so their kernels overlap the ensemble's on the GPU.  Each request's
+observables -- N_5, N_CS along the cooling-free path (ovl_ncs_update) and the
+gauge energy -- are streamed back every `observe_every` steps.
 
 No counterpart in the reference, whose driver runs one trajectory per job
-(Simulation.cpp).  Requests are SU(2) Wilson fermions in the fused form; all
-requests of a server share its precision.
+(Simulation.cpp).  All requests of a server share its precision (FP32 or FP64;
+overlap requests use the Chebyshev sign function).
 """
 from __future__ import annotations
 
@@ -16,8 +19,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .api import Ensemble, Params
-from .inputs import random_efield, random_links, u1_flux, volume
+from .api import Context, Ensemble, Params
+from .inputs import random_efield, random_efield_su3, random_links, random_links_su3, u1_flux, volume
 
 
 @dataclass
@@ -31,7 +34,11 @@ class Request:
     n_b: int = 0                 # U(1) flux quanta (QED.cpp:62-84); 0: none
     link_sigma: float = 0.3      # seeded random links, exp(i A.sigma/2), A ~ N(0, sigma^2)
     e_sigma: float = 0.1         # seeded random E
-    stochastic: bool = True      # Z2 stochastic vacuum modes; False: plane waves (n_modes = 8V)
+    stochastic: bool = True      # Z2 stochastic vacuum modes; False: plane waves (n_modes = 4 Nc V)
+    n_colours: int = 2           # 2: SU(2); 3: SU(3)
+    fermion: str = "wilson"      # or "overlap" (Chebyshev sign function)
+    cheb_degree: int = 64
+    m_dw: float = 1.0            # overlap: Wilson kernel mass -m_dw
     seed: int = 0
     observe_every: int = 50
     arrival: float = 0.0         # seconds after the server's start
@@ -44,14 +51,22 @@ class Request:
     def mode_sites(self) -> int:
         return self.n_modes * volume(self.N)
 
+    def batchable(self) -> bool:
+        """SU(2) Wilson requests join the batched ensemble."""
+        return self.n_colours == 2 and self.fermion == "wilson"
+
 
 def request_bytes(req: Request, precision: str) -> int:
     """Device memory of a request's context: four mode fields (psi, psimid,
-    and the two operator buffers), links, E and reduction scratch."""
+    and the two operator buffers; four more for the Chebyshev recurrence of
+    overlap requests), links, E and reduction scratch."""
     n_mb = (req.n_modes + 31) // 32
     V = volume(req.N)
+    comp = 4 * req.n_colours
     per_complex = {"fp64": 16, "fp32": 8, "fp40": 10}[precision]
-    return 4 * n_mb * V * 8 * 32 * per_complex + V * (96 + 72 + 48) + 64 * V * 8 + (8 << 20)
+    fields = 8 if req.fermion == "overlap" else 4
+    links = 3 * V * (144 + 80 + 64) if req.n_colours == 3 else V * (96 + 72 + 48)
+    return fields * n_mb * V * comp * 32 * per_complex + links + 64 * V * 8 + (8 << 20)
 
 
 class Server:
@@ -76,28 +91,45 @@ class Server:
         self.memory_bytes = int(memory_bytes)
         self.ensemble: Ensemble | None = None
         self.active: list[Request] = []  # in ensemble member order
+        self.solo: list[tuple[Request, object]] = []  # requests with contexts of their own
         self.done: list[Request] = []
         self.used_bytes = 0
         self._next_id = 0
 
     # ------------------------------------------------------------ members
     def _params(self, r: Request) -> Params:
-        return Params(N=tuple(r.N), n_modes=r.n_modes, first_mode=0, precision=self.precision, form="fused",
-                      m_fermion=r.m_fermion, r_wilson=1.0, m_dw=0.0, dt=r.dt, t_sphaleron=1e300,
+        if r.fermion == "overlap":
+            return Params(N=tuple(r.N), n_colours=r.n_colours, n_modes=r.n_modes, first_mode=0,
+                          precision=self.precision, fermion="overlap", sign_method="chebyshev",
+                          cheb_degree=r.cheb_degree, m_fermion=r.m_fermion, r_wilson=1.0, m_dw=r.m_dw, dt=r.dt,
+                          t_sphaleron=1e300, device=self.device)
+        return Params(N=tuple(r.N), n_colours=r.n_colours, n_modes=r.n_modes, first_mode=0, precision=self.precision,
+                      form="fused", m_fermion=r.m_fermion, r_wilson=1.0, m_dw=0.0, dt=r.dt, t_sphaleron=1e300,
                       device=self.device)
 
     def _admit(self, r: Request, now: float):
         p = self._params(r)
-        if self.ensemble is None:
+        if not r.batchable():
+            import torch
+
+            stream = torch.cuda.Stream(self.device)
+            p.stream = stream.cuda_stream
+            ctx = Context(p)
+            ctx.torch_stream = stream  # keeps the stream alive with the context
+        elif self.ensemble is None:
             self.ensemble = Ensemble([p])
             ctx = self.ensemble[0]
         else:
             ctx = self.ensemble.add(p)
-        ctx.set_links(random_links(r.N, r.link_sigma, r.seed))
-        ctx.set_efield(random_efield(r.N, r.e_sigma, r.seed + 1))
+        if r.n_colours == 3:
+            ctx.set_links(random_links_su3(r.N, r.link_sigma, r.seed))
+            ctx.set_efield(random_efield_su3(r.N, r.e_sigma, r.seed + 1))
+        else:
+            ctx.set_links(random_links(r.N, r.link_sigma, r.seed))
+            ctx.set_efield(random_efield(r.N, r.e_sigma, r.seed + 1))
         if r.n_b:
             ctx.set_u1(u1_flux(r.N, r.n_b))
-        if r.stochastic:
+        if r.stochastic and r.fermion == "wilson":  # the Z2 modes are projected with the Wilson h(p)
             ctx.set_stochastic_modes(seed=r.seed + 2)
         else:
             ctx.set_free_fermions()
@@ -106,7 +138,10 @@ class Server:
         r._step = 0
         r._ncs = 0.0
         self._observe(r, ctx)
-        self.active.append(r)
+        if r.batchable():
+            self.active.append(r)
+        else:
+            self.solo.append((r, ctx))
         self.used_bytes += request_bytes(r, self.precision)
 
     def _observe(self, r: Request, ctx):
@@ -118,6 +153,14 @@ class Server:
     def _retire(self, i: int, now: float):
         r = self.active.pop(i)
         self.ensemble.remove(i)
+        self._finish(r, now)
+
+    def _retire_solo(self, i: int, now: float):
+        r, ctx = self.solo.pop(i)
+        ctx.close()
+        self._finish(r, now)
+
+    def _finish(self, r: Request, now: float):
         r.finished = now
         self.used_bytes -= request_bytes(r, self.precision)
         self.done.append(r)
@@ -138,7 +181,7 @@ class Server:
         rejected = []
         t0 = time.perf_counter()
         work = 0
-        while pending or queue or self.active:
+        while pending or queue or self.active or self.solo:
             now = time.perf_counter() - t0
             while pending and pending[0].arrival <= now:
                 r = pending.pop(0)
@@ -148,26 +191,36 @@ class Server:
                     queue.append(r)
             while queue and self.used_bytes + request_bytes(queue[0], self.precision) <= self.memory_bytes:
                 self._admit(queue.pop(0), time.perf_counter() - t0)
-            if not self.active:
+            if not self.active and not self.solo:
                 if pending:
                     time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - t0))))
                 continue
             # a tick: as many steps as no active request passes an observation or its end
+            running = self.active + [r for r, _ in self.solo]
             k = self.tick_steps
-            for r in self.active:
+            for r in running:
                 k = min(k, r.steps - r._step, r.observe_every - r._step % r.observe_every)
-            self.ensemble.step(k)
-            for r in self.active:
+            if self.active:
+                self.ensemble.step(k)
+            for _, ctx in self.solo:  # queued on their own streams, beside the ensemble's graph
+                ctx.step(k)
+            for r in running:
                 r._step += k
                 work += k * r.mode_sites()
             for i in range(len(self.active) - 1, -1, -1):
                 r = self.active[i]
                 if r._step % r.observe_every == 0 or r._step == r.steps:
                     self._observe(r, self.ensemble[i])
+            for r, ctx in self.solo:
+                if r._step % r.observe_every == 0 or r._step == r.steps:
+                    self._observe(r, ctx)
             now = time.perf_counter() - t0
             for i in range(len(self.active) - 1, -1, -1):
                 if self.active[i]._step >= self.active[i].steps:
                     self._retire(i, now)
+            for i in range(len(self.solo) - 1, -1, -1):
+                if self.solo[i][0]._step >= self.solo[i][0].steps:
+                    self._retire_solo(i, now)
         wall = time.perf_counter() - t0
         lat = np.array([r.finished - r.arrival for r in self.done]) if self.done else np.zeros(1)
         wait = np.array([r.admitted - r.arrival for r in self.done]) if self.done else np.zeros(1)
@@ -177,25 +230,36 @@ class Server:
                 "queue_wait_p50_s": float(np.percentile(wait, 50)), "queue_wait_p99_s": float(np.percentile(wait, 99))}
 
     def close(self):
+        for _, ctx in self.solo:
+            ctx.close()
+        self.solo = []
         if self.ensemble is not None:
             self.ensemble.close()
             self.ensemble = None
 
 
 def poisson_requests(count: int, rate: float, seed: int, sizes=(8, 12, 16, 24), modes=(4096, 8192),
-                     steps=(200, 2000), observe_every: int = 50) -> list[Request]:
+                     steps=(200, 2000), observe_every: int = 50, su3_fraction: float = 0.0,
+                     overlap_fraction: float = 0.0, overlap_sizes=(8,), overlap_steps=(100, 200)) -> list[Request]:
     """`count` requests with exponential inter-arrival times (mean 1/rate s),
     N uniform over `sizes`, modes uniform over [modes[0], modes[1]] in pairs,
     steps uniform over [steps[0], steps[1]] in multiples of observe_every,
-    U(1) flux n_b uniform over {0, 2, 4, 8}."""
+    U(1) flux n_b uniform over {0, 2, 4, 8}.  A fraction `su3_fraction` are
+    SU(3), and a fraction `overlap_fraction` overlap fermions (Chebyshev degree
+    64) with N from `overlap_sizes` and steps from `overlap_steps` (an overlap
+    step costs ~130 Wilson steps)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for i in range(count):
         t += rng.exponential(1.0 / rate)
-        n = int(rng.choice(sizes))
+        overlap = bool(rng.random() < overlap_fraction)
+        nc = 3 if rng.random() < su3_fraction else 2
+        n = int(rng.choice(overlap_sizes if overlap else sizes))
         m = int(rng.integers(modes[0] // 64, modes[1] // 64 + 1)) * 64
-        s = int(rng.integers(steps[0] // observe_every, steps[1] // observe_every + 1)) * observe_every
-        out.append(Request(N=(n, n, n), n_modes=m, steps=s, n_b=int(rng.choice((0, 2, 4, 8))),
-                           seed=1000 * i + 17, observe_every=observe_every, arrival=t))
+        lo, hi = overlap_steps if overlap else steps
+        s = int(rng.integers(max(1, lo // observe_every), hi // observe_every + 1)) * observe_every
+        out.append(Request(N=(n, n, n), n_modes=m, steps=s, n_b=int(rng.choice((0, 2, 4, 8))), n_colours=nc,
+                           fermion="overlap" if overlap else "wilson", seed=1000 * i + 17,
+                           observe_every=observe_every, arrival=t))
     return out

@@ -69,6 +69,7 @@ def oracle():
         L.orc_coupled_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
                                            C.c_double, C.c_int]
         L.orc3_exp.argtypes = [C.c_double, _dp, _dp]
+        L.orc_set_free_kind.argtypes = [C.c_int]
         L.orc3_wilson_apply.argtypes = [P, _dp, _dp, _dp]
         L.orc3_update_links.argtypes = [P, _dp, _dp, C.c_double]
         L.orc3_update_efield.argtypes = [P, _dp, _dp, C.c_double]

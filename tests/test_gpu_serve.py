@@ -13,8 +13,8 @@ from overlap_b200.serve import Request, Server, request_bytes
 pytestmark = pytest.mark.gpu
 
 
-def req(i, N, modes, steps, arrival, n_b=0):
-    return Request(N=N, n_modes=modes, steps=steps, n_b=n_b, seed=100 + 7 * i, observe_every=10, arrival=arrival)
+def req(i, N, modes, steps, arrival, n_b=0, **kw):
+    return Request(N=N, n_modes=modes, steps=steps, n_b=n_b, seed=100 + 7 * i, observe_every=10, arrival=arrival, **kw)
 
 
 def same(a, b, precision):
@@ -49,3 +49,24 @@ def test_request_results_are_the_same_alone_and_in_the_mix(precision):
     serial, m2 = serve(mix, precision=precision, tick_steps=7, memory_bytes=budget)
     for seed, obs in mixed.items():
         assert same(serial[seed], obs, precision)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_su3_and_overlap_requests_alongside_the_batch(precision):
+    """SU(3) and overlap requests run as contexts of their own next to the
+    batched SU(2) ensemble: each result is the same alone and in the mix."""
+    mk = [lambda t: req(3, (4, 4, 6), 64, 30, t, n_colours=3),
+          lambda t: req(4, (4, 4, 4), 64, 20, t, fermion="overlap", cheb_degree=16, n_b=2),
+          lambda t: req(5, (4, 4, 4), 64, 20, t, fermion="overlap", cheb_degree=16, n_colours=3)]
+    alone = {}
+    for f in mk:
+        out, m = serve([f(0.0)], precision=precision, tick_steps=7)
+        assert m["requests"] == 1
+        alone.update(out)
+    mix = [req(1, (6, 6, 6), 96, 40, 0.0)] + [f(0.02 * (i + 1)) for i, f in enumerate(mk)]
+    mixed, m = serve(mix, precision=precision, tick_steps=7)
+    assert m["requests"] == 4 and m["rejected"] == 0
+    for f in mk:
+        seed = f(0).seed
+        assert mixed[seed].shape == alone[seed].shape
+        assert same(mixed[seed], alone[seed], precision), seed

@@ -14,7 +14,7 @@ from overlap_b200.inputs import unit_links, volume
 
 pytestmark = pytest.mark.gpu
 
-N = (4, 5, 6)
+N = (4, 6, 6)  # even: plane waves of odd N take the reference's axis branch at k = (N-1)/2
 KW = dict(N=N, form="fused", m_fermion=0.1, m_dw=0.0, dt=0.05, t_sphaleron=1e9)
 
 

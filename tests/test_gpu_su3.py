@@ -187,14 +187,17 @@ def test_reunitarized_links_stay_special_unitary():
     assert np.abs(np.linalg.det(M3) - 1).max() < 1e-14
 
 
+NE = (4, 4, 6)  # even sizes for plane waves (odd N takes the reference's axis branch at k = (N-1)/2)
+
+
 def test_plane_waves():
-    V = volume(N)
+    V = volume(NE)
     n = 12 * V
-    p = oracle_params(N, m=0.1, dt=0.05)
+    p = oracle_params(NE, m=0.1, dt=0.05)
     psi = np.zeros((n, V, 3, 4), np.complex128)
     mid = np.zeros_like(psi)
     assert oracle().orc3_free_fermions(C.byref(p), 0, n, ptr(f64(psi)), ptr(f64(mid))) == 0
-    with ctx3("fp64", n_modes=n) as ctx:
+    with ctx3("fp64", n_modes=n, N=NE) as ctx:
         assert ctx.set_free_fermions() == 0
         g_psi, g_mid = ctx.get_modes()
     assert rel_err(g_psi, psi) < 1e-13 and rel_err(g_mid, mid) < 1e-13
@@ -204,18 +207,18 @@ def _vacuum_energy(ctx, psi):
     """(1/2V) sum_m w_m <psi_m, h psi_m>, h = i D."""
     d = ctx.apply(psi)
     w = np.where(np.arange(psi.shape[0]) % 2 == 0, 1.0, -1.0)
-    return float(np.sum(w * np.einsum("msca,msca->m", np.conj(psi), 1j * d).real) / (2 * volume(N)))
+    return float(np.sum(w * np.einsum("msca,msca->m", np.conj(psi), 1j * d).real) / (2 * ctx.V))
 
 
 def test_stochastic_modes_reproduce_the_vacuum_energy():
-    V = volume(N)
-    with ctx3("fp64", n_modes=12 * V) as ctx:
-        ctx.set_links(unit_links_su3(N))
+    V = volume(NE)
+    with ctx3("fp64", n_modes=12 * V, N=NE) as ctx:
+        ctx.set_links(unit_links_su3(NE))
         ctx.set_free_fermions()
         e_pw = _vacuum_energy(ctx, ctx.get_modes()[0])
     for pairs in (1, 5):
-        with ctx3("fp64", n_modes=2 * pairs) as ctx:
-            ctx.set_links(unit_links_su3(N))
+        with ctx3("fp64", n_modes=2 * pairs, N=NE) as ctx:
+            ctx.set_links(unit_links_su3(NE))
             ctx.set_stochastic_modes(seed=21)
             psi, mid = ctx.get_modes()
             assert abs(_vacuum_energy(ctx, psi) - e_pw) <= 1e-12 * abs(e_pw)
