@@ -375,15 +375,18 @@ def ensemble_leg(steps, warmup, device):
 
 
 def serving_leg(count, device):
-    """The serving configuration: Poisson arrivals (mean 20/s) of SU(2) Wilson
-    trajectory requests, N uniform over {8, 12, 16, 24}, 4096-8192 Z2
-    stochastic modes, 200-2000 steps, U(1) flux n_B in {0, 2, 4, 8}, FP32
-    modes, admitted by device memory into one continuously batched ensemble;
-    N_5, N_CS and energy streamed every 50 steps.  A fixed number of requests
-    (time-boxed: the offered load exceeds the GPU's capacity)."""
+    """The serving configuration: Poisson arrivals (mean 20/s) of trajectory
+    requests, N uniform over {8, 12, 16, 24}, 4096-8192 modes, 200-2000 steps,
+    U(1) flux n_B in {0, 2, 4, 8}, FP32 modes; a quarter SU(3), an eighth
+    overlap fermions (Chebyshev degree 64, plane waves, N = 8 and 100-200
+    steps: an overlap step costs ~130 Wilson steps); the Wilson requests on Z2
+    stochastic modes.  Admitted by device memory: SU(2) Wilson requests into one
+    continuously batched ensemble, the others as contexts of their own beside
+    it; N_5, N_CS and energy streamed every 50 steps.  A fixed number of
+    requests (time-boxed: the offered load exceeds the GPU's capacity)."""
     from overlap_b200.serve import Server, poisson_requests
 
-    reqs = poisson_requests(count, 20.0, seed=7)
+    reqs = poisson_requests(count, 20.0, seed=7, su3_fraction=0.25, overlap_fraction=0.125)
     offered = sum(r.mode_sites() * r.steps for r in reqs) / max(reqs[-1].arrival, 1e-9)
     srv = Server(precision="fp32", device=device, tick_steps=50)
     try:
@@ -391,8 +394,13 @@ def serving_leg(count, device):
         streamed = sum(len(r.observables) for r in srv.done)
     finally:
         srv.close()
-    m.update({"config": f"{count} requests, Poisson 20/s, N in {{8,12,16,24}}, 4096-8192 Z2 modes, 200-2000 steps, "
-                        "n_B in {0,2,4,8}, FP32, observables every 50 steps",
+    kinds = {}
+    for r in reqs:
+        k = f"SU({r.n_colours}) {r.fermion}"
+        kinds[k] = kinds.get(k, 0) + 1
+    m.update({"config": f"{count} requests, Poisson 20/s, N in {{8,12,16,24}}, 4096-8192 modes, 200-2000 steps "
+                        "(overlap: N=8, 100-200 steps, Chebyshev degree 64), n_B in {0,2,4,8}, FP32, observables "
+                        "every 50 steps", "request_kinds": kinds,
               "offered_mode_site_updates_per_s": offered, "observations_streamed": streamed})
     return m
 

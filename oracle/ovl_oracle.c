@@ -1419,9 +1419,75 @@ void orc3_bulk(const orc_params *p, const double *U, const double *E, double *ou
     out[4] = 0.5 * (e2[0] + e2[1] + e2[2]);
     out[5] = 0.5 * (b2[0] + b2[1] + b2[2]);
     out[6] = gmax;
-    out[7] = sqrt(gsum / (3.0 * V));
+    out[7] = sqrt(gsum / (8.0 * V));  /* over the Nc^2 - 1 components (GaussLawViolation.cpp:64) */
     out[8] = umax;
     out[9] = sqrt(usum / (3.0 * V));
+}
+
+/* Gauss violation G^a(x) = sum_mu E_mu(x) - R(U_mu(x-mu)^+) E_mu(x-mu) into G
+ * (8 per site); returns the signed maximum (from 0), *avg the rms over the 8 V
+ * components. */
+static double gauss_violation3(const orc_params *p, const double *U, const double *E, double *G, double *avg) {
+    const int V = volume(p);
+    double mx = 0.0, sum = 0.0;
+    for (int s = 0; s < V; s++) {
+        double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int mu = 0; mu < 3; mu++) {
+            const int sm = shift(p, s, mu, -1);
+            m3 um = m3_load(U, sm, mu), umd = m3_dag(&um);
+            double R[8][8];
+            su3_adjoint(&umd, R);
+            for (int a = 0; a < 8; a++) {
+                double t = E[a + 8 * (mu + 3 * s)];
+                for (int b = 0; b < 8; b++) t -= R[a][b] * E[b + 8 * (mu + 3 * sm)];
+                g[a] += t;
+            }
+        }
+        for (int a = 0; a < 8; a++) {
+            G[a + 8 * s] = g[a];
+            mx = fmax(mx, g[a]);
+            sum += g[a] * g[a];
+        }
+    }
+    *avg = sqrt(sum / (8.0 * V));
+    return mx;
+}
+
+/* E_mu(x) -= gamma (G(x) - R(U_mu(x)) G(x + mu)) (GaussRestore.cpp:72-118, three colours) */
+static void gauss_update3(const orc_params *p, const double *U, const double *G, double *E, double gamma) {
+    const int V = volume(p);
+    for (int s = 0; s < V; s++)
+        for (int mu = 0; mu < 3; mu++) {
+            const int sp = shift(p, s, mu, +1);
+            m3 u = m3_load(U, s, mu);
+            double R[8][8];
+            su3_adjoint(&u, R);
+            for (int a = 0; a < 8; a++) {
+                double up = 0.0;
+                for (int b = 0; b < 8; b++) up += R[a][b] * G[b + 8 * sp];
+                E[a + 8 * (mu + 3 * s)] -= gamma * (G[a + 8 * s] - up);
+            }
+        }
+}
+
+/* GaussLawRestoration::Restore (GaussRestore.cpp:132-168) for three colours. */
+int orc3_gauss_restore(const orc_params *p, const double *U, double *E, int max_iter, double tol, double *out2) {
+    const int V = volume(p);
+    double *G = malloc(sizeof(double) * 8 * (size_t)V);
+    double avg = 0.0;
+    double mx = gauss_violation3(p, U, E, G, &avg);
+    int n = 0;
+    static const double gammas[3] = {7.0 / 24.0, 7.0 / 48.0, 7.0 / 72.0};
+    while (n < max_iter && mx > tol) {
+        for (int k = 0; k < 3; k++) {
+            mx = gauss_violation3(p, U, E, G, &avg);
+            gauss_update3(p, U, G, E, gammas[k]);
+        }
+        n++;
+    }
+    free(G);
+    if (out2) { out2[0] = mx; out2[1] = avg; }
+    return n;
 }
 
 /* Chebyshev coefficients of x^(-1/2) on [eps, 1] (c_0 with weight 1/2), by

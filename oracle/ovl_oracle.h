@@ -122,6 +122,7 @@ void orc3_charges(const orc_params *p, const double *U, const double *psi, int n
 double orc3_ncsdot(const orc_params *p, const double *U, const double *E);
 double orc3_delta_ncs(const orc_params *p, const double *Uold, const double *Unew);
 void orc3_bulk(const orc_params *p, const double *U, const double *E, double *out);
+int orc3_gauss_restore(const orc_params *p, const double *U, double *E, int max_iter, double tol, double *out2);
 void orc_chebyshev_coeffs(int K, double eps, double *c);
 void orc3_overlap_apply(const orc_params *p, const double *U, const double *phi, double *out, int K, double eps,
                         double lambda_max);

@@ -1268,18 +1268,18 @@ int ovl_fermion_energy(ovl_ctx *c, double *out) {
 int ovl_gauss_restore(ovl_ctx *c, int max_iter, double tol, int *iterations, double out[2]) {
     if (!c) return OVL_E_ARG;
     if (max_iter < 0 || !(tol >= 0.0)) return fail(c, OVL_E_ARG, "ovl_gauss_restore: max_iter=%d tol=%g", max_iter, tol);
-    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_gauss_restore: built for two colours");
     int rc = set_device(c);
     if (rc) return rc;
     double *G = nullptr;
-    if (cudaMalloc(&G, sizeof(double) * 3 * (size_t)c->L.V) != cudaSuccess) {
+    if (cudaMalloc(&G, sizeof(double) * c->e_comp * (size_t)c->L.V) != cudaSuccess) {
         cudaGetLastError();
         return fail(c, OVL_E_OOM, "ovl_gauss_restore: violation buffer");
     }
     auto done = [&](int status) { cudaFree(G); return status; };
     double *dv = c->dev_small + 16;  // {sum G^2, max}
     auto violation = [&]() -> int {
-        ovl::launch_gauss_violation(c->U, c->E, c->L, G, c->partial, dv, c->stream);
+        if (su3(c)) ovl::su3_launch_gauss_violation(c->U, c->E, c->L, G, c->partial, dv, c->stream);
+        else ovl::launch_gauss_violation(c->U, c->E, c->L, G, c->partial, dv, c->stream);
         return launched(c, 2, "gauss violation");
     };
     auto read_max = [&](double &mx) -> int {
@@ -1298,7 +1298,8 @@ int ovl_gauss_restore(ovl_ctx *c, int max_iter, double tol, int *iterations, dou
     while (n < max_iter && mx > tol) {
         for (double g : gammas) {
             if ((rc = violation())) return done(rc);
-            ovl::launch_gauss_update(c->U, G, c->E, c->L, g, c->stream);
+            if (su3(c)) ovl::su3_launch_gauss_update(c->U, G, c->E, c->L, g, c->stream);
+            else ovl::launch_gauss_update(c->U, G, c->E, c->L, g, c->stream);
             if ((rc = launched(c, 1, "gauss update"))) return done(rc);
         }
         n++;
@@ -1307,7 +1308,7 @@ int ovl_gauss_restore(ovl_ctx *c, int max_iter, double tol, int *iterations, dou
     if (iterations) *iterations = n;
     if (out) {
         out[0] = c->host_small[1];
-        out[1] = std::sqrt(c->host_small[0] / (3.0 * c->L.V));
+        out[1] = std::sqrt(c->host_small[0] / ((double)c->e_comp * c->L.V));  // GaussLawViolation.cpp:64
     }
     return done(OVL_OK);
 }

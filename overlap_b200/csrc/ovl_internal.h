@@ -259,5 +259,10 @@ void su3_launch_geodesic(const double *Uold, const double *Unew, double c, doubl
                          cudaStream_t stream);
 void su3_launch_bulk(const double *U, const double *E, const Lattice &L, double *partial, double *out,
                      cudaStream_t stream);
+// out2 = {sum of G^2, signed maximum}; G holds 8 components per site.
+void su3_launch_gauss_violation(const double *U, const double *E, const Lattice &L, double *G, double *partial,
+                                double *out2, cudaStream_t stream);
+void su3_launch_gauss_update(const double *U, const double *G, double *E, const Lattice &L, double gamma,
+                             cudaStream_t stream);
 
 }  // namespace ovl

@@ -614,7 +614,7 @@ __global__ void su3_bulk_finish_kernel(const double *__restrict__ partial, int n
     out[4] = 0.5 * (e2[0] + e2[1] + e2[2]);
     out[5] = 0.5 * (b2[0] + b2[1] + b2[2]);
     out[6] = fmax(gmax, 0.0);
-    out[7] = sqrt(s[6] / (3.0 * V));
+    out[7] = sqrt(s[6] / (8.0 * V));  // over the Nc^2 - 1 components (GaussLawViolation.cpp:64)
     out[8] = umax;
     out[9] = sqrt(s[7] / (3.0 * V));
 }
@@ -661,6 +661,86 @@ __global__ void su3_efield_kernel(const double *__restrict__ U, double *E, Latti
 void su3_launch_update_efield(const double *U, double *E, const Lattice &L, double dt_step, cudaStream_t s) {
     const int n = 3 * L.V;
     su3_efield_kernel<<<(n + 127) / 128, 128, 0, s>>>(U, E, L, -2.0 * dt_step);
+}
+
+// ------------------------------------------------------ Gauss restoration --
+// GaussLawRestoration (GAUSSLAWFIXING/GaussRestore.cpp:13-168) for three
+// colours: G^a(x) = sum_mu E_mu(x) - R(U_mu(x-mu)^+) E_mu(x-mu) into G (8 per
+// site), CTA partial sums of G^2 and signed maxima (from 0).
+__global__ void __launch_bounds__(kReduce3Threads)
+    su3_gauss_violation_kernel(const double *__restrict__ U, const double *__restrict__ E, Lattice L, double *G,
+                               double *partial) {
+    __shared__ double sh[32];
+    double sum = 0.0, mx = 0.0;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < L.V) {
+        int x, y, z;
+        site_coords(L, s, x, y, z);
+        double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int mu = 0; mu < 3; mu++) {
+            int c[3] = {x, y, z};
+            c[mu] -= 1;
+            const int sm = site_index(L, c[0], c[1], c[2]);
+            double t[8];
+            su3_transport(m3_dag(load_su3(U, sm, mu)), E + 8 * (mu + 3 * sm), t);
+            for (int a = 0; a < 8; a++) g[a] += E[a + 8 * (mu + 3 * s)] - t[a];
+        }
+        for (int a = 0; a < 8; a++) {
+            G[a + 8 * (size_t)s] = g[a];
+            sum += g[a] * g[a];
+            mx = fmax(mx, g[a]);
+        }
+    }
+    const double tsum = block_sum(sum, sh);
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmax(m, sh[w]);
+        partial[2 * blockIdx.x] = tsum;
+        partial[2 * blockIdx.x + 1] = m;
+    }
+}
+
+__global__ void su3_gauss_finish_kernel(const double *__restrict__ partial, int n, double *out2) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double sum = 0.0, mx = 0.0;
+    for (int i = 0; i < n; i++) {
+        sum += partial[2 * i];
+        mx = fmax(mx, partial[2 * i + 1]);
+    }
+    out2[0] = sum;
+    out2[1] = mx;
+}
+
+// E_mu(x) -= gamma (G(x) - R(U_mu(x)) G(x + mu))   (GaussRestore.cpp:72-118)
+__global__ void su3_gauss_update_kernel(const double *__restrict__ U, const double *__restrict__ G,
+                                        double *__restrict__ E, Lattice L, double gamma) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * L.V) return;
+    const int s = t / 3, mu = t % 3;
+    int x, y, z;
+    site_coords(L, s, x, y, z);
+    int c[3] = {x, y, z};
+    c[mu] += 1;
+    const int sp = site_index(L, c[0], c[1], c[2]);
+    double up[8];
+    su3_transport(load_su3(U, s, mu), G + 8 * (size_t)sp, up);
+    for (int a = 0; a < 8; a++) E[a + 8 * (size_t)t] -= gamma * (G[a + 8 * (size_t)s] - up[a]);
+}
+
+void su3_launch_gauss_violation(const double *U, const double *E, const Lattice &L, double *G, double *partial,
+                                double *out2, cudaStream_t s) {
+    const int nb = (L.V + kReduce3Threads - 1) / kReduce3Threads;
+    su3_gauss_violation_kernel<<<nb, kReduce3Threads, 0, s>>>(U, E, L, G, partial);
+    su3_gauss_finish_kernel<<<1, 32, 0, s>>>(partial, nb, out2);
+}
+
+void su3_launch_gauss_update(const double *U, const double *G, double *E, const Lattice &L, double gamma,
+                             cudaStream_t s) {
+    const int n = 3 * L.V;
+    su3_gauss_update_kernel<<<(n + 127) / 128, 128, 0, s>>>(U, G, E, L, gamma);
 }
 
 // ------------------------------------------------------------ FP32 links --

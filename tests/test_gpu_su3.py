@@ -275,6 +275,26 @@ def test_three_colour_limits_are_reported():
         with pytest.raises(OvlError):
             ctx3(**kw)
     with ctx3("fp64") as ctx:
-        for call in (ctx.currents, ctx.fermion_energy, lambda: ctx.gauss_restore(10, 1e-12)):
+        for call in (ctx.currents, ctx.fermion_energy):
             with pytest.raises(OvlError):
                 call()
+
+
+def test_gauss_restore():
+    """GaussLawRestoration::Restore for three colours against the oracle, on
+    quasi-particle fields (SetQuasiParticles restores Gauss's law after the
+    transform)."""
+    from overlap_b200.inputs import quasi_particles
+
+    U, E = quasi_particles(N, 4.0, 1.0, seed=22, n_colours=3)
+    p = oracle_params(N)
+    Eo = E.copy()
+    out = np.zeros(2)
+    n = oracle().orc3_gauss_restore(C.byref(p), ptr(f64(U)), ptr(Eo), 10000, 1e-14, ptr(out))
+    with ctx3("fp64") as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        r = ctx.gauss_restore(10000, 1e-14)
+        assert r["iterations"] == n and r["max"] <= 1e-14
+        assert rel_err(ctx.get_efield(), Eo) < 1e-12
+        assert ctx.bulk()["gauss_max"] <= 1e-14

@@ -112,7 +112,13 @@ def test_embedded_su2_ncsdot_bulk_and_delta_ncs():
     o3 = np.zeros(10)
     oracle().orc_bulk(C.byref(p), ptr(U2), ptr(E2), ptr(o2))
     oracle().orc3_bulk(C.byref(p), ptr(U3), ptr(E3), ptr(o3))
+    o3[7] *= np.sqrt(8.0 / 3.0)  # the Gauss rms runs over the Nc^2 - 1 components (GaussLawViolation.cpp:64)
     assert np.abs(o2[:8] - o3[:8]).max() < 1e-13 * np.abs(o2[:8]).max()
+    # Gauss restoration: the embedded run is the two-colour one
+    E2r, E3r = E2.copy(), E3.copy()
+    n2 = oracle().orc_gauss_restore(C.byref(p), ptr(U2), ptr(E2r), 10000, 1e-14, ptr(np.zeros(2)))
+    n3 = oracle().orc3_gauss_restore(C.byref(p), ptr(U3), ptr(E3r), 10000, 1e-14, ptr(np.zeros(2)))
+    assert n2 == n3 and np.abs(E3r[..., :3] - E2r).max() < 1e-13 and np.abs(E3r[..., 3:]).max() < 1e-14
     if have_reference("wilson"):
         U2b = U2.copy()
         for _ in range(5):
