@@ -1490,6 +1490,83 @@ int orc3_gauss_restore(const orc_params *p, const double *U, double *E, int max_
     return n;
 }
 
+/* dH_F/dtheta^a_mu(x) for three colours (orc_color_force with 3x3 links and
+ * t^a = lambda^a / 2): -(1/2V) sum_m w_m Re[psi(x)^+ g0 (1 - G_mu) i t^a U_mu(x) psi(x+mu)],
+ * out[a + 8 (mu + 3 site)]. */
+void orc3_color_force(const orc_params *p, const double *U, const double *psi, int nmodes, int first, double *out) {
+    const int V = volume(p);
+    cplx G[3][4][4], gp[3][4][4];
+    mat4_scale(-I, GX, G[0]);
+    mat4_scale(-I, GY, G[1]);
+    mat4_scale(-I, GZ, G[2]);
+    for (int mu = 0; mu < 3; mu++) {
+        cplx t[4][4];
+        for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) t[a][b] = (a == b) - G[mu][a][b];
+        mat4_mul(G0, t, gp[mu]);
+    }
+    m3 T[8];
+    for (int a = 0; a < 8; a++) T[a] = su3_generator(a);
+    memset(out, 0, sizeof(double) * 24 * (size_t)V);
+    const double pre = 1.0 / (2.0 * V);
+    for (int m = 0; m < nmodes; m++) {
+        const double w = ((first + m) % 2 == 0) ? 1.0 : -1.0;
+        const cplx *mode = (const cplx *)psi + (size_t)SPINOR3 * V * m;
+        for (int s = 0; s < V; s++) {
+            const cplx *f = mode + SPINOR3 * s;
+            for (int mu = 0; mu < 3; mu++) {
+                m3 M = m3_load(U, s, mu);
+                dress3(p, s, mu, &M);
+                const cplx *h = mode + SPINOR3 * shift(p, s, mu, +1);
+                for (int a = 0; a < 8; a++) {
+                    m3 A = m3_mul(&T[a], &M);  /* i t^a M */
+                    cplx b = 0;
+                    for (int i = 0; i < 3; i++)
+                        for (int j = 0; j < 3; j++)
+                            for (int al = 0; al < 4; al++)
+                                for (int be = 0; be < 4; be++)
+                                    if (gp[mu][al][be] != 0)
+                                        b += conj(f[4 * i + al]) * gp[mu][al][be] * I * A.m[i][j] * h[4 * j + be];
+                    out[a + 8 * (mu + 3 * s)] += -pre * w * creal(b);
+                }
+            }
+        }
+    }
+}
+
+double orc3_fermion_energy(const orc_params *p, const double *U, const double *psi, int nmodes, int first) {
+    const int V = volume(p);
+    const size_t per_mode = (size_t)2 * SPINOR3 * V;
+    double *work = malloc(sizeof(double) * per_mode);
+    double e = 0.0;
+    for (int m = 0; m < nmodes; m++) {
+        const double w = ((first + m) % 2 == 0) ? 1.0 : -1.0;
+        orc3_wilson_apply(p, U, psi + per_mode * m, work);
+        const cplx *f = (const cplx *)(psi + per_mode * m), *d = (const cplx *)work;
+        cplx t = 0;
+        for (int k = 0; k < SPINOR3 * V; k++) t += conj(f[k]) * I * d[k];
+        e += w * creal(t);
+    }
+    free(work);
+    return e / (2.0 * V);
+}
+
+/* The coupled leapfrog (orc_coupled_leapfrog) for three colours. */
+void orc3_coupled_leapfrog(const orc_params *p, double *U, double *E, double *psi, double *psimid, int nmodes,
+                           int first, int *tsteps, int nsteps, double g2, int gauge) {
+    const int V = volume(p);
+    double *force = malloc(sizeof(double) * 24 * (size_t)V);
+    for (int n = 0; n < nsteps; n++) {
+        orc3_wilson_leapfrog(p, U, E, psi, psimid, nmodes, tsteps, 1);
+        if (gauge) orc3_update_efield(p, U, E, p->dt);
+        if (g2 != 0.0) {
+            orc3_color_force(p, U, psi, nmodes, first, force);
+            for (size_t k = 0; k < 24 * (size_t)V; k++) E[k] += p->dt * g2 * force[k];
+        }
+    }
+    free(force);
+}
+
 /* Chebyshev coefficients of x^(-1/2) on [eps, 1] (c_0 with weight 1/2), by
  * Chebyshev-Gauss quadrature on max(4K, 256) nodes. */
 void orc_chebyshev_coeffs(int K, double eps, double *c) {

@@ -123,6 +123,10 @@ double orc3_ncsdot(const orc_params *p, const double *U, const double *E);
 double orc3_delta_ncs(const orc_params *p, const double *Uold, const double *Unew);
 void orc3_bulk(const orc_params *p, const double *U, const double *E, double *out);
 int orc3_gauss_restore(const orc_params *p, const double *U, double *E, int max_iter, double tol, double *out2);
+void orc3_color_force(const orc_params *p, const double *U, const double *psi, int nmodes, int first, double *out);
+double orc3_fermion_energy(const orc_params *p, const double *U, const double *psi, int nmodes, int first);
+void orc3_coupled_leapfrog(const orc_params *p, double *U, double *E, double *psi, double *psimid, int nmodes,
+                           int first, int *tsteps, int nsteps, double g2, int gauge);
 void orc_chebyshev_coeffs(int K, double eps, double *c);
 void orc3_overlap_apply(const orc_params *p, const double *U, const double *phi, double *out, int K, double eps,
                         double lambda_max);

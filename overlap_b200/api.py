@@ -344,8 +344,8 @@ class Context:
                 "iters": (int(it[0]), int(it[1]))}
 
     def color_force(self) -> np.ndarray:
-        """dH_F/dtheta^a_mu(x) as [V, 3 (mu), 3 (a)] (Wilson fermions)."""
-        o = np.empty((volume(self.params.N), 3, 3))
+        """dH_F/dtheta^a_mu(x) as [V, 3 (mu), Nc^2 - 1 (a)] (Wilson fermions)."""
+        o = np.empty((volume(self.params.N), 3, self.nc * self.nc - 1))
         self._check(self._L.ovl_color_force(self._ctx, _dp(o)))
         return o
 

@@ -584,8 +584,6 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
             return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: three-colour overlap fermions use the Chebyshev sign function");
         if (p->precision == OVL_PREC_FP40)
             return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: FP40 storage is built for two colours");
-        if (p->backreaction != 0.0)
-            return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: fermion back-reaction is built for two colours");
         if (p->ritz_auto)
             return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: three colours take spectral bounds from "
                                                     "ovl_set_spectral_bounds or the analytic bound, not ritz_auto");
@@ -671,7 +669,8 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
                                    ovl::bulk_partial_doubles(c->L), ovl::charges_partial_doubles(c->L, c->n_mb),
                                    ovl::force_partial_doubles(c->L, c->n_mb), ovl::energy_partial_doubles(),
                                    ovl::gauss_partial_doubles(c->L), ovl::su3_charges_partial_doubles(c->L, c->n_mb),
-                                   ovl::su3_reduce_partial_doubles(c->L)});
+                                   ovl::su3_reduce_partial_doubles(c->L),
+                                   ovl::su3_force_partial_doubles(c->L, c->n_mb)});
     if ((rc = alloc((void **)&c->partial, sizeof(double) * c->partial_doubles, "reduction scratch")) ||
         (rc = alloc((void **)&c->per_site, sizeof(double) * ovl::kCurrentsPerSite * V, "currents")) ||
         (rc = alloc((void **)&c->dev_small, sizeof(double) * 64, "results")) ||
@@ -937,6 +936,26 @@ int ovl_set_free_fermions(ovl_ctx *c, int *n_bad) {
     return OVL_OK;
 }
 
+// The fermion force dH_F/dtheta into out (8 or 3 per link), or E += coef * it.
+void launch_force(ovl_ctx *c, double *out, double *E, double coef) {
+    const double *u1 = c->u1_on ? c->u1 : nullptr;
+    if (su3(c) && fp32(c))
+        ovl::su3_launch_color_force<float>(c->U, u1, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->partial,
+                                           out, E, coef, c->stream);
+    else if (su3(c))
+        ovl::su3_launch_color_force<double>(c->U, u1, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->partial,
+                                            out, E, coef, c->stream);
+    else if (fp40(c))
+        ovl::launch_color_force40(c->U, u1, c->psi, c->psi_lo, c->L, c->n_mb, c->p.n_modes, c->p.first_mode,
+                                  c->partial, out, E, coef, c->stream);
+    else if (fp32(c))
+        ovl::launch_color_force<float>(c->U, u1, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->partial, out,
+                                       E, coef, c->stream);
+    else
+        ovl::launch_color_force<double>(c->U, u1, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->partial,
+                                        out, E, coef, c->stream);
+}
+
 // E += dt (staple force) + dt g^2 dH_F/dtheta after a step of the coupled
 // evolution (ovl_params.gauge_force, ovl_params.backreaction).
 int coupled_efield(ovl_ctx *c) {
@@ -952,16 +971,7 @@ int coupled_efield(ovl_ctx *c) {
     if (c->p.backreaction != 0.0) {
         {
             ProfScope ps(c, OVL_PROF_OBS);
-            const double coef = c->p.dt * c->p.backreaction;
-            if (fp40(c))
-                ovl::launch_color_force40(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->psi_lo, c->L, c->n_mb,
-                                          c->p.n_modes, c->p.first_mode, c->partial, nullptr, c->E, coef, c->stream);
-            else if (fp32(c))
-                ovl::launch_color_force<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
-                                               c->p.first_mode, c->partial, nullptr, c->E, coef, c->stream);
-            else
-                ovl::launch_color_force<double>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
-                                                c->p.first_mode, c->partial, nullptr, c->E, coef, c->stream);
+            launch_force(c, nullptr, c->E, c->p.dt * c->p.backreaction);
         }
         int rc = launched(c, 2, "fermion force");
         if (rc) return rc;
@@ -1207,24 +1217,15 @@ int ovl_update_efield(ovl_ctx *c, double dt_step) {
 int ovl_color_force(ovl_ctx *c, double *out) {
     if (!c || !out) return OVL_E_ARG;
     if (c->p.fermion != OVL_FERMION_WILSON) return fail(c, OVL_E_UNSUPPORTED, "ovl_color_force: Wilson fermions only");
-    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_color_force: built for two colours");
     int rc = set_device(c);
     if (rc) return rc;
     double *dev = nullptr;
-    const size_t n = (size_t)9 * c->L.V;
+    const size_t n = (size_t)c->e_comp * 3 * c->L.V;
     if (cudaMalloc(&dev, sizeof(double) * n) != cudaSuccess) {
         cudaGetLastError();
         return fail(c, OVL_E_OOM, "ovl_color_force: output buffer");
     }
-    if (fp40(c))
-        ovl::launch_color_force40(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->psi_lo, c->L, c->n_mb, c->p.n_modes,
-                                  c->p.first_mode, c->partial, dev, nullptr, 0.0, c->stream);
-    else if (fp32(c))
-        ovl::launch_color_force<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
-                                       c->p.first_mode, c->partial, dev, nullptr, 0.0, c->stream);
-    else
-        ovl::launch_color_force<double>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
-                                        c->p.first_mode, c->partial, dev, nullptr, 0.0, c->stream);
+    launch_force(c, dev, nullptr, 0.0);
     rc = launched(c, 2, "fermion force");
     cudaError_t e = rc ? cudaSuccess : cudaMemcpyAsync(out, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess && !rc) e = cudaStreamSynchronize(c->stream);
@@ -1237,11 +1238,22 @@ int ovl_color_force(ovl_ctx *c, double *out) {
 int ovl_fermion_energy(ovl_ctx *c, double *out) {
     if (!c || !out) return OVL_E_ARG;
     if (c->p.fermion != OVL_FERMION_WILSON) return fail(c, OVL_E_UNSUPPORTED, "ovl_fermion_energy: Wilson fermions only");
-    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_fermion_energy: built for two colours");
     int rc = set_device(c);
     if (rc) return rc;
     const double *u1 = c->u1_on ? c->u1 : nullptr;
-    if (fp40(c)) {
+    if (su3(c)) {
+        if (fp32(c)) {
+            ovl::su3_launch_hop<float>(su3_links(c), c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), 0.0, false,
+                                       c->stream);
+            ovl::su3_launch_fermion_energy<float>(c->psi, c->aux_dst, c->L, c->n_mb, c->p.n_modes, c->p.first_mode,
+                                                  c->partial, c->dev_small, c->stream);
+        } else {
+            ovl::su3_launch_hop<double>(su3_links(c), c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), 0.0, false,
+                                        c->stream);
+            ovl::su3_launch_fermion_energy<double>(c->psi, c->aux_dst, c->L, c->n_mb, c->p.n_modes, c->p.first_mode,
+                                                   c->partial, c->dev_small, c->stream);
+        }
+    } else if (fp40(c)) {
         ovl::HopConfig h;
         h.U = c->U;
         h.u1 = u1;

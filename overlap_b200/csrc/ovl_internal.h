@@ -264,5 +264,14 @@ void su3_launch_gauss_violation(const double *U, const double *E, const Lattice 
                                 double *out2, cudaStream_t stream);
 void su3_launch_gauss_update(const double *U, const double *G, double *E, const Lattice &L, double gamma,
                              cudaStream_t stream);
+// dH_F/dtheta^a per link into out[8 per link], or E += coef * it when out is null.
+size_t su3_force_partial_doubles(const Lattice &L, int n_mb);
+template <typename T>
+void su3_launch_color_force(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                            int first_mode, double *partial, double *out, double *E, double coef, cudaStream_t stream);
+// H_F = sum_m w_m Re <psi_m, i (D psi)_m> / 2V from psi and D psi.
+template <typename T>
+void su3_launch_fermion_energy(const void *psi, const void *dpsi, const Lattice &L, int n_mb, int n_modes,
+                               int first_mode, double *partial, double *out, cudaStream_t stream);
 
 }  // namespace ovl

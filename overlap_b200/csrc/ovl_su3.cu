@@ -372,56 +372,56 @@ __device__ inline double block_sum(double v, double *sh) {
     return t;
 }
 
-// Improved E.B per site (ChernSimonsOperators.cpp:128-439; improved_e /
-// improved_b of ovl_gauge.cu), one thread per site, CTA partial sums.
+// Improved E.B (ChernSimonsOperators.cpp:128-439; improved_e / improved_b of
+// ovl_gauge.cu), one thread per (site, direction): E_mu . B_mu, B_mu from the
+// plane orthogonal to mu; CTA partial sums.
 __global__ void __launch_bounds__(kReduce3Threads)
     su3_ncsdot_kernel(const double *__restrict__ U, const double *__restrict__ E, Lattice L, double *partial) {
     __shared__ double sh[32];
     double v = 0.0;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < L.V) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 3 * L.V) {
+        const int s = t / 3, mu = t % 3;
         int x, y, z;
         site_coords(L, s, x, y, z);
         const int plane[3][2] = {{1, 2}, {2, 0}, {0, 1}};
-        for (int mu = 0; mu < 3; mu++) {
-            // improved E_mu: -1/12, 7/12, 7/12, -1/12 of E_mu at x+mu, x, x-mu, x-2mu transported to x
-            int c[3] = {x, y, z};
-            c[mu] += 1;
-            const int sp = site_index(L, c[0], c[1], c[2]);
-            c[mu] -= 2;
-            const int sm = site_index(L, c[0], c[1], c[2]);
-            c[mu] -= 1;
-            const int smm = site_index(L, c[0], c[1], c[2]);
-            const cmat3<double> umd = m3_dag(load_su3(U, sm, mu));
-            double e[8], t[8];
-            for (int a = 0; a < 8; a++) e[a] = (7.0 / 12.0) * E[a + 8 * (mu + 3 * s)];
-            su3_transport(load_su3(U, s, mu), E + 8 * (mu + 3 * sp), t);
-            for (int a = 0; a < 8; a++) e[a] -= (1.0 / 12.0) * t[a];
-            su3_transport(umd, E + 8 * (mu + 3 * sm), t);
-            for (int a = 0; a < 8; a++) e[a] += (7.0 / 12.0) * t[a];
-            su3_transport(m3_mul(umd, m3_dag(load_su3(U, smm, mu))), E + 8 * (mu + 3 * smm), t);
-            for (int a = 0; a < 8; a++) e[a] -= (1.0 / 12.0) * t[a];
-            // improved B: 5/12 of the four plaquettes, -1/24 of the eight 2x1 rectangles
-            const int pm = plane[mu][0], pn = plane[mu][1];
-            cmat3<double> avg;
+        // improved E_mu: -1/12, 7/12, 7/12, -1/12 of E_mu at x+mu, x, x-mu, x-2mu transported to x
+        int c[3] = {x, y, z};
+        c[mu] += 1;
+        const int sp = site_index(L, c[0], c[1], c[2]);
+        c[mu] -= 2;
+        const int sm = site_index(L, c[0], c[1], c[2]);
+        c[mu] -= 1;
+        const int smm = site_index(L, c[0], c[1], c[2]);
+        const cmat3<double> umd = m3_dag(load_su3(U, sm, mu));
+        double e[8], w[8];
+        for (int a = 0; a < 8; a++) e[a] = (7.0 / 12.0) * E[a + 8 * (mu + 3 * s)];
+        su3_transport(load_su3(U, s, mu), E + 8 * (mu + 3 * sp), w);
+        for (int a = 0; a < 8; a++) e[a] -= (1.0 / 12.0) * w[a];
+        su3_transport(umd, E + 8 * (mu + 3 * sm), w);
+        for (int a = 0; a < 8; a++) e[a] += (7.0 / 12.0) * w[a];
+        su3_transport(m3_mul(umd, m3_dag(load_su3(U, smm, mu))), E + 8 * (mu + 3 * smm), w);
+        for (int a = 0; a < 8; a++) e[a] -= (1.0 / 12.0) * w[a];
+        // improved B: 5/12 of the four plaquettes, -1/24 of the eight 2x1 rectangles
+        const int pm = plane[mu][0], pn = plane[mu][1];
+        cmat3<double> avg;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) avg.m[i][j] = mk<double>(0.0, 0.0);
+        const int sg[4][2] = {{+1, +1}, {-1, +1}, {-1, -1}, {+1, -1}};
+        for (int q = 0; q < 4; q++) {
+            const cmat3<double> box = su3_loop(U, L, x, y, z, pm, pn, sg[q][0], sg[q][1], 1, 1);
+            const cmat3<double> r1 = su3_loop(U, L, x, y, z, pm, pn, sg[q][0], sg[q][1], 2, 1);
+            const cmat3<double> r2 = su3_loop(U, L, x, y, z, pm, pn, sg[q][0], sg[q][1], 1, 2);
             for (int i = 0; i < 3; i++)
-                for (int j = 0; j < 3; j++) avg.m[i][j] = mk<double>(0.0, 0.0);
-            const int sg[4][2] = {{+1, +1}, {-1, +1}, {-1, -1}, {+1, -1}};
-            for (int q = 0; q < 4; q++) {
-                const cmat3<double> box = su3_loop(U, L, x, y, z, pm, pn, sg[q][0], sg[q][1], 1, 1);
-                const cmat3<double> r1 = su3_loop(U, L, x, y, z, pm, pn, sg[q][0], sg[q][1], 2, 1);
-                const cmat3<double> r2 = su3_loop(U, L, x, y, z, pm, pn, sg[q][0], sg[q][1], 1, 2);
-                for (int i = 0; i < 3; i++)
-                    for (int j = 0; j < 3; j++)
-                        avg.m[i][j] = avg.m[i][j] + (5.0 / 12.0) * box.m[i][j] - (1.0 / 24.0) * (r1.m[i][j] + r2.m[i][j]);
-            }
-            double b[8];
-            su3_retr_ita(avg, b);
-            for (int a = 0; a < 8; a++) v += e[a] * 2.0 * b[a];
+                for (int j = 0; j < 3; j++)
+                    avg.m[i][j] = avg.m[i][j] + (5.0 / 12.0) * box.m[i][j] - (1.0 / 24.0) * (r1.m[i][j] + r2.m[i][j]);
         }
+        double b[8];
+        su3_retr_ita(avg, b);
+        for (int a = 0; a < 8; a++) v += e[a] * 2.0 * b[a];
     }
-    const double t = block_sum(v, sh);
-    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+    const double tot = block_sum(v, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = tot;
 }
 
 size_t su3_reduce_partial_doubles(const Lattice &L) {
@@ -429,7 +429,7 @@ size_t su3_reduce_partial_doubles(const Lattice &L) {
 }
 
 void su3_launch_ncsdot(const double *U, const double *E, const Lattice &L, double *partial, double *out, cudaStream_t s) {
-    const int nb = (L.V + kReduce3Threads - 1) / kReduce3Threads;
+    const int nb = (3 * L.V + kReduce3Threads - 1) / kReduce3Threads;
     su3_ncsdot_kernel<<<nb, kReduce3Threads, 0, s>>>(U, E, L, partial);
     su3_sum_rows_kernel<1><<<1, 256, 0, s>>>(partial, nb, 0.125 / (M_PI * M_PI), out);
 }
@@ -743,6 +743,172 @@ void su3_launch_gauss_update(const double *U, const double *G, double *E, const 
     su3_gauss_update_kernel<<<(n + 127) / 128, 128, 0, s>>>(U, G, E, L, gamma);
 }
 
+// ------------------------------------------------------------ back-reaction --
+// The fermion force on E for three colours (ovl_force.cu with 3x3 links and
+// t^a = lambda^a / 2): per site and mu the link-independent colour bilinears
+//   C_ij = sum_m w_m sum_ab conj(psi_ia(x)) [g0 (1 - G_mu)]_ab psi_jb(x+mu),
+// then dH_F/dtheta^a = (1/2V) Im tr(t^a Q), Q = M C^T, M the dressed link.
+constexpr int kForce3PerSite = 3 * 18;  // mu, (i, j), (re, im)
+
+template <typename T>
+__global__ void __launch_bounds__(kModeBlock *kSites3)
+    su3_force_modes_kernel(const cpx<T> *__restrict__ psi, Lattice L, int n_mb, int n_modes, int first_mode,
+                           double *__restrict__ partial) {
+    constexpr mono G0 = kGamma0;
+    constexpr mono G0M[3] = {mono_mul(kGamma0, kGammaX), mono_mul(kGamma0, kGammaY), mono_mul(kGamma0, kGammaZ)};
+    const int lane = threadIdx.x;
+    const int site = blockIdx.x * kSites3 + threadIdx.y;
+    const int g = blockIdx.y, groups = gridDim.y;
+    if (site >= L.V) return;  // whole warps exit together
+    int x, y, z;
+    site_coords(L, site, x, y, z);
+    int nb[3];
+    for (int mu = 0; mu < 3; mu++) {
+        int c[3] = {x, y, z};
+        c[mu] += 1;
+        nb[mu] = site_index(L, c[0], c[1], c[2]);
+    }
+    double acc[kForce3PerSite];
+#pragma unroll
+    for (int k = 0; k < kForce3PerSite; k++) acc[k] = 0.0;
+    for (int mb = g; mb < n_mb; mb += groups) {
+        const int mode = mb * kModeBlock + lane;
+        const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
+        cpx<double> f[3][kSpin];
+        const cpx<T> *pf = psi + field_index3(L.V, mb, site, 0, lane);
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int a = 0; a < kSpin; a++) {
+                const cpx<T> v = ld(pf + (c * kSpin + a) * kModeBlock);
+                f[c][a] = mk<double>((double)v.re, (double)v.im);
+            }
+#pragma unroll
+        for (int mu = 0; mu < 3; mu++) {
+            cpx<double> h[3][kSpin];
+            const cpx<T> *ph = psi + field_index3(L.V, mb, nb[mu], 0, lane);
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int a = 0; a < kSpin; a++) {
+                    const cpx<T> v = ld(ph + (c * kSpin + a) * kModeBlock);
+                    h[c][a] = mk<double>((double)v.re, (double)v.im);
+                }
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    const cpx<double> b0 = bilinear<double>(G0, f[i], h[j]);
+                    const cpx<double> b1 = bilinear<double>(G0M[mu], f[i], h[j]);
+                    const int k = 18 * mu + 2 * (3 * i + j);  // g0 (1 - G_mu) = g0 + i g0 g_mu
+                    acc[k] += w * (b0.re - b1.im);
+                    acc[k + 1] += w * (b0.im + b1.re);
+                }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kForce3PerSite; k++) {
+        double t = acc[k];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        acc[k] = t;
+    }
+    if (lane == 0) {
+        double *q = partial + ((size_t)g * L.V + site) * kForce3PerSite;
+#pragma unroll
+        for (int k = 0; k < kForce3PerSite; k++) q[k] = acc[k];
+    }
+}
+
+// One thread per (site, mu).  out != null: out[a + 8 (mu + 3 site)] =
+// dH_F/dtheta^a; otherwise E[a + 8 (mu + 3 site)] += coef dH_F/dtheta^a.
+template <bool U1>
+__global__ void su3_force_finish_kernel(const double *__restrict__ partial, int groups, const double *__restrict__ U,
+                                        const double *__restrict__ u1, Lattice L, double *__restrict__ out,
+                                        double *__restrict__ E, double coef) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * L.V) return;
+    const int site = t / 3, mu = t % 3;
+    cmat3<double> C;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) C.m[i][j] = mk<double>(0.0, 0.0);
+    for (int g = 0; g < groups; g++) {
+        const double *p = partial + ((size_t)g * L.V + site) * kForce3PerSite + 18 * mu;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) C.m[i][j] = C.m[i][j] + mk<double>(p[2 * (3 * i + j)], p[2 * (3 * i + j) + 1]);
+    }
+    const Links3<false, U1> lk{U, u1, L.N0 * L.N1};
+    const cmat3<double> M = lk.template get<double>(site, mu);
+    cmat3<double> Q;  // M C^T
+    for (int k = 0; k < 3; k++)
+        for (int i = 0; i < 3; i++) Q.m[k][i] = M.m[k][0] * C.m[i][0] + M.m[k][1] * C.m[i][1] + M.m[k][2] * C.m[i][2];
+    // Im tr(t^a Q) per generator (t^a = lambda^a / 2)
+    const double r3 = 0.57735026918962576451;
+    double f[8];
+    f[0] = 0.5 * (Q.m[1][0].im + Q.m[0][1].im);
+    f[1] = 0.5 * (Q.m[0][1].re - Q.m[1][0].re);  // Im((-i Q10 + i Q01)/2)
+    f[2] = 0.5 * (Q.m[0][0].im - Q.m[1][1].im);
+    f[3] = 0.5 * (Q.m[2][0].im + Q.m[0][2].im);
+    f[4] = 0.5 * (Q.m[0][2].re - Q.m[2][0].re);
+    f[5] = 0.5 * (Q.m[2][1].im + Q.m[1][2].im);
+    f[6] = 0.5 * (Q.m[1][2].re - Q.m[2][1].re);
+    f[7] = 0.5 * r3 * (Q.m[0][0].im + Q.m[1][1].im - 2.0 * Q.m[2][2].im);
+    const double sc = 1.0 / (2.0 * L.V);
+    const size_t o = 8 * (size_t)t;
+    for (int a = 0; a < 8; a++) {
+        if (out) out[o + a] = sc * f[a];
+        else E[o + a] += coef * sc * f[a];
+    }
+}
+
+int su3_force_groups(int n_mb) { return n_mb < 16 ? n_mb : 16; }
+
+size_t su3_force_partial_doubles(const Lattice &L, int n_mb) {
+    return (size_t)su3_force_groups(n_mb) * L.V * kForce3PerSite;
+}
+
+template <typename T>
+void su3_launch_color_force(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                            int first_mode, double *partial, double *out, double *E, double coef, cudaStream_t s) {
+    const int groups = su3_force_groups(n_mb);
+    const dim3 block(kModeBlock, kSites3), grid((L.V + kSites3 - 1) / kSites3, groups);
+    su3_force_modes_kernel<T><<<grid, block, 0, s>>>(reinterpret_cast<const cpx<T> *>(psi), L, n_mb, n_modes,
+                                                      first_mode, partial);
+    const int n = 3 * L.V;
+    if (u1) su3_force_finish_kernel<true><<<(n + 127) / 128, 128, 0, s>>>(partial, groups, U, u1, L, out, E, coef);
+    else su3_force_finish_kernel<false><<<(n + 127) / 128, 128, 0, s>>>(partial, groups, U, u1, L, out, E, coef);
+}
+
+// sum_m w_m Re <psi_m, i (D psi)_m> / 2V from psi and D psi (ovl_force.cu's
+// energy reduction for 12-component modes): CTA partial sums, one CTA adds them.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    su3_energy_partial_kernel(const cpx<T> *__restrict__ psi, const cpx<T> *__restrict__ dpsi, size_t n, int V,
+                              int n_modes, int first_mode, double *__restrict__ partial) {
+    __shared__ double sh[32];
+    const size_t per_mb = (size_t)V * kComp3 * kModeBlock;
+    double acc = 0.0;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int mode = (int)(e / per_mb) * kModeBlock + (int)(e % kModeBlock);
+        if (mode >= n_modes) continue;
+        const cpx<T> a = ld(psi + e), d = ld(dpsi + e);
+        const double im = (double)a.re * (double)d.im - (double)a.im * (double)d.re;  // Im conj(a) d
+        acc += (((first_mode + mode) & 1) == 0) ? -im : im;
+    }
+    const double t = block_sum(acc, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+}
+
+template <typename T>
+void su3_launch_fermion_energy(const void *psi, const void *dpsi, const Lattice &L, int n_mb, int n_modes,
+                               int first_mode, double *partial, double *out, cudaStream_t s) {
+    const size_t n = (size_t)n_mb * L.V * kComp3 * kModeBlock;
+    const int blocks = (int)std::min<size_t>((n + 255) / 256, 1024);
+    su3_energy_partial_kernel<T><<<blocks, 256, 0, s>>>(reinterpret_cast<const cpx<T> *>(psi),
+                                                         reinterpret_cast<const cpx<T> *>(dpsi), n, L.V, n_modes,
+                                                         first_mode, partial);
+    su3_sum_rows_kernel<1><<<1, 256, 0, s>>>(partial, blocks, 1.0 / (2.0 * L.V), out);
+}
+
 // ------------------------------------------------------------ FP32 links --
 // n = padded floats: link l's 18 doubles into floats [20 l, 20 l + 18), zeros after.
 __global__ void su3_links_f32_kernel(const double *__restrict__ U, float *U32, size_t n) {
@@ -764,7 +930,11 @@ void su3_launch_links_to_f32(const double *U, float *U32, const Lattice &L, cuda
                                          const double *, int, double, double, double, double, double, double, bool, int, \
                                          cudaStream_t, uint64_t *);                                                      \
     template void su3_launch_charges<T>(const double *, const double *, const void *, const Lattice &, int, int, int,   \
-                                        double, double *, double *, cudaStream_t);
+                                        double, double *, double *, cudaStream_t);                                      \
+    template void su3_launch_color_force<T>(const double *, const double *, const void *, const Lattice &, int, int,    \
+                                            int, double *, double *, double *, double, cudaStream_t);                   \
+    template void su3_launch_fermion_energy<T>(const void *, const void *, const Lattice &, int, int, int, double *,    \
+                                               double *, cudaStream_t);
 OVL_SU3_INSTANTIATE(double)
 OVL_SU3_INSTANTIATE(float)
 

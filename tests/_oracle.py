@@ -84,6 +84,11 @@ def oracle():
         L.orc3_bulk.argtypes = [P, _dp, _dp, _dp]
         L.orc3_gauss_restore.argtypes = [P, _dp, _dp, C.c_int, C.c_double, _dp]
         L.orc3_gauss_restore.restype = C.c_int
+        L.orc3_color_force.argtypes = [P, _dp, _dp, C.c_int, C.c_int, _dp]
+        L.orc3_fermion_energy.argtypes = [P, _dp, _dp, C.c_int, C.c_int]
+        L.orc3_fermion_energy.restype = C.c_double
+        L.orc3_coupled_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
+                                            C.c_double, C.c_int]
         L.orc_chebyshev_coeffs.argtypes = [C.c_int, C.c_double, _dp]
         L.orc3_overlap_apply.argtypes = [P, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double]
         L.orc3_overlap_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int,

@@ -270,12 +270,11 @@ def test_chebyshev_overlap_operator_and_leapfrog(precision):
 
 
 def test_three_colour_limits_are_reported():
-    for kw in (dict(precision="fp40"), dict(fermion="overlap", sign_method="zolotarev"), dict(backreaction=1.0),
-               dict(n_colours=4)):
+    for kw in (dict(precision="fp40"), dict(fermion="overlap", sign_method="zolotarev"), dict(n_colours=4)):
         with pytest.raises(OvlError):
             ctx3(**kw)
     with ctx3("fp64") as ctx:
-        for call in (ctx.currents, ctx.fermion_energy):
+        for call in (ctx.currents,):
             with pytest.raises(OvlError):
                 call()
 
@@ -298,3 +297,30 @@ def test_gauss_restore():
         assert r["iterations"] == n and r["max"] <= 1e-14
         assert rel_err(ctx.get_efield(), Eo) < 1e-12
         assert ctx.bulk()["gauss_max"] <= 1e-14
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_back_reaction_force_energy_and_coupled_leapfrog(precision):
+    """The fermion force on E, the fermion energy and the coupled step (gauge
+    force and back-reaction g^2 = 0.7) against the three-colour oracle."""
+    U = random_links_su3(N, 0.6, 40)
+    E = random_efield_su3(N, 0.3, 41)
+    psi, mid = modes3(M, 42), modes3(M, 43)
+    p = oracle_params(N, m=0.1, dt=0.05)
+    F = np.zeros((volume(N), 3, 8))
+    oracle().orc3_color_force(C.byref(p), ptr(f64(U)), ptr(f64(psi)), M, 0, ptr(F))
+    h = oracle().orc3_fermion_energy(C.byref(p), ptr(f64(U)), ptr(f64(psi)), M, 0)
+    o_U, o_E, o_psi, o_mid = f64(U).copy(), E.copy(), psi.copy(), mid.copy()
+    t = C.c_int(0)
+    oracle().orc3_coupled_leapfrog(C.byref(p), ptr(o_U), ptr(o_E), ptr(f64(o_psi)), ptr(f64(o_mid)), M, 0, C.byref(t),
+                                   3, 0.7, 1)
+    tol = TOL[precision]
+    with ctx3(precision, gauge_force=True, backreaction=0.7) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_modes(psi, mid)
+        assert rel_err(ctx.color_force(), F) < (1e-12 if precision == "fp64" else 1e-5)
+        assert abs(ctx.fermion_energy() - h) <= (1e-12 if precision == "fp64" else 1e-6) * abs(h)
+        ctx.step(3)
+        assert rel_err(ctx.get_efield(), o_E) < (1e-12 if precision == "fp64" else 1e-5)
+        assert rel_err(ctx.get_modes()[0], o_psi) < tol

@@ -234,3 +234,35 @@ def test_chebyshev_overlap_against_dense_polynomial():
     # the series approximates (h^2)^(-1/2) where h^2 >= eps lambda_max
     ok = lam >= eps * lmax
     assert np.abs(poly[ok] * np.sqrt(lam[ok]) - 1).max() < 0.05
+
+
+def test_color_force_is_the_energy_gradient_and_embeds_su2():
+    """dH_F/dtheta^a against a central difference of H_F along the link update
+    exp(i theta t^a) U of one link, and the SU(2) embedding against
+    orc_color_force (itself checked the same way)."""
+    N = (3, 4, 3)
+    V = volume(N)
+    U = f64(random_links_su3(N, 0.7, 30)).copy()
+    psi = random_modes3(6, N, 31)
+    p = oracle_params(N, m=0.1)
+    F = np.zeros((V, 3, 8))
+    oracle().orc3_color_force(C.byref(p), ptr(U), ptr(f64(psi)), 6, 0, ptr(F))
+    h = 1e-5
+    for (s, mu, a) in ((0, 0, 0), (5, 1, 4), (17, 2, 7), (30, 0, 2)):
+        vals = []
+        for sign in (+1, -1):
+            Ut = U.copy()
+            E = np.zeros((V, 3, 8))
+            E[s, mu, a] = 1.0
+            # exp(i cU E t) with cU = -dt_step: dt_step = -sign h moves theta^a by sign h
+            oracle().orc3_update_links(C.byref(p), ptr(Ut), ptr(E), -sign * h)
+            vals.append(oracle().orc3_fermion_energy(C.byref(p), ptr(Ut), ptr(f64(psi)), 6, 0))
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - F[s, mu, a]) < 1e-7 * max(1.0, np.abs(F).max()), (s, mu, a)
+    U2 = random_links(N, 0.6, 32)
+    psi2 = random_modes(6, N, 33)
+    F2 = np.zeros((V, 3, 3))
+    oracle().orc_color_force(C.byref(p), ptr(U2), ptr(f64(psi2)), 6, 1, ptr(F2))
+    F3 = np.zeros((V, 3, 8))
+    oracle().orc3_color_force(C.byref(p), ptr(f64(embed_su2_links(U2))), ptr(f64(embed_modes(psi2))), 6, 1, ptr(F3))
+    assert np.abs(F3[..., :3] - F2).max() < 1e-14 * max(1.0, np.abs(F2).max())
