@@ -41,6 +41,21 @@ __device__ inline int site_index(const Lattice &L, int x, int y, int z) {
     return x + L.N0 * (y + L.N1 * z);
 }
 
+// ------------------------------------------------------ compensated sums --
+// Neumaier's compensated summation (Z. angew. Math. Mech. 54, 1974): the
+// running sum s and the accumulated rounding c, so that a long sum of FP64
+// terms loses no more than a few units of the last place of the result.  The
+// global sums of the axial charge, the energy and E.B accumulate in it.
+struct CompSum {
+    double s = 0.0, c = 0.0;
+    __host__ __device__ void add(double x) {
+        const double t = s + x;
+        c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+        s = t;
+    }
+    __host__ __device__ double value() const { return s + c; }
+};
+
 // ----------------------------------------------------------------- complex --
 template <typename T> struct cpx { T re, im; };
 template <typename T> struct vec2_of;

@@ -186,15 +186,15 @@ __global__ void __launch_bounds__(kEnergyThreads)
     energy_partial_kernel(SRC psi, SRC dpsi, size_t n, int V, int n_modes, int first_mode, double *__restrict__ partial) {
     __shared__ double sh[kEnergyThreads];
     const size_t per_mb = (size_t)V * kComp * kModeBlock;
-    double acc = 0.0;
+    CompSum acc;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         const int mode = (int)(e / per_mb) * kModeBlock + (int)(e % kModeBlock);
         if (mode >= n_modes) continue;
         const cpx<double> a = psi(e), d = dpsi(e);
         const double im = a.re * d.im - a.im * d.re;  // Im conj(a) d
-        acc += (((first_mode + mode) & 1) == 0) ? -im : im;
+        acc.add((((first_mode + mode) & 1) == 0) ? -im : im);
     }
-    sh[threadIdx.x] = acc;
+    sh[threadIdx.x] = acc.value();
     __syncthreads();
     for (int s = kEnergyThreads / 2; s > 0; s >>= 1) {
         if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
@@ -206,9 +206,9 @@ __global__ void __launch_bounds__(kEnergyThreads)
 __global__ void __launch_bounds__(kEnergyThreads)
     energy_finish_kernel(const double *__restrict__ partial, int blocks, double scale, double *__restrict__ out) {
     __shared__ double sh[kEnergyThreads];
-    double acc = 0.0;
-    for (int b = threadIdx.x; b < blocks; b += kEnergyThreads) acc += partial[b];
-    sh[threadIdx.x] = acc;
+    CompSum acc;
+    for (int b = threadIdx.x; b < blocks; b += kEnergyThreads) acc.add(partial[b]);
+    sh[threadIdx.x] = acc.value();
     __syncthreads();
     for (int s = kEnergyThreads / 2; s > 0; s >>= 1) {
         if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];

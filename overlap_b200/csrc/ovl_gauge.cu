@@ -178,7 +178,7 @@ __device__ void improved_b(const double *__restrict__ U, const Lattice &L, int x
 __global__ void __launch_bounds__(kReduceThreads) ncsdot_kernel(const double *__restrict__ U, const double *__restrict__ E,
                                                                  Lattice L, double *partial) {
     __shared__ double sh[32];
-    double v[1] = {0.0};
+    CompSum sum;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.V; s += gridDim.x * blockDim.x) {
         int x, y, z;
         site_coords(L, s, x, y, z);
@@ -187,9 +187,10 @@ __global__ void __launch_bounds__(kReduceThreads) ncsdot_kernel(const double *__
             double e[3], b[3];
             improved_e(U, E, L, x, y, z, mu, e);
             improved_b(U, L, x, y, z, plane[mu][0], plane[mu][1], b);
-            v[0] += e[0] * b[0] + e[1] * b[1] + e[2] * b[2];
+            sum.add(e[0] * b[0] + e[1] * b[1] + e[2] * b[2]);
         }
     }
+    double v[1] = {sum.value()};
     block_reduce<1, false>(v, sh);
     if (threadIdx.x == 0) partial[blockIdx.x] = v[0];
 }
@@ -198,12 +199,15 @@ template <int NV, bool MAX_LAST>
 __global__ void finish_kernel(const double *__restrict__ partial, int n, double *out, double scale) {
     __shared__ double sh[32 * NV];
     double v[NV];
-    for (int k = 0; k < NV; k++) v[k] = (MAX_LAST && k == NV - 1) ? -1e300 : 0.0;
+    CompSum t[NV];
+    double mx = -1e300;
     for (int i = threadIdx.x; i < n; i += blockDim.x)
         for (int k = 0; k < NV; k++) {
-            double p = partial[(size_t)i * NV + k];
-            v[k] = (MAX_LAST && k == NV - 1) ? fmax(v[k], p) : v[k] + p;
+            const double p = partial[(size_t)i * NV + k];
+            if (MAX_LAST && k == NV - 1) mx = fmax(mx, p);
+            else t[k].add(p);
         }
+    for (int k = 0; k < NV; k++) v[k] = (MAX_LAST && k == NV - 1) ? mx : t[k].value();
     block_reduce<NV, MAX_LAST>(v, sh);
     if (threadIdx.x == 0)
         for (int k = 0; k < NV; k++) out[k] = (MAX_LAST && k == NV - 1) ? v[k] : scale * v[k];
@@ -336,15 +340,16 @@ __global__ void __launch_bounds__(kReduceThreads) bulk_kernel(const double *__re
 
 __global__ void bulk_finish_kernel(const double *__restrict__ partial, int n, Lattice L, double *out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double s[kBulkVals + 1];
-    for (int k = 0; k <= kBulkVals; k++) s[k] = 0.0;
+    CompSum cs[8];
     double gmax = 0.0, umax = 0.0;
     for (int i = 0; i < n; i++) {
         const double *p = partial + (size_t)i * (kBulkVals + 1);
-        for (int k = 0; k < 8; k++) s[k] += p[k];
+        for (int k = 0; k < 8; k++) cs[k].add(p[k]);
         gmax = fmax(gmax, p[9]);
         umax = fmax(umax, p[10]);
     }
+    double s[8];
+    for (int k = 0; k < 8; k++) s[k] = cs[k].value();
     const double V = (double)L.V;
     double e2[3], b2[3];
     for (int k = 0; k < 3; k++) { e2[k] = s[k] / V; b2[k] = s[3 + k] / V; }

@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
     const int lane = threadIdx.x;
     const int site = blockIdx.x * kCurrentsThreadsY + threadIdx.y;
     const int g = blockIdx.y;
-    double acc[kChargeVals] = {0.0, 0.0, 0.0, 0.0};
+    CompSum sum[kChargeVals];
     if (site < L.V) {
         int x, y, z;
         site_coords(L, site, x, y, z);
@@ -260,12 +260,15 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
                         cdot(f[c][3], chi[c][1]);
                 hop += b.im;
             }
-            acc[0] += w * nv;
-            acc[1] += w * 2.0 * zz.re;
-            acc[2] += w * -2.0 * zz.im;
-            acc[3] += w * (r * (-12.0 * zz.im + 2.0 * hop));
+            sum[0].add(w * nv);
+            sum[1].add(w * 2.0 * zz.re);
+            sum[2].add(w * -2.0 * zz.im);
+            sum[3].add(w * (r * (-12.0 * zz.im + 2.0 * hop)));
         }
     }
+    double acc[kChargeVals];
+#pragma unroll
+    for (int k = 0; k < kChargeVals; k++) acc[k] = sum[k].value();
 #pragma unroll
     for (int k = 0; k < kChargeVals; k++) {
         double t = acc[k];
@@ -287,10 +290,10 @@ __global__ void __launch_bounds__(kModeBlock *kCurrentsThreadsY)
 
 __global__ void charges_finish_kernel(const double *__restrict__ partial, int n, double scale, double *__restrict__ out4) {
     __shared__ double sh[kChargeVals][256];
-    double t[kChargeVals] = {0.0, 0.0, 0.0, 0.0};
+    CompSum t[kChargeVals];
     for (int i = threadIdx.x; i < n; i += blockDim.x)
-        for (int k = 0; k < kChargeVals; k++) t[k] += partial[(size_t)i * kChargeVals + k];
-    for (int k = 0; k < kChargeVals; k++) sh[k][threadIdx.x] = t[k];
+        for (int k = 0; k < kChargeVals; k++) t[k].add(partial[(size_t)i * kChargeVals + k]);
+    for (int k = 0; k < kChargeVals; k++) sh[k][threadIdx.x] = t[k].value();
     __syncthreads();
     for (int stride = blockDim.x / 2; stride > 0; stride >>= 1) {
         if ((int)threadIdx.x < stride)

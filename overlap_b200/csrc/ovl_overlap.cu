@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
     const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
     const int g = blockIdx.y;
     if (site >= L.V) return;
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    CompSum sum[8];
     for (int mb = g; mb < n_mb; mb += groups) {
         const int mode = mb * kModeBlock + lane;
         const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
@@ -273,10 +273,13 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
                 a2 = a2 + bilinear<double>(GA2[mu], f[c], o[c]);
             }
             // Re(z1 + (-i/2) z2) = Re z1 + Im z2 / 2
-            acc[mu] += w * (v1.re + 0.5 * v2.im);
-            acc[4 + mu] += w * (a1.re + 0.5 * a2.im);
+            sum[mu].add(w * (v1.re + 0.5 * v2.im));
+            sum[4 + mu].add(w * (a1.re + 0.5 * a2.im));
         }
     }
+    double acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc[k] = sum[k].value();
 #pragma unroll
     for (int k = 0; k < 8; k++) {
         double t = acc[k];

@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(kModeBlock *kSites3)
     __shared__ double sh[kSites3][4];
     const int lane = threadIdx.x;
     const int site = blockIdx.x * kSites3 + threadIdx.y;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    CompSum sum[4];
     if (site < L.V) {
         int x, y, z;
         site_coords(L, site, x, y, z);
@@ -266,12 +266,15 @@ __global__ void __launch_bounds__(kModeBlock *kSites3)
                 }
                 hop += b.im;
             }
-            acc[0] += w * nv;
-            acc[1] += w * 2.0 * zz.re;
-            acc[2] += w * -2.0 * zz.im;
-            acc[3] += w * (r * (-12.0 * zz.im + 2.0 * hop));
+            sum[0].add(w * nv);
+            sum[1].add(w * 2.0 * zz.re);
+            sum[2].add(w * -2.0 * zz.im);
+            sum[3].add(w * (r * (-12.0 * zz.im + 2.0 * hop)));
         }
     }
+    double acc[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) acc[k] = sum[k].value();
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         double t = acc[k];
@@ -296,11 +299,10 @@ __global__ void __launch_bounds__(kModeBlock *kSites3)
 template <int NV>
 __global__ void su3_sum_rows_kernel(const double *__restrict__ partial, int n, double scale, double *__restrict__ out) {
     __shared__ double sh[256][NV];
-    double t[NV];
-    for (int k = 0; k < NV; k++) t[k] = 0.0;
+    CompSum t[NV];
     for (int i = threadIdx.x; i < n; i += blockDim.x)
-        for (int k = 0; k < NV; k++) t[k] += partial[(size_t)i * NV + k];
-    for (int k = 0; k < NV; k++) sh[threadIdx.x][k] = t[k];
+        for (int k = 0; k < NV; k++) t[k].add(partial[(size_t)i * NV + k]);
+    for (int k = 0; k < NV; k++) sh[threadIdx.x][k] = t[k].value();
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
         if ((int)threadIdx.x < w)
@@ -597,13 +599,16 @@ __global__ void __launch_bounds__(kReduce3Threads)
 
 __global__ void su3_bulk_finish_kernel(const double *__restrict__ partial, int n, Lattice L, double *out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0}, gmax = -1e300, umax = 0.0;
+    CompSum cs[8];
+    double gmax = -1e300, umax = 0.0;
     for (int i = 0; i < n; i++) {
         const double *p = partial + (size_t)i * 10;
-        for (int k = 0; k < 8; k++) s[k] += p[k];
+        for (int k = 0; k < 8; k++) cs[k].add(p[k]);
         gmax = fmax(gmax, p[8]);
         umax = fmax(umax, p[9]);
     }
+    double s[8];
+    for (int k = 0; k < 8; k++) s[k] = cs[k].value();
     const double V = (double)L.V;
     double e2[3], b2[3];
     for (int k = 0; k < 3; k++) { e2[k] = s[k] / V; b2[k] = s[3 + k] / V; }
@@ -886,15 +891,15 @@ __global__ void __launch_bounds__(256)
                               int n_modes, int first_mode, double *__restrict__ partial) {
     __shared__ double sh[32];
     const size_t per_mb = (size_t)V * kComp3 * kModeBlock;
-    double acc = 0.0;
+    CompSum acc;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         const int mode = (int)(e / per_mb) * kModeBlock + (int)(e % kModeBlock);
         if (mode >= n_modes) continue;
         const cpx<T> a = ld(psi + e), d = ld(dpsi + e);
         const double im = (double)a.re * (double)d.im - (double)a.im * (double)d.re;  // Im conj(a) d
-        acc += (((first_mode + mode) & 1) == 0) ? -im : im;
+        acc.add((((first_mode + mode) & 1) == 0) ? -im : im);
     }
-    const double t = block_sum(acc, sh);
+    const double t = block_sum(acc.value(), sh);
     if (threadIdx.x == 0) partial[blockIdx.x] = t;
 }
 
