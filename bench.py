@@ -380,9 +380,9 @@ def serving_leg(count, device):
     U(1) flux n_B in {0, 2, 4, 8}, FP32 modes; a quarter SU(3), an eighth
     overlap fermions (Chebyshev degree 64, plane waves, N = 8 and 100-200
     steps: an overlap step costs ~130 Wilson steps); the Wilson requests on Z2
-    stochastic modes.  Admitted by device memory: SU(2) Wilson requests into one
-    continuously batched ensemble, the others as contexts of their own beside
-    it; N_5, N_CS and energy streamed every 50 steps.  A fixed number of
+    stochastic modes.  Admitted by device memory: Wilson requests (SU(2) and
+    SU(3)) into one continuously batched ensemble, overlap requests as contexts
+    of their own beside it; N_5, N_CS and energy streamed every 50 steps.  A fixed number of
     requests (time-boxed: the offered load exceeds the GPU's capacity)."""
     from overlap_b200.serve import Server, poisson_requests
 

@@ -1,8 +1,9 @@
-// Ensembles: independent trajectories (members) of their own lattice size
-// and mode count, stepped together.  One launch advances the hop work of every
-// member by a half step and one launch updates every member's links, so a
-// leapfrog step of the whole ensemble is five kernels (two half steps, two
-// link updates, the step counters), captured once as a CUDA graph.
+// Ensembles: independent trajectories (members) of their own lattice size,
+// mode count and colour count, stepped together.  One launch per group of
+// members (colours x U(1) background, at most kParamMembers each) advances
+// their hop work by a half step and one launch updates every member's links,
+// so a leapfrog step of the whole ensemble is a handful of kernels (the half
+// steps, two link updates, the step counters), captured once as a CUDA graph.
 //
 // Work is cut into tiles of SITES sites x one block of 32 modes (a warp per
 // site, as the single-trajectory kernels); tiles are numbered member by member
@@ -13,6 +14,7 @@
 #include "ovl_fp40.cuh"
 #include "ovl_internal.h"
 #include "ovl_stencil.cuh"
+#include "ovl_su3.cuh"
 
 namespace ovl {
 
@@ -33,69 +35,11 @@ template <typename T, int SITES> struct BatchOcc {
     static constexpr int kMinBlocks = (sizeof(T) == 4 ? 1024 : 512) / (kModeBlock * SITES);
 };
 
-constexpr int kMaxBatchLookup = 1024;  // members whose first tiles a CTA stages in shared memory
-
-// The member of tile `key`: the members' first tiles are staged in shared
-// memory (one coalesced load) and searched there.
-__device__ __forceinline__ int find_tile_member(const BatchMember *__restrict__ m, int count, long long key) {
-    __shared__ long long first[kMaxBatchLookup];
-    const int nthreads = blockDim.x * blockDim.y, tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int n = count < kMaxBatchLookup ? count : kMaxBatchLookup;
-    for (int i = tid; i < n; i += nthreads) first[i] = m[i].tile0;
-    __syncthreads();
-    if (count > kMaxBatchLookup) return find_member(m, count, key, &BatchMember::tile0);
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (first[mid] <= key) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 // phase 0: psi += dt D psimid; phase 1: psimid += dt D psi.  One launch covers
-// the members [0, count) of `members`: a group all with a U(1) background (U1)
-// or all without, tiles numbered on from the group's first member.
-template <typename T, int SITES, bool U1>
-__global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlocks)
-    wilson_batch_kernel(const BatchMember *__restrict__ members, int count, int phase) {
-    const long long key = (long long)blockIdx.x + members[0].tile0;
-    const int mi = find_tile_member(members, count, key);
-    const BatchMember &m = members[mi];
-    const Lattice L{m.N0, m.N1, m.N2, m.V};
-    const int nsb = (L.V + SITES - 1) / SITES;
-    const long long local = key - m.tile0;
-    const int mb = (int)(local / nsb);
-    const int site = (int)(local % nsb) * SITES + threadIdx.y;
-    if (site >= L.V) return;
-    const int lane = threadIdx.x;
-    const cpx<T> *src = reinterpret_cast<const cpx<T> *>(phase == 0 ? m.psimid : m.psi);
-    cpx<T> *dst = reinterpret_cast<cpx<T> *>(phase == 0 ? m.psi : m.psimid);
-    const int n01 = L.N0 * L.N1;
-    Spinor<T> acc;
-    if constexpr (sizeof(T) == 4)
-        wilson_site_lk(LinksF32<U1>{reinterpret_cast<const float4 *>(m.U32), reinterpret_cast<const float2 *>(m.u1_32),
-                                    n01},
-                       src, L, site, mb, lane, (T)m.amass, acc);
-    else
-        wilson_site_lk(LinksF64<U1>{m.U, reinterpret_cast<const double2 *>(m.u1), n01}, src, L, site, mb, lane,
-                       (T)m.amass, acc);
-    cpx<T> *out = dst + field_index(L.V, mb, site, 0, lane);
-    const T dt = (T)m.dt;
-#pragma unroll
-    for (int c = 0; c < kColours; c++)
-#pragma unroll
-        for (int a = 0; a < kSpin; a++) {
-            const cpx<T> d = finish_component(acc.c[c][a], a);
-            cpx<T> *o = out + (c * kSpin + a) * kModeBlock;
-            const cpx<T> v = ld(o);
-            st(o, v + dt * d);
-        }
-}
-
-// The same with the group's descriptors passed by value (kernel parameter
+// the members of one group (all with a U(1) background, U1, or all without;
+// at most kParamMembers), their descriptors passed by value (kernel parameter
 // space, read through the constant cache: no dependent global loads before a
-// CTA knows its member).
+// CTA finds its member); tiles numbered on from the first member's tile0.
 template <typename T, int SITES, bool U1>
 __global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlocks)
     wilson_batch_param_kernel(const __grid_constant__ BatchGroup g, int phase) {
@@ -138,6 +82,47 @@ __global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlo
         }
 }
 
+// Three-colour members (SU(3) links, 12-component modes), one group per U(1)
+// setting; descriptors by value as above.  FP32 modes read the padded FP32
+// link copy, FP64 modes the FP64 links.
+template <typename T, int SITES, bool U1>
+__global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlocks / 2)
+    wilson_batch3_kernel(const __grid_constant__ BatchGroup g, int phase) {
+    const long long key = (long long)blockIdx.x + g.m[0].tile0;
+    int lo = 0, hi = g.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (g.m[mid].tile0 <= key) lo = mid;
+        else hi = mid - 1;
+    }
+    const BatchMember &m = g.m[lo];
+    const Lattice L{m.N0, m.N1, m.N2, m.V};
+    const int nsb = (L.V + SITES - 1) / SITES;
+    const long long local = key - m.tile0;
+    const int mb = (int)(local / nsb);
+    const int site = (int)(local % nsb) * SITES + threadIdx.y;
+    if (site >= L.V) return;
+    const int lane = threadIdx.x;
+    const cpx<T> *src = reinterpret_cast<const cpx<T> *>(phase == 0 ? m.psimid : m.psi);
+    cpx<T> *dst = reinterpret_cast<cpx<T> *>(phase == 0 ? m.psi : m.psimid);
+    constexpr bool F32 = sizeof(T) == 4;
+    const Links3<F32, U1> lk{F32 ? (const void *)m.U32 : (const void *)m.U, F32 ? (const void *)m.u1_32 : (const void *)m.u1,
+                             L.N0 * L.N1};
+    Spinor3<T> acc;
+    wilson_site3(lk, src, L, site, mb, lane, (T)m.amass, acc);
+    cpx<T> *out = dst + field_index3(L.V, mb, site, 0, lane);
+    const T dt = (T)m.dt;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int a = 0; a < kSpin; a++) {
+            const cpx<T> v = acc.c[c][a];
+            const cpx<T> d = (T)0.5 * (a < 2 ? times_mi(v) : times_i(v));
+            cpx<T> *o = out + (c * kSpin + a) * kModeBlock;
+            st(o, ld(o) + dt * d);
+        }
+}
+
 // Link updates of every member, U <- exp(-i dt/2 E^a t^a) U where the member's
 // links move (Update.cpp:57 on its own step counter), with the FP32 copy kept.
 __global__ void links_batch_kernel(const BatchMember *__restrict__ members, int count, long long total) {
@@ -147,6 +132,19 @@ __global__ void links_batch_kernel(const BatchMember *__restrict__ members, int 
     const BatchMember &m = members[mi];
     const int k = (int)(l - m.link0);  // link of the member: 3 site + mu
     if (!(m.qs * (*m.tsteps * m.dt) < m.t_sphaleron)) return;
+    if (m.nc == 3) {  // SU(3): Dynamics.cpp:97-138 with the 3x3 exponential
+        const int site = k / 3, mu = k % 3;
+        cmat3<double> u = m3_mul(su3_exp(-0.5 * m.dt, m.E + 8 * (size_t)k), load_su3(m.U, site, mu));
+        if (m.reunit) u = su3_reunitarize(u);
+        store_su3(m.U, site, mu, u);
+        if (m.U32) {
+            float2 *p = reinterpret_cast<float2 *>(m.U32 + (size_t)kLink32Floats * k);
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) p[i + 3 * j] = float2{(float)u.m[i][j].re, (float)u.m[i][j].im};
+            p[9] = float2{0.0f, 0.0f};
+        }
+        return;
+    }
     const double *e = m.E + 3 * k;
     const quat g = qexp(-0.5 * m.dt, e[0], e[1], e[2]);
     const int site = k / 3, mu = k % 3;
@@ -167,40 +165,26 @@ __global__ void advance_batch_kernel(const BatchMember *__restrict__ members, in
 long long batch_tiles(int V, int n_mb, int sites) { return (long long)((V + sites - 1) / sites) * n_mb; }
 
 template <int SITES, bool U1>
-static void launch_hop(const BatchMember *members, int count, long long tiles, int phase, bool fp32, cudaStream_t s) {
+static void launch_hop_param(const BatchGroup &g, long long tiles, int phase, bool fp32, cudaStream_t s, int nc) {
     const dim3 block(kModeBlock, SITES);
-    if (fp32) wilson_batch_kernel<float, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(members, count, phase);
-    else wilson_batch_kernel<double, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(members, count, phase);
-}
-
-void launch_batch_hop(const BatchMember *members, int count, long long tiles, int sites, int phase, bool fp32, bool u1,
-                      cudaStream_t stream) {
-    if (count <= 0 || tiles <= 0) return;
-    if (u1) {
-        if (sites == 4) launch_hop<4, true>(members, count, tiles, phase, fp32, stream);
-        else launch_hop<8, true>(members, count, tiles, phase, fp32, stream);
-    } else {
-        if (sites == 4) launch_hop<4, false>(members, count, tiles, phase, fp32, stream);
-        else launch_hop<8, false>(members, count, tiles, phase, fp32, stream);
+    if (nc == 3) {
+        if (fp32) wilson_batch3_kernel<float, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(g, phase);
+        else wilson_batch3_kernel<double, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(g, phase);
+        return;
     }
-}
-
-template <int SITES, bool U1>
-static void launch_hop_param(const BatchGroup &g, long long tiles, int phase, bool fp32, cudaStream_t s) {
-    const dim3 block(kModeBlock, SITES);
     if (fp32) wilson_batch_param_kernel<float, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(g, phase);
     else wilson_batch_param_kernel<double, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(g, phase);
 }
 
 void launch_batch_hop_param(const BatchGroup &g, long long tiles, int sites, int phase, bool fp32, bool u1,
-                            cudaStream_t stream) {
+                            cudaStream_t stream, int nc) {
     if (g.count <= 0 || tiles <= 0) return;
     if (u1) {
-        if (sites == 4) launch_hop_param<4, true>(g, tiles, phase, fp32, stream);
-        else launch_hop_param<8, true>(g, tiles, phase, fp32, stream);
+        if (sites == 4) launch_hop_param<4, true>(g, tiles, phase, fp32, stream, nc);
+        else launch_hop_param<8, true>(g, tiles, phase, fp32, stream, nc);
     } else {
-        if (sites == 4) launch_hop_param<4, false>(g, tiles, phase, fp32, stream);
-        else launch_hop_param<8, false>(g, tiles, phase, fp32, stream);
+        if (sites == 4) launch_hop_param<4, false>(g, tiles, phase, fp32, stream, nc);
+        else launch_hop_param<8, false>(g, tiles, phase, fp32, stream, nc);
     }
 }
 

@@ -1508,11 +1508,12 @@ struct ovl_ensemble {
     bool fp32 = true;
     int sites = 0;  // sites per tile of the batched hop; 0 until tuned
     double tile_ms[2] = {0.0, 0.0};
-    std::vector<ovl::BatchMember> host;  // members without a U(1) background first, then those with
+    std::vector<ovl::BatchMember> host;  // members in group order (colours, then U(1) background)
     ovl::BatchMember *dev = nullptr;
     int *dev_tsteps = nullptr;
-    int groups[2] = {0, 0};            // members without / with U(1)
-    long long group_tiles[2] = {0, 0};
+    // groups: 2 x (nc - 2) + (U(1) on): two colours without / with U(1), three colours without / with
+    int groups[4] = {0, 0, 0, 0};
+    int step_launches = 0;  // kernels in the captured step graph
     long long tiles = 0, links = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1538,23 +1539,22 @@ int ens_fail(ovl_ensemble *e, int code, const char *fmt, ...) {
 
 // Descriptors of all members for tiles of `sites` sites; `tuning`: the hop
 // writes each member's operator buffer instead of psi (the state is kept).
+int ens_group(const ovl_ctx *c) { return 2 * (c->nc - 2) + (c->u1_on ? 1 : 0); }
+
 void ens_describe(ovl_ensemble *e, int sites, bool tuning) {
     e->host.resize(e->members.size());
-    // members without a U(1) background first (one kernel instance per group)
+    // members in group order (one kernel instance per group)
     std::vector<int> order;
-    for (int g = 0; g < 2; g++)
+    for (int g = 0; g < 4; g++)
         for (size_t i = 0; i < e->members.size(); i++)
-            if ((int)e->members[i]->u1_on == g) order.push_back((int)i);
-    e->groups[0] = e->groups[1] = 0;
-    e->group_tiles[0] = e->group_tiles[1] = 0;
+            if (ens_group(e->members[i]) == g) order.push_back((int)i);
+    for (int &n : e->groups) n = 0;
     long long tile = 0, link = 0;
     for (size_t k = 0; k < order.size(); k++) {
         const int i = order[k];
         ovl_ctx *c = e->members[i];
         ovl::BatchMember &m = e->host[k];
-        const int g = c->u1_on ? 1 : 0;
-        e->groups[g]++;
-        e->group_tiles[g] += ovl::batch_tiles(c->L.V, c->n_mb, sites);
+        e->groups[ens_group(c)]++;
         m.psi = tuning ? c->aux_dst : c->psi;
         m.psimid = c->psimid;
         m.U = c->U;
@@ -1569,6 +1569,8 @@ void ens_describe(ovl_ensemble *e, int sites, bool tuning) {
         m.V = c->L.V;
         m.n_mb = c->n_mb;
         m.reunit = c->p.reunitarize != 0;
+        m.nc = c->nc;
+        m.comp = c->comp;
         m.amass = amass(c->p);
         m.dt = c->p.dt;
         m.qs = c->p.qs;
@@ -1606,23 +1608,28 @@ bool ens_same_graph(const ovl_ensemble *e) {
            std::memcmp(e->captured.data(), e->host.data(), sizeof(ovl::BatchMember) * e->host.size()) == 0;
 }
 
-// The launches of one batched half step: each member group by its kernel,
-// its descriptors passed by value when they fit the parameter space (a
-// captured graph then holds them: it is recaptured when they change).
-void ens_hop(ovl_ensemble *e, int sites, int phase) {
-    int first = 0;
-    for (int g = 0; g < 2; g++) {
+// The launches of one batched half step: each member group by its kernel, in
+// chunks of at most kParamMembers descriptors passed by value (a captured
+// graph holds them: it is recaptured when they change).
+int ens_hop(ovl_ensemble *e, int sites, int phase) {
+    int first = 0, n_launch = 0;
+    for (int g = 0; g < 4; g++) {
         const int n = e->groups[g];
-        if (n > 0 && n <= ovl::kParamMembers) {
+        for (int c0 = 0; c0 < n; c0 += ovl::kParamMembers) {
             ovl::BatchGroup &bg = *e->param;
-            bg.count = n;
-            std::copy(e->host.begin() + first, e->host.begin() + first + n, bg.m);
-            ovl::launch_batch_hop_param(bg, e->group_tiles[g], sites, phase, e->fp32, g == 1, e->stream);
-        } else {
-            ovl::launch_batch_hop(e->dev + first, n, e->group_tiles[g], sites, phase, e->fp32, g == 1, e->stream);
+            bg.count = std::min(ovl::kParamMembers, n - c0);
+            long long tiles = 0;
+            for (int k = 0; k < bg.count; k++) {
+                const ovl::BatchMember &m = e->host[first + c0 + k];
+                bg.m[k] = m;
+                tiles += ovl::batch_tiles(m.V, m.n_mb, sites);
+            }
+            ovl::launch_batch_hop_param(bg, tiles, sites, phase, e->fp32, (g & 1) != 0, e->stream, g >= 2 ? 3 : 2);
+            n_launch++;
         }
         first += n;
     }
+    return n_launch;
 }
 
 }  // namespace
@@ -1643,8 +1650,7 @@ int ovl_ensemble_create(const ovl_params *members, int count, ovl_ensemble **out
             return ens_fail(nullptr, OVL_E_ARG, "ovl_ensemble_create: member %d: one precision and device for all", i);
         if (p.backreaction != 0.0 || p.gauge_force)
             return ens_fail(nullptr, OVL_E_UNSUPPORTED, "ovl_ensemble_create: member %d: no coupled evolution", i);
-        if (p.n_colours != 2)
-            return ens_fail(nullptr, OVL_E_UNSUPPORTED, "ovl_ensemble_create: member %d: two colours only", i);
+
     }
     ovl_ensemble *e = new (std::nothrow) ovl_ensemble();
     if (!e) return ens_fail(nullptr, OVL_E_OOM, "ovl_ensemble_create: host allocation");
@@ -1700,7 +1706,7 @@ int ovl_ensemble_add(ovl_ensemble *e, const ovl_params *member, int *index) {
         p.device != e->device)
         return ens_fail(e, OVL_E_ARG, "ovl_ensemble_add: the ensemble's precision and device");
     if (p.backreaction != 0.0 || p.gauge_force) return ens_fail(e, OVL_E_UNSUPPORTED, "ovl_ensemble_add: no coupled evolution");
-    if (p.n_colours != 2) return ens_fail(e, OVL_E_UNSUPPORTED, "ovl_ensemble_add: two colours only");
+
     if (cudaSetDevice(e->device) != cudaSuccess) return ens_fail(e, OVL_E_CUDA, "ovl_ensemble_add: device");
     ovl_params q = p;
     q.stream = reinterpret_cast<uint64_t>(e->stream);
@@ -1772,14 +1778,13 @@ int ens_tune(ovl_ensemble *e) {
         float total = 0.0f;
         for (int rep = 0; rep < 4; rep++) {
             cudaEventRecord(a, e->stream);
-            ens_hop(e, cand[k], 0);
+            e->launches += ens_hop(e, cand[k], 0);
             cudaEventRecord(b, e->stream);
             cudaEventSynchronize(b);
             float t = 0.0f;
             cudaEventElapsedTime(&t, a, b);
             if (rep > 0) total += t;
         }
-        e->launches += 4;
         e->tile_ms[k] = total / 3.0;
         if (e->tile_ms[k] < best) { best = e->tile_ms[k]; pick = cand[k]; }
     }
@@ -1792,21 +1797,22 @@ int ens_tune(ovl_ensemble *e) {
 }
 
 // One leapfrog step of every member (Update.cpp:48-79 per member): half step,
-// links, half step, links, step counters.
-void ens_enqueue_step(ovl_ensemble *e) {
+// links, half step, links, step counters.  Returns the launches enqueued.
+int ens_enqueue_step(ovl_ensemble *e) {
     const int n = (int)e->members.size();
-    ens_hop(e, e->sites, 0);
+    int nl = ens_hop(e, e->sites, 0);
     ovl::launch_batch_links(e->dev, n, e->links, e->stream);
-    ens_hop(e, e->sites, 1);
+    nl += ens_hop(e, e->sites, 1);
     ovl::launch_batch_links(e->dev, n, e->links, e->stream);
     ovl::launch_batch_advance(e->dev, n, e->stream);
+    return nl + 3;
 }
 
 int ens_capture(ovl_ensemble *e) {
     ens_free_graph(e);
     cudaError_t r = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
     if (r == cudaSuccess) {
-        ens_enqueue_step(e);
+        e->step_launches = ens_enqueue_step(e);
         r = cudaStreamEndCapture(e->stream, &e->graph);
     }
     if (r == cudaSuccess) r = cudaGraphInstantiate(&e->exec, e->graph, 0);
@@ -1839,7 +1845,7 @@ int ovl_ensemble_step(ovl_ensemble *e, int nsteps) {
         cudaError_t r = cudaGraphLaunch(e->exec, e->stream);
         if (r != cudaSuccess) return ens_fail(e, OVL_E_CUDA, "ovl_ensemble_step: graph launch: %s", cudaGetErrorString(r));
     }
-    e->launches += (uint64_t)(3 + (e->groups[0] > 0) * 2 + (e->groups[1] > 0) * 2) * nsteps;
+    e->launches += (uint64_t)e->step_launches * nsteps;
     for (ovl_ctx *c : e->members) c->tsteps += nsteps;
     cudaError_t r = cudaGetLastError();
     return r == cudaSuccess ? OVL_OK : ens_fail(e, OVL_E_CUDA, "ovl_ensemble_step: %s", cudaGetErrorString(r));

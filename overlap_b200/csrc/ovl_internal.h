@@ -127,16 +127,11 @@ struct BatchMember {
     int N0, N1, N2, V;
     int n_mb;
     int reunit;
+    int nc, comp;  // colours (2 or 3) and complex components per mode and site (4 nc)
     double amass, dt, qs, t_sphaleron;
     long long tile0, link0;
 };
 long long batch_tiles(int V, int n_mb, int sites);
-// phase 0: psi += dt D psimid, phase 1: psimid += dt D psi, for the `count`
-// members from `members` on (one group: all with a U(1) background, u1, or all
-// without; tiles numbered on from the group's first member's tile0); FP32
-// (fp32) or FP64 modes; sites per tile 4 or 8.
-void launch_batch_hop(const BatchMember *members, int count, long long tiles, int sites, int phase, bool fp32, bool u1,
-                      cudaStream_t stream);
 // Up to kParamMembers descriptors of a group passed by value (kernel
 // parameter space; 128 x 136 bytes stays inside the 32 KB parameter limit).
 constexpr int kParamMembers = 128;
@@ -146,7 +141,7 @@ struct BatchGroup {
 };
 static_assert(sizeof(BatchGroup) <= 32764, "kernel parameter limit");
 void launch_batch_hop_param(const BatchGroup &g, long long tiles, int sites, int phase, bool fp32, bool u1,
-                            cudaStream_t stream);
+                            cudaStream_t stream, int nc = 2);
 void launch_batch_links(const BatchMember *members, int count, long long total_links, cudaStream_t stream);
 void launch_batch_advance(const BatchMember *members, int count, cudaStream_t stream);
 // Stochastic vacuum modes (ovl_stochastic.cu): kind 0 FP64, 1 FP32, 2 FP40

@@ -1,8 +1,8 @@
 """Serving: trajectory requests arrive over time, are admitted as device
 memory frees up, and advance together (continuous batching: a request that
 arrives while others run joins at the next tick, and a finished one leaves).
-SU(2) Wilson requests share one batched ensemble (one CUDA graph per step for
-all of them); SU(3) and overlap requests, which the batched kernels do not
+Wilson requests (SU(2) and SU(3)) share one batched ensemble (one CUDA graph
+per step for all of them); overlap requests, which the batched kernels do not
 cover, run as contexts of their own on their own streams, stepped in the same
 ticks so their kernels overlap the ensemble's on the GPU.  Each request's
 observables -- N_5, N_CS along the cooling-free path (ovl_ncs_update) and the
@@ -52,8 +52,8 @@ class Request:
         return self.n_modes * volume(self.N)
 
     def batchable(self) -> bool:
-        """SU(2) Wilson requests join the batched ensemble."""
-        return self.n_colours == 2 and self.fermion == "wilson"
+        """Wilson requests (two or three colours) join the batched ensemble."""
+        return self.fermion == "wilson"
 
 
 def request_bytes(req: Request, precision: str) -> int:

@@ -75,3 +75,53 @@ def test_ensemble_rejects_unsupported_members():
     with pytest.raises(OvlError):
         Ensemble([Params(N=(4, 4, 4), n_modes=8, form="fused", precision="fp32"),
                   Params(N=(4, 4, 4), n_modes=8, form="fused", precision="fp64")])
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_three_colour_members_batch_beside_two_colour_ones(precision):
+    """SU(3) members (with and without a U(1) background) in the same ensemble
+    as SU(2) ones: one batched launch per group, each member as alone."""
+    from overlap_b200.inputs import random_efield_su3, random_links_su3, volume
+
+    def modes3(n, N, seed):
+        rng = np.random.default_rng(seed)
+        shape = (n, volume(N), 3, 4)
+        return rng.normal(0, np.sqrt(0.5), shape) + 1j * rng.normal(0, np.sqrt(0.5), shape)
+
+    kws = [dict(N=(4, 4, 6), n_modes=40, m_fermion=0.1, dt=0.05, t_sphaleron=1e9, n_colours=3),
+           dict(N=(4, 5, 4), n_modes=64, m_fermion=0.05, dt=0.05, t_sphaleron=1e9, n_colours=3, reunitarize=True),
+           dict(N=(6, 4, 4), n_modes=33, m_fermion=0.1, dt=0.05, t_sphaleron=1e9, n_colours=2)]
+    params = [Params(precision=precision, form="fused", m_dw=0.0, hop_variant=0, **kw) for kw in kws]
+
+    def setup(ctx, i, kw):
+        N = kw["N"]
+        if kw["n_colours"] == 3:
+            ctx.set_links(random_links_su3(N, 0.6, 50 + i))
+            ctx.set_efield(random_efield_su3(N, 0.3, 60 + i))
+            ctx.set_modes(modes3(kw["n_modes"], N, 70 + i), modes3(kw["n_modes"], N, 80 + i))
+        else:
+            ctx.set_links(random_links(N, 0.6, 50 + i))
+            ctx.set_efield(random_efield(N, 0.3, 60 + i))
+            ctx.set_modes(random_modes(kw["n_modes"], N, 70 + i), random_modes(kw["n_modes"], N, 80 + i))
+        if i == 1:
+            ctx.set_u1(phases(N, 9))
+
+    alone = []
+    for i, (p, kw) in enumerate(zip(params, kws)):
+        with Context(p) as ctx:
+            setup(ctx, i, kw)
+            ctx.step(4)
+            alone.append((ctx.get_modes()[0], ctx.get_links(), ctx.charges()["N5"]))
+    with Ensemble(params) as ens:
+        for i, kw in enumerate(kws):
+            setup(ens[i], i, kw)
+        ens.step(4)
+        n5 = ens.charges()[:, 1]
+        tol = 1e-13 if precision == "fp64" else 1e-5
+        for i in range(len(kws)):
+            psi, U, c = alone[i]
+            assert rel_err(ens[i].get_modes()[0], psi) < tol, i
+            assert rel_err(ens[i].get_links(), U) < 1e-13, i
+            assert abs(n5[i] - c) <= tol * max(1.0, abs(c)), i
+        # groups: SU(2) plain, SU(3) plain, SU(3) with U(1): 3 hop launches per half step + 3
+        assert ens.info()["launches"] >= 4 * 9

@@ -53,8 +53,9 @@ def test_request_results_are_the_same_alone_and_in_the_mix(precision):
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 def test_su3_and_overlap_requests_alongside_the_batch(precision):
-    """SU(3) and overlap requests run as contexts of their own next to the
-    batched SU(2) ensemble: each result is the same alone and in the mix."""
+    """SU(3) Wilson requests join the batched ensemble beside SU(2) ones, and
+    overlap requests run as contexts of their own next to it: each result is
+    the same alone and in the mix."""
     mk = [lambda t: req(3, (4, 4, 6), 64, 30, t, n_colours=3),
           lambda t: req(4, (4, 4, 4), 64, 20, t, fermion="overlap", cheb_degree=16, n_b=2),
           lambda t: req(5, (4, 4, 4), 64, 20, t, fermion="overlap", cheb_degree=16, n_colours=3)]
