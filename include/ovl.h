@@ -236,6 +236,14 @@ int ovl_solver_stats(const ovl_ctx *ctx, int out[3]);
  * Asynchronous on the context's stream (overlap: synchronises once per CG iteration). */
 int ovl_step(ovl_ctx *ctx, int nsteps);
 
+/* nsteps leapfrog steps as ovl_step, returning out = {N_V, N_5, PS} of the
+ * modes at the end (ovl_charges' first three values): in the fused Wilson form
+ * (two colours) they are summed inside the last step's second half step, which
+ * reads psi anyway, so the observation costs no extra pass over the modes
+ * (Currents.cpp:44-92 bilinears; the Wilson-term sum WA needs ovl_charges);
+ * in every other form the steps are followed by the charges kernel. */
+int ovl_step_observe(ovl_ctx *ctx, int nsteps, double out[3]);
+
 /* Leapfrog step counter Dynamics::tSteps. */
 int ovl_get_step_count(const ovl_ctx *ctx, int *steps);
 int ovl_set_step_count(ovl_ctx *ctx, int steps);

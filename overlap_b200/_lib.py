@@ -54,6 +54,7 @@ SIGNATURES = {
     "ovl_get_modes": ([_ctx, C.c_int, C.c_int, _dp, _dp], C.c_int),
     "ovl_set_free_fermions": ([_ctx, C.POINTER(C.c_int)], C.c_int),
     "ovl_step": ([_ctx, C.c_int], C.c_int),
+    "ovl_step_observe": ([_ctx, C.c_int, _dp], C.c_int),
     "ovl_get_step_count": ([_ctx, C.POINTER(C.c_int)], C.c_int),
     "ovl_set_step_count": ([_ctx, C.c_int], C.c_int),
     "ovl_currents": ([_ctx, _dp, _dp, _dp, _dp, _dp, _dp], C.c_int),

@@ -309,6 +309,13 @@ class Context:
         self._check(self._L.ovl_currents(self._ctx, *(_dp(out[k]) for k in ("jV", "jA", "jVw", "jAw", "PS", "WA"))))
         return out
 
+    def step_observe(self, nsteps: int = 1) -> dict:
+        """nsteps leapfrog steps, returning {NV, N5, PS} of the modes at the end,
+        summed inside the last half step in the fused Wilson form (ovl_step_observe)."""
+        o = np.empty(3)
+        self._check(self._L.ovl_step_observe(self._ctx, int(nsteps), _dp(o)))
+        return {"NV": o[0], "N5": o[1], "PS": o[2]}
+
     def charges(self) -> dict:
         o = np.empty(4)
         self._check(self._L.ovl_charges(self._ctx, _dp(o)))

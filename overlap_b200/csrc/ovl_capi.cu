@@ -72,6 +72,8 @@ struct ovl_ctx {
     void *ritz = nullptr;
     uint64_t ritz_calls = 0;
     double ritz_last[2] = {0.0, 0.0};
+    // charges summed inside the last half step (ovl_step_observe)
+    double *obs_partial = nullptr, *obs_scratch = nullptr;
     // per-kernel timing (ovl_profile_enable): event pairs per kind
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[OVL_PROF_KINDS];
@@ -738,7 +740,7 @@ int ovl_destroy(ovl_ctx *c) {
                     c->aux_src, c->aux_dst, c->ow.r, c->ow.q, c->ow.t, c->ow.x, c->ow.p, c->ow.part, c->ow.rnorm,
                     c->ow.alpha, c->ow.active, c->ow.dz, c->u_old, c->u_mid, c->e_mid, c->u1,
                     c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w, c->U32, c->u1_32, c->U_b, c->U32_b,
-                    c->psi_lo, c->psimid_lo, c->aux_src_lo, c->aux_dst_lo};
+                    c->psi_lo, c->psimid_lo, c->aux_src_lo, c->aux_dst_lo, c->obs_partial, c->obs_scratch};
     if (c->ow.host_count) cudaFreeHost(c->ow.host_count);
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -1063,6 +1065,76 @@ int ovl_step(ovl_ctx *c, int nsteps) {
         c->tsteps++;
         if ((rc = coupled_efield(c))) return rc;
     }
+    return OVL_OK;
+}
+
+int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) {
+    if (!c || !out) return OVL_E_ARG;
+    if (nsteps < 1) return fail(c, OVL_E_ARG, "ovl_step_observe: nsteps=%d", nsteps);
+    int rc = set_device(c);
+    if (rc) return rc;
+    const bool fused = !overlap(c) && !su3(c) && c->p.form == OVL_FORM_FUSED;
+    if (fused && c->hop_variant < 0 && (rc = autotune(c, nullptr))) return rc;
+    if (fused && c->mode_group < 0 && (rc = autotune_groups(c))) return rc;
+    if (!fused || (c->mode_group > 0 && c->mode_group < c->n_mb)) {
+        // other forms: the steps, then the charges kernel
+        double ch[4];
+        if ((rc = ovl_step(c, nsteps)) || (rc = ovl_charges(c, ch))) return rc;
+        for (int k = 0; k < 3; k++) out[k] = ch[k];
+        return OVL_OK;
+    }
+    if (nsteps > 1 && (rc = ovl_step(c, nsteps - 1))) return rc;
+    if (!c->obs_partial) {
+        if (cudaMalloc(&c->obs_partial, sizeof(double) * ovl::obs_partial_doubles(c->L, c->n_mb)) != cudaSuccess ||
+            cudaMalloc(&c->obs_scratch, sizeof(double) * 3 * 256) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, OVL_E_OOM, "ovl_step_observe: partial sums");
+        }
+    }
+    // the last step (Update.cpp:48-79); its second half step reads psi at the
+    // step's end and sums the charges on the way
+    const bool move = c->p.qs * (c->tsteps * c->p.dt) < c->p.t_sphaleron;
+    if ((rc = half_step(c, c->psimid, c->psi))) return rc;
+    if (move) {
+        {
+            ProfScope ps(c, OVL_PROF_LINKS);
+            launch_links(c, c->U, c->U32, 0.5 * c->p.dt);
+        }
+        if ((rc = launched(c, 1, "update links"))) return rc;
+    }
+    {
+        ProfScope ps(c, OVL_PROF_HOP);
+        const ovl::HopConfig hc = hop_config(c);
+        if (fp40(c))
+            ovl::launch_wilson40_observe(hc, c->psi, c->psi_lo, c->psimid, c->psimid_lo, c->L, c->n_mb, amass(c->p),
+                                         c->p.dt, c->p.n_modes, c->p.first_mode, c->obs_partial, c->stream);
+        else if (fp32(c))
+            ovl::launch_wilson_observe<float>(hc, c->psi, c->psimid, c->L, c->n_mb, amass(c->p), c->p.dt, c->p.n_modes,
+                                              c->p.first_mode, c->obs_partial, c->stream);
+        else
+            ovl::launch_wilson_observe<double>(hc, c->psi, c->psimid, c->L, c->n_mb, amass(c->p), c->p.dt,
+                                               c->p.n_modes, c->p.first_mode, c->obs_partial, c->stream);
+    }
+    if ((rc = launched(c, 1, "wilson (fused, observing)"))) return rc;
+    if (move) {
+        {
+            ProfScope ps(c, OVL_PROF_LINKS);
+            launch_links(c, c->U, c->U32, 0.5 * c->p.dt);
+        }
+        if ((rc = launched(c, 1, "update links"))) return rc;
+    }
+    c->tsteps++;
+    if ((rc = coupled_efield(c))) return rc;
+    {
+        ProfScope ps(c, OVL_PROF_OBS);
+        ovl::launch_obs_finish(c->obs_partial, ovl::obs_partial_doubles(c->L, c->n_mb) / 3, c->obs_scratch,
+                               1.0 / (2.0 * c->L.V), c->dev_small + 32, c->stream);
+    }
+    if ((rc = launched(c, 2, "charges (observing step)"))) return rc;
+    OVL_CUDA(c, cudaMemcpyAsync(c->host_small + 32, c->dev_small + 32, sizeof(double) * 3, cudaMemcpyDeviceToHost,
+                                c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 3; k++) out[k] = c->host_small[32 + k];
     return OVL_OK;
 }
 

@@ -31,6 +31,21 @@ template <typename T>
 void launch_wilson_tuned(const HopConfig &hc, const void *src, void *dst, const Lattice &L, int mb_first, int n_mb,
                          double amass, double dt, bool accumulate, cudaStream_t stream);
 void launch_links_to_f32(const double *U, float *U32, size_t n, cudaStream_t stream);
+// The fused half step dst += dt D src that also sums the local charges of src
+// (N_V, N_5, PS: the vacuum-weighted bilinears psi^+ psi, psi^+ g5 psi and
+// psi^+ i g0 g5 psi summed over modes and sites, Currents.cpp:44-92) on the way:
+// 3 doubles per CTA into `partial` (obs_partial_doubles), reduced by
+// launch_obs_finish into out3 (scaled by 1/2V).  FP32/FP64 modes (variant 0
+// stencil) or FP40 (src_lo / dst_lo set).
+size_t obs_partial_doubles(const Lattice &L, int n_mb);
+template <typename T>
+void launch_wilson_observe(const HopConfig &hc, const void *src, void *dst, const Lattice &L, int n_mb, double amass,
+                           double dt, int n_modes, int first_mode, double *partial, cudaStream_t stream);
+void launch_wilson40_observe(const HopConfig &hc, const void *src, const void *src_lo, void *dst, void *dst_lo,
+                             const Lattice &L, int n_mb, double amass, double dt, int n_modes, int first_mode,
+                             double *partial, cudaStream_t stream);
+void launch_obs_finish(const double *partial, size_t rows, double *scratch, double scale, double *out3,
+                       cudaStream_t stream);
 // Half step on 40-bit storage (uint2 high words + packed extension bytes,
 // ovl_fp40.cuh), FP64 arithmetic and FP64 links (hc.U, hc.u1); accumulate:
 // dst += dt D src, else dst (a buffer of n_mb blocks) = D src.  hc.variant:

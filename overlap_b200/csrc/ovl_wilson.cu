@@ -97,6 +97,140 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, HopOccupancy<T, VARI
     store_result<T, MODE>(dst, L.V, mb, site, lane, acc, dt);
 }
 
+// ------------------------------------------------- observing half step --
+constexpr int kObsVals = 3;
+
+// Vacuum-weighted local charges of one mode at one site (FP64 products; FP32
+// inputs multiply exactly in FP64): N_V += w |psi|^2, N_5 += w 2 Re z,
+// PS += -w 2 Im z with z = sum_c conj(psi_c0) psi_c2 + conj(psi_c1) psi_c3
+// (psi^+ g5 psi = 2 Re z, psi^+ i g0 g5 psi = -2 Im z in the Dirac basis).
+__device__ __forceinline__ void local_charges(const cpx<double> (&f)[kColours][kSpin], double w, double (&o)[kObsVals]) {
+    double nv = 0.0;
+    cpx<double> zz = mk<double>(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < kColours; c++) {
+#pragma unroll
+        for (int a = 0; a < kSpin; a++) nv += f[c][a].re * f[c][a].re + f[c][a].im * f[c][a].im;
+        zz = zz + cdot(f[c][0], f[c][2]) + cdot(f[c][1], f[c][3]);
+    }
+    o[0] = w * nv;
+    o[1] = w * 2.0 * zz.re;
+    o[2] = w * -2.0 * zz.im;
+}
+
+// Per-CTA sums (warp shuffles, then the warps in a fixed order) into partial.
+__device__ __forceinline__ void cta_partial(double (&o)[kObsVals], double *__restrict__ partial) {
+    __shared__ double sh[kSitesPerCta][kObsVals];
+#pragma unroll
+    for (int k = 0; k < kObsVals; k++) {
+        double t = o[k];
+        for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+        o[k] = t;
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < kObsVals; k++) sh[threadIdx.y][k] = o[k];
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        double *p = partial + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * kObsVals;
+        for (int k = 0; k < kObsVals; k++) {
+            double t = 0.0;
+            for (int j = 0; j < kSitesPerCta; j++) t += sh[j][k];
+            p[k] = t;
+        }
+    }
+}
+
+template <typename T, class LK>
+__global__ void __launch_bounds__(kModeBlock *kSitesPerCta, HopOccupancy<T, 0>::kMinBlocks)
+    wilson_observe_kernel(LK lk, const cpx<T> *__restrict__ src, cpx<T> *__restrict__ dst, Lattice L, T amass, T dt,
+                          int n_modes, int first_mode, double *__restrict__ partial) {
+    const int lane = threadIdx.x;
+    const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
+    const int mb = blockIdx.y;
+    double o[kObsVals] = {0.0, 0.0, 0.0};
+    if (site < L.V) {
+        Spinor<T> acc;
+        wilson_site_lk(lk, src, L, site, mb, lane, amass, acc);
+        store_result<T, 1>(dst, L.V, mb, site, lane, acc, dt);
+        // the site's own spinor again: an L1 hit, the stencil has just read it
+        const int mode = mb * kModeBlock + lane;
+        const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
+        const cpx<T> *p = src + field_index(L.V, mb, site, 0, lane);
+        cpx<double> f[kColours][kSpin];
+#pragma unroll
+        for (int c = 0; c < kColours; c++)
+#pragma unroll
+            for (int a = 0; a < kSpin; a++) {
+                const cpx<T> v = ld(p + (c * kSpin + a) * kModeBlock);
+                f[c][a] = mk<double>((double)v.re, (double)v.im);
+            }
+        local_charges(f, w, o);
+    }
+    cta_partial(o, partial);
+}
+
+size_t obs_partial_doubles(const Lattice &L, int n_mb) {
+    return (size_t)kObsVals * ((L.V + kSitesPerCta - 1) / kSitesPerCta) * n_mb;
+}
+
+template <typename T>
+void launch_wilson_observe(const HopConfig &hc, const void *src, void *dst, const Lattice &L, int n_mb, double amass,
+                           double dt, int n_modes, int first_mode, double *partial, cudaStream_t stream) {
+    const cpx<T> *s = reinterpret_cast<const cpx<T> *>(src);
+    cpx<T> *d = reinterpret_cast<cpx<T> *>(dst);
+    const dim3 block(kModeBlock, kSitesPerCta), grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
+    const int n01 = L.N0 * L.N1;
+    auto go = [&](const auto &lk) {
+        using LK = std::decay_t<decltype(lk)>;
+        wilson_observe_kernel<T, LK><<<grid, block, 0, stream>>>(lk, s, d, L, (T)amass, (T)dt, n_modes, first_mode,
+                                                                 partial);
+    };
+    if (std::is_same<T, float>::value && hc.U32 != nullptr) {
+        const float4 *u = reinterpret_cast<const float4 *>(hc.U32);
+        if (hc.u1_32) go(LinksF32<true>{u, reinterpret_cast<const float2 *>(hc.u1_32), n01});
+        else go(LinksF32<false>{u, nullptr, n01});
+    } else {
+        if (hc.u1) go(LinksF64<true>{hc.U, reinterpret_cast<const double2 *>(hc.u1), n01});
+        else go(LinksF64<false>{hc.U, nullptr, n01});
+    }
+}
+
+// Two-level fixed-order sum of `rows` rows of kObsVals: 256 CTAs sum
+// contiguous runs into scratch, one CTA sums those (compensated), scaled.
+__global__ void obs_rows_kernel(const double *__restrict__ partial, size_t rows, double *__restrict__ scratch) {
+    const size_t per = (rows + gridDim.x - 1) / gridDim.x, r0 = blockIdx.x * per;
+    const size_t r1 = r0 + per < rows ? r0 + per : rows;
+    __shared__ double sh[kObsVals][256];
+    CompSum t[kObsVals];
+    for (size_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+        for (int k = 0; k < kObsVals; k++) t[k].add(partial[r * kObsVals + k]);
+    for (int k = 0; k < kObsVals; k++) sh[k][threadIdx.x] = t[k].value();
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int k = 0; k < kObsVals; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < kObsVals; k++) scratch[blockIdx.x * kObsVals + k] = sh[k][0];
+}
+
+__global__ void obs_final_kernel(const double *__restrict__ scratch, int n, double scale, double *__restrict__ out3) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    CompSum t[kObsVals];
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < kObsVals; k++) t[k].add(scratch[i * kObsVals + k]);
+    for (int k = 0; k < kObsVals; k++) out3[k] = scale * t[k].value();
+}
+
+constexpr int kObsRowBlocks = 256;
+
+void launch_obs_finish(const double *partial, size_t rows, double *scratch, double scale, double *out3,
+                       cudaStream_t stream) {
+    obs_rows_kernel<<<kObsRowBlocks, 256, 0, stream>>>(partial, rows, scratch);
+    obs_final_kernel<<<1, 32, 0, stream>>>(scratch, kObsRowBlocks, scale, out3);
+}
+
 constexpr int kZChunk = 4;  // z sites per thread in the z-marching variant
 
 template <typename T, int MODE, class LK>
@@ -216,14 +350,20 @@ __device__ __forceinline__ void decode40(const Raw40 &r, Spinor<double> &s) {
 
 // MINB: CTAs of 8 warps per SM the register allocation must allow (2: 128
 // registers, 3: 80 registers with a few spills); the autotuner picks.
-template <int MODE, int MINB, class LK>
+// OBS: also sum the local charges of src into partial (as wilson_observe_kernel).
+template <int MODE, int MINB, class LK, bool OBS = false>
 __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, MINB)
     wilson_fp40_kernel(LK lk, const uint2 *__restrict__ src, const uint4 *__restrict__ src_lo, uint2 *__restrict__ dst,
-                       uint4 *__restrict__ dst_lo, Lattice L, double amass, double dt) {
+                       uint4 *__restrict__ dst_lo, Lattice L, double amass, double dt, int n_modes = 0,
+                       int first_mode = 0, double *__restrict__ partial = nullptr) {
     const int lane = threadIdx.x;
     const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
     const int mb = blockIdx.y;
-    if (site >= L.V) return;
+    double o[kObsVals] = {0.0, 0.0, 0.0};
+    if (site >= L.V) {
+        if (OBS) cta_partial(o, partial);
+        return;
+    }
     const int V = L.V;
     const Nbrs n = neighbours(L, site);
     Raw40 a, b;
@@ -231,6 +371,11 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, MINB)
     load_raw40(src, src_lo, V, mb, site, lane, a);
     load_raw40(src, src_lo, V, mb, n.xp, lane, b);
     decode40(a, f);
+    if (OBS) {
+        const int mode = mb * kModeBlock + lane;
+        const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
+        local_charges(f.c, w, o);
+    }
 #pragma unroll
     for (int c = 0; c < kColours; c++)
 #pragma unroll
@@ -275,6 +420,7 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, MINB)
             lw[k >> 1] |= pair << (16 * (k & 1));
         }
     dst_lo[((size_t)mb * V + site) * kModeBlock + lane] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    if (OBS) cta_partial(o, partial);
 }
 
 void launch_wilson40(const HopConfig &hc, const void *src, const void *src_lo, void *dst, void *dst_lo,
@@ -298,6 +444,24 @@ void launch_wilson40(const HopConfig &hc, const void *src, const void *src_lo, v
         } else {
             wilson_fp40_kernel<0, 2, LK><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt);
         }
+    };
+    if (hc.u1) go(LinksF64<true>{hc.U, reinterpret_cast<const double2 *>(hc.u1), n01});
+    else go(LinksF64<false>{hc.U, nullptr, n01});
+}
+
+void launch_wilson40_observe(const HopConfig &hc, const void *src, const void *src_lo, void *dst, void *dst_lo,
+                             const Lattice &L, int n_mb, double amass, double dt, int n_modes, int first_mode,
+                             double *partial, cudaStream_t stream) {
+    const uint2 *s = reinterpret_cast<const uint2 *>(src);
+    const uint4 *sl = reinterpret_cast<const uint4 *>(src_lo);
+    uint2 *d = reinterpret_cast<uint2 *>(dst);
+    uint4 *dl = reinterpret_cast<uint4 *>(dst_lo);
+    const dim3 block(kModeBlock, kSitesPerCta), grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
+    const int n01 = L.N0 * L.N1;
+    auto go = [&](const auto &lk) {
+        using LK = std::decay_t<decltype(lk)>;
+        wilson_fp40_kernel<1, 2, LK, true><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt, n_modes,
+                                                                        first_mode, partial);
     };
     if (hc.u1) go(LinksF64<true>{hc.U, reinterpret_cast<const double2 *>(hc.u1), n01});
     else go(LinksF64<false>{hc.U, nullptr, n01});
@@ -364,5 +528,9 @@ template void launch_wilson_tuned<double>(const HopConfig &, const void *, void 
 template void launch_wilson_tuned<float>(const HopConfig &, const void *, void *, const Lattice &, int, int, double,
                                          double, bool, cudaStream_t);
 template void launch_axpy<float>(void *, const void *, size_t, double, int, cudaStream_t);
+template void launch_wilson_observe<float>(const HopConfig &, const void *, void *, const Lattice &, int, double, double,
+                                           int, int, double *, cudaStream_t);
+template void launch_wilson_observe<double>(const HopConfig &, const void *, void *, const Lattice &, int, double,
+                                            double, int, int, double *, cudaStream_t);
 
 }  // namespace ovl

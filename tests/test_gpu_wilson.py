@@ -323,3 +323,31 @@ def test_fp40_free_fermions_and_observables_match_fp64():
         assert abs(out["fp40"][1][k] - out["fp64"][1][k]) < 1e-7
     assert abs(out["fp40"][2] - out["fp64"][2]) < 1e-9 * abs(out["fp64"][2])
     assert np.max(np.abs(out["fp40"][3] - out["fp64"][3])) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp40"])
+def test_step_observe_equals_step_then_charges(precision):
+    """ovl_step_observe sums N_V, N_5, PS inside the last half step: the same
+    state as ovl_step and the same charges as ovl_charges (both form the
+    bilinears in FP64 from the stored modes; only the summation order differs)."""
+    from overlap_b200.inputs import u1_flux
+
+    N = (4, 6, 6)
+    out = []
+    for observe in (False, True):
+        with Context(N=N, n_modes=80, first_mode=1, precision=precision, form="fused", m_fermion=0.05, m_dw=0.0,
+                     dt=0.05, t_sphaleron=1e9, hop_variant=0) as ctx:
+            ctx.set_links(random_links(N, 0.5, 3))
+            ctx.set_efield(random_efield(N, 0.3, 4))
+            ctx.set_u1(u1_flux(N, 2))
+            ctx.set_modes(random_modes(80, N, 5), random_modes(80, N, 6))
+            if observe:
+                ch = ctx.step_observe(3)
+            else:
+                ctx.step(3)
+                ch = ctx.charges()
+            out.append((ctx.get_modes()[0], ctx.get_links(), ch))
+    (p0, u0, c0), (p1, u1, c1) = out
+    assert np.array_equal(p0, p1) and np.array_equal(u0, u1)
+    for k in ("NV", "N5", "PS"):
+        assert abs(c0[k] - c1[k]) <= 1e-13 * max(1.0, abs(c0[k])), k
