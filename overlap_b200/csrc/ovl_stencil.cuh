@@ -124,33 +124,6 @@ __device__ __forceinline__ Nbrs neighbours(const Lattice &L, int site) {
     return n;
 }
 
-// The same stencil with every neighbour load issued one hop ahead of its use
-// (two spinor registers in flight), for more memory-level parallelism per warp.
-template <typename T, class LK>
-__device__ __forceinline__ void wilson_site_pipelined(const LK &lk, const cpx<T> *__restrict__ src, const Lattice &L,
-                                                      int site, int mb, int lane, T amass, Spinor<T> &acc) {
-    const int V = L.V;
-    const Nbrs n = neighbours(L, site);
-    Spinor<T> a, b;
-    load_spinor(src, V, mb, site, lane, a);
-    load_spinor(src, V, mb, n.xp, lane, b);
-#pragma unroll
-    for (int c = 0; c < kColours; c++)
-#pragma unroll
-        for (int s = 0; s < kSpin; s++) acc.c[c][s] = amass * a.c[c][s];
-    load_spinor(src, V, mb, n.xm, lane, a);
-    hop<T, 0, true>(acc, b, lk.template get<T>(site, 0));
-    load_spinor(src, V, mb, n.yp, lane, b);
-    hop<T, 0, false>(acc, a, lk.template get<T>(n.xm, 0));
-    load_spinor(src, V, mb, n.ym, lane, a);
-    hop<T, 1, true>(acc, b, lk.template get<T>(site, 1));
-    load_spinor(src, V, mb, n.zp, lane, b);
-    hop<T, 1, false>(acc, a, lk.template get<T>(n.ym, 1));
-    load_spinor(src, V, mb, n.zm, lane, a);
-    hop<T, 2, true>(acc, b, lk.template get<T>(site, 2));
-    hop<T, 2, false>(acc, a, lk.template get<T>(n.zm, 2));
-}
-
 // (D phi)(site) for the 32 modes of block mb (one per lane), before the
 // -i gamma_0 / 2 factor: amass phi(x) - sum of the six projected hops.
 template <typename T, class LK>

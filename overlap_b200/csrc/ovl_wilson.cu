@@ -53,8 +53,9 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
 }
 
 // Variants of the same half step for the autotuner (identical arithmetic):
-//   VARIANT 0  one site per thread, loads issued as the hops need them
-//   VARIANT 1  one site per thread, each neighbour load one hop ahead
+//   VARIANT 0  one site per warp, the 8 warps of a CTA on 8 consecutive sites
+//   VARIANT 1  one site per warp, the 8 warps of a CTA on a 4 x 2 (x, y) tile, so
+//              that x and y neighbours are read by warps of the same CTA (L1)
 //   VARIANT 2  one (x, y) column per thread marching in z: the z neighbours and
 //              the site itself come from registers (5 spinor loads per site
 //              instead of 7)
@@ -78,22 +79,33 @@ __device__ __forceinline__ void store_result(cpx<T> *__restrict__ dst, int V, in
         }
 }
 
-// CTAs of 8 warps per SM the compiler must fit: FP32 4 (<= 64 registers; 3 for
-// the pipelined variant, which holds two neighbour spinors), FP64 2.
+// CTAs of 8 warps per SM the compiler must fit: FP32 4 (<= 64 registers), FP64 2.
 template <typename T, int VARIANT> struct HopOccupancy {
-    static constexpr int kMinBlocks = sizeof(T) == 4 ? (VARIANT == 1 ? 3 : 4) : 2;
+    static constexpr int kMinBlocks = sizeof(T) == 4 ? 4 : 2;
 };
+
+constexpr int kTileX = 4, kTileY = kSitesPerCta / kTileX;  // the (x, y) tile of variant 1
 
 template <typename T, int MODE, int VARIANT, class LK>
 __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, HopOccupancy<T, VARIANT>::kMinBlocks)
     wilson_tuned_kernel(LK lk, const cpx<T> *__restrict__ src, cpx<T> *__restrict__ dst, Lattice L, T amass, T dt) {
     const int lane = threadIdx.x;
-    const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
     const int mb = blockIdx.y;
-    if (site >= L.V) return;
+    int site;
+    if (VARIANT == 1) {
+        const int ntx = (L.N0 + kTileX - 1) / kTileX, nty = (L.N1 + kTileY - 1) / kTileY;
+        const int t = blockIdx.x;
+        const int x = (t % ntx) * kTileX + (int)(threadIdx.y % kTileX);
+        const int y = ((t / ntx) % nty) * kTileY + (int)(threadIdx.y / kTileX);
+        const int z = t / (ntx * nty);
+        if (x >= L.N0 || y >= L.N1) return;
+        site = x + L.N0 * (y + L.N1 * z);
+    } else {
+        site = blockIdx.x * kSitesPerCta + threadIdx.y;
+        if (site >= L.V) return;
+    }
     Spinor<T> acc;
-    if (VARIANT == 1) wilson_site_pipelined(lk, src, L, site, mb, lane, amass, acc);
-    else wilson_site_lk(lk, src, L, site, mb, lane, amass, acc);
+    wilson_site_lk(lk, src, L, site, mb, lane, amass, acc);
     store_result<T, MODE>(dst, L.V, mb, site, lane, acc, dt);
 }
 
@@ -283,9 +295,13 @@ static void launch_variant(int variant, const LK &lk, const cpx<T> *s, cpx<T> *d
         wilson_zmarch_kernel<T, MODE, LK><<<grid, block, 0, stream>>>(lk, s, d, L, amass, dt);
         return;
     }
+    if (variant == 1) {
+        const int tiles = ((L.N0 + kTileX - 1) / kTileX) * ((L.N1 + kTileY - 1) / kTileY) * L.N2;
+        wilson_tuned_kernel<T, MODE, 1, LK><<<dim3(tiles, n_mb), block, 0, stream>>>(lk, s, d, L, amass, dt);
+        return;
+    }
     dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
-    if (variant == 1) wilson_tuned_kernel<T, MODE, 1, LK><<<grid, block, 0, stream>>>(lk, s, d, L, amass, dt);
-    else wilson_tuned_kernel<T, MODE, 0, LK><<<grid, block, 0, stream>>>(lk, s, d, L, amass, dt);
+    wilson_tuned_kernel<T, MODE, 0, LK><<<grid, block, 0, stream>>>(lk, s, d, L, amass, dt);
 }
 
 template <typename T>
