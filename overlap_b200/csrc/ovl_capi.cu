@@ -612,6 +612,9 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
         return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: FP40 storage is built for the fused Wilson form");
     if (p->form != OVL_FORM_PLAIN && p->form != OVL_FORM_FUSED) return fail(nullptr, OVL_E_ARG, "ovl_create: bad form");
     if (p->n_modes <= 0 || p->first_mode < 0) return fail(nullptr, OVL_E_ARG, "ovl_create: n_modes=%d first_mode=%d", p->n_modes, p->first_mode);
+    // mode blocks run along grid.y of the stencil launches (at most 65535)
+    if ((p->n_modes + ovl::kModeBlock - 1) / ovl::kModeBlock > 65535)
+        return fail(nullptr, OVL_E_ARG, "ovl_create: n_modes=%d above %d", p->n_modes, 65535 * ovl::kModeBlock);
     if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return fail(nullptr, OVL_E_ARG, "ovl_create: dt must be positive");
     if (p->mode_group < -1) return fail(nullptr, OVL_E_ARG, "ovl_create: mode_group=%d", p->mode_group);
     if (p->hop_variant < -1 || p->hop_variant >= ovl::kHopVariants)
