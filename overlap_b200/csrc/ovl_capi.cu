@@ -516,9 +516,16 @@ int run_currents(ovl_ctx *c) {
                                      c->per_site, c->stream, fp32(c), c->nc);
         return launched(c, 2, "overlap currents");
     }
-    if (su3(c))
-        return fail(c, OVL_E_UNSUPPORTED, "ovl_currents: per-site Wilson currents are built for two colours "
-                                          "(ovl_charges gives the lattice sums for three)");
+    if (su3(c)) {
+        ProfScope ps(c, OVL_PROF_OBS);
+        if (fp32(c))
+            ovl::su3_launch_currents<float>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
+                                            c->p.first_mode, c->p.r_wilson, c->partial, c->per_site, c->stream);
+        else
+            ovl::su3_launch_currents<double>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes,
+                                             c->p.first_mode, c->p.r_wilson, c->partial, c->per_site, c->stream);
+        return launched(c, 2, "currents (three colours)");
+    }
     ProfScope ps(c, OVL_PROF_OBS);
     if (fp40(c))
         ovl::launch_currents40(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->psi_lo, c->L, c->n_mb, c->p.n_modes,

@@ -259,6 +259,10 @@ void su3_chebyshev_apply(ChebyshevWork &w, const Su3Links &lk, const void *src, 
                          const double *coeff, int K, double eps, double lambda_max, double amass, double mdw, double mf,
                          double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches);
 size_t su3_charges_partial_doubles(const Lattice &L, int n_mb);
+// Per-site Wilson currents (kCurrentsPerSite values per site, as launch_currents).
+template <typename T>
+void su3_launch_currents(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                         int first_mode, double r_wilson, double *partial, double *per_site, cudaStream_t stream);
 template <typename T>
 void su3_launch_charges(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
                         int first_mode, double r_wilson, double *partial, double *out4, cudaStream_t stream);

@@ -294,6 +294,121 @@ __global__ void __launch_bounds__(kModeBlock *kSites3)
     }
 }
 
+// Per-site Wilson currents for three colours (currents_kernel of ovl_modes.cu,
+// Currents.cpp:7-394): per site the 18 vacuum-weighted mode sums jV^0..3,
+// jA^0..3, jVw^1..3, jAw^1..3, PS, WA (slots as kCurrentsPerSite), per group of
+// mode blocks into partial[g][site][18]; launch_currents_finish adds the groups.
+template <typename T>
+__device__ __forceinline__ cpx<double> colour_bilinear3(const mono &G, const cpx<double> (&f)[3][kSpin],
+                                                        const cpx<double> (&h)[3][kSpin]) {
+    return bilinear<double>(G, f[0], h[0]) + bilinear<double>(G, f[1], h[1]) + bilinear<double>(G, f[2], h[2]);
+}
+
+template <typename T>
+__device__ __forceinline__ void load_site3(const cpx<T> *__restrict__ psi, int V, int mb, int site, int lane,
+                                           cpx<double> (&f)[3][kSpin]) {
+    const cpx<T> *p = psi + field_index3(V, mb, site, 0, lane);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int a = 0; a < kSpin; a++) {
+            const cpx<T> v = ld(p + (c * kSpin + a) * kModeBlock);
+            f[c][a] = mk<double>((double)v.re, (double)v.im);
+        }
+}
+
+template <typename T, bool U1>
+__global__ void __launch_bounds__(kModeBlock *kSites3)
+    su3_currents_kernel(const double *__restrict__ U, const double *__restrict__ u1, const cpx<T> *__restrict__ psi,
+                        Lattice L, int n_mb, int n_modes, int first_mode, int groups, double r,
+                        double *__restrict__ partial) {
+    constexpr mono G1 = {{0, 1, 2, 3}, {0, 0, 0, 0}};
+    constexpr mono G5 = kGamma5;
+    constexpr mono G05 = mono_mul(kGamma0, kGamma5);
+    constexpr mono G0 = kGamma0;
+    constexpr mono GV[3] = {mono_mul(kGamma0, kGammaX), mono_mul(kGamma0, kGammaY), mono_mul(kGamma0, kGammaZ)};
+    constexpr mono GA[3] = {mono_mul(GV[0], kGamma5), mono_mul(GV[1], kGamma5), mono_mul(GV[2], kGamma5)};
+    const int lane = threadIdx.x;
+    const int site = blockIdx.x * kSites3 + threadIdx.y;
+    const int g = blockIdx.y;
+    if (site >= L.V) return;  // whole warps exit together
+    int x, y, z;
+    site_coords(L, site, x, y, z);
+    const int V = L.V;
+    int nb[3][2];
+    for (int mu = 0; mu < 3; mu++) {
+        int cp[3] = {x, y, z}, cm[3] = {x, y, z};
+        cp[mu] += 1;
+        cm[mu] -= 1;
+        nb[mu][0] = site_index(L, cp[0], cp[1], cp[2]);
+        nb[mu][1] = site_index(L, cm[0], cm[1], cm[2]);
+    }
+    const Links3<false, U1> lk{U, u1, L.N0 * L.N1};
+    CompSum acc[kCurrentsPerSite];
+    for (int mb = g; mb < n_mb; mb += groups) {
+        const int mode = mb * kModeBlock + lane;
+        const double w = mode >= n_modes ? 0.0 : (((first_mode + mode) & 1) == 0 ? 1.0 : -1.0);
+        cpx<double> f[3][kSpin];
+        load_site3(psi, V, mb, site, lane, f);
+        double v[kCurrentsPerSite];
+#pragma unroll
+        for (int k = 0; k < kCurrentsPerSite; k++) v[k] = 0.0;
+        v[0] = colour_bilinear3<T>(G1, f, f).re;
+        v[4] = colour_bilinear3<T>(G5, f, f).re;
+        const cpx<double> b05 = colour_bilinear3<T>(G05, f, f);
+        v[16] = -b05.im;
+        double wa = -6.0 * r * b05.im;
+        for (int mu = 0; mu < 3; mu++) {
+            cpx<double> h[3][kSpin], chi[3][kSpin];
+            load_site3(psi, V, mb, nb[mu][0], lane, h);  // forward: chi = U_mu(x) psi(x+mu)
+            {
+                const cmat3<double> M = lk.template get<double>(site, mu);
+#pragma unroll
+                for (int i = 0; i < 3; i++)
+#pragma unroll
+                    for (int a = 0; a < kSpin; a++)
+                        chi[i][a] = M.m[i][0] * h[0][a] + M.m[i][1] * h[1][a] + M.m[i][2] * h[2][a];
+            }
+            v[1 + mu] = colour_bilinear3<T>(GV[mu], f, chi).re;
+            v[5 + mu] = colour_bilinear3<T>(GA[mu], f, chi).re;
+            v[9 + mu] = r * colour_bilinear3<T>(G0, f, chi).im;
+            const double aw = r * colour_bilinear3<T>(G05, f, chi).im;
+            v[13 + mu] = aw;
+            wa += aw;
+            load_site3(psi, V, mb, nb[mu][1], lane, h);  // backward: chi = U_mu(x-mu)^+ psi(x-mu)
+            {
+                const cmat3<double> M = lk.template get<double>(nb[mu][1], mu);
+#pragma unroll
+                for (int i = 0; i < 3; i++)
+#pragma unroll
+                    for (int a = 0; a < kSpin; a++)
+                        chi[i][a] = cdot(M.m[0][i], h[0][a]) + cdot(M.m[1][i], h[1][a]) + cdot(M.m[2][i], h[2][a]);
+            }
+            wa += r * colour_bilinear3<T>(G05, f, chi).im;
+        }
+        v[17] = wa;
+#pragma unroll
+        for (int k = 0; k < kCurrentsPerSite; k++) acc[k].add(w * v[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < kCurrentsPerSite; k++) {
+        double t = acc[k].value();
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0) partial[((size_t)g * V + site) * kCurrentsPerSite + k] = t;
+    }
+}
+
+template <typename T>
+void su3_launch_currents(const double *U, const double *u1, const void *psi, const Lattice &L, int n_mb, int n_modes,
+                         int first_mode, double r, double *partial, double *per_site, cudaStream_t s) {
+    const int groups = currents_groups(n_mb);
+    const dim3 block(kModeBlock, kSites3), grid((L.V + kSites3 - 1) / kSites3, groups);
+    const cpx<T> *p = reinterpret_cast<const cpx<T> *>(psi);
+    if (u1) su3_currents_kernel<T, true><<<grid, block, 0, s>>>(U, u1, p, L, n_mb, n_modes, first_mode, groups, r, partial);
+    else su3_currents_kernel<T, false><<<grid, block, 0, s>>>(U, u1, p, L, n_mb, n_modes, first_mode, groups, r, partial);
+    launch_currents_finish(partial, groups, L, per_site, s);
+}
+
 // Sums `n` partial rows of `nv` values in a fixed order (one CTA: a strided
 // sum per thread, then a tree), scaled.
 template <int NV>
@@ -936,6 +1051,8 @@ void su3_launch_links_to_f32(const double *U, float *U32, const Lattice &L, cuda
                                          cudaStream_t, uint64_t *);                                                      \
     template void su3_launch_charges<T>(const double *, const double *, const void *, const Lattice &, int, int, int,   \
                                         double, double *, double *, cudaStream_t);                                      \
+    template void su3_launch_currents<T>(const double *, const double *, const void *, const Lattice &, int, int, int,  \
+                                         double, double *, double *, cudaStream_t);                                     \
     template void su3_launch_color_force<T>(const double *, const double *, const void *, const Lattice &, int, int,    \
                                             int, double *, double *, double *, double, cudaStream_t);                   \
     template void su3_launch_fermion_energy<T>(const void *, const void *, const Lattice &, int, int, int, double *,    \

@@ -273,10 +273,7 @@ def test_three_colour_limits_are_reported():
     for kw in (dict(precision="fp40"), dict(fermion="overlap", sign_method="zolotarev"), dict(n_colours=4)):
         with pytest.raises(OvlError):
             ctx3(**kw)
-    with ctx3("fp64") as ctx:
-        for call in (ctx.currents,):
-            with pytest.raises(OvlError):
-                call()
+
 
 
 def test_gauss_restore():
@@ -324,3 +321,41 @@ def test_back_reaction_force_energy_and_coupled_leapfrog(precision):
         ctx.step(3)
         assert rel_err(ctx.get_efield(), o_E) < (1e-12 if precision == "fp64" else 1e-5)
         assert rel_err(ctx.get_modes()[0], o_psi) < tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_currents_embed_su2_and_sum_to_the_charges(precision):
+    """Per-site Wilson currents for three colours: with SU(2) embedded and the
+    third colour empty they are the two-colour context's (pinned to the
+    reference); for SU(3) fields their lattice sums are the oracle's charges."""
+    U2 = random_links(N, 0.6, 44)
+    rng = np.random.default_rng(45)
+    psi2 = rng.normal(size=(M, volume(N), 2, 4)) + 1j * rng.normal(size=(M, volume(N), 2, 4))
+    with Context(N=N, n_modes=M, first_mode=1, precision=precision, form="fused", m_fermion=0.1, m_dw=0.0,
+                 dt=0.05, t_sphaleron=1e9, hop_variant=0) as c2:
+        c2.set_links(U2)
+        c2.set_u1(u1_flux(N, 2))
+        c2.set_modes(psi2, psi2)
+        cur2 = c2.currents()
+    psi3 = np.zeros((M, volume(N), 3, 4), np.complex128)
+    psi3[:, :, :2] = psi2
+    with ctx3(precision, first_mode=1) as c3:
+        c3.set_links(embed_su2_links(U2))
+        c3.set_u1(u1_flux(N, 2))
+        c3.set_modes(psi3, psi3)
+        cur3 = c3.currents()
+    for k in cur2:
+        scale = max(1.0, np.abs(cur2[k]).max())
+        assert np.abs(cur3[k] - cur2[k]).max() <= (1e-12 if precision == "fp64" else 1e-6) * scale, k
+    U = random_links_su3(N, 0.8, 46)
+    psi = modes3(M, 47)
+    want = np.zeros(4)
+    oracle().orc3_charges(C.byref(oracle_params(N, m=0.1)), ptr(f64(U)), ptr(f64(psi)), M, 0, ptr(want))
+    with ctx3(precision) as ctx:
+        ctx.set_links(U)
+        ctx.set_modes(psi, psi)
+        cur = ctx.currents()
+    got = [cur["jV"][:, 0].sum(), cur["jA"][:, 0].sum(), cur["PS"].sum(), cur["WA"].sum()]
+    scale = M * np.max(np.sum(np.abs(psi) ** 2, axis=(2, 3))) / (2 * volume(N))
+    # FP32 contexts store the modes rounded to FP32: the oracle's FP64 modes differ by that
+    assert np.abs(np.array(got) - want).max() <= (1e-11 if precision == "fp64" else 1e-6) * scale
