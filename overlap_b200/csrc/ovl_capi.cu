@@ -265,6 +265,8 @@ int next_coeffs(ovl_ctx *c, bool consume) {
     return OVL_OK;
 }
 
+ovl::HopConfig hop_config(const ovl_ctx *c);
+
 int run_overlap(ovl_ctx *c, const void *src, void *dst, int n_mb, int n_modes, bool accumulate, bool consume) {
     if (c->p.sign_method == OVL_SIGN_CHEBYSHEV) {
         double lo, hi;
@@ -281,11 +283,11 @@ int run_overlap(ovl_ctx *c, const void *src, void *dst, int n_mb, int n_modes, b
                                              c->p.cheb_degree, c->p.cheb_eps, hi, amass(c->p), c->p.m_dw,
                                              c->p.m_fermion, c->p.dt, accumulate, c->sm_count, c->stream, &nl);
         else if (fp32(c))
-            ovl::chebyshev_apply<float>(c->cw, c->U, c->u1_on ? c->u1 : nullptr, src, dst, c->L, n_mb, c->cheb.data(),
+            ovl::chebyshev_apply<float>(c->cw, hop_config(c), src, dst, c->L, n_mb, c->cheb.data(),
                                         c->p.cheb_degree, c->p.cheb_eps, hi, amass(c->p), c->p.m_dw, c->p.m_fermion,
                                         c->p.dt, accumulate, c->sm_count, c->stream, &nl);
         else
-            ovl::chebyshev_apply<double>(c->cw, c->U, c->u1_on ? c->u1 : nullptr, src, dst, c->L, n_mb, c->cheb.data(),
+            ovl::chebyshev_apply<double>(c->cw, hop_config(c), src, dst, c->L, n_mb, c->cheb.data(),
                                          c->p.cheb_degree, c->p.cheb_eps, hi, amass(c->p), c->p.m_dw, c->p.m_fermion,
                                          c->p.dt, accumulate, c->sm_count, c->stream, &nl);
         c->ostats.iterations = c->ostats.max_mode_iterations = c->p.cheb_degree;

@@ -41,19 +41,36 @@ void chebyshev_inverse_sqrt(int K, double eps, double *c) {
     }
 }
 
-// b_out = factor * (a * (-D w) + beta * b1) - b2 + ck * phi, per mode and site;
-// -D w is the stencil applied to w (the second half of X = -D^2 / lambda_max).
-template <typename T>
+// w = D b (the first half of X = -D^2 / lambda_max), with the links of LK.
+template <typename T, class LK>
 __global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
-    clenshaw_kernel(const double *__restrict__ links, const double2 *__restrict__ u1, const cpx<T> *__restrict__ w,
-                    const cpx<T> *__restrict__ b1, const cpx<T> *__restrict__ b2, const cpx<T> *__restrict__ phi,
-                    cpx<T> *__restrict__ bout, Lattice L, T amass, T a, T beta, T factor, T ck) {
+    cheb_wilson_kernel(LK lk, const cpx<T> *__restrict__ b, cpx<T> *__restrict__ w, Lattice L, T amass) {
     const int lane = threadIdx.x;
     const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
     const int mb = blockIdx.y;
     if (site >= L.V) return;
     Spinor<T> acc;
-    wilson_site(links, u1, w, L, site, mb, lane, amass, acc);
+    wilson_site_lk(lk, b, L, site, mb, lane, amass, acc);
+    cpx<T> *o = w + field_index(L.V, mb, site, 0, lane);
+#pragma unroll
+    for (int c = 0; c < kColours; c++)
+#pragma unroll
+        for (int s = 0; s < kSpin; s++) st(o + (c * kSpin + s) * kModeBlock, finish_component(acc.c[c][s], s));
+}
+
+// b_out = factor * (a * (-D w) + beta * b1) - b2 + ck * phi, per mode and site;
+// -D w is the stencil applied to w (the second half of X = -D^2 / lambda_max).
+template <typename T, class LK>
+__global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
+    clenshaw_kernel(LK lk, const cpx<T> *__restrict__ w, const cpx<T> *__restrict__ b1, const cpx<T> *__restrict__ b2,
+                    const cpx<T> *__restrict__ phi, cpx<T> *__restrict__ bout, Lattice L, T amass, T a, T beta,
+                    T factor, T ck) {
+    const int lane = threadIdx.x;
+    const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
+    const int mb = blockIdx.y;
+    if (site >= L.V) return;
+    Spinor<T> acc;
+    wilson_site_lk(lk, w, L, site, mb, lane, amass, acc);
     const size_t base = field_index(L.V, mb, site, 0, lane);
 #pragma unroll
     for (int c = 0; c < kColours; c++)
@@ -86,14 +103,13 @@ __global__ void overlap_finish_t_kernel(const cpx<T> *__restrict__ phi, const cp
     }
 }
 
-template <typename T>
-void chebyshev_apply(ChebyshevWork &w, const double *U, const double *u1, const void *src, void *dst, const Lattice &L,
-                     int n_mb, const double *coeff, int K, double eps, double lambda_max, double amass, double mdw,
-                     double mf, double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches) {
+template <typename T, class LK>
+static void cheb_run(const LK &lk, ChebyshevWork &w, const void *src, void *dst, const Lattice &L, int n_mb,
+                     const double *coeff, int K, double eps, double lambda_max, double amass, double mdw, double mf,
+                     double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches) {
     const size_t n = (size_t)n_mb * L.V * kComp * kModeBlock;
     dim3 block(kModeBlock, kSitesPerCta);
     dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
-    const double2 *ph = reinterpret_cast<const double2 *>(u1);
     const cpx<T> *phi = reinterpret_cast<const cpx<T> *>(src);
     cpx<T> *b[3] = {reinterpret_cast<cpx<T> *>(w.b0), reinterpret_cast<cpx<T> *>(w.b1), reinterpret_cast<cpx<T> *>(w.b2)};
     cpx<T> *tmp = reinterpret_cast<cpx<T> *>(w.w);
@@ -107,34 +123,50 @@ void chebyshev_apply(ChebyshevWork &w, const double *U, const double *u1, const 
     cudaMemsetAsync(b[1], 0, n * sizeof(cpx<T>), stream);
     cudaMemsetAsync(b[2], 0, n * sizeof(cpx<T>), stream);
     int i1 = 1, i2 = 2, io = 0;  // b_{k+1}, b_{k+2}, b_k
-    for (int k = K; k >= 1; k--) {
-        launch_wilson<T>(U, u1, b[i1], tmp, L, 0, n_mb, amass, 0.0, false, stream);
-        clenshaw_kernel<T><<<grid, block, 0, stream>>>(U, ph, tmp, b[i1], b[i2], phi, b[io], L, am, a, beta, (T)2,
-                                                      (T)(coeff[k] * scale));
+    for (int k = K; k >= 0; k--) {  // k = 0: y = t(X) b_1 - b_2 + c_0/2 phi (chi, scaled by lambda_max^-1/2)
+        cheb_wilson_kernel<T, LK><<<grid, block, 0, stream>>>(lk, b[i1], tmp, L, am);
+        clenshaw_kernel<T, LK><<<grid, block, 0, stream>>>(lk, tmp, b[i1], b[i2], phi, b[io], L, am, a, beta,
+                                                            (T)(k > 0 ? 2 : 1),
+                                                            (T)((k > 0 ? coeff[k] : 0.5 * coeff[0]) * scale));
         nl += 2;
         const int t = i2;
         i2 = i1;
         i1 = io;
         io = t;
     }
-    // y = t(X) b_1 - b_2 + c_0/2 phi  -> b[io] (chi, already scaled by lambda_max^-1/2)
-    launch_wilson<T>(U, u1, b[i1], tmp, L, 0, n_mb, amass, 0.0, false, stream);
-    clenshaw_kernel<T><<<grid, block, 0, stream>>>(U, ph, tmp, b[i1], b[i2], phi, b[io], L, am, a, beta, (T)1,
-                                                  (T)(0.5 * coeff[0] * scale));
-    // D chi, then the overlap combination
-    launch_wilson<T>(U, u1, b[io], tmp, L, 0, n_mb, amass, 0.0, false, stream);
+    // D chi (chi = b[i1]), then the overlap combination
+    cheb_wilson_kernel<T, LK><<<grid, block, 0, stream>>>(lk, b[i1], tmp, L, am);
     size_t blocks = (n + 255) / 256, cap = (size_t)sm_count * 16;
     overlap_finish_t_kernel<T><<<(int)(blocks < cap ? blocks : cap), 256, 0, stream>>>(
         phi, tmp, reinterpret_cast<cpx<T> *>(dst), n, (T)mdw, (T)mf, (T)dt, accumulate ? 1 : 0);
-    nl += 4;
+    nl += 2;
     if (launches) *launches += nl;
 }
 
-template void chebyshev_apply<float>(ChebyshevWork &, const double *, const double *, const void *, void *,
-                                     const Lattice &, int, const double *, int, double, double, double, double, double,
-                                     double, bool, int, cudaStream_t, uint64_t *);
-template void chebyshev_apply<double>(ChebyshevWork &, const double *, const double *, const void *, void *,
-                                      const Lattice &, int, const double *, int, double, double, double, double, double,
-                                      double, bool, int, cudaStream_t, uint64_t *);
+template <typename T>
+void chebyshev_apply(ChebyshevWork &w, const HopConfig &hc, const void *src, void *dst, const Lattice &L, int n_mb,
+                     const double *coeff, int K, double eps, double lambda_max, double amass, double mdw, double mf,
+                     double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches) {
+    const int n01 = L.N0 * L.N1;
+    auto go = [&](const auto &lk) {
+        cheb_run<T>(lk, w, src, dst, L, n_mb, coeff, K, eps, lambda_max, amass, mdw, mf, dt, accumulate, sm_count,
+                    stream, launches);
+    };
+    if (sizeof(T) == 4 && hc.U32 != nullptr) {  // FP32 modes: the FP32 link copy
+        const float4 *u = reinterpret_cast<const float4 *>(hc.U32);
+        if (hc.u1_32) go(LinksF32<true>{u, reinterpret_cast<const float2 *>(hc.u1_32), n01});
+        else go(LinksF32<false>{u, nullptr, n01});
+    } else {
+        if (hc.u1) go(LinksF64<true>{hc.U, reinterpret_cast<const double2 *>(hc.u1), n01});
+        else go(LinksF64<false>{hc.U, nullptr, n01});
+    }
+}
+
+template void chebyshev_apply<float>(ChebyshevWork &, const HopConfig &, const void *, void *, const Lattice &, int,
+                                     const double *, int, double, double, double, double, double, double, bool, int,
+                                     cudaStream_t, uint64_t *);
+template void chebyshev_apply<double>(ChebyshevWork &, const HopConfig &, const void *, void *, const Lattice &, int,
+                                      const double *, int, double, double, double, double, double, double, bool, int,
+                                      cudaStream_t, uint64_t *);
 
 }  // namespace ovl

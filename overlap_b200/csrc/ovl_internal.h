@@ -225,10 +225,12 @@ void chebyshev_inverse_sqrt(int K, double eps, double *c);
 struct ChebyshevWork {
     void *b0 = nullptr, *b1 = nullptr, *b2 = nullptr, *w = nullptr;  // one field each, mode precision
 };
+// The overlap operator with the Chebyshev series on all mode blocks; FP32 modes
+// take the FP32 link copy when hc.U32 is set.
 template <typename T>
-void chebyshev_apply(ChebyshevWork &w, const double *U, const double *u1, const void *src, void *dst, const Lattice &L,
-                     int n_mb, const double *coeff, int K, double eps, double lambda_max, double amass, double mdw,
-                     double mf, double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches);
+void chebyshev_apply(ChebyshevWork &w, const HopConfig &hc, const void *src, void *dst, const Lattice &L, int n_mb,
+                     const double *coeff, int K, double eps, double lambda_max, double amass, double mdw, double mf,
+                     double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches);
 
 // Free plane waves for local modes [0, n_modes) (global index first_mode + m):
 // Wilson spinors, or overlap spinors of Wilson kernel mass -m_dw.
