@@ -96,7 +96,8 @@ DTYPES = {"fp32": "f32 modes and hop arithmetic, f64 links",
 # The FP32 fused half-step kernel of each hop variant (ovl_wilson.cu).
 HOP_KERNELS = {0: "wilson_tuned_kernel<float,1,0,LinksF32<{u1}>>",
                1: "wilson_tuned_kernel<float,1,1,LinksF32<{u1}>>",
-               2: "wilson_zmarch_kernel<float,1,LinksF32<{u1}>>"}
+               2: "wilson_zmarch_kernel<float,1,LinksF32<{u1}>>",
+               3: "wilson_packed_kernel<1,{u1},false>"}
 
 
 def committed_traffic(kernel: str):
@@ -209,6 +210,8 @@ def reference_cpu(wl, steps: int, warmup: int, max_procs: int | None = None):
 
 # ---------------------------------------------------------------- GPU arm --
 def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-1, mode_group=0):
+    if hop_variant == 3 and precision != "fp32":
+        hop_variant = -1  # the packed-pair kernel is FP32's only: the others autotune
     import numpy as np
     import torch
 
@@ -522,8 +525,15 @@ def main():
                     help="the FP32-class form of the headline value (the other is reported beside it)")
     ap.add_argument("--mode-group", type=int, default=0,
                     help="fused form: mode blocks per group (0: whole batch, -1: autotune with the variant)")
-    ap.add_argument("--hop-variant", type=int, default=-1, choices=(-1, 0, 1, 2),
-                    help="-1: autotune the hop kernel before warm-up; 0-2: fixed variant")
+    # Variant 3 (two modes per thread on the paired FP32 instructions) is the
+    # default of the FP32 forms: it loses a short burst to variants 0/1 (4.9 vs
+    # 4.5 ms per half step at 1965 MHz, which is what the autotuner times) but
+    # draws less power per mode-site, and in this 100-step run under the 1 kW cap
+    # it held a higher clock and was faster (12.99-13.04 G vs 12.81-12.83 G
+    # mode-site updates/s, three alternating pairs).
+    ap.add_argument("--hop-variant", type=int, default=3, choices=(-1, 0, 1, 2, 3),
+                    help="-1: autotune the hop kernel before warm-up; 0-3: fixed variant (3: FP32 forms, the "
+                         "other forms autotune)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 forms")
     ap.add_argument("--modes", type=int, default=0, help="run a smaller case with this many modes (profiling)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,

@@ -30,7 +30,7 @@ extern "C" {
 /* Layout version of ovl_params and of the entry points; ovl_abi_version()
  * returns the value the library was built with.  A caller compiled against
  * another version must not pass its ovl_params to the library. */
-#define OVL_ABI_VERSION 5
+#define OVL_ABI_VERSION 6
 
 typedef enum {
     OVL_OK = 0,
@@ -92,8 +92,9 @@ typedef struct {
     int cheb_degree;
     double cheb_eps;
     /* Leapfrog hop kernel variant: -1 = time the variants on the first step and
-     * keep the fastest (ovl_autotune); 0, 1, 2 = fixed.  All variants give the
-     * same results. */
+     * keep the fastest (ovl_autotune); 0 .. OVL_HOP_VARIANTS-1 = fixed (3: FP32
+     * only).  All variants apply the same operator; they differ in the order
+     * of the FP32/FP64 roundings only. */
     int hop_variant;
     /* 1: project every link back onto SU(2) after each update (U / |U|,
      * MaxTraceProjection, SUNc/SU2/GroupOperations.cpp:261-281), or onto SU(3)
@@ -194,10 +195,14 @@ int ovl_apply(ovl_ctx *ctx, int count, const double *phi, double *out);
 
 /* Times the hop-kernel variants of the leapfrog half step on this context's
  * fields (its state is not changed) and keeps the fastest for later steps:
- * 0 = one site per thread, 1 = the same with neighbour loads issued one hop
- * ahead, 2 = (x, y) columns marching in z with register reuse.  *variant
- * receives the choice, ms[v] the time of one half step with variant v. */
-int ovl_autotune(ovl_ctx *ctx, int *variant, double ms[3]);
+ * 0 = one site per warp (32 modes), 8 consecutive sites per CTA; 1 = the same
+ * on a 4 x 2 (x, y) tile of sites per CTA; 2 = (x, y) columns marching in z
+ * with register reuse; 3 (FP32 only) = two modes per thread on the paired
+ * FP32 instructions, links built once per CTA in shared memory.  *variant
+ * receives the choice, ms[v] the time of one half step with variant v (0 for
+ * a variant the precision does not have). */
+#define OVL_HOP_VARIANTS 4
+int ovl_autotune(ovl_ctx *ctx, int *variant, double ms[OVL_HOP_VARIANTS]);
 
 /* The hop variant and mode grouping in use (after the autotuner ran, or as
  * set in ovl_params); -1 before either is known. */

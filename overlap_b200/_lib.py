@@ -18,7 +18,8 @@ STATUS_NAMES = {
 }
 
 
-ABI_VERSION = 5  # OVL_ABI_VERSION of include/ovl.h
+ABI_VERSION = 6  # OVL_ABI_VERSION of include/ovl.h
+HOP_VARIANTS = 4  # OVL_HOP_VARIANTS
 
 
 class ovl_params(C.Structure):

@@ -75,7 +75,7 @@ class Params:
     zolo_tol: float = 1e-12
     cg_max_iter: int = 1000
     cg_tol: float = 1e-16
-    hop_variant: int = -1            # -1: autotune on the first step; 0, 1, 2 fixed
+    hop_variant: int = -1            # -1: autotune on the first step; 0..3 fixed (3: FP32 only)
     reunitarize: bool = False        # project links onto SU(2) after each update
     gauge_force: bool = False        # coupled evolution: staple force on E every step
     backreaction: float = 0.0        # coupled evolution: g^2 of the fermion force on E
@@ -258,7 +258,7 @@ class Context:
         """Times the hop-kernel variants on this context's fields (state unchanged)
         and keeps the fastest: returns (variant, [ms per half step of each])."""
         v = C.c_int(0)
-        ms = np.zeros(3)
+        ms = np.zeros(_lib.HOP_VARIANTS)
         self._check(self._L.ovl_autotune(self._ctx, C.byref(v), _dp(ms)))
         return v.value, ms.tolist()
 

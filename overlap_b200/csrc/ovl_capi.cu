@@ -398,6 +398,8 @@ int autotune_groups(ovl_ctx *c) {
 
 // Times each hop-kernel variant on the live fields (psi -> operator buffer,
 // the context's state is not touched) and keeps the fastest.
+static_assert(ovl::kHopVariants == OVL_HOP_VARIANTS, "hop variant count of the header");
+
 int autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
@@ -405,7 +407,8 @@ int autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
     ovl::HopConfig h = hop_config(c);
     double best = 1e300;
     int pick = 0;
-    const int nv = fp40(c) ? ovl::kFp40Variants : ovl::kHopVariants;
+    // the packed kernel is FP32 only
+    const int nv = fp40(c) ? ovl::kFp40Variants : (fp32(c) ? ovl::kHopVariants : ovl::kPackedVariant);
     if (fp40(c)) cudaMemsetAsync(c->aux_dst_lo, 0, c->field_complex * 2, c->stream);
     if (ms_out)
         for (int v = 0; v < ovl::kHopVariants; v++) ms_out[v] = 0.0;
@@ -628,6 +631,8 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     if (p->mode_group < -1) return fail(nullptr, OVL_E_ARG, "ovl_create: mode_group=%d", p->mode_group);
     if (p->hop_variant < -1 || p->hop_variant >= ovl::kHopVariants)
         return fail(nullptr, OVL_E_ARG, "ovl_create: hop_variant=%d (-1 = autotune, 0..%d)", p->hop_variant, ovl::kHopVariants - 1);
+    if (p->hop_variant == ovl::kPackedVariant && p->precision != OVL_PREC_FP32)
+        return fail(nullptr, OVL_E_ARG, "ovl_create: hop_variant=%d (packed pairs) needs FP32 modes", p->hop_variant);
     const long long V = (long long)p->N[0] * p->N[1] * p->N[2];
     if (V > (1LL << 30) / 8) return fail(nullptr, OVL_E_ARG, "ovl_create: lattice too large");
 
@@ -1114,6 +1119,7 @@ int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) {
         }
         if ((rc = launched(c, 1, "update links"))) return rc;
     }
+    size_t obs_rows = ovl::obs_partial_doubles(c->L, c->n_mb) / 3;
     {
         ProfScope ps(c, OVL_PROF_HOP);
         const ovl::HopConfig hc = hop_config(c);
@@ -1121,11 +1127,11 @@ int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) {
             ovl::launch_wilson40_observe(hc, c->psi, c->psi_lo, c->psimid, c->psimid_lo, c->L, c->n_mb, amass(c->p),
                                          c->p.dt, c->p.n_modes, c->p.first_mode, c->obs_partial, c->stream);
         else if (fp32(c))
-            ovl::launch_wilson_observe<float>(hc, c->psi, c->psimid, c->L, c->n_mb, amass(c->p), c->p.dt, c->p.n_modes,
-                                              c->p.first_mode, c->obs_partial, c->stream);
+            obs_rows = ovl::launch_wilson_observe<float>(hc, c->psi, c->psimid, c->L, c->n_mb, amass(c->p), c->p.dt,
+                                                         c->p.n_modes, c->p.first_mode, c->obs_partial, c->stream);
         else
-            ovl::launch_wilson_observe<double>(hc, c->psi, c->psimid, c->L, c->n_mb, amass(c->p), c->p.dt,
-                                               c->p.n_modes, c->p.first_mode, c->obs_partial, c->stream);
+            obs_rows = ovl::launch_wilson_observe<double>(hc, c->psi, c->psimid, c->L, c->n_mb, amass(c->p), c->p.dt,
+                                                          c->p.n_modes, c->p.first_mode, c->obs_partial, c->stream);
     }
     if ((rc = launched(c, 1, "wilson (fused, observing)"))) return rc;
     if (move) {
@@ -1139,7 +1145,7 @@ int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) {
     if ((rc = coupled_efield(c))) return rc;
     {
         ProfScope ps(c, OVL_PROF_OBS);
-        ovl::launch_obs_finish(c->obs_partial, ovl::obs_partial_doubles(c->L, c->n_mb) / 3, c->obs_scratch,
+        ovl::launch_obs_finish(c->obs_partial, obs_rows, c->obs_scratch,
                                1.0 / (2.0 * c->L.V), c->dev_small + 32, c->stream);
     }
     if ((rc = launched(c, 2, "charges (observing step)"))) return rc;
@@ -1520,7 +1526,7 @@ int ovl_tuning(const ovl_ctx *c, int *variant, int *mode_group) {
     return OVL_OK;
 }
 
-int ovl_autotune(ovl_ctx *c, int *variant, double ms[3]) {
+int ovl_autotune(ovl_ctx *c, int *variant, double ms[OVL_HOP_VARIANTS]) {
     if (!c) return OVL_E_ARG;
     if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_autotune: one three-colour kernel, nothing to tune");
     int rc = set_device(c);

@@ -20,13 +20,16 @@ void launch_wilson(const double *links, const double *u1, const void *src, void 
                    int n_mb, double amass, double dt, bool accumulate, cudaStream_t stream);
 // Link sources and kernel variant of the leapfrog half step (chosen by the
 // autotuner, see ovl_autotune): U/u1 FP64 links and phases; U32/u1_32 their FP32
-// copies (used by the FP32 path when set); variant 0, 1 or 2.
+// copies (used by the FP32 path when set); variant 0..3.  Variant 3 (FP32
+// with the FP32 link copy only) is the packed-pair kernel: two modes per
+// thread on the paired FP32 instructions; FP64 runs variant 0 in its place.
 struct HopConfig {
     const double *U = nullptr, *u1 = nullptr;
     const float *U32 = nullptr, *u1_32 = nullptr;
     int variant = 0;
 };
-constexpr int kHopVariants = 3;
+constexpr int kHopVariants = 4;
+constexpr int kPackedVariant = 3;
 template <typename T>
 void launch_wilson_tuned(const HopConfig &hc, const void *src, void *dst, const Lattice &L, int mb_first, int n_mb,
                          double amass, double dt, bool accumulate, cudaStream_t stream);
@@ -36,11 +39,13 @@ void launch_links_to_f32(const double *U, float *U32, size_t n, cudaStream_t str
 // psi^+ i g0 g5 psi summed over modes and sites, Currents.cpp:44-92) on the way:
 // 3 doubles per CTA into `partial` (obs_partial_doubles), reduced by
 // launch_obs_finish into out3 (scaled by 1/2V).  FP32/FP64 modes (variant 0
-// stencil) or FP40 (src_lo / dst_lo set).
+// stencil, or the packed kernel for FP32 when hc.variant is kPackedVariant) or
+// FP40 (src_lo / dst_lo set).  partial holds obs_partial_doubles; the launch
+// returns the rows it wrote.
 size_t obs_partial_doubles(const Lattice &L, int n_mb);
 template <typename T>
-void launch_wilson_observe(const HopConfig &hc, const void *src, void *dst, const Lattice &L, int n_mb, double amass,
-                           double dt, int n_modes, int first_mode, double *partial, cudaStream_t stream);
+size_t launch_wilson_observe(const HopConfig &hc, const void *src, void *dst, const Lattice &L, int n_mb, double amass,
+                             double dt, int n_modes, int first_mode, double *partial, cudaStream_t stream);
 void launch_wilson40_observe(const HopConfig &hc, const void *src, const void *src_lo, void *dst, void *dst_lo,
                              const Lattice &L, int n_mb, double amass, double dt, int n_modes, int first_mode,
                              double *partial, cudaStream_t stream);

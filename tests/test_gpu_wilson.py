@@ -210,12 +210,14 @@ def test_errors_leave_the_context_usable():
         assert np.isfinite(ctx.charges()["NV"])
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
-@pytest.mark.parametrize("precision,form", [("fp64", "fused"), ("fp32", "fused"), ("fp64", "plain")])
+@pytest.mark.parametrize("variant,precision,form",
+                         [(v, p, f) for v in (0, 1, 2) for p, f in (("fp64", "fused"), ("fp32", "fused"), ("fp64", "plain"))]
+                         + [(3, "fp32", "fused"), (3, "fp32", "plain")])
 def test_every_hop_variant_matches_the_oracle(variant, precision, form):
     """The autotuner picks among kernel variants; each must give the same
     evolution (N = (4, 6, 5): an odd z extent exercises the partial z chunk of
-    the z-marching variant)."""
+    the z-marching variant, and V = 120 a partial last CTA of 16 sites in the
+    packed FP32 variant 3; 33 modes a ragged last lane pair)."""
     N = (4, 6, 5)
     n = 33
     U = random_links(N, 0.7, 51)
@@ -244,7 +246,7 @@ def test_autotune_keeps_state_and_reports_each_variant():
         before = ctx.get_modes()
         v, ms = ctx.autotune()
         after = ctx.get_modes()
-        assert v in (0, 1, 2) and len(ms) == 3 and all(t > 0 for t in ms)
+        assert v in (0, 1, 2, 3) and len(ms) == 4 and all(t > 0 for t in ms)
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
 
 
@@ -325,8 +327,13 @@ def test_fp40_free_fermions_and_observables_match_fp64():
     assert np.max(np.abs(out["fp40"][3] - out["fp64"][3])) < 1e-8
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp40"])
-def test_step_observe_equals_step_then_charges(precision):
+def test_packed_variant_is_fp32_only():
+    with pytest.raises(OvlError):
+        Context(N=(4, 4, 4), precision="fp64", form="fused", m_dw=0.0, dt=0.05, hop_variant=3)
+
+
+@pytest.mark.parametrize("precision,variant", [("fp64", 0), ("fp32", 0), ("fp32", 3), ("fp40", 0)])
+def test_step_observe_equals_step_then_charges(precision, variant):
     """ovl_step_observe sums N_V, N_5, PS inside the last half step: the same
     state as ovl_step and the same charges as ovl_charges (both form the
     bilinears in FP64 from the stored modes; only the summation order differs)."""
@@ -336,7 +343,7 @@ def test_step_observe_equals_step_then_charges(precision):
     out = []
     for observe in (False, True):
         with Context(N=N, n_modes=80, first_mode=1, precision=precision, form="fused", m_fermion=0.05, m_dw=0.0,
-                     dt=0.05, t_sphaleron=1e9, hop_variant=0) as ctx:
+                     dt=0.05, t_sphaleron=1e9, hop_variant=variant) as ctx:
             ctx.set_links(random_links(N, 0.5, 3))
             ctx.set_efield(random_efield(N, 0.3, 4))
             ctx.set_u1(u1_flux(N, 2))
