@@ -279,11 +279,12 @@ def time_e2e(ctx, wl, steps, device):
     return secs, h2d, d2h, ch
 
 
-def accuracy(wl, steps, every, device):
+def accuracy(wl, steps, every, device, hop_variant=-1):
     """FP32 and FP40 modes against FP64 on the same inputs over `steps` leapfrog
     steps: for o in (N_5, N_CS) the error max_t |o(t) - o_64(t)| / max_t |o_64(t) - o_64(0)|,
     N_CS accumulated every `every` steps by the cooling-path rule
-    (CoolingMethod::GetDeltaNCs, cooling off)."""
+    (CoolingMethod::GetDeltaNCs, cooling off).  Each form runs the hop variant
+    of the timed forms (hop_variant; 3 applies to FP32, the others autotune)."""
     import numpy as np
     import torch
 
@@ -292,8 +293,9 @@ def accuracy(wl, steps, every, device):
     N = wl["N"]
     series = {}
     for prec in ("fp64", "fp32", "fp40"):
+        hv = -1 if hop_variant == 3 and prec != "fp32" else hop_variant
         ctx = Context(N=N, n_modes=wl.get("modes"), precision=prec, form="fused", m_fermion=wl["m"], r_wilson=wl["r"],
-                      m_dw=wl["mdw"], dt=wl["dt"], t_sphaleron=1e300, device=device)
+                      m_dw=wl["mdw"], dt=wl["dt"], t_sphaleron=1e300, device=device, hop_variant=hv)
         setup_gauge(ctx, wl)
         ctx.set_free_fermions()
         ctx.ncs_update()
@@ -306,7 +308,7 @@ def accuracy(wl, steps, every, device):
         ctx.close()
         series[prec] = (np.array(n5), np.array(ncs))
         torch.cuda.synchronize(device)
-    out = {"steps": (steps // every) * every, "every": every}
+    out = {"steps": (steps // every) * every, "every": every, "fp32_hop_variant": hop_variant}
     for prec in ("fp32", "fp40"):
         o = {}
         for k, name in ((0, "N5"), (1, "NCS")):
@@ -633,7 +635,7 @@ def main():
 
     acc = None
     if args.accuracy_steps > 0 and rank == 0:
-        acc = accuracy(wl, args.accuracy_steps, 50, device)
+        acc = accuracy(wl, args.accuracy_steps, 50, device, args.hop_variant)
 
     # roofline of the dominant kernel (Wilson fused half step, FP32).  Ungrouped:
     # one event pair per half-step launch, 3 elements per mode-site (read the
