@@ -279,19 +279,24 @@ def time_e2e(ctx, wl, steps, device):
     return secs, h2d, d2h, ch
 
 
-def accuracy(wl, steps, every, device, hop_variant=-1):
+def accuracy(wl, steps, every, device, hop_variant=-1, field_modes=256):
     """FP32 and FP40 modes against FP64 on the same inputs over `steps` leapfrog
-    steps: for o in (N_5, N_CS) the error max_t |o(t) - o_64(t)| / max_t |o_64(t) - o_64(0)|,
-    N_CS accumulated every `every` steps by the cooling-path rule
-    (CoolingMethod::GetDeltaNCs, cooling off).  Each form runs the hop variant
-    of the timed forms (hop_variant; 3 applies to FP32, the others autotune)."""
+    steps, sampled every `every` steps.  For each observable o (N_5, N_CS, the
+    vector charge N_V = sum jV^0, the fermion energy H_F, the gauge energy T00,
+    the Gauss-law maximum): the error max_t |o(t) - o_64(t)| absolute, relative
+    to the FP64 span max_t |o_64(t) - o_64(0)| and relative to max_t |o_64(t)|.
+    N_CS is accumulated by the cooling-path rule (CoolingMethod::GetDeltaNCs,
+    cooling off).  Fields: ||psi - psi_64|| / ||psi_64|| over the first
+    `field_modes` modes at the end.  Each form runs the hop variant of the
+    timed forms (hop_variant; 3 applies to FP32, the others autotune)."""
     import numpy as np
     import torch
 
     from overlap_b200 import Context
 
     N = wl["N"]
-    series = {}
+    names = ("N5", "NCS", "NV", "HF", "T00", "gauss_max")
+    series, fields = {}, {}
     for prec in ("fp64", "fp32", "fp40"):
         hv = -1 if hop_variant == 3 and prec != "fp32" else hop_variant
         ctx = Context(N=N, n_modes=wl.get("modes"), precision=prec, form="fused", m_fermion=wl["m"], r_wilson=wl["r"],
@@ -299,25 +304,39 @@ def accuracy(wl, steps, every, device, hop_variant=-1):
         setup_gauge(ctx, wl)
         ctx.set_free_fermions()
         ctx.ncs_update()
-        n5 = [ctx.charges()["N5"]]
-        ncs = [0.0]
+
+        def sample(ncs):
+            ch, b = ctx.charges(), ctx.bulk()
+            return (ch["N5"], ncs, ch["NV"], ctx.fermion_energy(), b["T00"], b["gauss_max"])
+
+        rows = [sample(0.0)]
         for _ in range(steps // every):
             ctx.step(every)
-            n5.append(ctx.charges()["N5"])
-            ncs.append(ctx.ncs_update()[1])
+            rows.append(sample(ctx.ncs_update()[1]))
+        nf = min(field_modes, ctx.n_modes)
+        fields[prec] = ctx.get_modes(0, nf)[0]
         ctx.close()
-        series[prec] = (np.array(n5), np.array(ncs))
+        series[prec] = np.array(rows)
         torch.cuda.synchronize(device)
     out = {"steps": (steps // every) * every, "every": every, "fp32_hop_variant": hop_variant}
+    b = series["fp64"]
+    for k, name in enumerate(names):
+        span = float(np.max(np.abs(b[:, k] - b[0, k])))
+        out[f"{name}_fp64_final"] = float(b[-1, k])
+        out[f"{name}_fp64_span"] = span
     for prec in ("fp32", "fp40"):
         o = {}
-        for k, name in ((0, "N5"), (1, "NCS")):
-            a, b = series[prec][k], series["fp64"][k]
-            span = np.max(np.abs(b - b[0]))
-            o[f"{name}_rel_err"] = float(np.max(np.abs(a - b)) / span) if span > 0 else 0.0
-            out[f"{name}_fp64_final"] = float(b[-1])
-            out[f"{name}_fp64_span"] = float(span)
+        for k, name in enumerate(names):
+            err = float(np.max(np.abs(series[prec][:, k] - b[:, k])))
+            span = out[f"{name}_fp64_span"]
+            scale = float(np.max(np.abs(b[:, k])))
+            o[f"{name}_rel_err"] = err / span if span > 0 else (0.0 if err == 0 else None)
+            o[f"{name}_abs_err"] = err
+            o[f"{name}_err_of_value"] = err / scale if scale > 0 else 0.0
+        f64 = fields["fp64"]
+        o["field_rel_err"] = float(np.linalg.norm(fields[prec] - f64) / np.linalg.norm(f64))
         out[prec] = o
+    out["field_modes"] = int(fields["fp64"].shape[0])
     return out
 
 
