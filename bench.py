@@ -340,13 +340,15 @@ def accuracy(wl, steps, every, device, hop_variant=-1, field_modes=256):
     return out
 
 
-def ensemble_leg(steps, warmup, device):
+def ensemble_leg(steps, warmup, device, tile=0):
     """The batched-ensemble configuration: 64 independent SU(2) trajectories,
     16 each at N = 8, 10, 12, 16, 4096 Z2 stochastic vacuum modes each, U(1)
     flux n_B in {0, 2, 4, 8}, dt = 0.05, FP32 modes, seeded random links
     (sigma 0.3) and E (sigma 0.1).  Times `steps` leapfrog steps of the
     ensemble (one CUDA graph per step) against the same members stepped one
-    context at a time."""
+    context at a time, with the same arithmetic: tile 16 (packed-pair tiles)
+    against hop variant 3, tile 0 (the ensemble tunes its tiles) against
+    variant 0."""
     import numpy as np
     import torch
 
@@ -355,10 +357,13 @@ def ensemble_leg(steps, warmup, device):
 
     sizes = [8] * 16 + [10] * 16 + [12] * 16 + [16] * 16
     params = [Params(N=(n, n, n), n_modes=4096, precision="fp32", form="fused", m_fermion=0.05, r_wilson=1.0,
-                     m_dw=0.0, dt=0.05, t_sphaleron=1e300, device=device) for n in sizes]
+                     m_dw=0.0, dt=0.05, t_sphaleron=1e300, device=device, hop_variant=3 if tile == 16 else 0)
+              for n in sizes]
     work = sum(p.n_modes * n ** 3 for p, n in zip(params, sizes))  # mode-sites per step
     ens = Ensemble(params)
     try:
+        if tile:
+            ens.set_tile(tile)
         for i, n in enumerate(sizes):
             N = (n, n, n)
             ens[i].set_links(random_links(N, 0.3, 1000 + i))
@@ -398,7 +403,7 @@ def ensemble_leg(steps, warmup, device):
             "N5_finite": bool(np.all(np.isfinite(n5)))}
 
 
-def serving_leg(count, device):
+def serving_leg(count, device, tile=0):
     """The serving configuration: Poisson arrivals (mean 20/s) of trajectory
     requests, N uniform over {8, 12, 16, 24}, 4096-8192 modes, 200-2000 steps,
     U(1) flux n_B in {0, 2, 4, 8}, FP32 modes; a quarter SU(3), an eighth
@@ -407,12 +412,13 @@ def serving_leg(count, device):
     stochastic modes.  Admitted by device memory: Wilson requests (SU(2) and
     SU(3)) into one continuously batched ensemble, overlap requests as contexts
     of their own beside it; N_5, N_CS and energy streamed every 50 steps.  A fixed number of
-    requests (time-boxed: the offered load exceeds the GPU's capacity)."""
+    requests (time-boxed: the offered load exceeds the GPU's capacity).  tile: the
+    ensemble's tile shape (16: packed-pair tiles; 0: tuned)."""
     from overlap_b200.serve import Server, poisson_requests
 
     reqs = poisson_requests(count, 20.0, seed=7, su3_fraction=0.25, overlap_fraction=0.125)
     offered = sum(r.mode_sites() * r.steps for r in reqs) / max(reqs[-1].arrival, 1e-9)
-    srv = Server(precision="fp32", device=device, tick_steps=50)
+    srv = Server(precision="fp32", device=device, tick_steps=50, tile=tile)
     try:
         m = srv.serve(reqs)
         streamed = sum(len(r.observables) for r in srv.done)
@@ -642,11 +648,11 @@ def main():
 
     ens = None
     if not args.no_ensemble:
-        ens = ensemble_leg(max(3, min(K, 20)), 2, device)
+        ens = ensemble_leg(max(3, min(K, 20)), 2, device, tile=16 if args.hop_variant == 3 else 0)
 
     srv = None
     if not args.no_serving:
-        srv = serving_leg(args.serving_requests, device)
+        srv = serving_leg(args.serving_requests, device, tile=16 if args.hop_variant == 3 else 0)
 
     su3 = None
     if not args.no_su3:

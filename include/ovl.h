@@ -379,10 +379,19 @@ int ovl_ensemble_create(const ovl_params *members, int count, ovl_ensemble **out
 int ovl_ensemble_destroy(ovl_ensemble *ens);
 const char *ovl_ensemble_last_error(const ovl_ensemble *ens);
 int ovl_ensemble_member(ovl_ensemble *ens, int index, ovl_ctx **ctx);
-/* nsteps leapfrog steps of every member.  The first call times tiles of 4 and
- * 8 sites (x 32 modes) of the batched hop on the members' operator buffers and
- * keeps the faster. */
+/* nsteps leapfrog steps of every member.  Unless a tile shape was set
+ * (ovl_ensemble_set_tile), the first call times the tile shapes of the batched
+ * hop on the members' operator buffers and keeps the fastest. */
 int ovl_ensemble_step(ovl_ensemble *ens, int nsteps);
+/* Tile shape of the batched hop: 0 = time them on the next step (the
+ * default); 8 or 4 = that many sites x 32 modes per CTA, a warp per site;
+ * 16 = packed-pair tiles of 16 sites x 128 modes for FP32 two-colour members
+ * (the kernel body of hop variant 3: two modes per thread on the paired FP32
+ * instructions; the other members use tiles of 8).  The packed tiles lose a
+ * short timing to the 8-site tiles but draw less power per mode-site, which
+ * wins sustained runs under the power cap. */
+#define OVL_ENSEMBLE_TILES 3
+int ovl_ensemble_set_tile(ovl_ensemble *ens, int sites);
 /* Continuous batching: add a member (created on the ensemble's device and
  * stream, same precision; *index = its position) or remove member `index`
  * (its context is destroyed; later members move down by one).  Either makes
@@ -392,9 +401,10 @@ int ovl_ensemble_remove(ovl_ensemble *ens, int index);
 int ovl_ensemble_size(const ovl_ensemble *ens);
 /* ovl_charges of every member: out[4 i + k]. */
 int ovl_ensemble_charges(ovl_ensemble *ens, double *out);
-/* Sites per tile chosen (0 before the first step), the tuning times (ms, for
- * 8 and 4 sites) and the kernels launched. */
-int ovl_ensemble_info(const ovl_ensemble *ens, int *sites, double tile_ms[2], uint64_t *launches);
+/* Tile shape in use (0 before the first step), the tuning times (ms, for 8,
+ * 4 and 16 (packed, FP32 only) sites; 0 where not timed) and the kernels
+ * launched. */
+int ovl_ensemble_info(const ovl_ensemble *ens, int *sites, double tile_ms[OVL_ENSEMBLE_TILES], uint64_t *launches);
 int ovl_ensemble_synchronize(ovl_ensemble *ens);
 /* The ensemble's CUDA stream (cudaStream_t as an integer). */
 uint64_t ovl_ensemble_stream(const ovl_ensemble *ens);

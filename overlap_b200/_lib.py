@@ -20,6 +20,7 @@ STATUS_NAMES = {
 
 ABI_VERSION = 6  # OVL_ABI_VERSION of include/ovl.h
 HOP_VARIANTS = 4  # OVL_HOP_VARIANTS
+ENSEMBLE_TILES = 3  # OVL_ENSEMBLE_TILES: 8, 4 and 16 (packed) sites
 
 
 class ovl_params(C.Structure):
@@ -72,6 +73,7 @@ SIGNATURES = {
     "ovl_ensemble_remove": ([_ctx, C.c_int], C.c_int),
     "ovl_ensemble_size": ([_ctx], C.c_int),
     "ovl_ensemble_step": ([_ctx, C.c_int], C.c_int),
+    "ovl_ensemble_set_tile": ([_ctx, C.c_int], C.c_int),
     "ovl_ensemble_charges": ([_ctx, _dp], C.c_int),
     "ovl_ensemble_info": ([_ctx, C.POINTER(C.c_int), _dp, C.POINTER(C.c_uint64)], C.c_int),
     "ovl_ensemble_synchronize": ([_ctx], C.c_int),

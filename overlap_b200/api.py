@@ -459,11 +459,17 @@ class Ensemble:
         self._check(self._L.ovl_ensemble_charges(self._e, _dp(o)))
         return o
 
+    def set_tile(self, sites: int):
+        """Tile shape of the batched hop: 0 tune on the next step, 8 or 4 sites per
+        CTA, 16 packed-pair tiles (FP32 two-colour members)."""
+        self._check(self._L.ovl_ensemble_set_tile(self._e, int(sites)))
+
     def info(self) -> dict:
         sites, launches = C.c_int(0), C.c_uint64(0)
-        ms = np.zeros(2)
+        ms = np.zeros(_lib.ENSEMBLE_TILES)
         self._check(self._L.ovl_ensemble_info(self._e, C.byref(sites), _dp(ms), C.byref(launches)))
-        return {"sites": sites.value, "tile_ms": {8: float(ms[0]), 4: float(ms[1])}, "launches": launches.value}
+        return {"sites": sites.value, "tile_ms": {8: float(ms[0]), 4: float(ms[1]), 16: float(ms[2])},
+                "launches": launches.value}
 
     def synchronize(self):
         self._check(self._L.ovl_ensemble_synchronize(self._e))

@@ -13,6 +13,7 @@
 // host decisions.
 #include "ovl_fp40.cuh"
 #include "ovl_internal.h"
+#include "ovl_packed.cuh"
 #include "ovl_stencil.cuh"
 #include "ovl_su3.cuh"
 
@@ -53,9 +54,11 @@ __global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlo
     const BatchMember &m = g.m[lo];
     const Lattice L{m.N0, m.N1, m.N2, m.V};
     const int nsb = (L.V + SITES - 1) / SITES;
-    const long long local = key - m.tile0;
-    const int mb = (int)(local / nsb);
-    const int site = (int)(local % nsb) * SITES + threadIdx.y;
+    // a member's tiles number below 2^31: two fields of 32 B per mode-site and colour
+    // in 180 GB hold at most ~1.4e9 mode-sites, ~1.1e7 tiles of 4 sites x 32 modes
+    const int local = (int)(key - m.tile0);
+    const int mb = local / nsb;
+    const int site = (local - mb * nsb) * SITES + threadIdx.y;
     if (site >= L.V) return;
     const int lane = threadIdx.x;
     const cpx<T> *src = reinterpret_cast<const cpx<T> *>(phase == 0 ? m.psimid : m.psi);
@@ -82,6 +85,35 @@ __global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlo
         }
 }
 
+// FP32 two-colour members in packed-pair tiles: a CTA covers 16 sites x
+// kPkBlocks mode blocks of one member with the arithmetic of hop variant 3
+// (packed_tile: two modes per thread on the paired FP32 instructions, the
+// tile's links built once in shared memory).
+template <bool U1>
+__global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2)
+    wilson_batch_packed_kernel(const __grid_constant__ BatchGroup g, int phase) {
+    __shared__ float4 rec[kPkSites][6][kPkRecVec];
+    const long long key = (long long)blockIdx.x + g.m[0].tile0;
+    int lo = 0, hi = g.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (g.m[mid].tile0 <= key) lo = mid;
+        else hi = mid - 1;
+    }
+    const BatchMember &m = g.m[lo];
+    const Lattice L{m.N0, m.N1, m.N2, m.V};
+    const int nst = (L.V + kPkSites - 1) / kPkSites;
+    const int local = (int)(key - m.tile0);  // below 2^31 (see wilson_batch_param_kernel)
+    const int mbt = local / nst;
+    const int mb0 = mbt * kPkBlocks;
+    const float4 *src = reinterpret_cast<const float4 *>(phase == 0 ? m.psimid : m.psi);
+    float4 *dst = reinterpret_cast<float4 *>(phase == 0 ? m.psi : m.psimid);
+    double o[kObsVals] = {0.0, 0.0, 0.0};  // not observing
+    packed_tile<1, U1, false>(rec, reinterpret_cast<const float4 *>(m.U32), reinterpret_cast<const float2 *>(m.u1_32),
+                              src, dst, L, (local - mbt * nst) * kPkSites, mb0, min(m.n_mb, mb0 + kPkBlocks),
+                              (float)m.amass, (float)(0.5 * m.dt), 0, 0, o);
+}
+
 // Three-colour members (SU(3) links, 12-component modes), one group per U(1)
 // setting; descriptors by value as above.  FP32 modes read the padded FP32
 // link copy, FP64 modes the FP64 links.
@@ -98,9 +130,11 @@ __global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlo
     const BatchMember &m = g.m[lo];
     const Lattice L{m.N0, m.N1, m.N2, m.V};
     const int nsb = (L.V + SITES - 1) / SITES;
-    const long long local = key - m.tile0;
-    const int mb = (int)(local / nsb);
-    const int site = (int)(local % nsb) * SITES + threadIdx.y;
+    // a member's tiles number below 2^31: two fields of 32 B per mode-site and colour
+    // in 180 GB hold at most ~1.4e9 mode-sites, ~1.1e7 tiles of 4 sites x 32 modes
+    const int local = (int)(key - m.tile0);
+    const int mb = local / nsb;
+    const int site = (local - mb * nsb) * SITES + threadIdx.y;
     if (site >= L.V) return;
     const int lane = threadIdx.x;
     const cpx<T> *src = reinterpret_cast<const cpx<T> *>(phase == 0 ? m.psimid : m.psi);
@@ -162,7 +196,13 @@ __global__ void advance_batch_kernel(const BatchMember *__restrict__ members, in
     if (i < count) *members[i].tsteps += 1;
 }
 
-long long batch_tiles(int V, int n_mb, int sites) { return (long long)((V + sites - 1) / sites) * n_mb; }
+long long batch_tiles(int V, int n_mb, int sites, int nc, bool fp32) {
+    if (sites == kBatchPacked) {
+        if (nc == 2 && fp32) return (long long)((V + kPkSites - 1) / kPkSites) * ((n_mb + kPkBlocks - 1) / kPkBlocks);
+        sites = 8;
+    }
+    return (long long)((V + sites - 1) / sites) * n_mb;
+}
 
 template <int SITES, bool U1>
 static void launch_hop_param(const BatchGroup &g, long long tiles, int phase, bool fp32, cudaStream_t s, int nc) {
@@ -176,9 +216,21 @@ static void launch_hop_param(const BatchGroup &g, long long tiles, int phase, bo
     else wilson_batch_param_kernel<double, SITES, U1><<<(unsigned)tiles, block, 0, s>>>(g, phase);
 }
 
+template <bool U1> static void launch_hop_packed(const BatchGroup &g, long long tiles, int phase, cudaStream_t s) {
+    wilson_batch_packed_kernel<U1><<<(unsigned)tiles, dim3(kModeBlock, kSitesPerCta), 0, s>>>(g, phase);
+}
+
 void launch_batch_hop_param(const BatchGroup &g, long long tiles, int sites, int phase, bool fp32, bool u1,
                             cudaStream_t stream, int nc) {
     if (g.count <= 0 || tiles <= 0) return;
+    if (sites == kBatchPacked) {
+        if (nc == 2 && fp32) {
+            if (u1) launch_hop_packed<true>(g, tiles, phase, stream);
+            else launch_hop_packed<false>(g, tiles, phase, stream);
+            return;
+        }
+        sites = 8;
+    }
     if (u1) {
         if (sites == 4) launch_hop_param<4, true>(g, tiles, phase, fp32, stream, nc);
         else launch_hop_param<8, true>(g, tiles, phase, fp32, stream, nc);

@@ -1596,8 +1596,8 @@ struct ovl_ensemble {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool fp32 = true;
-    int sites = 0;  // sites per tile of the batched hop; 0 until tuned
-    double tile_ms[2] = {0.0, 0.0};
+    int sites = 0;  // tile shape of the batched hop (ovl_ensemble_set_tile); 0 until tuned
+    double tile_ms[OVL_ENSEMBLE_TILES] = {0.0, 0.0, 0.0};
     std::vector<ovl::BatchMember> host;  // members in group order (colours, then U(1) background)
     ovl::BatchMember *dev = nullptr;
     int *dev_tsteps = nullptr;
@@ -1667,7 +1667,7 @@ void ens_describe(ovl_ensemble *e, int sites, bool tuning) {
         m.t_sphaleron = c->p.t_sphaleron;
         m.tile0 = tile;
         m.link0 = link;
-        tile += ovl::batch_tiles(c->L.V, c->n_mb, sites);
+        tile += ovl::batch_tiles(c->L.V, c->n_mb, sites, c->nc, e->fp32);
         link += 3LL * c->L.V;
     }
     e->tiles = tile;
@@ -1712,7 +1712,7 @@ int ens_hop(ovl_ensemble *e, int sites, int phase) {
             for (int k = 0; k < bg.count; k++) {
                 const ovl::BatchMember &m = e->host[first + c0 + k];
                 bg.m[k] = m;
-                tiles += ovl::batch_tiles(m.V, m.n_mb, sites);
+                tiles += ovl::batch_tiles(m.V, m.n_mb, sites, m.nc, e->fp32);
             }
             ovl::launch_batch_hop_param(bg, tiles, sites, phase, e->fp32, (g & 1) != 0, e->stream, g >= 2 ? 3 : 2);
             n_launch++;
@@ -1858,11 +1858,12 @@ int ens_tune(ovl_ensemble *e) {
     if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess)
         return ens_fail(e, OVL_E_CUDA, "ensemble: events");
     for (ovl_ctx *c : e->members) cudaMemsetAsync(c->aux_dst, 0, c->field_complex * c->elem_bytes, e->stream);
-    const int cand[2] = {8, 4};
+    // tile shapes in the order of tile_ms; the packed tiles only for FP32
+    const int cand[OVL_ENSEMBLE_TILES] = {8, 4, ovl::kBatchPacked};
     double best = 1e300;
     int pick = 8;
     int rc = OVL_OK;
-    for (int k = 0; k < 2 && rc == OVL_OK; k++) {
+    for (int k = 0; k < (e->fp32 ? OVL_ENSEMBLE_TILES : 2) && rc == OVL_OK; k++) {
         ens_describe(e, cand[k], true);
         if ((rc = ens_upload(e))) break;
         float total = 0.0f;
@@ -1950,10 +1951,19 @@ int ovl_ensemble_charges(ovl_ensemble *e, double *out) {
     return OVL_OK;
 }
 
-int ovl_ensemble_info(const ovl_ensemble *e, int *sites, double tile_ms[2], uint64_t *launches) {
+int ovl_ensemble_set_tile(ovl_ensemble *e, int sites) {
+    if (!e) return OVL_E_ARG;
+    if (sites != 0 && sites != 4 && sites != 8 && sites != ovl::kBatchPacked)
+        return ens_fail(e, OVL_E_ARG, "ovl_ensemble_set_tile: sites=%d (0 = tune, 4, 8 or %d)", sites, ovl::kBatchPacked);
+    e->sites = sites;
+    return OVL_OK;
+}
+
+int ovl_ensemble_info(const ovl_ensemble *e, int *sites, double tile_ms[OVL_ENSEMBLE_TILES], uint64_t *launches) {
     if (!e) return OVL_E_ARG;
     if (sites) *sites = e->sites;
-    if (tile_ms) { tile_ms[0] = e->tile_ms[0]; tile_ms[1] = e->tile_ms[1]; }
+    if (tile_ms)
+        for (int k = 0; k < OVL_ENSEMBLE_TILES; k++) tile_ms[k] = e->tile_ms[k];
     if (launches) *launches = e->launches;
     return OVL_OK;
 }

@@ -133,9 +133,9 @@ void launch_color_force40(const double *U, const double *u1, const void *hi, con
 void launch_fermion_energy40(const void *hi, const void *lo, const void *dhi, const void *dlo, const Lattice &L,
                              int n_mb, int n_modes, int first_mode, double *partial, double *out, cudaStream_t stream);
 // Ensembles (ovl_batch.cu): one descriptor per member in device memory.
-// tile0: first tile of the member in the batched hop launch (tiles of `sites`
-// sites x one mode block, member by member); link0: first link in the batched
-// link update.  tsteps: the member's step counter on the device.
+// tile0: first tile of the member in the batched hop launch (batch_tiles tiles,
+// member by member); link0: first link in the batched link update.  tsteps:
+// the member's step counter on the device.
 struct BatchMember {
     void *psi, *psimid;
     double *U;
@@ -151,7 +151,12 @@ struct BatchMember {
     double amass, dt, qs, t_sphaleron;
     long long tile0, link0;
 };
-long long batch_tiles(int V, int n_mb, int sites);
+// Tiles of a member in the batched hop: `sites` = 4 or 8 sites x one mode
+// block (a warp per site), or kBatchPacked: FP32 two-colour members in
+// packed-pair tiles of 16 sites x 4 mode blocks (hop variant 3's kernel body),
+// the other members in tiles of 8 sites.
+constexpr int kBatchPacked = 16;
+long long batch_tiles(int V, int n_mb, int sites, int nc, bool fp32);
 // Up to kParamMembers descriptors of a group passed by value (kernel
 // parameter space; 128 x 136 bytes stays inside the 32 KB parameter limit).
 constexpr int kParamMembers = 128;

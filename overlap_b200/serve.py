@@ -79,10 +79,11 @@ class Server:
     """
 
     def __init__(self, precision: str = "fp32", device: int = 0, tick_steps: int = 25,
-                 memory_bytes: int | None = None):
+                 memory_bytes: int | None = None, tile: int = 0):
         import torch
 
         self.precision = precision
+        self.tile = int(tile)  # the ensemble's tile shape (ovl_ensemble_set_tile; 0 = tuned)
         self.device = device
         self.tick_steps = int(tick_steps)
         if memory_bytes is None:
@@ -118,6 +119,8 @@ class Server:
             ctx.torch_stream = stream  # keeps the stream alive with the context
         elif self.ensemble is None:
             self.ensemble = Ensemble([p])
+            if self.tile:
+                self.ensemble.set_tile(self.tile)
             ctx = self.ensemble[0]
         else:
             ctx = self.ensemble.add(p)

@@ -31,9 +31,18 @@ def phases(N, seed):
     return np.exp(1j * np.random.default_rng(seed).uniform(-np.pi, np.pi, (N[1], N[0], 2)))
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_ensemble_members_evolve_as_alone(precision):
-    params = [Params(precision=precision, form="fused", m_dw=0.0, hop_variant=0, **kw) for kw in MEMBERS]
+def solo_variant(precision, tile):
+    """The single-context hop variant with the arithmetic of the ensemble's tiles."""
+    return 3 if tile == 16 and precision == "fp32" else 0
+
+
+@pytest.mark.parametrize("precision,tile", [("fp32", 0), ("fp64", 0), ("fp32", 16), ("fp64", 16)])
+def test_ensemble_members_evolve_as_alone(precision, tile):
+    """tile 0: the tile shape is tuned; 16: packed-pair tiles for the FP32
+    members (FP64 members fall back to tiles of 8 sites); V = 120, 216, 80 and
+    2-3 mode blocks leave partial tiles."""
+    params = [Params(precision=precision, form="fused", m_dw=0.0, hop_variant=solo_variant(precision, tile), **kw)
+              for kw in MEMBERS]
     alone = []
     for i, (p, kw) in enumerate(zip(params, MEMBERS)):
         U, E, psi0, mid0 = inputs(i, kw)
@@ -46,6 +55,8 @@ def test_ensemble_members_evolve_as_alone(precision):
             ctx.step(5)
             alone.append((ctx.get_modes(), ctx.get_links(), ctx.charges()))
     with Ensemble(params) as ens:
+        if tile:
+            ens.set_tile(tile)
         for i, kw in enumerate(MEMBERS):
             U, E, psi0, mid0 = inputs(i, kw)
             ens[i].set_links(U)
@@ -66,7 +77,16 @@ def test_ensemble_members_evolve_as_alone(precision):
             assert ens[i].step_count == 5
             for k, name in enumerate(("NV", "N5", "PS", "WA")):
                 assert abs(ch[i, k] - c[name]) <= tol * max(1.0, abs(c[name])), (i, name)
-    assert info["sites"] in (4, 8) and info["launches"] >= 25
+    assert info["sites"] == tile if tile else info["sites"] in ((4, 8, 16) if precision == "fp32" else (4, 8))
+    assert info["launches"] >= 25
+
+
+def test_ensemble_rejects_an_unknown_tile_shape():
+    with Ensemble([Params(N=(4, 4, 4), n_modes=8, form="fused", precision="fp32")]) as ens:
+        with pytest.raises(OvlError):
+            ens.set_tile(5)
+        ens.set_tile(16)
+        ens.set_tile(0)
 
 
 def test_ensemble_rejects_unsupported_members():
@@ -77,10 +97,11 @@ def test_ensemble_rejects_unsupported_members():
                   Params(N=(4, 4, 4), n_modes=8, form="fused", precision="fp64")])
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_three_colour_members_batch_beside_two_colour_ones(precision):
+@pytest.mark.parametrize("precision,tile", [("fp32", 0), ("fp64", 0), ("fp32", 16)])
+def test_three_colour_members_batch_beside_two_colour_ones(precision, tile):
     """SU(3) members (with and without a U(1) background) in the same ensemble
-    as SU(2) ones: one batched launch per group, each member as alone."""
+    as SU(2) ones: one batched launch per group, each member as alone (with
+    packed tiles the SU(2) group runs packed, the SU(3) groups 8-site tiles)."""
     from overlap_b200.inputs import random_efield_su3, random_links_su3, volume
 
     def modes3(n, N, seed):
@@ -91,7 +112,8 @@ def test_three_colour_members_batch_beside_two_colour_ones(precision):
     kws = [dict(N=(4, 4, 6), n_modes=40, m_fermion=0.1, dt=0.05, t_sphaleron=1e9, n_colours=3),
            dict(N=(4, 5, 4), n_modes=64, m_fermion=0.05, dt=0.05, t_sphaleron=1e9, n_colours=3, reunitarize=True),
            dict(N=(6, 4, 4), n_modes=33, m_fermion=0.1, dt=0.05, t_sphaleron=1e9, n_colours=2)]
-    params = [Params(precision=precision, form="fused", m_dw=0.0, hop_variant=0, **kw) for kw in kws]
+    params = [Params(precision=precision, form="fused", m_dw=0.0,
+                     hop_variant=solo_variant(precision, tile) if kw["n_colours"] == 2 else 0, **kw) for kw in kws]
 
     def setup(ctx, i, kw):
         N = kw["N"]
@@ -113,6 +135,8 @@ def test_three_colour_members_batch_beside_two_colour_ones(precision):
             ctx.step(4)
             alone.append((ctx.get_modes()[0], ctx.get_links(), ctx.charges()["N5"]))
     with Ensemble(params) as ens:
+        if tile:
+            ens.set_tile(tile)
         for i, kw in enumerate(kws):
             setup(ens[i], i, kw)
         ens.step(4)

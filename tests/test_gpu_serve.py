@@ -33,12 +33,12 @@ def serve(reqs, **kw):
         s.close()
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_request_results_are_the_same_alone_and_in_the_mix(precision):
+@pytest.mark.parametrize("precision,tile", [("fp32", 0), ("fp64", 0), ("fp32", 16)])
+def test_request_results_are_the_same_alone_and_in_the_mix(precision, tile):
     a = lambda arrival: req(0, (4, 5, 6), 64, 60, arrival, n_b=2)
-    alone, _ = serve([a(0.0)], precision=precision, tick_steps=7)
+    alone, _ = serve([a(0.0)], precision=precision, tick_steps=7, tile=tile)
     mix = [req(1, (6, 6, 6), 96, 80, 0.0), a(0.05), req(2, (5, 4, 4), 32, 40, 0.08, n_b=4)]
-    mixed, m = serve(mix, precision=precision, tick_steps=7)
+    mixed, m = serve(mix, precision=precision, tick_steps=7, tile=tile)
     assert m["requests"] == 3 and m["rejected"] == 0
     assert m["latency_p50_s"] <= m["latency_p99_s"] and m["throughput"] > 0
     ref = alone[a(0).seed]
@@ -46,7 +46,7 @@ def test_request_results_are_the_same_alone_and_in_the_mix(precision):
     assert same(mixed[a(0).seed], ref, precision)
     # one request at a time: the budget admits the next only after the previous leaves
     budget = max(request_bytes(r, precision) for r in mix)
-    serial, m2 = serve(mix, precision=precision, tick_steps=7, memory_bytes=budget)
+    serial, m2 = serve(mix, precision=precision, tick_steps=7, memory_bytes=budget, tile=tile)
     for seed, obs in mixed.items():
         assert same(serial[seed], obs, precision)
 
