@@ -238,6 +238,20 @@ template <bool F32, bool U1> struct Links3 {
 // projected colour vectors h0, h1 are formed as the spinor arrives, multiplied
 // by the link, and the lower spin components rebuilt (the projections of hop()
 // in ovl_stencil.cuh).
+// a0 h0 + a1 h1 + a2 h2 (CONJ: conj(a_k) h_k) as two chains of fused
+// multiply-adds, one per real and imaginary part (the signs of the im * im
+// terms are operand negations, no extra instructions).
+template <typename T, bool CONJ>
+__device__ __forceinline__ cpx<T> row3(const cpx<T> &a0, const cpx<T> &a1, const cpx<T> &a2, const cpx<T> (&h)[3]) {
+    const T s = CONJ ? (T)1 : (T)-1;  // sign of a.im * h.im in the real part
+    cpx<T> k;
+    k.re = fma(a0.re, h[0].re, fma(s * a0.im, h[0].im, fma(a1.re, h[1].re, fma(s * a1.im, h[1].im,
+                                                                                fma(a2.re, h[2].re, s * a2.im * h[2].im)))));
+    k.im = fma(a0.re, h[0].im, fma(-s * a0.im, h[0].re, fma(a1.re, h[1].im, fma(-s * a1.im, h[1].re,
+                                                                                 fma(a2.re, h[2].im, -s * a2.im * h[2].re)))));
+    return k;
+}
+
 template <typename T, int MU, bool FWD>
 __device__ __forceinline__ void hop3(Spinor3<T> &acc, const cpx<T> *__restrict__ f, const cmat3<T> &M) {
     cpx<T> h0[3], h1[3];
@@ -260,11 +274,11 @@ __device__ __forceinline__ void hop3(Spinor3<T> &acc, const cpx<T> *__restrict__
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         if (FWD) {
-            k0[i] = M.m[i][0] * h0[0] + M.m[i][1] * h0[1] + M.m[i][2] * h0[2];
-            k1[i] = M.m[i][0] * h1[0] + M.m[i][1] * h1[1] + M.m[i][2] * h1[2];
+            k0[i] = row3<T, false>(M.m[i][0], M.m[i][1], M.m[i][2], h0);
+            k1[i] = row3<T, false>(M.m[i][0], M.m[i][1], M.m[i][2], h1);
         } else {
-            k0[i] = cdot(M.m[0][i], h0[0]) + cdot(M.m[1][i], h0[1]) + cdot(M.m[2][i], h0[2]);
-            k1[i] = cdot(M.m[0][i], h1[0]) + cdot(M.m[1][i], h1[1]) + cdot(M.m[2][i], h1[2]);
+            k0[i] = row3<T, true>(M.m[0][i], M.m[1][i], M.m[2][i], h0);
+            k1[i] = row3<T, true>(M.m[0][i], M.m[1][i], M.m[2][i], h1);
         }
     }
 #pragma unroll
