@@ -1955,7 +1955,13 @@ int ovl_ensemble_set_tile(ovl_ensemble *e, int sites) {
     if (!e) return OVL_E_ARG;
     if (sites != 0 && sites != 4 && sites != 8 && sites != ovl::kBatchPacked)
         return ens_fail(e, OVL_E_ARG, "ovl_ensemble_set_tile: sites=%d (0 = tune, 4, 8 or %d)", sites, ovl::kBatchPacked);
-    e->sites = sites;
+    if (sites != e->sites) {
+        // the captured step launches the old tile kernels even where the
+        // descriptors come out the same (a single member starts at tile 0)
+        if (cudaSetDevice(e->device) != cudaSuccess) return ens_fail(e, OVL_E_CUDA, "ovl_ensemble_set_tile: device");
+        ens_free_graph(e);
+        e->sites = sites;
+    }
     return OVL_OK;
 }
 
