@@ -103,10 +103,23 @@ __global__ void overlap_finish_t_kernel(const cpx<T> *__restrict__ phi, const cp
     }
 }
 
+// w = D b over all modes: FP32 with hop variant 3 (and the FP32 link copy) in
+// the packed-pair kernel's plain form, otherwise cheb_wilson_kernel.
 template <typename T, class LK>
-static void cheb_run(const LK &lk, ChebyshevWork &w, const void *src, void *dst, const Lattice &L, int n_mb,
-                     const double *coeff, int K, double eps, double lambda_max, double amass, double mdw, double mf,
-                     double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches) {
+static void d_pass(const LK &lk, const HopConfig &hc, const cpx<T> *b, cpx<T> *w, const Lattice &L, int n_mb, T amass,
+                   cudaStream_t stream) {
+    if (sizeof(T) == 4 && hc.variant == kPackedVariant && hc.U32 != nullptr) {
+        launch_wilson_tuned<float>(hc, b, w, L, 0, n_mb, (double)amass, 0.0, false, stream);
+        return;
+    }
+    cheb_wilson_kernel<T, LK><<<dim3((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb), dim3(kModeBlock, kSitesPerCta), 0,
+                                stream>>>(lk, b, w, L, amass);
+}
+
+template <typename T, class LK>
+static void cheb_run(const LK &lk, const HopConfig &hc, ChebyshevWork &w, const void *src, void *dst, const Lattice &L,
+                     int n_mb, const double *coeff, int K, double eps, double lambda_max, double amass, double mdw,
+                     double mf, double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches) {
     const size_t n = (size_t)n_mb * L.V * kComp * kModeBlock;
     dim3 block(kModeBlock, kSitesPerCta);
     dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
@@ -124,7 +137,7 @@ static void cheb_run(const LK &lk, ChebyshevWork &w, const void *src, void *dst,
     cudaMemsetAsync(b[2], 0, n * sizeof(cpx<T>), stream);
     int i1 = 1, i2 = 2, io = 0;  // b_{k+1}, b_{k+2}, b_k
     for (int k = K; k >= 0; k--) {  // k = 0: y = t(X) b_1 - b_2 + c_0/2 phi (chi, scaled by lambda_max^-1/2)
-        cheb_wilson_kernel<T, LK><<<grid, block, 0, stream>>>(lk, b[i1], tmp, L, am);
+        d_pass<T>(lk, hc, b[i1], tmp, L, n_mb, am, stream);
         clenshaw_kernel<T, LK><<<grid, block, 0, stream>>>(lk, tmp, b[i1], b[i2], phi, b[io], L, am, a, beta,
                                                             (T)(k > 0 ? 2 : 1),
                                                             (T)((k > 0 ? coeff[k] : 0.5 * coeff[0]) * scale));
@@ -135,7 +148,7 @@ static void cheb_run(const LK &lk, ChebyshevWork &w, const void *src, void *dst,
         io = t;
     }
     // D chi (chi = b[i1]), then the overlap combination
-    cheb_wilson_kernel<T, LK><<<grid, block, 0, stream>>>(lk, b[i1], tmp, L, am);
+    d_pass<T>(lk, hc, b[i1], tmp, L, n_mb, am, stream);
     size_t blocks = (n + 255) / 256, cap = (size_t)sm_count * 16;
     overlap_finish_t_kernel<T><<<(int)(blocks < cap ? blocks : cap), 256, 0, stream>>>(
         phi, tmp, reinterpret_cast<cpx<T> *>(dst), n, (T)mdw, (T)mf, (T)dt, accumulate ? 1 : 0);
@@ -149,7 +162,7 @@ void chebyshev_apply(ChebyshevWork &w, const HopConfig &hc, const void *src, voi
                      double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches) {
     const int n01 = L.N0 * L.N1;
     auto go = [&](const auto &lk) {
-        cheb_run<T>(lk, w, src, dst, L, n_mb, coeff, K, eps, lambda_max, amass, mdw, mf, dt, accumulate, sm_count,
+        cheb_run<T>(lk, hc, w, src, dst, L, n_mb, coeff, K, eps, lambda_max, amass, mdw, mf, dt, accumulate, sm_count,
                     stream, launches);
     };
     if (sizeof(T) == 4 && hc.U32 != nullptr) {  // FP32 modes: the FP32 link copy

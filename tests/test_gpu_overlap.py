@@ -117,7 +117,8 @@ def test_chebyshev_sign_agrees_with_zolotarev_form():
     """Chebyshev series of x^(-1/2) (degree 200 on [0.9 lambda_min / lambda_max, 1])
     against the reference's Zolotarev form on the same links and bounds; the
     Zolotarev coefficients are accurate to ~1e-7, so the forms agree to 1e-6.
-    FP32 Chebyshev agrees with FP64 Chebyshev to 1e-5."""
+    FP32 Chebyshev agrees with FP64 Chebyshev to 1e-5, also with the D passes
+    in the packed-pair kernel (hop variant 3)."""
     N = (4, 4, 4)
     U = random_links(N, 0.5, 131)
     R, _ = ref_setup(N, 16, 0, 0.1, 1.0, 1.4, 6.0, 0.05, U, np.zeros((volume(N), 3, 3)))
@@ -128,7 +129,9 @@ def test_chebyshev_sign_agrees_with_zolotarev_form():
     outs = {}
     for name, kw in (("zolo", dict(precision="fp64")),
                      ("cheb64", dict(precision="fp64", sign_method="chebyshev", cheb_degree=200, cheb_eps=eps)),
-                     ("cheb32", dict(precision="fp32", sign_method="chebyshev", cheb_degree=200, cheb_eps=eps))):
+                     ("cheb32", dict(precision="fp32", sign_method="chebyshev", cheb_degree=200, cheb_eps=eps)),
+                     ("cheb32p", dict(precision="fp32", sign_method="chebyshev", cheb_degree=200, cheb_eps=eps,
+                                      hop_variant=3))):
         with Context(N=N, n_modes=12, fermion="overlap", m_fermion=0.1, m_dw=1.4, dt=0.05, **kw) as ctx:
             ctx.set_links(U)
             ctx.set_spectral_bounds([b])
@@ -137,6 +140,7 @@ def test_chebyshev_sign_agrees_with_zolotarev_form():
                 assert ctx.solver_stats()["not_converged"] == 0
     assert rel_err(outs["cheb64"], outs["zolo"]) < 1e-6
     assert rel_err(outs["cheb32"], outs["cheb64"]) < 1e-5
+    assert rel_err(outs["cheb32p"], outs["cheb64"]) < 1e-5
 
 
 def test_chebyshev_overlap_leapfrog_fp32_runs_and_conserves_norm():
