@@ -74,6 +74,10 @@ struct ovl_ctx {
     double ritz_last[2] = {0.0, 0.0};
     // charges summed inside the last half step (ovl_step_observe)
     double *obs_partial = nullptr, *obs_scratch = nullptr;
+    // pipelined grouped step (FP32, hop variant 3): per-group counters, ticket,
+    // error word; pipe_ran: a pipelined step was enqueued since the last check
+    int *pipe = nullptr;
+    bool pipe_ran = false;
     // per-kernel timing (ovl_profile_enable): event pairs per kind
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[OVL_PROF_KINDS];
@@ -335,9 +339,27 @@ void *lo_of(const ovl_ctx *c, const void *field) {
     return nullptr;
 }
 
+// The pipelined form of grouped_pass: FP32 with hop variant 3 and the FP32
+// link copies, when the second half step reads the first one's output.
+// (Its tickets are 32-bit: 2 x groups x 16-site tiles, below 2^31 for any
+// fields that fit in device memory; checked all the same.)
+bool pipelined(const ovl_ctx *c, const ovl::HopConfig &h1, const ovl::HopConfig &h2, const void *dst1,
+               const void *src2) {
+    const long long items = 2LL * c->n_mb * ((c->L.V + 15) / 16);  // at most, groups of one block
+    return fp32(c) && c->pipe && h1.variant == ovl::kPackedVariant && h1.U32 && h2.U32 && dst1 == src2 &&
+           items < (1LL << 31) - 1;
+}
+
 void grouped_pass(ovl_ctx *c, const ovl::HopConfig &h1, const ovl::HopConfig &h2, const void *src1, void *dst1,
-                  const void *src2, void *dst2, int group) {
+                  const void *src2, void *dst2, int group, double *obs = nullptr) {
     const int G = (group <= 0 || group >= c->n_mb) ? c->n_mb : group;
+    if (pipelined(c, h1, h2, dst1, src2)) {
+        ovl::launch_wilson_pipeline(h1, h2, src1, dst1, dst2, c->L, c->n_mb, G, amass(c->p), c->p.dt, c->pipe,
+                                    c->sm_count, c->p.n_modes, c->p.first_mode, obs, c->stream);
+        c->launches += 1;
+        c->pipe_ran = true;
+        return;
+    }
     for (int g0 = 0; g0 < c->n_mb; g0 += G) {
         const int nmb = std::min(G, c->n_mb - g0);
         if (fp40(c)) {
@@ -702,6 +724,11 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     const size_t n_link32 = c->nc == 3 ? (size_t)ovl::kSu3Link32Floats * 3 * V : n_link;  // padded records
     if (p->precision == OVL_PREC_FP32 && (rc = alloc((void **)&c->U32, sizeof(float) * n_link32, "FP32 links")))
         return bail(rc);
+    if (p->precision == OVL_PREC_FP32 && c->nc == 2 && p->fermion == OVL_FERMION_WILSON) {
+        const size_t nb = sizeof(int) * ovl::pipeline_counters(c->n_mb);
+        if ((rc = alloc((void **)&c->pipe, nb, "pipeline counters"))) return bail(rc);
+        if (cudaMemset(c->pipe, 0, nb) != cudaSuccess) return bail(fail(c, OVL_E_CUDA, "ovl_create: counters"));
+    }
     c->hop_variant = c->nc == 3 ? 0 : p->hop_variant;  // one three-colour kernel: nothing to tune
     // grouping applies to the fused two-colour Wilson form; fixed when the variant is fixed
     if (p->form != OVL_FORM_FUSED || p->fermion != OVL_FERMION_WILSON || c->nc == 3) c->mode_group = 0;
@@ -757,7 +784,7 @@ int ovl_destroy(ovl_ctx *c) {
                     c->aux_src, c->aux_dst, c->ow.r, c->ow.q, c->ow.t, c->ow.x, c->ow.p, c->ow.part, c->ow.rnorm,
                     c->ow.alpha, c->ow.active, c->ow.dz, c->u_old, c->u_mid, c->e_mid, c->u1,
                     c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w, c->U32, c->u1_32, c->U_b, c->U32_b,
-                    c->psi_lo, c->psimid_lo, c->aux_src_lo, c->aux_dst_lo, c->obs_partial, c->obs_scratch};
+                    c->psi_lo, c->psimid_lo, c->aux_src_lo, c->aux_dst_lo, c->obs_partial, c->obs_scratch, c->pipe};
     if (c->ow.host_count) cudaFreeHost(c->ow.host_count);
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -1004,7 +1031,7 @@ int coupled_efield(ovl_ctx *c) {
 // links: the half-step links are built out of place in U_b (and U32_b), the
 // step-end links are U_b advanced in place, and U/U_b swap.  Per element the
 // arithmetic is that of ovl_step's ungrouped path.
-int grouped_step(ovl_ctx *c) {
+int grouped_step(ovl_ctx *c, double *obs = nullptr) {
     const bool move = c->p.qs * (c->tsteps * c->p.dt) < c->p.t_sphaleron;  // Update.cpp:57
     const size_t nl = (size_t)12 * c->L.V;
     if (move && !c->U_b) {
@@ -1028,7 +1055,7 @@ int grouped_step(ovl_ctx *c) {
     }
     {
         ProfScope ps(c, OVL_PROF_HOP);
-        grouped_pass(c, h1, h2, c->psimid, c->psi, c->psi, c->psimid, c->mode_group);
+        grouped_pass(c, h1, h2, c->psimid, c->psi, c->psi, c->psimid, c->mode_group, obs);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "wilson (grouped)");
@@ -1041,6 +1068,22 @@ int grouped_step(ovl_ctx *c) {
         if (rc) return rc;
         std::swap(c->U, c->U_b);
         std::swap(c->U32, c->U32_b);
+    }
+    return OVL_OK;
+}
+
+// The error word of the pipelined steps enqueued since the last check (a
+// second half step that waited past its bound left its tile undone).
+int check_pipeline(ovl_ctx *c) {
+    if (!c->pipe_ran) return OVL_OK;
+    c->pipe_ran = false;
+    int *err = reinterpret_cast<int *>(c->host_small + 63);  // a slot no other read uses
+    OVL_CUDA(c, cudaMemcpyAsync(err, c->pipe + ovl::pipeline_counters(c->n_mb) - 1, sizeof(int),
+                                cudaMemcpyDeviceToHost, c->stream));
+    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (*err) {
+        cudaMemsetAsync(c->pipe + ovl::pipeline_counters(c->n_mb) - 1, 0, sizeof(int), c->stream);
+        return fail(c, OVL_E_TIMEOUT, "ovl_step: a pipelined half step timed out waiting for its first half");
     }
     return OVL_OK;
 }
@@ -1082,7 +1125,7 @@ int ovl_step(ovl_ctx *c, int nsteps) {
         c->tsteps++;
         if ((rc = coupled_efield(c))) return rc;
     }
-    return OVL_OK;
+    return check_pipeline(c);
 }
 
 int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) {
@@ -1093,7 +1136,11 @@ int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) {
     const bool fused = !overlap(c) && !su3(c) && c->p.form == OVL_FORM_FUSED;
     if (fused && c->hop_variant < 0 && (rc = autotune(c, nullptr))) return rc;
     if (fused && c->mode_group < 0 && (rc = autotune_groups(c))) return rc;
-    if (!fused || (c->mode_group > 0 && c->mode_group < c->n_mb)) {
+    const bool grouped = c->mode_group > 0 && c->mode_group < c->n_mb;
+    const ovl::HopConfig hc0 = hop_config(c);
+    // the pipelined grouped step sums the charges in its second half steps
+    const bool pipe_obs = fused && grouped && pipelined(c, hc0, hc0, c->psi, c->psi);
+    if (!fused || (grouped && !pipe_obs)) {
         // other forms: the steps, then the charges kernel
         double ch[4];
         if ((rc = ovl_step(c, nsteps)) || (rc = ovl_charges(c, ch))) return rc;
@@ -1107,6 +1154,22 @@ int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) {
             cudaGetLastError();
             return fail(c, OVL_E_OOM, "ovl_step_observe: partial sums");
         }
+    }
+    if (pipe_obs) {
+        if ((rc = grouped_step(c, c->obs_partial))) return rc;
+        c->tsteps++;
+        if ((rc = coupled_efield(c))) return rc;
+        {
+            ProfScope ps(c, OVL_PROF_OBS);
+            ovl::launch_obs_finish(c->obs_partial, ovl::pipeline_obs_rows(c->L, c->n_mb, c->mode_group),
+                                   c->obs_scratch, 1.0 / (2.0 * c->L.V), c->dev_small + 32, c->stream);
+        }
+        if ((rc = launched(c, 2, "charges (observing step)"))) return rc;
+        OVL_CUDA(c, cudaMemcpyAsync(c->host_small + 32, c->dev_small + 32, sizeof(double) * 3,
+                                    cudaMemcpyDeviceToHost, c->stream));
+        if ((rc = check_pipeline(c))) return rc;  // synchronizes the stream
+        for (int k = 0; k < 3; k++) out[k] = c->host_small[32 + k];
+        return OVL_OK;
     }
     // the last step (Update.cpp:48-79); its second half step reads psi at the
     // step's end and sums the charges on the way

@@ -51,6 +51,18 @@ void launch_wilson40_observe(const HopConfig &hc, const void *src, const void *s
                              double *partial, cudaStream_t stream);
 void launch_obs_finish(const double *partial, size_t rows, double *scratch, double scale, double *out3,
                        cudaStream_t stream);
+// The grouped fused step in one persistent launch (FP32 packed pairs, hop
+// variant 3): b += dt D a with links h1 and then c += dt D b with links h2,
+// group by group of `group` mode blocks, each group's second half step while
+// its fields are still in L2.  counters: pipeline_counters(n_mb) ints, the last
+// an error word the launch sets (and never clears) when a wait times out.
+// partial (or null): the local charges of b summed in the second half steps,
+// kObsVals per row, pipeline_obs_rows rows.
+int pipeline_counters(int n_mb);
+size_t pipeline_obs_rows(const Lattice &L, int n_mb, int group);
+void launch_wilson_pipeline(const HopConfig &h1, const HopConfig &h2, const void *a, void *b, void *c,
+                            const Lattice &L, int n_mb, int group, double amass, double dt, int *counters, int sm_count,
+                            int n_modes, int first_mode, double *partial, cudaStream_t stream);
 // Half step on 40-bit storage (uint2 high words + packed extension bytes,
 // ovl_fp40.cuh), FP64 arithmetic and FP64 links (hc.U, hc.u1); accumulate:
 // dst += dt D src, else dst (a buffer of n_mb blocks) = D src.  hc.variant:

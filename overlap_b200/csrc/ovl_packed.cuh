@@ -173,15 +173,16 @@ constexpr int kPkBlocks = 4;
 // One CTA's tile: sites [site0, site0 + 16) x mode blocks [mb0, mb1) of the
 // fields src/dst (float4 views, mode block 0 at the pointers).  MODE 0:
 // dst = D src; 1: dst += dt D src (hdt = dt / 2, the 1/2 of D folded in,
-// exact).  OBS: the local charges of src are added into o (weights +-1 by
-// the parity of first_mode + mode, 0 beyond n_modes).  Every thread of the
-// CTA calls it (it holds a barrier); rec is the CTA's shared link records.
+// exact).  OBS (and observe, uniform over the CTA): the local charges of src
+// are added into o (weights +-1 by the parity of first_mode + mode, 0 beyond
+// n_modes).  Every thread of the CTA calls it (it holds a barrier); rec is the
+// CTA's shared link records.
 template <int MODE, bool U1, bool OBS>
 __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRecVec], const float4 *__restrict__ U32,
                                             const float2 *__restrict__ u1, const float4 *__restrict__ src,
                                             float4 *__restrict__ dst, const Lattice &L, int site0, int mb0, int mb1,
                                             float amass, float hdt, int n_modes, int first_mode,
-                                            double (&o)[kObsVals]) {
+                                            double (&o)[kObsVals], bool observe = true) {
     const int t = threadIdx.y * kModeBlock + threadIdx.x;
     const int sl = 2 * threadIdx.y + (threadIdx.x >> 4), q = threadIdx.x & 15;
     const int site = site0 + sl;
@@ -209,7 +210,7 @@ __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRec
                     acc[c][a].R = pr(amass * f.x, amass * f.z);
                     acc[c][a].I = pr(amass * f.y, amass * f.w);
                 }
-            if (OBS) {
+            if (OBS && observe) {
                 const int mode = mb * kModeBlock + 2 * q;
 #pragma unroll
                 for (int j = 0; j < 2; j++) {

@@ -16,6 +16,7 @@
 // CTAs resident at one time cover a compact window of one mode block and the
 // six neighbour reads of a site come from L1/L2 rather than HBM.
 
+#include <algorithm>
 #include <type_traits>
 
 #include "ovl_fp40.cuh"
@@ -111,8 +112,9 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, HopOccupancy<T, VARI
 }
 
 // ------------------------------------------------- observing half step --
-// Per-CTA sums (warp shuffles, then the warps in a fixed order) into partial.
-__device__ __forceinline__ void cta_partial(double (&o)[kObsVals], double *__restrict__ partial) {
+// The CTA's sums of o (warp shuffles, then the warps in a fixed order) into
+// row[0..kObsVals) (thread (0, 0) writes).
+__device__ __forceinline__ void cta_sum_row(double (&o)[kObsVals], double *__restrict__ row) {
     __shared__ double sh[kSitesPerCta][kObsVals];
 #pragma unroll
     for (int k = 0; k < kObsVals; k++) {
@@ -124,13 +126,18 @@ __device__ __forceinline__ void cta_partial(double (&o)[kObsVals], double *__res
         for (int k = 0; k < kObsVals; k++) sh[threadIdx.y][k] = o[k];
     __syncthreads();
     if (threadIdx.x == 0 && threadIdx.y == 0) {
-        double *p = partial + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * kObsVals;
         for (int k = 0; k < kObsVals; k++) {
             double t = 0.0;
             for (int j = 0; j < kSitesPerCta; j++) t += sh[j][k];
-            p[k] = t;
+            row[k] = t;
         }
     }
+    __syncthreads();  // sh is reused by the CTA's next call
+}
+
+// Per-CTA sums into partial, one row per CTA of the grid.
+__device__ __forceinline__ void cta_partial(double (&o)[kObsVals], double *__restrict__ partial) {
+    cta_sum_row(o, partial + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * kObsVals);
 }
 
 // The packed-pair half step over all sites and mode blocks (packed_tile).
@@ -167,6 +174,144 @@ static void launch_packed(const HopConfig &hc, const void *src, void *dst, const
     else
         wilson_packed_kernel<MODE, false, OBS><<<grid, block, 0, stream>>>(U, nullptr, s, d, L, n_mb, a, h, n_modes,
                                                                           first_mode, partial);
+}
+
+// ---------------------------------------------- pipelined grouped step --
+// The grouped fused step (both half steps, group by group of `group` mode
+// blocks) in one persistent launch of the packed-pair tile: CTAs take tiles
+// (16 sites x the group's mode blocks, of one half step) by ticket, in the
+// order
+//   H1(0), H1(1), H2(0), H1(2), H2(1), ..., H1(n-1), H2(n-2), H2(n-1)
+// (H1: b += dt D a with links U1; H2: c += dt D b with links U2), so that a
+// group's second half step runs two phases after its first, while the group's
+// fields are still in L2: 4 instead of 6 passes over HBM per leapfrog step.
+// A tile of H2(g) waits until every tile of H1(g) is done (a counter per
+// group, released after the tile's stores); those tiles hold earlier tickets,
+// taken by running CTAs whose H1 tiles never wait, so the wait ends.  It is
+// bounded all the same: past kPipeSpin polls the CTA sets the error word and
+// leaves the tile undone, and the host reports the step as failed.
+struct PipeArgs {
+    const float4 *U1, *U2;  // FP32 links of the two half steps
+    const float2 *u1;       // U(1) phases or null
+    const float4 *a;        // H1 source
+    float4 *b, *c;          // H1 destination = H2 source; H2 destination
+    Lattice L;
+    int n_mb, group, n_groups, tiles;  // tiles per (group, half step)
+    float amass, hdt;
+    int n_modes, first_mode;
+    int *done, *ticket, *err;  // counters: done[n_groups], ticket, error word
+    double *partial;           // OBS: kObsVals per (group, tile) of H2
+};
+constexpr long long kPipeSpin = 4000000;  // polls of ~100 ns: ~0.4 s
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Ticket phase j of 2n -> (group, half step) in the order above.
+__device__ __forceinline__ void pipe_phase(int j, int n, int &g, int &h) {
+    if (j == 2 * n - 1) { g = n - 1; h = 1; }
+    else if (j == 0) { g = 0; h = 0; }
+    else if (j & 1) { g = (j + 1) / 2; h = 0; }
+    else { g = j / 2 - 1; h = 1; }
+}
+
+template <bool U1, bool OBS>
+__global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2) wilson_pipeline_kernel(const __grid_constant__ PipeArgs p) {
+    __shared__ float4 rec[kPkSites][6][kPkRecVec];
+    __shared__ int s_item, s_go;
+    const int t = threadIdx.y * kModeBlock + threadIdx.x;
+    const int total = 2 * p.n_groups * p.tiles;
+    // the next ticket is taken while the current tile runs (its latency hidden);
+    // a CTA works its tickets in increasing order, so the smallest unfinished
+    // ticket is always a running tile whose dependencies are done: no deadlock
+    int next = 0;
+    if (t == 0) next = atomicAdd(p.ticket, 1);
+    for (;;) {
+        if (t == 0) {
+            s_item = next;
+            if (next < total) next = atomicAdd(p.ticket, 1);
+        }
+        __syncthreads();
+        const int item = s_item;
+        if (item >= total) break;  // the same for every thread of the CTA
+        const int j = item / p.tiles, tile = item - j * p.tiles;
+        int g, h;
+        pipe_phase(j, p.n_groups, g, h);
+        if (t == 0) {
+            int go = 1;
+            if (h == 1) {
+                long long polls = 0;
+                while (ld_acquire(p.done + g) < p.tiles) {
+                    if (++polls > kPipeSpin || *(volatile int *)p.err) {
+                        atomicExch(p.err, 1);
+                        go = 0;
+                        break;
+                    }
+                    __nanosleep(100);
+                }
+            }
+            s_go = go;
+        }
+        __syncthreads();
+        if (s_go) {  // the same for every thread of the CTA
+            const int mb0 = g * p.group, mb1 = min(p.n_mb, mb0 + p.group);
+            double o[kObsVals] = {0.0, 0.0, 0.0};
+            // one inlined tile body for both half steps (links and fields by h)
+            packed_tile<1, U1, OBS>(rec, h ? p.U2 : p.U1, p.u1, h ? p.b : p.a, h ? p.c : p.b, p.L, tile * kPkSites, mb0,
+                                    mb1, p.amass, p.hdt, p.n_modes, p.first_mode, o, h == 1);
+            if (OBS && h == 1) cta_sum_row(o, p.partial + ((size_t)g * p.tiles + tile) * kObsVals);
+        }
+        __syncthreads();  // every thread's stores of the tile are issued
+        if (t == 0 && h == 0) {
+            __threadfence();
+            atomicAdd(p.done + g, 1);
+        }
+    }
+}
+
+int pipeline_counters(int n_mb) { return n_mb + 2; }
+
+size_t pipeline_obs_rows(const Lattice &L, int n_mb, int group) {
+    return (size_t)((n_mb + group - 1) / group) * ((L.V + kPkSites - 1) / kPkSites);
+}
+
+void launch_wilson_pipeline(const HopConfig &h1, const HopConfig &h2, const void *a, void *b, void *c,
+                            const Lattice &L, int n_mb, int group, double amass, double dt, int *counters, int sm_count,
+                            int n_modes, int first_mode, double *partial, cudaStream_t stream) {
+    PipeArgs p;
+    p.U1 = reinterpret_cast<const float4 *>(h1.U32);
+    p.U2 = reinterpret_cast<const float4 *>(h2.U32);
+    p.u1 = reinterpret_cast<const float2 *>(h1.u1_32);
+    p.a = reinterpret_cast<const float4 *>(a);
+    p.b = reinterpret_cast<float4 *>(b);
+    p.c = reinterpret_cast<float4 *>(c);
+    p.L = L;
+    p.n_mb = n_mb;
+    p.group = group;
+    p.n_groups = (n_mb + group - 1) / group;
+    p.tiles = (L.V + kPkSites - 1) / kPkSites;
+    p.amass = (float)amass;
+    p.hdt = (float)(0.5 * dt);
+    p.n_modes = n_modes;
+    p.first_mode = first_mode;
+    p.done = counters;
+    p.ticket = counters + p.n_groups;
+    p.err = counters + n_mb + 1;  // sticky: reset by the caller after it reads it
+    p.partial = partial;
+    cudaMemsetAsync(counters, 0, sizeof(int) * (p.n_groups + 1), stream);
+    const long long items = 2LL * p.n_groups * p.tiles;
+    const int grid = (int)std::min<long long>(items, 2LL * sm_count);  // 2 CTAs per SM (128 registers)
+    const dim3 block(kModeBlock, kSitesPerCta);
+    if (p.u1) {
+        if (partial) wilson_pipeline_kernel<true, true><<<grid, block, 0, stream>>>(p);
+        else wilson_pipeline_kernel<true, false><<<grid, block, 0, stream>>>(p);
+    } else {
+        if (partial) wilson_pipeline_kernel<false, true><<<grid, block, 0, stream>>>(p);
+        else wilson_pipeline_kernel<false, false><<<grid, block, 0, stream>>>(p);
+    }
 }
 
 template <typename T, class LK>

@@ -250,13 +250,15 @@ def test_autotune_keeps_state_and_reports_each_variant():
         assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp40"])
+@pytest.mark.parametrize("precision,variant", [("fp64", 0), ("fp32", 0), ("fp40", 0), ("fp32", 3)])
 @pytest.mark.parametrize("group", [1, 3])
-def test_grouped_step_equals_the_ungrouped_step(precision, group):
+def test_grouped_step_equals_the_ungrouped_step(precision, variant, group):
     """The grouped fused step (both half steps per group of mode blocks, with the
     half-step links built out of place) does the same arithmetic per element as
     the ungrouped fused step: equal fields and links bit for bit, with moving
-    links, a ragged last group and the tSphaleron gate crossed mid-run."""
+    links, a ragged last group and the tSphaleron gate crossed mid-run.  With
+    hop variant 3 the grouped step is the pipelined persistent launch (second
+    half steps waiting on their group's first), V = 120 a partial last tile."""
     N = (4, 5, 6)
     n = 7 * 32 - 5
     U = random_links(N, 0.5, 71)
@@ -266,18 +268,47 @@ def test_grouped_step_equals_the_ungrouped_step(precision, group):
     out = {}
     for g in (0, group):
         with Context(N=N, n_modes=n, first_mode=1, precision=precision, form="fused", m_fermion=0.1, m_dw=0.0,
-                     dt=0.05, t_sphaleron=0.12, hop_variant=0, mode_group=g) as ctx:
+                     dt=0.05, t_sphaleron=0.12, hop_variant=variant, mode_group=g) as ctx:
             ctx.set_links(U)
             ctx.set_efield(E)
             ctx.set_modes(psi0, mid0)
             ctx.step(4)
-            assert ctx.tuning() == (0, g)
+            assert ctx.tuning() == (variant, g)
             psi, mid = ctx.get_modes()
             out[g] = (psi, mid, ctx.get_links(), ctx.charges()["N5"])
     a, b = out[0], out[group]
     for k in range(3):
         assert np.array_equal(a[k], b[k])
     assert a[3] == b[3]
+
+
+@pytest.mark.parametrize("group", [2, 5])
+def test_pipelined_observing_step_equals_step_then_charges(group):
+    """ovl_step_observe on the pipelined grouped step (FP32, hop variant 3) sums
+    the charges in its second half steps: the same fields as the ungrouped
+    packed step and the same charges as ovl_charges after it."""
+    from overlap_b200.inputs import u1_flux
+
+    N = (4, 6, 6)
+    n = 6 * 32 + 7
+    out = []
+    for g, observe in ((0, False), (group, True)):
+        with Context(N=N, n_modes=n, first_mode=1, precision="fp32", form="fused", m_fermion=0.05, m_dw=0.0,
+                     dt=0.05, t_sphaleron=1e9, hop_variant=3, mode_group=g) as ctx:
+            ctx.set_links(random_links(N, 0.5, 3))
+            ctx.set_efield(random_efield(N, 0.3, 4))
+            ctx.set_u1(u1_flux(N, 2))
+            ctx.set_modes(random_modes(n, N, 5), random_modes(n, N, 6))
+            if observe:
+                ch = ctx.step_observe(3)
+            else:
+                ctx.step(3)
+                ch = ctx.charges()
+            out.append((ctx.get_modes()[0], ctx.get_links(), ch))
+    (p0, u0, c0), (p1, u1, c1) = out
+    assert np.array_equal(p0, p1) and np.array_equal(u0, u1)
+    for k in ("NV", "N5", "PS"):
+        assert abs(c0[k] - c1[k]) <= 1e-13 * max(1.0, abs(c0[k])), k
 
 
 def test_fp40_storage_tracks_fp64_to_its_rounding():
