@@ -177,7 +177,9 @@ constexpr int kPkBlocks = 4;
 // are added into o (weights +-1 by the parity of first_mode + mode, 0 beyond
 // n_modes).  Every thread of the CTA calls it (it holds a barrier); rec is the
 // CTA's shared link records.
-template <int MODE, bool U1, bool OBS>
+// W: warps per CTA (2 W sites); DEPTH: neighbour spinors in flight per thread
+// (2: two register buffers alternate, each refilled two hops ahead).
+template <int MODE, bool U1, bool OBS, int W = kSitesPerCta, int DEPTH = 1>
 __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRecVec], const float4 *__restrict__ U32,
                                             const float2 *__restrict__ u1, const float4 *__restrict__ src,
                                             float4 *__restrict__ dst, const Lattice &L, int site0, int mb0, int mb1,
@@ -191,7 +193,7 @@ __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRec
     auto at = [&](int mb, int s) { return (((size_t)mb * L.V + s) * kComp) * (kModeBlock / 2) + q; };
     float4 v[kComp];
     if (live) load_spinor4(src + at(mb0, site), v);
-    if (t < kPkSites * 6) {
+    if (t < 2 * W * 6) {
         const int s = site0 + t / 6;
         if (s < L.V) build_link_record<U1>(U32, u1, L, s, t % 6, rec[t / 6][t % 6]);
     }
@@ -230,24 +232,46 @@ __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRec
                 }
             }
             cpair h0[kColours], h1[kColours];
-            load_spinor4(src + at(mb, n.xp), v);
-            pproject<0, true>(v, h0, h1);
-            load_spinor4(src + at(mb, n.xm), v);
-            pmulacc<0, true>(acc, h0, h1, r[0]);
-            pproject<0, false>(v, h0, h1);
-            load_spinor4(src + at(mb, n.yp), v);
-            pmulacc<0, false>(acc, h0, h1, r[3]);
-            pproject<1, true>(v, h0, h1);
-            load_spinor4(src + at(mb, n.ym), v);
-            pmulacc<1, true>(acc, h0, h1, r[1]);
-            pproject<1, false>(v, h0, h1);
-            load_spinor4(src + at(mb, n.zp), v);
-            pmulacc<1, false>(acc, h0, h1, r[4]);
-            pproject<2, true>(v, h0, h1);
-            load_spinor4(src + at(mb, n.zm), v);
-            pmulacc<2, true>(acc, h0, h1, r[2]);
-            pproject<2, false>(v, h0, h1);
-            pmulacc<2, false>(acc, h0, h1, r[5]);
+            if (DEPTH == 1) {
+                load_spinor4(src + at(mb, n.xp), v);
+                pproject<0, true>(v, h0, h1);
+                load_spinor4(src + at(mb, n.xm), v);
+                pmulacc<0, true>(acc, h0, h1, r[0]);
+                pproject<0, false>(v, h0, h1);
+                load_spinor4(src + at(mb, n.yp), v);
+                pmulacc<0, false>(acc, h0, h1, r[3]);
+                pproject<1, true>(v, h0, h1);
+                load_spinor4(src + at(mb, n.ym), v);
+                pmulacc<1, true>(acc, h0, h1, r[1]);
+                pproject<1, false>(v, h0, h1);
+                load_spinor4(src + at(mb, n.zp), v);
+                pmulacc<1, false>(acc, h0, h1, r[4]);
+                pproject<2, true>(v, h0, h1);
+                load_spinor4(src + at(mb, n.zm), v);
+                pmulacc<2, true>(acc, h0, h1, r[2]);
+                pproject<2, false>(v, h0, h1);
+                pmulacc<2, false>(acc, h0, h1, r[5]);
+            } else {
+                float4 w[kComp];  // the second buffer: v and w alternate
+                load_spinor4(src + at(mb, n.xp), v);
+                load_spinor4(src + at(mb, n.xm), w);
+                pproject<0, true>(v, h0, h1);
+                load_spinor4(src + at(mb, n.yp), v);
+                pmulacc<0, true>(acc, h0, h1, r[0]);
+                pproject<0, false>(w, h0, h1);
+                load_spinor4(src + at(mb, n.ym), w);
+                pmulacc<0, false>(acc, h0, h1, r[3]);
+                pproject<1, true>(v, h0, h1);
+                load_spinor4(src + at(mb, n.zp), v);
+                pmulacc<1, true>(acc, h0, h1, r[1]);
+                pproject<1, false>(w, h0, h1);
+                load_spinor4(src + at(mb, n.zm), w);
+                pmulacc<1, false>(acc, h0, h1, r[4]);
+                pproject<2, true>(v, h0, h1);
+                pmulacc<2, true>(acc, h0, h1, r[2]);
+                pproject<2, false>(w, h0, h1);
+                pmulacc<2, false>(acc, h0, h1, r[5]);
+            }
             // -i gamma_0 / 2: spins 0, 1 times -i/2, spins 2, 3 times +i/2
             float4 *out = dst + at(mb, site);
 #pragma unroll

@@ -128,7 +128,7 @@ __device__ __forceinline__ void cta_sum_row(double (&o)[kObsVals], double *__res
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         for (int k = 0; k < kObsVals; k++) {
             double t = 0.0;
-            for (int j = 0; j < kSitesPerCta; j++) t += sh[j][k];
+            for (int j = 0; j < (int)blockDim.y; j++) t += sh[j][k];  // the CTA's warps (at most kSitesPerCta)
             row[k] = t;
         }
     }
@@ -140,30 +140,36 @@ __device__ __forceinline__ void cta_partial(double (&o)[kObsVals], double *__res
     cta_sum_row(o, partial + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * kObsVals);
 }
 
-// The packed-pair half step over all sites and mode blocks (packed_tile).
+// The packed-pair half step over all sites and mode blocks (packed_tile):
+// CTAs of kPkWarps warps (2 kPkWarps sites), kPkDepth neighbour spinors in
+// flight per thread, kPkMinBlocks CTAs per SM.
+constexpr int kPkWarps = 4, kPkDepth = 2, kPkMinBlocks = 3;
+constexpr int kPkCtaSites = 2 * kPkWarps;
+
 template <int MODE, bool U1, bool OBS>
-__global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2)
+__global__ void __launch_bounds__(kModeBlock *kPkWarps, kPkMinBlocks)
     wilson_packed_kernel(const float4 *__restrict__ U32, const float2 *__restrict__ u1, const float4 *__restrict__ src,
                          float4 *__restrict__ dst, Lattice L, int n_mb, float amass, float hdt, int n_modes,
                          int first_mode, double *__restrict__ partial) {
-    __shared__ float4 rec[kPkSites][6][kPkRecVec];
+    __shared__ float4 rec[kPkCtaSites][6][kPkRecVec];
     const int mb0 = blockIdx.y * kPkBlocks;
     double o[kObsVals] = {0.0, 0.0, 0.0};
-    packed_tile<MODE, U1, OBS>(rec, U32, u1, src, dst, L, blockIdx.x * kPkSites, mb0, min(n_mb, mb0 + kPkBlocks), amass,
-                               hdt, n_modes, first_mode, o);
+    packed_tile<MODE, U1, OBS, kPkWarps, kPkDepth>(rec, U32, u1, src, dst, L, blockIdx.x * kPkCtaSites, mb0,
+                                                   min(n_mb, mb0 + kPkBlocks), amass, hdt, n_modes, first_mode, o);
     if (OBS) cta_partial(o, partial);
 }
 
 
 // Rows of kObsVals partial sums the packed observing launch writes.
 size_t packed_obs_rows(const Lattice &L, int n_mb) {
-    return (size_t)((L.V + kPkSites - 1) / kPkSites) * ((n_mb + kPkBlocks - 1) / kPkBlocks);
+    return (size_t)((L.V + kPkCtaSites - 1) / kPkCtaSites) * ((n_mb + kPkBlocks - 1) / kPkBlocks);
 }
 
 template <int MODE, bool OBS>
 static void launch_packed(const HopConfig &hc, const void *src, void *dst, const Lattice &L, int n_mb, double amass,
                           double dt, int n_modes, int first_mode, double *partial, cudaStream_t stream) {
-    const dim3 block(kModeBlock, kSitesPerCta), grid((L.V + kPkSites - 1) / kPkSites, (n_mb + kPkBlocks - 1) / kPkBlocks);
+    const dim3 block(kModeBlock, kPkWarps),
+        grid((L.V + kPkCtaSites - 1) / kPkCtaSites, (n_mb + kPkBlocks - 1) / kPkBlocks);
     const float4 *U = reinterpret_cast<const float4 *>(hc.U32);
     const float4 *s = reinterpret_cast<const float4 *>(src);
     float4 *d = reinterpret_cast<float4 *>(dst);
