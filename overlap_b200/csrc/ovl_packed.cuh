@@ -160,6 +160,36 @@ __device__ __forceinline__ void pmulacc(cpair (&acc)[kColours][kSpin], const cpa
     }
 }
 
+// The local charges (local_charges) of the two modes of v, colour by colour
+// with independent partial sums: the FP64 products are exact (FP32 inputs),
+// only the order of the FP64 additions differs from local_charges.
+__device__ __forceinline__ void pair_charges(const float4 (&v)[kComp], int mode, int n_modes, int first_mode,
+                                             double (&o)[kObsVals]) {
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const double w = mode + j >= n_modes ? 0.0 : (((first_mode + mode + j) & 1) == 0 ? 1.0 : -1.0);
+        double nv[kColours], zr[kColours], zi[kColours];
+#pragma unroll
+        for (int c = 0; c < kColours; c++) {
+            double re[kSpin], im[kSpin];
+#pragma unroll
+            for (int a = 0; a < kSpin; a++) {
+                const float4 x = v[c * kSpin + a];
+                re[a] = j == 0 ? (double)x.x : (double)x.z;
+                im[a] = j == 0 ? (double)x.y : (double)x.w;
+            }
+            nv[c] = fma(re[0], re[0], im[0] * im[0]) + fma(re[1], re[1], im[1] * im[1]) +
+                    (fma(re[2], re[2], im[2] * im[2]) + fma(re[3], re[3], im[3] * im[3]));
+            // conj(f0) f2 + conj(f1) f3
+            zr[c] = fma(re[0], re[2], im[0] * im[2]) + fma(re[1], re[3], im[1] * im[3]);
+            zi[c] = fma(re[0], im[2], -im[0] * re[2]) + fma(re[1], im[3], -im[1] * re[3]);
+        }
+        o[0] += w * (nv[0] + nv[1]);
+        o[1] += w * 2.0 * (zr[0] + zr[1]);
+        o[2] += w * -2.0 * (zi[0] + zi[1]);
+    }
+}
+
 __device__ __forceinline__ void load_spinor4(const float4 *__restrict__ p, float4 (&v)[kComp]) {
 #pragma unroll
     for (int k = 0; k < kComp; k++) v[k] = __ldg(p + k * (kModeBlock / 2));
@@ -212,25 +242,9 @@ __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRec
                     acc[c][a].R = pr(amass * f.x, amass * f.z);
                     acc[c][a].I = pr(amass * f.y, amass * f.w);
                 }
-            if (OBS && observe) {
-                const int mode = mb * kModeBlock + 2 * q;
-#pragma unroll
-                for (int j = 0; j < 2; j++) {
-                    const double w = mode + j >= n_modes ? 0.0 : (((first_mode + mode + j) & 1) == 0 ? 1.0 : -1.0);
-                    cpx<double> f[kColours][kSpin];
-#pragma unroll
-                    for (int c = 0; c < kColours; c++)
-#pragma unroll
-                        for (int a = 0; a < kSpin; a++) {
-                            const float4 x = v[c * kSpin + a];
-                            f[c][a] = j == 0 ? mk<double>(x.x, x.y) : mk<double>(x.z, x.w);
-                        }
-                    double oj[kObsVals];
-                    local_charges(f, w, oj);
-#pragma unroll
-                    for (int k = 0; k < kObsVals; k++) o[k] += oj[k];
-                }
-            }
+            float4 w[kComp];  // the second buffer (DEPTH 2): the first neighbour is in flight during the sums
+            if (DEPTH == 2) load_spinor4(src + at(mb, n.xp), w);
+            if (OBS && observe) pair_charges(v, mb * kModeBlock + 2 * q, n_modes, first_mode, o);
             cpair h0[kColours], h1[kColours];
             if (DEPTH == 1) {
                 load_spinor4(src + at(mb, n.xp), v);
@@ -251,25 +265,23 @@ __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRec
                 pmulacc<2, true>(acc, h0, h1, r[2]);
                 pproject<2, false>(v, h0, h1);
                 pmulacc<2, false>(acc, h0, h1, r[5]);
-            } else {
-                float4 w[kComp];  // the second buffer: v and w alternate
-                load_spinor4(src + at(mb, n.xp), v);
-                load_spinor4(src + at(mb, n.xm), w);
-                pproject<0, true>(v, h0, h1);
-                load_spinor4(src + at(mb, n.yp), v);
+            } else {  // w holds xp (issued above), v is free once the site's own spinor is used
+                load_spinor4(src + at(mb, n.xm), v);
+                pproject<0, true>(w, h0, h1);
+                load_spinor4(src + at(mb, n.yp), w);
                 pmulacc<0, true>(acc, h0, h1, r[0]);
-                pproject<0, false>(w, h0, h1);
-                load_spinor4(src + at(mb, n.ym), w);
+                pproject<0, false>(v, h0, h1);
+                load_spinor4(src + at(mb, n.ym), v);
                 pmulacc<0, false>(acc, h0, h1, r[3]);
-                pproject<1, true>(v, h0, h1);
-                load_spinor4(src + at(mb, n.zp), v);
+                pproject<1, true>(w, h0, h1);
+                load_spinor4(src + at(mb, n.zp), w);
                 pmulacc<1, true>(acc, h0, h1, r[1]);
-                pproject<1, false>(w, h0, h1);
-                load_spinor4(src + at(mb, n.zm), w);
+                pproject<1, false>(v, h0, h1);
+                load_spinor4(src + at(mb, n.zm), v);
                 pmulacc<1, false>(acc, h0, h1, r[4]);
-                pproject<2, true>(v, h0, h1);
+                pproject<2, true>(w, h0, h1);
                 pmulacc<2, true>(acc, h0, h1, r[2]);
-                pproject<2, false>(w, h0, h1);
+                pproject<2, false>(v, h0, h1);
                 pmulacc<2, false>(acc, h0, h1, r[5]);
             }
             // -i gamma_0 / 2: spins 0, 1 times -i/2, spins 2, 3 times +i/2
