@@ -85,14 +85,17 @@ __global__ void __launch_bounds__(kModeBlock *SITES, BatchOcc<T, SITES>::kMinBlo
         }
 }
 
-// FP32 two-colour members in packed-pair tiles: a CTA covers 16 sites x
-// kPkBlocks mode blocks of one member with the arithmetic of hop variant 3
-// (packed_tile: two modes per thread on the paired FP32 instructions, the
-// tile's links built once in shared memory).
+// FP32 two-colour members in packed-pair tiles: a CTA covers kBatchPkSites
+// sites x kPkBlocks mode blocks of one member with the arithmetic and shape
+// of hop variant 3 (packed_tile: two modes per thread on the paired FP32
+// instructions, the tile's links built once in shared memory, CTAs of
+// kBatchPkWarps warps with two neighbour spinors in flight per thread).
+constexpr int kBatchPkWarps = 4, kBatchPkSites = 2 * kBatchPkWarps;
+
 template <bool U1>
-__global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2)
+__global__ void __launch_bounds__(kModeBlock *kBatchPkWarps, 3)
     wilson_batch_packed_kernel(const __grid_constant__ BatchGroup g, int phase) {
-    __shared__ float4 rec[kPkSites][6][kPkRecVec];
+    __shared__ float4 rec[kBatchPkSites][6][kPkRecVec];
     const long long key = (long long)blockIdx.x + g.m[0].tile0;
     int lo = 0, hi = g.count - 1;
     while (lo < hi) {
@@ -102,16 +105,17 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2)
     }
     const BatchMember &m = g.m[lo];
     const Lattice L{m.N0, m.N1, m.N2, m.V};
-    const int nst = (L.V + kPkSites - 1) / kPkSites;
+    const int nst = (L.V + kBatchPkSites - 1) / kBatchPkSites;
     const int local = (int)(key - m.tile0);  // below 2^31 (see wilson_batch_param_kernel)
     const int mbt = local / nst;
     const int mb0 = mbt * kPkBlocks;
     const float4 *src = reinterpret_cast<const float4 *>(phase == 0 ? m.psimid : m.psi);
     float4 *dst = reinterpret_cast<float4 *>(phase == 0 ? m.psi : m.psimid);
     double o[kObsVals] = {0.0, 0.0, 0.0};  // not observing
-    packed_tile<1, U1, false>(rec, reinterpret_cast<const float4 *>(m.U32), reinterpret_cast<const float2 *>(m.u1_32),
-                              src, dst, L, (local - mbt * nst) * kPkSites, mb0, min(m.n_mb, mb0 + kPkBlocks),
-                              (float)m.amass, (float)(0.5 * m.dt), 0, 0, o);
+    packed_tile<1, U1, false, kBatchPkWarps, 2>(rec, reinterpret_cast<const float4 *>(m.U32),
+                                                reinterpret_cast<const float2 *>(m.u1_32), src, dst, L,
+                                                (local - mbt * nst) * kBatchPkSites, mb0, min(m.n_mb, mb0 + kPkBlocks),
+                                                (float)m.amass, (float)(0.5 * m.dt), 0, 0, o);
 }
 
 // Three-colour members (SU(3) links, 12-component modes), one group per U(1)
@@ -198,7 +202,8 @@ __global__ void advance_batch_kernel(const BatchMember *__restrict__ members, in
 
 long long batch_tiles(int V, int n_mb, int sites, int nc, bool fp32) {
     if (sites == kBatchPacked) {
-        if (nc == 2 && fp32) return (long long)((V + kPkSites - 1) / kPkSites) * ((n_mb + kPkBlocks - 1) / kPkBlocks);
+        if (nc == 2 && fp32)
+            return (long long)((V + kBatchPkSites - 1) / kBatchPkSites) * ((n_mb + kPkBlocks - 1) / kPkBlocks);
         sites = 8;
     }
     return (long long)((V + sites - 1) / sites) * n_mb;
@@ -217,7 +222,7 @@ static void launch_hop_param(const BatchGroup &g, long long tiles, int phase, bo
 }
 
 template <bool U1> static void launch_hop_packed(const BatchGroup &g, long long tiles, int phase, cudaStream_t s) {
-    wilson_batch_packed_kernel<U1><<<(unsigned)tiles, dim3(kModeBlock, kSitesPerCta), 0, s>>>(g, phase);
+    wilson_batch_packed_kernel<U1><<<(unsigned)tiles, dim3(kModeBlock, kBatchPkWarps), 0, s>>>(g, phase);
 }
 
 void launch_batch_hop_param(const BatchGroup &g, long long tiles, int sites, int phase, bool fp32, bool u1,
