@@ -90,6 +90,7 @@ SIGNATURES = {
     "ovl_set_spectral_bounds": ([_ctx, _dp, C.c_int], C.c_int),
     "ovl_apply": ([_ctx, C.c_int, _dp, _dp], C.c_int),
     "ovl_autotune": ([_ctx, C.POINTER(C.c_int), _dp], C.c_int),
+    "ovl_pipeline_selftest": ([_ctx, C.POINTER(C.c_int)], C.c_int),
     "ovl_zolotarev": ([C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp], C.c_int),
     "ovl_solver_stats": ([_ctx, C.POINTER(C.c_int)], C.c_int),
     "ovl_ncsdot_noalloc": ([_vp, _vp, C.c_int, C.c_int, C.c_int, _vp, C.c_uint64], C.c_int),

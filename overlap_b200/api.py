@@ -266,6 +266,13 @@ class Context:
         """Z2-noise vacuum modes (pairs sqrt(V / pairs) (P+ eta, P- eta)) in place of plane waves."""
         self._check(self._L.ovl_set_stochastic_modes(self._ctx, int(seed) & (2**64 - 1), int(total_pairs)))
 
+    def pipeline_selftest(self) -> int:
+        """ovl_pipeline_selftest: the status a timed-out pipelined wait produces
+        (OVL_E_TIMEOUT = 4 when the detection works)."""
+        code = C.c_int(0)
+        self._check(self._L.ovl_pipeline_selftest(self._ctx, C.byref(code)))
+        return code.value
+
     def tuning(self) -> tuple[int, int]:
         """(hop variant, mode blocks per group) in use; -1 before the autotuner ran."""
         v, g = C.c_int(-1), C.c_int(-1)

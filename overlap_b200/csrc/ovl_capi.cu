@@ -1589,6 +1589,25 @@ int ovl_tuning(const ovl_ctx *c, int *variant, int *mode_group) {
     return OVL_OK;
 }
 
+int ovl_pipeline_selftest(ovl_ctx *c, int *code) {
+    if (!c || !code) return OVL_E_ARG;
+    const ovl::HopConfig h = hop_config(c);
+    if (!pipelined(c, h, h, c->aux_dst, c->aux_dst) || c->n_mb < 2)
+        return fail(c, OVL_E_UNSUPPORTED, "ovl_pipeline_selftest: needs FP32 Wilson modes, hop variant 3, 2+ mode blocks");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if ((rc = check_pipeline(c))) return rc;  // nothing pending from earlier steps
+    // groups of one block; tickets start past H1(0)'s tiles, which nobody takes
+    const int tiles = (int)(ovl::pipeline_obs_rows(c->L, 1, 1));
+    ovl::launch_wilson_pipeline(h, h, c->psimid, c->aux_dst, c->aux_src, c->L, c->n_mb, 1, amass(c->p), c->p.dt,
+                                c->pipe, c->sm_count, 0, 0, nullptr, c->stream, tiles);
+    c->launches += 2;
+    c->pipe_ran = true;
+    *code = check_pipeline(c);
+    c->err.clear();
+    return OVL_OK;
+}
+
 int ovl_autotune(ovl_ctx *c, int *variant, double ms[OVL_HOP_VARIANTS]) {
     if (!c) return OVL_E_ARG;
     if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_autotune: one three-colour kernel, nothing to tune");

@@ -57,12 +57,14 @@ void launch_obs_finish(const double *partial, size_t rows, double *scratch, doub
 // its fields are still in L2.  counters: pipeline_counters(n_mb) ints, the last
 // an error word the launch sets (and never clears) when a wait times out.
 // partial (or null): the local charges of b summed in the second half steps,
-// kObsVals per row, pipeline_obs_rows rows.
+// kObsVals per row, pipeline_obs_rows rows.  first_ticket > 0 (self-test
+// only) starts the ticket counter there, so the tiles before it are never
+// taken and the second half steps that wait on them time out.
 int pipeline_counters(int n_mb);
 size_t pipeline_obs_rows(const Lattice &L, int n_mb, int group);
 void launch_wilson_pipeline(const HopConfig &h1, const HopConfig &h2, const void *a, void *b, void *c,
                             const Lattice &L, int n_mb, int group, double amass, double dt, int *counters, int sm_count,
-                            int n_modes, int first_mode, double *partial, cudaStream_t stream);
+                            int n_modes, int first_mode, double *partial, cudaStream_t stream, int first_ticket = 0);
 // Half step on 40-bit storage (uint2 high words + packed extension bytes,
 // ovl_fp40.cuh), FP64 arithmetic and FP64 links (hc.U, hc.u1); accumulate:
 // dst += dt D src, else dst (a buffer of n_mb blocks) = D src.  hc.variant:

@@ -208,7 +208,7 @@ struct PipeArgs {
     int *done, *ticket, *err;  // counters: done[n_groups], ticket, error word
     double *partial;           // OBS: kObsVals per (group, tile) of H2
 };
-constexpr long long kPipeSpin = 4000000;  // polls of ~100 ns: ~0.4 s
+constexpr long long kPipeSpin = 1000000;  // polls of ~0.1-0.6 us: well under a second
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
     int v;
@@ -284,9 +284,11 @@ size_t pipeline_obs_rows(const Lattice &L, int n_mb, int group) {
     return (size_t)((n_mb + group - 1) / group) * ((L.V + kPkSites - 1) / kPkSites);
 }
 
+__global__ void set_int_kernel(int *p, int v) { *p = v; }
+
 void launch_wilson_pipeline(const HopConfig &h1, const HopConfig &h2, const void *a, void *b, void *c,
                             const Lattice &L, int n_mb, int group, double amass, double dt, int *counters, int sm_count,
-                            int n_modes, int first_mode, double *partial, cudaStream_t stream) {
+                            int n_modes, int first_mode, double *partial, cudaStream_t stream, int first_ticket) {
     PipeArgs p;
     p.U1 = reinterpret_cast<const float4 *>(h1.U32);
     p.U2 = reinterpret_cast<const float4 *>(h2.U32);
@@ -308,6 +310,7 @@ void launch_wilson_pipeline(const HopConfig &h1, const HopConfig &h2, const void
     p.err = counters + n_mb + 1;  // sticky: reset by the caller after it reads it
     p.partial = partial;
     cudaMemsetAsync(counters, 0, sizeof(int) * (p.n_groups + 1), stream);
+    if (first_ticket) set_int_kernel<<<1, 1, 0, stream>>>(p.ticket, first_ticket);
     const long long items = 2LL * p.n_groups * p.tiles;
     const int grid = (int)std::min<long long>(items, 2LL * sm_count);  // 2 CTAs per SM (128 registers)
     const dim3 block(kModeBlock, kSitesPerCta);

@@ -311,6 +311,24 @@ def test_pipelined_observing_step_equals_step_then_charges(group):
         assert abs(c0[k] - c1[k]) <= 1e-13 * max(1.0, abs(c0[k])), k
 
 
+def test_pipelined_wait_times_out_on_a_counter_nobody_sets():
+    """Failure detection without a GPU fault: the self-test withholds the first
+    group's first-half tiles, so the second half steps waiting on them run out
+    their bounded wait; the host reads OVL_E_TIMEOUT, the modes are untouched
+    and the context keeps working."""
+    N = (4, 4, 4)
+    with Context(N=N, n_modes=96, precision="fp32", form="fused", m_fermion=0.1, m_dw=0.0, dt=0.05,
+                 t_sphaleron=1e9, hop_variant=3, mode_group=1) as ctx:
+        ctx.set_links(random_links(N, 0.5, 91))
+        ctx.set_modes(random_modes(96, N, 92), random_modes(96, N, 93))
+        before = ctx.get_modes()
+        assert ctx.pipeline_selftest() == 4  # OVL_E_TIMEOUT
+        after = ctx.get_modes()
+        assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+        ctx.step(2)  # the pipelined step runs normally afterwards
+        assert np.isfinite(ctx.charges()["N5"])
+
+
 def test_fp40_storage_tracks_fp64_to_its_rounding():
     """40-bit storage (the top 40 bits of each FP64 real, FP64 hop arithmetic):
     the leapfrog follows the oracle to the storage rounding (2^-29 per write),
