@@ -17,6 +17,7 @@ MEMBERS = [
     dict(N=(4, 5, 6), n_modes=70, first_mode=1, m_fermion=0.1, dt=0.05, t_sphaleron=1e9),
     dict(N=(6, 6, 6), n_modes=33, first_mode=0, m_fermion=0.05, dt=0.04, t_sphaleron=0.1, reunitarize=True),
     dict(N=(5, 4, 4), n_modes=64, first_mode=2, m_fermion=0.2, dt=0.05, t_sphaleron=1e9),
+    dict(N=(5, 5, 3), n_modes=45, first_mode=0, m_fermion=0.1, dt=0.05, t_sphaleron=1e9),  # V = 75: a partial tile
 ]
 
 

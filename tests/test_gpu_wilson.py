@@ -376,6 +376,35 @@ def test_fp40_free_fermions_and_observables_match_fp64():
     assert np.max(np.abs(out["fp40"][3] - out["fp64"][3])) < 1e-8
 
 
+@pytest.mark.parametrize("form", ["fused", "plain"])
+def test_packed_variant_on_a_ragged_lattice(form):
+    """Hop variant 3 where neither the sites nor the modes fill its tiles:
+    V = 75 (a CTA of 8 sites runs past the lattice), 45 modes (the last mode
+    block 13 of 32 lanes, an odd lane pair half empty); the leapfrog against the
+    oracle, and the observing step's charges against ovl_charges."""
+    N = (5, 5, 3)
+    n = 45
+    U = random_links(N, 0.6, 61)
+    E = random_efield(N, 0.3, 62)
+    psi0 = random_modes(n, N, 63)
+    mid0 = random_modes(n, N, 64)
+    p = oracle_params(N, m=0.1, mdw=0.0, dt=0.05, t_sph=1e9)
+    opsi, omid, _, _ = oracle_leapfrog(p, U, E, psi0, mid0, 3)
+    with Context(N=N, n_modes=n, first_mode=1, precision="fp32", form=form, m_fermion=0.1, m_dw=0.0, dt=0.05,
+                 t_sphaleron=1e9, hop_variant=3) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_modes(psi0, mid0)
+        ctx.step(3)
+        psi, mid = ctx.get_modes()
+        assert rel_err(psi, opsi) < tol("fp32") and rel_err(mid, omid) < tol("fp32")
+        if form == "fused":
+            ch = ctx.step_observe(1)
+            ref = ctx.charges()
+            for k in ("NV", "N5", "PS"):
+                assert abs(ch[k] - ref[k]) <= 1e-13 * max(1.0, abs(ref[k])), k
+
+
 def test_packed_variant_is_fp32_only():
     with pytest.raises(OvlError):
         Context(N=(4, 4, 4), precision="fp64", form="fused", m_dw=0.0, dt=0.05, hop_variant=3)
