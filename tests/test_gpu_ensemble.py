@@ -82,6 +82,44 @@ def test_ensemble_members_evolve_as_alone(precision, tile):
     assert info["launches"] >= 25
 
 
+def test_tile_shape_change_between_steps():
+    """Changing the tile shape between steps (ovl_ensemble_set_tile drops the
+    captured step graph; a single member's descriptor is the same for every
+    shape) keeps the evolution right: 3 steps with 8-site tiles, then 3 with
+    packed tiles, agree with the member stepped alone with hop variant 0 and
+    then 3 to FP32 rounding, and the ensemble reports the shape set.  (Both tile
+    kernels compute the same operator, so this checks the results, not which
+    kernel ran.)"""
+    kw = dict(N=(4, 5, 6), n_modes=70, first_mode=1, m_fermion=0.1, dt=0.05, t_sphaleron=1e9)
+    U, E, psi0, mid0 = inputs(0, kw)
+    p0 = Params(precision="fp32", form="fused", m_dw=0.0, hop_variant=0, **kw)
+    with Context(p0) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_modes(psi0, mid0)
+        ctx.step(3)
+        psi3, mid3 = ctx.get_modes()
+        U3, E3 = ctx.get_links(), ctx.get_efield()
+    with Context(Params(precision="fp32", form="fused", m_dw=0.0, hop_variant=3, **kw)) as ctx:
+        ctx.set_links(U3)
+        ctx.set_efield(E3)
+        ctx.set_modes(psi3, mid3)
+        ctx.step(3)
+        alone = ctx.get_modes()
+    with Ensemble([p0]) as ens:
+        ens.set_tile(8)
+        ens[0].set_links(U)
+        ens[0].set_efield(E)
+        ens[0].set_modes(psi0, mid0)
+        ens.step(3)
+        assert ens.info()["sites"] == 8
+        ens.set_tile(16)
+        ens.step(3)
+        assert ens.info()["sites"] == 16
+        got = ens[0].get_modes()
+    assert rel_err(got[0], alone[0]) < 1e-5 and rel_err(got[1], alone[1]) < 1e-5
+
+
 def test_ensemble_rejects_an_unknown_tile_shape():
     with Ensemble([Params(N=(4, 4, 4), n_modes=8, form="fused", precision="fp32")]) as ens:
         with pytest.raises(OvlError):
