@@ -394,7 +394,7 @@ int ovl_ensemble_member(ovl_ensemble *ens, int index, ovl_ctx **ctx);
 int ovl_ensemble_step(ovl_ensemble *ens, int nsteps);
 /* Tile shape of the batched hop: 0 = time them on the next step (the
  * default); 8 or 4 = that many sites x 32 modes per CTA, a warp per site;
- * 16 = packed-pair tiles (8 sites x 128 modes per CTA) for FP32 two-colour members
+ * 16 = packed-pair tiles (8 sites x 256 modes per CTA) for FP32 two-colour members
  * (the kernel body of hop variant 3: two modes per thread on the paired FP32
  * instructions; the other members use tiles of 8).  The packed tiles lose a
  * short timing to the 8-site tiles but draw less power per mode-site, which

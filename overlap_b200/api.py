@@ -468,7 +468,7 @@ class Ensemble:
 
     def set_tile(self, sites: int):
         """Tile shape of the batched hop: 0 tune on the next step, 8 or 4 sites per
-        CTA, 16 packed-pair tiles (8 sites x 128 modes per CTA; FP32 two-colour members)."""
+        CTA, 16 packed-pair tiles (8 sites x 256 modes per CTA; FP32 two-colour members)."""
         self._check(self._L.ovl_ensemble_set_tile(self._e, int(sites)))
 
     def info(self) -> dict:

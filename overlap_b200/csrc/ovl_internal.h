@@ -167,7 +167,7 @@ struct BatchMember {
 };
 // Tiles of a member in the batched hop: `sites` = 4 or 8 sites x one mode
 // block (a warp per site), or kBatchPacked: FP32 two-colour members in
-// packed-pair tiles of 8 sites x 4 mode blocks (hop variant 3's kernel body),
+// packed-pair tiles of 8 sites x 8 mode blocks (hop variant 3's kernel body),
 // the other members in tiles of 8 sites.
 constexpr int kBatchPacked = 16;
 long long batch_tiles(int V, int n_mb, int sites, int nc, bool fp32);

@@ -198,7 +198,7 @@ __device__ __forceinline__ void load_spinor4(const float4 *__restrict__ p, float
 // A CTA runs kPkBlocks mode blocks of its 16 sites one after the other on the
 // same link records; the first block's own-site spinor is in flight while the
 // records are built.
-constexpr int kPkBlocks = 4;
+constexpr int kPkBlocks = 8;
 
 // One CTA's tile: sites [site0, site0 + 16) x mode blocks [mb0, mb1) of the
 // fields src/dst (float4 views, mode block 0 at the pointers).  MODE 0:
