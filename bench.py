@@ -208,6 +208,108 @@ def reference_cpu(wl, steps: int, warmup: int, max_procs: int | None = None):
             "seconds": slowest, "wall_seconds": wall}
 
 
+# --------------------------------------------------------- oracle slice --
+# The checker for the accuracy leg: a 64-mode slice of the workload (global
+# modes 4096-4159, one MPI rank of 512) advanced by the oracle (the plain-C
+# restatement, tests' checker) on host cores while the GPU legs run, started in
+# spawned processes before any CUDA call.  Each process restores Gauss's law
+# (the reference's algorithm, restated) on the workload's fields itself.
+SLICE_FIRST, SLICE_MODES, SLICE_PROCS = 4096, 64, 4
+
+
+def _oracle_slice_worker(args):
+    wl, first, count, steps = args
+    sys.path.insert(0, str(ROOT / "tests"))
+    import ctypes as C
+
+    import numpy as np
+
+    from _oracle import oracle, orc_params, ptr
+    from overlap_b200.inputs import u1_flux
+
+    N = wl["N"]
+    V = volume(N)
+    p = orc_params(tuple(N), r=wl["r"], m=wl["m"], mdw=wl["mdw"], dt=wl["dt"])
+    U, E = gauge_fields(wl)
+    U, E = np.ascontiguousarray(U), np.ascontiguousarray(E)
+    if wl.get("init") == "quasi":
+        oracle().orc_gauss_restore(C.byref(p), ptr(U), ptr(E), 10000, 1e-14, ptr(np.zeros(2)))
+    U0, E0 = U.copy(), E.copy()
+    psi = np.zeros((count, V, 2, 4), np.complex128)
+    mid = np.zeros_like(psi)
+    oracle().orc_free_fermions(C.byref(p), first, count, ptr(psi.view(np.float64)), ptr(mid.view(np.float64)))
+    u1 = np.ascontiguousarray(u1_flux(N, wl["nb"])).view(np.float64).ravel() if wl.get("nb") else None
+    oracle().orc_set_u1(ptr(u1) if u1 is not None else None)
+    t = C.c_int(0)
+    t0 = time.perf_counter()
+    oracle().orc_wilson_leapfrog(C.byref(p), ptr(U), ptr(E), ptr(psi.view(np.float64)), ptr(mid.view(np.float64)),
+                                 count, C.byref(t), steps)
+    secs = time.perf_counter() - t0
+    cur = [np.zeros(4 * V) for _ in range(4)] + [np.zeros(V), np.zeros(V)]
+    oracle().orc_wilson_currents(C.byref(p), ptr(U), ptr(psi.view(np.float64)), count, first, *[ptr(a) for a in cur])
+    oracle().orc_set_u1(None)
+    charges = np.array([cur[0].reshape(V, 4)[:, 0].sum(), cur[1].reshape(V, 4)[:, 0].sum(), cur[4].sum()])
+    return psi, mid, U, charges, U0, E0, secs
+
+
+def oracle_slice_start(wl, steps):
+    """Starts the oracle slice (SLICE_PROCS spawned processes); returns the pool
+    and its pending result."""
+    ctx = mp.get_context("spawn")
+    pool = ctx.Pool(SLICE_PROCS)
+    per = SLICE_MODES // SLICE_PROCS
+    jobs = [(wl, SLICE_FIRST + k * per, per, steps) for k in range(SLICE_PROCS)]
+    return pool, pool.map_async(_oracle_slice_worker, jobs), steps
+
+
+def oracle_slice_compare(handle, wl, device, hop_variant):
+    """The GPU forms on the oracle's slice, same fields and steps: FP64 fused
+    and FP32 fused (hop variant `hop_variant`).  Errors: fields max |a - b| /
+    max |b|, links the same, charges N_V, N_5, PS of the slice absolute and over
+    the sum of the modes' contributions (64 x 1/2 for plane waves)."""
+    import numpy as np
+
+    from overlap_b200 import Context
+    from overlap_b200.inputs import u1_flux
+
+    pool, pending, steps = handle
+    res = pending.get()
+    pool.close()
+    pool.join()
+    psi = np.concatenate([r[0] for r in res])
+    mid = np.concatenate([r[1] for r in res])
+    oU = res[0][2]
+    och = sum(r[3] for r in res)
+    U0, E0 = res[0][4], res[0][5]
+    N = wl["N"]
+    scale = SLICE_MODES * 0.5
+    out = {"slice": f"global modes {SLICE_FIRST}-{SLICE_FIRST + SLICE_MODES - 1} (one MPI rank of 512)",
+           "steps": steps, "oracle_seconds": max(r[6] for r in res), "oracle_processes": SLICE_PROCS,
+           "oracle_charges": {"NV": och[0], "N5": och[1], "PS": och[2]}}
+    for prec, hv in (("fp64", -1), ("fp32", hop_variant if hop_variant == 3 else -1)):
+        with Context(N=N, n_modes=SLICE_MODES, first_mode=SLICE_FIRST, precision=prec, form="fused",
+                     m_fermion=wl["m"], r_wilson=wl["r"], m_dw=wl["mdw"], dt=wl["dt"], t_sphaleron=1e300,
+                     device=device, hop_variant=hv) as ctx:
+            ctx.set_links(U0)
+            ctx.set_efield(E0)
+            if wl.get("nb"):
+                ctx.set_u1(u1_flux(N, wl["nb"]))
+            ctx.set_free_fermions()
+            ctx.step(steps)
+            gp, gm = ctx.get_modes()
+            ch = ctx.charges()
+            o = {"hop_variant": ctx.tuning()[0],
+                 "field_rel_err": max(float(np.max(np.abs(gp - psi)) / np.max(np.abs(psi))),
+                                      float(np.max(np.abs(gm - mid)) / np.max(np.abs(mid)))),
+                 "links_rel_err": float(np.max(np.abs(ctx.get_links() - oU)) / np.max(np.abs(oU)))}
+            for k, name in enumerate(("NV", "N5", "PS")):
+                err = abs(ch[name] - och[k])
+                o[f"{name}_abs_err"] = err
+                o[f"{name}_err_of_mode_sum"] = err / scale
+            out[prec] = o
+    return out
+
+
 # ---------------------------------------------------------------- GPU arm --
 def time_form(wl, precision, form, steps, warmup, device, profile, hop_variant=-1, mode_group=0):
     if hop_variant == 3 and precision != "fp32":
@@ -565,6 +667,8 @@ def main():
     ap.add_argument("--modes", type=int, default=0, help="run a smaller case with this many modes (profiling)")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="FP32-vs-FP64 accuracy leg length in leapfrog steps (0 = skip)")
+    ap.add_argument("--no-oracle-slice", action="store_true",
+                    help="skip the oracle's 64-mode slice beside the accuracy leg")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     N = wl["N"]
@@ -588,10 +692,12 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            steps = max(1, min(args.steps, 20))
-            cpu = reference_cpu(wl, steps=steps, warmup=min(args.warmup, 1))
+            # the GPU arm's step and warm-up counts; a step is one leapfrog step of
+            # every process's 64-mode slice (about 0.15 s per process at N=16)
+            steps, warmup = max(1, args.steps), max(3, args.warmup)
+            cpu = reference_cpu(wl, steps=steps, warmup=warmup)
             line = {"metric": METRIC, "value": cpu["value"], "unit": METRIC, "n_gpus": args.gpus, "steps": steps,
-                    "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * cpu["seconds"] / steps,
+                    "warmup": warmup, "ms_per_step": 1e3 * cpu["seconds"] / steps,
                     "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                     "data": "synthetic", "config": config, "impl": "reference",
                     "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
@@ -604,6 +710,10 @@ def main():
         # before any CUDA call (spawned workers)
         # about 2.5 s per process: 12 steps of a 64-mode slice at N=16, 60 at N=8
         cpu = reference_cpu(wl, steps=12 if args.workload == "n16" else 60, warmup=0, max_procs=64)
+    orc_slice = None
+    if rank == 0 and args.accuracy_steps > 0 and not args.no_oracle_slice:
+        # the checker of the accuracy leg, on host cores while the GPU legs run
+        orc_slice = oracle_slice_start(wl, args.accuracy_steps)
 
     import torch
 
@@ -661,6 +771,8 @@ def main():
     acc = None
     if args.accuracy_steps > 0 and rank == 0:
         acc = accuracy(wl, args.accuracy_steps, 50, device, args.hop_variant)
+        if orc_slice is not None:
+            acc["vs_oracle_slice"] = oracle_slice_compare(orc_slice, wl, device, args.hop_variant)
 
     # roofline of the dominant kernel (Wilson fused half step, FP32).  Ungrouped:
     # one event pair per half-step launch, 3 elements per mode-site (read the
@@ -695,7 +807,10 @@ def main():
                     "d2h_bytes_per_step": d2h,
                     "path": "C ABI, host buffers: ovl_set_links + ovl_set_efield (pinned) + ovl_step_observe(1) (N_V, N_5, PS read back)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "kernel": kernel + f" ({head} fused half step)",
+                         "traffic": traffic,
+                         "traffic_source": "profiles/traffic.json: ncu DRAM bytes of a 2048-mode capture of this "
+                                           "kernel, scaled by the mode count (committed, not measured in this run)",
+                         "kernel": kernel + f" ({head} fused half step)",
                          "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": per_launch_ms,
                          "unit_of_work": unit,
                          "peak_source": peak_kind},

@@ -247,7 +247,11 @@ int ovl_solver_stats(const ovl_ctx *ctx, int out[3]);
  * (FERMIONS/WILSON/Update.cpp:48-79; overlap: FERMIONS/OVERLAP/OverlapUpdate.cpp:99-135):
  * psi += dt D(psimid); links half step while Time() < tSphaleron;
  * psimid += dt D(psi); links half step; step counter + 1.
- * Asynchronous on the context's stream (overlap: synchronises once per CG iteration). */
+ * Asynchronous on the context's stream (overlap: synchronises once per CG iteration).
+ * OVL_E_TIMEOUT (only the pipelined grouped step, FP32 hop variant 3 with
+ * mode_group > 0, waits on the device) is read once at the end of the call:
+ * the modes and the step counter are then undefined, and the caller restores
+ * them from its last saved state. */
 int ovl_step(ovl_ctx *ctx, int nsteps);
 
 /* nsteps leapfrog steps as ovl_step, returning out = {N_V, N_5, PS} of the
@@ -350,7 +354,10 @@ int ovl_device_modes(ovl_ctx *ctx, void **psi, void **psimid, size_t *bytes);
  * a fixed 8 KiB device array inside the library, so lattices above 262144
  * sites (64^3) are rejected with OVL_E_ARG.  The first call on a device looks
  * up that array's address: make it before any stream capture.  Calls share the
- * array: calls that overlap on the GPU race and must be serialised. */
+ * array: calls that overlap on the GPU race and must be serialised.  Devices
+ * with an ordinal of 64 or more give OVL_E_UNSUPPORTED; a failed launch gives
+ * OVL_E_CUDA, while a CUDA error left pending by other work is not reported
+ * (nor cleared) by this call. */
 int ovl_ncsdot_noalloc(const double *links, const double *efield, int N0, int N1, int N2, double *out,
                        uint64_t stream);
 

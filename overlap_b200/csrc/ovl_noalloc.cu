@@ -20,7 +20,12 @@
 //
 // Set-up: the first call on each device, with that device current, looks up
 // the array's device address (cudaGetSymbolAddress) and caches it.  Make that
-// first call before any stream capture begins.
+// first call before any stream capture begins.  Devices with an ordinal of 64
+// or more are not served (OVL_E_UNSUPPORTED).
+//
+// Errors: an error already pending in the runtime from other work is left in
+// place and not reported as this call's; a launch of this call that fails is
+// reported as OVL_E_CUDA and its error cleared.
 
 #include <mutex>
 
@@ -47,7 +52,8 @@ extern "C" int ovl_ncsdot_noalloc(const double *links, const double *efield, int
     const long long V = (long long)N0 * N1 * N2;
     if (V > (long long)kNoAllocPartials * 256) return OVL_E_ARG;  // beyond the scratch array
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return OVL_E_CUDA;
+    if (cudaGetDevice(&dev) != cudaSuccess) return OVL_E_CUDA;
+    if (dev < 0 || dev >= kMaxDevices) return OVL_E_UNSUPPORTED;
     double *partials = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -60,7 +66,14 @@ extern "C" int ovl_ncsdot_noalloc(const double *links, const double *efield, int
     }
     const ovl::Lattice L{N0, N1, N2, (int)V};
     const int blocks = ovl::ncsdot_blocks_exact(L);
+    // the runtime's last error before and after the launches: a change is this
+    // call's failure; an error that was already there belongs to earlier work
+    const cudaError_t before = cudaPeekAtLastError();
     ovl::launch_ncsdot_into(links, efield, L, blocks, partials, out, reinterpret_cast<cudaStream_t>(stream));
-    if (cudaGetLastError() != cudaSuccess) return OVL_E_CUDA;
+    const cudaError_t after = cudaPeekAtLastError();
+    if (after != before) {
+        cudaGetLastError();
+        return OVL_E_CUDA;
+    }
     return OVL_OK;
 }

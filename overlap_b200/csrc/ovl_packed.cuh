@@ -190,9 +190,14 @@ __device__ __forceinline__ void pair_charges(const float4 (&v)[kComp], int mode,
     }
 }
 
+// COH false: read-only data of the launch, through the non-coherent path
+// (ld.global.nc).  COH true: data that the same launch writes as well (the
+// pipelined step's fields), read with ordinary coherent loads (ld.global.ca),
+// which the memory model orders after an acquire.
+template <bool COH = false>
 __device__ __forceinline__ void load_spinor4(const float4 *__restrict__ p, float4 (&v)[kComp]) {
 #pragma unroll
-    for (int k = 0; k < kComp; k++) v[k] = __ldg(p + k * (kModeBlock / 2));
+    for (int k = 0; k < kComp; k++) v[k] = COH ? __ldca(p + k * (kModeBlock / 2)) : __ldg(p + k * (kModeBlock / 2));
 }
 
 // A CTA runs kPkBlocks mode blocks of its 16 sites one after the other on the
@@ -208,8 +213,9 @@ constexpr int kPkBlocks = 8;
 // n_modes).  Every thread of the CTA calls it (it holds a barrier); rec is the
 // CTA's shared link records.
 // W: warps per CTA (2 W sites); DEPTH: neighbour spinors in flight per thread
-// (2: two register buffers alternate, each refilled two hops ahead).
-template <int MODE, bool U1, bool OBS, int W = kSitesPerCta, int DEPTH = 1>
+// (2: two register buffers alternate, each refilled two hops ahead).  COH:
+// src is written elsewhere in the same launch (load_spinor4).
+template <int MODE, bool U1, bool OBS, int W = kSitesPerCta, int DEPTH = 1, bool COH = false>
 __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRecVec], const float4 *__restrict__ U32,
                                             const float2 *__restrict__ u1, const float4 *__restrict__ src,
                                             float4 *__restrict__ dst, const Lattice &L, int site0, int mb0, int mb1,
@@ -222,7 +228,7 @@ __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRec
     // float4 index of component 0 of (mb, s) for this thread's lane pair
     auto at = [&](int mb, int s) { return (((size_t)mb * L.V + s) * kComp) * (kModeBlock / 2) + q; };
     float4 v[kComp];
-    if (live) load_spinor4(src + at(mb0, site), v);
+    if (live) load_spinor4<COH>(src + at(mb0, site), v);
     if (t < 2 * W * 6) {
         const int s = site0 + t / 6;
         if (s < L.V) build_link_record<U1>(U32, u1, L, s, t % 6, rec[t / 6][t % 6]);
@@ -232,7 +238,7 @@ __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRec
         const Nbrs n = neighbours(L, site);
         const float4(*r)[kPkRecVec] = rec[sl];
         for (int mb = mb0; mb < mb1; mb++) {
-            if (mb > mb0) load_spinor4(src + at(mb, site), v);
+            if (mb > mb0) load_spinor4<COH>(src + at(mb, site), v);
             cpair acc[kColours][kSpin];
 #pragma unroll
             for (int c = 0; c < kColours; c++)
@@ -243,41 +249,41 @@ __device__ __forceinline__ void packed_tile(float4 (*__restrict__ rec)[6][kPkRec
                     acc[c][a].I = pr(amass * f.y, amass * f.w);
                 }
             float4 w[kComp];  // the second buffer (DEPTH 2): the first neighbour is in flight during the sums
-            if (DEPTH == 2) load_spinor4(src + at(mb, n.xp), w);
+            if (DEPTH == 2) load_spinor4<COH>(src + at(mb, n.xp), w);
             if (OBS && observe) pair_charges(v, mb * kModeBlock + 2 * q, n_modes, first_mode, o);
             cpair h0[kColours], h1[kColours];
             if (DEPTH == 1) {
-                load_spinor4(src + at(mb, n.xp), v);
+                load_spinor4<COH>(src + at(mb, n.xp), v);
                 pproject<0, true>(v, h0, h1);
-                load_spinor4(src + at(mb, n.xm), v);
+                load_spinor4<COH>(src + at(mb, n.xm), v);
                 pmulacc<0, true>(acc, h0, h1, r[0]);
                 pproject<0, false>(v, h0, h1);
-                load_spinor4(src + at(mb, n.yp), v);
+                load_spinor4<COH>(src + at(mb, n.yp), v);
                 pmulacc<0, false>(acc, h0, h1, r[3]);
                 pproject<1, true>(v, h0, h1);
-                load_spinor4(src + at(mb, n.ym), v);
+                load_spinor4<COH>(src + at(mb, n.ym), v);
                 pmulacc<1, true>(acc, h0, h1, r[1]);
                 pproject<1, false>(v, h0, h1);
-                load_spinor4(src + at(mb, n.zp), v);
+                load_spinor4<COH>(src + at(mb, n.zp), v);
                 pmulacc<1, false>(acc, h0, h1, r[4]);
                 pproject<2, true>(v, h0, h1);
-                load_spinor4(src + at(mb, n.zm), v);
+                load_spinor4<COH>(src + at(mb, n.zm), v);
                 pmulacc<2, true>(acc, h0, h1, r[2]);
                 pproject<2, false>(v, h0, h1);
                 pmulacc<2, false>(acc, h0, h1, r[5]);
             } else {  // w holds xp (issued above), v is free once the site's own spinor is used
-                load_spinor4(src + at(mb, n.xm), v);
+                load_spinor4<COH>(src + at(mb, n.xm), v);
                 pproject<0, true>(w, h0, h1);
-                load_spinor4(src + at(mb, n.yp), w);
+                load_spinor4<COH>(src + at(mb, n.yp), w);
                 pmulacc<0, true>(acc, h0, h1, r[0]);
                 pproject<0, false>(v, h0, h1);
-                load_spinor4(src + at(mb, n.ym), v);
+                load_spinor4<COH>(src + at(mb, n.ym), v);
                 pmulacc<0, false>(acc, h0, h1, r[3]);
                 pproject<1, true>(w, h0, h1);
-                load_spinor4(src + at(mb, n.zp), w);
+                load_spinor4<COH>(src + at(mb, n.zp), w);
                 pmulacc<1, true>(acc, h0, h1, r[1]);
                 pproject<1, false>(v, h0, h1);
-                load_spinor4(src + at(mb, n.zm), v);
+                load_spinor4<COH>(src + at(mb, n.zm), v);
                 pmulacc<1, false>(acc, h0, h1, r[4]);
                 pproject<2, true>(w, h0, h1);
                 pmulacc<2, true>(acc, h0, h1, r[2]);

@@ -194,8 +194,12 @@ static void launch_packed(const HopConfig &hc, const void *src, void *dst, const
 // A tile of H2(g) waits until every tile of H1(g) is done (a counter per
 // group, released after the tile's stores); those tiles hold earlier tickets,
 // taken by running CTAs whose H1 tiles never wait, so the wait ends.  It is
-// bounded all the same: past kPipeSpin polls the CTA sets the error word and
-// leaves the tile undone, and the host reports the step as failed.
+// bounded all the same: after kPipeWaitNs of elapsed time (the GPU's
+// %globaltimer) or kPipeSpin polls, whichever comes first, the CTA sets the
+// error word and leaves the tile undone, and the host reports the step as
+// failed.  Both half steps read fields the launch also writes (H1's source is
+// H2's destination, H2's source is H1's destination), so their spinor loads
+// are coherent ones (packed_tile with COH), not the read-only path.
 struct PipeArgs {
     const float4 *U1, *U2;  // FP32 links of the two half steps
     const float2 *u1;       // U(1) phases or null
@@ -208,7 +212,14 @@ struct PipeArgs {
     int *done, *ticket, *err;  // counters: done[n_groups], ticket, error word
     double *partial;           // OBS: kObsVals per (group, tile) of H2
 };
-constexpr long long kPipeSpin = 1000000;  // polls of ~0.1-0.6 us: well under a second
+constexpr long long kPipeWaitNs = 1000000000LL;  // 1 s of elapsed time
+constexpr long long kPipeSpin = 20000000;        // polls (>= 2 s with the 100 ns sleeps): a second bound
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
     int v;
@@ -250,8 +261,10 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2) wilson_pipeline_k
             int go = 1;
             if (h == 1) {
                 long long polls = 0;
+                const unsigned long long t0 = global_ns();
                 while (ld_acquire(p.done + g) < p.tiles) {
-                    if (++polls > kPipeSpin || *(volatile int *)p.err) {
+                    if (++polls > kPipeSpin || (long long)(global_ns() - t0) > kPipeWaitNs ||
+                        *(volatile int *)p.err) {
                         atomicExch(p.err, 1);
                         go = 0;
                         break;
@@ -266,8 +279,9 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2) wilson_pipeline_k
             const int mb0 = g * p.group, mb1 = min(p.n_mb, mb0 + p.group);
             double o[kObsVals] = {0.0, 0.0, 0.0};
             // one inlined tile body for both half steps (links and fields by h)
-            packed_tile<1, U1, OBS>(rec, h ? p.U2 : p.U1, p.u1, h ? p.b : p.a, h ? p.c : p.b, p.L, tile * kPkSites, mb0,
-                                    mb1, p.amass, p.hdt, p.n_modes, p.first_mode, o, h == 1);
+            packed_tile<1, U1, OBS, kSitesPerCta, 1, true>(rec, h ? p.U2 : p.U1, p.u1, h ? p.b : p.a, h ? p.c : p.b, p.L,
+                                                           tile * kPkSites, mb0, mb1, p.amass, p.hdt, p.n_modes,
+                                                           p.first_mode, o, h == 1);
             if (OBS && h == 1) cta_sum_row(o, p.partial + ((size_t)g * p.tiles + tile) * kObsVals);
         }
         __syncthreads();  // every thread's stores of the tile are issued

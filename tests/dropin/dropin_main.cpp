@@ -1,6 +1,6 @@
 // Drop-in test program: the reference's own Simulation-style build with the
-// Wilson hot path replaced by include/ovl_dropin.hpp (the GPU path), exactly
-// as INTEGRATION.md tells a maintainer to do it.  Test infrastructure: built by
+// Wilson hot path replaced by include/ovl_dropin.hpp (the GPU path), the way
+// a maintainer of the reference would include it.  Test infrastructure: built by
 // tests/dropin/Makefile where the reference tree exists, run by
 // tests/test_gpu_dropin.py, which compares its output with the reference.
 //

@@ -120,6 +120,43 @@ def test_tile_shape_change_between_steps():
     assert rel_err(got[0], alone[0]) < 1e-5 and rel_err(got[1], alone[1]) < 1e-5
 
 
+def test_packed_tiles_beyond_one_cta_row_of_mode_blocks():
+    """Packed-pair tiles run 8 mode blocks per CTA; a member of 300 modes (10
+    blocks, the last one 12 of 32 lanes) needs a second row of them (mbt > 0 in
+    wilson_batch_packed_kernel), beside a member of 70 modes, one with a U(1)
+    background: each member as alone with hop variant 3."""
+    kws = [dict(N=(4, 5, 6), n_modes=300, first_mode=1, m_fermion=0.1, dt=0.05, t_sphaleron=1e9),
+           dict(N=(4, 5, 6), n_modes=70, first_mode=0, m_fermion=0.05, dt=0.05, t_sphaleron=0.1)]
+    params = [Params(precision="fp32", form="fused", m_dw=0.0, hop_variant=3, **kw) for kw in kws]
+    alone = []
+    for i, (p, kw) in enumerate(zip(params, kws)):
+        U, E, psi0, mid0 = inputs(i, kw)
+        with Context(p) as ctx:
+            ctx.set_links(U)
+            ctx.set_efield(E)
+            if i == 0:
+                ctx.set_u1(phases(kw["N"], 8))
+            ctx.set_modes(psi0, mid0)
+            ctx.step(4)
+            alone.append((ctx.get_modes(), ctx.charges()))
+    with Ensemble(params) as ens:
+        ens.set_tile(16)
+        for i, kw in enumerate(kws):
+            U, E, psi0, mid0 = inputs(i, kw)
+            ens[i].set_links(U)
+            ens[i].set_efield(E)
+            if i == 0:
+                ens[i].set_u1(phases(kw["N"], 8))
+            ens[i].set_modes(psi0, mid0)
+        ens.step(4)
+        ch = ens.charges()
+        for i in range(len(kws)):
+            (psi, mid), c = alone[i]
+            bpsi, bmid = ens[i].get_modes()
+            assert rel_err(bpsi, psi) < 1e-5 and rel_err(bmid, mid) < 1e-5, i
+            assert abs(ch[i, 1] - c["N5"]) <= 1e-5 * max(1.0, abs(c["N5"])), i
+
+
 def test_ensemble_rejects_an_unknown_tile_shape():
     with Ensemble([Params(N=(4, 4, 4), n_modes=8, form="fused", precision="fp32")]) as ens:
         with pytest.raises(OvlError):

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from _helpers import current_scale, oracle_currents, oracle_leapfrog, oracle_params, random_modes, rel_err
-from _oracle import have_reference, ptr, reference
+from _oracle import have_reference, oracle, ptr, reference
 from overlap_b200 import Context, OvlError
 from overlap_b200.inputs import random_efield, random_links, unit_links, volume
 
@@ -403,6 +403,64 @@ def test_packed_variant_on_a_ragged_lattice(form):
             ref = ctx.charges()
             for k in ("NV", "N5", "PS"):
                 assert abs(ch[k] - ref[k]) <= 1e-13 * max(1.0, abs(ref[k])), k
+
+
+@pytest.mark.parametrize("form", ["fused", "plain"])
+def test_packed_variant_beyond_one_cta_row_of_mode_blocks(form):
+    """300 modes = 10 mode blocks, the last one 12 of 32 lanes: a CTA of the
+    packed kernel runs 8 mode blocks, so the second row of CTAs (blockIdx.y = 1)
+    holds blocks 8 and 9.  With a U(1) background, against the oracle with the
+    same phases; in the fused form the observing step's charges (one row of
+    partial sums per CTA, indexed by blockIdx.y) against ovl_charges."""
+    from overlap_b200.inputs import u1_flux
+
+    N = (4, 5, 6)
+    n = 300
+    U = random_links(N, 0.6, 31)
+    E = random_efield(N, 0.3, 32)
+    psi0 = random_modes(n, N, 33)
+    mid0 = random_modes(n, N, 34)
+    u1 = u1_flux(N, 3)
+    p = oracle_params(N, m=0.1, mdw=0.0, dt=0.05, t_sph=1e9)
+    oracle().orc_set_u1(ptr(np.ascontiguousarray(u1).view(np.float64).ravel()))
+    try:
+        opsi, omid, _, _ = oracle_leapfrog(p, U, E, psi0, mid0, 3)
+    finally:
+        oracle().orc_set_u1(None)
+    with Context(N=N, n_modes=n, first_mode=1, precision="fp32", form=form, m_fermion=0.1, m_dw=0.0, dt=0.05,
+                 t_sphaleron=1e9, hop_variant=3) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_u1(u1)
+        ctx.set_modes(psi0, mid0)
+        ctx.step(3)
+        psi, mid = ctx.get_modes()
+        assert rel_err(psi, opsi) < tol("fp32") and rel_err(mid, omid) < tol("fp32")
+        if form == "fused":
+            ch = ctx.step_observe(1)
+            ref = ctx.charges()
+            for k in ("NV", "N5", "PS"):
+                assert abs(ch[k] - ref[k]) <= 1e-13 * max(1.0, abs(ref[k])), k
+
+
+@pytest.mark.parametrize("group", [4, 9])
+def test_pipelined_step_beyond_one_cta_row_of_mode_blocks(group):
+    """The pipelined grouped step (hop variant 3) on 10 mode blocks in groups
+    of 4 (a ragged last group of 2) and of 9 (one group past a CTA row of the
+    ungrouped kernel): bit for bit the ungrouped packed step."""
+    N = (4, 5, 6)
+    n = 300
+    out = {}
+    for g in (0, group):
+        with Context(N=N, n_modes=n, first_mode=1, precision="fp32", form="fused", m_fermion=0.1, m_dw=0.0,
+                     dt=0.05, t_sphaleron=1e9, hop_variant=3, mode_group=g) as ctx:
+            ctx.set_links(random_links(N, 0.5, 41))
+            ctx.set_efield(random_efield(N, 0.3, 42))
+            ctx.set_modes(random_modes(n, N, 43), random_modes(n, N, 44))
+            ctx.step(3)
+            out[g] = (*ctx.get_modes(), ctx.get_links())
+    for k in range(3):
+        assert np.array_equal(out[0][k], out[group][k])
 
 
 def test_packed_variant_is_fp32_only():

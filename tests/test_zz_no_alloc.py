@@ -1,15 +1,16 @@
-"""ovl_ncsdot_noalloc, the allocation-free NCsDot, against the context entry point.
+"""ovl_ncsdot_noalloc, the allocation-free NCsDot, against the context entry
+point and against the oracle.
 
 The allocation-free entry point serves callers that cannot allocate device
 memory (a step loop that must not block on an allocation, or memory owned by
 another allocator): they pass device inputs and a device output, and the
 library's fixed scratch array holds the partial sums.  This file is collected
 last so that a failure here comes after every other test has run."""
-import ctypes as C
-
 import numpy as np
 import pytest
 
+from _helpers import oracle_params
+from _oracle import oracle, ptr
 from overlap_b200 import Context, _lib
 from overlap_b200.inputs import random_efield, random_links
 
@@ -35,7 +36,14 @@ def context_ncsdot(U, E, N):
         return ctx.ncsdot()
 
 
-def test_noalloc_ncsdot_matches_context_entry_on_consecutive_calls():
+def oracle_ncsdot(U, E, N):
+    import ctypes as C
+
+    p = oracle_params(N)
+    return oracle().orc_ncsdot(C.byref(p), ptr(np.ascontiguousarray(U)), ptr(np.ascontiguousarray(E)))
+
+
+def test_noalloc_ncsdot_matches_context_entry_and_oracle_on_consecutive_calls():
     torch = pytest.importorskip("torch")
     # the second call has a smaller lattice, so stale partial sums of the first
     # call would be read if the entry point did not overwrite what it reads
@@ -44,7 +52,27 @@ def test_noalloc_ncsdot_matches_context_entry_on_consecutive_calls():
         E = random_efield(N, 0.5, seed + 100)
         got = noalloc_ncsdot(U, E, N, torch)
         want = context_ncsdot(U, E, N)
+        orc = oracle_ncsdot(U, E, N)
         assert abs(got - want) <= 1e-13 * max(1.0, abs(want)), (N, got, want)
+        assert abs(got - orc) <= 1e-12 * max(1.0, abs(orc)), (N, got, orc)
+
+
+def test_noalloc_ncsdot_at_its_size_limit():
+    # 64^3 sites use all 1024 partial sums of the scratch array
+    torch = pytest.importorskip("torch")
+    N = (64, 64, 64)
+    U = random_links(N, 0.7, 11)
+    E = random_efield(N, 0.4, 12)
+    got = noalloc_ncsdot(U, E, N, torch)
+    want = context_ncsdot(U, E, N)
+    assert abs(got - want) <= 1e-12 * max(1.0, abs(want)), (got, want)
+    # and a small lattice right after, on the same array
+    n2 = (4, 5, 6)
+    U2 = random_links(n2, 0.8, 13)
+    E2 = random_efield(n2, 0.3, 14)
+    got2 = noalloc_ncsdot(U2, E2, n2, torch)
+    orc2 = oracle_ncsdot(U2, E2, n2)
+    assert abs(got2 - orc2) <= 1e-12 * max(1.0, abs(orc2)), (got2, orc2)
 
 
 def test_noalloc_rejects_lattices_beyond_its_scratch():
