@@ -269,9 +269,13 @@ void launch_free_fermions(void *psi, void *psimid, const Lattice &L, int n_modes
 // u1) for FP64 modes, the FP32 copies (U32, u1_32) for FP32 modes; u1 / u1_32
 // null without a U(1) background.
 constexpr int kSu3Link32Floats = 20;  // FP32 link copy: 18 floats per link padded to 80 bytes
+// variant: 0 the scalar three-colour stencil (one mode per thread); 3 (FP32
+// with the FP32 link copy only) the packed-pair stencil (two modes per thread
+// on the paired FP32 instructions, ovl_su3_packed.cuh).
 struct Su3Links {
     const double *U = nullptr, *u1 = nullptr;
     const float *U32 = nullptr, *u1_32 = nullptr;
+    int variant = 0;
 };
 template <typename T>
 void su3_launch_hop(const Su3Links &lk, const void *src, void *dst, const Lattice &L, int mb0, int n_mb, double amass,

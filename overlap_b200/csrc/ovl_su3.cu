@@ -10,6 +10,7 @@
 
 #include "ovl_internal.h"
 #include "ovl_su3.cuh"
+#include "ovl_su3_packed.cuh"
 
 namespace ovl {
 
@@ -55,10 +56,50 @@ static void hop3_launch(const Su3Links &lk, const void *src, void *dst, const La
         links, reinterpret_cast<const cpx<T> *>(src), reinterpret_cast<cpx<T> *>(dst), L, mb0, (T)amass, (T)dt);
 }
 
+// The packed-pair stencil (variant 3, FP32): CTAs of kPk3Warps warps (2
+// kPk3Warps sites) running kPk3Blocks mode blocks each on one set of link
+// records.  MODE 0: dst = D src, 1: dst += dt D src, 2: the Clenshaw term.
+constexpr int kPk3Warps = 4, kPk3Sites = 2 * kPk3Warps, kPk3Blocks = 8, kPk3MinBlocks = 4;
+
+template <int MODE, bool U1>
+__global__ void __launch_bounds__(kModeBlock *kPk3Warps, kPk3MinBlocks)
+    su3_packed_kernel(const float4 *__restrict__ U32, const float2 *__restrict__ u1, const float4 *__restrict__ src,
+                      float4 *__restrict__ dst, Lattice L, int n_mb, float amass, float hdt, const ClenshawArgs cl) {
+    __shared__ float4 rec[kPk3Sites][6][kPk3RecVec];
+    const int mb0 = blockIdx.y * kPk3Blocks;
+    packed_tile3<MODE, U1, kPk3Warps>(rec, U32, u1, src, dst, L, blockIdx.x * kPk3Sites, mb0,
+                                      min(n_mb, mb0 + kPk3Blocks), amass, hdt, cl);
+}
+
+template <int MODE>
+static void packed3_launch(const Su3Links &lk, const void *src, void *dst, const Lattice &L, int n_mb, double amass,
+                           double dt, const ClenshawArgs &cl, cudaStream_t s) {
+    const dim3 block(kModeBlock, kPk3Warps), grid((L.V + kPk3Sites - 1) / kPk3Sites, (n_mb + kPk3Blocks - 1) / kPk3Blocks);
+    const float4 *U = reinterpret_cast<const float4 *>(lk.U32);
+    const float4 *a = reinterpret_cast<const float4 *>(src);
+    float4 *d = reinterpret_cast<float4 *>(dst);
+    const float am = (float)amass, h = (float)(0.5 * dt);
+    if (lk.u1_32)
+        su3_packed_kernel<MODE, true><<<grid, block, 0, s>>>(U, reinterpret_cast<const float2 *>(lk.u1_32), a, d, L,
+                                                             n_mb, am, h, cl);
+    else
+        su3_packed_kernel<MODE, false><<<grid, block, 0, s>>>(U, nullptr, a, d, L, n_mb, am, h, cl);
+}
+
+static bool packed3(const Su3Links &lk, size_t elem) { return elem == 4 && lk.variant == kPackedVariant && lk.U32; }
+
 template <typename T>
 void su3_launch_hop(const Su3Links &lk, const void *src, void *dst, const Lattice &L, int mb0, int n_mb, double amass,
                     double dt, bool accumulate, cudaStream_t s) {
     constexpr bool F32 = sizeof(T) == 4;
+    if (packed3(lk, sizeof(T))) {
+        const size_t off = field_index3(L.V, mb0, 0, 0, 0);
+        const cpx<T> *a = reinterpret_cast<const cpx<T> *>(src) + off;
+        cpx<T> *d = reinterpret_cast<cpx<T> *>(dst) + (accumulate ? off : 0);
+        if (accumulate) packed3_launch<1>(lk, a, d, L, n_mb, amass, dt, ClenshawArgs{}, s);
+        else packed3_launch<0>(lk, a, d, L, n_mb, amass, 0.0, ClenshawArgs{}, s);
+        return;
+    }
     const bool u1 = F32 ? lk.u1_32 != nullptr : lk.u1 != nullptr;
     if (accumulate) {
         if (u1) hop3_launch<T, 1, F32, true>(lk, src, dst, L, mb0, n_mb, amass, dt, s);
@@ -162,11 +203,20 @@ static void cheb3(ChebyshevWork &w, const Su3Links &lk, const void *src, void *d
     cudaMemsetAsync(b[2], 0, n * sizeof(cpx<T>), stream);
     int i1 = 1, i2 = 2, io = 0;
     uint64_t nl = 0;
+    const bool pk = packed3(lk, sizeof(T));
     for (int k = K; k >= 0; k--) {
-        su3_wilson_kernel<T, 0, Links3<F32, U1>><<<grid, block, 0, stream>>>(links, b[i1], tmp, L, 0, am, (T)0);
-        su3_clenshaw_kernel<T, Links3<F32, U1>><<<grid, block, 0, stream>>>(
-            links, tmp, b[i1], b[i2], phi, b[io], L, am, a, beta, (T)(k > 0 ? 2 : 1),
-            (T)((k > 0 ? coeff[k] : 0.5 * coeff[0]) * scale));
+        const T factor = (T)(k > 0 ? 2 : 1), ck = (T)((k > 0 ? coeff[k] : 0.5 * coeff[0]) * scale);
+        if (pk) {
+            packed3_launch<0>(lk, b[i1], tmp, L, n_mb, amass, 0.0, ClenshawArgs{}, stream);
+            const ClenshawArgs cl{reinterpret_cast<const float4 *>(b[i1]), reinterpret_cast<const float4 *>(b[i2]),
+                                  reinterpret_cast<const float4 *>(phi), (float)a, (float)beta, (float)factor,
+                                  (float)ck};
+            packed3_launch<2>(lk, tmp, b[io], L, n_mb, amass, 0.0, cl, stream);
+        } else {
+            su3_wilson_kernel<T, 0, Links3<F32, U1>><<<grid, block, 0, stream>>>(links, b[i1], tmp, L, 0, am, (T)0);
+            su3_clenshaw_kernel<T, Links3<F32, U1>><<<grid, block, 0, stream>>>(links, tmp, b[i1], b[i2], phi, b[io], L,
+                                                                                am, a, beta, factor, ck);
+        }
         nl += 2;
         const int t = i2;
         i2 = i1;
@@ -174,7 +224,8 @@ static void cheb3(ChebyshevWork &w, const Su3Links &lk, const void *src, void *d
         io = t;
     }
     // chi = b[i1]; D chi, then the overlap combination
-    su3_wilson_kernel<T, 0, Links3<F32, U1>><<<grid, block, 0, stream>>>(links, b[i1], tmp, L, 0, am, (T)0);
+    if (pk) packed3_launch<0>(lk, b[i1], tmp, L, n_mb, amass, 0.0, ClenshawArgs{}, stream);
+    else su3_wilson_kernel<T, 0, Links3<F32, U1>><<<grid, block, 0, stream>>>(links, b[i1], tmp, L, 0, am, (T)0);
     const size_t blocks = (n + 255) / 256, cap = (size_t)sm_count * 16;
     su3_overlap_finish_kernel<T><<<(int)std::min(blocks, cap), 256, 0, stream>>>(
         phi, tmp, reinterpret_cast<cpx<T> *>(dst), n, (T)mdw, (T)mf, (T)dt, accumulate ? 1 : 0);
