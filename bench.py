@@ -576,6 +576,7 @@ def su3_overlap_leg(steps, warmup, device, modes=0):
         b.synchronize()
         ms = a.elapsed_time(b)
         launches = ctx.launch_count - l0
+        variant = ctx.tuning()[0]
         t0 = time.perf_counter()
         ch = ctx.charges()
         t1 = time.perf_counter()
@@ -584,18 +585,25 @@ def su3_overlap_leg(steps, warmup, device, modes=0):
     finally:
         ctx.close()
     field = M * V * 12 * 8  # one FP32 mode field
-    # per overlap application: 7 field passes per Clenshaw term (w = D b: read b,
+    # algorithmic bytes of one overlap application (the minimum: each Clenshaw
+    # term reads b_{k+1} and b_{k+2} and writes b_k once, 3 K elements per
+    # mode-site, plus 6 for phi, D chi and the combination into the destination)
+    alg = field * (3 * K + 6)
+    # the field passes the kernels make as built: 7 per term (w = D b: read b,
     # write w; term: read w, b_1, b_2, phi, write b_0), K + 1 terms, then D chi
     # (2) and the combination into the destination (4); two memsets (2)
-    alg = field * (7 * (K + 1) + 8)
+    built = field * (7 * (K + 1) + 8)
     half_ms = ms / (2 * steps)
     peak, peak_kind = measured_peaks()
     return {"config": f"SU(3), N=12^3, overlap (Chebyshev degree {K}, [eps, 1] = [{eps}, 1]), Wilson kernel mass -1, "
                       f"{M} plane-wave modes FP32, FP64 links reunitarised, random links sigma 0.5, E sigma 0.1",
             "value": M * V * steps / (ms / 1e3), "unit": METRIC, "steps": steps, "ms_per_step": ms / steps,
             "launches_per_step": launches / steps,
+            "hop_variant": variant,
             "overlap_application": {"ms": half_ms, "algorithmic_bytes": alg, "achieved_GBs": alg / (half_ms / 1e3) / 1e9,
-                                    "frac_of_peak": alg / (half_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind},
+                                    "frac_of_peak": alg / (half_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind,
+                                    "bytes_as_built": built,
+                                    "built_GBs": built / (half_ms / 1e3) / 1e9},
             "observables_per_step_ms": {"N5": 1e3 * (t1 - t0), "N_CS": 1e3 * (t2 - t1)},
             "N5": ch["N5"], "delta_NCS": d}
 

@@ -170,6 +170,7 @@ ovl::Su3Links su3_links(const ovl_ctx *c) {
     lk.u1 = c->u1_on ? c->u1 : nullptr;
     lk.U32 = c->U32;
     lk.u1_32 = c->u1_on ? c->u1_32 : nullptr;
+    lk.variant = c->hop_variant < 0 ? 0 : c->hop_variant;
     return lk;
 }
 
@@ -270,12 +271,14 @@ int next_coeffs(ovl_ctx *c, bool consume) {
 }
 
 ovl::HopConfig hop_config(const ovl_ctx *c);
+int su3_autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]);
 
 int run_overlap(ovl_ctx *c, const void *src, void *dst, int n_mb, int n_modes, bool accumulate, bool consume) {
     if (c->p.sign_method == OVL_SIGN_CHEBYSHEV) {
         double lo, hi;
         int rc = take_bounds(c, consume, lo, hi);
         if (rc) return rc;
+        if (su3(c) && c->hop_variant < 0 && (rc = su3_autotune(c, nullptr))) return rc;
         ProfScope ps(c, OVL_PROF_HOP);
         uint64_t nl = 0;
         if (su3(c) && fp32(c))
@@ -378,6 +381,56 @@ void grouped_pass(ovl_ctx *c, const ovl::HopConfig &h1, const ovl::HopConfig &h2
     }
 }
 
+// Times candidates 0..n-1 of one launch (run(k) enqueues candidate k on
+// `stream` and returns the kernels it launched) and writes each one's time per
+// launch into ms[k].  First a burst: one warm-up and three timed launches per
+// candidate.  Where the fastest burst takes kSustainMinMs or more, the GPU
+// reaches its power cap within a run of such launches, and then the clock a
+// kernel holds depends on its own power draw: each candidate is timed again
+// over windows of about kSustainWindowMs of back-to-back launches, timing the
+// second half of each window, twice in the order 0..n-1, n-1..0 (a drift of
+// the clock over the tuning cancels), and ms[k] is the mean of its two
+// windows.  Returns false if an event could not be created.
+constexpr double kSustainMinMs = 1.0, kSustainWindowMs = 200.0;
+
+template <class F>
+bool time_candidates(cudaStream_t stream, int n, F run, double *ms, uint64_t &launches) {
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return false;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return false;
+    }
+    auto timed = [&](int k, int warm, int reps) {
+        for (int r = 0; r < warm; r++) launches += run(k);
+        cudaEventRecord(e0, stream);
+        for (int r = 0; r < reps; r++) launches += run(k);
+        cudaEventRecord(e1, stream);
+        cudaEventSynchronize(e1);
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        return (double)t / reps;
+    };
+    double best = 1e300;
+    for (int k = 0; k < n; k++) {
+        ms[k] = timed(k, 1, 3);
+        best = std::min(best, ms[k]);
+    }
+    if (best >= kSustainMinMs) {
+        std::vector<double> sum(n, 0.0);
+        for (int pass = 0; pass < 2; pass++)
+            for (int i = 0; i < n; i++) {
+                const int k = pass == 0 ? i : n - 1 - i;
+                const int half = std::max(4, (int)(0.5 * kSustainWindowMs / std::max(ms[k], 1e-3)));
+                sum[k] += timed(k, half, half);
+            }
+        for (int k = 0; k < n; k++) ms[k] = 0.5 * sum[k];
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return true;
+}
+
 // Candidate group sizes (mode blocks) of the grouped fused step; 0 = whole batch.
 constexpr int kGroupCandidates[] = {0, 1, 2, 4, 8};
 
@@ -423,48 +476,71 @@ int autotune_groups(ovl_ctx *c) {
 static_assert(ovl::kHopVariants == OVL_HOP_VARIANTS, "hop variant count of the header");
 
 int autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
-    cudaEvent_t e0, e1;
-    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
-        return fail(c, OVL_E_CUDA, "autotune: events");
     ovl::HopConfig h = hop_config(c);
-    double best = 1e300;
-    int pick = 0;
     // the packed kernel is FP32 only
     const int nv = fp40(c) ? ovl::kFp40Variants : (fp32(c) ? ovl::kHopVariants : ovl::kPackedVariant);
     if (fp40(c)) cudaMemsetAsync(c->aux_dst_lo, 0, c->field_complex * 2, c->stream);
-    if (ms_out)
-        for (int v = 0; v < ovl::kHopVariants; v++) ms_out[v] = 0.0;
-    for (int v = 0; v < nv; v++) {
+    double ms[ovl::kHopVariants] = {0.0, 0.0, 0.0, 0.0};
+    uint64_t nl = 0;
+    auto run = [&](int v) {
         h.variant = v;
-        float total = 0.0f;
-        for (int rep = 0; rep < 4; rep++) {
-            cudaEventRecord(e0, c->stream);
-            if (fp40(c))
-                ovl::launch_wilson40(h, c->psi, c->psi_lo, c->aux_dst, c->aux_dst_lo, c->L, 0, c->n_mb, amass(c->p),
-                                     c->p.dt, true, c->stream);
-            else if (fp32(c)) ovl::launch_wilson_tuned<float>(h, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
-            else ovl::launch_wilson_tuned<double>(h, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
-            cudaEventRecord(e1, c->stream);
-            cudaEventSynchronize(e1);
-            float t = 0.0f;
-            cudaEventElapsedTime(&t, e0, e1);
-            if (rep > 0) total += t;  // first run warms caches and clocks
-        }
-        const double ms = total / 3.0;
-        if (ms_out) ms_out[v] = ms;
-        if (ms < best) { best = ms; pick = v; }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+        if (fp40(c))
+            ovl::launch_wilson40(h, c->psi, c->psi_lo, c->aux_dst, c->aux_dst_lo, c->L, 0, c->n_mb, amass(c->p),
+                                 c->p.dt, true, c->stream);
+        else if (fp32(c)) ovl::launch_wilson_tuned<float>(h, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        else ovl::launch_wilson_tuned<double>(h, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), c->p.dt, true, c->stream);
+        return 1;
+    };
+    if (!time_candidates(c->stream, nv, run, ms, nl)) return fail(c, OVL_E_CUDA, "autotune: events");
+    int pick = 0;
+    for (int v = 1; v < nv; v++)
+        if (ms[v] < ms[pick]) pick = v;
+    if (ms_out)
+        for (int v = 0; v < ovl::kHopVariants; v++) ms_out[v] = ms[v];
     c->hop_variant = pick;
-    int rc = launched(c, 4 * nv, "autotune");
+    int rc = launched(c, (int)nl, "autotune");
     if (!rc && c->mode_group < 0) rc = autotune_groups(c);
     return rc;
+}
+
+// Three colours, FP32: the scalar stencil (variant 0) against the packed-pair
+// stencil (variant 3), timed on the operator buffer as the context uses the
+// stencil (fused half step for Wilson contexts, the D pass of the Chebyshev
+// series for overlap contexts); the state is not touched.
+int su3_autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
+    if (ms_out)
+        for (int v = 0; v < ovl::kHopVariants; v++) ms_out[v] = 0.0;
+    if (!fp32(c)) {
+        c->hop_variant = 0;
+        return OVL_OK;
+    }
+    const int cand[2] = {0, ovl::kPackedVariant};
+    double ms[2] = {0.0, 0.0};
+    uint64_t nl = 0;
+    ovl::Su3Links lk = su3_links(c);
+    const bool acc = !overlap(c);
+    auto run = [&](int k) {
+        lk.variant = cand[k];
+        ovl::su3_launch_hop<float>(lk, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), acc ? c->p.dt : 0.0, acc,
+                                   c->stream);
+        return 1;
+    };
+    if (!time_candidates(c->stream, 2, run, ms, nl)) return fail(c, OVL_E_CUDA, "autotune: events");
+    c->hop_variant = ms[1] < ms[0] ? cand[1] : cand[0];
+    if (ms_out) {
+        ms_out[0] = ms[0];
+        ms_out[ovl::kPackedVariant] = ms[1];
+    }
+    return launched(c, (int)nl, "autotune (three colours)");
 }
 
 // The three-colour half step: fused (dst += dt D src in one pass) or plain
 // (D src into the derivative buffer chunk by chunk, then the axpy).
 int su3_half_step(ovl_ctx *c, const void *src, void *dst) {
+    if (c->hop_variant < 0) {
+        int rc = su3_autotune(c, nullptr);
+        if (rc) return rc;
+    }
     const ovl::Su3Links lk = su3_links(c);
     const Lattice &L = c->L;
     if (c->p.form == OVL_FORM_FUSED) {
@@ -729,7 +805,13 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
         if ((rc = alloc((void **)&c->pipe, nb, "pipeline counters"))) return bail(rc);
         if (cudaMemset(c->pipe, 0, nb) != cudaSuccess) return bail(fail(c, OVL_E_CUDA, "ovl_create: counters"));
     }
-    c->hop_variant = c->nc == 3 ? 0 : p->hop_variant;  // one three-colour kernel: nothing to tune
+    // three colours: the scalar stencil (0) or, FP32 only, the packed one (3); -1 tunes between them
+    if (c->nc == 3)
+        c->hop_variant = p->precision == OVL_PREC_FP32 && (p->hop_variant < 0 || p->hop_variant == ovl::kPackedVariant)
+                             ? p->hop_variant
+                             : 0;
+    else
+        c->hop_variant = p->hop_variant;
     // grouping applies to the fused two-colour Wilson form; fixed when the variant is fixed
     if (p->form != OVL_FORM_FUSED || p->fermion != OVL_FERMION_WILSON || c->nc == 3) c->mode_group = 0;
     else c->mode_group = p->mode_group;
@@ -1610,11 +1692,10 @@ int ovl_pipeline_selftest(ovl_ctx *c, int *code) {
 
 int ovl_autotune(ovl_ctx *c, int *variant, double ms[OVL_HOP_VARIANTS]) {
     if (!c) return OVL_E_ARG;
-    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_autotune: one three-colour kernel, nothing to tune");
     int rc = set_device(c);
     if (rc) return rc;
     double t[ovl::kHopVariants];
-    if ((rc = autotune(c, t))) return rc;
+    if ((rc = su3(c) ? su3_autotune(c, t) : autotune(c, t))) return rc;
     if (variant) *variant = c->hop_variant;
     if (ms)
         for (int v = 0; v < ovl::kHopVariants; v++) ms[v] = t[v];
@@ -1933,39 +2014,36 @@ int ovl_ensemble_member(ovl_ensemble *e, int index, ovl_ctx **ctx) {
 
 namespace {
 
-// Sites per tile of the batched hop: times tiles of 4 and 8 sites on a half
-// step that writes the members' operator buffers (the state is kept).
+// Sites per tile of the batched hop: times tiles of 8 and 4 sites (and, FP32,
+// the packed-pair tiles) on a half step that writes the members' operator
+// buffers (the state is kept), by time_candidates: a sustained window per
+// candidate where a half step takes a millisecond or more.
 int ens_tune(ovl_ensemble *e) {
-    cudaEvent_t a, b;
-    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess)
-        return ens_fail(e, OVL_E_CUDA, "ensemble: events");
     for (ovl_ctx *c : e->members) cudaMemsetAsync(c->aux_dst, 0, c->field_complex * c->elem_bytes, e->stream);
     // tile shapes in the order of tile_ms; the packed tiles only for FP32
     const int cand[OVL_ENSEMBLE_TILES] = {8, 4, ovl::kBatchPacked};
-    double best = 1e300;
-    int pick = 8;
-    int rc = OVL_OK;
-    for (int k = 0; k < (e->fp32 ? OVL_ENSEMBLE_TILES : 2) && rc == OVL_OK; k++) {
-        ens_describe(e, cand[k], true);
-        if ((rc = ens_upload(e))) break;
-        float total = 0.0f;
-        for (int rep = 0; rep < 4; rep++) {
-            cudaEventRecord(a, e->stream);
-            e->launches += ens_hop(e, cand[k], 0);
-            cudaEventRecord(b, e->stream);
-            cudaEventSynchronize(b);
-            float t = 0.0f;
-            cudaEventElapsedTime(&t, a, b);
-            if (rep > 0) total += t;
+    const int n = e->fp32 ? OVL_ENSEMBLE_TILES : 2;
+    int rc = OVL_OK, cur = -1;
+    auto run = [&](int k) -> uint64_t {
+        if (k != cur) {  // describe and upload when the candidate changes (in an untimed warm-up launch)
+            ens_describe(e, cand[k], true);
+            if (rc == OVL_OK) rc = ens_upload(e);
+            cur = k;
         }
-        e->tile_ms[k] = total / 3.0;
-        if (e->tile_ms[k] < best) { best = e->tile_ms[k]; pick = cand[k]; }
+        return rc == OVL_OK ? (uint64_t)ens_hop(e, cand[k], 0) : 0;
+    };
+    double ms[OVL_ENSEMBLE_TILES] = {0.0, 0.0, 0.0};
+    uint64_t nl = 0;
+    if (!time_candidates(e->stream, n, run, ms, nl)) return ens_fail(e, OVL_E_CUDA, "ensemble: events");
+    e->launches += nl;
+    int pick = 0;
+    for (int k = 0; k < n; k++) {
+        e->tile_ms[k] = ms[k];
+        if (ms[k] < ms[pick]) pick = k;
     }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
     cudaError_t r = cudaGetLastError();
     if (rc == OVL_OK && r != cudaSuccess) rc = ens_fail(e, OVL_E_CUDA, "ensemble tuning: %s", cudaGetErrorString(r));
-    e->sites = pick;
+    e->sites = cand[pick];
     return rc;
 }
 

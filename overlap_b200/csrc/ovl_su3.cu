@@ -59,7 +59,7 @@ static void hop3_launch(const Su3Links &lk, const void *src, void *dst, const La
 // The packed-pair stencil (variant 3, FP32): CTAs of kPk3Warps warps (2
 // kPk3Warps sites) running kPk3Blocks mode blocks each on one set of link
 // records.  MODE 0: dst = D src, 1: dst += dt D src, 2: the Clenshaw term.
-constexpr int kPk3Warps = 4, kPk3Sites = 2 * kPk3Warps, kPk3Blocks = 8, kPk3MinBlocks = 4;
+constexpr int kPk3Warps = 4, kPk3Sites = 2 * kPk3Warps, kPk3Blocks = 8, kPk3MinBlocks = 3;
 
 template <int MODE, bool U1>
 __global__ void __launch_bounds__(kModeBlock *kPk3Warps, kPk3MinBlocks)

@@ -46,27 +46,22 @@ __device__ __forceinline__ void build_link_record3(const float4 *__restrict__ U3
     nim[9] = make_float2(0.0f, 0.0f);
 }
 
-// k0 = A h0, k1 = A h1 for colour three-vectors of pairs, row by row (one row
-// of the record live at a time).
-__device__ __forceinline__ void pmul3x2(const float4 *__restrict__ rec, const cpair (&h0)[kColours3],
-                                        const cpair (&h1)[kColours3], cpair (&k0)[kColours3],
-                                        cpair (&k1)[kColours3]) {
+// Row i of k0 = A h0, k1 = A h1 for colour three-vectors of pairs.
+__device__ __forceinline__ void pmul3_row(const float4 *__restrict__ rec, int i, const cpair (&h0)[kColours3],
+                                          const cpair (&h1)[kColours3], cpair &k0, cpair &k1) {
     const float2 *nim = reinterpret_cast<const float2 *>(rec + 9);
-#pragma unroll
-    for (int i = 0; i < 3; i++) {
-        const float4 a0 = rec[3 * i], a1 = rec[3 * i + 1], a2 = rec[3 * i + 2];
-        const float2 n0 = nim[3 * i], n1 = nim[3 * i + 1], n2 = nim[3 * i + 2];
-        const float2 r0 = pr(a0.x, a0.y), r1 = pr(a1.x, a1.y), r2 = pr(a2.x, a2.y);
-        const float2 m0 = pr(a0.z, a0.w), m1 = pr(a1.z, a1.w), m2 = pr(a2.z, a2.w);
-        k0[i].R = __ffma2_rn(r0, h0[0].R, __ffma2_rn(n0, h0[0].I, __ffma2_rn(r1, h0[1].R, __ffma2_rn(n1, h0[1].I,
-                  __ffma2_rn(r2, h0[2].R, __fmul2_rn(n2, h0[2].I))))));
-        k0[i].I = __ffma2_rn(r0, h0[0].I, __ffma2_rn(m0, h0[0].R, __ffma2_rn(r1, h0[1].I, __ffma2_rn(m1, h0[1].R,
-                  __ffma2_rn(r2, h0[2].I, __fmul2_rn(m2, h0[2].R))))));
-        k1[i].R = __ffma2_rn(r0, h1[0].R, __ffma2_rn(n0, h1[0].I, __ffma2_rn(r1, h1[1].R, __ffma2_rn(n1, h1[1].I,
-                  __ffma2_rn(r2, h1[2].R, __fmul2_rn(n2, h1[2].I))))));
-        k1[i].I = __ffma2_rn(r0, h1[0].I, __ffma2_rn(m0, h1[0].R, __ffma2_rn(r1, h1[1].I, __ffma2_rn(m1, h1[1].R,
-                  __ffma2_rn(r2, h1[2].I, __fmul2_rn(m2, h1[2].R))))));
-    }
+    const float4 a0 = rec[3 * i], a1 = rec[3 * i + 1], a2 = rec[3 * i + 2];
+    const float2 n0 = nim[3 * i], n1 = nim[3 * i + 1], n2 = nim[3 * i + 2];
+    const float2 r0 = pr(a0.x, a0.y), r1 = pr(a1.x, a1.y), r2 = pr(a2.x, a2.y);
+    const float2 m0 = pr(a0.z, a0.w), m1 = pr(a1.z, a1.w), m2 = pr(a2.z, a2.w);
+    k0.R = __ffma2_rn(r0, h0[0].R, __ffma2_rn(n0, h0[0].I, __ffma2_rn(r1, h0[1].R, __ffma2_rn(n1, h0[1].I,
+           __ffma2_rn(r2, h0[2].R, __fmul2_rn(n2, h0[2].I))))));
+    k0.I = __ffma2_rn(r0, h0[0].I, __ffma2_rn(m0, h0[0].R, __ffma2_rn(r1, h0[1].I, __ffma2_rn(m1, h0[1].R,
+           __ffma2_rn(r2, h0[2].I, __fmul2_rn(m2, h0[2].R))))));
+    k1.R = __ffma2_rn(r0, h1[0].R, __ffma2_rn(n0, h1[0].I, __ffma2_rn(r1, h1[1].R, __ffma2_rn(n1, h1[1].I,
+           __ffma2_rn(r2, h1[2].R, __fmul2_rn(n2, h1[2].I))))));
+    k1.I = __ffma2_rn(r0, h1[0].I, __ffma2_rn(m0, h1[0].R, __ffma2_rn(r1, h1[1].I, __ffma2_rn(m1, h1[1].R,
+           __ffma2_rn(r2, h1[2].I, __fmul2_rn(m2, h1[2].R))))));
 }
 
 // The projections of pproject (ovl_packed.cuh) for three colours.
@@ -95,34 +90,35 @@ __device__ __forceinline__ void pproject3(const float4 (&v)[kComp3], cpair (&h0)
     }
 }
 
-// acc -= the rebuilt four-spinor of the hop (pmulacc of ovl_packed.cuh, three colours).
+// acc -= the rebuilt four-spinor of the hop (pmulacc of ovl_packed.cuh, three
+// colours), row by row, so one row of products is live at a time.
 template <int MU, bool FWD>
 __device__ __forceinline__ void pmulacc3(cpair (&acc)[kColours3][kSpin], const cpair (&h0)[kColours3],
                                          const cpair (&h1)[kColours3], const float4 *__restrict__ rec) {
-    cpair k0[kColours3], k1[kColours3];
-    pmul3x2(rec, h0, h1, k0, k1);
 #pragma unroll
     for (int c = 0; c < kColours3; c++) {
+        cpair k0, k1;
+        pmul3_row(rec, c, h0, h1, k0, k1);
         cpair *a = acc[c];
-        a[0].R = psub(a[0].R, k0[c].R);
-        a[0].I = psub(a[0].I, k0[c].I);
-        a[1].R = psub(a[1].R, k1[c].R);
-        a[1].I = psub(a[1].I, k1[c].I);
+        a[0].R = psub(a[0].R, k0.R);
+        a[0].I = psub(a[0].I, k0.I);
+        a[1].R = psub(a[1].R, k1.R);
+        a[1].I = psub(a[1].I, k1.I);
         if (MU == 0) {  // forward: spin 2 = -i h1, spin 3 = -i h0; backward: +i
-            a[2].R = FWD ? psub(a[2].R, k1[c].I) : padd(a[2].R, k1[c].I);
-            a[2].I = FWD ? padd(a[2].I, k1[c].R) : psub(a[2].I, k1[c].R);
-            a[3].R = FWD ? psub(a[3].R, k0[c].I) : padd(a[3].R, k0[c].I);
-            a[3].I = FWD ? padd(a[3].I, k0[c].R) : psub(a[3].I, k0[c].R);
+            a[2].R = FWD ? psub(a[2].R, k1.I) : padd(a[2].R, k1.I);
+            a[2].I = FWD ? padd(a[2].I, k1.R) : psub(a[2].I, k1.R);
+            a[3].R = FWD ? psub(a[3].R, k0.I) : padd(a[3].R, k0.I);
+            a[3].I = FWD ? padd(a[3].I, k0.R) : psub(a[3].I, k0.R);
         } else if (MU == 1) {  // forward: spin 2 = -h1, spin 3 = +h0; backward: +h1, -h0
-            a[2].R = FWD ? padd(a[2].R, k1[c].R) : psub(a[2].R, k1[c].R);
-            a[2].I = FWD ? padd(a[2].I, k1[c].I) : psub(a[2].I, k1[c].I);
-            a[3].R = FWD ? psub(a[3].R, k0[c].R) : padd(a[3].R, k0[c].R);
-            a[3].I = FWD ? psub(a[3].I, k0[c].I) : padd(a[3].I, k0[c].I);
+            a[2].R = FWD ? padd(a[2].R, k1.R) : psub(a[2].R, k1.R);
+            a[2].I = FWD ? padd(a[2].I, k1.I) : psub(a[2].I, k1.I);
+            a[3].R = FWD ? psub(a[3].R, k0.R) : padd(a[3].R, k0.R);
+            a[3].I = FWD ? psub(a[3].I, k0.I) : padd(a[3].I, k0.I);
         } else {  // forward: spin 2 = -i h0, spin 3 = +i h1; backward: +i h0, -i h1
-            a[2].R = FWD ? psub(a[2].R, k0[c].I) : padd(a[2].R, k0[c].I);
-            a[2].I = FWD ? padd(a[2].I, k0[c].R) : psub(a[2].I, k0[c].R);
-            a[3].R = FWD ? padd(a[3].R, k1[c].I) : psub(a[3].R, k1[c].I);
-            a[3].I = FWD ? psub(a[3].I, k1[c].R) : padd(a[3].I, k1[c].R);
+            a[2].R = FWD ? psub(a[2].R, k0.I) : padd(a[2].R, k0.I);
+            a[2].I = FWD ? padd(a[2].I, k0.R) : psub(a[2].I, k0.R);
+            a[3].R = FWD ? padd(a[3].R, k1.I) : psub(a[3].R, k1.I);
+            a[3].I = FWD ? psub(a[3].I, k1.R) : padd(a[3].I, k1.R);
         }
     }
 }

@@ -52,9 +52,11 @@ def oracle_leapfrog3(p, U, E, psi, mid, steps):
     return psi, mid, U.view(np.complex128).reshape(-1, 3, 9)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision,variant", [("fp64", 0), ("fp32", 0), ("fp32", 3)])
 @pytest.mark.parametrize("u1", [False, True])
-def test_wilson_operator(precision, u1):
+def test_wilson_operator(precision, variant, u1):
+    """Variant 0: the scalar stencil; 3: the packed-pair FP32 stencil (V = 60:
+    a partial last CTA of 8 sites; 40 modes: a half-empty second mode block)."""
     U = random_links_su3(N, 0.8, 1)
     phi = modes3(M, 2)
     p = oracle_params(N, m=0.1)
@@ -67,27 +69,29 @@ def test_wilson_operator(precision, u1):
             oracle().orc3_wilson_apply(C.byref(p), ptr(f64(U)), ptr(f64(phi[m])), ptr(f64(want[m])))
     finally:
         oracle().orc_set_u1(None)
-    with ctx3(precision) as ctx:
+    with ctx3(precision, hop_variant=variant) as ctx:
         ctx.set_links(U)
         if u1:
             ctx.set_u1(ph)
         got = ctx.apply(phi)
+        assert ctx.tuning()[0] == variant
     assert rel_err(got, want) < TOL[precision]
 
 
-@pytest.mark.parametrize("precision,form", [("fp64", "plain"), ("fp64", "fused"), ("fp32", "fused"),
-                                            ("fp32", "plain")])
-def test_leapfrog_with_moving_links(precision, form):
+@pytest.mark.parametrize("precision,form,variant", [("fp64", "plain", 0), ("fp64", "fused", 0), ("fp32", "fused", 0),
+                                                    ("fp32", "plain", 0), ("fp32", "fused", 3), ("fp32", "plain", 3)])
+def test_leapfrog_with_moving_links(precision, form, variant):
     U = random_links_su3(N, 0.7, 3)
     E = random_efield_su3(N, 0.4, 4)
     psi, mid = modes3(M, 5), modes3(M, 6)
     p = oracle_params(N, m=0.1, dt=0.05)
     o_psi, o_mid, o_U = oracle_leapfrog3(p, U, E, psi, mid, 4)
-    with ctx3(precision, form, plain_chunk_modes=32) as ctx:
+    with ctx3(precision, form, plain_chunk_modes=32, hop_variant=variant) as ctx:
         ctx.set_links(U)
         ctx.set_efield(E)
         ctx.set_modes(psi, mid)
         ctx.step(4)
+        assert ctx.tuning()[0] == variant
         g_psi, g_mid = ctx.get_modes()
         assert rel_err(ctx.get_links(), o_U) < 1e-13
     assert max(rel_err(g_psi, o_psi), rel_err(g_mid, o_mid)) < TOL[precision]
@@ -230,8 +234,8 @@ def _overlap_kw(precision):
                 precision=precision, form="fused")
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_chebyshev_overlap_operator_and_leapfrog(precision):
+@pytest.mark.parametrize("precision,variant", [("fp64", 0), ("fp32", 0), ("fp32", 3)])
+def test_chebyshev_overlap_operator_and_leapfrog(precision, variant):
     U = random_links_su3(N, 0.6, 16)
     E = random_efield_su3(N, 0.3, 17)
     phi = modes3(40, 18)  # two mode blocks: the split recurrence
@@ -246,7 +250,7 @@ def test_chebyshev_overlap_operator_and_leapfrog(precision):
     oracle().orc3_overlap_leapfrog(C.byref(p), ptr(o_U), ptr(E), ptr(f64(o_psi)), ptr(f64(o_mid)), 40, C.byref(t), 2, 48,
                                    0.01, lmax)
     tol = 1e-11 if precision == "fp64" else 1e-4
-    with ctx3(n_modes=40, **_overlap_kw(precision)) as ctx:
+    with ctx3(n_modes=40, hop_variant=variant, **_overlap_kw(precision)) as ctx:
         ctx.set_links(U)
         ctx.set_efield(E)
         assert rel_err(ctx.apply(phi), want) < tol
@@ -267,6 +271,53 @@ def test_chebyshev_overlap_operator_and_leapfrog(precision):
     a2 = np.einsum("msca,ab,mscb->m", np.conj(o_psi), g5 @ g0, O).imag
     n5 = float(np.sum(w * (a1 + 0.5 * a2)) / (2 * volume(N)))
     assert abs(ch["N5"] - n5) <= (1e-10 if precision == "fp64" else 1e-4) * max(1.0, abs(n5))
+
+
+def test_packed_stencil_beyond_one_cta_row_of_mode_blocks():
+    """300 modes = 10 mode blocks (the last 12 of 32 lanes): a CTA of the packed
+    three-colour kernel runs 8 mode blocks, so a second row of CTAs holds blocks
+    8 and 9.  Fused leapfrog with moving links and a U(1) background against
+    the oracle with the same phases."""
+    n = 300
+    U = random_links_su3(N, 0.7, 31)
+    E = random_efield_su3(N, 0.4, 32)
+    psi, mid = modes3(n, 33), modes3(n, 34)
+    ph = u1_flux(N, 2)
+    p = oracle_params(N, m=0.1, dt=0.05)
+    oracle().orc_set_u1(ptr(np.ascontiguousarray(ph).view(np.float64)))
+    try:
+        o_psi, o_mid, o_U = oracle_leapfrog3(p, U, E, psi, mid, 3)
+    finally:
+        oracle().orc_set_u1(None)
+    with ctx3("fp32", "fused", n_modes=n, hop_variant=3) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_u1(ph)
+        ctx.set_modes(psi, mid)
+        ctx.step(3)
+        g_psi, g_mid = ctx.get_modes()
+    assert max(rel_err(g_psi, o_psi), rel_err(g_mid, o_mid)) < TOL["fp32"]
+
+
+@pytest.mark.parametrize("fermion", ["wilson", "overlap"])
+def test_autotune_chooses_between_the_three_colour_stencils(fermion):
+    """FP32 three-colour contexts time the scalar (0) and packed (3) stencils;
+    the state is kept, and FP64 contexts have the scalar stencil only."""
+    kw = _overlap_kw("fp32") if fermion == "overlap" else dict(precision="fp32", form="fused")
+    with ctx3(n_modes=40, **kw) as ctx:
+        U = random_links_su3(N, 0.5, 41)
+        ctx.set_links(U)
+        ctx.set_modes(modes3(40, 42), modes3(40, 43))
+        before = ctx.get_modes()
+        v, ms = ctx.autotune()
+        assert v in (0, 3) and ms[0] > 0 and ms[3] > 0 and ms[1] == ms[2] == 0
+        assert ctx.tuning()[0] == v
+        after = ctx.get_modes()
+        assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+    with ctx3("fp64", "fused") as ctx:
+        ctx.set_links(random_links_su3(N, 0.5, 44))
+        v, ms = ctx.autotune()
+        assert v == 0
 
 
 def test_three_colour_limits_are_reported():
