@@ -57,6 +57,51 @@ struct CompSum {
 };
 
 // ----------------------------------------------------------------- complex --
+// The GPU's global nanosecond timer (bounds for waits on other CTAs).
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// A load with acquire semantics at GPU scope (pairs with a fence + atomic release).
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Bounds of a wait on other CTAs: elapsed time, and a poll count as a second
+// bound (>= 2 s with the 100 ns sleeps between polls).
+constexpr long long kWaitNs = 1000000000LL;
+constexpr long long kWaitPolls = 20000000;
+
+// One thread waits until *counter >= target.  It gives up when the wait runs
+// past either bound, or at once when *err is set (another CTA gave up); giving
+// up sets *err.  Returns whether the count was reached.
+__device__ __forceinline__ bool wait_count(const int *counter, int target, int *err) {
+    long long polls = 0;
+    const unsigned long long t0 = global_ns();
+    while (ld_acquire(counter) < target) {
+        if (++polls > kWaitPolls || (long long)(global_ns() - t0) > kWaitNs || *(volatile int *)err) {
+            atomicExch(err, 1);
+            return false;
+        }
+        __nanosleep(100);
+    }
+    return true;
+}
+
+// Phase j of 2n of a two-phase pipeline over n groups -> (group g, phase h) in
+// the order (0,0), (1,0), (0,1), (2,0), (1,1), ..., (n-1,0), (n-2,1), (n-1,1):
+// a group's second phase runs two phases after its first.
+__device__ __forceinline__ void pipe_phase(int j, int n, int &g, int &h) {
+    if (j == 2 * n - 1) { g = n - 1; h = 1; }
+    else if (j == 0) { g = 0; h = 0; }
+    else if (j & 1) { g = (j + 1) / 2; h = 0; }
+    else { g = j / 2 - 1; h = 1; }
+}
+
 template <typename T> struct cpx { T re, im; };
 template <typename T> struct vec2_of;
 template <> struct vec2_of<double> { using type = double2; };

@@ -129,17 +129,23 @@ __device__ __forceinline__ void load_spinor4_3(const float4 *__restrict__ p, flo
     for (int k = 0; k < kComp3; k++) v[k] = COH ? __ldca(p + k * (kModeBlock / 2)) : __ldg(p + k * (kModeBlock / 2));
 }
 
-// The per-term constants of the Clenshaw epilogue (MODE 2 of packed_tile3):
+// The constants of the epilogues of packed_tile3.  MODE 2, a Clenshaw term:
 // out = factor (a (-D w) + beta b1) - b2 + ck phi, D w the stencil on src.
+// MODE 3, the overlap combination (OverlapU.cpp:188-202) with D chi the
+// stencil on src: o = mdw [ -i g0 cp phi + cm D chi ] into out (accumulate 0)
+// or out += dt o (accumulate 1).
 struct ClenshawArgs {
     const float4 *b1, *b2, *phi;
     float a, beta, factor, ck;
+    float mdw, cp, cm, dt;
+    int accumulate;
 };
 
 // One CTA's tile: sites [site0, site0 + 2W) x mode blocks [mb0, mb1) of src
 // and dst (float4 views, mode block 0 at the pointers).  MODE 0: dst = D src;
 // 1: dst += dt D src (hdt = dt / 2: the 1/2 of D folded in, exact); 2: the
-// Clenshaw epilogue (cl).  COH: src is written elsewhere in the same launch
+// Clenshaw epilogue, 3: the overlap combination (cl).  COH: src is written
+// elsewhere in the same launch
 // (coherent loads).  Every thread of the CTA calls it (it holds a barrier).
 template <int MODE, bool U1, int W, bool COH = false>
 __device__ __forceinline__ void packed_tile3(float4 (*__restrict__ rec)[6][kPk3RecVec],
@@ -209,6 +215,19 @@ __device__ __forceinline__ void packed_tile3(float4 (*__restrict__ rec)[6][kPk3R
                     const float4 d = dst[i];
                     dst[i] = make_float4(fmaf(h, x.I.x, d.x), fmaf(-h, x.R.x, d.y), fmaf(h, x.I.y, d.z),
                                          fmaf(-h, x.R.y, d.w));
+                } else if (MODE == 3) {
+                    // -i g0 phi = sg (im, -re);  D chi = (1/2) sg (I, -R)
+                    const float4 f = __ldg(cl.phi + i);
+                    const float g = cl.mdw * sg, hc = 0.5f * cl.cm;
+                    const float4 o4 = make_float4(g * fmaf(cl.cp, f.y, hc * x.I.x), -g * fmaf(cl.cp, f.x, hc * x.R.x),
+                                                  g * fmaf(cl.cp, f.w, hc * x.I.y), -g * fmaf(cl.cp, f.z, hc * x.R.y));
+                    if (cl.accumulate) {
+                        const float4 d = dst[i];
+                        dst[i] = make_float4(fmaf(cl.dt, o4.x, d.x), fmaf(cl.dt, o4.y, d.y), fmaf(cl.dt, o4.z, d.z),
+                                             fmaf(cl.dt, o4.w, d.w));
+                    } else {
+                        dst[i] = o4;
+                    }
                 } else {
                     // -D w = -(1/2) sg (I, -R); a (-D w) + beta b1, then factor (.) - b2 + ck phi
                     const float h = -0.5f * sg * cl.a;

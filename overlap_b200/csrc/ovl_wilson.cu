@@ -194,10 +194,9 @@ static void launch_packed(const HopConfig &hc, const void *src, void *dst, const
 // A tile of H2(g) waits until every tile of H1(g) is done (a counter per
 // group, released after the tile's stores); those tiles hold earlier tickets,
 // taken by running CTAs whose H1 tiles never wait, so the wait ends.  It is
-// bounded all the same: after kPipeWaitNs of elapsed time (the GPU's
-// %globaltimer) or kPipeSpin polls, whichever comes first, the CTA sets the
-// error word and leaves the tile undone, and the host reports the step as
-// failed.  Both half steps read fields the launch also writes (H1's source is
+// bounded all the same (wait_count: 1 s of the GPU's %globaltimer, or a
+// poll count, whichever comes first): the CTA then sets the error word and
+// leaves the tile undone, and the host reports the step as failed.  Both half steps read fields the launch also writes (H1's source is
 // H2's destination, H2's source is H1's destination), so their spinor loads
 // are coherent ones (packed_tile with COH), not the read-only path.
 struct PipeArgs {
@@ -212,28 +211,9 @@ struct PipeArgs {
     int *done, *ticket, *err;  // counters: done[n_groups], ticket, error word
     double *partial;           // OBS: kObsVals per (group, tile) of H2
 };
-constexpr long long kPipeWaitNs = 1000000000LL;  // 1 s of elapsed time
-constexpr long long kPipeSpin = 20000000;        // polls (>= 2 s with the 100 ns sleeps): a second bound
 
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
 
-__device__ __forceinline__ int ld_acquire(const int *p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 
-// Ticket phase j of 2n -> (group, half step) in the order above.
-__device__ __forceinline__ void pipe_phase(int j, int n, int &g, int &h) {
-    if (j == 2 * n - 1) { g = n - 1; h = 1; }
-    else if (j == 0) { g = 0; h = 0; }
-    else if (j & 1) { g = (j + 1) / 2; h = 0; }
-    else { g = j / 2 - 1; h = 1; }
-}
 
 template <bool U1, bool OBS>
 __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2) wilson_pipeline_kernel(const __grid_constant__ PipeArgs p) {
@@ -259,19 +239,7 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2) wilson_pipeline_k
         pipe_phase(j, p.n_groups, g, h);
         if (t == 0) {
             int go = 1;
-            if (h == 1) {
-                long long polls = 0;
-                const unsigned long long t0 = global_ns();
-                while (ld_acquire(p.done + g) < p.tiles) {
-                    if (++polls > kPipeSpin || (long long)(global_ns() - t0) > kPipeWaitNs ||
-                        *(volatile int *)p.err) {
-                        atomicExch(p.err, 1);
-                        go = 0;
-                        break;
-                    }
-                    __nanosleep(100);
-                }
-            }
+            if (h == 1) go = wait_count(p.done + g, p.tiles, p.err) ? 1 : 0;
             s_go = go;
         }
         __syncthreads();
