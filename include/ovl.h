@@ -204,13 +204,11 @@ int ovl_apply(ovl_ctx *ctx, int count, const double *phi, double *out);
 #define OVL_HOP_VARIANTS 4
 int ovl_autotune(ovl_ctx *ctx, int *variant, double ms[OVL_HOP_VARIANTS]);
 
-/* Failure-detection self-test of the launches that wait on other CTAs:
- * the pipelined grouped step (FP32 Wilson modes, hop variant 3, at least two
- * mode blocks) or, on a three-colour FP32 overlap context with the Chebyshev
- * sign and hop variant 3, the pipelined Clenshaw term.  Runs one pipelined
- * pass on scratch buffers with the first group's first-phase tiles never
- * handed out, so the tiles that wait on them give up after their bounded wait
- * (1 s) and set the error word.  *code receives what ovl_step would have
+/* Failure-detection self-test of the pipelined grouped step (FP32 Wilson
+ * modes, hop variant 3, at least two mode blocks): runs one pipelined pass on
+ * the operator buffers with the first group's first-half tiles never handed
+ * out, so the second-half tiles that wait on them give up after their bounded
+ * wait (1 s) and set the error word.  *code receives what ovl_step would have
  * returned (OVL_E_TIMEOUT when the detection works).  The context's modes and
  * links are not touched. */
 int ovl_pipeline_selftest(ovl_ctx *ctx, int *code);

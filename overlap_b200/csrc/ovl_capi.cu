@@ -272,7 +272,6 @@ int next_coeffs(ovl_ctx *c, bool consume) {
 
 ovl::HopConfig hop_config(const ovl_ctx *c);
 int su3_autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]);
-int check_cheb_pipeline(ovl_ctx *c);
 
 int run_overlap(ovl_ctx *c, const void *src, void *dst, int n_mb, int n_modes, bool accumulate, bool consume) {
     if (c->p.sign_method == OVL_SIGN_CHEBYSHEV) {
@@ -280,16 +279,6 @@ int run_overlap(ovl_ctx *c, const void *src, void *dst, int n_mb, int n_modes, b
         int rc = take_bounds(c, consume, lo, hi);
         if (rc) return rc;
         if (su3(c) && c->hop_variant < 0 && (rc = su3_autotune(c, nullptr))) return rc;
-        if (su3(c) && !c->cw.w && c->hop_variant != ovl::kPackedVariant) {
-            // the scalar stencil's two-launch terms need the full temporary
-            const size_t bytes = c->field_complex * c->elem_bytes;
-            if (cudaMalloc(&c->cw.w, bytes) != cudaSuccess) {
-                cudaGetLastError();
-                c->cw.w = nullptr;
-                return fail(c, OVL_E_OOM, "overlap operator: Clenshaw temporary (%zu bytes)", bytes);
-            }
-        }
-        const bool piped = su3(c) && c->hop_variant == ovl::kPackedVariant && c->cw.pipe;
         ProfScope ps(c, OVL_PROF_HOP);
         uint64_t nl = 0;
         if (su3(c) && fp32(c))
@@ -310,8 +299,7 @@ int run_overlap(ovl_ctx *c, const void *src, void *dst, int n_mb, int n_modes, b
                                          c->p.dt, accumulate, c->sm_count, c->stream, &nl);
         c->ostats.iterations = c->ostats.max_mode_iterations = c->p.cheb_degree;
         c->ostats.not_converged = lo < c->p.cheb_eps * hi ? 1 : 0;
-        if ((rc = launched(c, (int)nl, "overlap operator (Chebyshev)"))) return rc;
-        return piped ? check_cheb_pipeline(c) : OVL_OK;
+        return launched(c, (int)nl, "overlap operator (Chebyshev)");
     }
     int rc = next_coeffs(c, consume);
     if (rc) return rc;
@@ -443,12 +431,6 @@ bool time_candidates(cudaStream_t stream, int n, F run, double *ms, uint64_t &la
     return true;
 }
 
-// Pipelined Clenshaw terms (three colours, FP32, packed stencil): mode blocks
-// per group and groups in the ring of D b buffers.  Two blocks of a 12^3
-// lattice are 10.6 MB per field: three ring slots and the groups' b vectors in
-// flight stay well inside the 126 MB L2.
-constexpr int kChebGroup = 2, kChebRing = 3;
-
 // Candidate group sizes (mode blocks) of the grouped fused step; 0 = whole batch.
 constexpr int kGroupCandidates[] = {0, 1, 2, 4, 8};
 
@@ -523,8 +505,9 @@ int autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
 
 // Three colours, FP32: the scalar stencil (variant 0) against the packed-pair
 // stencil (variant 3), timed on the operator buffer as the context uses the
-// stencil (fused half step for Wilson contexts, the D pass of the Chebyshev
-// series for overlap contexts); the state is not touched.
+// stencil (the fused half step for Wilson contexts; for overlap contexts a
+// Chebyshev series of degree 3, whose D passes and final combination differ
+// between the variants); the state is not touched.
 int su3_autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
     if (ms_out)
         for (int v = 0; v < ovl::kHopVariants; v++) ms_out[v] = 0.0;
@@ -536,9 +519,22 @@ int su3_autotune(ovl_ctx *c, double ms_out[ovl::kHopVariants]) {
     double ms[2] = {0.0, 0.0};
     uint64_t nl = 0;
     ovl::Su3Links lk = su3_links(c);
-    const bool acc = !overlap(c);
-    auto run = [&](int k) {
+    const bool cheb = overlap(c) && c->p.sign_method == OVL_SIGN_CHEBYSHEV;
+    if (cheb) {
+        cudaMemsetAsync(c->cw.b1, 0, c->field_complex * c->elem_bytes, c->stream);
+        cudaMemsetAsync(c->cw.b2, 0, c->field_complex * c->elem_bytes, c->stream);
+    }
+    const double lmax = std::pow(0.5 * std::fabs(amass(c->p)) + 3.0, 2);
+    auto run = [&](int k) -> uint64_t {
         lk.variant = cand[k];
+        if (cheb) {  // a Chebyshev series of degree 3 (four terms and the combination), psi -> aux_dst
+            uint64_t n = 0;
+            ovl::su3_chebyshev_apply<float>(c->cw, lk, c->psi, c->aux_dst, c->L, c->n_mb, c->cheb.data(),
+                                            std::min(3, c->p.cheb_degree), c->p.cheb_eps, lmax, amass(c->p), c->p.m_dw,
+                                            c->p.m_fermion, c->p.dt, false, c->sm_count, c->stream, &n);
+            return n;
+        }
+        const bool acc = !overlap(c);
         ovl::su3_launch_hop<float>(lk, c->psi, c->aux_dst, c->L, 0, c->n_mb, amass(c->p), acc ? c->p.dt : 0.0, acc,
                                    c->stream);
         return 1;
@@ -658,20 +654,6 @@ int run_currents(ovl_ctx *c) {
         ovl::launch_currents<double>(c->U, c->u1_on ? c->u1 : nullptr, c->psi, c->L, c->n_mb, c->p.n_modes, c->p.first_mode, c->p.r_wilson,
                                      c->partial, c->per_site, c->stream);
     return launched(c, 2, "currents");
-}
-
-// The error word of the pipelined Clenshaw terms of one overlap application
-// (a tile that waited past its bound left its part of the result undone).
-int check_cheb_pipeline(ovl_ctx *c) {
-    int *err = reinterpret_cast<int *>(c->host_small + 62);  // a slot no other read uses
-    int *dev = c->cw.pipe + ovl::cheb_pipe_counters(c->n_mb, c->cw.group) - 1;
-    OVL_CUDA(c, cudaMemcpyAsync(err, dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
-    if (*err) {
-        cudaMemsetAsync(dev, 0, sizeof(int), c->stream);
-        return fail(c, OVL_E_TIMEOUT, "overlap operator: a pipelined Clenshaw term timed out waiting for its first phase");
-    }
-    return OVL_OK;
 }
 
 }  // namespace
@@ -850,23 +832,8 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
     if (p->fermion == OVL_FERMION_OVERLAP && p->sign_method == OVL_SIGN_CHEBYSHEV) {
         ovl::ChebyshevWork &w = c->cw;
         if ((rc = alloc(&w.b0, field_bytes, "Clenshaw b")) || (rc = alloc(&w.b1, field_bytes, "Clenshaw b")) ||
-            (rc = alloc(&w.b2, field_bytes, "Clenshaw b")))
+            (rc = alloc(&w.b2, field_bytes, "Clenshaw b")) || (rc = alloc(&w.w, field_bytes, "Clenshaw temporary")))
             return bail(rc);
-        if (c->nc == 3 && p->precision == OVL_PREC_FP32) {
-            // the pipelined terms of the packed stencil: a ring of kChebRing
-            // groups of kChebGroup mode blocks in place of the full temporary
-            // (allocated later only if the scalar stencil is chosen)
-            w.group = std::min(kChebGroup, c->n_mb);
-            w.ring_slots = kChebRing;
-            const size_t block_bytes = field_bytes / c->n_mb;
-            const size_t nb = sizeof(int) * ovl::cheb_pipe_counters(c->n_mb, w.group);
-            if ((rc = alloc(&w.ring, block_bytes * w.group * w.ring_slots, "Clenshaw ring")) ||
-                (rc = alloc((void **)&w.pipe, nb, "Clenshaw counters")))
-                return bail(rc);
-            if (cudaMemset(w.pipe, 0, nb) != cudaSuccess) return bail(fail(c, OVL_E_CUDA, "ovl_create: counters"));
-        } else if ((rc = alloc(&w.w, field_bytes, "Clenshaw temporary"))) {
-            return bail(rc);
-        }
         c->cheb.assign(p->cheb_degree + 1, 0.0);
         ovl::chebyshev_inverse_sqrt(p->cheb_degree, p->cheb_eps, c->cheb.data());
     }
@@ -912,7 +879,7 @@ int ovl_destroy(ovl_ctx *c) {
     void *bufs[] = {c->psi, c->psimid, c->U, c->E, c->deriv, c->per_site, c->partial, c->dev_small, c->dev_int,
                     c->aux_src, c->aux_dst, c->ow.r, c->ow.q, c->ow.t, c->ow.x, c->ow.p, c->ow.part, c->ow.rnorm,
                     c->ow.alpha, c->ow.active, c->ow.dz, c->u_old, c->u_mid, c->e_mid, c->u1,
-                    c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w, c->cw.ring, c->cw.pipe, c->U32, c->u1_32, c->U_b, c->U32_b,
+                    c->cw.b0, c->cw.b1, c->cw.b2, c->cw.w, c->U32, c->u1_32, c->U_b, c->U32_b,
                     c->psi_lo, c->psimid_lo, c->aux_src_lo, c->aux_dst_lo, c->obs_partial, c->obs_scratch, c->pipe};
     if (c->ow.host_count) cudaFreeHost(c->ow.host_count);
     for (void *b : bufs)
@@ -1720,20 +1687,6 @@ int ovl_tuning(const ovl_ctx *c, int *variant, int *mode_group) {
 
 int ovl_pipeline_selftest(ovl_ctx *c, int *code) {
     if (!c || !code) return OVL_E_ARG;
-    if (su3(c) && overlap(c) && c->cw.pipe && c->hop_variant == ovl::kPackedVariant) {
-        // one pipelined Clenshaw term on the Clenshaw buffers (scratch between
-        // applications) with group 0's first-phase tiles never handed out
-        int rc = set_device(c);
-        if (rc) return rc;
-        const int tiles = (c->L.V + 7) / 8;
-        ovl::su3_launch_cheb_term(su3_links(c), c->cw.b1, c->cw.b2, c->psi, c->cw.b0, c->cw.ring, c->cw.ring_slots,
-                                  c->cw.group, c->cw.pipe, c->L, c->n_mb, amass(c->p), 1.0, 0.0, 2.0, 0.0, c->sm_count,
-                                  c->stream, tiles);
-        c->launches += 2;
-        *code = check_cheb_pipeline(c);
-        c->err.clear();
-        return OVL_OK;
-    }
     const ovl::HopConfig h = hop_config(c);
     if (!pipelined(c, h, h, c->aux_dst, c->aux_dst) || c->n_mb < 2)
         return fail(c, OVL_E_UNSUPPORTED, "ovl_pipeline_selftest: needs FP32 Wilson modes, hop variant 3, 2+ mode blocks");

@@ -71,6 +71,13 @@ __device__ __forceinline__ int ld_acquire(const int *p) {
     return v;
 }
 
+// *p += v with release semantics at GPU scope: the writes this thread has
+// made or observed (through a CTA barrier, cumulativity) are visible to a
+// thread that reads the count with ld_acquire.
+__device__ __forceinline__ void red_release_add(int *p, int v) {
+    asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Bounds of a wait on other CTAs: elapsed time, and a poll count as a second
 // bound (>= 2 s with the 100 ns sleeps between polls).
 constexpr long long kWaitNs = 1000000000LL;

@@ -246,19 +246,11 @@ void overlap_apply(OverlapWork &w, const double *U, const double *u1, const void
 // Chebyshev form of the overlap sign function (ovl_chebyshev.cu).
 constexpr int kMaxChebDegree = 1024;
 void chebyshev_inverse_sqrt(int K, double eps, double *c);
-// b0, b1, b2: Clenshaw vectors (one field each, mode precision); w: the full
-// temporary D b of the two-launch terms.  The pipelined terms (three colours,
-// FP32, packed stencil) use instead `ring` (ring_slots x group mode blocks)
-// and `pipe` (cheb_pipe_counters ints, the last an error word set when a
-// bounded wait expires, never cleared by the device).
+// Clenshaw vectors b0, b1, b2 and the temporary w = D b (one field each, mode
+// precision).
 struct ChebyshevWork {
     void *b0 = nullptr, *b1 = nullptr, *b2 = nullptr, *w = nullptr;
-    void *ring = nullptr;
-    int *pipe = nullptr;
-    int group = 0, ring_slots = 0;
 };
-int cheb_pipe_counters(int n_mb, int group);
-
 // The overlap operator with the Chebyshev series on all mode blocks; FP32 modes
 // take the FP32 link copy when hc.U32 is set.
 template <typename T>
@@ -287,14 +279,6 @@ struct Su3Links {
     const float *U32 = nullptr, *u1_32 = nullptr;
     int variant = 0;
 };
-// One pipelined Clenshaw term of the three-colour packed stencil (FP32):
-// b0 = factor (a (-D D b1) + beta b1) - b2 + ck phi over all mode blocks, in
-// one persistent launch (ovl_su3.cu).  counters: cheb_pipe_counters ints, the
-// last an error word the launch sets (never clears) when a wait times out.
-// first_ticket > 0 (self-test only): the tiles before it are never taken.
-void su3_launch_cheb_term(const Su3Links &lk, const void *b1, const void *b2, const void *phi, void *b0, void *ring,
-                          int slots, int group, int *counters, const Lattice &L, int n_mb, double amass, double a,
-                          double beta, double factor, double ck, int sm_count, cudaStream_t s, int first_ticket);
 template <typename T>
 void su3_launch_hop(const Su3Links &lk, const void *src, void *dst, const Lattice &L, int mb0, int n_mb, double amass,
                     double dt, bool accumulate, cudaStream_t stream);

@@ -186,131 +186,6 @@ __global__ void su3_overlap_finish_kernel(const cpx<T> *__restrict__ phi, const 
     }
 }
 
-// ------------------------------------------------ pipelined Clenshaw term --
-// One Chebyshev term in one persistent launch of the packed stencil.  Groups
-// of `group` mode blocks; per group two phases, A: w = D b1 into slot g % R of
-// a ring of R group-sized buffers, and B: b0 = factor (a (-D w) + beta b1) - b2
-// + ck phi from that slot.  CTAs take 8-site tiles by ticket in the order of
-// pipe_phase -- A(0), A(1), B(0), A(2), B(1), ... -- so a group's w is still in
-// L2 when B reads it, and so is the b1 that A just read: per term the modes
-// cross HBM four times (b1, b2, phi in, b0 out) instead of seven, and the ring
-// replaces the full-size temporary.  A tile of B(g) waits until every tile of
-// A(g) is done; a tile of A(g) with g >= R waits until B(g - R) is done (its
-// slot is free).  Those tiles hold earlier tickets, taken by running CTAs that
-// work their tickets in order, so the waits end; they are bounded all the same
-// (wait_count), and a CTA that gives up sets the error word and leaves its
-// tile undone for the host to report.
-struct Cheb3Pipe {
-    const float4 *U32;
-    const float2 *u1;
-    const float4 *b1, *b2, *phi;
-    float4 *b0, *ring;
-    Lattice L;
-    int n_mb, group, n_groups, tiles, slots;
-    float amass, a, beta, factor, ck;
-    int *doneA, *doneB, *ticket, *err;
-};
-
-int cheb_pipe_counters(int n_mb, int group) { return 2 * ((n_mb + group - 1) / group) + 2; }
-
-__global__ void su3_set_int_kernel(int *p, int v) { *p = v; }
-
-template <bool U1>
-__global__ void __launch_bounds__(kModeBlock *kPk3Warps, kPk3MinBlocks)
-    su3_cheb_term_kernel(const __grid_constant__ Cheb3Pipe p) {
-    __shared__ float4 rec[kPk3Sites][6][kPk3RecVec];
-    __shared__ int s_item, s_go;
-    const int t = threadIdx.y * kModeBlock + threadIdx.x;
-    const int total = 2 * p.n_groups * p.tiles;
-    const size_t blk = (size_t)p.L.V * kComp3 * (kModeBlock / 2);  // float4 per mode block
-    int next = 0;
-    if (t == 0) next = atomicAdd(p.ticket, 1);
-    for (;;) {
-        if (t == 0) {
-            s_item = next;
-            if (next < total) next = atomicAdd(p.ticket, 1);
-        }
-        __syncthreads();
-        const int item = s_item;
-        if (item >= total) break;  // the same for every thread of the CTA
-        const int j = item / p.tiles, tile = item - j * p.tiles;
-        int g, h;
-        pipe_phase(j, p.n_groups, g, h);
-        if (t == 0) {
-            bool go = true;
-            if (h == 1) go = wait_count(p.doneA + g, p.tiles, p.err);
-            else if (g >= p.slots) go = wait_count(p.doneB + (g - p.slots), p.tiles, p.err);
-            s_go = go ? 1 : 0;
-        }
-        __syncthreads();
-        if (s_go) {  // the same for every thread of the CTA
-            const int mb0 = g * p.group, nb = min(p.n_mb, mb0 + p.group) - mb0;
-            float4 *slot = p.ring + (size_t)(g % p.slots) * p.group * blk;
-            const size_t off = (size_t)mb0 * blk;
-            if (h == 0) {
-                packed_tile3<0, U1, kPk3Warps>(rec, p.U32, p.u1, p.b1 + off, slot, p.L, tile * kPk3Sites, 0, nb,
-                                               p.amass, 0.0f, ClenshawArgs{});
-            } else {
-                ClenshawArgs cl{};
-                cl.b1 = p.b1 + off;
-                cl.b2 = p.b2 + off;
-                cl.phi = p.phi + off;
-                cl.a = p.a;
-                cl.beta = p.beta;
-                cl.factor = p.factor;
-                cl.ck = p.ck;
-                packed_tile3<2, U1, kPk3Warps, true>(rec, p.U32, p.u1, slot, p.b0 + off, p.L, tile * kPk3Sites, 0, nb,
-                                                     p.amass, 0.0f, cl);
-            }
-        }
-        __syncthreads();  // every thread's loads and stores of the tile are issued
-        if (t == 0) {
-            __threadfence();
-            atomicAdd((h ? p.doneB : p.doneA) + g, 1);
-        }
-    }
-}
-
-// Launches one pipelined term; counters = cheb_pipe_counters ints (the last the
-// error word, left as it is).  first_ticket > 0 (self-test only) starts the
-// ticket counter there, so the tiles before it are never taken and the tiles
-// that wait on them run out their bounded wait.
-void su3_launch_cheb_term(const Su3Links &lk, const void *b1, const void *b2, const void *phi, void *b0, void *ring,
-                          int slots, int group, int *counters, const Lattice &L, int n_mb, double amass, double a,
-                          double beta, double factor, double ck, int sm_count, cudaStream_t s, int first_ticket) {
-    if (slots < 2 || group < 1) return;  // a ring of one slot would wait on later tickets
-    Cheb3Pipe p;
-    p.U32 = reinterpret_cast<const float4 *>(lk.U32);
-    p.u1 = reinterpret_cast<const float2 *>(lk.u1_32);
-    p.b1 = reinterpret_cast<const float4 *>(b1);
-    p.b2 = reinterpret_cast<const float4 *>(b2);
-    p.phi = reinterpret_cast<const float4 *>(phi);
-    p.b0 = reinterpret_cast<float4 *>(b0);
-    p.ring = reinterpret_cast<float4 *>(ring);
-    p.L = L;
-    p.n_mb = n_mb;
-    p.group = group;
-    p.n_groups = (n_mb + group - 1) / group;
-    p.tiles = (L.V + kPk3Sites - 1) / kPk3Sites;
-    p.slots = slots;
-    p.amass = (float)amass;
-    p.a = (float)a;
-    p.beta = (float)beta;
-    p.factor = (float)factor;
-    p.ck = (float)ck;
-    p.doneA = counters;
-    p.doneB = counters + p.n_groups;
-    p.ticket = counters + 2 * p.n_groups;
-    p.err = counters + 2 * p.n_groups + 1;
-    cudaMemsetAsync(counters, 0, sizeof(int) * (2 * p.n_groups + 1), s);
-    if (first_ticket) su3_set_int_kernel<<<1, 1, 0, s>>>(p.ticket, first_ticket);
-    const long long items = 2LL * p.n_groups * p.tiles;
-    const int grid = (int)std::min<long long>(items, (long long)kPk3MinBlocks * sm_count);
-    const dim3 block(kModeBlock, kPk3Warps);
-    if (p.u1) su3_cheb_term_kernel<true><<<grid, block, 0, s>>>(p);
-    else su3_cheb_term_kernel<false><<<grid, block, 0, s>>>(p);
-}
-
 template <typename T, bool F32, bool U1>
 static void cheb3(ChebyshevWork &w, const Su3Links &lk, const void *src, void *dst, const Lattice &L, int n_mb,
                   const double *coeff, int K, double eps, double lambda_max, double amass, double mdw, double mf,
@@ -328,26 +203,16 @@ static void cheb3(ChebyshevWork &w, const Su3Links &lk, const void *src, void *d
     cudaMemsetAsync(b[2], 0, n * sizeof(cpx<T>), stream);
     int i1 = 1, i2 = 2, io = 0;
     uint64_t nl = 0;
+    // variant 3 (FP32): the D passes in the packed stencil, and the overlap
+    // combination fused into the last one
     const bool pk = packed3(lk, sizeof(T));
-    const bool piped = pk && w.ring && w.pipe;
     for (int k = K; k >= 0; k--) {
         const T factor = (T)(k > 0 ? 2 : 1), ck = (T)((k > 0 ? coeff[k] : 0.5 * coeff[0]) * scale);
-        if (piped) {
-            su3_launch_cheb_term(lk, b[i1], b[i2], phi, b[io], w.ring, w.ring_slots, w.group, w.pipe, L, n_mb, amass,
-                                 (double)a, (double)beta, (double)factor, (double)ck, sm_count, stream, 0);
-            nl += 1;
-        } else if (pk) {
-            packed3_launch<0>(lk, b[i1], tmp, L, n_mb, amass, 0.0, ClenshawArgs{}, stream);
-            const ClenshawArgs cl{reinterpret_cast<const float4 *>(b[i1]), reinterpret_cast<const float4 *>(b[i2]),
-                                  reinterpret_cast<const float4 *>(phi), (float)a, (float)beta, (float)factor,
-                                  (float)ck};
-            packed3_launch<2>(lk, tmp, b[io], L, n_mb, amass, 0.0, cl, stream);
-        } else {
-            su3_wilson_kernel<T, 0, Links3<F32, U1>><<<grid, block, 0, stream>>>(links, b[i1], tmp, L, 0, am, (T)0);
-            su3_clenshaw_kernel<T, Links3<F32, U1>><<<grid, block, 0, stream>>>(links, tmp, b[i1], b[i2], phi, b[io], L,
-                                                                                am, a, beta, factor, ck);
-        }
-        if (!piped) nl += 2;
+        if (pk) packed3_launch<0>(lk, b[i1], tmp, L, n_mb, amass, 0.0, ClenshawArgs{}, stream);
+        else su3_wilson_kernel<T, 0, Links3<F32, U1>><<<grid, block, 0, stream>>>(links, b[i1], tmp, L, 0, am, (T)0);
+        su3_clenshaw_kernel<T, Links3<F32, U1>><<<grid, block, 0, stream>>>(links, tmp, b[i1], b[i2], phi, b[io], L, am,
+                                                                            a, beta, factor, ck);
+        nl += 2;
         const int t = i2;
         i2 = i1;
         i1 = io;

@@ -252,13 +252,23 @@ __device__ __forceinline__ cpx<T> row3(const cpx<T> &a0, const cpx<T> &a1, const
     return k;
 }
 
-template <typename T, int MU, bool FWD>
+// COH false: read-only data (ld.global.nc); true: data the same launch writes
+// (coherent ld.global.ca, ordered after an acquire).
+template <bool COH, typename T> __device__ __forceinline__ cpx<T> ld3(const cpx<T> *p) {
+    if (!COH) return ld(p);
+    using V2 = typename vec2_of<T>::type;
+    const V2 v = __ldca(reinterpret_cast<const V2 *>(p));
+    return mk<T>(v.x, v.y);
+}
+
+template <typename T, int MU, bool FWD, bool COH = false>
 __device__ __forceinline__ void hop3(Spinor3<T> &acc, const cpx<T> *__restrict__ f, const cmat3<T> &M) {
     cpx<T> h0[3], h1[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         const cpx<T> *p = f + c * kSpin * kModeBlock;
-        const cpx<T> p0 = ld(p), p1 = ld(p + kModeBlock), p2 = ld(p + 2 * kModeBlock), p3 = ld(p + 3 * kModeBlock);
+        const cpx<T> p0 = ld3<COH>(p), p1 = ld3<COH>(p + kModeBlock), p2 = ld3<COH>(p + 2 * kModeBlock),
+                     p3 = ld3<COH>(p + 3 * kModeBlock);
         if (MU == 0) {
             h0[c] = FWD ? p0 + times_i(p3) : p0 - times_i(p3);
             h1[c] = FWD ? p1 + times_i(p2) : p1 - times_i(p2);
@@ -300,7 +310,7 @@ __device__ __forceinline__ void hop3(Spinor3<T> &acc, const cpx<T> *__restrict__
 }
 
 // (D phi)(site) before the -i gamma_0 / 2 factor, for the 32 modes of block mb.
-template <typename T, class LK>
+template <typename T, class LK, bool COH = false>
 __device__ __forceinline__ void wilson_site3(const LK &lk, const cpx<T> *__restrict__ src, const Lattice &L, int site,
                                              int mb, int lane, T amass, Spinor3<T> &acc) {
     int x, y, z;
@@ -316,13 +326,13 @@ __device__ __forceinline__ void wilson_site3(const LK &lk, const cpx<T> *__restr
 #pragma unroll
     for (int c = 0; c < 3; c++)
 #pragma unroll
-        for (int a = 0; a < kSpin; a++) acc.c[c][a] = amass * ld(f + (c * kSpin + a) * kModeBlock);
-    hop3<T, 0, true>(acc, src + field_index3(V, mb, xp, 0, lane), lk.template get<T>(site, 0));
-    hop3<T, 0, false>(acc, src + field_index3(V, mb, xm, 0, lane), lk.template get<T>(xm, 0));
-    hop3<T, 1, true>(acc, src + field_index3(V, mb, yp, 0, lane), lk.template get<T>(site, 1));
-    hop3<T, 1, false>(acc, src + field_index3(V, mb, ym, 0, lane), lk.template get<T>(ym, 1));
-    hop3<T, 2, true>(acc, src + field_index3(V, mb, zp, 0, lane), lk.template get<T>(site, 2));
-    hop3<T, 2, false>(acc, src + field_index3(V, mb, zm, 0, lane), lk.template get<T>(zm, 2));
+        for (int a = 0; a < kSpin; a++) acc.c[c][a] = amass * ld3<COH>(f + (c * kSpin + a) * kModeBlock);
+    hop3<T, 0, true, COH>(acc, src + field_index3(V, mb, xp, 0, lane), lk.template get<T>(site, 0));
+    hop3<T, 0, false, COH>(acc, src + field_index3(V, mb, xm, 0, lane), lk.template get<T>(xm, 0));
+    hop3<T, 1, true, COH>(acc, src + field_index3(V, mb, yp, 0, lane), lk.template get<T>(site, 1));
+    hop3<T, 1, false, COH>(acc, src + field_index3(V, mb, ym, 0, lane), lk.template get<T>(ym, 1));
+    hop3<T, 2, true, COH>(acc, src + field_index3(V, mb, zp, 0, lane), lk.template get<T>(site, 2));
+    hop3<T, 2, false, COH>(acc, src + field_index3(V, mb, zm, 0, lane), lk.template get<T>(zm, 2));
 }
 
 }  // namespace ovl

@@ -129,23 +129,20 @@ __device__ __forceinline__ void load_spinor4_3(const float4 *__restrict__ p, flo
     for (int k = 0; k < kComp3; k++) v[k] = COH ? __ldca(p + k * (kModeBlock / 2)) : __ldg(p + k * (kModeBlock / 2));
 }
 
-// The constants of the epilogues of packed_tile3.  MODE 2, a Clenshaw term:
-// out = factor (a (-D w) + beta b1) - b2 + ck phi, D w the stencil on src.
-// MODE 3, the overlap combination (OverlapU.cpp:188-202) with D chi the
-// stencil on src: o = mdw [ -i g0 cp phi + cm D chi ] into out (accumulate 0)
-// or out += dt o (accumulate 1).
+// The constants of the overlap-combination epilogue (MODE 3 of packed_tile3,
+// OverlapU.cpp:188-202) with D chi the stencil on src:
+// o = mdw [ -i g0 cp phi + cm D chi ] into out (accumulate 0) or out += dt o
+// (accumulate 1).
 struct ClenshawArgs {
-    const float4 *b1, *b2, *phi;
-    float a, beta, factor, ck;
+    const float4 *phi;
     float mdw, cp, cm, dt;
     int accumulate;
 };
 
 // One CTA's tile: sites [site0, site0 + 2W) x mode blocks [mb0, mb1) of src
 // and dst (float4 views, mode block 0 at the pointers).  MODE 0: dst = D src;
-// 1: dst += dt D src (hdt = dt / 2: the 1/2 of D folded in, exact); 2: the
-// Clenshaw epilogue, 3: the overlap combination (cl).  COH: src is written
-// elsewhere in the same launch
+// 1: dst += dt D src (hdt = dt / 2: the 1/2 of D folded in, exact); 3: the
+// overlap combination (cl).  COH: src is written elsewhere in the same launch
 // (coherent loads).  Every thread of the CTA calls it (it holds a barrier).
 template <int MODE, bool U1, int W, bool COH = false>
 __device__ __forceinline__ void packed_tile3(float4 (*__restrict__ rec)[6][kPk3RecVec],
@@ -215,7 +212,7 @@ __device__ __forceinline__ void packed_tile3(float4 (*__restrict__ rec)[6][kPk3R
                     const float4 d = dst[i];
                     dst[i] = make_float4(fmaf(h, x.I.x, d.x), fmaf(-h, x.R.x, d.y), fmaf(h, x.I.y, d.z),
                                          fmaf(-h, x.R.y, d.w));
-                } else if (MODE == 3) {
+                } else {  // MODE 3
                     // -i g0 phi = sg (im, -re);  D chi = (1/2) sg (I, -R)
                     const float4 f = __ldg(cl.phi + i);
                     const float g = cl.mdw * sg, hc = 0.5f * cl.cm;
@@ -228,16 +225,6 @@ __device__ __forceinline__ void packed_tile3(float4 (*__restrict__ rec)[6][kPk3R
                     } else {
                         dst[i] = o4;
                     }
-                } else {
-                    // -D w = -(1/2) sg (I, -R); a (-D w) + beta b1, then factor (.) - b2 + ck phi
-                    const float h = -0.5f * sg * cl.a;
-                    const float4 b1 = __ldg(cl.b1 + i), b2 = __ldg(cl.b2 + i), f = __ldg(cl.phi + i);
-                    const float tx0 = fmaf(h, x.I.x, cl.beta * b1.x), ty0 = fmaf(-h, x.R.x, cl.beta * b1.y);
-                    const float tx1 = fmaf(h, x.I.y, cl.beta * b1.z), ty1 = fmaf(-h, x.R.y, cl.beta * b1.w);
-                    dst[i] = make_float4(fmaf(cl.ck, f.x, fmaf(cl.factor, tx0, -b2.x)),
-                                         fmaf(cl.ck, f.y, fmaf(cl.factor, ty0, -b2.y)),
-                                         fmaf(cl.ck, f.z, fmaf(cl.factor, tx1, -b2.z)),
-                                         fmaf(cl.ck, f.w, fmaf(cl.factor, ty1, -b2.w)));
                 }
             }
     }

@@ -253,10 +253,7 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, 2) wilson_pipeline_k
             if (OBS && h == 1) cta_sum_row(o, p.partial + ((size_t)g * p.tiles + tile) * kObsVals);
         }
         __syncthreads();  // every thread's stores of the tile are issued
-        if (t == 0 && h == 0) {
-            __threadfence();
-            atomicAdd(p.done + g, 1);
-        }
+        if (t == 0 && h == 0) red_release_add(p.done + g, 1);
     }
 }
 

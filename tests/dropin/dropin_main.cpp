@@ -1,13 +1,22 @@
-// Drop-in test program: the reference's own Simulation-style build with the
-// Wilson hot path replaced by include/ovl_dropin.hpp (the GPU path), the way
-// a maintainer of the reference would include it.  Test infrastructure: built by
-// tests/dropin/Makefile where the reference tree exists, run by
-// tests/test_gpu_dropin.py, which compares its output with the reference.
+// Drop-in test program: the reference's own Simulation-style build with its
+// fermion hot path replaced by include/ovl_dropin.hpp and its gauge routines
+// (NCsDot, UpdateGaugeLinks, UpdateElectricFields) by include/ovl_dropin_gauge.hpp
+// (the GPU path), the way a maintainer of the reference would include them.
+// Built twice by tests/dropin/Makefile where the reference tree exists: with
+// the Wilson fermions (ovl_dropin_test) and with OVL_TEST_OVERLAP defined, the
+// overlap fermions (ovl_dropin_overlap_test).  Test infrastructure, run by
+// tests/test_gpu_dropin.py, which compares the fermion results with the
+// reference compiled from source.  The gauge routines are checked in this
+// process: the reference's own definitions stay in the build under the names
+// the renaming macros give them, and run on the same fields.
 //
 // usage: ovl_dropin_test N0 N1 N2 nranks rank m r mdw tsph dt steps in.bin out.bin
 //   in.bin : links double[V*12] then efield double[V*9]
-//   out.bin: psi, psimid (local modes, reference layout), links, then the six
-//            current arrays of ComputeCurrents (captured at MPI_Reduce)
+//   out.bin: psi, psimid (local modes, reference layout), links, the current
+//            arrays of ComputeCurrents (captured at MPI_Reduce: six for Wilson,
+//            jV and jA for overlap), then NCsDot (drop-in, reference), E after
+//            UpdateElectricFields(dt) (drop-in, reference), U after
+//            UpdateGaugeLinks(dt) (drop-in, reference), all on the input fields
 #include <cstdio>
 #include <sstream>
 #include <vector>
@@ -15,7 +24,11 @@
 #include "Definitions.cpp"
 #define SU_Nc_FLAG SU2_FLAG
 #define METRIC_FLAG MINKOWSKI_FLAG
+#ifdef OVL_TEST_OVERLAP
+#define FERMION_FLAG OVERLAP_FLAG
+#else
 #define FERMION_FLAG WILSON_FLAG
+#endif
 
 ovlref_reduce_hook_t ovlref_reduce_hook = nullptr;
 
@@ -37,18 +50,27 @@ DOUBLE rWilson = 1.0;
 DOUBLE MDWHeight = 1.4;
 INT BFlux = 1;
 #include "CALC/ChernSimonsOperators.cpp"
+#define NCsDot OVL_ReferenceNCsDot
 #include "TOPOLOGY/ChernSimonsDerivative.cpp"
+#undef NCsDot
+#define UpdateGaugeLinks OVL_ReferenceUpdateGaugeLinks
+#define UpdateElectricFields OVL_ReferenceUpdateElectricFields
+#define Update OVL_ReferenceUpdate
 #include "DYNAMICS/Dynamics.cpp"
+#undef UpdateGaugeLinks
+#undef UpdateElectricFields
+#undef Update
 namespace Dynamics {
 DOUBLE harness_dt = 0.02;
 DOUBLE harness_time() { return Qs * (tSteps * harness_dt); }
 }
 #define dTau harness_dt
 #define Time harness_time
+#include "ovl_dropin_gauge.hpp"  // NCsDot, UpdateGaugeLinks, UpdateElectricFields, Update on the GPU
 #include "QED/QED.cpp"
 #include "DiracAlgebra.cpp"
 #include "FERMIONS/FermionField.cpp"
-#include "ovl_dropin.hpp"  // in place of FERMIONS/WILSON/{EvolutionOperator,Update,Currents}.cpp
+#include "ovl_dropin.hpp"  // in place of the fermion kind's EvolutionOperator, Update and Currents files
 #include "INITIALCONDITIONS/FERMIONS/SetFreeFermions.cpp"
 
 static std::vector<std::vector<double>> g_reduced;
@@ -77,6 +99,26 @@ int main(int argc, char **argv) {
     if (std::fread(GLinks::U->U, sizeof(double), 12 * V, in) != (size_t)(12 * V)) return 3;
     if (std::fread(EFields::E->E, sizeof(double), 9 * V, in) != (size_t)(9 * V)) return 3;
     std::fclose(in);
+    // the gauge routines, drop-in and reference, on the input fields
+    const std::vector<double> U0(GLinks::U->U, GLinks::U->U + 12 * V), E0(EFields::E->E, EFields::E->E + 9 * V);
+    const double dt = Dynamics::harness_dt;
+    const double ncs[2] = {ChernSimonsNumber::NCsDot(GLinks::U, EFields::E),
+                           ChernSimonsNumber::OVL_ReferenceNCsDot(GLinks::U, EFields::E)};
+    std::vector<double> gauge_out[4];
+    for (int k = 0; k < 2; k++) {  // E after UpdateElectricFields: drop-in, reference
+        std::copy(E0.begin(), E0.end(), EFields::E->E);
+        if (k == 0) Dynamics::UpdateElectricFields(0, N0 - 1, 0, N1 - 1, 0, N2 - 1, GLinks::U, EFields::E, dt);
+        else Dynamics::OVL_ReferenceUpdateElectricFields(0, N0 - 1, 0, N1 - 1, 0, N2 - 1, GLinks::U, EFields::E, dt);
+        gauge_out[k].assign(EFields::E->E, EFields::E->E + 9 * V);
+    }
+    std::copy(E0.begin(), E0.end(), EFields::E->E);
+    for (int k = 0; k < 2; k++) {  // U after UpdateGaugeLinks: drop-in, reference
+        std::copy(U0.begin(), U0.end(), GLinks::U->U);
+        if (k == 0) Dynamics::UpdateGaugeLinks(0, N0 - 1, 0, N1 - 1, 0, N2 - 1, GLinks::U, EFields::E, dt);
+        else Dynamics::OVL_ReferenceUpdateGaugeLinks(0, N0 - 1, 0, N1 - 1, 0, N2 - 1, GLinks::U, EFields::E, dt);
+        gauge_out[2 + k].assign(GLinks::U->U, GLinks::U->U + 12 * V);
+    }
+    std::copy(U0.begin(), U0.end(), GLinks::U->U);
     std::ostringstream quiet;
     std::streambuf *err = std::cerr.rdbuf(quiet.rdbuf());
     InitialConditions::SetFreeFermions(Fermions::Psi, Fermions::PsiMid);
@@ -92,6 +134,8 @@ int main(int argc, char **argv) {
     for (INT s = 0; s < MPIModePartition::ModesPerNode; s++) std::fwrite(Fermions::PsiMid->GetMode(s), sizeof(double), 16 * V, out);
     std::fwrite(GLinks::U->U, sizeof(double), 12 * V, out);
     for (auto &a : g_reduced) std::fwrite(a.data(), sizeof(double), a.size(), out);
+    std::fwrite(ncs, sizeof(double), 2, out);
+    for (auto &a : gauge_out) std::fwrite(a.data(), sizeof(double), a.size(), out);
     std::fclose(out);
     std::printf("%d %d\n", MPIModePartition::FirstIndex, MPIModePartition::ModesPerNode);
     return 0;

@@ -320,46 +320,6 @@ def test_autotune_chooses_between_the_three_colour_stencils(fermion):
         assert v == 0
 
 
-def test_pipelined_chebyshev_terms_over_many_groups():
-    """The pipelined Clenshaw terms (packed stencil, FP32) on 300 modes: 10
-    mode blocks in 5 groups of 2 share a ring of 3 slots, so the first phase of
-    groups 3 and 4 waits for the second phase of groups 0 and 1.  Against the
-    oracle's overlap operator, with a U(1) background."""
-    n = 300
-    U = random_links_su3(N, 0.6, 51)
-    phi = modes3(n, 52)
-    ph = u1_flux(N, 3)
-    p = oracle_params(N, m=0.05, mdw=1.0, dt=0.05)
-    lmax = (0.5 * abs(6 + 2 * 0.05 - 2 * 1.0) + 3.0) ** 2
-    want = np.zeros_like(phi)
-    oracle().orc_set_u1(ptr(np.ascontiguousarray(ph).view(np.float64)))
-    try:
-        for m in range(n):
-            oracle().orc3_overlap_apply(C.byref(p), ptr(f64(U)), ptr(f64(phi[m])), ptr(f64(want[m])), 48, 0.01, lmax)
-    finally:
-        oracle().orc_set_u1(None)
-    with ctx3(n_modes=n, hop_variant=3, **_overlap_kw("fp32")) as ctx:
-        ctx.set_links(U)
-        ctx.set_u1(ph)
-        assert rel_err(ctx.apply(phi), want) < 1e-4
-
-
-def test_pipelined_chebyshev_wait_times_out_on_a_counter_nobody_sets():
-    """Failure detection without a GPU fault: the self-test runs one pipelined
-    Clenshaw term with the first group's first-phase tiles never handed out, so
-    the tiles waiting on them run out their bounded wait; the host reads
-    OVL_E_TIMEOUT, the modes are untouched and the operator keeps working."""
-    with ctx3(n_modes=96, hop_variant=3, **_overlap_kw("fp32")) as ctx:
-        ctx.set_links(random_links_su3(N, 0.5, 61))
-        ctx.set_modes(modes3(96, 62), modes3(96, 63))
-        before = ctx.get_modes()
-        assert ctx.pipeline_selftest() == 4  # OVL_E_TIMEOUT
-        after = ctx.get_modes()
-        assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
-        ctx.step(1)
-        assert np.isfinite(ctx.charges()["N5"])
-
-
 def test_three_colour_limits_are_reported():
     for kw in (dict(precision="fp40"), dict(fermion="overlap", sign_method="zolotarev"), dict(n_colours=4)):
         with pytest.raises(OvlError):
