@@ -448,9 +448,8 @@ def ensemble_leg(steps, warmup, device, tile=0):
     flux n_B in {0, 2, 4, 8}, dt = 0.05, FP32 modes, seeded random links
     (sigma 0.3) and E (sigma 0.1).  Times `steps` leapfrog steps of the
     ensemble (one CUDA graph per step) against the same members stepped one
-    context at a time, with the same arithmetic: tile 16 (packed-pair tiles)
-    against hop variant 3, tile 0 (the ensemble tunes its tiles) against
-    variant 0."""
+    context at a time with the packed kernel (hop variant 3).  tile 0: the
+    ensemble tunes its tiles; 16: packed-pair tiles."""
     import numpy as np
     import torch
 
@@ -459,7 +458,7 @@ def ensemble_leg(steps, warmup, device, tile=0):
 
     sizes = [8] * 16 + [10] * 16 + [12] * 16 + [16] * 16
     params = [Params(N=(n, n, n), n_modes=4096, precision="fp32", form="fused", m_fermion=0.05, r_wilson=1.0,
-                     m_dw=0.0, dt=0.05, t_sphaleron=1e300, device=device, hop_variant=3 if tile == 16 else 0)
+                     m_dw=0.0, dt=0.05, t_sphaleron=1e300, device=device, hop_variant=3)
               for n in sizes]
     work = sum(p.n_modes * n ** 3 for p, n in zip(params, sizes))  # mode-sites per step
     ens = Ensemble(params)
@@ -662,13 +661,11 @@ def main():
                     help="the FP32-class form of the headline value (the other is reported beside it)")
     ap.add_argument("--mode-group", type=int, default=0,
                     help="fused form: mode blocks per group (0: whole batch, -1: autotune with the variant)")
-    # Variant 3 (two modes per thread on the paired FP32 instructions) is the
-    # default of the FP32 forms: it loses a short burst to variants 0/1 (4.9 vs
-    # 4.5 ms per half step at 1965 MHz, which is what the autotuner times) but
-    # draws less power per mode-site, and in this 100-step run under the 1 kW cap
-    # it held a higher clock and was faster (12.99-13.04 G vs 12.81-12.83 G
-    # mode-site updates/s, three alternating pairs).
-    ap.add_argument("--hop-variant", type=int, default=3, choices=(-1, 0, 1, 2, 3),
+    # -1: the library's autotuner picks the hop kernel (and the ensemble its
+    # tiles).  Where a launch takes a millisecond or more it times each
+    # candidate over sustained windows, under the power cap that sets the clock
+    # of a long run, so it sees the packed kernel's lower power per mode-site.
+    ap.add_argument("--hop-variant", type=int, default=-1, choices=(-1, 0, 1, 2, 3),
                     help="-1: autotune the hop kernel before warm-up; 0-3: fixed variant (3: FP32 forms, the "
                          "other forms autotune)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 forms")

@@ -1933,7 +1933,8 @@ int ovl_ensemble_create(const ovl_params *members, int count, ovl_ensemble **out
     for (int i = 0; i < count; i++) {
         ovl_params p = members[i];
         p.stream = reinterpret_cast<uint64_t>(e->stream);
-        p.hop_variant = 0;
+        // stepped alone, a member runs variant 0 or, FP32 and asked for, the packed kernel
+        p.hop_variant = p.precision == OVL_PREC_FP32 && p.hop_variant == ovl::kPackedVariant ? ovl::kPackedVariant : 0;
         p.mode_group = 0;
         ovl_ctx *c = nullptr;
         int rc = ovl_create(&p, &c);
@@ -1977,7 +1978,7 @@ int ovl_ensemble_add(ovl_ensemble *e, const ovl_params *member, int *index) {
     if (cudaSetDevice(e->device) != cudaSuccess) return ens_fail(e, OVL_E_CUDA, "ovl_ensemble_add: device");
     ovl_params q = p;
     q.stream = reinterpret_cast<uint64_t>(e->stream);
-    q.hop_variant = 0;
+    q.hop_variant = q.precision == OVL_PREC_FP32 && q.hop_variant == ovl::kPackedVariant ? ovl::kPackedVariant : 0;
     q.mode_group = 0;
     ovl_ctx *c = nullptr;
     int rc = ovl_create(&q, &c);
