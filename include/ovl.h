@@ -151,6 +151,8 @@ int ovl_destroy(ovl_ctx *ctx);
 const char *ovl_last_error(const ovl_ctx *ctx);
 
 /* Gauge fields, host <-> device, reference layouts (GLinks::U->U, EFields::E->E). */
+/* The uploads return once the host array may be reused: at once for pageable
+ * memory (the copy has been staged), after the copy for page-locked memory. */
 int ovl_set_links(ovl_ctx *ctx, const double *links);
 int ovl_get_links(ovl_ctx *ctx, double *links);
 int ovl_set_efield(ovl_ctx *ctx, const double *efield);
@@ -321,6 +323,17 @@ int ovl_color_force(ovl_ctx *ctx, double *out);
 /* H_F = (1/2V) sum_m w_m Re <psi_m, h_W psi_m> of the current modes and links.
  * No reference counterpart.  Wilson only. */
 int ovl_fermion_energy(ovl_ctx *ctx, double *out);
+
+/* InitialConditions::HandmadeSphaleron::Setup (INITIALCONDITIONS/HandmadeSphaleron.cpp:114-170),
+ * the production driver's gauge start (Simulation.cpp:580): the links become
+ * the unit links and E the field that carries them, by the link update of the
+ * leapfrog, to the pure gauge G(x) G(x+mu)^+ in the time t_sphaleron, with
+ * G(x) in SU(2) from the reference's map of the lattice torus onto S^3 of
+ * width r_sphaleron (rSphaleron, Simulation.cpp:168).  u_final (host
+ * double[V][3][4], or NULL) receives G(x) G(x+mu)^+.  Create the context with
+ * t_sphaleron equal to the transition time, so the leapfrog moves the links
+ * while Time() < t_sphaleron and stops at the final ones.  Two colours. */
+int ovl_set_handmade_sphaleron(ovl_ctx *ctx, double r_sphaleron, double t_sphaleron, double *u_final);
 
 /* GaussLawRestoration::Restore (GAUSSLAWFIXING/GaussRestore.cpp:132-168) on the
  * context's links and E: while the signed maximum of the Gauss-law violation

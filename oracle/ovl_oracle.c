@@ -298,6 +298,62 @@ void orc_wilson_leapfrog(const orc_params *p, double *U, const double *E, double
     free(work);
 }
 
+/* ----------------------------------------------------- handmade sphaleron -- */
+
+/* Lattice coordinate i of extent n -> angle on the torus: the arctangent map
+ * centred on the lattice that concentrates the winding within a width r
+ * (LocalizedLatticeMap, HandmadeSphaleron.cpp:7-18). */
+static double torus_angle(int i, int n, double r) {
+    const double b = 1.0 / r, h = n / 2.0;
+    return 2.0 * M_PI * (atan(b * (i - h)) - atan(b * (-h))) / (atan(b * h) - atan(-b * h));
+}
+
+/* The site's element of SU(2) on S^3: torus angles -> R^3 by tan((t - pi) / 2)
+ * (the point at infinity where an angle is 0 or 2 pi), then the inverse
+ * stereographic projection (TorusProjection, InverseStereographicProjection,
+ * HandmadeSphaleron.cpp:22-70). */
+static quat sphaleron_g(const orc_params *p, int s, double r) {
+    int c[3];
+    coords_of(p, s, c);
+    double t[3];
+    int inf = 0;
+    for (int k = 0; k < 3; k++) {
+        t[k] = torus_angle(c[k], p->N[k], r);
+        if (t[k] == 0.0 || t[k] == 2.0 * M_PI) inf = 1;
+    }
+    quat g = {{0.0, 0.0, 0.0, 1.0}};
+    if (!inf) {
+        const double x = tan(0.5 * (t[0] - M_PI)), y = tan(0.5 * (t[1] - M_PI)), z = tan(0.5 * (t[2] - M_PI));
+        const double q = x * x + y * y + z * z, u = (q - 1.0) / (q + 1.0);
+        g.v[0] = (1.0 - u) * x;
+        g.v[1] = (1.0 - u) * y;
+        g.v[2] = (1.0 - u) * z;
+        g.v[3] = u;
+    }
+    return g;
+}
+
+void orc_handmade_sphaleron(const orc_params *p, double r_sph, double t_sph, double *U, double *E, double *Ufinal,
+                            double *G) {
+    const int V = volume(p);
+    for (int s = 0; s < V; s++) {
+        const quat g = sphaleron_g(p, s, r_sph);
+        if (G) memcpy(G + 4 * s, g.v, sizeof g.v);
+        for (int mu = 0; mu < 3; mu++) {
+            /* the final link G(x) 1 G(x+mu)^+ and the algebra element A with
+             * exp(-i A^a t^a) = final link (MatrixILog with C = -1,
+             * SU2/AlgebraOperations.cpp:59-74), divided by the transition time */
+            const quat b = q_mul(g, q_dag(sphaleron_g(p, shift(p, s, mu, 1), r_sph)));
+            if (Ufinal) memcpy(Ufinal + 4 * (mu + 3 * s), b.v, sizeof b.v);
+            const double d = sqrt(b.v[0] * b.v[0] + b.v[1] * b.v[1] + b.v[2] * b.v[2]);
+            const double m = d != 0.0 ? 2.0 * atan2(d, b.v[3]) / (-d) : 0.0;
+            for (int a = 0; a < 3; a++) E[a + 3 * (mu + 3 * s)] = (m * b.v[a]) * (1.0 / t_sph);
+            const quat one = q_unit();
+            memcpy(U + 4 * (mu + 3 * s), one.v, sizeof one.v);
+        }
+    }
+}
+
 /* ------------------------------------------------------------ plane waves -- */
 
 /* Wilson spinors (GetWilsonDiracSpinor, FermionField.cpp:145-317) or, with

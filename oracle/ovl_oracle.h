@@ -105,6 +105,15 @@ double orc_ritz(const orc_params *p, const double *U, const double *start, doubl
  * {signed max, rms} of the last violation computed. */
 int orc_gauss_restore(const orc_params *p, const double *U, double *E, int max_iter, double tol, double *out2);
 
+/* InitialConditions::HandmadeSphaleron::Setup (INITIALCONDITIONS/HandmadeSphaleron.cpp:114-170)
+ * with sphaleron width r_sph and transition time t_sph: the gauge transformation
+ * G(x) (torus map, projection to R^3, inverse stereographic projection onto S^3,
+ * :7-70) written to G (double[V][4], or NULL); U = unit links; Ufinal =
+ * G(x) G(x+mu)^+ (or NULL); E = -i log(Ufinal) / t_sph (GeodesicInterpolation
+ * from the unit links, :73-101). */
+void orc_handmade_sphaleron(const orc_params *p, double r_sph, double t_sph, double *U, double *E, double *Ufinal,
+                            double *G);
+
 /* ---- SU(3) (three colours; no reference counterpart, see ovl_oracle.c) ----
  * links double[V][3][9][2] (U_ij at i + 3j), E double[V][3][8],
  * modes [mode][site][colour 3][spin 4][re, im]. */

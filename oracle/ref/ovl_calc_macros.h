@@ -91,3 +91,27 @@
     for (int avg_a = 0; avg_a < SUNcAlgebra::VectorSize; avg_a++) { \
         E0Loc[avg_a] = E1Loc[avg_a] = E2Loc[avg_a] = B0Loc[avg_a] = B1Loc[avg_a] = B2Loc[avg_a] = 0.0; \
     }
+
+/* CALC/GaugeTransformation.cpp (missing; used by
+ * GAUGETRANSFORMATION/GaugeTransformation.cpp:112-160): the gauge transformation
+ * of links and electric fields by G(x),
+ *   U'_mu(x) = G(x) U_mu(x) G(x+mu)^+ ,   E'_mu(x) = G(x) E_mu(x) G(x)^+ ,
+ * the convention under which the Gauss-law transport of
+ * GAUSSLAWFIXING/GaussRestore.cpp:90-102 (U G(x+mu) U^+) is covariant; the
+ * field rotation uses the reference's own AdjointMultiplication.  Parity with
+ * the missing original is unpinned; the handmade sphaleron built with it has
+ * the vacuum N_CS of its final links equal to the winding number of G
+ * (tests/test_sphaleron.py). */
+#define PERFORM_GAUGE_LINK_TRANSFORMATION(x, y, z)                                                                   \
+    for (INT ovl_mu = 0; ovl_mu < Lattice::Dimension; ovl_mu++) {                                                   \
+        SU_Nc_FUNDAMENTAL_FORMAT ovl_gu[SUNcGroup::MatrixSize];                                                     \
+        SUNcGroup::Operations::UU(G->Get(x, y, z), UOld->Get(x, y, z, ovl_mu), ovl_gu);                             \
+        SUNcGroup::Operations::UD(ovl_gu, G->Get((x) + (ovl_mu == 0), (y) + (ovl_mu == 1), (z) + (ovl_mu == 2)),    \
+                                  UNew->Get(x, y, z, ovl_mu));                                                      \
+    }
+
+#define PERFORM_ELECTRIC_FIELD_TRANSFORMATION(x, y, z)                                                               \
+    for (INT ovl_mu = 0; ovl_mu < Lattice::Dimension; ovl_mu++) {                                                   \
+        SUNcAlgebra::Operations::AdjointMultiplication(G->Get(x, y, z), EOld->Get(x, y, z, ovl_mu, 0),              \
+                                                       ENew->Get(x, y, z, ovl_mu, 0));                              \
+    }

@@ -67,6 +67,18 @@ DOUBLE harness_time();
 #include "OBSERVABLES/GaussLawViolation.cpp"
 #include "OBSERVABLES/UnitarityViolation.cpp"
 #include "GAUSSLAWFIXING/GaussRestore.cpp"
+/* The handmade sphaleron initial condition and what it calls
+ * (INITIALCONDITIONS/HandmadeSphaleron.cpp:114-170; rSphaleron is a global of
+ * Simulation.cpp:168). */
+DOUBLE rSphaleron = 6.0;
+#include "LATTICE/GaugeTransformations.cpp"
+#include "GAUGETRANSFORMATION/GaugeTransformation.cpp"
+#include "INITIALCONDITIONS/SetZero.cpp"
+#include "TOPOLOGY/VacuumEstimator.cpp"
+#include "LATTICE/Indexing.cpp"
+#include "TOPOLOGY/WindingNumber.cpp"
+#include "TOPOLOGY/IntegralEstimateMethod.cpp"
+#include "INITIALCONDITIONS/HandmadeSphaleron.cpp"
 #include "QED/QED.cpp"
 #include "DiracAlgebra.cpp"
 #include "FERMIONS/FermionField.cpp"
@@ -248,6 +260,37 @@ void ovlref_gauss_restore(double *out2) {
     GaussLawRestoration::Restore(GLinks::U, EFields::E);
     out2[0] = GaussLawRestoration::GlobalMaxViolation;
     out2[1] = GaussLawRestoration::GlobalAvgViolation;
+}
+
+/* InitialConditions::HandmadeSphaleron::Setup(GLinks::U, UFinal, EFields::E, G)
+ * with rSphaleron = r_sph and tSphaleron = t_sph: the links become the unit
+ * links, E the geodesic field that carries them to UFinal = G(x) G(x+mu)^+ in
+ * the time t_sph.  u_final (double[V][3][4], or NULL) receives UFinal, g
+ * (double[V][4], or NULL) the gauge transformation, out4 (or NULL)
+ * {WindingNumber::Measure(G), WindingNumber::IntegralEstimate::Measure(G),
+ *  VacuumEstimator::NCS(unit links), VacuumEstimator::NCS(UFinal)}. */
+void ovlref_handmade_sphaleron(double r_sph, double t_sph, double *u_final, double *g, double *out4) {
+    Quiet q;
+    rSphaleron = r_sph;
+    tSphaleron = t_sph;
+    Dynamics::SetMetric();
+    GaugeTransformations *&G = GaugeTransformation::G;
+    if (G && (G->N[0] != Lattice::N[0] || G->N[1] != Lattice::N[1] || G->N[2] != Lattice::N[2])) {
+        delete G;  // sized for an earlier lattice
+        G = nullptr;
+    }
+    if (!G) GaugeTransformation::Init();
+    GaugeLinks UFinal(Lattice::N[0], Lattice::N[1], Lattice::N[2], 1, 1, 1);
+    InitialConditions::HandmadeSphaleron::Setup(GLinks::U, &UFinal, EFields::E, GaugeTransformation::G);
+    const INT V = Lattice::Volume;
+    if (u_final) std::memcpy(u_final, UFinal.U, sizeof(double) * 12 * V);
+    if (g) std::memcpy(g, GaugeTransformation::G->G, sizeof(double) * 4 * V);
+    if (out4) {
+        out4[0] = WindingNumber::Measure(GaugeTransformation::G);
+        out4[1] = WindingNumber::IntegralEstimate::Measure(GaugeTransformation::G);
+        out4[2] = ChernSimonsNumber::VacuumEstimator::NCS(GLinks::U);
+        out4[3] = ChernSimonsNumber::VacuumEstimator::NCS(&UFinal);
+    }
 }
 
 /* Observables::Bulk::Update: out[0..7] = T00, TXX, TYY, TZZ, E-part, B-part, and

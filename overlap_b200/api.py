@@ -369,6 +369,15 @@ class Context:
         self._check(self._L.ovl_fermion_energy(self._ctx, _dp(o)))
         return float(o[0])
 
+    def set_handmade_sphaleron(self, r_sphaleron: float, t_sphaleron: float, final_links: bool = False):
+        """InitialConditions::HandmadeSphaleron::Setup on the device: unit links and
+        the E field that carries them to the pure gauge G(x) G(x+mu)^+ in the time
+        t_sphaleron.  Returns the final links [V, 3, 4] when asked."""
+        out = np.empty((self.V, 3, 4)) if final_links else None
+        self._check(self._L.ovl_set_handmade_sphaleron(self._ctx, float(r_sphaleron), float(t_sphaleron),
+                                                       _dp(out) if out is not None else None))
+        return out
+
     def gauss_restore(self, max_iter: int = 10000, tol: float = 1e-14) -> dict:
         """GaussLawRestoration::Restore on the device: {"iterations", "max", "avg"}."""
         n = C.c_int(0)

@@ -322,6 +322,19 @@ ovl::HopConfig hop_config(const ovl_ctx *c) {
     return h;
 }
 
+// Whether a host buffer is page-locked.  A copy from pageable memory has been
+// staged when cudaMemcpyAsync returns, so the caller may reuse the buffer at
+// once; a copy from page-locked memory may still be reading it, so the upload
+// then waits for the copy before returning.
+bool page_locked(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;  // unknown: wait, the safe choice
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 void refresh_links32(ovl_ctx *c) {
     if (c->U32) {
         if (su3(c)) ovl::su3_launch_links_to_f32(c->U, c->U32, c->L, c->stream);
@@ -904,7 +917,7 @@ int ovl_set_links(ovl_ctx *c, const double *links) {
     if (rc) return rc;
     OVL_CUDA(c, cudaMemcpyAsync(c->U, links, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
     refresh_links32(c);
-    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (page_locked(links)) OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     return OVL_OK;
 }
 
@@ -925,7 +938,7 @@ int ovl_set_efield(ovl_ctx *c, const double *efield) {
     int rc = set_device(c);
     if (rc) return rc;
     OVL_CUDA(c, cudaMemcpyAsync(c->E, efield, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
-    OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (page_locked(efield)) OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     return OVL_OK;
 }
 
@@ -1524,6 +1537,30 @@ int ovl_fermion_energy(ovl_ctx *c, double *out) {
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     *out = c->host_small[0];
     return OVL_OK;
+}
+
+int ovl_set_handmade_sphaleron(ovl_ctx *c, double r_sphaleron, double t_sphaleron, double *u_final) {
+    if (!c) return OVL_E_ARG;
+    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_set_handmade_sphaleron: two colours only");
+    if (!(r_sphaleron > 0.0) || !(t_sphaleron > 0.0))
+        return fail(c, OVL_E_ARG, "ovl_set_handmade_sphaleron: r=%g t=%g", r_sphaleron, t_sphaleron);
+    int rc = set_device(c);
+    if (rc) return rc;
+    const size_t n = (size_t)12 * c->L.V;
+    double *uf = nullptr;
+    if (u_final && cudaMalloc(&uf, sizeof(double) * n) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, OVL_E_OOM, "ovl_set_handmade_sphaleron: final links");
+    }
+    ovl::launch_sphaleron(c->U, c->E, uf, c->L, r_sphaleron, t_sphaleron, c->stream);
+    refresh_links32(c);
+    rc = launched(c, 1, "handmade sphaleron");
+    cudaError_t e = cudaSuccess;
+    if (!rc && uf) e = cudaMemcpyAsync(u_final, uf, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
+    if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (uf) cudaFree(uf);
+    if (rc) return rc;
+    return e == cudaSuccess ? OVL_OK : cuda_fail(c, e, "ovl_set_handmade_sphaleron");
 }
 
 int ovl_gauss_restore(ovl_ctx *c, int max_iter, double tol, int *iterations, double out[2]) {

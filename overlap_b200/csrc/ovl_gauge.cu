@@ -270,6 +270,55 @@ void launch_geodesic(const double *Uold, const double *Unew, double c, double *U
     geodesic_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Uold, Unew, c, Umid, Emid, n);
 }
 
+// ----------------------------------------------------- handmade sphaleron --
+// InitialConditions::HandmadeSphaleron::Setup (INITIALCONDITIONS/HandmadeSphaleron.cpp:114-170):
+// G(x) in SU(2) from the site's lattice coordinates -- arctangent map onto the
+// torus (LocalizedLatticeMap, :7-18), tan((t - pi) / 2) onto R^3 with the point
+// at infinity where an angle is 0 or 2 pi (TorusProjection, :22-31), inverse
+// stereographic projection onto S^3 (:35-60) --; the links start at 1 and the
+// field E = -i log(G(x) G(x+mu)^+) / t_sph (GeodesicInterpolation from the unit
+// links, MatrixILog with C = -1, :73-101) carries them to G(x) G(x+mu)^+ in the
+// time t_sph.  One thread per link; the two G's it needs are recomputed.
+__device__ __forceinline__ double torus_angle(int i, int n, double r) {
+    const double b = 1.0 / r, h = n / 2.0;
+    return 2.0 * M_PI * (atan(b * (i - h)) - atan(b * (-h))) / (atan(b * h) - atan(-b * h));
+}
+
+__device__ __forceinline__ quat sphaleron_g(const Lattice &L, int x, int y, int z, double r) {
+    const double tx = torus_angle(x, L.N0, r), ty = torus_angle(y, L.N1, r), tz = torus_angle(z, L.N2, r);
+    const double tp = 2.0 * M_PI;
+    if (tx == 0.0 || tx == tp || ty == 0.0 || ty == tp || tz == 0.0 || tz == tp) return quat{0.0, 0.0, 0.0, 1.0};
+    const double a = tan(0.5 * (tx - M_PI)), b = tan(0.5 * (ty - M_PI)), c = tan(0.5 * (tz - M_PI));
+    const double q = a * a + b * b + c * c, u = (q - 1.0) / (q + 1.0);
+    return quat{(1.0 - u) * a, (1.0 - u) * b, (1.0 - u) * c, u};
+}
+
+__global__ void sphaleron_kernel(double *U, double *E, double *Ufinal, Lattice L, double r, double inv_t,
+                                 int n_links) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n_links) return;
+    const int site = l / 3, mu = l % 3;
+    int x, y, z;
+    site_coords(L, site, x, y, z);
+    const quat g = sphaleron_g(L, x, y, z, r);
+    const quat gn = sphaleron_g(L, mu == 0 ? (x + 1) % L.N0 : x, mu == 1 ? (y + 1) % L.N1 : y,
+                                mu == 2 ? (z + 1) % L.N2 : z, r);
+    const quat b = qmul(g, qdag(gn));
+    const double d = sqrt(b.v0 * b.v0 + b.v1 * b.v1 + b.v2 * b.v2);
+    const double m = d != 0.0 ? 2.0 * atan2(d, b.s) / (-1.0 * d) : 0.0;
+    E[3 * l + 0] = (m * b.v0) * inv_t;
+    E[3 * l + 1] = (m * b.v1) * inv_t;
+    E[3 * l + 2] = (m * b.v2) * inv_t;
+    store_link(U, site, mu, quat{0.0, 0.0, 0.0, 1.0});
+    if (Ufinal) store_link(Ufinal, site, mu, b);
+}
+
+void launch_sphaleron(double *U, double *E, double *Ufinal, const Lattice &L, double r, double t,
+                      cudaStream_t stream) {
+    const int n = 3 * L.V;
+    sphaleron_kernel<<<(n + 255) / 256, 256, 0, stream>>>(U, E, Ufinal, L, r, 1.0 / t, n);
+}
+
 // ------------------------------------------------------------------- bulk --
 // Per-thread sums: E^2 per direction (3), B^2 per direction (3), Gauss
 // violation squares, unitarity squares, unitarity max, Gauss max (last, max-reduced).

@@ -89,6 +89,9 @@ void launch_ncsdot(const double *U, const double *E, const Lattice &L, double *p
 int ncsdot_blocks_exact(const Lattice &L);
 void launch_ncsdot_into(const double *U, const double *E, const Lattice &L, int blocks, double *partial, double *out,
                         cudaStream_t stream);
+// The handmade sphaleron start: U = 1, E carrying it to G(x) G(x+mu)^+ in time
+// t (written to Ufinal when set).
+void launch_sphaleron(double *U, double *E, double *Ufinal, const Lattice &L, double r, double t, cudaStream_t stream);
 void launch_geodesic(const double *Uold, const double *Unew, double c, double *Umid, double *Emid, const Lattice &L,
                      cudaStream_t stream);
 size_t bulk_partial_doubles(const Lattice &L);

@@ -90,6 +90,7 @@ def oracle():
         L.orc3_coupled_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
                                             C.c_double, C.c_int]
         L.orc_chebyshev_coeffs.argtypes = [C.c_int, C.c_double, _dp]
+        L.orc_handmade_sphaleron.argtypes = [P, C.c_double, C.c_double, _dp, _dp, _dp, _dp]
         L.orc3_overlap_apply.argtypes = [P, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double]
         L.orc3_overlap_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int,
                                             C.c_double, C.c_double]
@@ -130,6 +131,7 @@ def reference(kind: str = "wilson"):
         L.ovlref_apply.argtypes = [_dp, _dp, C.c_double, C.c_double]
         L.ovlref_set_step_count.argtypes = [C.c_int]
         L.ovlref_gauss_restore.argtypes = [_dp]
+        L.ovlref_handmade_sphaleron.argtypes = [C.c_double, C.c_double, _dp, _dp, _dp]
         if kind == "overlap":
             L.ovlref_ritz_bounds.argtypes = [_dp]
             L.ovlref_ritz_solve.argtypes = [_dp, C.c_double]
