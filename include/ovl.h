@@ -335,6 +335,18 @@ int ovl_fermion_energy(ovl_ctx *ctx, double *out);
  * while Time() < t_sphaleron and stops at the final ones.  Two colours. */
 int ovl_set_handmade_sphaleron(ovl_ctx *ctx, double r_sphaleron, double t_sphaleron, double *u_final);
 
+/* InitialConditions::SetQuasiParticles (INITIALCONDITIONS/SetQuasiParticles.cpp:28-220)
+ * on the device, unit spacing, Minkowski metric, two or three colours:
+ * transverse gauge-field modes with occupancy n0 / sqrt(p^2/Qs^2 + 0.1) below
+ * qs (zero above), E = i omega A per mode, backward Fourier transform, links
+ * U = exp(-i A^a t^a); then, when gauss_max_iter > 0, GaussLawRestoration::Restore
+ * with tolerance 1e-14 (as SetQuasiParticles does; *iterations receives its
+ * iterations).  The complex Gaussian amplitudes of each (momentum, colour
+ * component) come from a counter-based generator keyed by `seed` (SplitMix64
+ * with Box-Muller; the reference draws them from GSL in loop order), so the
+ * fields are reproducible and independent of the launch shape. */
+int ovl_set_quasi_particles(ovl_ctx *ctx, double n0, double qs, uint64_t seed, int gauss_max_iter, int *iterations);
+
 /* GaussLawRestoration::Restore (GAUSSLAWFIXING/GaussRestore.cpp:132-168) on the
  * context's links and E: while the signed maximum of the Gauss-law violation
  * exceeds tol and fewer than max_iter iterations ran, three damped steps

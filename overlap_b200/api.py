@@ -369,6 +369,15 @@ class Context:
         self._check(self._L.ovl_fermion_energy(self._ctx, _dp(o)))
         return float(o[0])
 
+    def set_quasi_particles(self, n0: float, qs: float, seed: int, gauss_max_iter: int = 10000) -> int:
+        """InitialConditions::SetQuasiParticles on the device (quasi-particle links and E,
+        then Gauss's law restored unless gauss_max_iter is 0); returns the restoration's
+        iterations.  Noise from the counter-based generator of ovl_set_quasi_particles."""
+        it = C.c_int(0)
+        self._check(self._L.ovl_set_quasi_particles(self._ctx, float(n0), float(qs), int(seed) & (2**64 - 1),
+                                                    int(gauss_max_iter), C.byref(it)))
+        return it.value
+
     def set_handmade_sphaleron(self, r_sphaleron: float, t_sphaleron: float, final_links: bool = False):
         """InitialConditions::HandmadeSphaleron::Setup on the device: unit links and
         the E field that carries them to the pure gauge G(x) G(x+mu)^+ in the time

@@ -21,7 +21,7 @@ OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libovl_b200.so"
 SOURCES = ["ovl_capi.cu", "ovl_wilson.cu", "ovl_gauge.cu", "ovl_modes.cu", "ovl_noalloc.cu", "ovl_overlap.cu",
            "ovl_chebyshev.cu", "ovl_zolotarev.cpp", "ovl_force.cu", "ovl_ritz.cu", "ovl_batch.cu",
-           "ovl_stochastic.cu", "ovl_su3.cu"]
+           "ovl_stochastic.cu", "ovl_su3.cu", "ovl_quasi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

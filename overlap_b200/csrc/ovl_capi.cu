@@ -1563,6 +1563,30 @@ int ovl_set_handmade_sphaleron(ovl_ctx *c, double r_sphaleron, double t_sphalero
     return e == cudaSuccess ? OVL_OK : cuda_fail(c, e, "ovl_set_handmade_sphaleron");
 }
 
+int ovl_set_quasi_particles(ovl_ctx *c, double n0, double qs, uint64_t seed, int gauss_max_iter, int *iterations) {
+    if (!c) return OVL_E_ARG;
+    if (!(n0 >= 0.0) || !(qs > 0.0) || gauss_max_iter < 0)
+        return fail(c, OVL_E_ARG, "ovl_set_quasi_particles: n0=%g qs=%g gauss_max_iter=%d", n0, qs, gauss_max_iter);
+    int rc = set_device(c);
+    if (rc) return rc;
+    void *scratch = nullptr;
+    const size_t bytes = ovl::quasi_particle_scratch_bytes(c->L, c->nc);
+    if (cudaMalloc(&scratch, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, OVL_E_OOM, "ovl_set_quasi_particles: %zu bytes of momentum-space fields", bytes);
+    }
+    ovl::launch_quasi_particles(c->U, c->E, scratch, c->L, c->nc, n0, qs, seed, c->sm_count, c->stream);
+    refresh_links32(c);
+    rc = launched(c, 5, "quasi-particles");
+    const cudaError_t e = rc ? cudaSuccess : cudaStreamSynchronize(c->stream);
+    cudaFree(scratch);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(c, e, "ovl_set_quasi_particles");
+    if (iterations) *iterations = 0;
+    if (gauss_max_iter > 0) return ovl_gauss_restore(c, gauss_max_iter, 1e-14, iterations, nullptr);
+    return OVL_OK;
+}
+
 int ovl_gauss_restore(ovl_ctx *c, int max_iter, double tol, int *iterations, double out[2]) {
     if (!c) return OVL_E_ARG;
     if (max_iter < 0 || !(tol >= 0.0)) return fail(c, OVL_E_ARG, "ovl_gauss_restore: max_iter=%d tol=%g", max_iter, tol);

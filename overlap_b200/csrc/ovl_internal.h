@@ -89,6 +89,12 @@ void launch_ncsdot(const double *U, const double *E, const Lattice &L, double *p
 int ncsdot_blocks_exact(const Lattice &L);
 void launch_ncsdot_into(const double *U, const double *E, const Lattice &L, int blocks, double *partial, double *out,
                         cudaStream_t stream);
+// Quasi-particle gauge fields (ovl_quasi.cu): links and E of nc colours from
+// occupancy n0 below qs, noise from `seed`; scratch holds
+// quasi_particle_scratch_bytes.
+size_t quasi_particle_scratch_bytes(const Lattice &L, int nc);
+void launch_quasi_particles(double *U, double *E, void *scratch, const Lattice &L, int nc, double n0, double qs,
+                            uint64_t seed, int sm_count, cudaStream_t stream);
 // The handmade sphaleron start: U = 1, E carrying it to G(x) G(x+mu)^+ in time
 // t (written to Ufinal when set).
 void launch_sphaleron(double *U, double *E, double *Ufinal, const Lattice &L, double r, double t, cudaStream_t stream);

@@ -139,7 +139,40 @@ def embed_su2_efield(E2: np.ndarray) -> np.ndarray:
 
 
 # -------------------------------------------------------- quasi-particles --
-def quasi_particles(N, n0: float, qs: float, seed: int, n_colours: int = 2):
+_MASK64 = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def _mix64(z: np.ndarray) -> np.ndarray:
+    """SplitMix64 finaliser (Steele, Lea and Flood, OOPSLA 2014) on uint64 arrays."""
+    with np.errstate(over="ignore"):
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def counter_gaussians(N, ncomp: int, seed: int) -> np.ndarray:
+    """The counter-based complex Gaussians of ovl_set_quasi_particles (include/ovl.h):
+    for counter n = (kx + N0 (ky + N1 kz)) ncomp + a, key = mix64(seed ^ mix64(n)),
+    u_j = ((mix64(key + j) >> 11) + 1) 2^-53, Box-Muller pairs (u0, u1), (u2, u3).
+    Returns g[kx, ky, kz, a, (c1, c2), (re, im)] of unit normal variables."""
+    N = tuple(int(n) for n in N)
+    kx, ky, kz = np.meshgrid(*[np.arange(n) for n in N], indexing="ij")
+    site = (kx + N[0] * (ky + N[1] * kz)).astype(np.uint64)
+    n = site[..., None] * np.uint64(ncomp) + np.arange(ncomp, dtype=np.uint64)
+    key = _mix64(np.uint64(seed) ^ _mix64(n))
+    with np.errstate(over="ignore"):
+        u = [((_mix64(key + np.uint64(j)) >> np.uint64(11)) + np.uint64(1)).astype(np.float64) * 2.0 ** -53
+             for j in range(4)]
+    g = np.empty(N + (ncomp, 2, 2))
+    for pair in range(2):
+        r = np.sqrt(-2.0 * np.log(u[2 * pair]))
+        g[..., pair, 0] = r * np.cos(2.0 * np.pi * u[2 * pair + 1])
+        g[..., pair, 1] = r * np.sin(2.0 * np.pi * u[2 * pair + 1])
+    return g
+
+
+def quasi_particles(N, n0: float, qs: float, seed: int, n_colours: int = 2, generator: str = "numpy"):
     """Quasi-particle gauge fields, InitialConditions::SetQuasiParticles
     (INITIALCONDITIONS/SetQuasiParticles.cpp:28-157) for a = 1, Minkowski metric:
     per lattice momentum p_mu = -i (1 - e^{-2 pi i k_mu / N_mu}) (LATTICE/Momenta.cpp:4-8),
@@ -151,8 +184,10 @@ def quasi_particles(N, n0: float, qs: float, seed: int, n_colours: int = 2):
     (FFTW_BACKWARD), A(x) = 2 Re A / V, E(x) = 2 Re E / V, and U = exp(-i A^a t^a).
 
     The reference draws c_1, c_2 from its GSL generator in (kx, ky, kz, a) order;
-    here numpy's generator draws them in the same order, so the fields follow the
-    same distribution but are not the same numbers.  Returns (links, E) in the
+    here numpy's generator draws them in the same order (generator "numpy"), so
+    the fields follow the same distribution but are not the same numbers, or
+    the counter-based generator of the device version (generator "counter",
+    counter_gaussians), which then gives the device's fields.  Returns (links, E) in the
     layouts of Context.set_links / set_efield; restore Gauss's law afterwards
     (Context.gauss_restore), as the reference does.
     """
@@ -176,7 +211,7 @@ def quasi_particles(N, n0: float, qs: float, seed: int, n_colours: int = 2):
     xi2 = [np.where(p2 > 0, (cdp[(m + 1) % 3] * np.conj(xi1[(m + 2) % 3]) - cdp[(m + 2) % 3] * np.conj(xi1[(m + 1) % 3])) / om,
                     0.0) for m in range(3)]
     # complex Gaussians c_1, c_2 per (kx, ky, kz, a), drawn in that loop order
-    g = rng.normal(size=N + (ncomp, 2, 2))
+    g = rng.normal(size=N + (ncomp, 2, 2)) if generator == "numpy" else counter_gaussians(N, ncomp, seed)
     c = (g[..., 0] + 1j * g[..., 1]) / np.sqrt(2.0)  # [..., a, (c1, c2)]
     V = N[0] * N[1] * N[2]
     amp = np.sqrt(occ) * np.sqrt(V)

@@ -43,8 +43,23 @@ def test_quasi_particle_electric_energy_follows_the_occupancy():
     psq = sum((np.sign(c.real) * np.abs(c)) ** 2 for c in cdp)
     f = np.where(psq < qs * qs, n0 / np.sqrt(psq / qs ** 2 + 0.1), 0.0)
     want = 2 * 3 * np.sum(f * omega)
-    got = np.mean([np.sum(quasi_particles(N, n0, qs, seed=s)[1] ** 2) for s in range(24)])
-    assert abs(got / want - 1) < 0.1
+    for generator in ("numpy", "counter"):  # numpy's generator, and the device version's counter-based one
+        got = np.mean([np.sum(quasi_particles(N, n0, qs, seed=s, generator=generator)[1] ** 2) for s in range(24)])
+        assert abs(got / want - 1) < 0.1, generator
     # nothing above Qs: no occupied mode, no field
     U, E = quasi_particles(N, n0, 1e-3, seed=1)
     assert np.abs(E).max() == 0.0 and np.abs(U[..., 3] - 1).max() == 0.0
+
+
+def test_counter_generator_gives_independent_unit_normals():
+    """The counter-based Gaussians of the device's quasi-particles: mean 0,
+    variance 1, uncorrelated between neighbouring counters, and a function of
+    (seed, momentum, component) only."""
+    from overlap_b200.inputs import counter_gaussians
+
+    g = counter_gaussians((16, 16, 16), 8, 11).reshape(-1)
+    assert abs(g.mean()) < 0.01 and abs(g.var() - 1.0) < 0.01
+    assert abs(np.corrcoef(g[:-1], g[1:])[0, 1]) < 0.01
+    a = counter_gaussians((4, 4, 4), 3, 5)
+    assert np.array_equal(a, counter_gaussians((4, 4, 4), 3, 5))
+    assert not np.array_equal(a, counter_gaussians((4, 4, 4), 3, 6))
