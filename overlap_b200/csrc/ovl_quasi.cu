@@ -9,7 +9,8 @@
 // with the transverse polarisation vectors xi1, xi2 of
 // MISC/MinkowskiWaveVectors.cpp:7-44 (base vector (1/sqrt3, 1/sqrt2, 1/sqrt6)),
 // omega = |p|, the occupancy f(p) = n0 / sqrt(|p|^2/Qs^2 + 0.1) below Qs and 0
-// above (SingleParticleDistribution, :27-40), and complex Gaussians c1, c2 of
+// above (SingleParticleDistribution, :27-40; a mode on |p| = Qs is not
+// occupied, decided with a 1e-12 margin), and complex Gaussians c1, c2 of
 // unit variance.  The unnormalised backward transform to position space
 // (FFTW_BACKWARD in the reference) runs as three passes of one-dimensional
 // transforms; then A(x) = 2 Re A / V, E(x) = 2 Re E / V and
@@ -33,6 +34,11 @@
 namespace ovl {
 
 namespace {
+
+// A mode exactly on |p| = Qs is not occupied (the strict test of
+// SingleParticleDistribution); the margin keeps rounding from deciding modes
+// on that boundary (|p|^2 = 4 sin^2(pi/6) = 1 for k/N = 1/6, say).
+constexpr double kEdge = 1.0 - 1e-12;
 
 __device__ __forceinline__ uint64_t qp_mix64(uint64_t z) {
     z += 0x9e3779b97f4a7c15ull;
@@ -69,7 +75,7 @@ __global__ void qp_fill_kernel(cpx<double> *__restrict__ A, cpx<double> *__restr
             psq += pv * pv;
         }
         const double omega = sqrt(p2);
-        const double occ = psq < qs * qs ? n0 / sqrt(psq / (qs * qs) + 0.1) : 0.0;
+        const double occ = psq < kEdge * qs * qs ? n0 / sqrt(psq / (qs * qs) + 0.1) : 0.0;
         // transverse polarisation vectors (zero at p = 0)
         cpx<double> xi1[3] = {mk<double>(0.0, 0.0), mk<double>(0.0, 0.0), mk<double>(0.0, 0.0)};
         cpx<double> xi2[3] = {mk<double>(0.0, 0.0), mk<double>(0.0, 0.0), mk<double>(0.0, 0.0)};

@@ -200,7 +200,8 @@ def quasi_particles(N, n0: float, qs: float, seed: int, n_colours: int = 2, gene
     omega = np.sqrt(p2)
     pv = [np.sign(c.real) * np.abs(c) for c in cdp]
     psq = sum(v * v for v in pv)
-    occ = np.where(psq < qs * qs, n0 / np.sqrt(psq / (qs * qs) + 0.1), 0.0)
+    # a mode on |p| = Qs is not occupied; the margin keeps rounding from deciding it
+    occ = np.where(psq < (1.0 - 1e-12) * qs * qs, n0 / np.sqrt(psq / (qs * qs) + 0.1), 0.0)
     base = np.array([1 / np.sqrt(3.0), 1 / np.sqrt(2.0), 1 / (np.sqrt(2.0) * np.sqrt(3.0))])
     safe = np.where(p2 > 0, p2, 1.0)
     bdp = base[0] * cdp[0] + base[1] * cdp[1] + base[2] * cdp[2]
