@@ -335,6 +335,29 @@ int ovl_fermion_energy(ovl_ctx *ctx, double *out);
  * while Time() < t_sphaleron and stops at the final ones.  Two colours. */
 int ovl_set_handmade_sphaleron(ovl_ctx *ctx, double r_sphaleron, double t_sphaleron, double *u_final);
 
+/* InitialConditions::SetOverlapQEDEigenfunctions (INITIALCONDITIONS/FERMIONS/
+ * SetOverlapQEDEigenfunctions.cpp:5-86), the reference's production fermion
+ * start: the context's modes become eigenmodes of the overlap Hamiltonian of
+ * OverlapQEDEigenfunctions::Setup (BASIS/OverlapQEDEigenfunctions.cpp:141-591)
+ * -- links carrying the context's U(1) background (ovl_set_u1; none: phases 1)
+ * in colour (0,0) and zero elsewhere, as ConvertU1GaugeLinks sets them --
+ * with global mode g at particle index g % 2 and level g / 2: particles on the
+ * positive eigenvalues from the smallest up, antiparticles on the negative ones
+ * from the one nearest zero down; psi = sqrt(V) v, psimid = psi e^{-i omega dt/2}.
+ * The reference reconstructs h_ov from overlap applications (Zolotarev sign
+ * function) and calls LAPACK's zheev; here h_ov is built densely with the
+ * exact sign function and diagonalised on the device (cuSOLVER), so it agrees
+ * with the reference's to the accuracy of the reference's approximation.
+ * Eigenvectors are defined up to a phase (and within a degenerate level up to
+ * a unitary mixing): the modes' bilinears summed over complete levels do not
+ * depend on that choice.  eigenvalues (host double[D], D = 8 V, or NULL):
+ * ascending; h_ov (host complex double[D][D] column-major, index
+ * site + V (spin + 4 colour), or NULL): the matrix; *n_bad (or NULL): modes
+ * whose frequency has the wrong sign for their particle index, plus zero
+ * eigenvalues of h_W.  Two-colour overlap contexts with first_mode + n_modes <= D;
+ * dense D x D matrices limit it to D^2 < 2^31 (lattices up to about 16^3). */
+int ovl_set_qed_eigenmodes(ovl_ctx *ctx, double *eigenvalues, double *h_ov, int *n_bad);
+
 /* InitialConditions::SetQuasiParticles (INITIALCONDITIONS/SetQuasiParticles.cpp:28-220)
  * on the device, unit spacing, Minkowski metric, two or three colours:
  * transverse gauge-field modes with occupancy n0 / sqrt(p^2/Qs^2 + 0.1) below

@@ -92,6 +92,18 @@ DOUBLE rSphaleron = 6.0;
 #include "FERMIONS/OVERLAP/OverlapCurrents.cpp"
 #endif
 #include "INITIALCONDITIONS/FERMIONS/SetFreeFermions.cpp"
+#if FERMION_FLAG == OVERLAP_FLAG
+/* The U(1)-background overlap eigenmodes (INITIALCONDITIONS/FERMIONS/BASIS/
+ * OverlapQEDEigenfunctions.cpp): only the construction of the Hamiltonian is
+ * run here.  Its Eigensystem class calls LAPACK's zheev, absent from this
+ * machine: the symbol is defined below so the class links; the harness never
+ * calls Diagonalize. */
+#include "MISC/LapackDiagonalization.cpp"
+#include "INITIALCONDITIONS/FERMIONS/BASIS/OverlapQEDEigenfunctions.cpp"
+extern "C" void zheev(char const *, char const *, INT *, COMPLEX *, INT *, DOUBLE *, COMPLEX *, int *, DOUBLE *, INT *info) {
+    *info = 1;  // not available
+}
+#endif
 
 namespace Dynamics {
 DOUBLE harness_time() {
@@ -292,6 +304,39 @@ void ovlref_handmade_sphaleron(double r_sph, double t_sph, double *u_final, doub
         out4[3] = ChernSimonsNumber::VacuumEstimator::NCS(&UFinal);
     }
 }
+
+#if FERMION_FLAG == OVERLAP_FLAG
+/* The overlap Hamiltonian in the U(1) background of n_b flux quanta, built as
+ * OverlapQEDEigenfunctions::Setup builds it (:141-440): links
+ * ConvertU1GaugeLinks(QED::U) -- the U(1) phase in colour (0,0), every other
+ * entry zero --, spectral bounds by the reference's Ritz solver
+ * (ComputeRitzEigenvalues, a start vector from its RNG), then column j of
+ * H = i OverlapOperator::Compute(e_j).  Setup applies the operator to a random
+ * orthonormal basis and transforms back; the standard basis e_j gives the same
+ * matrix without that round-off.  H: complex double[D][D] column-major,
+ * D = 4 Nc V, index site + V (spin + 4 colour); bounds2 = {MinEValue, MaxEValue}. */
+void ovlref_qed_hamiltonian(int n_b, double *H, double *bounds2) {
+    Quiet q;
+    QED::SetConstantMagneticField(n_b);
+    OverlapQEDEigenfunctions::ConvertU1GaugeLinks(QED::U, EvolutionOperator::Ucc);
+    Dynamics::Fermions::ComputeRitzEigenvalues();
+    const DOUBLE lo = Dynamics::Fermions::MinEValue, hi = Dynamics::Fermions::MaxEValue;
+    bounds2[0] = lo;
+    bounds2[1] = hi;
+    const INT V = Lattice::Volume, D = 4 * Nc * V;
+    std::vector<wcf> in(V), out(V);
+    COMPLEX *h = reinterpret_cast<COMPLEX *>(H);
+    for (INT j = 0; j < D; j++) {
+        std::memset(in.data(), 0, sizeof(wcf) * V);
+        const INT site = j % V, spin = (j / V) % 4, colour = j / (4 * V);
+        in[site].c[colour].f[spin] = COMPLEX(1.0, 0.0);
+        EvolutionOperator::OverlapOperator::Compute(EvolutionOperator::Ucc, in.data(), out.data(), lo, hi);
+        for (INT s = 0; s < V; s++)
+            for (INT c = 0; c < Nc; c++)
+                for (INT a = 0; a < 4; a++) h[(s + V * (a + 4 * c)) + (size_t)D * j] = COMPLEX(0.0, 1.0) * out[s].c[c].f[a];
+    }
+}
+#endif
 
 /* Observables::Bulk::Update: out[0..7] = T00, TXX, TYY, TZZ, E-part, B-part, and
  * the Gauss-law and unitarity max/avg violations (out[6..9]). */

@@ -85,6 +85,7 @@ SIGNATURES = {
     "ovl_fermion_energy": ([_ctx, _dp], C.c_int),
     "ovl_gauss_restore": ([_ctx, C.c_int, C.c_double, C.POINTER(C.c_int), _dp], C.c_int),
     "ovl_set_handmade_sphaleron": ([_ctx, C.c_double, C.c_double, _dp], C.c_int),
+    "ovl_set_qed_eigenmodes": ([_ctx, _dp, _dp, C.POINTER(C.c_int)], C.c_int),
     "ovl_set_quasi_particles": ([_ctx, C.c_double, C.c_double, C.c_uint64, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "ovl_bulk": ([_ctx, _dp], C.c_int),
     "ovl_synchronize": ([_ctx], C.c_int),

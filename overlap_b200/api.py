@@ -369,6 +369,19 @@ class Context:
         self._check(self._L.ovl_fermion_energy(self._ctx, _dp(o)))
         return float(o[0])
 
+    def set_qed_eigenmodes(self, hamiltonian: bool = False):
+        """InitialConditions::SetOverlapQEDEigenfunctions on the device: the modes
+        become eigenmodes of the overlap Hamiltonian in the context's U(1)
+        background.  Returns (eigenvalues ascending, n_bad[, h_ov [D, D]])."""
+        D = 8 * self.V
+        w = np.empty(D)
+        h = np.empty(2 * D * D) if hamiltonian else None
+        bad = C.c_int(0)
+        self._check(self._L.ovl_set_qed_eigenmodes(self._ctx, _dp(w), _dp(h) if h is not None else None, C.byref(bad)))
+        if hamiltonian:
+            return w, bad.value, h.view(np.complex128).reshape(D, D).T  # column-major -> [row, column]
+        return w, bad.value
+
     def set_quasi_particles(self, n0: float, qs: float, seed: int, gauss_max_iter: int = 10000) -> int:
         """InitialConditions::SetQuasiParticles on the device (quasi-particle links and E,
         then Gauss's law restored unless gauss_max_iter is 0); returns the restoration's

@@ -21,7 +21,7 @@ OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "libovl_b200.so"
 SOURCES = ["ovl_capi.cu", "ovl_wilson.cu", "ovl_gauge.cu", "ovl_modes.cu", "ovl_noalloc.cu", "ovl_overlap.cu",
            "ovl_chebyshev.cu", "ovl_zolotarev.cpp", "ovl_force.cu", "ovl_ritz.cu", "ovl_batch.cu",
-           "ovl_stochastic.cu", "ovl_su3.cu", "ovl_quasi.cu"]
+           "ovl_stochastic.cu", "ovl_su3.cu", "ovl_quasi.cu", "ovl_eigen.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -56,7 +56,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
             print(res.stderr, file=sys.stderr)
         objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart", "-lcusolver", "-lcublas"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stderr}")

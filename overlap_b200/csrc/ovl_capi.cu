@@ -1539,6 +1539,53 @@ int ovl_fermion_energy(ovl_ctx *c, double *out) {
     return OVL_OK;
 }
 
+int ovl_set_qed_eigenmodes(ovl_ctx *c, double *eigenvalues, double *h_ov, int *n_bad) {
+    if (!c) return OVL_E_ARG;
+    if (su3(c) || !overlap(c))
+        return fail(c, OVL_E_UNSUPPORTED, "ovl_set_qed_eigenmodes: two-colour overlap contexts only");
+    const long long D = 4LL * c->nc * c->L.V;
+    if (c->p.first_mode + (long long)c->p.n_modes > D)
+        return fail(c, OVL_E_ARG, "ovl_set_qed_eigenmodes: modes %d..%d beyond the %lld eigenmodes", c->p.first_mode,
+                    c->p.first_mode + c->p.n_modes - 1, D);
+    if (D * D > (1LL << 31)) return fail(c, OVL_E_ARG, "ovl_set_qed_eigenmodes: dense %lld x %lld beyond 2^31", D, D);
+    int rc = set_device(c);
+    if (rc) return rc;
+    const size_t stage = sizeof(double2) * (size_t)c->p.n_modes * c->L.V * c->comp;
+    double2 *a = nullptr, *b = nullptr;
+    if (cudaMalloc(&a, stage) != cudaSuccess || cudaMalloc(&b, stage) != cudaSuccess) {
+        cudaGetLastError();
+        if (a) cudaFree(a);
+        return fail(c, OVL_E_OOM, "ovl_set_qed_eigenmodes: staging");
+    }
+    int zero = 0, bad = 0;
+    const int r = ovl::qed_eigenmodes(c->u1_on ? c->u1 : nullptr, c->L, amass(c->p), c->p.m_dw, c->p.m_fermion,
+                                      c->p.dt, c->p.first_mode, c->p.n_modes, a, b, eigenvalues, h_ov, &zero, &bad,
+                                      c->sm_count, c->stream);
+    if (r == 0) {
+        const double *pa = reinterpret_cast<const double *>(a), *pb = reinterpret_cast<const double *>(b);
+        if (fp40(c)) {
+            ovl::launch_ref_to_blocks<double>(pa, c->psi, c->L, 0, c->p.n_modes, c->stream, c->psi_lo);
+            ovl::launch_ref_to_blocks<double>(pb, c->psimid, c->L, 0, c->p.n_modes, c->stream, c->psimid_lo);
+        } else if (fp32(c)) {
+            ovl::launch_ref_to_blocks<float>(pa, c->psi, c->L, 0, c->p.n_modes, c->stream);
+            ovl::launch_ref_to_blocks<float>(pb, c->psimid, c->L, 0, c->p.n_modes, c->stream);
+        } else {
+            ovl::launch_ref_to_blocks<double>(pa, c->psi, c->L, 0, c->p.n_modes, c->stream);
+            ovl::launch_ref_to_blocks<double>(pb, c->psimid, c->L, 0, c->p.n_modes, c->stream);
+        }
+        c->launches += 7;
+    }
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(a);
+    cudaFree(b);
+    if (r == 2) return fail(c, OVL_E_OOM, "ovl_set_qed_eigenmodes: dense matrices of %lld x %lld", D, D);
+    if (r == 3) return fail(c, OVL_E_NOT_CONVERGED, "ovl_set_qed_eigenmodes: diagonalisation did not converge");
+    if (r != 0) return fail(c, OVL_E_CUDA, "ovl_set_qed_eigenmodes: cuSOLVER / cuBLAS call failed");
+    if (e != cudaSuccess) return cuda_fail(c, e, "ovl_set_qed_eigenmodes");
+    if (n_bad) *n_bad = bad + zero;
+    return OVL_OK;
+}
+
 int ovl_set_handmade_sphaleron(ovl_ctx *c, double r_sphaleron, double t_sphaleron, double *u_final) {
     if (!c) return OVL_E_ARG;
     if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_set_handmade_sphaleron: two colours only");

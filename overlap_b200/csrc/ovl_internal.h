@@ -89,6 +89,13 @@ void launch_ncsdot(const double *U, const double *E, const Lattice &L, double *p
 int ncsdot_blocks_exact(const Lattice &L);
 void launch_ncsdot_into(const double *U, const double *E, const Lattice &L, int blocks, double *partial, double *out,
                         cudaStream_t stream);
+// Overlap eigenmodes in the U(1) background (ovl_eigen.cu): modes
+// [first_mode, first_mode + count) of the dense, exactly diagonalised h_ov
+// into psi_ref / mid_ref (reference layout, device); 0 on success, 1 library
+// error, 2 out of memory, 3 no convergence.
+int qed_eigenmodes(const double *u1, const Lattice &L, double amass, double mdw, double mf, double dt, int first_mode,
+                   int count, double2 *psi_ref, double2 *mid_ref, double *omega_host, double *h_host, int *zero_modes,
+                   int *bad, int sm_count, cudaStream_t stream);
 // Quasi-particle gauge fields (ovl_quasi.cu): links and E of nc colours from
 // occupancy n0 below qs, noise from `seed`; scratch holds
 // quasi_particle_scratch_bytes.

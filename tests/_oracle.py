@@ -141,5 +141,6 @@ def reference(kind: str = "wilson"):
             L.ovlref_take_bounds.argtypes = [_dp, C.c_int]
             L.ovlref_take_bounds.restype = C.c_int
             L.ovlref_last_bounds.argtypes = [_dp]
+            L.ovlref_qed_hamiltonian.argtypes = [C.c_int, _dp, _dp]
         _refs[kind] = L
     return _refs[kind]
