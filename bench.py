@@ -504,35 +504,51 @@ def ensemble_leg(steps, warmup, device, tile=0):
             "N5_finite": bool(np.all(np.isfinite(n5)))}
 
 
-def serving_leg(count, device, tile=0):
-    """The serving configuration: Poisson arrivals (mean 20/s) of trajectory
-    requests, N uniform over {8, 12, 16, 24}, 4096-8192 modes, 200-2000 steps,
-    U(1) flux n_B in {0, 2, 4, 8}, FP32 modes; a quarter SU(3), an eighth
-    overlap fermions (Chebyshev degree 64, plane waves, N = 8 and 100-200
-    steps: an overlap step costs ~130 Wilson steps); the Wilson requests on Z2
-    stochastic modes.  Admitted by device memory: Wilson requests (SU(2) and
-    SU(3)) into one continuously batched ensemble, overlap requests as contexts
-    of their own beside it; N_5, N_CS and energy streamed every 50 steps.  A fixed number of
-    requests (time-boxed: the offered load exceeds the GPU's capacity).  tile: the
-    ensemble's tile shape (16: packed-pair tiles; 0: tuned)."""
-    from overlap_b200.serve import Server, poisson_requests
+def serving_leg(count, device, tile=0, time_box=60.0):
+    """The serving configuration: `count` Poisson arrivals (mean 20/s) of
+    trajectory requests, N uniform over {8, 12, 16, 24}, 4096-8192 modes,
+    200-2000 steps, U(1) flux n_B in {0, 2, 4, 8}, FP32 modes; a quarter
+    SU(3), an eighth overlap fermions (Chebyshev degree 64, plane waves), the
+    Wilson requests on Z2 stochastic modes.  Admitted by device memory: Wilson
+    requests (SU(2) and SU(3)) into one continuously batched ensemble on the
+    stream of highest priority, overlap requests as contexts of their own
+    beside it; N_5, N_CS and energy streamed every 50 steps.  The offered load
+    is far above the GPU's capacity (one overlap step on 24^3 with 8192 modes
+    is about a second of GPU time), so the leg is time-boxed: it serves for
+    `time_box` seconds and reports the offered and the sustained load, the
+    requests completed, still running, queued and not yet arrived, and
+    latency over the completed ones.  Queued requests are admitted smallest
+    total work first, every one that fits (in arrival order two or three
+    overlap requests on 24^3 fill the memory and nothing finishes inside the
+    box).  tile: the ensemble's tile shape (16: packed-pair tiles; 0: tuned)."""
+    from overlap_b200.serve import Server, poisson_requests, request_cost
 
     reqs = poisson_requests(count, 20.0, seed=7, su3_fraction=0.25, overlap_fraction=0.125)
-    offered = sum(r.mode_sites() * r.steps for r in reqs) / max(reqs[-1].arrival, 1e-9)
-    srv = Server(precision="fp32", device=device, tick_steps=50, tile=tile)
+    window = max(reqs[-1].arrival, 1e-9)
+    offered = sum(r.mode_sites() * r.steps for r in reqs) / window
+    offered_cost = sum(request_cost(r) * r.steps for r in reqs) / window
+    srv = Server(precision="fp32", device=device, tick_steps=50, tile=tile, admission="shortest")
     try:
-        m = srv.serve(reqs)
-        streamed = sum(len(r.observables) for r in srv.done)
+        m = srv.serve(reqs, time_box=time_box)
+        streamed = sum(len(r.observables) for r in reqs)
+        done_kinds = {}
+        for r in srv.done:
+            k = f"SU({r.n_colours}) {r.fermion}"
+            done_kinds[k] = done_kinds.get(k, 0) + 1
     finally:
         srv.close()
     kinds = {}
     for r in reqs:
         k = f"SU({r.n_colours}) {r.fermion}"
         kinds[k] = kinds.get(k, 0) + 1
-    m.update({"config": f"{count} requests, Poisson 20/s, N in {{8,12,16,24}}, 4096-8192 modes, 200-2000 steps "
-                        "(overlap: N=8, 100-200 steps, Chebyshev degree 64), n_B in {0,2,4,8}, FP32, observables "
-                        "every 50 steps", "request_kinds": kinds,
-              "offered_mode_site_updates_per_s": offered, "observations_streamed": streamed})
+    m.update({"config": f"{count} requests, Poisson 20/s (arrival window {window:.1f} s), N in {{8,12,16,24}}, "
+                        "4096-8192 modes, 200-2000 steps, Wilson or overlap (Chebyshev degree 64), SU(2)/SU(3), "
+                        "n_B in {0,2,4,8}, FP32, observables every 50 steps; admission by device memory, smallest "
+                        f"work first; time-boxed at {time_box:g} s, latency over the requests completed in the box",
+              "request_kinds": kinds, "completed_kinds": done_kinds,
+              "offered_mode_site_updates_per_s": offered, "offered_wilson_equivalent_per_s": offered_cost,
+              "sustained_over_offered": m["throughput_wilson_equivalent"] / offered_cost,
+              "observations_streamed": streamed})
     return m
 
 
@@ -656,7 +672,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-su3", action="store_true", help="skip the SU(3) overlap leg")
     ap.add_argument("--su3-steps", type=int, default=3, help="timed leapfrog steps of the SU(3) overlap leg")
-    ap.add_argument("--serving-requests", type=int, default=12, help="requests of the serving leg")
+    ap.add_argument("--serving-requests", type=int, default=256, help="requests of the serving leg")
+    ap.add_argument("--serving-time-box", type=float, default=60.0, help="seconds the serving leg serves")
     ap.add_argument("--headline", choices=("fp40", "fp32"), default="fp32",
                     help="the FP32-class form of the headline value (the other is reported beside it)")
     ap.add_argument("--mode-group", type=int, default=0,
@@ -767,7 +784,8 @@ def main():
 
     srv = None
     if not args.no_serving:
-        srv = serving_leg(args.serving_requests, device, tile=16 if args.hop_variant == 3 else 0)
+        srv = serving_leg(args.serving_requests, device, tile=16 if args.hop_variant == 3 else 0,
+                          time_box=args.serving_time_box)
 
     su3 = None
     if not args.no_su3:

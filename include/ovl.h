@@ -437,7 +437,11 @@ int ovl_profile_read(ovl_ctx *ctx, double ms[OVL_PROF_KINDS], uint64_t launches[
  * counterpart: its MPI ranks split the modes of one trajectory.  Members:
  * Wilson fermions, fused form, FP32 or FP64 (one precision and device for
  * all), no coupled evolution.  Members are set up and measured through their
- * contexts (ovl_ensemble_member; do not destroy them: the ensemble owns them). */
+ * contexts (ovl_ensemble_member; do not destroy them: the ensemble owns them).
+ * The ensemble's stream is members[0].stream when not 0 (the caller keeps it
+ * alive until ovl_ensemble_destroy; a stream of high priority puts the
+ * ensemble's kernels ahead of other streams' on the GPU), else a non-blocking
+ * stream of its own; all members run on it (their own streams are ignored). */
 typedef struct ovl_ensemble ovl_ensemble;
 int ovl_ensemble_create(const ovl_params *members, int count, ovl_ensemble **out);
 int ovl_ensemble_destroy(ovl_ensemble *ens);

@@ -1051,10 +1051,14 @@ int ovl_set_stochastic_modes(ovl_ctx *c, uint64_t seed, int total_pairs) {
     if (rc) return rc;
     const int chunk = std::min(c->n_mb, 64);
     const size_t bytes = sizeof(double) * 2 * (size_t)chunk * c->L.V * c->comp * ovl::kModeBlock;
+    // stream-ordered scratch: its release does not wait for the other streams
+    // of the device (a cudaFree would), so a context set up beside running
+    // ones does not stall them
     double *a = nullptr, *b = nullptr;
-    if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess) {
+    if (cudaMallocAsync(&a, bytes, c->stream) != cudaSuccess || cudaMallocAsync(&b, bytes, c->stream) != cudaSuccess) {
         cudaGetLastError();
-        if (a) cudaFree(a);
+        if (a) cudaFreeAsync(a, c->stream);
+        cudaStreamSynchronize(c->stream);
         return fail(c, OVL_E_OOM, "ovl_set_stochastic_modes: scratch");
     }
     const int kind = fp40(c) ? 2 : fp32(c) ? 1 : 0;
@@ -1063,9 +1067,9 @@ int ovl_set_stochastic_modes(ovl_ctx *c, uint64_t seed, int total_pairs) {
                                  c->p.first_mode, amass(c->p), c->p.dt, seed, total_pairs, a, b, chunk, c->stream, &nl,
                                  c->nc);
     rc = launched(c, (int)nl, "stochastic modes");
+    cudaFreeAsync(a, c->stream);
+    cudaFreeAsync(b, c->stream);
     cudaError_t e = cudaStreamSynchronize(c->stream);
-    cudaFree(a);
-    cudaFree(b);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(c, e, "ovl_set_stochastic_modes");
     return OVL_OK;
@@ -1880,12 +1884,15 @@ struct ovl_ensemble {
     std::vector<ovl_ctx *> members;
     int device = 0;
     cudaStream_t stream = nullptr;
+    bool own_stream = false;  // created here (members[0].stream was 0)
     bool fp32 = true;
     int sites = 0;  // tile shape of the batched hop (ovl_ensemble_set_tile); 0 until tuned
     double tile_ms[OVL_ENSEMBLE_TILES] = {0.0, 0.0, 0.0};
     std::vector<ovl::BatchMember> host;  // members in group order (colours, then U(1) background)
+    std::vector<int> ts_host;             // step counters, uploaded with the descriptors
     ovl::BatchMember *dev = nullptr;
     int *dev_tsteps = nullptr;
+    size_t dev_capacity = 0;  // members dev and dev_tsteps hold (grown by doubling)
     // groups: 2 x (nc - 2) + (U(1) on): two colours without / with U(1), three colours without / with
     int groups[4] = {0, 0, 0, 0};
     int step_launches = 0;  // kernels in the captured step graph
@@ -1959,14 +1966,20 @@ void ens_describe(ovl_ensemble *e, int sites, bool tuning) {
     e->links = link;
 }
 
+// The descriptors and step counters go up from pageable host vectors: each
+// copy has been staged when cudaMemcpyAsync returns, so the vectors may change
+// at once and the host does not wait for the stream (the ensemble's earlier
+// work, or work it was made to wait for, may still be running).
 int ens_upload(ovl_ensemble *e) {
-    std::vector<int> ts(e->members.size());
-    for (size_t i = 0; i < ts.size(); i++) ts[i] = e->members[i]->tsteps;
+    e->ts_host.resize(e->members.size());
+    for (size_t i = 0; i < e->ts_host.size(); i++) e->ts_host[i] = e->members[i]->tsteps;
     cudaError_t r = cudaMemcpyAsync(e->dev, e->host.data(), sizeof(ovl::BatchMember) * e->host.size(),
                                     cudaMemcpyHostToDevice, e->stream);
     if (r == cudaSuccess)
-        r = cudaMemcpyAsync(e->dev_tsteps, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice, e->stream);
-    if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);  // ts lives on this stack frame
+        r = cudaMemcpyAsync(e->dev_tsteps, e->ts_host.data(), sizeof(int) * e->ts_host.size(),
+                            cudaMemcpyHostToDevice, e->stream);
+    if (r == cudaSuccess && (page_locked(e->host.data()) || page_locked(e->ts_host.data())))
+        r = cudaStreamSynchronize(e->stream);
     return r == cudaSuccess ? OVL_OK : ens_fail(e, OVL_E_CUDA, "ensemble: descriptor upload: %s", cudaGetErrorString(r));
 }
 
@@ -2036,8 +2049,15 @@ int ovl_ensemble_create(const ovl_params *members, int count, ovl_ensemble **out
     };
     e->device = p0.device;
     e->fp32 = p0.precision == OVL_PREC_FP32;
-    if (cudaSetDevice(e->device) != cudaSuccess || cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
-        return bail(ens_fail(e, OVL_E_CUDA, "ovl_ensemble_create: device %d / stream", e->device));
+    if (cudaSetDevice(e->device) != cudaSuccess)
+        return bail(ens_fail(e, OVL_E_CUDA, "ovl_ensemble_create: device %d", e->device));
+    if (p0.stream) {
+        e->stream = reinterpret_cast<cudaStream_t>(p0.stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(ens_fail(e, OVL_E_CUDA, "ovl_ensemble_create: stream"));
+        e->own_stream = true;
+    }
     for (int i = 0; i < count; i++) {
         ovl_params p = members[i];
         p.stream = reinterpret_cast<uint64_t>(e->stream);
@@ -2049,11 +2069,13 @@ int ovl_ensemble_create(const ovl_params *members, int count, ovl_ensemble **out
         if (rc) return bail(ens_fail(e, rc, "ovl_ensemble_create: member %d: %s", i, ovl_last_error(nullptr)));
         e->members.push_back(c);
     }
-    if (cudaMalloc(&e->dev, sizeof(ovl::BatchMember) * count) != cudaSuccess ||
-        cudaMalloc(&e->dev_tsteps, sizeof(int) * count) != cudaSuccess) {
+    const size_t cap = std::max<size_t>(16, (size_t)count);
+    if (cudaMalloc(&e->dev, sizeof(ovl::BatchMember) * cap) != cudaSuccess ||
+        cudaMalloc(&e->dev_tsteps, sizeof(int) * cap) != cudaSuccess) {
         cudaGetLastError();
         return bail(ens_fail(e, OVL_E_OOM, "ovl_ensemble_create: descriptors"));
     }
+    e->dev_capacity = cap;
     *out = e;
     return OVL_OK;
 }
@@ -2066,7 +2088,7 @@ int ovl_ensemble_destroy(ovl_ensemble *e) {
     for (ovl_ctx *c : e->members) ovl_destroy(c);
     if (e->dev) cudaFree(e->dev);
     if (e->dev_tsteps) cudaFree(e->dev_tsteps);
-    if (e->stream) cudaStreamDestroy(e->stream);
+    if (e->stream && e->own_stream) cudaStreamDestroy(e->stream);
     delete e;
     return OVL_OK;
 }
@@ -2091,23 +2113,29 @@ int ovl_ensemble_add(ovl_ensemble *e, const ovl_params *member, int *index) {
     ovl_ctx *c = nullptr;
     int rc = ovl_create(&q, &c);
     if (rc) return ens_fail(e, rc, "ovl_ensemble_add: %s", ovl_last_error(nullptr));
-    // descriptor arrays sized for the new count (the step graph bakes in
-    // their address, the count and the tiles: it is captured again)
-    ovl::BatchMember *dev = nullptr;
-    int *ts = nullptr;
+    // descriptor arrays for the new count, grown by doubling (a cudaFree
+    // waits for the whole device); the step graph bakes in their address,
+    // the count and the tiles: it is captured again
     const size_t n = e->members.size() + 1;
-    if (cudaMalloc(&dev, sizeof(ovl::BatchMember) * n) != cudaSuccess || cudaMalloc(&ts, sizeof(int) * n) != cudaSuccess) {
-        cudaGetLastError();
-        if (dev) cudaFree(dev);
-        ovl_destroy(c);
-        return ens_fail(e, OVL_E_OOM, "ovl_ensemble_add: descriptors");
-    }
     cudaStreamSynchronize(e->stream);
+    if (n > e->dev_capacity) {
+        const size_t cap = std::max(n, 2 * e->dev_capacity);
+        ovl::BatchMember *dev = nullptr;
+        int *ts = nullptr;
+        if (cudaMalloc(&dev, sizeof(ovl::BatchMember) * cap) != cudaSuccess ||
+            cudaMalloc(&ts, sizeof(int) * cap) != cudaSuccess) {
+            cudaGetLastError();
+            if (dev) cudaFree(dev);
+            ovl_destroy(c);
+            return ens_fail(e, OVL_E_OOM, "ovl_ensemble_add: descriptors");
+        }
+        cudaFree(e->dev);
+        cudaFree(e->dev_tsteps);
+        e->dev = dev;
+        e->dev_tsteps = ts;
+        e->dev_capacity = cap;
+    }
     ens_free_graph(e);
-    cudaFree(e->dev);
-    cudaFree(e->dev_tsteps);
-    e->dev = dev;
-    e->dev_tsteps = ts;
     e->members.push_back(c);
     if (index) *index = (int)n - 1;
     return OVL_OK;

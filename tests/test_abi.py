@@ -114,3 +114,39 @@ def test_poisson_requests_are_seeded_and_in_range():
     assert all(r.N[0] in (8, 12, 16, 24) and 4096 <= r.n_modes <= 8192 and 200 <= r.steps <= 2000 for r in a)
     assert all(x.arrival < y.arrival for x, y in zip(a, a[1:]))
     assert request_bytes(a[0], "fp32") < request_bytes(a[0], "fp64")
+
+
+def test_serving_requests_follow_the_stated_mix():
+    """Every kind of request (SU(2)/SU(3), Wilson/overlap) draws N from
+    {8, 12, 16, 24} and 200-2000 steps; an overlap step costs two Chebyshev
+    series of K + 1 terms in Wilson-step units."""
+    from overlap_b200.serve import Request, poisson_requests, request_cost
+    reqs = poisson_requests(256, 20.0, seed=7, su3_fraction=0.25, overlap_fraction=0.125)
+    ov = [r for r in reqs if r.fermion == "overlap"]
+    assert 16 <= len(ov) <= 48 and 40 <= sum(r.n_colours == 3 for r in reqs) <= 90
+    assert {r.N[0] for r in ov} == {8, 12, 16, 24}
+    assert min(r.steps for r in ov) >= 200 and max(r.steps for r in ov) <= 2000 and max(r.steps for r in ov) > 1000
+    assert all(r.cheb_degree == 64 for r in ov)
+    w = Request(N=(8, 8, 8), n_modes=4096, steps=1)
+    o = Request(N=(8, 8, 8), n_modes=4096, steps=1, fermion="overlap", cheb_degree=64)
+    assert request_cost(w) == 4096 * 512 and request_cost(o) / request_cost(w) == 2 * 65 * 7 / 6
+    assert request_cost(Request(N=(8, 8, 8), n_modes=4096, steps=1, n_colours=3)) == 1.5 * request_cost(w)
+
+
+def test_serving_chunks_end_at_observations_and_hold_a_bounded_gpu_time():
+    """A chunk of a group holds about tick_seconds of GPU work and at least
+    one step (an overlap request on 24^3 takes about a second per step), and
+    ends at the next observation point or last step of any request in it."""
+    from overlap_b200.serve import Request, Server
+    s = Server.__new__(Server)
+    s.rate_wilson, s.tick_seconds, s.tick_steps = 1.2e10, 0.5, 50
+    w = [Request(N=(n, n, n), n_modes=6144, steps=1000) for n in (8, 12, 16, 24)]
+    o = Request(N=(24, 24, 24), n_modes=8192, steps=1000, fermion="overlap")
+    for r in w + [o]:
+        r._step = 0
+    assert s._chunk_steps(w) == 48 and s._chunk_steps([o]) == 1
+    assert s._chunk_steps(w[:1]) == 50
+    w[2]._step = 37  # next observation in 13 steps
+    assert s._chunk_steps(w) == 13
+    w[0]._step = 990  # ten steps left
+    assert s._chunk_steps(w[:1]) == 10

@@ -71,3 +71,69 @@ def test_su3_and_overlap_requests_alongside_the_batch(precision):
         seed = f(0).seed
         assert mixed[seed].shape == alone[seed].shape
         assert same(mixed[seed], alone[seed], precision), seed
+
+
+def test_time_box_accounts_for_every_request():
+    """A time-boxed serve stops at the box: requests that finished inside it
+    are counted with their latency, the ones still running, queued or not yet
+    arrived are reported as such, and the server closes cleanly with work in
+    flight."""
+    import time
+
+    reqs = [req(0, (4, 4, 4), 32, 20, 0.0),                  # finishes early
+            req(1, (8, 8, 8), 256, 10 ** 6, 0.0),            # runs past the box
+            req(2, (8, 8, 8), 256, 10 ** 6, 0.0),            # waits for memory: queued
+            req(3, (4, 4, 4), 32, 20, 3600.0)]               # arrives after the box
+    budget = request_bytes(reqs[0], "fp32") + request_bytes(reqs[1], "fp32")
+    s = Server(precision="fp32", tick_steps=10, memory_bytes=budget)
+    try:
+        t0 = time.perf_counter()
+        m = s.serve(reqs, time_box=2.0)
+        wall = time.perf_counter() - t0
+        assert m["time_boxed"] and 2.0 <= m["wall_s"] <= wall < 30.0
+        assert m["requests"] == 1 and [r.seed for r in s.done] == [reqs[0].seed]
+        assert m["in_flight_at_end"] == 1 and m["queued_at_end"] == 1 and m["not_arrived_at_end"] == 1
+        assert m["admitted"] == 2 and m["rejected"] == 0
+        assert m["throughput"] > 0 and m["throughput_wilson_equivalent"] == m["throughput"]
+        assert len(reqs[1].observables) >= 2  # streamed while it ran
+    finally:
+        s.close()
+
+
+def test_shortest_first_admission_backfills_past_a_large_request():
+    """In arrival order a small request waits behind a large one that does not
+    fit; admitted smallest first it runs beside the request already on the
+    GPU and finishes inside the box."""
+    reqs = lambda: [req(1, (8, 8, 8), 256, 10 ** 6, 0.0),   # runs past the box
+                    req(2, (8, 8, 8), 256, 10 ** 6, 0.0),   # does not fit beside it
+                    req(0, (4, 4, 4), 32, 20, 0.01)]        # fits beside it
+    budget = request_bytes(reqs()[0], "fp32") + request_bytes(reqs()[2], "fp32")
+    out = {}
+    for admission in ("fifo", "shortest"):
+        s = Server(precision="fp32", tick_steps=10, memory_bytes=budget, admission=admission)
+        try:
+            out[admission] = s.serve(reqs(), time_box=2.0)
+        finally:
+            s.close()
+    assert out["fifo"]["requests"] == 0 and out["fifo"]["queued_at_end"] == 2
+    assert out["shortest"]["requests"] == 1 and out["shortest"]["queued_at_end"] == 1
+    assert out["shortest"]["admitted"] == 2
+
+
+def test_running_requests_share_the_gpu_time_equally():
+    """The GPU's time goes to the running requests in equal shares: two Wilson
+    requests in the batched ensemble and an overlap request of its own, all
+    running through the box, each get about a third of the chunks' time (the
+    ensemble's chunk time split between its members)."""
+    reqs = [req(0, (8, 8, 8), 256, 10 ** 6, 0.0), req(1, (6, 6, 6), 128, 10 ** 6, 0.0),
+            req(2, (4, 4, 4), 64, 10 ** 6, 0.0, fermion="overlap", cheb_degree=16)]
+    s = Server(precision="fp32", tick_steps=10, tick_seconds=0.05)
+    try:
+        m = s.serve(reqs, time_box=4.0)
+    finally:
+        s.close()
+    assert m["in_flight_at_end"] == 3 and m["requests"] == 0
+    g = np.array([r.gpu_s for r in reqs])
+    assert g.min() > 0 and g.max() < 2.0 * g.min(), g
+    assert abs(g[0] - g[1]) < 1e-9 * g[0]  # one chunk time, split between the members
+    assert 0.0 < m["gpu_busy_fraction"] <= 1.05
