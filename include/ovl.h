@@ -30,7 +30,7 @@ extern "C" {
 /* Layout version of ovl_params and of the entry points; ovl_abi_version()
  * returns the value the library was built with.  A caller compiled against
  * another version must not pass its ovl_params to the library. */
-#define OVL_ABI_VERSION 6
+#define OVL_ABI_VERSION 7
 
 typedef enum {
     OVL_OK = 0,
@@ -378,6 +378,25 @@ int ovl_set_quasi_particles(ovl_ctx *ctx, double n0, double qs, uint64_t seed, i
  * run; out = {signed max, rms} of the last violation computed (either may be
  * NULL). */
 int ovl_gauss_restore(ovl_ctx *ctx, int max_iter, double tol, int *iterations, double out[2]);
+
+/* The context's links and E written as the reference's configuration files
+ * (IO::SaveConfiguration, IO/SaveConfiguration.cpp:3-62): one line per link,
+ * z outermost, then y, x and the direction mu innermost.  Link file: "x y z
+ * mu " and the link's numbers each followed by a space (two colours: the four
+ * real parameters in the layout of ovl_set_links; three colours: the nine
+ * elements as "re im" pairs); E file: "x y z mu" and the Nc^2-1 components,
+ * each preceded by a space.  Numbers as %.15g (the reference's
+ * OUTPUT_PRECISION of 15 digits).  A NULL path skips that file.  File names
+ * are the caller's (the reference composes "UOutT<t>ID<seed>.txt"). */
+int ovl_save_configuration(ovl_ctx *ctx, const char *u_path, const char *e_path);
+
+/* IO::LoadConfiguration (IO/LoadConfiguration.cpp:3-148): reads link and E
+ * files in that format (lines in any order, blank lines skipped) into the
+ * context.  Every link must appear exactly once, inside the lattice; the
+ * reference exits when the count is wrong, this returns OVL_E_ARG naming the
+ * file and line and leaves both fields unchanged.  A NULL path skips that
+ * field.  Non-finite numbers give OVL_E_NONFINITE. */
+int ovl_load_configuration(ovl_ctx *ctx, const char *u_path, const char *e_path);
 
 /* Observables::Bulk::Update + GaussLaw + Unitarity (OBSERVABLES/BulkObservables.cpp:133-143,
  * GaussLawViolation.cpp:13-61, UnitarityViolation.cpp:13-51):

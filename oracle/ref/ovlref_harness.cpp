@@ -67,6 +67,9 @@ DOUBLE harness_time();
 #include "OBSERVABLES/GaussLawViolation.cpp"
 #include "OBSERVABLES/UnitarityViolation.cpp"
 #include "GAUSSLAWFIXING/GaussRestore.cpp"
+#include "IO/InputManagement.cpp"
+#include "IO/SaveConfiguration.cpp"
+#include "IO/LoadConfiguration.cpp"
 /* The handmade sphaleron initial condition and what it calls
  * (INITIALCONDITIONS/HandmadeSphaleron.cpp:114-170; rSphaleron is a global of
  * Simulation.cpp:168). */
@@ -355,6 +358,26 @@ void ovlref_bulk(double *out) {
     Observables::Unitarity::UpdateViolation(0, Lattice::N[0] - 1, 0, Lattice::N[1] - 1, 0, Lattice::N[2] - 1, GLinks::U);
     out[8] = Observables::Unitarity::GlobalMaxViolation;
     out[9] = Observables::Unitarity::GlobalAvgViolation;
+}
+
+/* IO::SaveConfiguration (IO/SaveConfiguration.cpp:3-62) of the current links
+ * and E, as the reference runs it: files <dir>/<uname>ID<seed>.txt and
+ * <dir>/<ename>ID<seed>.txt. */
+void ovlref_save_configuration(const char *dir, long seed, const char *uname, const char *ename) {
+    IO::OutputDirectory = std::string(dir) + "/";
+    RandomNumberGenerator::MySEED = seed;
+    IO::SaveConfiguration(uname, ename);
+}
+
+/* IO::LoadConfiguration (IO/LoadConfiguration.cpp:3-148) of <dir>/<ufile> and
+ * <dir>/<efile> into the current links and E (the files must hold every link:
+ * the reference exits otherwise). */
+void ovlref_load_configuration(const char *dir, const char *ufile, const char *efile) {
+    Dynamics::SetMetric();
+    IO::InputDirectory = std::string(dir) + "/";
+    IO::InputUFile = ufile;
+    IO::InputEFile = efile;
+    IO::LoadConfiguration(GLinks::U, EFields::E);
 }
 
 /* QED::SetConstantMagneticField (QED/QED.cpp:62-84); out = 2*N0*N1 complex. */

@@ -18,7 +18,7 @@ STATUS_NAMES = {
 }
 
 
-ABI_VERSION = 6  # OVL_ABI_VERSION of include/ovl.h
+ABI_VERSION = 7  # OVL_ABI_VERSION of include/ovl.h
 HOP_VARIANTS = 4  # OVL_HOP_VARIANTS
 ENSEMBLE_TILES = 3  # OVL_ENSEMBLE_TILES: 8, 4 and 16 (packed) sites
 
@@ -88,6 +88,8 @@ SIGNATURES = {
     "ovl_set_qed_eigenmodes": ([_ctx, _dp, _dp, C.POINTER(C.c_int)], C.c_int),
     "ovl_set_quasi_particles": ([_ctx, C.c_double, C.c_double, C.c_uint64, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "ovl_bulk": ([_ctx, _dp], C.c_int),
+    "ovl_save_configuration": ([_ctx, C.c_char_p, C.c_char_p], C.c_int),
+    "ovl_load_configuration": ([_ctx, C.c_char_p, C.c_char_p], C.c_int),
     "ovl_synchronize": ([_ctx], C.c_int),
     "ovl_device_modes": ([_ctx, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_size_t)], C.c_int),
     "ovl_set_spectral_bounds": ([_ctx, _dp, C.c_int], C.c_int),

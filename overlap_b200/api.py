@@ -413,6 +413,18 @@ class Context:
         keys = ("T00", "TXX", "TYY", "TZZ", "electric", "magnetic", "gauss_max", "gauss_avg", "unitarity_max", "unitarity_avg")
         return dict(zip(keys, o.tolist()))
 
+    def save_configuration(self, u_path=None, e_path=None):
+        """Writes the links and E as the reference's configuration text files
+        (ovl_save_configuration, IO/SaveConfiguration.cpp); None skips a file."""
+        enc = lambda q: None if q is None else str(q).encode()
+        self._check(self._L.ovl_save_configuration(self._ctx, enc(u_path), enc(e_path)))
+
+    def load_configuration(self, u_path=None, e_path=None):
+        """Reads links and E from the reference's configuration text files
+        (ovl_load_configuration, IO/LoadConfiguration.cpp); None skips a field."""
+        enc = lambda q: None if q is None else str(q).encode()
+        self._check(self._L.ovl_load_configuration(self._ctx, enc(u_path), enc(e_path)))
+
     def device_modes(self):
         psi, mid, nbytes = C.c_void_p(), C.c_void_p(), C.c_size_t()
         self._check(self._L.ovl_device_modes(self._ctx, C.byref(psi), C.byref(mid), C.byref(nbytes)))

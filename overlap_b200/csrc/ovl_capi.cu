@@ -2,7 +2,9 @@
 // transfers in the reference's layouts, and the leapfrog driver.
 
 #include <algorithm>
+#include <cctype>
 #include <cmath>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -977,6 +979,158 @@ int ovl_get_efield(ovl_ctx *c, double *efield) {
     OVL_CUDA(c, cudaMemcpyAsync(efield, c->E, sizeof(double) * c->e_comp * 3 * c->L.V, cudaMemcpyDeviceToHost,
                                 c->stream));
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return OVL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Gauge configurations as text files in the reference's format
+// (IO/SaveConfiguration.cpp:3-62, IO/LoadConfiguration.cpp:3-148): one line
+// per link, z outermost, then y, x and the direction innermost.  Numbers are
+// printed as the reference's streams print them at OUTPUT_PRECISION (the 15
+// digits of std::numeric_limits<double>::digits10, default float format),
+// which is printf's %.15g.
+
+namespace {
+
+struct FileCloser {
+    void operator()(FILE *f) const {
+        if (f) std::fclose(f);
+    }
+};
+using File = std::unique_ptr<FILE, FileCloser>;
+
+// Appends "%.15g" of v and the separator to a line buffer.
+void put_number(std::string &line, double v, const char *sep_before, const char *sep_after) {
+    char buf[40];
+    std::snprintf(buf, sizeof buf, "%s%.15g%s", sep_before, v, sep_after);
+    line += buf;
+}
+
+// Parses "x y z mu v_0 ... v_{n-1}" into the site/direction and n values;
+// false when the line holds fewer numbers.  Extra numbers are ignored, as the
+// reference's stream extraction ignores them.
+bool parse_record(const char *line, int &x, int &y, int &z, int &mu, double *v, int n) {
+    char *end = nullptr;
+    const char *q = line;
+    long coords[4];
+    for (int k = 0; k < 4; k++) {
+        coords[k] = std::strtol(q, &end, 10);
+        if (end == q) return false;
+        q = end;
+    }
+    x = (int)coords[0];
+    y = (int)coords[1];
+    z = (int)coords[2];
+    mu = (int)coords[3];
+    for (int k = 0; k < n; k++) {
+        v[k] = std::strtod(q, &end);
+        if (end == q) return false;
+        q = end;
+    }
+    return true;
+}
+
+bool blank(const char *line) {
+    for (const char *q = line; *q; q++)
+        if (!std::isspace((unsigned char)*q)) return false;
+    return true;
+}
+
+// Reads every record of `path` into dst[site][mu][n]; each link exactly once.
+int read_records(ovl_ctx *c, const char *path, int n, std::vector<double> &dst, const char *what) {
+    File f(std::fopen(path, "r"));
+    if (!f) return fail(c, OVL_E_ARG, "ovl_load_configuration: cannot open %s file %s", what, path);
+    const int V = c->L.V;
+    dst.assign((size_t)n * 3 * V, 0.0);
+    std::vector<unsigned char> seen((size_t)3 * V, 0);
+    std::vector<char> line(64 + 64 * (size_t)n);
+    std::vector<double> v(n);
+    long records = 0, lineno = 0;
+    while (std::fgets(line.data(), (int)line.size(), f.get())) {
+        lineno++;
+        const size_t len = std::strlen(line.data());
+        if (len + 1 == line.size() && line[len - 1] != '\n')
+            return fail(c, OVL_E_ARG, "ovl_load_configuration: %s file %s line %ld too long", what, path, lineno);
+        if (blank(line.data())) continue;
+        int x, y, z, mu;
+        if (!parse_record(line.data(), x, y, z, mu, v.data(), n))
+            return fail(c, OVL_E_ARG, "ovl_load_configuration: %s file %s line %ld: expected x y z mu and %d numbers",
+                        what, path, lineno, n);
+        if (x < 0 || x >= c->L.N0 || y < 0 || y >= c->L.N1 || z < 0 || z >= c->L.N2 || mu < 0 || mu > 2)
+            return fail(c, OVL_E_ARG, "ovl_load_configuration: %s file %s line %ld: link (%d %d %d %d) outside %dx%dx%d",
+                        what, path, lineno, x, y, z, mu, c->L.N0, c->L.N1, c->L.N2);
+        const size_t link = 3 * ((size_t)x + (size_t)c->L.N0 * ((size_t)y + (size_t)c->L.N1 * z)) + mu;
+        if (seen[link]++)
+            return fail(c, OVL_E_ARG, "ovl_load_configuration: %s file %s line %ld: link (%d %d %d %d) given twice", what,
+                        path, lineno, x, y, z, mu);
+        std::memcpy(&dst[link * n], v.data(), sizeof(double) * n);
+        records++;
+    }
+    if (records != 3L * V)
+        return fail(c, OVL_E_ARG, "ovl_load_configuration: %s file %s holds %ld links, the lattice %ld", what, path,
+                    records, 3L * V);
+    return OVL_OK;
+}
+
+}  // namespace
+
+int ovl_save_configuration(ovl_ctx *c, const char *u_path, const char *e_path) {
+    if (!c) return OVL_E_ARG;
+    const int V = c->L.V;
+    std::vector<double> U, E;
+    int rc;
+    if (u_path) {
+        U.resize((size_t)c->link_doubles * 3 * V);
+        if ((rc = ovl_get_links(c, U.data()))) return rc;
+    }
+    if (e_path) {
+        E.resize((size_t)c->e_comp * 3 * V);
+        if ((rc = ovl_get_efield(c, E.data()))) return rc;
+    }
+    File fu(u_path ? std::fopen(u_path, "w") : nullptr), fe(e_path ? std::fopen(e_path, "w") : nullptr);
+    if (u_path && !fu) return fail(c, OVL_E_ARG, "ovl_save_configuration: cannot write %s", u_path);
+    if (e_path && !fe) return fail(c, OVL_E_ARG, "ovl_save_configuration: cannot write %s", e_path);
+    std::string line;
+    for (int z = 0; z < c->L.N2; z++)
+        for (int y = 0; y < c->L.N1; y++)
+            for (int x = 0; x < c->L.N0; x++)
+                for (int mu = 0; mu < 3; mu++) {
+                    const size_t link = 3 * ((size_t)x + (size_t)c->L.N0 * ((size_t)y + (size_t)c->L.N1 * z)) + mu;
+                    char head[64];
+                    std::snprintf(head, sizeof head, "%d %d %d %d", x, y, z, mu);
+                    if (fu) {
+                        // SUNcGroup::IO::MatrixToString: every number followed by a space
+                        line = head;
+                        line += ' ';
+                        const double *u = &U[link * c->link_doubles];
+                        for (int k = 0; k < c->link_doubles; k++) put_number(line, u[k], "", " ");
+                        line += '\n';
+                        std::fputs(line.c_str(), fu.get());
+                    }
+                    if (fe) {
+                        line = head;
+                        const double *e = &E[link * c->e_comp];
+                        for (int a = 0; a < c->e_comp; a++) put_number(line, e[a], " ", "");
+                        line += '\n';
+                        std::fputs(line.c_str(), fe.get());
+                    }
+                }
+    if ((fu && std::ferror(fu.get())) || (fe && std::ferror(fe.get())))
+        return fail(c, OVL_E_ARG, "ovl_save_configuration: write error");
+    if ((fu && std::fclose(fu.release()) != 0) || (fe && std::fclose(fe.release()) != 0))
+        return fail(c, OVL_E_ARG, "ovl_save_configuration: write error on close");
+    return OVL_OK;
+}
+
+int ovl_load_configuration(ovl_ctx *c, const char *u_path, const char *e_path) {
+    if (!c) return OVL_E_ARG;
+    std::vector<double> U, E;
+    int rc;
+    // both files are read and checked before either field changes
+    if (u_path && (rc = read_records(c, u_path, c->link_doubles, U, "link"))) return rc;
+    if (e_path && (rc = read_records(c, e_path, c->e_comp, E, "electric field"))) return rc;
+    if (u_path && (rc = ovl_set_links(c, U.data()))) return rc;
+    if (e_path && (rc = ovl_set_efield(c, E.data()))) return rc;
     return OVL_OK;
 }
 

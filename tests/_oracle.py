@@ -132,6 +132,8 @@ def reference(kind: str = "wilson"):
         L.ovlref_set_step_count.argtypes = [C.c_int]
         L.ovlref_gauss_restore.argtypes = [_dp]
         L.ovlref_handmade_sphaleron.argtypes = [C.c_double, C.c_double, _dp, _dp, _dp]
+        L.ovlref_save_configuration.argtypes = [C.c_char_p, C.c_long, C.c_char_p, C.c_char_p]
+        L.ovlref_load_configuration.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p]
         if kind == "overlap":
             L.ovlref_ritz_bounds.argtypes = [_dp]
             L.ovlref_ritz_solve.argtypes = [_dp, C.c_double]
