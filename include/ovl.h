@@ -379,6 +379,37 @@ int ovl_set_quasi_particles(ovl_ctx *ctx, double n0, double qs, uint64_t seed, i
  * NULL). */
 int ovl_gauss_restore(ovl_ctx *ctx, int max_iter, double tol, int *iterations, double out[2]);
 
+/* Gradient-flow cooling of a copy of the context's links and the Chern-Simons
+ * calibration along it: ChernSimonsNumber::CoolingMethod's standard cooling
+ * (Cooling::CoolNSave, GRADIENTFLOW/Cooling.cpp:162-183) followed by its
+ * calibration (CoolingMethod::Calibrate -> Cooling::ContinueCooling,
+ * TOPOLOGY/CoolingMethod.cpp:168-196, Cooling.cpp:185-199).
+ *   Standard phase: the links, E = 0, cooling time and step count reset;
+ *   standard_steps steps of GradientFlow::StandardUpdate
+ *   (GRADIENTFLOW/GradientFlow.cpp:35-175), blocking to twice the lattice
+ *   spacing (LATTICE/GaugeLinks.cpp:126-153) after every step whose count is a
+ *   multiple of block_frequency 8^level while level < standard_blocking.
+ *   Calibration phase: from the cooled links, E = 0, Delta N_CS = 0, the count
+ *   and time continuing, steps of GradientFlow::CalibrationUpdate up to
+ *   standard_steps + calibration_steps in all, blocking while level <
+ *   calibration_blocking; each step adds DcTau/2 NCsDot(U, E) before and after
+ *   its link update.
+ * log (may be NULL): calibration_steps + 1 rows of 5 doubles, the rows of the
+ * reference's calibration log (Cooling.cpp:87-108): cooling time, magnetic and
+ * electric energy (Observables::Bulk at the current spacing), Delta N_CS along
+ * the calibration path so far, and the vacuum N_CS estimate
+ * (TOPOLOGY/VacuumEstimator.cpp:7-85) -- before the first step and after each.
+ * *log_rows = rows written; out = {Delta N_CS along the calibration path,
+ * cooling time at the end, blocking level at the end}; cooled_links (may be
+ * NULL; room for the context's links suffices) receives the links after the
+ * standard phase, on the lattice cooled_N (may be NULL).  The context's own
+ * links are not changed.  Each blocking needs every lattice extent >= 2 when
+ * it happens (OVL_E_ARG before anything runs otherwise).  The reference's
+ * driver calls this with block_frequency 32, standard_blocking 0 and
+ * calibration_blocking 2. */
+int ovl_cool(ovl_ctx *ctx, int standard_steps, int standard_blocking, int calibration_steps, int calibration_blocking,
+             int block_frequency, double *log, int *log_rows, double out[3], double *cooled_links, int cooled_N[3]);
+
 /* The context's links and E written as the reference's configuration files
  * (IO::SaveConfiguration, IO/SaveConfiguration.cpp:3-62): one line per link,
  * z outermost, then y, x and the direction mu innermost.  Link file: "x y z

@@ -1696,3 +1696,185 @@ void orc3_overlap_leapfrog(const orc_params *p, double *U, const double *E, doub
     }
     free(work);
 }
+
+/* ------------------------------------------------------------ cooling -- */
+/* Gradient-flow cooling and the Chern-Simons calibration, both colours
+ * (GRADIENTFLOW/GradientFlow.cpp:35-190, GRADIENTFLOW/Cooling.cpp:71-201,
+ * TOPOLOGY/CoolingMethod.cpp:168-196, TOPOLOGY/VacuumEstimator.cpp:7-85,
+ * LATTICE/GaugeLinks.cpp:126-153), Minkowski metric, aScale 1, spacing
+ * a = 2^level in every direction. */
+
+/* f(a,b,c) as the vacuum estimator reads it: the Levi-Civita symbol for two
+ * colours; for three, the reference's table written for labels 1..8 called
+ * with components 0..7 (SU3/AlgebraOperations.cpp:28-76), so only the
+ * entries with all labels <= 7 are reached. */
+static double cool_f(int nc, int a, int b, int c) {
+    const int prod = (a - b) * (a - c) * (c - b);
+    if (prod == 0) return 0.0;
+    if (nc == 2) return 0.5 * prod;
+    int t[3] = {a, b, c};
+    for (int i = 0; i < 3; i++)
+        for (int j = i + 1; j < 3; j++)
+            if (t[j] < t[i]) { int x = t[i]; t[i] = t[j]; t[j] = x; }
+    const int key = 100 * t[0] + 10 * t[1] + t[2];
+    double base = 0.0;
+    if (key == 123) base = 1.0;
+    else if (key == 147 || key == 246 || key == 257 || key == 345) base = 0.5;
+    else if (key == 156 || key == 367) base = -0.5;
+    return prod > 0 ? base : -base;
+}
+
+/* ReTrIGenU(2, U_mu(s)): 2 Re tr(i t^a U). */
+static void cool_algebra(const orc_params *p, int nc, const double *U, int s, int mu, double *A) {
+    (void)p;
+    if (nc == 2) {
+        quat q = q_load(U, s, mu);
+        for (int a = 0; a < 3; a++) A[a] = 2.0 * q_retr_ita(q, a);
+    } else {
+        m3 V = m3_load(U, s, mu);
+        for (int a = 0; a < 8; a++) A[a] = 2.0 * su3_retr_ita(&V, a);
+    }
+}
+
+double orc_vacuum_ncs(const orc_params *p, int nc, const double *U) {
+    const int V = volume(p), na = nc * nc - 1;
+    double sum = 0.0;
+    for (int s = 0; s < V; s++) {
+        double A[3][8];
+        for (int mu = 0; mu < 3; mu++) {
+            double ap[8], am[8];
+            cool_algebra(p, nc, U, s, mu, ap);
+            cool_algebra(p, nc, U, shift(p, s, mu, -1), mu, am);
+            for (int a = 0; a < na; a++) A[mu][a] = 0.5 * (ap[a] + am[a]);
+        }
+        for (int a = 0; a < na; a++)
+            for (int b = 0; b < na; b++)
+                for (int c = 0; c < na; c++) {
+                    const double f = cool_f(nc, a, b, c);
+                    if (f != 0.0) sum += 1.0 / (16.0 * M_PI * M_PI) * f * A[0][a] * A[1][b] * A[2][c];
+                }
+    }
+    return sum;
+}
+
+void orc_block_links(const orc_params *p, int nc, const double *U, double *Uout) {
+    orc_params q = *p;
+    for (int k = 0; k < 3; k++) q.N[k] = p->N[k] / 2;
+    const int Vb = volume(&q);
+    for (int s = 0; s < Vb; s++) {
+        int c[3];
+        coords_of(&q, s, c);
+        for (int mu = 0; mu < 3; mu++) {
+            int f[3] = {2 * c[0], 2 * c[1], 2 * c[2]};
+            const int s0 = site_of(p, f[0], f[1], f[2]);
+            f[mu] += 1;
+            const int s1 = site_of(p, f[0], f[1], f[2]);
+            if (nc == 2) {
+                quat u = q_mul(q_load(U, s0, mu), q_load(U, s1, mu));
+                memcpy(Uout + 4 * (mu + 3 * s), u.v, sizeof u.v);
+            } else {
+                m3 a = m3_load(U, s0, mu), b = m3_load(U, s1, mu);
+                m3 u = m3_mul(&a, &b);
+                m3_store(Uout, s, mu, &u);
+            }
+        }
+    }
+}
+
+typedef struct {
+    orc_params q;  /* the current lattice */
+    int nc;
+    double *U, *Ub, *E;
+    double a, aCube, tau, dncs;
+    int steps, blocking;
+    double *log;
+    int rows, max_rows;
+} cool_state;
+
+static size_t cool_link_doubles(int nc) { return nc == 3 ? 18 : 4; }
+
+static void cool_row(cool_state *st) {
+    const int nc = st->nc;
+    double b[10];
+    if (nc == 2) orc_bulk(&st->q, st->U, st->E, b);
+    else orc3_bulk(&st->q, st->U, st->E, b);
+    const double c = (st->a / st->aCube) * (st->a / st->aCube);  /* Bulk::SetConstants */
+    if (st->log && st->rows < st->max_rows) {
+        double *r = st->log + 5 * (size_t)st->rows;
+        r[0] = st->tau;
+        r[1] = c * b[5];
+        r[2] = c * b[4];
+        r[3] = st->dncs;
+        r[4] = orc_vacuum_ncs(&st->q, nc, st->U);
+    }
+    st->rows++;
+}
+
+static void cool_step(cool_state *st, int calibrate) {
+    const int nc = st->nc, V = volume(&st->q);
+    const double s = 0.5 / M_SQRT2, pw = pow(st->aCube, 2.0 / 3.0);
+    const double DcTau = s * s * pw;
+    const double gamma = -2.0 * st->aCube, cE = 1.0 / (st->a * st->a);
+    const double cU = -1.0 * (st->a * st->a * (s * s * pw)) / st->aCube;
+    const double cS = st->a * st->a / st->aCube;
+    memset(st->E, 0, sizeof(double) * (size_t)(nc * nc - 1) * 3 * V);
+    /* E = gamma cE^2 (staple sum): the staple routine adds -2 dt (staple sum) */
+    if (nc == 2) orc_update_efield(&st->q, st->U, st->E, -0.5 * gamma * cE * cE);
+    else orc3_update_efield(&st->q, st->U, st->E, -0.5 * gamma * cE * cE);
+    if (calibrate) st->dncs += 0.5 * DcTau * (cS * (nc == 2 ? orc_ncsdot(&st->q, st->U, st->E) : orc3_ncsdot(&st->q, st->U, st->E)));
+    if (nc == 2) orc_update_links(&st->q, st->U, st->E, -cU);
+    else orc3_update_links(&st->q, st->U, st->E, -cU);
+    if (calibrate) st->dncs += 0.5 * DcTau * (cS * (nc == 2 ? orc_ncsdot(&st->q, st->U, st->E) : orc3_ncsdot(&st->q, st->U, st->E)));
+    st->steps++;
+    st->tau += DcTau;
+}
+
+static void cool_perform(cool_state *st, int max_steps, int max_blocking, int block_frequency, int calibrate) {
+    if (calibrate) cool_row(st);
+    while (st->steps < max_steps) {
+        cool_step(st, calibrate);
+        if (calibrate) cool_row(st);
+        long long period = block_frequency;
+        for (int k = 0; k < st->blocking; k++) period *= 8;
+        if (st->steps % period == 0 && st->blocking < max_blocking) {
+            orc_block_links(&st->q, st->nc, st->U, st->Ub);
+            double *t = st->U; st->U = st->Ub; st->Ub = t;
+            for (int k = 0; k < 3; k++) st->q.N[k] /= 2;
+            st->a *= 2.0;
+            st->aCube = st->a * st->a * st->a;
+            memset(st->E, 0, sizeof(double) * (size_t)(st->nc * st->nc - 1) * 3 * volume(&st->q));
+            st->blocking++;
+        }
+    }
+}
+
+int orc_cool(const orc_params *p, int nc, const double *U0, int standard_steps, int standard_blocking,
+             int calibration_steps, int calibration_blocking, int block_frequency, double *log, int *rows,
+             double out[3], double *cooled, int cooled_N[3]) {
+    const int V = volume(p);
+    const size_t nl = cool_link_doubles(nc) * 3 * (size_t)V, ne = (size_t)(nc * nc - 1) * 3 * V;
+    cool_state st;
+    memset(&st, 0, sizeof st);
+    st.q = *p;
+    st.nc = nc;
+    st.U = malloc(sizeof(double) * nl);
+    st.Ub = malloc(sizeof(double) * nl);
+    st.E = calloc(ne, sizeof(double));
+    memcpy(st.U, U0, sizeof(double) * nl);
+    st.a = 1.0;
+    st.aCube = 1.0;
+    /* CoolNSave */
+    cool_perform(&st, standard_steps, standard_blocking, block_frequency, 0);
+    if (cooled_N) for (int k = 0; k < 3; k++) cooled_N[k] = st.q.N[k];
+    if (cooled) memcpy(cooled, st.U, sizeof(double) * cool_link_doubles(nc) * 3 * (size_t)volume(&st.q));
+    /* Calibrate: DeltaNCsCooling = 0, E zero, counters continue */
+    st.dncs = 0.0;
+    memset(st.E, 0, sizeof(double) * ne);
+    st.log = log;
+    st.max_rows = calibration_steps + 1;
+    cool_perform(&st, standard_steps + calibration_steps, calibration_blocking, block_frequency, 1);
+    if (rows) *rows = st.rows;
+    if (out) { out[0] = st.dncs; out[1] = st.tau; out[2] = st.blocking; }
+    free(st.U); free(st.Ub); free(st.E);
+    return 0;
+}

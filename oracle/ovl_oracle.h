@@ -142,6 +142,20 @@ void orc3_overlap_apply(const orc_params *p, const double *U, const double *phi,
 void orc3_overlap_leapfrog(const orc_params *p, double *U, const double *E, double *psi, double *psimid, int nmodes,
                            int *tsteps, int nsteps, int K, double eps, double lambda_max);
 
+/* Gradient-flow cooling (nc = 2 or 3): the vacuum N_CS estimate
+ * (TOPOLOGY/VacuumEstimator.cpp:7-85), blocking to twice the spacing
+ * (LATTICE/GaugeLinks.cpp:126-153, Uout on N/2), and the standard cooling then
+ * the calibration of ChernSimonsNumber::CoolingMethod (Cooling.cpp:71-201,
+ * CoolingMethod.cpp:168-196) with the rows of its calibration log:
+ * {cooling time, magnetic, electric, Delta N_CS, vacuum N_CS}; out = {Delta
+ * N_CS, final cooling time, final blocking level}; cooled = the links after
+ * the standard phase on cooled_N. */
+double orc_vacuum_ncs(const orc_params *p, int nc, const double *U);
+void orc_block_links(const orc_params *p, int nc, const double *U, double *Uout);
+int orc_cool(const orc_params *p, int nc, const double *U0, int standard_steps, int standard_blocking,
+             int calibration_steps, int calibration_blocking, int block_frequency, double *log, int *rows,
+             double out[3], double *cooled, int cooled_N[3]);
+
 #ifdef __cplusplus
 }
 #endif

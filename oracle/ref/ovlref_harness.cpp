@@ -82,6 +82,9 @@ DOUBLE rSphaleron = 6.0;
 #include "TOPOLOGY/WindingNumber.cpp"
 #include "TOPOLOGY/IntegralEstimateMethod.cpp"
 #include "INITIALCONDITIONS/HandmadeSphaleron.cpp"
+#include "GRADIENTFLOW/GradientFlow.cpp"
+#include "GRADIENTFLOW/Cooling.cpp"
+#include "TOPOLOGY/CoolingMethod.cpp"
 #include "QED/QED.cpp"
 #include "DiracAlgebra.cpp"
 #include "FERMIONS/FermionField.cpp"
@@ -378,6 +381,77 @@ void ovlref_load_configuration(const char *dir, const char *ufile, const char *e
     IO::InputUFile = ufile;
     IO::InputEFile = efile;
     IO::LoadConfiguration(GLinks::U, EFields::E);
+}
+
+/* Gradient-flow cooling of the current links with the reference's own
+ * routines: Cooling::Perform for the standard phase (CoolNSave's order: fields
+ * set up, flow reset), then the calibration phase of Cooling::ContinueCooling
+ * stepped here with GradientFlow::CalibrationUpdate, Observables::Bulk,
+ * VacuumEstimator::NCS and Block, so that every log value is kept at full
+ * precision (the reference prints them at the stream's default 6 digits).
+ * log: rows {cooling time, magnetic, electric, DeltaNCsCooling, vacuum N_CS};
+ * out = {DeltaNCsCooling, cooling time, blocking level}; cooled = the links
+ * after the standard phase, cooledN their lattice. */
+void ovlref_cool(int standard_steps, int standard_blocking, int calibration_steps, int calibration_blocking,
+                 int block_frequency, double *log, int *rows, double *out, double *cooled, int *cooledN) {
+    Dynamics::SetMetric();
+    Cooling::BlockFrequency = block_frequency;
+    Cooling::Allocate(GLinks::U);
+    Cooling::DynamicFields::BlockingNumber = 0;
+    Cooling::Setup(GLinks::U);
+    GradientFlow::Reset();
+    Cooling::Perform("ovlref_standard", standard_steps, standard_blocking, 0);
+    GaugeLinks *U = Cooling::DynamicFields::U;
+    for (int k = 0; k < 3; k++) cooledN[k] = U->N[k];
+    std::memcpy(cooled, U->Get(0, 0, 0, 0), sizeof(double) * 4 * 3 * U->N[0] * U->N[1] * U->N[2]);
+    // ContinueCooling from the cooled links (E zero), DeltaNCsCooling reset as Calibrate does
+    ChernSimonsNumber::DeltaNCsCooling = 0.0;
+    Cooling::DynamicFields::E->SetZero();
+    int n = 0;
+    auto row = [&]() {
+        Observables::Bulk::Update(Cooling::DynamicFields::U, Cooling::DynamicFields::E);
+        double *r = log + 5 * n++;
+        r[0] = GradientFlow::CoolingTime();
+        r[1] = Observables::Bulk::MAGNETIC();
+        r[2] = Observables::Bulk::ELECTRIC();
+        r[3] = ChernSimonsNumber::DeltaNCsCooling;
+        r[4] = ChernSimonsNumber::VacuumEstimator::NCS(Cooling::DynamicFields::U);
+    };
+    row();
+    const int total = standard_steps + calibration_steps;
+    while (GradientFlow::CoolingSteps < total) {
+        GradientFlow::CalibrationUpdate(Cooling::DynamicFields::U, Cooling::DynamicFields::E);
+        row();
+        if (GradientFlow::CoolingSteps % (Cooling::BlockFrequency * INT(std::pow(8, Cooling::DynamicFields::BlockingNumber))) == 0 &&
+            Cooling::DynamicFields::BlockingNumber < calibration_blocking) {
+            Block(&Cooling::DynamicFields::U);
+            Block(&Cooling::DynamicFields::E);
+            Cooling::DynamicFields::BlockingNumber++;
+        }
+    }
+    *rows = n;
+    out[0] = ChernSimonsNumber::DeltaNCsCooling;
+    out[1] = GradientFlow::CoolingTime();
+    out[2] = Cooling::DynamicFields::BlockingNumber;
+    Cooling::Cleanup();
+}
+
+/* The driver's own calibration, unchanged (Simulation.cpp:425-431:
+ * CoolingMethod::Init, Start, Calibrate) with the given schedule: the
+ * reference writes <dir>/VacuumCoolingT0ID<seed>.log at 6 digits. */
+void ovlref_cool_driver_log(const char *dir, long seed, int standard_steps, int standard_blocking,
+                            int calibration_steps, int calibration_blocking, int block_frequency) {
+    Dynamics::SetMetric();
+    IO::OutputDirectory = std::string(dir) + "/";
+    RandomNumberGenerator::MySEED = seed;
+    Cooling::BlockFrequency = block_frequency;
+    ChernSimonsNumber::CoolingMethod::StandardCoolingMaxSteps = standard_steps;
+    ChernSimonsNumber::CoolingMethod::StandardBlockingLevel = standard_blocking;
+    ChernSimonsNumber::CoolingMethod::CalibrationCoolingMaxSteps = calibration_steps;
+    ChernSimonsNumber::CoolingMethod::CalibrationBlockingLevel = calibration_blocking;
+    ChernSimonsNumber::CoolingMethod::Init();
+    ChernSimonsNumber::CoolingMethod::Start();
+    ChernSimonsNumber::CoolingMethod::Calibrate();
 }
 
 /* QED::SetConstantMagneticField (QED/QED.cpp:62-84); out = 2*N0*N1 complex. */

@@ -413,6 +413,28 @@ class Context:
         keys = ("T00", "TXX", "TYY", "TZZ", "electric", "magnetic", "gauss_max", "gauss_avg", "unitarity_max", "unitarity_avg")
         return dict(zip(keys, o.tolist()))
 
+    def cool(self, calibration_steps: int, standard_steps: int = 0, standard_blocking: int = 0,
+             calibration_blocking: int = 2, block_frequency: int = 32) -> dict:
+        """Gradient-flow cooling of a copy of the links and the Chern-Simons
+        calibration along it (ovl_cool: CoolingMethod's standard cooling, then
+        its calibration; GRADIENTFLOW/Cooling.cpp).  Returns the calibration log
+        (rows: cooling time, magnetic, electric, Delta N_CS so far, vacuum
+        N_CS), Delta N_CS along the calibration path, the final cooling time and
+        blocking level, and the links after the standard phase."""
+        log = np.empty((calibration_steps + 1, 5))
+        rows, out = C.c_int(0), np.empty(3)
+        cooled = np.empty(self.V * 3 * (18 if self.nc == 3 else 4))
+        dims = (C.c_int * 3)()
+        self._check(self._L.ovl_cool(self._ctx, int(standard_steps), int(standard_blocking), int(calibration_steps),
+                                     int(calibration_blocking), int(block_frequency), _dp(log), C.byref(rows),
+                                     _dp(out), _dp(cooled), dims))
+        Nc = tuple(dims)
+        Vc = Nc[0] * Nc[1] * Nc[2]
+        links = cooled[:Vc * 3 * (18 if self.nc == 3 else 4)]
+        links = links.view(np.complex128).reshape(Vc, 3, 9) if self.nc == 3 else links.reshape(Vc, 3, 4)
+        return {"log": log[:rows.value], "delta_ncs": float(out[0]), "cooling_time": float(out[1]),
+                "blocking": int(out[2]), "cooled_N": Nc, "cooled_links": links.copy()}
+
     def save_configuration(self, u_path=None, e_path=None):
         """Writes the links and E as the reference's configuration text files
         (ovl_save_configuration, IO/SaveConfiguration.cpp); None skips a file."""

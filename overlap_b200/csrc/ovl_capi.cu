@@ -1617,6 +1617,222 @@ int ovl_ncs_update(ovl_ctx *c, double *delta, double *total) {
     return OVL_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Gradient-flow cooling and the Chern-Simons calibration
+// (GRADIENTFLOW/GradientFlow.cpp:35-190, GRADIENTFLOW/Cooling.cpp:71-201,
+// TOPOLOGY/CoolingMethod.cpp:129-200), Minkowski metric, aScale 1, lattice
+// spacing a = 2^(blockings) in every direction.  With the reference's
+// constants a cooling step is
+//   E    = -2 aCube / a^4 (staple sum)        (UpdateElectricFields, set not added)
+//   U   <- exp(i cU E) U, cU = -a^2 s^2 aCube^(2/3) / aCube
+//   tau += s^2 aCube^(2/3),  s = SqrtDcTauOverSpacing = 0.5 / sqrt 2
+// and the calibration adds DcTau/2 NCsDot(U, E) before and after the link
+// update.  NCsDot carries a^2 / aCube and the bulk energies (a / aCube)^2 per
+// direction; with a a power of two these factors are exact.
+
+namespace {
+
+struct CoolRun {
+    ovl_ctx *c;
+    double *U, *Ub, *E;  // the cooling links, the blocking target, the flow field
+    double *vals;        // per log row: NCsDot before, after, bulk[10], vacuum
+    ovl::Lattice L;
+    double a = 1.0, aCube = 1.0;
+    int steps = 0, blocking = 0;
+    double tau = 0.0;
+    std::vector<double> row_a, row_tau;  // per log row: spacing and cooling time
+    std::vector<int> row_step;           // per log row: whether a step preceded it (its NCsDot pair)
+    int rows = 0, max_rows = 0;
+};
+
+constexpr int kCoolVals = 13;
+
+double flow_s2() {
+    const double s = 0.5 / M_SQRT2;  // GradientFlow::SqrtDcTauOverSpacing
+    return s * s;
+}
+
+int cool_record(CoolRun &r, bool after_step) {
+    ovl_ctx *c = r.c;
+    if (r.rows >= r.max_rows) return fail(c, OVL_E_ARG, "ovl_cool: log rows");
+    double *v = r.vals + (size_t)kCoolVals * r.rows;
+    if (su3(c)) ovl::su3_launch_bulk(r.U, r.E, r.L, c->partial, v + 2, c->stream);
+    else ovl::launch_bulk(r.U, r.E, r.L, c->partial, v + 2, c->stream);
+    ovl::launch_vacuum_ncs(r.U, r.L, c->nc, c->partial, v + 12, c->stream);
+    r.row_a.push_back(r.a);
+    r.row_tau.push_back(r.tau);
+    r.row_step.push_back(after_step ? 1 : 0);
+    r.rows++;
+    return launched(c, 4, "cooling observables");
+}
+
+// GradientFlow::StandardUpdate / CalibrationUpdate.
+int cool_step(CoolRun &r, bool calibrate) {
+    ovl_ctx *c = r.c;
+    const double s2 = flow_s2(), pw = std::pow(r.aCube, 2.0 / 3.0);
+    const double DcTau = s2 * pw;                       // aScale = 1
+    const double gamma = (-2.0) * r.aCube;              // MetricDeterminant = aScale = 1
+    const double cE = 1.0 / (r.a * r.a);                // gUpMetric = 1
+    const double cU = (-1.0) * (r.a * r.a * (s2 * pw)) / r.aCube;
+    const size_t n_e = (size_t)c->e_comp * 3 * r.L.V;
+    OVL_CUDA(c, cudaMemsetAsync(r.E, 0, sizeof(double) * n_e, c->stream));
+    // the staple kernels add -2 dt (staple sum): dt = -gamma cE^2 / 2
+    const double dt_e = -0.5 * gamma * cE * cE;
+    if (su3(c)) ovl::su3_launch_update_efield(r.U, r.E, r.L, dt_e, c->stream);
+    else ovl::launch_update_efield(r.U, r.E, nullptr, r.L, dt_e, c->stream);
+    double *v = r.vals + (size_t)kCoolVals * r.rows;  // the row this step's calibration values go with
+    if (calibrate) {
+        if (su3(c)) ovl::su3_launch_ncsdot(r.U, r.E, r.L, c->partial, v, c->stream);
+        else ovl::launch_ncsdot(r.U, r.E, r.L, c->partial, v, c->stream);
+    }
+    // the link kernels apply exp(-i dt E): dt = -cU
+    if (su3(c)) ovl::su3_launch_update_links(r.U, r.E, r.L, -cU, nullptr, false, c->stream);
+    else ovl::launch_update_links(r.U, r.E, r.L, -cU, c->stream);
+    if (calibrate) {
+        if (su3(c)) ovl::su3_launch_ncsdot(r.U, r.E, r.L, c->partial, v + 1, c->stream);
+        else ovl::launch_ncsdot(r.U, r.E, r.L, c->partial, v + 1, c->stream);
+    }
+    r.steps++;
+    r.tau += DcTau;
+    return launched(c, calibrate ? 7 : 3, "cooling step");
+}
+
+// Block(&U), Block(&E): links onto the lattice of twice the spacing, E zero.
+int cool_block(CoolRun &r) {
+    ovl_ctx *c = r.c;
+    ovl::Lattice Lb{r.L.N0 / 2, r.L.N1 / 2, r.L.N2 / 2, 0};
+    Lb.V = Lb.N0 * Lb.N1 * Lb.N2;
+    ovl::launch_block_links(r.U, r.L, r.Ub, Lb, c->nc, c->stream);
+    std::swap(r.U, r.Ub);
+    r.L = Lb;
+    r.a *= 2.0;
+    r.aCube = r.a * r.a * r.a;
+    OVL_CUDA(c, cudaMemsetAsync(r.E, 0, sizeof(double) * c->e_comp * 3 * r.L.V, c->stream));
+    r.blocking++;
+    return launched(c, 2, "blocking");
+}
+
+// Cooling::Perform: up to max_steps steps in all, blocking every
+// block_frequency 8^level steps while level < max_blocking; with calibrate,
+// CalibrationUpdate and a log row before the first step and after each one.
+int cool_perform(CoolRun &r, int max_steps, int max_blocking, int block_frequency, bool calibrate) {
+    int rc;
+    if (calibrate && (rc = cool_record(r, false))) return rc;
+    while (r.steps < max_steps) {
+        if ((rc = cool_step(r, calibrate))) return rc;
+        if (calibrate && (rc = cool_record(r, true))) return rc;
+        long long period = block_frequency;
+        for (int k = 0; k < r.blocking; k++) period *= 8;
+        if (r.steps % period == 0 && r.blocking < max_blocking && (rc = cool_block(r))) return rc;
+    }
+    return OVL_OK;
+}
+
+// The lattice sizes the schedule blocks at, checked before anything runs.
+int cool_check_schedule(ovl_ctx *c, int standard_steps, int standard_blocking, int total_steps,
+                        int calibration_blocking, int block_frequency) {
+    int n[3] = {c->L.N0, c->L.N1, c->L.N2}, blocking = 0;
+    for (int step = 1; step <= total_steps; step++) {
+        const int max_b = step <= standard_steps ? standard_blocking : calibration_blocking;
+        long long period = block_frequency;
+        for (int k = 0; k < blocking && period < (1LL << 40); k++) period *= 8;
+        if (step % period == 0 && blocking < max_b) {
+            if (n[0] < 2 || n[1] < 2 || n[2] < 2)
+                return fail(c, OVL_E_ARG, "ovl_cool: blocking %dx%dx%d at cooling step %d", n[0], n[1], n[2], step);
+            for (int k = 0; k < 3; k++) n[k] /= 2;
+            blocking++;
+        }
+    }
+    return OVL_OK;
+}
+
+}  // namespace
+
+int ovl_cool(ovl_ctx *c, int standard_steps, int standard_blocking, int calibration_steps, int calibration_blocking,
+             int block_frequency, double *log, int *log_rows, double out[3], double *cooled_links, int cooled_N[3]) {
+    if (!c) return OVL_E_ARG;
+    if (standard_steps < 0 || calibration_steps < 0 || standard_blocking < 0 || calibration_blocking < 0 ||
+        block_frequency < 1)
+        return fail(c, OVL_E_ARG, "ovl_cool: steps %d, %d, blocking %d, %d, block frequency %d", standard_steps,
+                    calibration_steps, standard_blocking, calibration_blocking, block_frequency);
+    if ((long long)standard_steps + calibration_steps > (1LL << 30)) return fail(c, OVL_E_ARG, "ovl_cool: steps");
+    int rc = set_device(c);
+    if (rc) return rc;
+    const int total = standard_steps + calibration_steps;
+    if ((rc = cool_check_schedule(c, standard_steps, standard_blocking, total, calibration_blocking, block_frequency)))
+        return rc;
+    const size_t n_link = (size_t)c->link_doubles * 3 * c->L.V, n_e = (size_t)c->e_comp * 3 * c->L.V;
+    CoolRun r;
+    r.c = c;
+    r.L = c->L;
+    r.max_rows = calibration_steps + 1;
+    double *mem = nullptr;
+    const size_t doubles = 2 * n_link + n_e + (size_t)kCoolVals * r.max_rows;
+    if (cudaMalloc(&mem, sizeof(double) * doubles) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, OVL_E_OOM, "ovl_cool: cooling fields");
+    }
+    auto done = [&](int status) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(mem);
+        return status;
+    };
+    r.U = mem;
+    r.Ub = mem + n_link;
+    r.E = mem + 2 * n_link;
+    r.vals = mem + 2 * n_link + n_e;
+    // CoolNSave: the hot links, E zero, counters reset, standard cooling
+    OVL_CUDA(c, cudaMemcpyAsync(r.U, c->U, sizeof(double) * n_link, cudaMemcpyDeviceToDevice, c->stream));
+    OVL_CUDA(c, cudaMemsetAsync(r.E, 0, sizeof(double) * n_e, c->stream));
+    if ((rc = cool_perform(r, standard_steps, standard_blocking, block_frequency, false))) return done(rc);
+    if (cooled_N) {
+        cooled_N[0] = r.L.N0;
+        cooled_N[1] = r.L.N1;
+        cooled_N[2] = r.L.N2;
+    }
+    if (cooled_links) {
+        if (cudaMemcpyAsync(cooled_links, r.U, sizeof(double) * c->link_doubles * 3 * r.L.V, cudaMemcpyDeviceToHost,
+                            c->stream) != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess)
+            return done(fail(c, OVL_E_CUDA, "ovl_cool: cooled links"));
+    }
+    // Calibrate: continue from the cooled links (E zero) up to both phases' steps, with the log
+    OVL_CUDA(c, cudaMemsetAsync(r.E, 0, sizeof(double) * c->e_comp * 3 * r.L.V, c->stream));
+    if ((rc = cool_perform(r, total, calibration_blocking, block_frequency, true))) return done(rc);
+    std::vector<double> h((size_t)kCoolVals * r.rows);
+    if (cudaMemcpyAsync(h.data(), r.vals, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return done(fail(c, OVL_E_CUDA, "ovl_cool: log"));
+    // rows in the reference's order: cooling time, magnetic, electric, Delta N_CS along the path, vacuum N_CS
+    double dncs = 0.0;
+    for (int k = 0; k < r.rows; k++) {
+        const double *v = &h[(size_t)kCoolVals * k];
+        const double a = r.row_a[k];
+        if (r.row_step[k]) {
+            // the step ran on the lattice of the row before any blocking that followed it
+            const double s2 = flow_s2(), aCube = a * a * a;
+            const double DcTau = s2 * std::pow(aCube, 2.0 / 3.0), cS = a * a / aCube;
+            dncs += 0.5 * DcTau * (cS * v[0]);
+            dncs += 0.5 * DcTau * (cS * v[1]);
+        }
+        const double cB = (a / (a * a * a)) * (a / (a * a * a));
+        if (log) {
+            double *row = log + 5 * (size_t)k;
+            row[0] = r.row_tau[k];
+            row[1] = cB * v[2 + 5];
+            row[2] = cB * v[2 + 4];
+            row[3] = dncs;
+            row[4] = v[12];
+        }
+    }
+    if (log_rows) *log_rows = r.rows;
+    if (out) {
+        out[0] = dncs;
+        out[1] = r.tau;
+        out[2] = r.blocking;
+    }
+    return done(OVL_OK);
+}
+
 int ovl_update_links(ovl_ctx *c, double dt_step) {
     if (!c) return OVL_E_ARG;
     int rc = set_device(c);

@@ -7,6 +7,7 @@
 
 #include "ovl_device.cuh"
 #include "ovl_internal.h"
+#include "ovl_su3.cuh"
 
 namespace ovl {
 
@@ -492,6 +493,112 @@ void launch_bulk(const double *U, const double *E, const Lattice &L, double *par
     const int nb = reduce_blocks(L.V);
     bulk_kernel<<<nb, kReduceThreads, 0, stream>>>(U, E, L, partial);
     bulk_finish_kernel<<<1, 32, 0, stream>>>(partial, nb, L, out);
+}
+
+// ------------------------------------------------------------- cooling ----
+// Blocking (LATTICE/GaugeLinks.cpp:126-153): the link of the lattice with
+// twice the spacing is the product of the two fine links it spans,
+// U'_mu(x) = U_mu(2x) U_mu(2x + mu).  Lout = L halved in every direction.
+template <int NC>
+__global__ void block_links_kernel(const double *__restrict__ U, Lattice L, double *__restrict__ Uout, Lattice Lout) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= 3 * Lout.V) return;
+    const int site = l / 3, mu = l % 3;
+    int x, y, z;
+    site_coords(Lout, site, x, y, z);
+    int c[3] = {2 * x, 2 * y, 2 * z};
+    const int s0 = site_index(L, c[0], c[1], c[2]);
+    c[mu] += 1;
+    const int s1 = site_index(L, c[0], c[1], c[2]);
+    if (NC == 2) store_link(Uout, site, mu, qmul(load_link(U, s0, mu), load_link(U, s1, mu)));
+    else store_su3(Uout, site, mu, m3_mul(load_su3(U, s0, mu), load_su3(U, s1, mu)));
+}
+
+void launch_block_links(const double *U, const Lattice &L, double *Uout, const Lattice &Lout, int nc,
+                        cudaStream_t stream) {
+    const int n = 3 * Lout.V;
+    if (nc == 3) block_links_kernel<3><<<(n + 127) / 128, 128, 0, stream>>>(U, L, Uout, Lout);
+    else block_links_kernel<2><<<(n + 127) / 128, 128, 0, stream>>>(U, L, Uout, Lout);
+}
+
+// The structure constants f(a, b, c) exactly as the vacuum estimator reads
+// them.  Two colours: (a-b)(a-c)(c-b)/2, the Levi-Civita symbol on 0..2
+// (SU2/AlgebraOperations.cpp:21-25).  Three colours: the reference's table
+// (SU3/AlgebraOperations.cpp:28-76) is written for generator labels 1..8 and
+// the estimator calls it with components 0..7, so the entries it reaches are
+// those whose three labels are all at most 7 -- f123 = 1, f147 = f246 = f257 =
+// f345 = 1/2, f156 = f367 = -1/2 -- applied to components with those numbers;
+// the sign is that of (a-b)(a-c)(c-b).
+__device__ __forceinline__ double vacuum_f(int nc, int a, int b, int c) {
+    const int prod = (a - b) * (a - c) * (c - b);
+    if (prod == 0) return 0.0;
+    const double sgn = prod > 0 ? 1.0 : -1.0;
+    if (nc == 2) return 0.5 * prod;
+    const int lo = min(a, min(b, c)), hi = max(a, max(b, c)), mid = a + b + c - lo - hi;
+    const int key = 100 * lo + 10 * mid + hi;
+    switch (key) {
+        case 123: return sgn;
+        case 147: case 246: case 257: case 345: return 0.5 * sgn;
+        case 156: case 367: return -0.5 * sgn;
+        default: return 0.0;
+    }
+}
+
+// 2 Re tr(i t^a U) of one link: ReTrIGenU(2, U) (SU2/GroupOperations.cpp:86-92,
+// SU3/GroupOperations.cpp:120-130).
+template <int NC>
+__device__ __forceinline__ void link_algebra(const double *__restrict__ U, int site, int mu, double *A) {
+    if (NC == 2) {
+        const quat q = load_link(U, site, mu);
+        A[0] = -2.0 * q.v0;
+        A[1] = -2.0 * q.v1;
+        A[2] = -2.0 * q.v2;
+    } else {
+        su3_retr_ita(load_su3(U, site, mu), A);
+        for (int a = 0; a < 8; a++) A[a] *= 2.0;
+    }
+}
+
+// ChernSimonsNumber::VacuumEstimator::NCS (TOPOLOGY/VacuumEstimator.cpp:7-85):
+// with A_mu(x) = (ReTrIGenU(2, U_mu(x)) + ReTrIGenU(2, U_mu(x - mu))) / 2,
+// sum over sites of f(a,b,c) A_x^a A_y^b A_z^c / (16 pi^2).
+template <int NC>
+__global__ void __launch_bounds__(kReduceThreads) vacuum_ncs_kernel(const double *__restrict__ U, Lattice L,
+                                                                     double *partial) {
+    constexpr int NA = NC * NC - 1;
+    __shared__ double sh[32];
+    CompSum sum;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.V; s += gridDim.x * blockDim.x) {
+        int x, y, z;
+        site_coords(L, s, x, y, z);
+        double A[3][NA];
+        for (int mu = 0; mu < 3; mu++) {
+            double ap[NA], am[NA];
+            int c[3] = {x, y, z};
+            c[mu] -= 1;
+            link_algebra<NC>(U, s, mu, ap);
+            link_algebra<NC>(U, site_index(L, c[0], c[1], c[2]), mu, am);
+            for (int a = 0; a < NA; a++) A[mu][a] = 0.5 * (ap[a] + am[a]);
+        }
+        double local = 0.0;
+        for (int a = 0; a < NA; a++)
+            for (int b = 0; b < NA; b++)
+                for (int c = 0; c < NA; c++) {
+                    const double f = vacuum_f(NC, a, b, c);
+                    if (f != 0.0) local += f * A[0][a] * A[1][b] * A[2][c];
+                }
+        sum.add(local);
+    }
+    double v[1] = {sum.value()};
+    block_reduce<1, false>(v, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v[0];
+}
+
+void launch_vacuum_ncs(const double *U, const Lattice &L, int nc, double *partial, double *out, cudaStream_t stream) {
+    const int nb = reduce_blocks(L.V);
+    if (nc == 3) vacuum_ncs_kernel<3><<<nb, kReduceThreads, 0, stream>>>(U, L, partial);
+    else vacuum_ncs_kernel<2><<<nb, kReduceThreads, 0, stream>>>(U, L, partial);
+    finish_kernel<1, false><<<1, kReduceThreads, 0, stream>>>(partial, nb, out, 1.0 / (16.0 * M_PI * M_PI));
 }
 
 }  // namespace ovl

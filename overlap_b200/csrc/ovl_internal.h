@@ -108,6 +108,12 @@ void launch_sphaleron(double *U, double *E, double *Ufinal, const Lattice &L, do
 void launch_geodesic(const double *Uold, const double *Unew, double c, double *Umid, double *Emid, const Lattice &L,
                      cudaStream_t stream);
 size_t bulk_partial_doubles(const Lattice &L);
+// Gradient-flow cooling (GRADIENTFLOW/Cooling.cpp): blocking to twice the
+// spacing and the vacuum N_CS estimate; both colours; the estimate needs
+// ncsdot_partial_doubles of partial.
+void launch_block_links(const double *U, const Lattice &L, double *Uout, const Lattice &Lout, int nc,
+                        cudaStream_t stream);
+void launch_vacuum_ncs(const double *U, const Lattice &L, int nc, double *partial, double *out, cudaStream_t stream);
 // Gauss-law restoration: violation G[3V] with out[0] = sum G^2, out[1] = signed
 // max; then E_mu -= gamma (G - U G(x+mu) U^+).
 size_t gauss_partial_doubles(const Lattice &L);

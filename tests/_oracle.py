@@ -91,6 +91,12 @@ def oracle():
                                             C.c_double, C.c_int]
         L.orc_chebyshev_coeffs.argtypes = [C.c_int, C.c_double, _dp]
         L.orc_handmade_sphaleron.argtypes = [P, C.c_double, C.c_double, _dp, _dp, _dp, _dp]
+        L.orc_vacuum_ncs.argtypes = [P, C.c_int, _dp]
+        L.orc_vacuum_ncs.restype = C.c_double
+        L.orc_block_links.argtypes = [P, C.c_int, _dp, _dp]
+        L.orc_cool.argtypes = [P, C.c_int, _dp] + [C.c_int] * 5 + [_dp, C.POINTER(C.c_int), _dp, _dp,
+                                                                   C.POINTER(C.c_int)]
+        L.orc_cool.restype = C.c_int
         L.orc3_overlap_apply.argtypes = [P, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double]
         L.orc3_overlap_leapfrog.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int,
                                             C.c_double, C.c_double]
@@ -134,6 +140,8 @@ def reference(kind: str = "wilson"):
         L.ovlref_handmade_sphaleron.argtypes = [C.c_double, C.c_double, _dp, _dp, _dp]
         L.ovlref_save_configuration.argtypes = [C.c_char_p, C.c_long, C.c_char_p, C.c_char_p]
         L.ovlref_load_configuration.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p]
+        L.ovlref_cool.argtypes = [C.c_int] * 5 + [_dp, C.POINTER(C.c_int), _dp, _dp, C.POINTER(C.c_int)]
+        L.ovlref_cool_driver_log.argtypes = [C.c_char_p, C.c_long] + [C.c_int] * 5
         if kind == "overlap":
             L.ovlref_ritz_bounds.argtypes = [_dp]
             L.ovlref_ritz_solve.argtypes = [_dp, C.c_double]

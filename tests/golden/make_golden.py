@@ -6,7 +6,7 @@ seeded inputs and stores inputs and outputs.  The fixtures pin the oracle
 restatement (tests/test_oracle_pin.py) and the GPU path (tests/test_gpu_*.py)
 on machines without the reference.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case names]
 """
 from __future__ import annotations
 
@@ -111,16 +111,41 @@ def run_gauss_case(name: str, c: dict) -> dict:
     return dict(N=np.array(N), links=U, efield=E, efield_restored=E1, max_violation=out[0], avg_violation=out[1])
 
 
+# Gradient-flow cooling and the Chern-Simons calibration (GRADIENTFLOW/Cooling.cpp,
+# TOPOLOGY/CoolingMethod.cpp) with blocking in both phases: block_frequency 2 blocks
+# the standard phase at step 2 and the calibration phase at step 16.
+COOL_CASES = {"cooling_n8": dict(N=(8, 8, 8), link_sigma=0.6, seed=41, standard_steps=3, standard_blocking=1,
+                                 calibration_steps=20, calibration_blocking=2, block_frequency=2)}
+
+
+def run_cool_case(name: str, c: dict) -> dict:
+    import ctypes as C
+
+    R = reference("wilson")
+    N = c["N"]
+    R.ovlref_init(*N, 1, 0, 0.1, 1.0, 0.0, 6.0, 0.05, 1.0, 1)
+    U = random_links(N, c["link_sigma"], c["seed"])
+    R.ovlref_set_links(ptr(U))
+    log = np.zeros((c["calibration_steps"] + 1, 5))
+    rows, out, cooled, cn = C.c_int(0), np.zeros(3), np.zeros_like(U), (C.c_int * 3)()
+    R.ovlref_cool(c["standard_steps"], c["standard_blocking"], c["calibration_steps"], c["calibration_blocking"],
+                  c["block_frequency"], ptr(log), C.byref(rows), ptr(out), ptr(cooled), cn)
+    Nc = tuple(cn)
+    return dict(N=np.array(N), links=U, schedule=np.array([c[k] for k in ("standard_steps", "standard_blocking",
+                                                                           "calibration_steps", "calibration_blocking",
+                                                                           "block_frequency")]),
+                log=log[:rows.value], out=out, cooled_N=np.array(Nc),
+                cooled=cooled.reshape(-1)[:4 * 3 * Nc[0] * Nc[1] * Nc[2]].reshape(-1, 3, 4))
+
+
+RUNNERS = [(CASES, run_case), (RITZ_CASES, run_ritz_case), (GAUSS_CASES, run_gauss_case), (COOL_CASES, run_cool_case)]
+
 if __name__ == "__main__":
-    for name, c in CASES.items():
-        out = HERE / f"{name}.npz"
-        np.savez_compressed(out, **run_case(name, c))
-        print(out, out.stat().st_size, "bytes")
-    for name, c in RITZ_CASES.items():
-        out = HERE / f"{name}.npz"
-        np.savez_compressed(out, **run_ritz_case(name, c))
-        print(out, out.stat().st_size, "bytes")
-    for name, c in GAUSS_CASES.items():
-        out = HERE / f"{name}.npz"
-        np.savez_compressed(out, **run_gauss_case(name, c))
-        print(out, out.stat().st_size, "bytes")
+    only = set(sys.argv[1:])  # case names to (re)generate; all when none are given
+    for cases, run in RUNNERS:
+        for name, c in cases.items():
+            if only and name not in only:
+                continue
+            out = HERE / f"{name}.npz"
+            np.savez_compressed(out, **run(name, c))
+            print(out, out.stat().st_size, "bytes")
