@@ -85,8 +85,9 @@ typedef struct {
     /* OVL_SIGN_ZOLOTAREV (the reference's rational approximation, FP64) or
      * OVL_SIGN_CHEBYSHEV: (h_W^2)^(-1/2) as a degree-cheb_degree Chebyshev
      * series of x^(-1/2) on [cheb_eps, 1] after scaling h_W^2 by lambda_max
-     * (FP32 or FP64).  Without a bounds schedule (and, for two colours, without
-     * ritz_auto) lambda_max = (|6r + 2m - 2M|/2 + 3)^2, a bound on h_W^2 for every
+     * (FP32 or FP64).  With ritz_auto lambda_max = 1.05 times the Ritz estimate
+     * (ovl_ritz_bounds) before every application; without a bounds schedule or
+     * ritz_auto lambda_max = (|6r + 2m - 2M|/2 + 3)^2, a bound on h_W^2 for every
      * gauge field.  Three colours: Chebyshev only. */
     int sign_method;
     int cheb_degree;
@@ -234,7 +235,9 @@ int ovl_zolotarev(double lambda_min, double lambda_max, double tol, int npoles, 
  * vector of the reference's distribution from the context's generator).
  * out = {MinEValue, MaxEValue} = {0.95 lambda_min, 1.05 lambda_max};
  * raw = {lambda_min, lambda_max} and iters = iterations per problem when not
- * NULL.  Works for both fermion kinds (the Wilson kernel of the context). */
+ * NULL.  Works for both fermion kinds (the Wilson kernel of the context) and
+ * both colour counts (the reference's solver is written for two; for three
+ * the same iteration runs on the three-colour h_W^2, start [V][3][4]). */
 int ovl_ritz_bounds(ovl_ctx *ctx, const double *start, double out[2], double raw[2], int iters[2]);
 
 /* Statistics of the last overlap application.  Zolotarev: out[0] = lockstep

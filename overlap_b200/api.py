@@ -344,14 +344,14 @@ class Context:
     def ritz_bounds(self, start: np.ndarray | None = None) -> dict:
         """ComputeRitzEigenvalues on the GPU: {"bounds": (MinEValue, MaxEValue),
         "raw": (lambda_min, lambda_max), "iters": (n_min, n_max)}; start is one
-        mode [V, 2, 4] complex (None: drawn from the context's generator)."""
+        mode [V, Nc, 4] complex (None: drawn from the context's generator)."""
         out, raw = np.empty(2), np.empty(2)
         it = (C.c_int * 2)()
         sp = None
         if start is not None:
             start = np.ascontiguousarray(start, dtype=np.complex128)
-            if start.size != 8 * volume(self.params.N):
-                raise ValueError("start must hold one mode (V x 2 x 4 complex)")
+            if start.size != 4 * self.nc * volume(self.params.N):
+                raise ValueError(f"start must hold one mode (V x {self.nc} x 4 complex)")
             sp = _dp(start.view(np.float64))
         self._check(self._L.ovl_ritz_bounds(self._ctx, sp, _dp(out), _dp(raw), it))
         return {"bounds": (float(out[0]), float(out[1])), "raw": (float(raw[0]), float(raw[1])),

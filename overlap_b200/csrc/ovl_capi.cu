@@ -196,8 +196,8 @@ double wilson_norm_bound2(const ovl_params &p) {
 // MaxEValue = 1.05 lambda_max, with MaximumIterations 2000, NumberOfRestarts 100,
 // NormRatio 1e-16 (:53-58).
 int ritz_bounds(ovl_ctx *c, const double *start, double out[2], double raw[2], int iters[2]) {
-    if (!c->ritz && !(c->ritz = ovl::ritz_create(c->L.V))) return fail(c, OVL_E_OOM, "Ritz solver: work space");
-    const size_t n = (size_t)c->L.V * ovl::kComp;
+    if (!c->ritz && !(c->ritz = ovl::ritz_create(c->L.V, c->nc))) return fail(c, OVL_E_OOM, "Ritz solver: work space");
+    const size_t n = (size_t)c->L.V * 4 * c->nc;
     if (start)
         OVL_CUDA(c, cudaMemcpyAsync(ovl::ritz_start_buffer(c->ritz), start, sizeof(double2) * n, cudaMemcpyHostToDevice,
                                     c->stream));
@@ -234,7 +234,7 @@ int ritz_bounds(ovl_ctx *c, const double *start, double out[2], double raw[2], i
 int take_bounds(ovl_ctx *c, bool consume, double &lo, double &hi) {
     // the Chebyshev series without a schedule or Ritz bounds: on [eps, 1] of
     // h^2 / (the bound on h_W^2 that holds for every gauge field)
-    if (c->bounds.empty() && c->p.sign_method == OVL_SIGN_CHEBYSHEV && (su3(c) || !c->p.ritz_auto)) {
+    if (c->bounds.empty() && c->p.sign_method == OVL_SIGN_CHEBYSHEV && !c->p.ritz_auto) {
         hi = wilson_norm_bound2(c->p);
         lo = c->p.cheb_eps * hi;
         return OVL_OK;
@@ -725,9 +725,6 @@ int ovl_create(const ovl_params *p, ovl_ctx **out) {
             return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: three-colour overlap fermions use the Chebyshev sign function");
         if (p->precision == OVL_PREC_FP40)
             return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: FP40 storage is built for two colours");
-        if (p->ritz_auto)
-            return fail(nullptr, OVL_E_UNSUPPORTED, "ovl_create: three colours take spectral bounds from "
-                                                    "ovl_set_spectral_bounds or the analytic bound, not ritz_auto");
     }
     if (p->fermion != OVL_FERMION_WILSON && p->fermion != OVL_FERMION_OVERLAP)
         return fail(nullptr, OVL_E_ARG, "ovl_create: fermion kind %d", p->fermion);
@@ -2093,7 +2090,6 @@ int ovl_launch_count(const ovl_ctx *c, uint64_t *count) {
 
 int ovl_ritz_bounds(ovl_ctx *c, const double *start, double out[2], double raw[2], int iters[2]) {
     if (!c || !out) return OVL_E_ARG;
-    if (su3(c)) return fail(c, OVL_E_UNSUPPORTED, "ovl_ritz_bounds: built for two colours");
     int rc = set_device(c);
     if (rc) return rc;
     return ritz_bounds(c, start, out, raw, iters);

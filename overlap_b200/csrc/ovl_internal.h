@@ -150,7 +150,7 @@ void launch_fermion_energy(const void *psi, const void *dpsi, const Lattice &L, 
 // Ritz solver for the overlap spectral bounds (ovl_ritz.cu): work space for a
 // lattice of V sites, the start vector buffer (compact [V][8] double2), a
 // seeded uniform start vector, and the run: out = {lambda_min, -lambda_max}.
-void *ritz_create(int V);
+void *ritz_create(int V, int nc);
 void ritz_destroy(void *work);
 double2 *ritz_start_buffer(void *work);
 void launch_ritz_random_start(void *work, uint64_t seed, uint64_t call, cudaStream_t stream);

@@ -9,7 +9,8 @@
 // 2x2 Rayleigh-Ritz, and a new search direction p = g + beta (p - x <x, p>).
 //
 // Both problems run together, one per blockIdx.y, on vectors in a compact
-// layout [problem][site][colour * 4 + spin] (double2): one thread per site.
+// layout [problem][site][colour * 4 + spin] (double2): one thread per site;
+// NCOMP = 4 Nc components per site (two or three colours).
 // Each step is a fixed sequence of kernels; every dot product is reduced per
 // CTA into a partial buffer and the next kernel adds the partials in a fixed
 // order (every CTA computes bit-identical scalars, so all take the same
@@ -22,6 +23,7 @@
 
 #include "ovl_internal.h"
 #include "ovl_stencil.cuh"
+#include "ovl_su3.cuh"
 
 namespace ovl {
 
@@ -112,10 +114,11 @@ __device__ __forceinline__ double *part_of(double *base, int slot, int prob, int
     return base + ((size_t)slot * 2 + prob) * nblocks * kRitzParts;
 }
 
-// <a, b> = sum conj(a) b over the 8 components of one site
+// <a, b> = sum conj(a) b over the NCOMP components of one site
+template <int NCOMP>
 __device__ __forceinline__ void site_dot(const double2 *a, const double2 *b, double &re, double &im) {
 #pragma unroll
-    for (int k = 0; k < kComp; k++) {
+    for (int k = 0; k < NCOMP; k++) {
         const double2 u = a[k], w = b[k];
         re += u.x * w.x + u.y * w.y;
         im += u.x * w.y - u.y * w.x;
@@ -123,15 +126,16 @@ __device__ __forceinline__ void site_dot(const double2 *a, const double2 *b, dou
 }
 
 // x = start for both problems; partial |x|^2 -> slot 0
+template <int NCOMP>
 __global__ void __launch_bounds__(kRitzThreads)
     ritz_start_kernel(const double2 *__restrict__ start, double2 *x, int V, RitzArgs a, double *part) {
     const int prob = blockIdx.y, site = blockIdx.x * kRitzThreads + threadIdx.x;
     double v[kRitzParts] = {0.0, 0.0, 0.0, 0.0};
     if (site < V) {
-        double2 *xs = x + ((size_t)prob * V + site) * kComp;
+        double2 *xs = x + ((size_t)prob * V + site) * NCOMP;
 #pragma unroll
-        for (int k = 0; k < kComp; k++) {
-            const double2 s = start[(size_t)site * kComp + k];
+        for (int k = 0; k < NCOMP; k++) {
+            const double2 s = start[(size_t)site * NCOMP + k];
             xs[k] = s;
             v[0] += s.x * s.x + s.y * s.y;
         }
@@ -140,6 +144,7 @@ __global__ void __launch_bounds__(kRitzThreads)
 }
 
 // x /= |x| (slot 0)
+template <int NCOMP>
 __global__ void __launch_bounds__(kRitzThreads)
     ritz_scale_x_kernel(double2 *x, int V, RitzArgs a, double *part) {
     const int prob = blockIdx.y, site = blockIdx.x * kRitzThreads + threadIdx.x;
@@ -147,67 +152,92 @@ __global__ void __launch_bounds__(kRitzThreads)
     reduce_partials(part_of(part, 0, prob, a.nblocks), a.nblocks, 1, r);
     const double s = 1.0 / sqrt(r[0]);
     if (site < V) {
-        double2 *xs = x + ((size_t)prob * V + site) * kComp;
+        double2 *xs = x + ((size_t)prob * V + site) * NCOMP;
 #pragma unroll
-        for (int k = 0; k < kComp; k++) xs[k] = make_double2(xs[k].x * s, xs[k].y * s);
+        for (int k = 0; k < NCOMP; k++) xs[k] = make_double2(xs[k].x * s, xs[k].y * s);
     }
 }
 
 // SECOND = false: dst = D src.  SECOND = true: dst = -sign D src (= sign A v
 // when src = D v) and partials <da, dst> (k = 0, 1) and <db, dst> (k = 2, 3,
-// when db is set) -> slot 0.
-template <bool U1, bool SECOND>
+// when db is set) -> slot 0.  NC colours: the two-colour stencil of
+// ovl_stencil.cuh or the three-colour one of ovl_su3.cuh on the compact layout.
+template <int NC, bool U1, bool SECOND, class LK>
 __global__ void __launch_bounds__(kRitzThreads)
-    ritz_apply_kernel(LinksF64<U1> lk, const double2 *__restrict__ src, double2 *__restrict__ dst,
+    ritz_apply_kernel(LK lk, const double2 *__restrict__ src, double2 *__restrict__ dst,
                       const double2 *__restrict__ da, const double2 *__restrict__ db, Lattice L, double amass,
                       const RitzScalars *__restrict__ st, RitzArgs a, double *part) {
+    constexpr int NCOMP = 4 * NC;
     const int prob = blockIdx.y, site = blockIdx.x * kRitzThreads + threadIdx.x;
     if (ritz_stopped(st, prob)) return;
     const int V = L.V;
     const size_t off = (size_t)prob * V;
     double v[kRitzParts] = {0.0, 0.0, 0.0, 0.0};
     if (site < V) {
-        const double2 *s = src + off * kComp;
+        const double2 *s = src + off * NCOMP;
         const Nbrs n = neighbours(L, site);
-        Spinor<double> acc, f;
-        load_compact(s, site, f);
-#pragma unroll
-        for (int c = 0; c < kColours; c++)
-#pragma unroll
-            for (int s2 = 0; s2 < kSpin; s2++) acc.c[c][s2] = amass * f.c[c][s2];
-        load_compact(s, n.xp, f);
-        hop<double, 0, true>(acc, f, lk.template get<double>(site, 0));
-        load_compact(s, n.xm, f);
-        hop<double, 0, false>(acc, f, lk.template get<double>(n.xm, 0));
-        load_compact(s, n.yp, f);
-        hop<double, 1, true>(acc, f, lk.template get<double>(site, 1));
-        load_compact(s, n.ym, f);
-        hop<double, 1, false>(acc, f, lk.template get<double>(n.ym, 1));
-        load_compact(s, n.zp, f);
-        hop<double, 2, true>(acc, f, lk.template get<double>(site, 2));
-        load_compact(s, n.zm, f);
-        hop<double, 2, false>(acc, f, lk.template get<double>(n.zm, 2));
         const double scale = SECOND ? -a.sign[prob] : 1.0;
-        double2 o[kComp];
+        double2 o[NCOMP];
+        if constexpr (NC == 2) {
+            Spinor<double> acc, f;
+            load_compact(s, site, f);
 #pragma unroll
-        for (int c = 0; c < kColours; c++)
+            for (int c = 0; c < kColours; c++)
 #pragma unroll
-            for (int s2 = 0; s2 < kSpin; s2++) {
-                const cpx<double> r = finish_component(acc.c[c][s2], s2);
-                o[c * kSpin + s2] = make_double2(scale * r.re, scale * r.im);
-            }
-        double2 *d = dst + (off + site) * kComp;
+                for (int s2 = 0; s2 < kSpin; s2++) acc.c[c][s2] = amass * f.c[c][s2];
+            load_compact(s, n.xp, f);
+            hop<double, 0, true>(acc, f, lk.template get<double>(site, 0));
+            load_compact(s, n.xm, f);
+            hop<double, 0, false>(acc, f, lk.template get<double>(n.xm, 0));
+            load_compact(s, n.yp, f);
+            hop<double, 1, true>(acc, f, lk.template get<double>(site, 1));
+            load_compact(s, n.ym, f);
+            hop<double, 1, false>(acc, f, lk.template get<double>(n.ym, 1));
+            load_compact(s, n.zp, f);
+            hop<double, 2, true>(acc, f, lk.template get<double>(site, 2));
+            load_compact(s, n.zm, f);
+            hop<double, 2, false>(acc, f, lk.template get<double>(n.zm, 2));
 #pragma unroll
-        for (int k = 0; k < kComp; k++) d[k] = o[k];
+            for (int c = 0; c < kColours; c++)
+#pragma unroll
+                for (int s2 = 0; s2 < kSpin; s2++) {
+                    const cpx<double> r = finish_component(acc.c[c][s2], s2);
+                    o[c * kSpin + s2] = make_double2(scale * r.re, scale * r.im);
+                }
+        } else {
+            const cpx<double> *f = reinterpret_cast<const cpx<double> *>(s);
+            Spinor3<double> acc;
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int s2 = 0; s2 < kSpin; s2++) acc.c[c][s2] = amass * ld(f + (size_t)site * NCOMP + c * kSpin + s2);
+            hop3<double, 0, true, false, 1>(acc, f + (size_t)n.xp * NCOMP, lk.template get<double>(site, 0));
+            hop3<double, 0, false, false, 1>(acc, f + (size_t)n.xm * NCOMP, lk.template get<double>(n.xm, 0));
+            hop3<double, 1, true, false, 1>(acc, f + (size_t)n.yp * NCOMP, lk.template get<double>(site, 1));
+            hop3<double, 1, false, false, 1>(acc, f + (size_t)n.ym * NCOMP, lk.template get<double>(n.ym, 1));
+            hop3<double, 2, true, false, 1>(acc, f + (size_t)n.zp * NCOMP, lk.template get<double>(site, 2));
+            hop3<double, 2, false, false, 1>(acc, f + (size_t)n.zm * NCOMP, lk.template get<double>(n.zm, 2));
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int s2 = 0; s2 < kSpin; s2++) {
+                    const cpx<double> r = finish_component(acc.c[c][s2], s2);
+                    o[c * kSpin + s2] = make_double2(scale * r.re, scale * r.im);
+                }
+        }
+        double2 *d = dst + (off + site) * NCOMP;
+#pragma unroll
+        for (int k = 0; k < NCOMP; k++) d[k] = o[k];
         if (SECOND) {
-            site_dot(da + (off + site) * kComp, o, v[0], v[1]);
-            if (db) site_dot(db + (off + site) * kComp, o, v[2], v[3]);
+            site_dot<NCOMP>(da + (off + site) * NCOMP, o, v[0], v[1]);
+            if (db) site_dot<NCOMP>(db + (off + site) * NCOMP, o, v[2], v[3]);
         }
     }
     if (SECOND) block_partials(v, 4, part_of(part, 0, prob, a.nblocks) + (size_t)blockIdx.x * kRitzParts);
 }
 
 // Restart (RitzSolver.cpp:138-166): xy = <x, y>; g = p = y - xy x; |g|^2 -> slot 1.
+template <int NCOMP>
 __global__ void __launch_bounds__(kRitzThreads)
     ritz_restart_kernel(const double2 *__restrict__ x, const double2 *__restrict__ y, double2 *__restrict__ g,
                         double2 *__restrict__ praw, int V, RitzScalars *st, RitzArgs a, double *part) {
@@ -222,9 +252,9 @@ __global__ void __launch_bounds__(kRitzThreads)
     }
     double v[kRitzParts] = {0.0, 0.0, 0.0, 0.0};
     if (site < V) {
-        const size_t o = ((size_t)prob * V + site) * kComp;
+        const size_t o = ((size_t)prob * V + site) * NCOMP;
 #pragma unroll
-        for (int k = 0; k < kComp; k++) {
+        for (int k = 0; k < NCOMP; k++) {
             const double2 xv = x[o + k], yv = y[o + k];
             const double2 gv = make_double2(yv.x - (xr * xv.x - xi * xv.y), yv.y - (xr * xv.y + xi * xv.x));
             g[o + k] = gv;
@@ -237,6 +267,7 @@ __global__ void __launch_bounds__(kRitzThreads)
 
 // p = praw / |praw| (slot 1); pnorm; gnormim = |praw|^2 on a restart (p = g
 // there), else the gnorm of this step.
+template <int NCOMP>
 __global__ void __launch_bounds__(kRitzThreads)
     ritz_normp_kernel(const double2 *__restrict__ praw, double2 *__restrict__ p, int V, int restart, RitzScalars *st,
                       RitzArgs a, const double *part) {
@@ -250,14 +281,15 @@ __global__ void __launch_bounds__(kRitzThreads)
         st[prob].gnormim = restart ? r[0] : st[prob].gnorm;
     }
     if (site < V) {
-        const size_t o = ((size_t)prob * V + site) * kComp;
+        const size_t o = ((size_t)prob * V + site) * NCOMP;
 #pragma unroll
-        for (int k = 0; k < kComp; k++) p[o + k] = make_double2(praw[o + k].x / pn, praw[o + k].y / pn);
+        for (int k = 0; k < NCOMP; k++) p[o + k] = make_double2(praw[o + k].x / pn, praw[o + k].y / pn);
     }
 }
 
 // The rotation of x in the (x, p) plane (RitzSolver.cpp:176-222), from slot 0:
 // pz = Re <p, z>, xz = Re <x, z>.  Then <x, x>, <x, y> -> slot 1.
+template <int NCOMP>
 __global__ void __launch_bounds__(kRitzThreads)
     ritz_rotate_kernel(double2 *x, double2 *y, const double2 *__restrict__ p, const double2 *__restrict__ z, int V,
                        RitzScalars *st, RitzArgs a, double *part) {
@@ -300,10 +332,10 @@ __global__ void __launch_bounds__(kRitzThreads)
     }
     double v[kRitzParts] = {0.0, 0.0, 0.0, 0.0};
     if (site < V) {
-        const size_t o = ((size_t)prob * V + site) * kComp;
-        double2 xn[kComp], yn[kComp];
+        const size_t o = ((size_t)prob * V + site) * NCOMP;
+        double2 xn[NCOMP], yn[NCOMP];
 #pragma unroll
-        for (int k = 0; k < kComp; k++) {
+        for (int k = 0; k < NCOMP; k++) {
             const double2 xv = x[o + k], pv = p[o + k], yv = y[o + k], zv = z[o + k];
             xn[k] = make_double2(xv.x * ct + pv.x * sn, xv.y * ct + pv.y * sn);
             yn[k] = make_double2(yv.x * ct + zv.x * sn, yv.y * ct + zv.y * sn);
@@ -311,14 +343,15 @@ __global__ void __launch_bounds__(kRitzThreads)
             y[o + k] = yn[k];
         }
         double im0 = 0.0;
-        site_dot(xn, xn, v[0], im0);
-        site_dot(xn, yn, v[1], v[2]);
+        site_dot<NCOMP>(xn, xn, v[0], im0);
+        site_dot<NCOMP>(xn, yn, v[1], v[2]);
     }
     block_partials(v, 3, part_of(part, 1, prob, a.nblocks) + (size_t)blockIdx.x * kRitzParts);
 }
 
 // x normalised, xy = <x, y> / |x|, g = y - xy x (RitzSolver.cpp:224-243), from
 // slot 1.  Then |g|^2, <x, p> -> slot 0.
+template <int NCOMP>
 __global__ void __launch_bounds__(kRitzThreads)
     ritz_residual_kernel(double2 *x, const double2 *__restrict__ y, double2 *__restrict__ g,
                          const double2 *__restrict__ p, int V, RitzScalars *st, RitzArgs a, double *part) {
@@ -334,10 +367,10 @@ __global__ void __launch_bounds__(kRitzThreads)
     }
     double v[kRitzParts] = {0.0, 0.0, 0.0, 0.0};
     if (site < V) {
-        const size_t o = ((size_t)prob * V + site) * kComp;
-        double2 xn[kComp], gn[kComp];
+        const size_t o = ((size_t)prob * V + site) * NCOMP;
+        double2 xn[NCOMP], gn[NCOMP];
 #pragma unroll
-        for (int k = 0; k < kComp; k++) {
+        for (int k = 0; k < NCOMP; k++) {
             const double2 xv = x[o + k], yv = y[o + k];
             xn[k] = make_double2(xv.x * xnorm, xv.y * xnorm);
             gn[k] = make_double2(yv.x - (xr * xn[k].x - xi * xn[k].y), yv.y - (xr * xn[k].y + xi * xn[k].x));
@@ -345,14 +378,15 @@ __global__ void __launch_bounds__(kRitzThreads)
             g[o + k] = gn[k];
         }
         double im0 = 0.0;
-        site_dot(gn, gn, v[0], im0);
-        site_dot(xn, p + o, v[1], v[2]);
+        site_dot<NCOMP>(gn, gn, v[0], im0);
+        site_dot<NCOMP>(xn, p + o, v[1], v[2]);
     }
     block_partials(v, 3, part_of(part, 0, prob, a.nblocks) + (size_t)blockIdx.x * kRitzParts);
 }
 
 // Stopping tests and the new search direction (RitzSolver.cpp:245-284), from
 // slot 0: gnorm = |g|^2, xp = <x, p>.  praw = g + beta (p - x xp); |praw|^2 -> slot 1.
+template <int NCOMP>
 __global__ void __launch_bounds__(kRitzThreads)
     ritz_direction_kernel(const double2 *__restrict__ x, const double2 *__restrict__ g, const double2 *__restrict__ p,
                           double2 *__restrict__ praw, int V, RitzScalars *st, RitzArgs a, double *part) {
@@ -369,9 +403,9 @@ __global__ void __launch_bounds__(kRitzThreads)
     const double beta = gnorm / gnormim * pnorm;
     double v[kRitzParts] = {0.0, 0.0, 0.0, 0.0};
     if (!stop && site < V) {
-        const size_t o = ((size_t)prob * V + site) * kComp;
+        const size_t o = ((size_t)prob * V + site) * NCOMP;
 #pragma unroll
-        for (int k = 0; k < kComp; k++) {
+        for (int k = 0; k < NCOMP; k++) {
             const double2 xv = x[o + k], gv = g[o + k], pv = p[o + k];
             const double2 xxp = make_double2(xv.x * xpr - xv.y * xpi, xv.x * xpi + xv.y * xpr);
             const double2 pn = make_double2(gv.x + beta * (pv.x - xxp.x), gv.y + beta * (pv.y - xxp.y));
@@ -415,18 +449,20 @@ struct RitzWork {
     RitzScalars *st = nullptr;
     RitzScalars *host = nullptr;  // pinned
     int V = 0;
+    int nc = 2;  // colours: vectors of 4 nc components per site
 };
 
-size_t ritz_work_bytes(int V) {
+size_t ritz_work_bytes(int V, int nc) {
     const int nblocks = (V + kRitzThreads - 1) / kRitzThreads;
-    return sizeof(double2) * kComp * (size_t)V * (7 * 2 + 1) + sizeof(double) * 4 * nblocks * kRitzParts +
+    return sizeof(double2) * 4 * nc * (size_t)V * (7 * 2 + 1) + sizeof(double) * 4 * nblocks * kRitzParts +
            2 * sizeof(RitzScalars);
 }
 
-void *ritz_create(int V) {
+void *ritz_create(int V, int nc) {
     RitzWork *w = new RitzWork;
     w->V = V;
-    const size_t vec = sizeof(double2) * kComp * (size_t)V * 2;
+    w->nc = nc;
+    const size_t vec = sizeof(double2) * 4 * nc * (size_t)V * 2;
     const int nblocks = (V + kRitzThreads - 1) / kRitzThreads;
     double2 **bufs[] = {&w->x, &w->y, &w->z, &w->t, &w->p, &w->praw, &w->g};
     bool ok = true;
@@ -457,31 +493,39 @@ double2 *ritz_start_buffer(void *work) { return static_cast<RitzWork *>(work)->s
 
 void launch_ritz_random_start(void *work, uint64_t seed, uint64_t call, cudaStream_t stream) {
     RitzWork &w = *static_cast<RitzWork *>(work);
-    const size_t n = (size_t)w.V * kComp;
+    const size_t n = (size_t)w.V * 4 * w.nc;
     const int blocks = (int)std::min<size_t>((n + 255) / 256, 1024);
     ritz_random_start_kernel<<<blocks, 256, 0, stream>>>(w.start, n, seed, call);
 }
 
-template <bool U1>
+template <int NC, bool U1>
 static void launch_apply(const RitzWork &w, const double *U, const double *u1, const Lattice &L, double amass,
                          const double2 *src, double2 *dst, const double2 *da, const double2 *db, bool second,
                          const RitzArgs &a, dim3 grid, cudaStream_t stream) {
-    LinksF64<U1> lk{U, reinterpret_cast<const double2 *>(u1), L.N0 * L.N1};
-    if (second)
-        ritz_apply_kernel<U1, true><<<grid, kRitzThreads, 0, stream>>>(lk, src, dst, da, db, L, amass, w.st, a, w.part);
-    else
-        ritz_apply_kernel<U1, false><<<grid, kRitzThreads, 0, stream>>>(lk, src, dst, da, db, L, amass, w.st, a,
-                                                                        w.part);
+    if constexpr (NC == 2) {
+        LinksF64<U1> lk{U, reinterpret_cast<const double2 *>(u1), L.N0 * L.N1};
+        if (second)
+            ritz_apply_kernel<2, U1, true><<<grid, kRitzThreads, 0, stream>>>(lk, src, dst, da, db, L, amass, w.st, a,
+                                                                             w.part);
+        else
+            ritz_apply_kernel<2, U1, false><<<grid, kRitzThreads, 0, stream>>>(lk, src, dst, da, db, L, amass, w.st, a,
+                                                                              w.part);
+    } else {
+        Links3<false, U1> lk{U, u1, L.N0 * L.N1};
+        if (second)
+            ritz_apply_kernel<3, U1, true><<<grid, kRitzThreads, 0, stream>>>(lk, src, dst, da, db, L, amass, w.st, a,
+                                                                             w.part);
+        else
+            ritz_apply_kernel<3, U1, false><<<grid, kRitzThreads, 0, stream>>>(lk, src, dst, da, db, L, amass, w.st, a,
+                                                                              w.part);
+    }
 }
 
-// Runs both Ritz problems from the start vector already in the start buffer
-// (compact [V][8] double2).  out: {lambda_min, -lambda_max as returned by the
-// sign = -1 problem}; iters: steps per problem.  Returns a CUDA error or
-// cudaSuccess; *launches counts kernels.
-cudaError_t ritz_run(void *work, const double *U, const double *u1, const Lattice &L, double amass, int max_iter,
-                     int nrestart, double delitr, double out[2], int iters[2], cudaStream_t stream,
-                     uint64_t *launches) {
-    RitzWork &w = *static_cast<RitzWork *>(work);
+template <int NC>
+static cudaError_t ritz_run_nc(RitzWork &w, const double *U, const double *u1, const Lattice &L, double amass,
+                               int max_iter, int nrestart, double delitr, double out[2], int iters[2],
+                               cudaStream_t stream, uint64_t *launches) {
+    constexpr int NCOMP = 4 * NC;
     const int V = L.V;
     RitzArgs a;
     a.nblocks = (V + kRitzThreads - 1) / kRitzThreads;
@@ -494,12 +538,12 @@ cudaError_t ritz_run(void *work, const double *U, const double *u1, const Lattic
     cudaError_t e = cudaMemsetAsync(w.st, 0, 2 * sizeof(RitzScalars), stream);
     if (e != cudaSuccess) return e;
     auto apply = [&](const double2 *src, double2 *dst, const double2 *da, const double2 *db, bool second) {
-        if (u1) launch_apply<true>(w, U, u1, L, amass, src, dst, da, db, second, a, grid, stream);
-        else launch_apply<false>(w, U, u1, L, amass, src, dst, da, db, second, a, grid, stream);
+        if (u1) launch_apply<NC, true>(w, U, u1, L, amass, src, dst, da, db, second, a, grid, stream);
+        else launch_apply<NC, false>(w, U, u1, L, amass, src, dst, da, db, second, a, grid, stream);
         nl++;
     };
-    ritz_start_kernel<<<grid, kRitzThreads, 0, stream>>>(w.start, w.x, V, a, w.part);
-    ritz_scale_x_kernel<<<grid, kRitzThreads, 0, stream>>>(w.x, V, a, w.part);
+    ritz_start_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.start, w.x, V, a, w.part);
+    ritz_scale_x_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, V, a, w.part);
     nl += 2;
     // Host loop: restarts every nrestart steps; the done flags are read back
     // every kPoll steps (both problems step in lockstep until they stop).
@@ -510,16 +554,16 @@ cudaError_t ritz_run(void *work, const double *U, const double *u1, const Lattic
         // restart: y = sign A x, xy, g = p = y - xy x
         apply(w.x, w.t, nullptr, nullptr, false);
         apply(w.t, w.y, w.x, nullptr, true);
-        ritz_restart_kernel<<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.g, w.praw, V, w.st, a, w.part);
-        ritz_normp_kernel<<<grid, kRitzThreads, 0, stream>>>(w.praw, w.p, V, 1, w.st, a, w.part);
+        ritz_restart_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.g, w.praw, V, w.st, a, w.part);
+        ritz_normp_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.praw, w.p, V, 1, w.st, a, w.part);
         nl += 2;
         for (int itt = 1; itt <= nrestart; itt++) {
             apply(w.p, w.t, nullptr, nullptr, false);
             apply(w.t, w.z, w.p, w.x, true);
-            ritz_rotate_kernel<<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.p, w.z, V, w.st, a, w.part);
-            ritz_residual_kernel<<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.g, w.p, V, w.st, a, w.part);
-            ritz_direction_kernel<<<grid, kRitzThreads, 0, stream>>>(w.x, w.g, w.p, w.praw, V, w.st, a, w.part);
-            ritz_normp_kernel<<<grid, kRitzThreads, 0, stream>>>(w.praw, w.p, V, 0, w.st, a, w.part);
+            ritz_rotate_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.p, w.z, V, w.st, a, w.part);
+            ritz_residual_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.g, w.p, V, w.st, a, w.part);
+            ritz_direction_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.g, w.p, w.praw, V, w.st, a, w.part);
+            ritz_normp_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.praw, w.p, V, 0, w.st, a, w.part);
             nl += 4;
             step++;
             if (step % kPoll == 0 || itt == nrestart || step >= max_iter) {
@@ -545,6 +589,19 @@ cudaError_t ritz_run(void *work, const double *U, const double *u1, const Lattic
     }
     if (launches) *launches += nl;
     return cudaSuccess;
+}
+
+// Runs both Ritz problems from the start vector already in the start buffer
+// (compact [V][4 nc] double2; links of the work space's colour count).  out:
+// {lambda_min, -lambda_max as returned by the sign = -1 problem}; iters: steps
+// per problem.  Returns a CUDA error or cudaSuccess; *launches counts kernels.
+cudaError_t ritz_run(void *work, const double *U, const double *u1, const Lattice &L, double amass, int max_iter,
+                     int nrestart, double delitr, double out[2], int iters[2], cudaStream_t stream,
+                     uint64_t *launches) {
+    RitzWork &w = *static_cast<RitzWork *>(work);
+    if (w.nc == 3)
+        return ritz_run_nc<3>(w, U, u1, L, amass, max_iter, nrestart, delitr, out, iters, stream, launches);
+    return ritz_run_nc<2>(w, U, u1, L, amass, max_iter, nrestart, delitr, out, iters, stream, launches);
 }
 
 }  // namespace ovl

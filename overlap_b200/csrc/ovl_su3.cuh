@@ -261,14 +261,16 @@ template <bool COH, typename T> __device__ __forceinline__ cpx<T> ld3(const cpx<
     return mk<T>(v.x, v.y);
 }
 
-template <typename T, int MU, bool FWD, bool COH = false>
+// STRIDE: elements between consecutive components of one spinor (the mode
+// block's 32 lanes, or 1 for a single vector stored component by component).
+template <typename T, int MU, bool FWD, bool COH = false, int STRIDE = kModeBlock>
 __device__ __forceinline__ void hop3(Spinor3<T> &acc, const cpx<T> *__restrict__ f, const cmat3<T> &M) {
     cpx<T> h0[3], h1[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        const cpx<T> *p = f + c * kSpin * kModeBlock;
-        const cpx<T> p0 = ld3<COH>(p), p1 = ld3<COH>(p + kModeBlock), p2 = ld3<COH>(p + 2 * kModeBlock),
-                     p3 = ld3<COH>(p + 3 * kModeBlock);
+        const cpx<T> *p = f + c * kSpin * STRIDE;
+        const cpx<T> p0 = ld3<COH>(p), p1 = ld3<COH>(p + STRIDE), p2 = ld3<COH>(p + 2 * STRIDE),
+                     p3 = ld3<COH>(p + 3 * STRIDE);
         if (MU == 0) {
             h0[c] = FWD ? p0 + times_i(p3) : p0 - times_i(p3);
             h1[c] = FWD ? p1 + times_i(p2) : p1 - times_i(p2);

@@ -102,3 +102,82 @@ def test_overlap_without_bounds_or_ritz_auto_is_an_error():
         ctx.set_links(random_links((4, 4, 4), 0.3, 1))
         with pytest.raises(OvlError):
             ctx.step(1)
+
+
+def dense_hw3(N, U, m, mdw, u1=None):
+    """h_W of three colours as a dense matrix, column by column from the
+    oracle's -i h_W (orc3_wilson_apply), reference layout [V][3][4]."""
+    p = oracle_params(N, m=m, mdw=mdw)
+    D = 12 * volume(N)
+    H = np.zeros((D, D), complex)
+    Uf = np.ascontiguousarray(U).view(np.float64)
+    if u1 is not None:
+        oracle().orc_set_u1(ptr(np.ascontiguousarray(u1).view(np.float64).ravel()))
+    try:
+        e, out = np.zeros(D, complex), np.zeros(D, complex)
+        for k in range(D):
+            e[:] = 0.0
+            e[k] = 1.0
+            oracle().orc3_wilson_apply(C.byref(p), ptr(Uf), ptr(e.view(np.float64)), ptr(out.view(np.float64)))
+            H[:, k] = 1j * out
+    finally:
+        oracle().orc_set_u1(None)
+    return H
+
+
+@pytest.mark.parametrize("with_u1", [False, True])
+def test_three_colour_ritz_finds_the_extreme_eigenvalues(with_u1):
+    """The Ritz iteration on the three-colour h_W^2 converges to the smallest
+    and the largest eigenvalue of the dense matrix."""
+    from overlap_b200.inputs import random_links_su3
+
+    N = (4, 3, 4)
+    V = volume(N)
+    U = random_links_su3(N, 0.6, 501)
+    ph = np.exp(1j * np.random.default_rng(502).uniform(-np.pi, np.pi, (N[1], N[0], 2))) if with_u1 else None
+    H = dense_hw3(N, U, 0.05, 1.3, ph)
+    assert np.max(np.abs(H - H.conj().T)) < 1e-13
+    w2 = np.linalg.eigvalsh(H) ** 2
+    lo, hi = w2.min(), w2.max()
+    rng = np.random.default_rng(503)
+    start = rng.uniform(0, 1, (V, 3, 4)) + 1j * rng.uniform(0, 1, (V, 3, 4))
+    with Context(N=N, n_colours=3, n_modes=4, fermion="overlap", sign_method="chebyshev", m_fermion=0.05, m_dw=1.3,
+                 ritz_seed=9) as ctx:
+        ctx.set_links(U)
+        if with_u1:
+            ctx.set_u1(ph)
+        r = ctx.ritz_bounds(start)
+        r2 = ctx.ritz_bounds()  # from the context's generator
+    for q in (r, r2):
+        assert abs(q["raw"][0] - lo) <= 1e-10 * hi and abs(q["raw"][1] - hi) <= 1e-10 * hi
+    assert r["bounds"] == pytest.approx((0.95 * r["raw"][0], 1.05 * r["raw"][1]), rel=1e-15)
+
+
+def test_three_colour_overlap_with_ritz_bounds_before_every_application():
+    """ritz_auto on a three-colour Chebyshev overlap context: every application
+    scales h_W^2 by 1.05 times the Ritz lambda_max, so it equals a context given
+    those bounds as a schedule (to the Ritz iteration's round-off), and differs
+    from the analytic bound's scaling."""
+    from overlap_b200.inputs import random_links_su3
+
+    N = (4, 4, 4)
+    V = volume(N)
+    U = random_links_su3(N, 0.5, 601)
+    rng = np.random.default_rng(602)
+    phi = rng.normal(size=(6, V, 3, 4)) + 1j * rng.normal(size=(6, V, 3, 4))
+    kw = dict(N=N, n_colours=3, n_modes=6, fermion="overlap", sign_method="chebyshev", cheb_degree=48, cheb_eps=0.01,
+              m_fermion=0.05, m_dw=1.0, precision="fp64")
+    with Context(ritz_auto=1, ritz_seed=3, **kw) as a:
+        a.set_links(U)
+        b = a.ritz_bounds()["bounds"]
+        out_a = a.apply(phi)
+    with Context(**kw) as c:
+        c.set_links(U)
+        c.set_spectral_bounds([b])
+        out_b = c.apply(phi)
+        c.set_spectral_bounds([(0.01 * 25.0, 25.0)])  # the analytic bound (|6r - 2M|/2 + 3)^2 + 2m terms aside
+        out_loose = c.apply(phi)
+    scale = np.max(np.abs(out_b))
+    assert np.max(np.abs(out_a - out_b)) < 1e-9 * scale
+    assert np.max(np.abs(out_loose - out_b)) > 1e-6 * scale
+    assert b[1] < 25.0
