@@ -7,6 +7,8 @@ reference used, through ovl_set_spectral_bounds.  The reference's Zolotarev
 approximation is accurate to ~1e-7 (single-precision square roots in its
 coefficients) and its CG stops at a relative residual ~1e-8: both sides run the
 same coefficients and the same per-mode stopping rule, and agree to 1e-11."""
+import functools
+
 import numpy as np
 import pytest
 
@@ -162,6 +164,88 @@ def test_chebyshev_overlap_leapfrog_fp32_runs_and_conserves_norm():
         psi, _ = ctx.get_modes()
         assert abs(np.sum(np.abs(psi) ** 2) / n0 - 1.0) < 0.2
         assert np.isfinite(ctx.charges()["N5"])
+
+
+def _embedded_chebyshev_oracle(N, U, E, psi, mid, steps, K, eps, lmax, m, mdw, dt):
+    """The FP64 Chebyshev overlap leapfrog of two colours: the three-colour
+    oracle (orc3_overlap_leapfrog) on the fields embedded in the upper-left
+    colour block, where the third colour is free and stays empty (the
+    embedding reproduces every two-colour oracle function, tests/test_oracle_su3.py).
+    Returns the two-colour modes, the links and N_5 of the final modes."""
+    import ctypes as C
+
+    from _helpers import oracle_params
+    from _oracle import oracle
+    from overlap_b200.inputs import embed_su2_efield, embed_su2_links
+
+    def f64(a):
+        return np.ascontiguousarray(a).view(np.float64)
+
+    def embed(q):
+        out = np.zeros(q.shape[:2] + (3, 4), complex)
+        out[:, :, :2, :] = q
+        return out
+
+    p = oracle_params(N, m=m, mdw=mdw, dt=dt)
+    U3, E3 = embed_su2_links(U).copy(), embed_su2_efield(E)
+    o_psi, o_mid = embed(psi), embed(mid)
+    t = C.c_int(0)
+    oracle().orc3_overlap_leapfrog(C.byref(p), ptr(f64(U3)), ptr(f64(E3)), ptr(f64(o_psi)), ptr(f64(o_mid)),
+                                   psi.shape[0], C.byref(t), steps, K, eps, lmax)
+    O = np.zeros_like(o_psi)
+    for k in range(psi.shape[0]):
+        oracle().orc3_overlap_apply(C.byref(p), ptr(f64(U3)), ptr(f64(o_psi[k])), ptr(f64(O[k])), K, eps, lmax)
+    # overlap N_5 (OverlapCurrents.cpp:35-212): local bilinears with O = -i h_ov psi
+    g5 = np.array([[0, 0, 1, 0], [0, 0, 0, 1], [1, 0, 0, 0], [0, 1, 0, 0]], complex)
+    g0 = np.diag([1, 1, -1, -1]).astype(complex)
+    w = np.where(np.arange(psi.shape[0]) % 2 == 0, 1.0, -1.0)
+    a1 = np.einsum("msca,ab,mscb->m", np.conj(o_psi), g5, o_psi).real
+    a2 = np.einsum("msca,ab,mscb->m", np.conj(o_psi), g5 @ g0, O).imag
+    n5 = float(np.sum(w * (a1 + 0.5 * a2)) / (2 * volume(N)))
+    assert np.max(np.abs(o_psi[:, :, 2, :])) == 0.0
+    return o_psi[:, :, :2, :], o_mid[:, :, :2, :], n5
+
+
+_CHEB_CASE = dict(N=(4, 4, 4), m=0.05, mdw=1.0, dt=0.05, K=96, eps=0.01, steps=100, modes=16)
+
+
+@functools.lru_cache(maxsize=1)
+def _cheb_case():
+    c = _CHEB_CASE
+    N = c["N"]
+    lmax = (0.5 * abs(6 + 2 * c["m"] - 2 * c["mdw"]) + 3.0) ** 2  # the context's bound without a schedule
+    U, E = random_links(N, 0.5, 151), random_efield(N, 0.2, 152)
+    psi0, mid0 = random_modes(c["modes"], N, 153), random_modes(c["modes"], N, 154)
+    want = _embedded_chebyshev_oracle(N, U, E, psi0, mid0, c["steps"], c["K"], c["eps"], lmax, c["m"], c["mdw"], c["dt"])
+    return U, E, psi0, mid0, want
+
+
+@pytest.mark.parametrize("precision,variant", [("fp64", 0), ("fp32", 0), ("fp32", 3)])
+def test_chebyshev_overlap_leapfrog_matches_the_fp64_oracle(precision, variant):
+    """Two colours, 100 leapfrog steps with moving links, Chebyshev degree 96
+    on the analytic bound: the modes and N_5 against the FP64 Chebyshev
+    oracle leapfrog.  FP64 to 1e-10; FP32 (the serving and bench form) to
+    1e-4 in the fields and 1e-5 of |N_5| in the axial charge (measured: 1e-6
+    and 5.5e-6; N_5 sums bilinears of alternating sign, so its relative
+    error exceeds the fields')."""
+    c = _CHEB_CASE
+    N, m, mdw, dt, K, eps, steps = c["N"], c["m"], c["mdw"], c["dt"], c["K"], c["eps"], c["steps"]
+    U, E, psi0, mid0, (o_psi, o_mid, n5) = _cheb_case()
+    with Context(N=N, n_modes=c["modes"], fermion="overlap", sign_method="chebyshev", cheb_degree=K, cheb_eps=eps,
+                 m_fermion=m, m_dw=mdw, dt=dt, precision=precision, hop_variant=variant) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_modes(psi0, mid0)
+        ctx.step(steps)
+        g_psi, g_mid = ctx.get_modes()
+        g_n5 = ctx.charges()["N5"]
+    err = max(rel_err(g_psi, o_psi), rel_err(g_mid, o_mid))
+    n5_err = abs(g_n5 - n5) / max(abs(n5), 1e-300)
+    print(f"{precision} v{variant}: fields {err:.2e}, N5 {g_n5:.12e} vs {n5:.12e} (rel {n5_err:.2e})")
+    if precision == "fp64":
+        assert err < 1e-10 and n5_err < 1e-10
+    else:
+        assert err < 1e-4 and n5_err < 1e-5
 
 
 @pytest.mark.skipif(not have_reference("overlap"), reason="reference overlap build absent")
