@@ -402,11 +402,13 @@ void grouped_pass(ovl_ctx *c, const ovl::HopConfig &h1, const ovl::HopConfig &h2
 // candidate.  Where the fastest burst takes kSustainMinMs or more, the GPU
 // reaches its power cap within a run of such launches, and then the clock a
 // kernel holds depends on its own power draw: each candidate is timed again
-// over windows of about kSustainWindowMs of back-to-back launches, timing the
-// second half of each window, twice in the order 0..n-1, n-1..0 (a drift of
-// the clock over the tuning cancels), and ms[k] is the mean of its two
-// windows.  Returns false if an event could not be created.
-constexpr double kSustainMinMs = 1.0, kSustainWindowMs = 200.0;
+// over windows of about kSustainWindowMs of back-to-back launches (the second
+// half of each window timed), in kSustainRounds rounds whose order alternates
+// 0..n-1, n-1..0 (a drift of the clock over the tuning cancels), and ms[k] is
+// the median of its rounds (one window caught by a clock excursion does not
+// decide).  Returns false if an event could not be created.
+constexpr double kSustainMinMs = 1.0, kSustainWindowMs = 120.0;
+constexpr int kSustainRounds = 6;
 
 template <class F>
 bool time_candidates(cudaStream_t stream, int n, F run, double *ms, uint64_t &launches) {
@@ -432,14 +434,17 @@ bool time_candidates(cudaStream_t stream, int n, F run, double *ms, uint64_t &la
         best = std::min(best, ms[k]);
     }
     if (best >= kSustainMinMs) {
-        std::vector<double> sum(n, 0.0);
-        for (int pass = 0; pass < 2; pass++)
+        std::vector<std::vector<double>> w(n);
+        for (int round = 0; round < kSustainRounds; round++)
             for (int i = 0; i < n; i++) {
-                const int k = pass == 0 ? i : n - 1 - i;
+                const int k = round % 2 == 0 ? i : n - 1 - i;
                 const int half = std::max(4, (int)(0.5 * kSustainWindowMs / std::max(ms[k], 1e-3)));
-                sum[k] += timed(k, half, half);
+                w[k].push_back(timed(k, half, half));
             }
-        for (int k = 0; k < n; k++) ms[k] = 0.5 * sum[k];
+        for (int k = 0; k < n; k++) {
+            std::sort(w[k].begin(), w[k].end());
+            ms[k] = 0.5 * (w[k][(kSustainRounds - 1) / 2] + w[k][kSustainRounds / 2]);
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
