@@ -442,6 +442,25 @@ __global__ void ritz_random_start_kernel(double2 *start, size_t n, uint64_t seed
 
 // ---------------------------------------------------------------- host side --
 
+// The iteration between two reads of the stop flags (kRitzPoll steps, with or
+// without the restart that opens a cycle of nrestart steps) captured once as
+// CUDA graphs and replayed; recaptured when an argument they bake in changes.
+constexpr int kRitzPoll = 25;
+
+struct RitzGraphs {
+    cudaGraphExec_t restart = nullptr, plain = nullptr;
+    const double *U = nullptr, *u1 = nullptr;
+    int N[3] = {0, 0, 0};
+    double amass = 0.0, delitr = 0.0;
+    int max_iter = 0;
+    bool failed = false;  // capture not possible on this stream: step the loop instead
+    void release() {
+        if (restart) cudaGraphExecDestroy(restart);
+        if (plain) cudaGraphExecDestroy(plain);
+        restart = plain = nullptr;
+    }
+};
+
 struct RitzWork {
     double2 *x = nullptr, *y = nullptr, *z = nullptr, *t = nullptr, *p = nullptr, *praw = nullptr, *g = nullptr;
     double2 *start = nullptr;
@@ -450,6 +469,7 @@ struct RitzWork {
     RitzScalars *host = nullptr;  // pinned
     int V = 0;
     int nc = 2;  // colours: vectors of 4 nc components per site
+    RitzGraphs graphs;
 };
 
 size_t ritz_work_bytes(int V, int nc) {
@@ -486,6 +506,7 @@ void ritz_destroy(void *work) {
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (w->host) cudaFreeHost(w->host);
+    w->graphs.release();
     delete w;
 }
 
@@ -545,36 +566,91 @@ static cudaError_t ritz_run_nc(RitzWork &w, const double *U, const double *u1, c
     ritz_start_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.start, w.x, V, a, w.part);
     ritz_scale_x_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, V, a, w.part);
     nl += 2;
-    // Host loop: restarts every nrestart steps; the done flags are read back
-    // every kPoll steps (both problems step in lockstep until they stop).
-    constexpr int kPoll = 25;
-    int step = 0;
-    bool finished = false;
-    while (!finished) {
-        // restart: y = sign A x, xy, g = p = y - xy x
+    // restart: y = sign A x, xy, g = p = y - xy x
+    auto restart_seq = [&]() {
         apply(w.x, w.t, nullptr, nullptr, false);
         apply(w.t, w.y, w.x, nullptr, true);
         ritz_restart_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.g, w.praw, V, w.st, a, w.part);
         ritz_normp_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.praw, w.p, V, 1, w.st, a, w.part);
         nl += 2;
-        for (int itt = 1; itt <= nrestart; itt++) {
-            apply(w.p, w.t, nullptr, nullptr, false);
-            apply(w.t, w.z, w.p, w.x, true);
-            ritz_rotate_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.p, w.z, V, w.st, a, w.part);
-            ritz_residual_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.g, w.p, V, w.st, a, w.part);
-            ritz_direction_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.g, w.p, w.praw, V, w.st, a, w.part);
-            ritz_normp_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.praw, w.p, V, 0, w.st, a, w.part);
-            nl += 4;
-            step++;
-            if (step % kPoll == 0 || itt == nrestart || step >= max_iter) {
-                if ((e = cudaGetLastError()) != cudaSuccess) return e;
-                if ((e = cudaMemcpyAsync(w.host, w.st, 2 * sizeof(RitzScalars), cudaMemcpyDeviceToHost, stream)) !=
-                    cudaSuccess)
-                    return e;
-                if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
-                if ((w.host[0].done && w.host[1].done) || step >= max_iter) {
-                    finished = true;
-                    break;
+    };
+    auto step_seq = [&]() {
+        apply(w.p, w.t, nullptr, nullptr, false);
+        apply(w.t, w.z, w.p, w.x, true);
+        ritz_rotate_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.p, w.z, V, w.st, a, w.part);
+        ritz_residual_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.y, w.g, w.p, V, w.st, a, w.part);
+        ritz_direction_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.x, w.g, w.p, w.praw, V, w.st, a, w.part);
+        ritz_normp_kernel<NCOMP><<<grid, kRitzThreads, 0, stream>>>(w.praw, w.p, V, 0, w.st, a, w.part);
+        nl += 4;
+    };
+    auto poll = [&](bool &finished, int step) -> cudaError_t {
+        cudaError_t r;
+        if ((r = cudaGetLastError()) != cudaSuccess) return r;
+        if ((r = cudaMemcpyAsync(w.host, w.st, 2 * sizeof(RitzScalars), cudaMemcpyDeviceToHost, stream)) !=
+            cudaSuccess)
+            return r;
+        if ((r = cudaStreamSynchronize(stream)) != cudaSuccess) return r;
+        finished = (w.host[0].done && w.host[1].done) || step >= max_iter;
+        return cudaSuccess;
+    };
+    // The graphs replace the loop below when the restart cycle and the step
+    // limit are whole numbers of poll intervals: the same kernels in the same
+    // order, so the same results.
+    RitzGraphs &gr = w.graphs;
+    bool graphs = !gr.failed && nrestart % kRitzPoll == 0 && max_iter % kRitzPoll == 0;
+    if (graphs && !(gr.restart && gr.U == U && gr.u1 == u1 && gr.N[0] == L.N0 && gr.N[1] == L.N1 && gr.N[2] == L.N2 &&
+                    gr.amass == amass && gr.delitr == delitr && gr.max_iter == max_iter)) {
+        gr.release();
+        auto capture = [&](bool with_restart, cudaGraphExec_t &exec) {
+            if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+            const uint64_t nl0 = nl;
+            if (with_restart) restart_seq();
+            for (int i = 0; i < kRitzPoll; i++) step_seq();
+            nl = nl0;  // counted when replayed
+            cudaGraph_t g = nullptr;
+            if (cudaStreamEndCapture(stream, &g) != cudaSuccess || !g) return false;
+            const bool ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+            cudaGraphDestroy(g);
+            return ok;
+        };
+        if (capture(true, gr.restart) && capture(false, gr.plain)) {
+            gr.U = U;
+            gr.u1 = u1;
+            gr.N[0] = L.N0;
+            gr.N[1] = L.N1;
+            gr.N[2] = L.N2;
+            gr.amass = amass;
+            gr.delitr = delitr;
+            gr.max_iter = max_iter;
+        } else {
+            cudaGetLastError();
+            gr.release();
+            gr.failed = true;
+            graphs = false;
+        }
+    }
+    int step = 0;
+    bool finished = false;
+    if (graphs) {
+        // one graph per poll interval, the restart one opening each cycle
+        while (!finished) {
+            const bool restart = step % nrestart == 0;
+            if ((e = cudaGraphLaunch(restart ? gr.restart : gr.plain, stream)) != cudaSuccess) return e;
+            nl += (restart ? 4 : 0) + 6 * kRitzPoll;
+            step += kRitzPoll;
+            if ((e = poll(finished, step)) != cudaSuccess) return e;
+        }
+    } else {
+        // Host loop: restarts every nrestart steps; the done flags are read back
+        // every kRitzPoll steps (both problems step in lockstep until they stop).
+        while (!finished) {
+            restart_seq();
+            for (int itt = 1; itt <= nrestart; itt++) {
+                step_seq();
+                step++;
+                if (step % kRitzPoll == 0 || itt == nrestart || step >= max_iter) {
+                    if ((e = poll(finished, step)) != cudaSuccess) return e;
+                    if (finished) break;
                 }
             }
         }
