@@ -437,8 +437,24 @@ int ovl_load_configuration(ovl_ctx *ctx, const char *u_path, const char *e_path)
  * out = {T00, TXX, TYY, TZZ, electric, magnetic, gauss max, gauss avg, unitarity max, unitarity avg}. */
 int ovl_bulk(ovl_ctx *ctx, double out[10]);
 
-/* Waits for all work queued on the context's stream. */
+/* Waits for all work queued on the context's stream; reports OVL_E_TIMEOUT
+ * for a pipelined half step queued by ovl_step_observe_async that timed out. */
 int ovl_synchronize(ovl_ctx *ctx);
+
+/* Asynchronous forms for callers that keep the GPU busy across steps (a step
+ * loop that uploads each step's gauge fields and reads each step's charges):
+ * the work is queued on the context's stream and the call returns.
+ * ovl_upload_gauge_async: ovl_set_links and ovl_set_efield (either may be
+ * NULL) from page-locked host memory (OVL_E_ARG otherwise), which the copy
+ * reads until the stream reaches it: keep the buffers unchanged until then
+ * (ovl_synchronize, or an event recorded on the stream after the call).
+ * ovl_step_observe_async: ovl_step_observe with its three charges copied into
+ * `out`, page-locked host memory (OVL_E_ARG otherwise), valid once the
+ * stream has passed the call.  Fused two-colour Wilson forms queue without
+ * waiting; the other forms complete before returning.  No counterpart in the
+ * reference (its steps are synchronous). */
+int ovl_upload_gauge_async(ovl_ctx *ctx, const double *links, const double *efield);
+int ovl_step_observe_async(ovl_ctx *ctx, int nsteps, double *out);
 
 /* Device addresses and layout of the mode fields, for callers that keep their
  * own device buffers.  Layout: [mode/32][site][colour*4+spin][mode%32] complex of

@@ -89,6 +89,8 @@ SIGNATURES = {
     "ovl_set_quasi_particles": ([_ctx, C.c_double, C.c_double, C.c_uint64, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "ovl_bulk": ([_ctx, _dp], C.c_int),
     "ovl_save_configuration": ([_ctx, C.c_char_p, C.c_char_p], C.c_int),
+    "ovl_upload_gauge_async": ([_ctx, _dp, _dp], C.c_int),
+    "ovl_step_observe_async": ([_ctx, C.c_int, _dp], C.c_int),
     "ovl_cool": ([_ctx, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.POINTER(C.c_int), _dp, _dp,
                   C.POINTER(C.c_int)], C.c_int),
     "ovl_load_configuration": ([_ctx, C.c_char_p, C.c_char_p], C.c_int),

@@ -323,6 +323,33 @@ class Context:
         self._check(self._L.ovl_step_observe(self._ctx, int(nsteps), _dp(o)))
         return {"NV": o[0], "N5": o[1], "PS": o[2]}
 
+    @staticmethod
+    def _pinned_view(a, size, what):
+        """The float64 buffer of `a` itself (no copy: the copy queued from it
+        runs after the call returns)."""
+        if not isinstance(a, np.ndarray) or a.dtype not in (np.float64, np.complex128) or not a.flags.c_contiguous:
+            raise ValueError(f"{what}: a C-contiguous float64/complex128 array in page-locked memory")
+        v = a.view(np.float64)
+        if v.size != size:
+            raise ValueError(f"{what}: expected {size} doubles, got {v.size}")
+        return v
+
+    def upload_gauge_async(self, links=None, efield=None):
+        """ovl_upload_gauge_async: links and/or E from page-locked arrays (e.g.
+        torch.empty(..., pin_memory=True).numpy()) copied on the context's
+        stream; keep them unchanged until the stream has passed the copy."""
+        nl = self.V * 3 * (18 if self.nc == 3 else 4)
+        ne = self.V * 3 * (self.nc * self.nc - 1)
+        lp = _dp(self._pinned_view(links, nl, "links")) if links is not None else None
+        ep = _dp(self._pinned_view(efield, ne, "efield")) if efield is not None else None
+        self._check(self._L.ovl_upload_gauge_async(self._ctx, lp, ep))
+
+    def step_observe_async(self, nsteps: int, out) -> None:
+        """ovl_step_observe_async: queues nsteps leapfrog steps; {NV, N5, PS} of
+        the modes at the end land in `out` (3 doubles, page-locked) once the
+        stream has passed the call."""
+        self._check(self._L.ovl_step_observe_async(self._ctx, int(nsteps), _dp(self._pinned_view(out, 3, "out"))))
+
     def charges(self) -> dict:
         o = np.empty(4)
         self._check(self._L.ovl_charges(self._ctx, _dp(o)))

@@ -946,6 +946,24 @@ int ovl_set_efield(ovl_ctx *c, const double *efield) {
     return OVL_OK;
 }
 
+int ovl_upload_gauge_async(ovl_ctx *c, const double *links, const double *efield) {
+    if (!c) return OVL_E_ARG;
+    if ((links && !page_locked(links)) || (efield && !page_locked(efield)))
+        return fail(c, OVL_E_ARG, "ovl_upload_gauge_async: the fields must be page-locked host memory");
+    const size_t nl = (size_t)c->link_doubles * 3 * c->L.V, ne = (size_t)c->e_comp * 3 * c->L.V;
+    if (links && !all_finite(links, nl)) return fail(c, OVL_E_NONFINITE, "ovl_upload_gauge_async: non-finite link component");
+    if (efield && !all_finite(efield, ne))
+        return fail(c, OVL_E_NONFINITE, "ovl_upload_gauge_async: non-finite field component");
+    int rc = set_device(c);
+    if (rc) return rc;
+    if (links) {
+        OVL_CUDA(c, cudaMemcpyAsync(c->U, links, sizeof(double) * nl, cudaMemcpyHostToDevice, c->stream));
+        refresh_links32(c);
+    }
+    if (efield) OVL_CUDA(c, cudaMemcpyAsync(c->E, efield, sizeof(double) * ne, cudaMemcpyHostToDevice, c->stream));
+    return OVL_OK;
+}
+
 int ovl_set_u1(ovl_ctx *c, const double *u1) {
     if (!c) return OVL_E_ARG;
     if (!u1) {
@@ -1397,7 +1415,11 @@ int ovl_step(ovl_ctx *c, int nsteps) {
     return check_pipeline(c);
 }
 
-int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) {
+// The steps of ovl_step_observe.  async: the charges are copied into `out`
+// (page-locked) on the stream and the call returns without waiting (the fused
+// two-colour forms; the others complete before returning); otherwise through
+// the context's pinned mirror, waited for.
+static int step_observe(ovl_ctx *c, int nsteps, double *out, bool async) {
     if (!c || !out) return OVL_E_ARG;
     if (nsteps < 1) return fail(c, OVL_E_ARG, "ovl_step_observe: nsteps=%d", nsteps);
     int rc = set_device(c);
@@ -1434,8 +1456,9 @@ int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) {
                                    c->obs_scratch, 1.0 / (2.0 * c->L.V), c->dev_small + 32, c->stream);
         }
         if ((rc = launched(c, 2, "charges (observing step)"))) return rc;
-        OVL_CUDA(c, cudaMemcpyAsync(c->host_small + 32, c->dev_small + 32, sizeof(double) * 3,
+        OVL_CUDA(c, cudaMemcpyAsync(async ? out : c->host_small + 32, c->dev_small + 32, sizeof(double) * 3,
                                     cudaMemcpyDeviceToHost, c->stream));
+        if (async) return OVL_OK;  // a timed-out wait is reported by ovl_synchronize
         if ((rc = check_pipeline(c))) return rc;  // synchronizes the stream
         for (int k = 0; k < 3; k++) out[k] = c->host_small[32 + k];
         return OVL_OK;
@@ -1481,11 +1504,20 @@ int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) {
                                1.0 / (2.0 * c->L.V), c->dev_small + 32, c->stream);
     }
     if ((rc = launched(c, 2, "charges (observing step)"))) return rc;
-    OVL_CUDA(c, cudaMemcpyAsync(c->host_small + 32, c->dev_small + 32, sizeof(double) * 3, cudaMemcpyDeviceToHost,
-                                c->stream));
+    OVL_CUDA(c, cudaMemcpyAsync(async ? out : c->host_small + 32, c->dev_small + 32, sizeof(double) * 3,
+                                cudaMemcpyDeviceToHost, c->stream));
+    if (async) return OVL_OK;
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
     for (int k = 0; k < 3; k++) out[k] = c->host_small[32 + k];
     return OVL_OK;
+}
+
+int ovl_step_observe(ovl_ctx *c, int nsteps, double out[3]) { return step_observe(c, nsteps, out, false); }
+
+int ovl_step_observe_async(ovl_ctx *c, int nsteps, double *out) {
+    if (!c || !out) return OVL_E_ARG;
+    if (!page_locked(out)) return fail(c, OVL_E_ARG, "ovl_step_observe_async: out must be page-locked host memory");
+    return step_observe(c, nsteps, out, true);
 }
 
 int ovl_get_step_count(const ovl_ctx *c, int *steps) {
@@ -2076,7 +2108,7 @@ int ovl_synchronize(ovl_ctx *c) {
     int rc = set_device(c);
     if (rc) return rc;
     OVL_CUDA(c, cudaStreamSynchronize(c->stream));
-    return OVL_OK;
+    return check_pipeline(c);  // a timed-out wait of a step queued without waiting
 }
 
 int ovl_device_modes(ovl_ctx *c, void **psi, void **psimid, size_t *bytes) {
