@@ -22,7 +22,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .api import Context, Ensemble, Params
+from .api import Context, Ensemble, OvlError, Params
 from .inputs import random_efield, random_efield_su3, random_links, random_links_su3, u1_flux, volume
 
 
@@ -51,6 +51,7 @@ class Request:
     finished: float = float("nan")
     gpu_s: float = 0.0           # GPU time of its chunks, a chunk's shared by the requests in it
     observables: list = field(default_factory=list)  # (step, N5, N_CS, energy)
+    error: str = ""              # why its set-up failed, if it did
 
     def mode_sites(self) -> int:
         return self.n_modes * volume(self.N)
@@ -166,24 +167,44 @@ class Server:
             self._phases[name] = self._phases.get(name, 0.0) + t[-1] - t[-2]
 
         p = self._params(r)
-        if not r.batchable():
-            import torch
+        ctx, member = None, None  # the request's context; its index in the ensemble
+        try:
+            if not r.batchable():
+                import torch
 
-            stream = torch.cuda.Stream(self.device)
-            p.stream = stream.cuda_stream
-            ctx = Context(p)
-            ctx.torch_stream = stream  # keeps the stream alive with the context
-        elif self.ensemble is None:
-            import torch
+                stream = torch.cuda.Stream(self.device)
+                p.stream = stream.cuda_stream
+                ctx = Context(p)
+                ctx.torch_stream = stream  # keeps the stream alive with the context
+            elif self.ensemble is None:
+                import torch
 
-            self._ens_stream = torch.cuda.Stream(self.device)
-            p.stream = self._ens_stream.cuda_stream  # the ensemble runs on the first member's stream
-            self.ensemble = Ensemble([p])
-            if self.tile:
-                self.ensemble.set_tile(self.tile)
-            ctx = self.ensemble[0]
+                self._ens_stream = torch.cuda.Stream(self.device)
+                p.stream = self._ens_stream.cuda_stream  # the ensemble runs on the first member's stream
+                ensemble = Ensemble([p])
+                self.ensemble, member = ensemble, 0
+                if self.tile:
+                    self.ensemble.set_tile(self.tile)
+                ctx = self.ensemble[0]
+            else:
+                ctx = self.ensemble.add(p)
+                member = len(self.ensemble) - 1
+            self._setup(r, ctx, now, phase)
+        except OvlError:
+            # the request leaves no trace: its context (or ensemble member) is released
+            if member is not None:
+                self.ensemble.remove(member)
+            elif ctx is not None:
+                ctx.close()
+            raise
+        if r.batchable():
+            self.active.append(r)
         else:
-            ctx = self.ensemble.add(p)
+            self.solo.append((r, ctx))
+        self.used_bytes += request_bytes(r, self.precision)
+
+    def _setup(self, r: Request, ctx, now: float, phase):
+        """The request's fields and first observation on its new context."""
         phase("create_s")
         fut = getattr(r, "_inputs", None)
         links, efield, u1 = fut.result() if fut is not None else request_inputs(r)
@@ -204,11 +225,6 @@ class Server:
         r._ncs = 0.0
         self._observe(r, ctx)
         phase("first_observation_s")
-        if r.batchable():
-            self.active.append(r)
-        else:
-            self.solo.append((r, ctx))
-        self.used_bytes += request_bytes(r, self.precision)
 
     def _observe(self, r: Request, ctx):
         n5 = ctx.charges()["N5"]
@@ -244,7 +260,9 @@ class Server:
         """Runs `requests` (arrival times relative to now) to completion, or
         until `time_box` seconds have passed, and returns latency and
         throughput figures.  A request larger than the whole memory budget is
-        rejected (finished = NaN, in `rejected`).  With a time box the figures
+        rejected (finished = NaN, in `rejected`); one whose set-up on the device
+        raises (OvlError: out of device memory, say) fails alone (`failed`, the
+        message in request.error) and the others go on.  With a time box the figures
         count what finished inside it (and the work of the chunks queued at its
         end); the requests still running, queued or not yet arrived at its end
         are reported as such."""
@@ -258,8 +276,10 @@ class Server:
             r.observables = []
             r.admitted = r.finished = float("nan")
             r.gpu_s = 0.0
+            r.error = ""
         queue: list[Request] = []
         rejected = []
+        failed = []  # set-up raised: error text in request.error
         inflight = {}  # group key ("ensemble" or a solo rid) -> (start, end, steps, requests)
         vtime = {}  # group key -> GPU seconds per request it carried
         last_end = [None]  # end event of the chunk queued last
@@ -343,17 +363,24 @@ class Server:
             # admission (into the ensemble only while it has no chunk queued)
             h0 = time.perf_counter()
             admitted = []
+
+            def admit(q):
+                try:
+                    self._admit(q, clock())
+                    admitted.append(q)
+                except OvlError as e:  # set-up failed (device memory, say): the request fails alone
+                    q.error = str(e)
+                    failed.append(q)
+
             if self.admission == "shortest":
                 queue.sort(key=lambda q: request_cost(q) * q.steps)
                 for q in list(queue):
                     if fits(q) and ("ensemble" not in inflight or not q.batchable()):
                         queue.remove(q)
-                        admitted.append(q)
-                        self._admit(q, clock())
+                        admit(q)
             else:
                 while queue and fits(queue[0]) and ("ensemble" not in inflight or not queue[0].batchable()):
-                    admitted.append(queue[0])
-                    self._admit(queue.pop(0), clock())
+                    admit(queue.pop(0))
             for q in admitted:
                 key = "ensemble" if q.batchable() else q.rid
                 if key not in vtime:
@@ -403,7 +430,7 @@ class Server:
         admitted = [r for r in requests if r.admitted == r.admitted]  # not NaN
         all_wait = np.array([r.admitted - r.arrival for r in admitted]) if admitted else np.zeros(1)
         work, work_cost = acc["work"], acc["cost"]
-        return {"requests": len(self.done), "rejected": len(rejected), "wall_s": wall,
+        return {"requests": len(self.done), "rejected": len(rejected), "failed": len(failed), "wall_s": wall,
                 "throughput": work / wall if wall > 0 else 0.0, "unit": "mode-site updates/s",
                 "throughput_wilson_equivalent": work_cost / wall if wall > 0 else 0.0,
                 "gpu_busy_fraction": acc["gpu_s"] / wall if wall > 0 else 0.0,

@@ -137,3 +137,18 @@ def test_running_requests_share_the_gpu_time_equally():
     assert g.min() > 0 and g.max() < 2.0 * g.min(), g
     assert abs(g[0] - g[1]) < 1e-9 * g[0]  # one chunk time, split between the members
     assert 0.0 < m["gpu_busy_fraction"] <= 1.05
+
+
+@pytest.mark.parametrize("fermion", ["wilson", "overlap"])
+def test_a_request_whose_setup_fails_fails_alone(fermion):
+    """A request the library refuses at set-up (here a 2^3 lattice, below the
+    contexts' minimum extent) is reported as failed with the library's message;
+    the ensemble or the server goes on, and the other requests' results are
+    those they have alone."""
+    kw = dict(fermion="overlap", cheb_degree=16) if fermion == "overlap" else {}
+    good = lambda t: req(8, (4, 4, 4), 64, 20, t, **kw)
+    bad = req(9, (2, 2, 2), 64, 20, 0.01, **kw)
+    alone, _ = serve([good(0.0)], precision="fp64", tick_steps=7)
+    mixed, m = serve([good(0.0), bad, req(10, (4, 4, 6), 32, 20, 0.02)], precision="fp64", tick_steps=7)
+    assert m["requests"] == 2 and m["failed"] == 1 and "N[0]=2" in bad.error
+    assert same(mixed[good(0).seed], alone[good(0).seed], "fp64")
