@@ -408,7 +408,7 @@ int ovl_gauss_restore(ovl_ctx *ctx, int max_iter, double tol, int *iterations, d
  * standard phase, on the lattice cooled_N (may be NULL).  The context's own
  * links are not changed.  Each blocking needs every lattice extent >= 2 when
  * it happens (OVL_E_ARG before anything runs otherwise).  The reference's
- * driver calls this with block_frequency 32, standard_blocking 0 and
+ * driver (Simulation.cpp:258-265) calls this with block_frequency 32, standard_blocking 0 and
  * calibration_blocking 2. */
 int ovl_cool(ovl_ctx *ctx, int standard_steps, int standard_blocking, int calibration_steps, int calibration_blocking,
              int block_frequency, double *log, int *log_rows, double out[3], double *cooled_links, int cooled_N[3]);

@@ -436,7 +436,7 @@ void ovlref_cool(int standard_steps, int standard_blocking, int calibration_step
     Cooling::Cleanup();
 }
 
-/* The driver's own calibration, unchanged (Simulation.cpp:425-431:
+/* The reference driver's own calibration, unchanged (Simulation.cpp:425-431:
  * CoolingMethod::Init, Start, Calibrate) with the given schedule: the
  * reference writes <dir>/VacuumCoolingT0ID<seed>.log at 6 digits. */
 void ovlref_cool_driver_log(const char *dir, long seed, int standard_steps, int standard_blocking,

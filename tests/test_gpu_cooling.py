@@ -36,7 +36,7 @@ def test_cooling_matches_golden(golden_dir):
     assert np.max(np.abs(r["cooled_links"] - g["cooled"])) < 1e-13
 
 
-@pytest.mark.parametrize("nc,N,schedule", [(2, (16, 16, 8), (0, 0, 40, 2, 32)),   # the driver's schedule
+@pytest.mark.parametrize("nc,N,schedule", [(2, (16, 16, 8), (0, 0, 40, 2, 32)),   # the reference driver's schedule
                                            (2, (8, 8, 4), (5, 1, 12, 2, 2)),
                                            (2, (5, 6, 4), (4, 0, 6, 0, 32)),
                                            (3, (8, 4, 8), (3, 1, 10, 2, 2)),

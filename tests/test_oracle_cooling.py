@@ -66,7 +66,7 @@ def test_cooling_matches_golden(golden_dir):
 
 
 @pytest.mark.skipif(not have_reference("wilson"), reason="reference build not present")
-@pytest.mark.parametrize("N,schedule", [((6, 4, 8), (0, 0, 40, 2, 32)),      # the driver's blocking schedule
+@pytest.mark.parametrize("N,schedule", [((6, 4, 8), (0, 0, 40, 2, 32)),      # the reference driver's blocking schedule
                                         ((8, 8, 4), (5, 1, 12, 2, 2)),       # blocking in both phases
                                         ((5, 6, 4), (4, 0, 6, 0, 32))])      # odd extent, no blocking
 def test_cooling_matches_the_reference(N, schedule):
