@@ -322,102 +322,104 @@ class Server:
 
         prep = ThreadPoolExecutor(max_workers=1)
         boxed = False
-        while pending or queue or self.active or self.solo:
-            now = clock()
-            if time_box is not None and now >= time_box:
-                boxed = True
-                break
-            while pending and pending[0].arrival <= now:
-                r = pending.pop(0)
-                if request_bytes(r, self.precision) > self.memory_bytes:
-                    rejected.append(r)
-                else:
-                    r._inputs = prep.submit(request_inputs, r)  # generated while the GPU works
-                    queue.append(r)
-            busy = False
-            # chunks that ended: account, stream the observables due, retire
-            h0 = time.perf_counter()
-            if "ensemble" in inflight and inflight["ensemble"][1].query():
-                account("ensemble", *inflight.pop("ensemble"))
-                for i in range(len(self.active) - 1, -1, -1):
-                    r = self.active[i]
-                    if r._step % r.observe_every == 0 or r._step == r.steps:
-                        self._observe(r, self.ensemble[i])
-                for i in range(len(self.active) - 1, -1, -1):
-                    if self.active[i]._step >= self.active[i].steps:
-                        self._retire(i, clock())
-                if not self.active:
-                    vtime.pop("ensemble", None)
-                busy = True
-            for i in range(len(self.solo) - 1, -1, -1):
-                r, ctx = self.solo[i]
-                if r.rid in inflight and inflight[r.rid][1].query():
-                    account(r.rid, *inflight.pop(r.rid))
-                    if r._step % r.observe_every == 0 or r._step == r.steps:
-                        self._observe(r, ctx)
-                    if r._step >= r.steps:
-                        self._retire_solo(i, clock())
-                        vtime.pop(r.rid, None)
+        try:
+            while pending or queue or self.active or self.solo:
+                now = clock()
+                if time_box is not None and now >= time_box:
+                    boxed = True
+                    break
+                while pending and pending[0].arrival <= now:
+                    r = pending.pop(0)
+                    if request_bytes(r, self.precision) > self.memory_bytes:
+                        rejected.append(r)
+                    else:
+                        r._inputs = prep.submit(request_inputs, r)  # generated while the GPU works
+                        queue.append(r)
+                busy = False
+                # chunks that ended: account, stream the observables due, retire
+                h0 = time.perf_counter()
+                if "ensemble" in inflight and inflight["ensemble"][1].query():
+                    account("ensemble", *inflight.pop("ensemble"))
+                    for i in range(len(self.active) - 1, -1, -1):
+                        r = self.active[i]
+                        if r._step % r.observe_every == 0 or r._step == r.steps:
+                            self._observe(r, self.ensemble[i])
+                    for i in range(len(self.active) - 1, -1, -1):
+                        if self.active[i]._step >= self.active[i].steps:
+                            self._retire(i, clock())
+                    if not self.active:
+                        vtime.pop("ensemble", None)
                     busy = True
-            host["observe_s"] += time.perf_counter() - h0
-            # admission (into the ensemble only while it has no chunk queued)
-            h0 = time.perf_counter()
-            admitted = []
+                for i in range(len(self.solo) - 1, -1, -1):
+                    r, ctx = self.solo[i]
+                    if r.rid in inflight and inflight[r.rid][1].query():
+                        account(r.rid, *inflight.pop(r.rid))
+                        if r._step % r.observe_every == 0 or r._step == r.steps:
+                            self._observe(r, ctx)
+                        if r._step >= r.steps:
+                            self._retire_solo(i, clock())
+                            vtime.pop(r.rid, None)
+                        busy = True
+                host["observe_s"] += time.perf_counter() - h0
+                # admission (into the ensemble only while it has no chunk queued)
+                h0 = time.perf_counter()
+                admitted = []
 
-            def admit(q):
-                try:
-                    self._admit(q, clock())
-                    admitted.append(q)
-                except OvlError as e:  # set-up failed (device memory, say): the request fails alone
-                    q.error = str(e)
-                    failed.append(q)
+                def admit(q):
+                    try:
+                        self._admit(q, clock())
+                        admitted.append(q)
+                    except OvlError as e:  # set-up failed (device memory, say): the request fails alone
+                        q.error = str(e)
+                        failed.append(q)
 
-            if self.admission == "shortest":
-                queue.sort(key=lambda q: request_cost(q) * q.steps)
-                for q in list(queue):
-                    if fits(q) and ("ensemble" not in inflight or not q.batchable()):
-                        queue.remove(q)
-                        admit(q)
-            else:
-                while queue and fits(queue[0]) and ("ensemble" not in inflight or not queue[0].batchable()):
-                    admit(queue.pop(0))
-            for q in admitted:
-                key = "ensemble" if q.batchable() else q.rid
-                if key not in vtime:
-                    start_group(key)
-                busy = True
-            host["admit_s"] += time.perf_counter() - h0
-            # the next chunks: up to two on the GPU, each for the group with the
-            # least GPU time per request, counting the estimate of a chunk it
-            # has queued; if that group has one queued already, none is added
-            while len(inflight) < 2:
-                groups = [("ensemble", None, self.active)] if self.active else []
-                groups += [(r.rid, ctx, [r]) for r, ctx in self.solo]
-                if not groups:
-                    break
-
-                def projected(g):
-                    v = vtime.get(g[0], 0.0)
-                    if g[0] in inflight:
-                        _, _, k, grp = inflight[g[0]]
-                        v += k * sum(request_cost(r) for r in grp) / (self.rate_wilson * len(grp))
-                    return v
-
-                key, ctx, grp = min(groups, key=projected)
-                if key in inflight:
-                    break
-                if key == "ensemble":
-                    queue_chunk(key, self._ens_stream, self.ensemble.step, self._chunk_steps(grp), list(grp))
+                if self.admission == "shortest":
+                    queue.sort(key=lambda q: request_cost(q) * q.steps)
+                    for q in list(queue):
+                        if fits(q) and ("ensemble" not in inflight or not q.batchable()):
+                            queue.remove(q)
+                            admit(q)
                 else:
-                    queue_chunk(key, ctx.torch_stream, ctx.step, self._chunk_steps(grp), list(grp))
-                busy = True
-            if not busy:
-                host["idle_polls"] += 1
-                if self.active or self.solo:
-                    time.sleep(0.0005)
-                elif pending:
-                    time.sleep(max(0.0, min(0.05, pending[0].arrival - clock())))
-        prep.shutdown(wait=False, cancel_futures=True)
+                    while queue and fits(queue[0]) and ("ensemble" not in inflight or not queue[0].batchable()):
+                        admit(queue.pop(0))
+                for q in admitted:
+                    key = "ensemble" if q.batchable() else q.rid
+                    if key not in vtime:
+                        start_group(key)
+                    busy = True
+                host["admit_s"] += time.perf_counter() - h0
+                # the next chunks: up to two on the GPU, each for the group with the
+                # least GPU time per request, counting the estimate of a chunk it
+                # has queued; if that group has one queued already, none is added
+                while len(inflight) < 2:
+                    groups = [("ensemble", None, self.active)] if self.active else []
+                    groups += [(r.rid, ctx, [r]) for r, ctx in self.solo]
+                    if not groups:
+                        break
+
+                    def projected(g):
+                        v = vtime.get(g[0], 0.0)
+                        if g[0] in inflight:
+                            _, _, k, grp = inflight[g[0]]
+                            v += k * sum(request_cost(r) for r in grp) / (self.rate_wilson * len(grp))
+                        return v
+
+                    key, ctx, grp = min(groups, key=projected)
+                    if key in inflight:
+                        break
+                    if key == "ensemble":
+                        queue_chunk(key, self._ens_stream, self.ensemble.step, self._chunk_steps(grp), list(grp))
+                    else:
+                        queue_chunk(key, ctx.torch_stream, ctx.step, self._chunk_steps(grp), list(grp))
+                    busy = True
+                if not busy:
+                    host["idle_polls"] += 1
+                    if self.active or self.solo:
+                        time.sleep(0.0005)
+                    elif pending:
+                        time.sleep(max(0.0, min(0.05, pending[0].arrival - clock())))
+        finally:
+            prep.shutdown(wait=False, cancel_futures=True)  # also when a step raises
         for r in queue:
             r._inputs = None
         in_flight = len(self.active) + len(self.solo)
