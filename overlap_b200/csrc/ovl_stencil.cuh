@@ -124,6 +124,42 @@ __device__ __forceinline__ Nbrs neighbours(const Lattice &L, int site) {
     return n;
 }
 
+// The six FP64 link matrices of one site's hops, gathered once per CTA in
+// shared memory and reused over the CTA's mode blocks: entries 0..2 the links
+// U_mu(site), 3..5 the links U_mu(site - mu) (the backward hop takes their
+// dagger itself), each as LK delivers it (dressed with the U(1) phase when one
+// is set).  get() is called by the stencil with the site itself for the
+// forward hops and with its backward neighbours, which differ from the site on
+// every lattice the library accepts (N >= 3).
+struct LinksTable {
+    const cmat2<double> *t;
+    int site;
+    template <typename T> __device__ __forceinline__ cmat2<T> get(int s, int mu) const {
+        static_assert(sizeof(T) == 8, "the link table holds FP64 matrices");
+        return t[(s == site ? 0 : 3) + mu];
+    }
+};
+
+// Fills tab[j][dir] for the CTA's sites site_of(j) (j < SITES; a negative
+// site: none) from lk; every thread of the CTA calls it (it holds a barrier).
+template <int SITES, class LK, class SiteOf>
+__device__ __forceinline__ void fill_link_table(const LK &lk, const Lattice &L, const SiteOf &site_of,
+                                                cmat2<double> (*tab)[6]) {
+    const int t = threadIdx.y * kModeBlock + threadIdx.x;
+    if (t < SITES * 6) {
+        const int s = site_of(t / 6), dir = t % 6, mu = dir % 3;
+        if (s >= 0) {
+            int ls = s;
+            if (dir >= 3) {
+                const Nbrs n = neighbours(L, s);
+                ls = mu == 0 ? n.xm : (mu == 1 ? n.ym : n.zm);
+            }
+            tab[t / 6][dir] = lk.template get<double>(ls, mu);
+        }
+    }
+    __syncthreads();
+}
+
 // (D phi)(site) for the 32 modes of block mb (one per lane), before the
 // -i gamma_0 / 2 factor: amass phi(x) - sum of the six projected hops.
 template <typename T, class LK>

@@ -87,25 +87,49 @@ template <typename T, int VARIANT> struct HopOccupancy {
 };
 
 constexpr int kTileX = 4, kTileY = kSitesPerCta / kTileX;  // the (x, y) tile of variant 1
+// Mode blocks a CTA of the FP64 row-tile stencils runs on one gathering of its
+// sites' links (the FP64 variant 0 and the FP40 half steps).
+constexpr int kLinkBlocks = 8;
 
-template <typename T, int MODE, int VARIANT, class LK>
+// MBLK > 1 (FP64, variants 0 and 1): a CTA runs its 8 sites for MBLK mode
+// blocks [MBLK blockIdx.y, ...) of the n_mb, with the sites' links gathered
+// once in shared memory (fill_link_table): the link loads and the U(1)
+// dressing are done once per CTA instead of once per mode block.
+template <typename T, int MODE, int VARIANT, class LK, int MBLK = 1>
 __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, HopOccupancy<T, VARIANT>::kMinBlocks)
-    wilson_tuned_kernel(LK lk, const cpx<T> *__restrict__ src, cpx<T> *__restrict__ dst, Lattice L, T amass, T dt) {
+    wilson_tuned_kernel(LK lk, const cpx<T> *__restrict__ src, cpx<T> *__restrict__ dst, Lattice L, T amass, T dt,
+                        int n_mb = 0) {
     const int lane = threadIdx.x;
-    const int mb = blockIdx.y;
-    int site;
-    if (VARIANT == 1) {
-        const int ntx = (L.N0 + kTileX - 1) / kTileX, nty = (L.N1 + kTileY - 1) / kTileY;
-        const int t = blockIdx.x;
-        const int x = (t % ntx) * kTileX + (int)(threadIdx.y % kTileX);
-        const int y = ((t / ntx) % nty) * kTileY + (int)(threadIdx.y / kTileX);
-        const int z = t / (ntx * nty);
-        if (x >= L.N0 || y >= L.N1) return;
-        site = x + L.N0 * (y + L.N1 * z);
-    } else {
-        site = blockIdx.x * kSitesPerCta + threadIdx.y;
-        if (site >= L.V) return;
+    // the site of warp j of this CTA, or -1
+    auto site_of = [&](int j) {
+        if (VARIANT == 1) {
+            const int ntx = (L.N0 + kTileX - 1) / kTileX, nty = (L.N1 + kTileY - 1) / kTileY;
+            const int t = blockIdx.x;
+            const int x = (t % ntx) * kTileX + j % kTileX;
+            const int y = ((t / ntx) % nty) * kTileY + j / kTileX;
+            const int z = t / (ntx * nty);
+            return x < L.N0 && y < L.N1 ? x + L.N0 * (y + L.N1 * z) : -1;
+        }
+        const int s = blockIdx.x * kSitesPerCta + j;
+        return s < L.V ? s : -1;
+    };
+    const int site = site_of(threadIdx.y);
+    if constexpr (MBLK > 1) {
+        static_assert(VARIANT <= 1 && sizeof(T) == 8, "the link table serves the FP64 tiles");
+        __shared__ cmat2<double> tab[kSitesPerCta][6];
+        fill_link_table<kSitesPerCta>(lk, L, site_of, tab);
+        if (site < 0) return;
+        const LinksTable lt{tab[threadIdx.y], site};
+        const int mb0 = blockIdx.y * MBLK, mb1 = min(n_mb, mb0 + MBLK);
+        for (int mb = mb0; mb < mb1; mb++) {
+            Spinor<T> acc;
+            wilson_site_lk(lt, src, L, site, mb, lane, amass, acc);
+            store_result<T, MODE>(dst, L.V, mb, site, lane, acc, dt);
+        }
+        return;
     }
+    const int mb = blockIdx.y;
+    if (site < 0) return;
     Spinor<T> acc;
     wilson_site_lk(lk, src, L, site, mb, lane, amass, acc);
     store_result<T, MODE>(dst, L.V, mb, site, lane, acc, dt);
@@ -452,7 +476,16 @@ static void launch_variant(int variant, const LK &lk, const cpx<T> *s, cpx<T> *d
     }
     if (variant == 1) {
         const int tiles = ((L.N0 + kTileX - 1) / kTileX) * ((L.N1 + kTileY - 1) / kTileY) * L.N2;
-        wilson_tuned_kernel<T, MODE, 1, LK><<<dim3(tiles, n_mb), block, 0, stream>>>(lk, s, d, L, amass, dt);
+        if constexpr (sizeof(T) == 8)
+            wilson_tuned_kernel<T, MODE, 1, LK, kLinkBlocks>
+                <<<dim3(tiles, (n_mb + kLinkBlocks - 1) / kLinkBlocks), block, 0, stream>>>(lk, s, d, L, amass, dt, n_mb);
+        else
+            wilson_tuned_kernel<T, MODE, 1, LK><<<dim3(tiles, n_mb), block, 0, stream>>>(lk, s, d, L, amass, dt);
+        return;
+    }
+    if constexpr (sizeof(T) == 8) {
+        const dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, (n_mb + kLinkBlocks - 1) / kLinkBlocks);
+        wilson_tuned_kernel<T, MODE, 0, LK, kLinkBlocks><<<grid, block, 0, stream>>>(lk, s, d, L, amass, dt, n_mb);
         return;
     }
     dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
@@ -527,19 +560,14 @@ __device__ __forceinline__ void decode40(const Raw40 &r, Spinor<double> &s) {
 // MINB: CTAs of 8 warps per SM the register allocation must allow (2: 128
 // registers, 3: 80 registers with a few spills); the autotuner picks.
 // OBS: also sum the local charges of src into partial (as wilson_observe_kernel).
-template <int MODE, int MINB, class LK, bool OBS = false>
-__global__ void __launch_bounds__(kModeBlock *kSitesPerCta, MINB)
-    wilson_fp40_kernel(LK lk, const uint2 *__restrict__ src, const uint4 *__restrict__ src_lo, uint2 *__restrict__ dst,
-                       uint4 *__restrict__ dst_lo, Lattice L, double amass, double dt, int n_modes = 0,
-                       int first_mode = 0, double *__restrict__ partial = nullptr) {
+// One site and mode block of the FP40 half step (lane = the mode in the block);
+// OBS: the local charges of src are added into o.
+template <int MODE, bool OBS, class LK>
+__device__ __forceinline__ void fp40_site(const LK &lk, const uint2 *__restrict__ src, const uint4 *__restrict__ src_lo,
+                                          uint2 *__restrict__ dst, uint4 *__restrict__ dst_lo, const Lattice &L,
+                                          int site, int mb, double amass, double dt, int n_modes, int first_mode,
+                                          double (&o)[kObsVals]) {
     const int lane = threadIdx.x;
-    const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
-    const int mb = blockIdx.y;
-    double o[kObsVals] = {0.0, 0.0, 0.0};
-    if (site >= L.V) {
-        if (OBS) cta_partial(o, partial);
-        return;
-    }
     const int V = L.V;
     const Nbrs n = neighbours(L, site);
     Raw40 a, b;
@@ -596,6 +624,35 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, MINB)
             lw[k >> 1] |= pair << (16 * (k & 1));
         }
     dst_lo[((size_t)mb * V + site) * kModeBlock + lane] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+
+// MBLK > 1 (not observing): a CTA runs its 8 sites for MBLK mode blocks
+// [MBLK blockIdx.y, ...) of the n_mb, with the sites' links gathered once in
+// shared memory (fill_link_table) instead of loaded and dressed with the U(1)
+// phase once per mode block.
+template <int MODE, int MINB, class LK, bool OBS = false, int MBLK = 1>
+__global__ void __launch_bounds__(kModeBlock *kSitesPerCta, MINB)
+    wilson_fp40_kernel(LK lk, const uint2 *__restrict__ src, const uint4 *__restrict__ src_lo, uint2 *__restrict__ dst,
+                       uint4 *__restrict__ dst_lo, Lattice L, double amass, double dt, int n_modes = 0,
+                       int first_mode = 0, double *__restrict__ partial = nullptr, int n_mb = 0) {
+    const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
+    double o[kObsVals] = {0.0, 0.0, 0.0};
+    if constexpr (MBLK > 1) {
+        static_assert(!OBS, "the observing half step keeps one mode block per CTA row");
+        __shared__ cmat2<double> tab[kSitesPerCta][6];
+        const int site0 = blockIdx.x * kSitesPerCta;
+        fill_link_table<kSitesPerCta>(lk, L, [&](int j) { return site0 + j < L.V ? site0 + j : -1; }, tab);
+        if (site >= L.V) return;
+        const LinksTable lt{tab[threadIdx.y], site};
+        const int mb0 = blockIdx.y * MBLK, mb1 = min(n_mb, mb0 + MBLK);
+        for (int mb = mb0; mb < mb1; mb++) fp40_site<MODE, false>(lt, src, src_lo, dst, dst_lo, L, site, mb, amass, dt, 0, 0, o);
+        return;
+    }
+    if (site >= L.V) {
+        if (OBS) cta_partial(o, partial);
+        return;
+    }
+    fp40_site<MODE, OBS>(lk, src, src_lo, dst, dst_lo, L, site, blockIdx.y, amass, dt, n_modes, first_mode, o);
     if (OBS) cta_partial(o, partial);
 }
 
@@ -610,15 +667,20 @@ void launch_wilson40(const HopConfig &hc, const void *src, const void *src_lo, v
     uint2 *d = reinterpret_cast<uint2 *>(dst) + (accumulate ? off : 0);
     uint4 *dl = reinterpret_cast<uint4 *>(dst_lo) + (accumulate ? loff : 0);
     dim3 block(kModeBlock, kSitesPerCta);
-    dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
+    dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, (n_mb + kLinkBlocks - 1) / kLinkBlocks);
     const int n01 = L.N0 * L.N1;
     auto go = [&](const auto &lk) {
         using LK = std::decay_t<decltype(lk)>;
         if (accumulate) {
-            if (hc.variant == 1) wilson_fp40_kernel<1, 3, LK><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt);
-            else wilson_fp40_kernel<1, 2, LK><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt);
+            if (hc.variant == 1)
+                wilson_fp40_kernel<1, 3, LK, false, kLinkBlocks><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass,
+                                                                                            dt, 0, 0, nullptr, n_mb);
+            else
+                wilson_fp40_kernel<1, 2, LK, false, kLinkBlocks><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass,
+                                                                                            dt, 0, 0, nullptr, n_mb);
         } else {
-            wilson_fp40_kernel<0, 2, LK><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt);
+            wilson_fp40_kernel<0, 2, LK, false, kLinkBlocks><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt,
+                                                                                        0, 0, nullptr, n_mb);
         }
     };
     if (hc.u1) go(LinksF64<true>{hc.U, reinterpret_cast<const double2 *>(hc.u1), n01});
