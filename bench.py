@@ -762,7 +762,7 @@ def main():
         ctx, fp32 = time_form(wl, head, "fused", K, W, device, profile=True, hop_variant=args.hop_variant,
                                  mode_group=args.mode_group)
     clk = clocks.summary()
-    e2e_steps = max(3, min(K, 20))
+    e2e_steps = max(3, min(K, 60))
     e2e_secs, h2d, d2h, _ = time_e2e(ctx, wl, e2e_steps, device)
     ctx.close()
     del ctx
