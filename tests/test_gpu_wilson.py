@@ -443,6 +443,44 @@ def test_packed_variant_beyond_one_cta_row_of_mode_blocks(form):
                 assert abs(ch[k] - ref[k]) <= 1e-13 * max(1.0, abs(ref[k])), k
 
 
+@pytest.mark.parametrize("precision,form,variant",
+                         [("fp64", "fused", 0), ("fp64", "fused", 1), ("fp64", "plain", 0), ("fp64", "plain", 1),
+                          ("fp40", "fused", 0), ("fp40", "fused", 1)])
+def test_link_table_tiles_on_a_ragged_lattice(precision, form, variant):
+    """The FP64 stencils (variants 0 and 1) and the FP40 half steps gather a
+    CTA's links once in shared memory and run 8 mode blocks on them.  300 modes
+    = 10 mode blocks: the second row of CTAs holds blocks 8 and 9, the last one
+    12 of 32 lanes.  N = (3, 5, 4), V = 60: variant 0's last CTA holds 4 of its
+    8 sites, and variant 1's 4 x 2 tiles stop short in x (3 of 4) and in y (1
+    of 2 on the last row).  With a U(1) background, which the gathered links
+    carry, against the oracle with the same phases."""
+    from overlap_b200.inputs import u1_flux
+
+    N = (3, 5, 4)
+    n = 300
+    U = random_links(N, 0.6, 61)
+    E = random_efield(N, 0.3, 62)
+    psi0 = random_modes(n, N, 63)
+    mid0 = random_modes(n, N, 64)
+    u1 = u1_flux(N, 2)
+    p = oracle_params(N, m=0.1, mdw=0.0, dt=0.05, t_sph=1e9)
+    oracle().orc_set_u1(ptr(np.ascontiguousarray(u1).view(np.float64).ravel()))
+    try:
+        opsi, omid, _, _ = oracle_leapfrog(p, U, E, psi0, mid0, 3)
+    finally:
+        oracle().orc_set_u1(None)
+    bar = tol("fp64") if precision == "fp64" else 1e-7  # FP40: the storage rounding, 2^-29 per write
+    with Context(N=N, n_modes=n, first_mode=1, precision=precision, form=form, m_fermion=0.1, m_dw=0.0, dt=0.05,
+                 t_sphaleron=1e9, hop_variant=variant) as ctx:
+        ctx.set_links(U)
+        ctx.set_efield(E)
+        ctx.set_u1(u1)
+        ctx.set_modes(psi0, mid0)
+        ctx.step(3)
+        psi, mid = ctx.get_modes()
+        assert rel_err(psi, opsi) < bar and rel_err(mid, omid) < bar
+
+
 @pytest.mark.parametrize("group", [4, 9])
 def test_pipelined_step_beyond_one_cta_row_of_mode_blocks(group):
     """The pipelined grouped step (hop variant 3) on 10 mode blocks in groups
