@@ -41,47 +41,83 @@ void chebyshev_inverse_sqrt(int K, double eps, double *c) {
     }
 }
 
-// w = D b (the first half of X = -D^2 / lambda_max), with the links of LK.
-template <typename T, class LK>
-__global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
-    cheb_wilson_kernel(LK lk, const cpx<T> *__restrict__ b, cpx<T> *__restrict__ w, Lattice L, T amass) {
-    const int lane = threadIdx.x;
+// The mode blocks of a CTA's row and the links its warps read.  TABLE (FP64):
+// a CTA runs mblk mode blocks on its sites' links gathered once in shared
+// memory (fill_link_table); otherwise one mode block with LK itself.  Every
+// thread of the CTA calls body(links, site, mb) for each of its mode blocks.
+template <typename T, bool TABLE, class LK, class Body>
+__device__ __forceinline__ void cheb_blocks(const LK &lk, const Lattice &L, int n_mb, int mblk, Body &&body) {
     const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
-    const int mb = blockIdx.y;
-    if (site >= L.V) return;
-    Spinor<T> acc;
-    wilson_site_lk(lk, b, L, site, mb, lane, amass, acc);
-    cpx<T> *o = w + field_index(L.V, mb, site, 0, lane);
+    if constexpr (TABLE) {
+        static_assert(sizeof(T) == 8, "the link table holds FP64 matrices");
+        __shared__ cmat2<double> tab[kSitesPerCta][6];
+        const int site0 = blockIdx.x * kSitesPerCta;
+        fill_link_table<kSitesPerCta>(lk, L, [&](int j) { return site0 + j < L.V ? site0 + j : -1; }, tab);
+        if (site >= L.V) return;
+        const LinksTable lt{tab[threadIdx.y], site};
+        const int mb0 = blockIdx.y * mblk, mb1 = min(n_mb, mb0 + mblk);
+        for (int mb = mb0; mb < mb1; mb++) body(lt, site, mb);
+    } else {
+        if (site >= L.V) return;
+        body(lk, site, (int)blockIdx.y);
+    }
+}
+
+// Launches K<TABLE> on the grid of n_mb mode blocks: in FP64 with mblk =
+// link_blocks(...) mode blocks per CTA when that is more than one.
+template <typename T, class Launch>
+static void cheb_launch(const Lattice &L, int n_mb, Launch &&launch) {
+    const int gx = (L.V + kSitesPerCta - 1) / kSitesPerCta;
+    if constexpr (sizeof(T) == 8) {
+        const int m = link_blocks(gx, n_mb, current_sm_count());
+        if (m > 1) {
+            launch(std::true_type{}, dim3(gx, (n_mb + m - 1) / m), m);
+            return;
+        }
+    }
+    launch(std::false_type{}, dim3(gx, n_mb), 1);
+}
+
+// w = D b (the first half of X = -D^2 / lambda_max), with the links of LK.
+template <typename T, class LK, bool TABLE>
+__global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
+    cheb_wilson_kernel(LK lk, const cpx<T> *__restrict__ b, cpx<T> *__restrict__ w, Lattice L, T amass, int n_mb,
+                       int mblk) {
+    const int lane = threadIdx.x;
+    cheb_blocks<T, TABLE>(lk, L, n_mb, mblk, [&](const auto &links, int site, int mb) {
+        Spinor<T> acc;
+        wilson_site_lk(links, b, L, site, mb, lane, amass, acc);
+        cpx<T> *o = w + field_index(L.V, mb, site, 0, lane);
 #pragma unroll
-    for (int c = 0; c < kColours; c++)
+        for (int c = 0; c < kColours; c++)
 #pragma unroll
-        for (int s = 0; s < kSpin; s++) st(o + (c * kSpin + s) * kModeBlock, finish_component(acc.c[c][s], s));
+            for (int s = 0; s < kSpin; s++) st(o + (c * kSpin + s) * kModeBlock, finish_component(acc.c[c][s], s));
+    });
 }
 
 // b_out = factor * (a * (-D w) + beta * b1) - b2 + ck * phi, per mode and site;
 // -D w is the stencil applied to w (the second half of X = -D^2 / lambda_max).
-template <typename T, class LK>
+template <typename T, class LK, bool TABLE>
 __global__ void __launch_bounds__(kModeBlock *kSitesPerCta)
     clenshaw_kernel(LK lk, const cpx<T> *__restrict__ w, const cpx<T> *__restrict__ b1, const cpx<T> *__restrict__ b2,
                     const cpx<T> *__restrict__ phi, cpx<T> *__restrict__ bout, Lattice L, T amass, T a, T beta,
-                    T factor, T ck) {
+                    T factor, T ck, int n_mb, int mblk) {
     const int lane = threadIdx.x;
-    const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
-    const int mb = blockIdx.y;
-    if (site >= L.V) return;
-    Spinor<T> acc;
-    wilson_site_lk(lk, w, L, site, mb, lane, amass, acc);
-    const size_t base = field_index(L.V, mb, site, 0, lane);
+    cheb_blocks<T, TABLE>(lk, L, n_mb, mblk, [&](const auto &links, int site, int mb) {
+        Spinor<T> acc;
+        wilson_site_lk(links, w, L, site, mb, lane, amass, acc);
+        const size_t base = field_index(L.V, mb, site, 0, lane);
 #pragma unroll
-    for (int c = 0; c < kColours; c++)
+        for (int c = 0; c < kColours; c++)
 #pragma unroll
-        for (int s = 0; s < kSpin; s++) {
-            const size_t i = base + (c * kSpin + s) * kModeBlock;
-            const cpx<T> dw = finish_component(acc.c[c][s], s);
-            const cpx<T> v1 = ld(b1 + i), v2 = ld(b2 + i), f = ld(phi + i);
-            const cpx<T> tx = mk<T>(-a * dw.re + beta * v1.re, -a * dw.im + beta * v1.im);
-            st(bout + i, mk<T>(factor * tx.re - v2.re + ck * f.re, factor * tx.im - v2.im + ck * f.im));
-        }
+            for (int s = 0; s < kSpin; s++) {
+                const size_t i = base + (c * kSpin + s) * kModeBlock;
+                const cpx<T> dw = finish_component(acc.c[c][s], s);
+                const cpx<T> v1 = ld(b1 + i), v2 = ld(b2 + i), f = ld(phi + i);
+                const cpx<T> tx = mk<T>(-a * dw.re + beta * v1.re, -a * dw.im + beta * v1.im);
+                st(bout + i, mk<T>(factor * tx.re - v2.re + ck * f.re, factor * tx.im - v2.im + ck * f.im));
+            }
+    });
 }
 
 // out = M [ -i g0 (1 + m/2) phi + (1 - m/2) dchi ];  dst = out or dst += dt out
@@ -112,8 +148,10 @@ static void d_pass(const LK &lk, const HopConfig &hc, const cpx<T> *b, cpx<T> *w
         launch_wilson_tuned<float>(hc, b, w, L, 0, n_mb, (double)amass, 0.0, false, stream);
         return;
     }
-    cheb_wilson_kernel<T, LK><<<dim3((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb), dim3(kModeBlock, kSitesPerCta), 0,
-                                stream>>>(lk, b, w, L, amass);
+    cheb_launch<T>(L, n_mb, [&](auto table, dim3 grid, int m) {
+        cheb_wilson_kernel<T, LK, decltype(table)::value><<<grid, dim3(kModeBlock, kSitesPerCta), 0, stream>>>(
+            lk, b, w, L, amass, n_mb, m);
+    });
 }
 
 template <typename T, class LK>
@@ -122,7 +160,6 @@ static void cheb_run(const LK &lk, const HopConfig &hc, ChebyshevWork &w, const 
                      double mf, double dt, bool accumulate, int sm_count, cudaStream_t stream, uint64_t *launches) {
     const size_t n = (size_t)n_mb * L.V * kComp * kModeBlock;
     dim3 block(kModeBlock, kSitesPerCta);
-    dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
     const cpx<T> *phi = reinterpret_cast<const cpx<T> *>(src);
     cpx<T> *b[3] = {reinterpret_cast<cpx<T> *>(w.b0), reinterpret_cast<cpx<T> *>(w.b1), reinterpret_cast<cpx<T> *>(w.b2)};
     cpx<T> *tmp = reinterpret_cast<cpx<T> *>(w.w);
@@ -138,9 +175,11 @@ static void cheb_run(const LK &lk, const HopConfig &hc, ChebyshevWork &w, const 
     int i1 = 1, i2 = 2, io = 0;  // b_{k+1}, b_{k+2}, b_k
     for (int k = K; k >= 0; k--) {  // k = 0: y = t(X) b_1 - b_2 + c_0/2 phi (chi, scaled by lambda_max^-1/2)
         d_pass<T>(lk, hc, b[i1], tmp, L, n_mb, am, stream);
-        clenshaw_kernel<T, LK><<<grid, block, 0, stream>>>(lk, tmp, b[i1], b[i2], phi, b[io], L, am, a, beta,
-                                                            (T)(k > 0 ? 2 : 1),
-                                                            (T)((k > 0 ? coeff[k] : 0.5 * coeff[0]) * scale));
+        const T factor = (T)(k > 0 ? 2 : 1), ck = (T)((k > 0 ? coeff[k] : 0.5 * coeff[0]) * scale);
+        cheb_launch<T>(L, n_mb, [&](auto table, dim3 grid, int m) {
+            clenshaw_kernel<T, LK, decltype(table)::value><<<grid, block, 0, stream>>>(
+                lk, tmp, b[i1], b[i2], phi, b[io], L, am, a, beta, factor, ck, n_mb, m);
+        });
         nl += 2;
         const int t = i2;
         i2 = i1;

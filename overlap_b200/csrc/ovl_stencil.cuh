@@ -131,6 +131,28 @@ __device__ __forceinline__ Nbrs neighbours(const Lattice &L, int site) {
 // is set).  get() is called by the stencil with the site itself for the
 // forward hops and with its backward neighbours, which differ from the site on
 // every lattice the library accepts (N >= 3).
+// Mode blocks a CTA of the FP64 stencils runs on one gathering of its sites'
+// links: kLinkBlocks, halved while the grid would hold fewer than 4 CTAs per
+// SM (small lattices or few modes); 1 selects the stencil without the table.
+constexpr int kLinkBlocks = 8;
+inline int link_blocks(int site_ctas, int n_mb, int sm_count) {
+    int m = kLinkBlocks;
+    while (m > 1 && (long long)site_ctas * ((n_mb + m - 1) / m) < 4LL * sm_count) m /= 2;
+    return m;
+}
+// SMs of the current device (cached per device).
+inline int current_sm_count() {
+    static int cache[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+    if (cache[dev] == 0) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cache[dev] = n > 0 ? n : 1;
+    }
+    return cache[dev];
+}
+
 struct LinksTable {
     const cmat2<double> *t;
     int site;

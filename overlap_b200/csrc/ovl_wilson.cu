@@ -87,18 +87,15 @@ template <typename T, int VARIANT> struct HopOccupancy {
 };
 
 constexpr int kTileX = 4, kTileY = kSitesPerCta / kTileX;  // the (x, y) tile of variant 1
-// Mode blocks a CTA of the FP64 row-tile stencils runs on one gathering of its
-// sites' links (the FP64 variant 0 and the FP40 half steps).
-constexpr int kLinkBlocks = 8;
 
-// MBLK > 1 (FP64, variants 0 and 1): a CTA runs its 8 sites for MBLK mode
-// blocks [MBLK blockIdx.y, ...) of the n_mb, with the sites' links gathered
-// once in shared memory (fill_link_table): the link loads and the U(1)
-// dressing are done once per CTA instead of once per mode block.
-template <typename T, int MODE, int VARIANT, class LK, int MBLK = 1>
+// TABLE (FP64, variants 0 and 1): a CTA runs its 8 sites for mblk mode blocks
+// [mblk blockIdx.y, ...) of the n_mb, with the sites' links gathered once in
+// shared memory (fill_link_table): the link loads and the U(1) dressing are
+// done once per CTA instead of once per mode block.
+template <typename T, int MODE, int VARIANT, class LK, bool TABLE = false>
 __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, HopOccupancy<T, VARIANT>::kMinBlocks)
     wilson_tuned_kernel(LK lk, const cpx<T> *__restrict__ src, cpx<T> *__restrict__ dst, Lattice L, T amass, T dt,
-                        int n_mb = 0) {
+                        int n_mb = 0, int mblk = 1) {
     const int lane = threadIdx.x;
     // the site of warp j of this CTA, or -1
     auto site_of = [&](int j) {
@@ -114,13 +111,13 @@ __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, HopOccupancy<T, VARI
         return s < L.V ? s : -1;
     };
     const int site = site_of(threadIdx.y);
-    if constexpr (MBLK > 1) {
+    if constexpr (TABLE) {
         static_assert(VARIANT <= 1 && sizeof(T) == 8, "the link table serves the FP64 tiles");
         __shared__ cmat2<double> tab[kSitesPerCta][6];
         fill_link_table<kSitesPerCta>(lk, L, site_of, tab);
         if (site < 0) return;
         const LinksTable lt{tab[threadIdx.y], site};
-        const int mb0 = blockIdx.y * MBLK, mb1 = min(n_mb, mb0 + MBLK);
+        const int mb0 = blockIdx.y * mblk, mb1 = min(n_mb, mb0 + mblk);
         for (int mb = mb0; mb < mb1; mb++) {
             Spinor<T> acc;
             wilson_site_lk(lt, src, L, site, mb, lane, amass, acc);
@@ -476,19 +473,26 @@ static void launch_variant(int variant, const LK &lk, const cpx<T> *s, cpx<T> *d
     }
     if (variant == 1) {
         const int tiles = ((L.N0 + kTileX - 1) / kTileX) * ((L.N1 + kTileY - 1) / kTileY) * L.N2;
-        if constexpr (sizeof(T) == 8)
-            wilson_tuned_kernel<T, MODE, 1, LK, kLinkBlocks>
-                <<<dim3(tiles, (n_mb + kLinkBlocks - 1) / kLinkBlocks), block, 0, stream>>>(lk, s, d, L, amass, dt, n_mb);
-        else
-            wilson_tuned_kernel<T, MODE, 1, LK><<<dim3(tiles, n_mb), block, 0, stream>>>(lk, s, d, L, amass, dt);
-        return;
-    }
-    if constexpr (sizeof(T) == 8) {
-        const dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, (n_mb + kLinkBlocks - 1) / kLinkBlocks);
-        wilson_tuned_kernel<T, MODE, 0, LK, kLinkBlocks><<<grid, block, 0, stream>>>(lk, s, d, L, amass, dt, n_mb);
+        if constexpr (sizeof(T) == 8) {
+            const int m = link_blocks(tiles, n_mb, current_sm_count());
+            if (m > 1) {
+                wilson_tuned_kernel<T, MODE, 1, LK, true>
+                    <<<dim3(tiles, (n_mb + m - 1) / m), block, 0, stream>>>(lk, s, d, L, amass, dt, n_mb, m);
+                return;
+            }
+        }
+        wilson_tuned_kernel<T, MODE, 1, LK><<<dim3(tiles, n_mb), block, 0, stream>>>(lk, s, d, L, amass, dt);
         return;
     }
     dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
+    if constexpr (sizeof(T) == 8) {
+        const int m = link_blocks(grid.x, n_mb, current_sm_count());
+        if (m > 1) {
+            wilson_tuned_kernel<T, MODE, 0, LK, true>
+                <<<dim3(grid.x, (n_mb + m - 1) / m), block, 0, stream>>>(lk, s, d, L, amass, dt, n_mb, m);
+            return;
+        }
+    }
     wilson_tuned_kernel<T, MODE, 0, LK><<<grid, block, 0, stream>>>(lk, s, d, L, amass, dt);
 }
 
@@ -626,25 +630,25 @@ __device__ __forceinline__ void fp40_site(const LK &lk, const uint2 *__restrict_
     dst_lo[((size_t)mb * V + site) * kModeBlock + lane] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
 }
 
-// MBLK > 1 (not observing): a CTA runs its 8 sites for MBLK mode blocks
-// [MBLK blockIdx.y, ...) of the n_mb, with the sites' links gathered once in
+// TABLE (not observing): a CTA runs its 8 sites for mblk mode blocks
+// [mblk blockIdx.y, ...) of the n_mb, with the sites' links gathered once in
 // shared memory (fill_link_table) instead of loaded and dressed with the U(1)
 // phase once per mode block.
-template <int MODE, int MINB, class LK, bool OBS = false, int MBLK = 1>
+template <int MODE, int MINB, class LK, bool OBS = false, bool TABLE = false>
 __global__ void __launch_bounds__(kModeBlock *kSitesPerCta, MINB)
     wilson_fp40_kernel(LK lk, const uint2 *__restrict__ src, const uint4 *__restrict__ src_lo, uint2 *__restrict__ dst,
                        uint4 *__restrict__ dst_lo, Lattice L, double amass, double dt, int n_modes = 0,
-                       int first_mode = 0, double *__restrict__ partial = nullptr, int n_mb = 0) {
+                       int first_mode = 0, double *__restrict__ partial = nullptr, int n_mb = 0, int mblk = 1) {
     const int site = blockIdx.x * kSitesPerCta + threadIdx.y;
     double o[kObsVals] = {0.0, 0.0, 0.0};
-    if constexpr (MBLK > 1) {
+    if constexpr (TABLE) {
         static_assert(!OBS, "the observing half step keeps one mode block per CTA row");
         __shared__ cmat2<double> tab[kSitesPerCta][6];
         const int site0 = blockIdx.x * kSitesPerCta;
         fill_link_table<kSitesPerCta>(lk, L, [&](int j) { return site0 + j < L.V ? site0 + j : -1; }, tab);
         if (site >= L.V) return;
         const LinksTable lt{tab[threadIdx.y], site};
-        const int mb0 = blockIdx.y * MBLK, mb1 = min(n_mb, mb0 + MBLK);
+        const int mb0 = blockIdx.y * mblk, mb1 = min(n_mb, mb0 + mblk);
         for (int mb = mb0; mb < mb1; mb++) fp40_site<MODE, false>(lt, src, src_lo, dst, dst_lo, L, site, mb, amass, dt, 0, 0, o);
         return;
     }
@@ -667,20 +671,29 @@ void launch_wilson40(const HopConfig &hc, const void *src, const void *src_lo, v
     uint2 *d = reinterpret_cast<uint2 *>(dst) + (accumulate ? off : 0);
     uint4 *dl = reinterpret_cast<uint4 *>(dst_lo) + (accumulate ? loff : 0);
     dim3 block(kModeBlock, kSitesPerCta);
-    dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, (n_mb + kLinkBlocks - 1) / kLinkBlocks);
+    dim3 grid((L.V + kSitesPerCta - 1) / kSitesPerCta, n_mb);
+    const int m = link_blocks(grid.x, n_mb, current_sm_count());
     const int n01 = L.N0 * L.N1;
     auto go = [&](const auto &lk) {
         using LK = std::decay_t<decltype(lk)>;
-        if (accumulate) {
-            if (hc.variant == 1)
-                wilson_fp40_kernel<1, 3, LK, false, kLinkBlocks><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass,
-                                                                                            dt, 0, 0, nullptr, n_mb);
+        if (m > 1) {
+            const dim3 g2(grid.x, (n_mb + m - 1) / m);
+            if (!accumulate)
+                wilson_fp40_kernel<0, 2, LK, false, true><<<g2, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt, 0, 0,
+                                                                                   nullptr, n_mb, m);
+            else if (hc.variant == 1)
+                wilson_fp40_kernel<1, 3, LK, false, true><<<g2, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt, 0, 0,
+                                                                                   nullptr, n_mb, m);
             else
-                wilson_fp40_kernel<1, 2, LK, false, kLinkBlocks><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass,
-                                                                                            dt, 0, 0, nullptr, n_mb);
+                wilson_fp40_kernel<1, 2, LK, false, true><<<g2, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt, 0, 0,
+                                                                                   nullptr, n_mb, m);
+            return;
+        }
+        if (accumulate) {
+            if (hc.variant == 1) wilson_fp40_kernel<1, 3, LK><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt);
+            else wilson_fp40_kernel<1, 2, LK><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt);
         } else {
-            wilson_fp40_kernel<0, 2, LK, false, kLinkBlocks><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt,
-                                                                                        0, 0, nullptr, n_mb);
+            wilson_fp40_kernel<0, 2, LK><<<grid, block, 0, stream>>>(lk, s, sl, d, dl, L, amass, dt);
         }
     };
     if (hc.u1) go(LinksF64<true>{hc.U, reinterpret_cast<const double2 *>(hc.u1), n01});
@@ -739,6 +752,25 @@ void launch_wilson(const double *links, const double *u1, const void *src, void 
     const cpx<T> *s = reinterpret_cast<const cpx<T> *>(src);
     cpx<T> *d = reinterpret_cast<cpx<T> *>(dst);
     const double2 *ph = reinterpret_cast<const double2 *>(u1);
+    if constexpr (sizeof(T) == 8) {
+        // the same site function and store as wilson_kernel, on links gathered once per CTA
+        const int m = link_blocks(grid.x, n_mb, current_sm_count());
+        if (m > 1) {
+            const dim3 g2(grid.x, (n_mb + m - 1) / m);
+            auto go = [&](const auto &lk) {
+                using LK = std::decay_t<decltype(lk)>;
+                if (accumulate)
+                    wilson_tuned_kernel<T, 1, 0, LK, true><<<g2, block, 0, stream>>>(lk, s + off, d + off, L, (T)amass,
+                                                                                    (T)dt, n_mb, m);
+                else
+                    wilson_tuned_kernel<T, 0, 0, LK, true><<<g2, block, 0, stream>>>(lk, s + off, d, L, (T)amass, (T)dt,
+                                                                                    n_mb, m);
+            };
+            if (ph) go(LinksF64<true>{links, ph, L.N0 * L.N1});
+            else go(LinksF64<false>{links, nullptr, L.N0 * L.N1});
+            return;
+        }
+    }
     if (accumulate)
         wilson_kernel<T, 1><<<grid, block, 0, stream>>>(links, ph, s + off, d + off, L, (T)amass, (T)dt);
     else

@@ -270,3 +270,71 @@ def test_overlap_plane_waves_match_reference(precision, sign):
         psi, mid = ctx.get_modes()
     tol = 1e-14 if precision == "fp64" else 1e-7
     assert rel_err(psi, rpsi) < tol and rel_err(mid, rmid) < tol
+
+
+def test_overlap_beyond_one_cta_row_of_mode_blocks():
+    """300 modes = 10 mode blocks (the last 12 of 32 lanes) on N = (4, 5, 5),
+    V = 100, whose last CTA of 8 sites holds 4: the Zolotarev form against the
+    reference's own application on modes of both rows of mode blocks (the
+    stopping rule leaves 3e-11 here), the Chebyshev form (a recurrence per mode)
+    on the last modes against a context that holds only those, and against the
+    reference to the Zolotarev approximation's 1e-6."""
+    N = (4, 5, 5)
+    U = random_links(N, 0.5, 151)
+    R, _ = ref_setup(N, 16, 0, 0.1, 1.0, 1.4, 6.0, 0.05, U, np.zeros((volume(N), 3, 3)))
+    b = np.zeros(2)
+    R.ovlref_ritz_bounds(ptr(b))
+    phis = random_modes(300, N, 152)
+    pick = list(range(0, 256, 51)) + list(range(256, 300, 9))
+    ref = np.zeros((len(pick),) + phis.shape[1:], phis.dtype)
+    for j, i in enumerate(pick):
+        R.ovlref_apply(ptr(np.ascontiguousarray(phis[i]).view(np.float64)), ptr(ref[j].view(np.float64)), b[0], b[1])
+    with Context(N=N, n_modes=300, fermion="overlap", precision="fp64", m_fermion=0.1, r_wilson=1.0, m_dw=1.4,
+                 dt=0.05) as ctx:
+        ctx.set_links(U)
+        ctx.set_spectral_bounds([b])
+        out = ctx.apply(phis)
+        assert ctx.solver_stats()["not_converged"] == 0
+    assert rel_err(out[pick], ref) < 5e-11
+    eps = 0.9 * b[0] / b[1]
+    cheb = dict(fermion="overlap", precision="fp64", sign_method="chebyshev", cheb_degree=200, cheb_eps=eps,
+                m_fermion=0.1, r_wilson=1.0, m_dw=1.4, dt=0.05)
+    with Context(N=N, n_modes=300, **cheb) as ctx:
+        ctx.set_links(U)
+        ctx.set_spectral_bounds([b])
+        outc = ctx.apply(phis)
+    with Context(N=N, n_modes=44, **cheb) as ctx:
+        ctx.set_links(U)
+        ctx.set_spectral_bounds([b])
+        outs = ctx.apply(phis[256:])
+    assert rel_err(outc[256:], outs) < 1e-13
+    assert rel_err(outc[pick], ref) < 1e-6
+
+
+@pytest.mark.parametrize("method", ["zolotarev", "chebyshev"])
+def test_overlap_link_table_mode_blocks_per_cta(method):
+    """In FP64 the stencils of both sign methods run up to 8 mode blocks per CTA
+    on links gathered once in shared memory (fewer while the grid would hold
+    under 4 CTAs per SM).  On N = (7, 7, 7), V = 343, 3400 modes (107 mode
+    blocks) give 8 per CTA on a 148-SM B200, 72 modes one: the last 72 modes of
+    the large context against a context that holds only them.  Each mode's
+    Chebyshev recurrence is its own (1e-13); the multi-shift CG stops each mode
+    by its own residual (1e-11)."""
+    N = (7, 7, 7)
+    U = random_links(N, 0.5, 161)
+    phis = random_modes(3400, N, 162)
+    kw = dict(fermion="overlap", precision="fp64", m_fermion=0.1, r_wilson=1.0, m_dw=1.4, dt=0.05)
+    with Context(N=N, n_modes=1, **kw) as ctx:
+        ctx.set_links(U)
+        b = np.array(ctx.ritz_bounds(phis[0])["bounds"])
+    if method == "chebyshev":
+        kw.update(sign_method="chebyshev", cheb_degree=120, cheb_eps=0.9 * b[0] / b[1])
+    with Context(N=N, n_modes=3400, **kw) as ctx:
+        ctx.set_links(U)
+        ctx.set_spectral_bounds([b])
+        out = ctx.apply(phis)
+    with Context(N=N, n_modes=72, **kw) as ctx:
+        ctx.set_links(U)
+        ctx.set_spectral_bounds([b])
+        sub = ctx.apply(phis[3328:])
+    assert rel_err(out[3328:], sub) < (1e-13 if method == "chebyshev" else 1e-11)

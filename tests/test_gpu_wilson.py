@@ -446,14 +446,11 @@ def test_packed_variant_beyond_one_cta_row_of_mode_blocks(form):
 @pytest.mark.parametrize("precision,form,variant",
                          [("fp64", "fused", 0), ("fp64", "fused", 1), ("fp64", "plain", 0), ("fp64", "plain", 1),
                           ("fp40", "fused", 0), ("fp40", "fused", 1)])
-def test_link_table_tiles_on_a_ragged_lattice(precision, form, variant):
-    """The FP64 stencils (variants 0 and 1) and the FP40 half steps gather a
-    CTA's links once in shared memory and run 8 mode blocks on them.  300 modes
-    = 10 mode blocks: the second row of CTAs holds blocks 8 and 9, the last one
-    12 of 32 lanes.  N = (3, 5, 4), V = 60: variant 0's last CTA holds 4 of its
-    8 sites, and variant 1's 4 x 2 tiles stop short in x (3 of 4) and in y (1
-    of 2 on the last row).  With a U(1) background, which the gathered links
-    carry, against the oracle with the same phases."""
+def test_fp64_fp40_stencils_on_a_ragged_lattice_beyond_one_cta_row(precision, form, variant):
+    """300 modes = 10 mode blocks (the last one 12 of 32 lanes) on N = (3, 5, 4),
+    V = 60: variant 0's last CTA holds 4 of its 8 sites, and variant 1's 4 x 2
+    tiles stop short in x (3 of 4) and in y.  With a U(1) background, against
+    the oracle with the same phases."""
     from overlap_b200.inputs import u1_flux
 
     N = (3, 5, 4)
@@ -479,6 +476,46 @@ def test_link_table_tiles_on_a_ragged_lattice(precision, form, variant):
         ctx.step(3)
         psi, mid = ctx.get_modes()
         assert rel_err(psi, opsi) < bar and rel_err(mid, omid) < bar
+
+
+@pytest.mark.parametrize("n", [40, 960, 3400])
+@pytest.mark.parametrize("precision,form", [("fp64", "fused"), ("fp64", "plain"), ("fp40", "fused")])
+def test_link_table_mode_blocks_per_cta(precision, form, n):
+    """FP64 variants 0 and 1 and the FP40 half steps run up to 8 mode blocks per
+    CTA on links gathered once in shared memory, halving the count while the
+    grid would hold fewer than 4 CTAs per SM, down to 1 (the stencil without
+    the table).  On N = (7, 7, 7), V = 343 (the last CTA of 8 sites holds 7;
+    variant 1's 4 x 2 tiles stop short in x and y), 40, 960 and 3400 modes
+    (2, 30 and 107 mode blocks, the last ones partial) give 1, 2 and 8 mode
+    blocks per CTA on a 148-SM B200.  With a U(1) background, against hop
+    variant 2 (one mode block per CTA, no table, the same arithmetic in the same
+    order): FP64 bit for bit, FP40 to its storage rounding."""
+    from overlap_b200.inputs import u1_flux
+
+    N = (7, 7, 7)
+    U = random_links(N, 0.6, 71)
+    E = random_efield(N, 0.3, 72)
+    psi0 = random_modes(n, N, 73)
+    mid0 = random_modes(n, N, 74)
+    u1 = u1_flux(N, 2)
+
+    def run(prec, variant):
+        with Context(N=N, n_modes=n, first_mode=1, precision=prec, form=form, m_fermion=0.1, m_dw=0.0, dt=0.05,
+                     t_sphaleron=1e9, hop_variant=variant) as ctx:
+            ctx.set_links(U)
+            ctx.set_efield(E)
+            ctx.set_u1(u1)
+            ctx.set_modes(psi0, mid0)
+            ctx.step(3)
+            return ctx.get_modes()
+
+    ref = run("fp64", 2)
+    for variant in (0, 1):
+        psi, mid = run(precision, variant)
+        if precision == "fp64":
+            assert np.array_equal(psi, ref[0]) and np.array_equal(mid, ref[1]), variant
+        else:
+            assert rel_err(psi, ref[0]) < 1e-7 and rel_err(mid, ref[1]) < 1e-7, variant
 
 
 @pytest.mark.parametrize("group", [4, 9])
